@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Krylov-Schur eigensolver on the 3-D 128^3 Laplacian.
+
+Workload (one "step" = one full EPSSolve from the seeded start vector):
+  3-D 7-point Dirichlet Laplacian on a 128^3 grid (n = 2,097,152, 14,581,760
+  nonzeros, FP64 CSR), nev = 32 largest real, ncv = 80, tol = 1e-8, start
+  vector N(0,1) from seed 0.  Metric: seconds until every requested residual
+  is <= 1e-8 (lower is better), plus the HBM bandwidth of the dominant kernel.
+
+  --impl b200       the CUDA library (default)
+  --impl reference  the CPU oracle (a restatement of SLEPc's EPSSolve, which
+                    itself cannot be built here without PETSc) on all host
+                    cores, on a bounded sample of the workload extrapolated
+                    to the full solve.
+
+Multi-GPU (torchrun): every rank solves its own replica (the workload does
+not shard in this build); timings are the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from slepc_b200 import problems as P  # noqa: E402
+
+# Column visits (sum over Lanczos steps j of j+2) of a full solve of this
+# workload, measured by the GPU arm (stats.column_visits); the reference arm
+# uses it to extrapolate its bounded CPU sample to a full solve.
+FULL_SOLVE_COLUMN_VISITS = {128: None}
+
+SPMV_BYTES_PER_NNZ = 12  # 8-byte value + 4-byte column index
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--grid", type=int, default=128)
+    p.add_argument("--nev", type=int, default=32)
+    p.add_argument("--ncv", type=int, default=80)
+    p.add_argument("--cpu-restarts", type=int, default=2, help="restarts in the bounded CPU sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        load = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """Per-launch DRAM traffic of the Gram-Schmidt pass kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "gs_pass_kernel_128cubed.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_algorithmic_byte:"):
+            try:
+                return float(line.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+def workload(grid):
+    csr = P.laplacian_3d(grid)
+    n = len(csr[0]) - 1
+    return csr, n, P.start_vector(n, 0)
+
+
+def config_dict(args, n, nnz, extra=None):
+    d = {"workload": f"3-D 7-point Laplacian {args.grid}^3, nev={args.nev} largest real, ncv={args.ncv}, tol=1e-8, "
+                     "FP64 CSR, Krylov-Schur (CGS+DGKS, thick restart)",
+         "n": n, "nnz": nnz, "nev": args.nev, "ncv": args.ncv, "tol": 1e-8, "start_vector": "N(0,1) seed 0",
+         "l2": "inputs larger than L2: basis V is n x 81 FP64 = %.2f GB, CSR %.0f MB (L2 = 126 MB)"
+               % (n * 81 * 8 / 1e9, (nnz * 12 + (n + 1) * 4) / 1e6),
+         "parallelism": "replicas" if args.gpus > 1 else "single GPU"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+def cpu_sample(csr, v0, args, threads):
+    import oracle
+
+    oracle.set_threads(threads)
+    A = P.to_scipy(csr)
+    t0 = time.perf_counter()
+    r = oracle.eps_solve(A, v0, nev=args.nev, ncv=args.ncv, which=oracle.LARGEST_REAL,
+                         max_restarts=args.cpu_restarts, want_vectors=False)
+    t = time.perf_counter() - t0
+    return t, r
+
+
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return 0
+    csr, n, v0 = workload(args.grid)
+    threads = os.cpu_count() or 1
+    full_visits = FULL_SOLVE_COLUMN_VISITS.get(args.grid)
+    if full_visits is None:
+        print(json.dumps({"impl": "reference", "unavailable": "no full-solve column count recorded for this grid"}))
+        return 0
+    for _ in range(args.warmup):
+        cpu_sample(csr, v0, args, threads)
+    times, visits = [], None
+    for _ in range(args.steps):
+        t, r = cpu_sample(csr, v0, args, threads)
+        times.append(t)
+        visits = r.column_visits
+    per_visit = statistics.mean(times) / visits
+    value = per_visit * full_visits
+    sample = (f"first {args.cpu_restarts} restart(s) of the solve ({visits} Gram-Schmidt column visits, "
+              f"{statistics.mean(times):.1f} s), extrapolated to the {full_visits} column visits of a full solve")
+    line = {"impl": "reference", "metric": "time_to_all_residuals_le_1e-8", "value": value, "unit": "s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": statistics.mean(times) * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (generated 3-D Laplacian, seeded start vector)",
+            "config": config_dict(args, n, int(csr[0][-1])),
+            "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_b200(args):
+    import torch
+
+    import slepc_b200 as S
+
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    csr, n, v0 = workload(args.grid)
+    nnz = int(csr[0][-1])
+    A = S.Mat().createAIJ(csr)
+    E = S.EPS().create()
+    E.setOperators(A)
+    E.setProblemType(S.EPS.ProblemType.HEP)
+    E.setDimensions(args.nev, args.ncv)
+    E.setTolerances(1e-8)
+    E.setWhichEigenpairs(S.LARGEST_REAL)
+    # start vector resident in HBM: the timed region starts with inputs on the device
+    v0_dev = torch.from_numpy(v0).cuda()
+    E.setInitialSpaceDevice(v0_dev.data_ptr())
+
+    for _ in range(args.warmup):
+        E.solve()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    launches0 = S.kernel_launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        E.solve()
+    ev1.record()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = S.kernel_launch_count() - launches0
+    ms_per_step = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+
+    # correctness of what was timed: every requested pair converged, residuals in FP64 on the device
+    nconv = E.getConverged()
+    reason = E.getConvergedReason()
+    resid = [E.computeError(i) for i in range(nconv)]
+    stats = E.getStats()
+
+    # roofline of the dominant kernel (the fused Gram-Schmidt pass): one more solve with per-phase events
+    E.setTiming(True)
+    E.solve()
+    tstats = E.getStats()
+    E.setTiming(False)
+    peak, peak_kind = measured_peaks()
+    gs_gbs = tstats["gs_bytes"] / (tstats["ms_orth"] * 1e-3) / 1e9 if tstats["ms_orth"] > 0 else None
+    spmv_bytes = nnz * SPMV_BYTES_PER_NNZ + (n + 1) * 4 + 2 * n * 8
+    spmv_gbs = (spmv_bytes * tstats["lanczos_steps"] / (tstats["ms_spmv"] * 1e-3) / 1e9
+                if tstats["ms_spmv"] > 0 else None)
+    tr = profiled_traffic()
+
+    # end to end through the one-call host API: host CSR + start vector in, eigenpairs out
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    h_csr = (pin(csr[0]), pin(csr[1]), pin(csr[2]))
+    h_v0 = pin(v0)
+    barrier()
+    t0 = time.perf_counter()
+    e2e_last = None
+    for _ in range(args.steps):
+        e2e_last = S.solve_csr_host(h_csr, h_v0, args.nev, args.ncv, tol=1e-8, which=S.LARGEST_REAL)
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
+    h2d = csr[0].nbytes + csr[1].nbytes + csr[2].nbytes + v0.nbytes
+    d2h = e2e_last["nconv"] * (n * 8 + 16)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        t, r = cpu_sample(csr, v0, args, threads)
+        value = t / r.column_visits * stats["column_visits"]
+        cpu = {"value": value, "unit": "s", "cores": threads, "kind": "port",
+               "sample": (f"first {args.cpu_restarts} restart(s) of the same solve on {threads} host threads "
+                          f"({r.column_visits} Gram-Schmidt column visits in {t:.1f} s), extrapolated to the "
+                          f"{stats['column_visits']} column visits of the full GPU solve")}
+
+    if rank == 0:
+        line = {"metric": "time_to_all_residuals_le_1e-8", "value": ms_per_step / 1e3, "unit": "s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (generated 3-D Laplacian, seeded N(0,1) start vector)",
+                "config": config_dict(args, n, nnz, {
+                    "restarts": stats["restarts"], "lanczos_steps": stats["lanczos_steps"],
+                    "gs_passes": stats["gs_passes"], "column_visits": stats["column_visits"],
+                    "nconv": nconv, "reason": reason, "max_rel_residual": max(resid) if resid else None}),
+                "roofline": {"kernel": "gs_pass_kernel (fused CGS update+dot, DGKS on device)", "bound": "hbm",
+                             "achieved": gs_gbs, "peak": peak, "unit": "GB/s",
+                             "frac": (gs_gbs / peak) if gs_gbs else None,
+                             "peak_kind": peak_kind,
+                             "traffic": (tr * tstats["gs_bytes"] / max(tstats["gs_passes"], 1)) if tr else None,
+                             "spmv_achieved": spmv_gbs, "spmv_frac": (spmv_gbs / peak) if spmv_gbs else None,
+                             "share_orth": tstats["ms_orth"] / tstats["ms_total"] if tstats["ms_total"] else None,
+                             "share_spmv": tstats["ms_spmv"] / tstats["ms_total"] if tstats["ms_total"] else None,
+                             "share_restart": tstats["ms_restart"] / tstats["ms_total"] if tstats["ms_total"] else None},
+                "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+                "gpu_launches": int(launches),
+                "clocks": clk,
+                "cpu_baseline": cpu}
+        print(json.dumps(line))
+    E.destroy()
+    A.destroy()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,219 @@
+/*
+ * slepc_b200.h -- C ABI of the B200-native Krylov-Schur inner loop.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, an explicit CUDA stream
+ * (passed as void*) and an int status.  Every entry point names the SLEPc
+ * interface it replaces (paths relative to the SLEPc 3.22 source tree).
+ *
+ * Three object kinds mirror SLEPc's:
+ *   b200_mat  -- a CSR matrix resident in HBM with a hand-written SpMV
+ *                (the new Mat SpMV type, in place of MATAIJCUSPARSE's MatMult)
+ *   b200_bv   -- a column-major basis of vectors resident in HBM
+ *                (the new BV type: the BVOps table of bvimpl.h:25-61)
+ *   b200_eps  -- the Hermitian Krylov-Schur solver that drives them
+ *                (EPSSolve with EPSKRYLOVSCHUR, problem type EPS_HEP)
+ *
+ * Pointers marked _dev are device (HBM) addresses; pointers marked _host are
+ * host addresses.  All work is ordered on the object's stream; entry points
+ * that return host values synchronise that stream.
+ */
+#ifndef SLEPC_B200_H
+#define SLEPC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (the PetscErrorCode analogue; 0 = success). */
+typedef int b200_status;
+#define B200_OK 0
+#define B200_ERR_ARG 1        /* invalid argument (PETSC_ERR_ARG_OUTOFRANGE / _SIZ / _WRONG) */
+#define B200_ERR_CUDA 2       /* a CUDA runtime call failed */
+#define B200_ERR_LAPACK 3     /* LAPACK returned info != 0 (SlepcCheckLapackInfo) */
+#define B200_ERR_INNER 4      /* invalid inner product (BV_SafeSqrt, bvimpl.h:121-141) */
+#define B200_ERR_BREAKDOWN 5  /* start vector zero or in the deflation space (epssolve.c:864-867) */
+#define B200_ERR_NOMEM 6      /* device allocation failed */
+#define B200_ERR_STATE 7      /* call out of order (e.g. EPSGetEigenpair before EPSSolve) */
+#define B200_ERR_DEVICE 8     /* a kernel reported a device-side error (bounded wait expired, NaN) */
+
+/* Which eigenpairs (EPSWhich, include/slepceps.h; comparators src/sys/slepcsc.c:152-210). */
+#define B200_LARGEST_MAGNITUDE 1
+#define B200_SMALLEST_MAGNITUDE 2
+#define B200_LARGEST_REAL 3
+#define B200_SMALLEST_REAL 4
+
+/* Converged reasons (EPSConvergedReason, include/slepceps.h). */
+#define B200_CONVERGED_TOL 1
+#define B200_CONVERGED_ITERATING 0
+#define B200_DIVERGED_ITS (-1)
+#define B200_DIVERGED_BREAKDOWN (-2)
+
+/* Error types for b200_eps_compute_error (EPSErrorType). */
+#define B200_ERROR_ABSOLUTE 0
+#define B200_ERROR_RELATIVE 1
+
+typedef struct b200_mat_s *b200_mat;
+typedef struct b200_bv_s *b200_bv;
+typedef struct b200_eps_s *b200_eps;
+
+/* Library information and the last error message (thread-local). */
+const char *b200_version(void);
+const char *b200_last_error(void);
+/* Number of kernels this library has launched in this process (all devices). */
+uint64_t b200_kernel_launch_count(void);
+
+/* ------------------------------------------------------------------ Mat --- */
+
+/* Create a square CSR matrix in HBM from host arrays (copied).  Replaces
+ * MatCreateSeqAIJWithArrays + MatSetType(MATAIJCUSPARSE) + MatAssembly, whose
+ * MatMult is called from BVMatMultColumn (src/sys/classes/bv/interface/bvops.c:862-890)
+ * and STApply (src/sys/classes/st/interface/stsolve.c:45-60). */
+b200_status b200_mat_create_csr(int n, int64_t nnz, const int *rowptr_host, const int *colind_host,
+                                const double *vals_host, void *stream, b200_mat *A);
+/* Same, from arrays already in HBM (copied device to device). */
+b200_status b200_mat_create_csr_device(int n, int64_t nnz, const int *rowptr_dev, const int *colind_dev,
+                                       const double *vals_dev, void *stream, b200_mat *A);
+/* y = A x on device vectors (MatMult). */
+b200_status b200_mat_mult(b200_mat A, const double *x_dev, double *y_dev);
+b200_status b200_mat_get_size(b200_mat A, int *n, int64_t *nnz);
+/* Lanes per row chosen for the SpMV (1..32), for tests and reports. */
+b200_status b200_mat_get_lanes(b200_mat A, int *lanes);
+b200_status b200_mat_destroy(b200_mat A);
+
+/* Stateless SpMV on raw device CSR arrays (the kernel behind b200_mat_mult). */
+b200_status b200_csr_spmv(int n, const int *rowptr_dev, const int *colind_dev, const double *vals_dev,
+                          const double *x_dev, double *y_dev, int lanes, void *stream);
+
+/* ------------------------------------------------------------------- BV --- */
+
+/* Create a basis of m columns of length n in HBM (BVCreate + BVSetSizes +
+ * BVSetType, src/sys/classes/bv/interface/bvbasic.c).  Columns are stored
+ * column-major with a leading dimension ld >= n (a multiple of 32). */
+b200_status b200_bv_create(int n, int m, void *stream, b200_bv *bv);
+b200_status b200_bv_destroy(b200_bv bv);
+b200_status b200_bv_get_sizes(b200_bv bv, int *n, int *m, int *ld);
+/* Device address of the storage (BVGetArray, bvimpl.h getarray). */
+b200_status b200_bv_get_array(b200_bv bv, double **V_dev);
+/* BVSetActiveColumns / BVGetActiveColumns (bvbasic.c). */
+b200_status b200_bv_set_active_columns(b200_bv bv, int l, int k);
+b200_status b200_bv_get_active_columns(b200_bv bv, int *l, int *k);
+/* BVSetOrthogonalization eta (bvfunc.c:178 default 0.7071); CGS with refinement if needed. */
+b200_status b200_bv_set_orthog_eta(b200_bv bv, double eta);
+/* Copy a column from/to host memory (BVGetColumn + VecGetArray / VecSetValues). */
+b200_status b200_bv_set_column(b200_bv bv, int j, const double *x_host);
+b200_status b200_bv_get_column(b200_bv bv, int j, double *x_host);
+/* Copy column j to/from a device vector (BVCopyVec / BVInsertVec). */
+b200_status b200_bv_copy_vec(b200_bv bv, int j, double *x_dev);
+b200_status b200_bv_insert_vec(b200_bv bv, int j, const double *x_dev);
+
+/* BVOrthogonalizeColumn (src/sys/classes/bv/interface/bvorthog.c:315-340):
+ * classical Gram-Schmidt against columns 0..j-1 with DGKS refinement "if
+ * needed" (bvorthog.c:145-217).  H_host (nullable) receives j+1 values: the
+ * coefficients and then the norm. */
+b200_status b200_bv_orthogonalize_column(b200_bv bv, int j, double *H_host, double *norm, int *lindep);
+/* BVOrthonormalizeColumn (bvorthog.c:380-427, replace = FALSE): the same,
+ * then column j is scaled by 1/norm. */
+b200_status b200_bv_orthonormalize_column(b200_bv bv, int j, double *norm, int *lindep);
+/* BVOrthogonalizeVec (bvorthog.c:238-262): a device vector against the k active columns. */
+b200_status b200_bv_orthogonalize_vec(b200_bv bv, double *v_dev, double *H_host, double *norm, int *lindep);
+/* BVOrthogonalize with BV_ORTHOG_BLOCK_GS (bvorthog.c:505-560, :726-767):
+ * columns l..k-1 one by one; R_host (nullable, ldr >= k) receives R. */
+b200_status b200_bv_orthogonalize(b200_bv bv, double *R_host, int ldr);
+
+/* BVMultInPlace (bvops.c:220-245; BVMultInPlace_BLAS_CUDA bvcuda.cu:65-112):
+ * V(:,s:e) = V(:,l:k) * Q(l:k,s:e) with the active columns l,k.  Q is a host
+ * column-major matrix with leading dimension ldq (>= k). */
+b200_status b200_bv_mult_inplace(b200_bv bv, const double *Q_host, int ldq, int s, int e);
+/* Same with Q already in HBM. */
+b200_status b200_bv_mult_inplace_device(b200_bv bv, const double *Q_dev, int ldq, int s, int e);
+/* BVMult (bvops.c:47-85): Y(:,ly:ky) = alpha*X(:,lx:kx)*Q(lx:kx,ly:ky) + beta*Y(:,ly:ky). */
+b200_status b200_bv_mult(b200_bv Y, double alpha, double beta, b200_bv X, const double *Q_host, int ldq);
+/* BVMultVec (bvops.c:96-134): y = beta*y + alpha*X(:,l:k)*q, q_host of length k-l. */
+b200_status b200_bv_mult_vec(b200_bv X, double alpha, double beta, double *y_dev, const double *q_host);
+/* BVDot (bvglobal.c): M(ly:ky,lx:kx) = Y(:,ly:ky)^T X(:,lx:kx), M_host column-major ldm. */
+b200_status b200_bv_dot(b200_bv X, b200_bv Y, double *M_host, int ldm);
+/* BVDotVec (bvglobal.c): q = X(:,l:k)^T y, q_host of length k-l. */
+b200_status b200_bv_dot_vec(b200_bv X, const double *y_dev, double *q_host);
+/* BVScaleColumn / BVScale (bvops.c) -- j < 0 scales the active columns. */
+b200_status b200_bv_scale_column(b200_bv bv, int j, double alpha);
+/* BVNormColumn (NORM_2) and BVNorm (NORM_FROBENIUS of the active columns). */
+b200_status b200_bv_norm_column(b200_bv bv, int j, double *nrm);
+b200_status b200_bv_norm(b200_bv bv, double *nrm);
+/* BVCopyColumn (bvops.c): column i <- column j. */
+b200_status b200_bv_copy_column(b200_bv bv, int j, int i);
+/* BVMatMultColumn (bvops.c:862-890): column j+1 <- A * column j. */
+b200_status b200_bv_mat_mult_column(b200_bv bv, b200_mat A, int j);
+/* BVMatLanczos (src/sys/classes/bv/interface/bvkrylov.c:165-226): Lanczos
+ * steps j = k..m-1 with full CGS+DGKS reorthogonalisation.  alpha_host and
+ * beta_host (length >= m) receive T's diagonal and off-diagonal at k..m-1;
+ * on breakdown m is reduced to the step that broke down. */
+b200_status b200_bv_mat_lanczos(b200_bv bv, b200_mat A, int k, int *m, double *alpha_host, double *beta_host,
+                                double *beta, int *breakdown);
+
+/* ------------------------------------------------------------------ EPS --- */
+
+/* EPSCreate + EPSSetType(EPSKRYLOVSCHUR) + EPSSetProblemType(EPS_HEP)
+ * (src/eps/interface/epsbasic.c, src/eps/impls/krylov/krylovschur/krylovschur.c). */
+b200_status b200_eps_create(void *stream, b200_eps *eps);
+b200_status b200_eps_destroy(b200_eps eps);
+/* EPSSetOperators(eps,A,NULL). */
+b200_status b200_eps_set_operators(b200_eps eps, b200_mat A);
+/* EPSSetDimensions (nev, ncv, mpd; ncv/mpd <= 0 take EPSSetDimensions_Default, epssetup.c:669-713). */
+b200_status b200_eps_set_dimensions(b200_eps eps, int nev, int ncv, int mpd);
+/* EPSSetTolerances (tol <= 0 -> 1e-8, slepcmath.h:25; max_it <= 0 -> max(100,2n/ncv), krylovschur.c:113). */
+b200_status b200_eps_set_tolerances(b200_eps eps, double tol, int max_it);
+/* EPSSetWhichEigenpairs (B200_LARGEST_MAGNITUDE ... B200_SMALLEST_REAL). */
+b200_status b200_eps_set_which_eigenpairs(b200_eps eps, int which);
+/* EPSKrylovSchurSetRestart (krylovschur.c:351-361), keep in [0.1,0.9]. */
+b200_status b200_eps_krylovschur_set_restart(b200_eps eps, double keep);
+/* EPSSetInitialSpace with one vector (epssetup.c:613, inserted at setup by BVInsertVecs). */
+b200_status b200_eps_set_initial_space(b200_eps eps, const double *v0_host);
+b200_status b200_eps_set_initial_space_device(b200_eps eps, const double *v0_dev);
+/* Stop after this many restarts (0 = no cap; used to time bounded samples). */
+b200_status b200_eps_set_max_restarts(b200_eps eps, int max_restarts);
+/* EPSSolve (src/eps/interface/epssolve.c:119-229 -> EPSSolve_KrylovSchur_Default, krylovschur.c:227-348). */
+b200_status b200_eps_solve(b200_eps eps);
+b200_status b200_eps_get_converged(b200_eps eps, int *nconv);
+b200_status b200_eps_get_iteration_number(b200_eps eps, int *its);
+b200_status b200_eps_get_converged_reason(b200_eps eps, int *reason);
+/* EPSGetEigenpair (epssolve.c:406): eigenvalue and (nullable) eigenvector copied to the host. */
+b200_status b200_eps_get_eigenpair(b200_eps eps, int i, double *eigr, double *x_host);
+/* Device address of the i-th eigenvector (valid until the next solve). */
+b200_status b200_eps_get_eigenvector_device(b200_eps eps, int i, const double **x_dev);
+/* EPSGetErrorEstimate (epssolve.c) and EPSComputeError (epssolve.c:742-838). */
+b200_status b200_eps_get_error_estimate(b200_eps eps, int i, double *errest);
+b200_status b200_eps_compute_error(b200_eps eps, int i, int type, double *error);
+/* Counters of the last solve: Lanczos steps, Gram-Schmidt passes that did
+ * work, restarts, kernels launched, algorithmic bytes of the Gram-Schmidt
+ * passes, and device time of each kernel family (ms, CUDA events; the
+ * per-family times are 0 unless timing is on). */
+typedef struct {
+  int64_t lanczos_steps;
+  int64_t gs_passes;
+  int64_t restarts;
+  int64_t kernel_launches;
+  double ms_spmv, ms_orth, ms_restart, ms_total;
+  int64_t gs_bytes;
+  int64_t column_visits;  /* sum over Lanczos steps j of (j+2): basis columns one CGS pass reads */
+} b200_eps_stats;
+b200_status b200_eps_get_stats(b200_eps eps, b200_eps_stats *stats);
+/* Enable per-phase CUDA-event timing (adds events around each phase). */
+b200_status b200_eps_set_timing(b200_eps eps, int on);
+
+/* One call from host buffers to host results: create the matrix, solve,
+ * copy eigenvalues (nconv), eigenvectors (n x nconv column-major, nullable)
+ * and error estimates (nullable) back.  info_host[0..4] = nconv, its,
+ * reason, lanczos steps, restarts.  This is the end-to-end entry point that
+ * an EPSSolve caller with host data would bind. */
+b200_status b200_eps_solve_csr_host(int n, int64_t nnz, const int *rowptr_host, const int *colind_host,
+                                    const double *vals_host, const double *v0_host, int nev, int ncv, int mpd,
+                                    double tol, int max_it, int which, double *evals_host, double *X_host,
+                                    double *errest_host, int *info_host, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SLEPC_B200_H */

@@ -1,0 +1,725 @@
+/*
+ * ks_oracle.c -- CPU oracle for the Hermitian Krylov-Schur inner loop.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker that the GPU library is
+ * compared against; it is never linked into the product library.  Only the
+ * tests, the smoke check and the CPU-baseline leg of the benchmark load it.
+ *
+ * It restates, in plain C on the host, the arithmetic of the SLEPc 3.22 path
+ *
+ *   EPSSolve -> EPSSolve_KrylovSchur_Default -> BVMatLanczos ->
+ *   BVOrthonormalizeColumn (CGS + DGKS "if needed") -> DSSolve_HEP_QR ->
+ *   DSSort -> DSUpdateExtraRow -> EPSKrylovConvergence -> DSTruncate ->
+ *   BVMultInPlace -> BVCopyColumn
+ *
+ * with the same order of operations, the same BLAS/LAPACK calls (dgemv,
+ * dgemm, dlartg, drot, dsteqr, dsytrd, dorgtr from the OpenBLAS that ships
+ * with scipy) and the same default parameters.  Each function names the
+ * reference lines it follows (paths relative to the SLEPc source tree).
+ *
+ * Deliberate difference: PETSc's random number generator (used by
+ * BVSetRandomColumn after a Lanczos breakdown) is not part of the SLEPc
+ * tree, so a counter-based splitmix64 uniform [0,1) generator stands in for
+ * it.  The initial vector is always supplied by the caller
+ * (EPSSetInitialSpace semantics, src/eps/interface/epssolve.c:852).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <float.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ---- BLAS / LAPACK from scipy's bundled OpenBLAS (exported with a scipy_ prefix) ---- */
+extern void scipy_dgemv_(const char *, const int *, const int *, const double *, const double *,
+                         const int *, const double *, const int *, const double *, double *, const int *,
+                         size_t);
+extern void scipy_dgemm_(const char *, const char *, const int *, const int *, const int *, const double *,
+                         const double *, const int *, const double *, const int *, const double *, double *,
+                         const int *, size_t, size_t);
+extern void scipy_dlartg_(const double *, const double *, double *, double *, double *);
+extern void scipy_drot_(const int *, double *, const int *, double *, const int *, const double *,
+                        const double *);
+extern void scipy_dsteqr_(const char *, const int *, double *, double *, double *, const int *, double *,
+                          int *, size_t);
+extern void scipy_dsytrd_(const char *, const int *, double *, const int *, double *, double *, double *,
+                          double *, const int *, int *, size_t);
+extern void scipy_dorgtr_(const char *, const int *, double *, const int *, const double *, double *,
+                          const int *, int *, size_t);
+extern void scipy_openblas_set_num_threads(int);
+
+#define ORC_MACHINE_EPS DBL_EPSILON
+
+/* status codes (mirroring the product's b200_status numbering) */
+enum { ORC_OK = 0, ORC_ERR_ARG = 1, ORC_ERR_LAPACK = 3, ORC_ERR_INNER = 4, ORC_ERR_BREAKDOWN = 5 };
+
+/* sorting criteria, src/sys/slepcsc.c:152-210 */
+enum { ORC_LARGEST_MAGNITUDE = 1, ORC_SMALLEST_MAGNITUDE = 2, ORC_LARGEST_REAL = 3, ORC_SMALLEST_REAL = 4 };
+
+/* converged reasons, include/slepceps.h (EPSConvergedReason) */
+enum { ORC_CONVERGED_TOL = 1, ORC_DIVERGED_ITS = -1, ORC_DIVERGED_BREAKDOWN = -2, ORC_ITERATING = 0 };
+
+void oracle_set_threads(int nthreads)
+{
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+  if (nthreads > 0) scipy_openblas_set_num_threads(nthreads);
+}
+
+/* ======================================================================
+ * CSR sparse matrix-vector product y = A x (PETSc MatMult_SeqAIJ semantics:
+ * each row summed in index order).
+ * ====================================================================== */
+void oracle_spmv(int n, const int *rowptr, const int *colind, const double *vals, const double *x, double *y)
+{
+  int i;
+#pragma omp parallel for schedule(static)
+  for (i = 0; i < n; i++) {
+    double s = 0.0;
+    for (int p = rowptr[i]; p < rowptr[i + 1]; p++) s += vals[p] * x[colind[p]];
+    y[i] = s;
+  }
+}
+
+static double nrm2(int n, const double *x)
+{
+  /* plain two-norm; PETSc VecNorm(NORM_2) -> BLASnrm2 */
+  double s = 0.0;
+  int i;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+  for (i = 0; i < n; i++) s += x[i] * x[i];
+  return sqrt(s);
+}
+
+/* counter-based uniform [0,1) generator standing in for PETSc's VecSetRandom */
+static uint64_t splitmix64(uint64_t z)
+{
+  z += 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+double oracle_random_entry(uint64_t seed, uint64_t stream, uint64_t i)
+{
+  uint64_t z = splitmix64(seed ^ splitmix64(stream * 0x100000001B3ULL + i));
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+/* ======================================================================
+ * BV: column-major basis V (n rows, m columns, leading dimension ld) plus
+ * the coefficient buffer of BVGetBufferVec (m x m, column j holds the
+ * Gram-Schmidt coefficients of column j; column 0 doubles as scratch),
+ * src/sys/classes/bv/interface/bvbasic.c:775-790.  No constraints (nc=0).
+ * ====================================================================== */
+typedef struct {
+  int n, m, ld;
+  double *V;
+  double *buf;     /* m*m */
+  double *hvec;    /* scratch for the vector variant */
+  double *cvec;
+  double eta;      /* orthog_eta, bvfunc.c:178 */
+  double deftol;   /* 10*eps, bvfunc.c:184 */
+  uint64_t seed;
+  uint64_t nrand;  /* number of random columns generated so far */
+} obv;
+
+/* BV_SafeSqrt, include/slepc/private/bvimpl.h:121-141 (definite inner product) */
+static int safe_sqrt(const obv *bv, double alpha, double *res)
+{
+  if (!(alpha > -bv->deftol)) return ORC_ERR_INNER;
+  *res = (alpha < 0.0) ? 0.0 : sqrt(alpha);
+  return ORC_OK;
+}
+
+/* BVDotVec_BLAS_Private (bvblas.c:240-261): q = V(:,0:k)^T y via gemv "C" */
+static void bv_dotvec(const obv *bv, int k, const double *y, double *q)
+{
+  const double one = 1.0, zero = 0.0;
+  const int inc = 1;
+  if (k <= 0) return;
+  scipy_dgemv_("C", &bv->n, &k, &one, bv->V, &bv->ld, y, &inc, &zero, q, &inc, 1);
+}
+
+/* BVMultVec_BLAS_Private (bvblas.c:50-66): y = beta*y + alpha*V(:,0:k) q */
+static void bv_multvec(const obv *bv, int k, double alpha, const double *q, double beta, double *y)
+{
+  const int inc = 1;
+  if (k <= 0) return;
+  scipy_dgemv_("N", &bv->n, &k, &alpha, bv->V, &bv->ld, q, &inc, &beta, y, &inc, 1);
+}
+
+/*
+ * BVOrthogonalizeCGS1, bvorthog.c:91-132, for a column (v == NULL) or for an
+ * external vector.  j = number of columns to orthogonalize against (the
+ * column index itself in the column case).  c receives the new coefficients,
+ * h accumulates them (BV_AddCoefficients, bvimpl.h:308-325).
+ */
+static int cgs1(obv *bv, int j, double *v, double *h, double *c, double *onorm, double *norm)
+{
+  double beta = 0.0, sum;
+  int i, st;
+  int col = (v == NULL);
+  double *w = col ? bv->V + (size_t)j * bv->ld : v;
+
+  if (onorm || norm) {
+    if (col) {
+      /* BVDotColumnInc (bvorthog.c:32-47): includes column j against itself */
+      bv_dotvec(bv, j + 1, w, c);
+      if ((st = safe_sqrt(bv, c[j], &beta))) return st;  /* BV_SquareRoot */
+    } else {
+      bv_dotvec(bv, j, w, c);
+      beta = nrm2(bv->n, w);                                /* BVNormVec */
+    }
+  } else {
+    bv_dotvec(bv, j, w, c);
+  }
+  /* q = v - V h (BVMultColumn / BVMultVec) */
+  bv_multvec(bv, j, -1.0, c, 1.0, w);
+  if (onorm) *onorm = beta;
+  if (norm) {
+    /* estimate |v'| from |v| (bvorthog.c:124-127) */
+    sum = 0.0;
+    for (i = 0; i < j; i++) sum += c[i] * c[i];                  /* BV_SquareSum */
+    *norm = beta * beta - sum;
+    if (*norm <= 0.0) *norm = nrm2(bv->n, w);
+    else *norm = sqrt(*norm);
+  }
+  for (i = 0; i < j; i++) h[i] += c[i];                         /* BV_AddCoefficients */
+  return ORC_OK;
+}
+
+/*
+ * BVOrthogonalizeGS with BV_ORTHOG_CGS and BV_ORTHOG_REFINE_IFNEEDED,
+ * bvorthog.c:145-217.  Returns the final norm and the lindep flag; in the
+ * column case stores the norm next to the coefficients (bvorthog.c:209-214).
+ */
+static int orthogonalize_gs(obv *bv, int j, double *v, double *norm, int *lindep)
+{
+  double *h, *c, onrm = 0.0, nrm = 0.0;
+  int l, st, i;
+  if (v) { h = bv->hvec; c = bv->cvec; }
+  else { h = bv->buf + (size_t)j * bv->m; c = bv->buf; /* column 0 = scratch */ }
+  for (i = 0; i < j; i++) h[i] = 0.0;                          /* BV_CleanCoefficients */
+  if ((st = cgs1(bv, j, v, h, c, &onrm, &nrm))) return st;
+  l = 1;
+  while (l < 3 && nrm != 0.0 && fabs(nrm) < bv->eta * fabs(onrm)) {
+    l++;
+    if ((st = cgs1(bv, j, v, h, c, &onrm, &nrm))) return st;
+  }
+  *lindep = !(nrm != 0.0 && fabs(nrm) >= bv->eta * fabs(onrm));
+  if (norm) {
+    *norm = nrm;
+    if (!v) h[j] = (*lindep) ? 0.0 : nrm;                       /* BV_SetValue(bv,k,k,h,...) */
+  }
+  return ORC_OK;
+}
+
+/* BVSetRandomColumn stand-in (bvops.c:360-379) */
+static void set_random_column(obv *bv, int j)
+{
+  double *w = bv->V + (size_t)j * bv->ld;
+  uint64_t stream = bv->nrand++;
+  for (int i = 0; i < bv->n; i++) w[i] = oracle_random_entry(bv->seed, stream, (uint64_t)i);
+}
+
+static void scale_column(obv *bv, int j, double alpha)
+{
+  double *w = bv->V + (size_t)j * bv->ld;
+  int i;
+  if (alpha == 1.0) return;
+#pragma omp parallel for schedule(static)
+  for (i = 0; i < bv->n; i++) w[i] *= alpha;
+}
+
+/* BVOrthonormalizeColumn, bvorthog.c:380-427 (replace = FALSE) */
+static int orthonormalize_column(obv *bv, int j, double *norm, int *lindep)
+{
+  double nrm;
+  int lnd, st;
+  if ((st = orthogonalize_gs(bv, j, NULL, &nrm, &lnd))) return st;
+  if (nrm != 1.0 && nrm != 0.0) scale_column(bv, j, 1.0 / nrm);
+  if (norm) *norm = nrm;
+  if (lindep) *lindep = lnd;
+  return ORC_OK;
+}
+
+/* ======================================================================
+ * DS of type HEP, compact (arrowhead + tridiagonal) storage.
+ * T holds d (diagonal) at T[0..ld) and e (off-diagonal/arrow) at T[ld..2ld);
+ * Q is ld x ld column-major.  src/sys/classes/ds/impls/hep/dshep.c
+ * ====================================================================== */
+typedef struct {
+  int ld, n, l, k, t;
+  int state;     /* 0 RAW, 1 INTERMEDIATE, 2 CONDENSED, 3 TRUNCATED */
+  double *d, *e, *Q, *rwork;
+  int *perm;
+  int which;
+} ods;
+
+/* DSSetIdentity, dspriv.c:407-426: zero columns l..n-1, unit diagonal */
+static void ds_set_identity(ods *ds)
+{
+  memset(ds->Q + (size_t)ds->l * ds->ld, 0, sizeof(double) * (size_t)ds->ld * (ds->n - ds->l));
+  for (int i = ds->l; i < ds->n; i++) ds->Q[i + (size_t)i * ds->ld] = 1.0;
+}
+
+/* DSArrowTridiag, dshep.c:221-265 (Rutishauser's reduction of an arrowhead) */
+static void ds_arrow_tridiag(int n, double *d, double *e, double *Q, int ld)
+{
+  int i, j, j2;
+  const int one = 1;
+  double c, s, p, off, temp;
+  if (n <= 2) return;
+  for (j = 0; j < n - 2; j++) {
+    temp = e[j + 1];
+    scipy_dlartg_(&temp, &e[j], &c, &s, &e[j + 1]);
+    s = -s;
+    temp = d[j + 1];
+    e[j] = c * s * (temp - d[j]);
+    d[j + 1] = s * s * d[j] + c * c * temp;
+    d[j] = c * c * d[j] + s * s * temp;
+    j2 = j + 2;
+    scipy_drot_(&j2, Q + (size_t)j * ld, &one, Q + (size_t)(j + 1) * ld, &one, &c, &s);
+    for (i = j - 1; i >= 0; i--) {
+      off = -s * e[i];
+      e[i] = c * e[i];
+      temp = e[i + 1];
+      scipy_dlartg_(&temp, &off, &c, &s, &e[i + 1]);
+      s = -s;
+      temp = (d[i] - d[i + 1]) * s - 2.0 * c * e[i];
+      p = s * temp;
+      d[i + 1] += p;
+      d[i] -= p;
+      e[i] = -e[i] - c * temp;
+      scipy_drot_(&j2, Q + (size_t)i * ld, &one, Q + (size_t)(i + 1) * ld, &one, &c, &s);
+    }
+  }
+}
+
+/* SlepcCompare* comparators, src/sys/slepcsc.c:152-210 (real case) */
+static int sc_compare(int which, double a, double b)
+{
+  double x, y;
+  switch (which) {
+  case ORC_LARGEST_MAGNITUDE: x = fabs(a); y = fabs(b); return (x < y) ? 1 : (x > y) ? -1 : 0;
+  case ORC_SMALLEST_MAGNITUDE: x = fabs(a); y = fabs(b); return (x > y) ? 1 : (x < y) ? -1 : 0;
+  case ORC_LARGEST_REAL: return (a < b) ? 1 : (a > b) ? -1 : 0;
+  case ORC_SMALLEST_REAL: return (a > b) ? 1 : (a < b) ? -1 : 0;
+  default: return 0;
+  }
+}
+
+/* DSSolve_HEP_QR (compact), dshep.c:383-427 with DSIntermediate_HEP :267-321 */
+static int ds_solve_hep_qr(ods *ds, double *wr)
+{
+  int i, info = 0, n1, ld = ds->ld, l = ds->l, n = ds->n;
+  size_t off = (size_t)l + (size_t)l * ld;
+  int na = ds->k - l + 1;
+  if (na < 0) na = 0;
+  ds_set_identity(ds);
+  if (ds->state < 1) ds_arrow_tridiag(na, ds->d + l, ds->e + l, ds->Q + off, ld);
+  for (i = 0; i < l; i++) wr[i] = ds->d[i];
+  n1 = n - l;
+  if (n1 > 0) scipy_dsteqr_("V", &n1, ds->d + l, ds->e + l, ds->Q + off, &ld, ds->rwork, &info, 1);
+  if (info) return ORC_ERR_LAPACK;
+  for (i = l; i < n; i++) wr[i] = ds->d[i];
+  if (n > 1) memset(ds->e, 0, sizeof(double) * (size_t)(n - 1));
+  ds->state = 2;
+  return ORC_OK;
+}
+
+/* DSSortEigenvaluesReal_Private (dspriv.c:254-273) + DSPermuteColumns_Private (:279-301) + DSSort_HEP (dshep.c:323-347) */
+static void ds_sort_hep(ods *ds, double *wr)
+{
+  int i, j, tmp, result, l = ds->l, n = ds->n, ld = ds->ld, p, k;
+  int *perm = ds->perm;
+  double re, rtmp;
+  for (i = 0; i < n; i++) perm[i] = i;
+  for (i = l + 1; i < ds->t; i++) {
+    re = ds->d[perm[i]];
+    j = i - 1;
+    result = sc_compare(ds->which, re, ds->d[perm[j]]);
+    while (result < 0 && j >= l) {
+      tmp = perm[j]; perm[j] = perm[j + 1]; perm[j + 1] = tmp; j--;
+      if (j >= l) result = sc_compare(ds->which, re, ds->d[perm[j]]);
+    }
+  }
+  for (i = l; i < n; i++) wr[i] = ds->d[perm[i]];
+  for (i = l; i < n; i++) {
+    p = perm[i];
+    if (p != i) {
+      j = i + 1;
+      while (perm[j] != i) j++;
+      perm[j] = p; perm[i] = i;
+      for (k = 0; k < n; k++) {
+        rtmp = ds->Q[k + (size_t)p * ld]; ds->Q[k + (size_t)p * ld] = ds->Q[k + (size_t)i * ld]; ds->Q[k + (size_t)i * ld] = rtmp;
+      }
+    }
+  }
+  for (i = l; i < n; i++) ds->d[i] = wr[i];
+}
+
+/* DSUpdateExtraRow_HEP (compact), dshep.c:349-381 */
+static void ds_update_extra_row(ods *ds)
+{
+  int n = ds->n, ld = ds->ld;
+  double beta = ds->e[n - 1];
+  for (int i = 0; i < n; i++) ds->e[i] = beta * ds->Q[n - 1 + (size_t)i * ld];
+  ds->k = n;
+}
+
+/* DSTruncate_HEP (compact, trim = FALSE), dshep.c:643-671 */
+static void ds_truncate(ods *ds, int n)
+{
+  ds->k = n;        /* extra row present */
+  ds->t = ds->n;
+  ds->n = n;
+  ds->state = 3;
+}
+
+/* ======================================================================
+ * EPS Krylov-Schur (Hermitian, Ritz extraction, locking) solve.
+ * ====================================================================== */
+typedef struct {
+  int nconv, its, reason;
+  long lanczos_steps;   /* total number of SpMV+orthonormalization steps */
+  long gs_passes;       /* total number of CGS passes (DGKS refinements included) */
+  long column_visits;   /* sum over Lanczos steps j of (j+2): basis columns one CGS pass reads */
+  int restarts_done;
+} orc_info;
+
+/* EPSGetStartVector, epssolve.c:841-870 (i > 0 uses a random vector) */
+static int get_start_vector(obv *bv, int i, int *breakdown)
+{
+  double norm;
+  int lindep, st;
+  if (i > 0) set_random_column(bv, i);
+  if ((st = orthogonalize_gs(bv, i, NULL, &norm, &lindep))) return st;
+  if (breakdown) *breakdown = lindep;
+  else if (lindep || norm == 0.0) return ORC_ERR_BREAKDOWN;
+  scale_column(bv, i, 1.0 / norm);
+  return ORC_OK;
+}
+
+/*
+ * oracle_eps_solve: EPSSolve (epssolve.c:119-229) on a Hermitian CSR matrix
+ * with EPSKRYLOVSCHUR defaults.
+ *   which    : ORC_LARGEST_MAGNITUDE ... ORC_SMALLEST_REAL
+ *   v0       : initial vector (EPSSetInitialSpace with one vector)
+ *   ncv, mpd : subspace dimensions (mpd <= 0 means mpd = ncv)
+ *   max_it   : <= 0 means max(100, 2n/ncv), krylovschur.c:113
+ *   max_restarts : > 0 stops after that many restarts (bounded CPU sample;
+ *                  reason stays ITERATING); 0 = run to completion
+ * Outputs: eigr[ncv+1] and errest[ncv+1] in the solver's internal order,
+ * X (n x nconv, ld = n) the converged Ritz vectors sorted by SlepcSortEigenvalues,
+ * evals (nconv) sorted values; info.
+ */
+int oracle_eps_solve(int n, const int *rowptr, const int *colind, const double *vals, const double *v0,
+                     int nev, int ncv, int mpd, double tol, int max_it, int which, int max_restarts,
+                     double *evals, double *X, double *errest_out, int *info_out)
+{
+  obv bv;
+  ods ds;
+  orc_info info;
+  int st = ORC_OK, i, j, k, l, nv, breakdown = 0, lindep, m, nconv_loc;
+  double beta = 0.0, norm, *eigr, *errest;
+  int *perm;
+  const double keep = 0.5;
+
+  memset(&info, 0, sizeof(info));
+  if (n <= 0 || nev <= 0 || ncv <= nev || ncv > n) return ORC_ERR_ARG;
+  if (mpd <= 0) mpd = ncv;
+  if (max_it <= 0) max_it = (2 * n / ncv > 100) ? 2 * n / ncv : 100;
+
+  bv.n = n; bv.m = ncv + 1; bv.ld = n;
+  bv.V = (double *)calloc((size_t)bv.ld * bv.m, sizeof(double));
+  bv.buf = (double *)calloc((size_t)bv.m * bv.m, sizeof(double));
+  bv.hvec = (double *)calloc(bv.m, sizeof(double));
+  bv.cvec = (double *)calloc(bv.m, sizeof(double));
+  bv.eta = 0.7071; bv.deftol = 10 * ORC_MACHINE_EPS; bv.seed = 0x5eedULL; bv.nrand = 0;
+
+  ds.ld = ncv + 1; ds.n = 0; ds.l = 0; ds.k = 0; ds.t = 0; ds.state = 0; ds.which = which;
+  ds.d = (double *)calloc((size_t)3 * ds.ld, sizeof(double));
+  ds.e = ds.d + ds.ld;
+  ds.Q = (double *)calloc((size_t)ds.ld * ds.ld, sizeof(double));
+  ds.rwork = (double *)calloc((size_t)2 * ds.ld + 2, sizeof(double));
+  ds.perm = (int *)calloc(ds.ld, sizeof(int));
+  eigr = (double *)calloc(ds.ld, sizeof(double));
+  errest = (double *)calloc(ds.ld, sizeof(double));
+  perm = (int *)calloc(ds.ld, sizeof(int));
+
+  /* EPSSetUp: BVInsertVecs(V,0,&k,IS,TRUE) (epssetup.c:424, bvfunc.c:331-374) */
+  memcpy(bv.V, v0, sizeof(double) * (size_t)n);
+  if ((st = orthogonalize_gs(&bv, 0, NULL, &norm, &lindep))) goto done;
+  if (norm == 0.0 || lindep) { st = ORC_ERR_BREAKDOWN; goto done; }
+  scale_column(&bv, 0, 1.0 / norm);
+  /* EPSGetStartVector(eps,0,NULL) with nini = 1 */
+  if ((st = get_start_vector(&bv, 0, NULL))) goto done;
+
+  l = 0;
+  info.reason = ORC_ITERATING;
+  while (info.reason == ORC_ITERATING) {
+    info.its++;
+    nv = (info.nconv + mpd < ncv) ? info.nconv + mpd : ncv;
+    /* DSSetDimensions(ds,nv,nconv,nconv+l) */
+    ds.n = nv; ds.t = nv; ds.l = info.nconv; ds.k = info.nconv + l;
+    /* BVMatLanczos(V,Op,T,nconv+l,&nv,&beta,&breakdown), bvkrylov.c:165-226 */
+    k = info.nconv + l;
+    m = nv;
+    breakdown = 0;
+    for (j = k; j < m; j++) {
+      oracle_spmv(n, rowptr, colind, vals, bv.V + (size_t)j * bv.ld, bv.V + (size_t)(j + 1) * bv.ld);
+      if ((st = orthonormalize_column(&bv, j + 1, &beta, &lindep))) goto done;
+      info.lanczos_steps++;
+      info.column_visits += j + 2;
+      if (lindep) { m = j + 1; breakdown = 1; break; }
+    }
+    for (j = k; j < m; j++) {
+      ds.d[j] = bv.buf[j + (size_t)(j + 1) * bv.m];      /* alpha_j */
+      ds.e[j] = bv.buf[j + 1 + (size_t)(j + 1) * bv.m];  /* beta_j */
+    }
+    nv = m;
+    ds.n = nv; ds.t = nv; ds.l = info.nconv; ds.k = info.nconv + l;
+    ds.state = l ? 0 : 1;                                 /* RAW : INTERMEDIATE */
+
+    /* DSSolve + DSSort + DSUpdateExtraRow */
+    if ((st = ds_solve_hep_qr(&ds, eigr))) goto done;
+    ds_sort_hep(&ds, eigr);
+    ds_update_extra_row(&ds);
+
+    /* EPSKrylovConvergence (epskrylov.c:207-295), EPSConvergedRelative (epsdefault.c:224-232) */
+    {
+      int marker = -1, kk;
+      for (kk = info.nconv; kk < nv; kk++) {
+        double re = eigr[kk];
+        double resnorm = fabs(ds.Q[ds.n - 1 + (size_t)kk * ds.ld]) * beta * 1.0;
+        double wabs = fabs(re);
+        errest[kk] = (wabs != 0.0) ? resnorm / wabs : DBL_MAX;
+        if (marker == -1 && errest[kk] >= tol) marker = kk;
+        if (marker != -1) break;
+      }
+      if (marker != -1) kk = marker;
+      k = kk;
+    }
+    /* EPSStoppingBasic, epsdefault.c:290-305 */
+    if (k >= nev) info.reason = ORC_CONVERGED_TOL;
+    else if (info.its >= max_it) info.reason = ORC_DIVERGED_ITS;
+    nconv_loc = k;
+    (void)nconv_loc;
+
+    /* update l (krylovschur.c:290-296) */
+    if (info.reason != ORC_ITERATING || breakdown || k == nv) l = 0;
+    else {
+      l = (int)((nv - k) * keep);
+      if (l < 1) l = 1;
+    }
+
+    if (info.reason == ORC_ITERATING) {
+      if (breakdown || k == nv) {
+        if (k < nev) {
+          int bd = 0;
+          if ((st = get_start_vector(&bv, k, &bd))) goto done;
+          if (bd) info.reason = ORC_DIVERGED_BREAKDOWN;
+        }
+      } else {
+        ds_truncate(&ds, k + l);
+      }
+    }
+    /* BVMultInPlace(V,Q,nconv,k+l) with active columns [nconv,nv) (bvblas.c:74-106, 64-row blocks) */
+    {
+      int s = info.nconv, e = k + l, ncols = e - s, kq = nv - info.nconv, bs = 64, rr;
+      const double one = 1.0, zero = 0.0;
+      if (ncols > 0 && kq > 0) {
+        double *work = (double *)malloc(sizeof(double) * (size_t)bs * ncols);
+        const double *pb = ds.Q + (size_t)info.nconv + (size_t)s * ds.ld;
+        double *A = bv.V + (size_t)info.nconv * bv.ld;
+        int r0 = n % bs;
+        if (r0) {
+          scipy_dgemm_("N", "N", &r0, &ncols, &kq, &one, A, &bv.ld, pb, &ds.ld, &zero, work, &r0, 1, 1);
+          for (j = 0; j < ncols; j++) memcpy(bv.V + (size_t)(s + j) * bv.ld, work + (size_t)j * r0, sizeof(double) * r0);
+        }
+        for (rr = r0; rr < n; rr += bs) {
+          scipy_dgemm_("N", "N", &bs, &ncols, &kq, &one, A + rr, &bv.ld, pb, &ds.ld, &zero, work, &bs, 1, 1);
+          for (j = 0; j < ncols; j++) memcpy(bv.V + (size_t)(s + j) * bv.ld + rr, work + (size_t)j * bs, sizeof(double) * bs);
+        }
+        free(work);
+      }
+    }
+    if (info.reason == ORC_ITERATING && !breakdown) {
+      /* BVCopyColumn(V,nv,k+l) */
+      memcpy(bv.V + (size_t)(k + l) * bv.ld, bv.V + (size_t)nv * bv.ld, sizeof(double) * (size_t)n);
+    }
+    info.nconv = k;
+    info.restarts_done++;
+    if (max_restarts > 0 && info.restarts_done >= max_restarts && info.reason == ORC_ITERATING) break;
+  }
+
+  /* EPSSolve post-processing: SlepcSortEigenvalues (slepcsc.c:89-149, real case) */
+  for (i = 0; i < ncv; i++) perm[i] = i;
+  for (i = info.nconv - 1; i >= 0; i--) {
+    double re = eigr[perm[i]];
+    j = i + 1;
+    while (j < info.nconv) {
+      if (sc_compare(which, re, eigr[perm[j]]) <= 0) break;
+      int tmp = perm[j - 1]; perm[j - 1] = perm[j]; perm[j] = tmp;
+      j++;
+    }
+  }
+  for (i = 0; i < info.nconv; i++) {
+    if (evals) evals[i] = eigr[perm[i]];
+    if (errest_out) errest_out[i] = errest[perm[i]];
+    if (X) memcpy(X + (size_t)i * n, bv.V + (size_t)perm[i] * bv.ld, sizeof(double) * (size_t)n);
+  }
+
+done:
+  if (info_out) {
+    info_out[0] = info.nconv;
+    info_out[1] = info.its;
+    info_out[2] = info.reason;
+    info_out[3] = (int)info.lanczos_steps;
+    info_out[4] = info.restarts_done;
+    info_out[5] = (int)info.column_visits;
+  }
+  free(bv.V); free(bv.buf); free(bv.hvec); free(bv.cvec);
+  free(ds.d); free(ds.Q); free(ds.rwork); free(ds.perm);
+  free(eigr); free(errest); free(perm);
+  return st;
+}
+
+/* ======================================================================
+ * Building blocks exposed for known-answer tests (BV and DS unit level).
+ * ====================================================================== */
+
+/* BVOrthogonalizeColumn (bvorthog.c:315-340) on a caller-owned V (ld x m).
+ * H receives j+1 values (coefficients, then the norm), as BV_StoreCoefficients. */
+int oracle_bv_orthogonalize_column(int n, int m, int ld, double *V, int j, double *H, double *norm, int *lindep)
+{
+  obv bv;
+  int st, lnd = 0;
+  double nrm = 0.0;
+  bv.n = n; bv.m = m; bv.ld = ld; bv.V = V;
+  bv.buf = (double *)calloc((size_t)m * m, sizeof(double));
+  bv.hvec = (double *)calloc(m + 1, sizeof(double));
+  bv.cvec = (double *)calloc(m + 1, sizeof(double));
+  bv.eta = 0.7071; bv.deftol = 10 * ORC_MACHINE_EPS; bv.seed = 0x5eedULL; bv.nrand = 0;
+  st = orthogonalize_gs(&bv, j, NULL, &nrm, &lnd);
+  if (!st && H) for (int i = 0; i <= j; i++) H[i] = bv.buf[i + (size_t)j * m];
+  if (norm) *norm = nrm;
+  if (lindep) *lindep = lnd;
+  free(bv.buf); free(bv.hvec); free(bv.cvec);
+  return st;
+}
+
+/* BVOrthonormalizeColumn (bvorthog.c:380-427): orthogonalize then scale by 1/norm */
+int oracle_bv_orthonormalize_column(int n, int m, int ld, double *V, int j, double *H, double *norm, int *lindep)
+{
+  double nrm = 0.0;
+  int st = oracle_bv_orthogonalize_column(n, m, ld, V, j, H, &nrm, lindep);
+  if (st) return st;
+  if (nrm != 1.0 && nrm != 0.0) {
+    double alpha = 1.0 / nrm;
+    for (int i = 0; i < n; i++) V[i + (size_t)j * ld] *= alpha;
+  }
+  if (norm) *norm = nrm;
+  return ORC_OK;
+}
+
+/* BVOrthogonalizeVec (bvorthog.c:238-262): v against the k active columns of V */
+int oracle_bv_orthogonalize_vec(int n, int k, int ld, const double *V, double *v, double *H, double *norm, int *lindep)
+{
+  obv bv;
+  int st, lnd = 0;
+  double nrm = 0.0;
+  bv.n = n; bv.m = k; bv.ld = ld; bv.V = (double *)V;
+  bv.buf = NULL;
+  bv.hvec = (double *)calloc(k + 1, sizeof(double));
+  bv.cvec = (double *)calloc(k + 1, sizeof(double));
+  bv.eta = 0.7071; bv.deftol = 10 * ORC_MACHINE_EPS; bv.seed = 0x5eedULL; bv.nrand = 0;
+  st = orthogonalize_gs(&bv, k, v, &nrm, &lnd);
+  if (!st && H) for (int i = 0; i < k; i++) H[i] = bv.hvec[i];
+  if (norm) *norm = nrm;
+  if (lindep) *lindep = lnd;
+  free(bv.hvec); free(bv.cvec);
+  return st;
+}
+
+/* BVMultInPlace_BLAS_Private (bvblas.c:74-106): V(:,s:e) = V(:,l:k) * Q(l:k,s:e) */
+int oracle_bv_multinplace(int n, int ld, double *V, int l, int k, const double *Q, int ldq, int s, int e)
+{
+  int ncols = e - s, kq = k - l, bs = 64, rr, j;
+  const double one = 1.0, zero = 0.0;
+  if (ncols <= 0 || kq <= 0 || n <= 0) return ORC_OK;
+  double *work = (double *)malloc(sizeof(double) * (size_t)bs * ncols);
+  const double *pb = Q + (size_t)l + (size_t)s * ldq;
+  double *A = V + (size_t)l * ld;
+  int r0 = n % bs;
+  if (r0) {
+    scipy_dgemm_("N", "N", &r0, &ncols, &kq, &one, A, &ld, pb, &ldq, &zero, work, &r0, 1, 1);
+    for (j = 0; j < ncols; j++) memcpy(V + (size_t)(s + j) * ld, work + (size_t)j * r0, sizeof(double) * r0);
+  }
+  for (rr = r0; rr < n; rr += bs) {
+    scipy_dgemm_("N", "N", &bs, &ncols, &kq, &one, A + rr, &ld, pb, &ldq, &zero, work, &bs, 1, 1);
+    for (j = 0; j < ncols; j++) memcpy(V + (size_t)(s + j) * ld + rr, work + (size_t)j * bs, sizeof(double) * bs);
+  }
+  free(work);
+  return ORC_OK;
+}
+
+/* DSSolve_HEP_QR on a dense symmetric A (non-compact path: sytrd + orgtr + steqr,
+ * dshep.c:289-307 and :383-427) followed by DSSort_HEP.  Outputs sorted wr and Q. */
+int oracle_ds_hep_dense(int n, int ld, const double *A, int which, double *wr, double *Q)
+{
+  int info = 0, lwork = ld * ld, i;
+  double *d = (double *)calloc(ld, sizeof(double)), *e = (double *)calloc(ld, sizeof(double));
+  double *tau = (double *)calloc(ld, sizeof(double)), *work = (double *)calloc((size_t)lwork + 64, sizeof(double));
+  double *rwork = (double *)calloc(2 * ld + 2, sizeof(double));
+  ods ds;
+  int st = ORC_OK;
+  memset(Q, 0, sizeof(double) * (size_t)ld * ld);
+  for (int c = 0; c < n; c++) for (int r = 0; r < n; r++) Q[r + (size_t)c * ld] = A[r + (size_t)c * ld];
+  scipy_dsytrd_("L", &n, Q, &ld, d, e, tau, work, &lwork, &info, 1);
+  if (info) { st = ORC_ERR_LAPACK; goto out; }
+  scipy_dorgtr_("L", &n, Q, &ld, tau, work, &lwork, &info, 1);
+  if (info) { st = ORC_ERR_LAPACK; goto out; }
+  scipy_dsteqr_("V", &n, d, e, Q, &ld, rwork, &info, 1);
+  if (info) { st = ORC_ERR_LAPACK; goto out; }
+  ds.ld = ld; ds.n = n; ds.l = 0; ds.k = 0; ds.t = n; ds.which = which; ds.d = d; ds.e = e; ds.Q = Q;
+  ds.perm = (int *)calloc(ld, sizeof(int));
+  ds_sort_hep(&ds, wr);
+  free(ds.perm);
+  for (i = 0; i < n; i++) wr[i] = d[i];
+out:
+  free(d); free(e); free(tau); free(work); free(rwork);
+  return st;
+}
+
+/* Compact HEP solve of an arrowhead+tridiagonal T (d,e with arrow rows l..k-1),
+ * as used inside Krylov-Schur: DSSolve + DSSort + DSUpdateExtraRow. */
+int oracle_ds_hep_compact(int ld, int n, int l, int k, int raw, int which, double *d, double *e, double *Q, double *wr)
+{
+  ods ds;
+  int st;
+  ds.ld = ld; ds.n = n; ds.l = l; ds.k = k; ds.t = n; ds.state = raw ? 0 : 1; ds.which = which;
+  ds.d = d; ds.e = e; ds.Q = Q;
+  ds.rwork = (double *)calloc(2 * ld + 2, sizeof(double));
+  ds.perm = (int *)calloc(ld, sizeof(int));
+  st = ds_solve_hep_qr(&ds, wr);
+  if (!st) { ds_sort_hep(&ds, wr); ds_update_extra_row(&ds); }
+  free(ds.rwork); free(ds.perm);
+  return st;
+}
+
+/* Relative residual ||A x - lambda x|| / |lambda| (EPSComputeError, epssolve.c:742-838,
+ * EPSComputeResidualNorm_Private :666-722) */
+double oracle_residual(int n, const int *rowptr, const int *colind, const double *vals, const double *x, double lambda)
+{
+  double *u = (double *)malloc(sizeof(double) * (size_t)n), r;
+  oracle_spmv(n, rowptr, colind, vals, x, u);
+  if (fabs(lambda) > ORC_MACHINE_EPS) for (int i = 0; i < n; i++) u[i] -= lambda * x[i];
+  r = nrm2(n, u);
+  free(u);
+  return r / fabs(lambda);
+}

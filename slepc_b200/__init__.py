@@ -1,0 +1,463 @@
+"""B200-native Hermitian Krylov-Schur eigensolver (SLEPc's EPSKRYLOVSCHUR inner loop).
+
+Python mirror of the C ABI in ``include/slepc_b200.h``.  Class and method
+names follow slepc4py (``EPS.setOperators``, ``setProblemType``,
+``setDimensions``, ``setTolerances``, ``setWhichEigenpairs``,
+``setInitialSpace``, ``solve``, ``getConverged``, ``getEigenpair``,
+``computeError`` ...; ``BV.orthogonalizeColumn``, ``multInPlace`` ...), so code
+written against SLEPc reads the same.  Every call goes to the CUDA library
+``libslepc_b200.so``; there is no CPU fallback: if the library or a GPU is
+missing the calls raise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libslepc_b200.so")
+
+# EPSWhich
+LARGEST_MAGNITUDE, SMALLEST_MAGNITUDE, LARGEST_REAL, SMALLEST_REAL = 1, 2, 3, 4
+# EPSConvergedReason
+CONVERGED_TOL, CONVERGED_ITERATING, DIVERGED_ITS, DIVERGED_BREAKDOWN = 1, 0, -1, -2
+# EPSErrorType
+ERROR_ABSOLUTE, ERROR_RELATIVE = 0, 1
+
+_STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "LAPACK error", 4: "invalid inner product",
+           5: "breakdown", 6: "out of device memory", 7: "wrong call order", 8: "device-side error"}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_vp = ctypes.c_void_p
+_lib = None
+
+
+class B200Error(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"slepc_b200: {_STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class EPSStats(ctypes.Structure):
+    _fields_ = [("lanczos_steps", ctypes.c_int64), ("gs_passes", ctypes.c_int64), ("restarts", ctypes.c_int64),
+                ("kernel_launches", ctypes.c_int64), ("ms_spmv", ctypes.c_double), ("ms_orth", ctypes.c_double),
+                ("ms_restart", ctypes.c_double), ("ms_total", ctypes.c_double), ("gs_bytes", ctypes.c_int64),
+                ("column_visits", ctypes.c_int64)]
+
+
+_SIGS = {
+    "b200_version": (ctypes.c_char_p, []),
+    "b200_last_error": (ctypes.c_char_p, []),
+    "b200_kernel_launch_count": (ctypes.c_uint64, []),
+    "b200_mat_create_csr": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, _ip, _ip, _dp, _vp, _vp]),
+    "b200_mat_create_csr_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp]),
+    "b200_mat_mult": (ctypes.c_int, [_vp, _vp, _vp]),
+    "b200_mat_get_size": (ctypes.c_int, [_vp, _ip, ctypes.POINTER(ctypes.c_int64)]),
+    "b200_mat_get_lanes": (ctypes.c_int, [_vp, _ip]),
+    "b200_mat_destroy": (ctypes.c_int, [_vp]),
+    "b200_csr_spmv": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
+    "b200_bv_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "b200_bv_destroy": (ctypes.c_int, [_vp]),
+    "b200_bv_get_sizes": (ctypes.c_int, [_vp, _ip, _ip, _ip]),
+    "b200_bv_get_array": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_void_p)]),
+    "b200_bv_set_active_columns": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    "b200_bv_get_active_columns": (ctypes.c_int, [_vp, _ip, _ip]),
+    "b200_bv_set_orthog_eta": (ctypes.c_int, [_vp, ctypes.c_double]),
+    "b200_bv_set_column": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    "b200_bv_get_column": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    "b200_bv_copy_vec": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
+    "b200_bv_insert_vec": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
+    "b200_bv_orthogonalize_column": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp, _ip]),
+    "b200_bv_orthonormalize_column": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _ip]),
+    "b200_bv_orthogonalize_vec": (ctypes.c_int, [_vp, _vp, _dp, _dp, _ip]),
+    "b200_bv_orthogonalize": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
+    "b200_bv_mult_inplace": (ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "b200_bv_mult_inplace_device": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "b200_bv_mult": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _vp, _dp, ctypes.c_int]),
+    "b200_bv_mult_vec": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _vp, _dp]),
+    "b200_bv_dot": (ctypes.c_int, [_vp, _vp, _dp, ctypes.c_int]),
+    "b200_bv_dot_vec": (ctypes.c_int, [_vp, _vp, _dp]),
+    "b200_bv_scale_column": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double]),
+    "b200_bv_norm_column": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    "b200_bv_norm": (ctypes.c_int, [_vp, _dp]),
+    "b200_bv_copy_column": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    "b200_bv_mat_mult_column": (ctypes.c_int, [_vp, _vp, ctypes.c_int]),
+    "b200_bv_mat_lanczos": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _ip, _dp, _dp, _dp, _ip]),
+    "b200_eps_create": (ctypes.c_int, [_vp, _vp]),
+    "b200_eps_destroy": (ctypes.c_int, [_vp]),
+    "b200_eps_set_operators": (ctypes.c_int, [_vp, _vp]),
+    "b200_eps_set_dimensions": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "b200_eps_set_tolerances": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int]),
+    "b200_eps_set_which_eigenpairs": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_eps_krylovschur_set_restart": (ctypes.c_int, [_vp, ctypes.c_double]),
+    "b200_eps_set_initial_space": (ctypes.c_int, [_vp, _dp]),
+    "b200_eps_set_initial_space_device": (ctypes.c_int, [_vp, _vp]),
+    "b200_eps_set_max_restarts": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_eps_set_timing": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_eps_solve": (ctypes.c_int, [_vp]),
+    "b200_eps_get_converged": (ctypes.c_int, [_vp, _ip]),
+    "b200_eps_get_iteration_number": (ctypes.c_int, [_vp, _ip]),
+    "b200_eps_get_converged_reason": (ctypes.c_int, [_vp, _ip]),
+    "b200_eps_get_eigenpair": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp]),
+    "b200_eps_get_eigenvector_device": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "b200_eps_get_error_estimate": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    "b200_eps_compute_error": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _dp]),
+    "b200_eps_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(EPSStats)]),
+    "b200_eps_solve_csr_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, _ip, _ip, _dp, _dp, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                               ctypes.c_int, _dp, _dp, _dp, _ip, _vp]),
+}
+
+
+def lib():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise B200Error(2, f"{LIB_PATH} is missing: build it with `python slepc_b200/build.py`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    return list(_SIGS.keys())
+
+
+def _check(status):
+    if status != 0:
+        raise B200Error(status, lib().b200_last_error().decode())
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip)
+
+
+def kernel_launch_count():
+    return int(lib().b200_kernel_launch_count())
+
+
+class Mat:
+    """CSR matrix resident in HBM (the new Mat SpMV type)."""
+
+    def __init__(self):
+        self.handle = ctypes.c_void_p()
+        self.n = 0
+        self.nnz = 0
+
+    def createAIJ(self, csr, stream=None):
+        rowptr, colind, vals = csr
+        rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+        colind = np.ascontiguousarray(colind, dtype=np.int32)
+        vals = np.ascontiguousarray(vals, dtype=np.float64)
+        n = len(rowptr) - 1
+        _check(lib().b200_mat_create_csr(n, int(rowptr[-1]), _i(rowptr), _i(colind), _d(vals), stream,
+                                         ctypes.byref(self.handle)))
+        self.n, self.nnz = n, int(rowptr[-1])
+        return self
+
+    def createAIJDevice(self, n, nnz, rowptr_ptr, colind_ptr, vals_ptr, stream=None):
+        _check(lib().b200_mat_create_csr_device(n, nnz, rowptr_ptr, colind_ptr, vals_ptr, stream,
+                                                ctypes.byref(self.handle)))
+        self.n, self.nnz = n, nnz
+        return self
+
+    def mult(self, x_ptr, y_ptr):
+        _check(lib().b200_mat_mult(self.handle, x_ptr, y_ptr))
+
+    def getLanes(self):
+        v = ctypes.c_int()
+        _check(lib().b200_mat_get_lanes(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def destroy(self):
+        if self.handle:
+            lib().b200_mat_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+class BV:
+    """Column-major basis of vectors resident in HBM (the new BV type)."""
+
+    def __init__(self):
+        self.handle = ctypes.c_void_p()
+
+    def create(self, n, m, stream=None):
+        _check(lib().b200_bv_create(n, m, stream, ctypes.byref(self.handle)))
+        return self
+
+    def getSizes(self):
+        n, m, ld = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().b200_bv_get_sizes(self.handle, ctypes.byref(n), ctypes.byref(m), ctypes.byref(ld)))
+        return n.value, m.value, ld.value
+
+    def getArrayPointer(self):
+        p = ctypes.c_void_p()
+        _check(lib().b200_bv_get_array(self.handle, ctypes.byref(p)))
+        return p.value
+
+    def setActiveColumns(self, l, k):
+        _check(lib().b200_bv_set_active_columns(self.handle, l, k))
+
+    def getActiveColumns(self):
+        l, k = ctypes.c_int(), ctypes.c_int()
+        _check(lib().b200_bv_get_active_columns(self.handle, ctypes.byref(l), ctypes.byref(k)))
+        return l.value, k.value
+
+    def setOrthogonalizationEta(self, eta):
+        _check(lib().b200_bv_set_orthog_eta(self.handle, eta))
+
+    def setColumn(self, j, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        _check(lib().b200_bv_set_column(self.handle, j, _d(x)))
+
+    def getColumn(self, j):
+        n = self.getSizes()[0]
+        x = np.empty(n)
+        _check(lib().b200_bv_get_column(self.handle, j, _d(x)))
+        return x
+
+    def setColumns(self, X):
+        for j in range(X.shape[1]):
+            self.setColumn(j, X[:, j])
+
+    def getColumns(self, k=None):
+        n, m, _ = self.getSizes()
+        k = m if k is None else k
+        return np.stack([self.getColumn(j) for j in range(k)], axis=1)
+
+    def orthogonalizeColumn(self, j):
+        """BVOrthogonalizeColumn: returns (H[0..j] with the norm last, norm, lindep)."""
+        H = np.zeros(j + 1)
+        nrm, lnd = ctypes.c_double(), ctypes.c_int()
+        _check(lib().b200_bv_orthogonalize_column(self.handle, j, _d(H), ctypes.byref(nrm), ctypes.byref(lnd)))
+        return H, nrm.value, bool(lnd.value)
+
+    def orthonormalizeColumn(self, j):
+        nrm, lnd = ctypes.c_double(), ctypes.c_int()
+        _check(lib().b200_bv_orthonormalize_column(self.handle, j, ctypes.byref(nrm), ctypes.byref(lnd)))
+        return nrm.value, bool(lnd.value)
+
+    def orthogonalizeVec(self, v_ptr, k):
+        H = np.zeros(max(k, 1))
+        nrm, lnd = ctypes.c_double(), ctypes.c_int()
+        _check(lib().b200_bv_orthogonalize_vec(self.handle, v_ptr, _d(H), ctypes.byref(nrm), ctypes.byref(lnd)))
+        return H[:k], nrm.value, bool(lnd.value)
+
+    def orthogonalize(self, k):
+        R = np.zeros((k, k), order="F")
+        _check(lib().b200_bv_orthogonalize(self.handle, _d(R), k))
+        return R
+
+    def multInPlace(self, Q, s, e):
+        Q = np.asfortranarray(Q, dtype=np.float64)
+        _check(lib().b200_bv_mult_inplace(self.handle, _d(Q), Q.shape[0], s, e))
+
+    def mult(self, alpha, beta, X, Q):
+        Q = np.asfortranarray(Q, dtype=np.float64)
+        _check(lib().b200_bv_mult(self.handle, alpha, beta, X.handle, _d(Q), Q.shape[0]))
+
+    def multVec(self, alpha, beta, y_ptr, q):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        _check(lib().b200_bv_mult_vec(self.handle, alpha, beta, y_ptr, _d(q)))
+
+    def dot(self, Y):
+        """BVDot: M = Y^T X over the active columns (M is Y.k x X.k)."""
+        _, kx = self.getActiveColumns()
+        _, ky = Y.getActiveColumns()
+        M = np.zeros((max(ky, 1), max(kx, 1)), order="F")
+        _check(lib().b200_bv_dot(self.handle, Y.handle, _d(M), max(ky, 1)))
+        return M[:ky, :kx]
+
+    def dotVec(self, y_ptr, k):
+        q = np.zeros(max(k, 1))
+        _check(lib().b200_bv_dot_vec(self.handle, y_ptr, _d(q)))
+        return q[:k]
+
+    def scaleColumn(self, j, alpha):
+        _check(lib().b200_bv_scale_column(self.handle, j, alpha))
+
+    def scale(self, alpha):
+        _check(lib().b200_bv_scale_column(self.handle, -1, alpha))
+
+    def normColumn(self, j):
+        v = ctypes.c_double()
+        _check(lib().b200_bv_norm_column(self.handle, j, ctypes.byref(v)))
+        return v.value
+
+    def norm(self):
+        v = ctypes.c_double()
+        _check(lib().b200_bv_norm(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def copyColumn(self, j, i):
+        _check(lib().b200_bv_copy_column(self.handle, j, i))
+
+    def matMultColumn(self, A, j):
+        _check(lib().b200_bv_mat_mult_column(self.handle, A.handle, j))
+
+    def matLanczos(self, A, k, m):
+        """BVMatLanczos: returns (alpha, beta_vec, m, beta, breakdown)."""
+        mm = ctypes.c_int(m)
+        alpha, betav = np.zeros(m + 1), np.zeros(m + 1)
+        beta, bd = ctypes.c_double(), ctypes.c_int()
+        _check(lib().b200_bv_mat_lanczos(self.handle, A.handle, k, ctypes.byref(mm), _d(alpha), _d(betav),
+                                         ctypes.byref(beta), ctypes.byref(bd)))
+        return alpha, betav, mm.value, beta.value, bool(bd.value)
+
+    def destroy(self):
+        if self.handle:
+            lib().b200_bv_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+class EPS:
+    """Hermitian Krylov-Schur eigensolver (EPSKRYLOVSCHUR with EPS_HEP)."""
+
+    class Which:
+        LARGEST_MAGNITUDE, SMALLEST_MAGNITUDE, LARGEST_REAL, SMALLEST_REAL = 1, 2, 3, 4
+
+    class ProblemType:
+        HEP = 1
+
+    def __init__(self):
+        self.handle = ctypes.c_void_p()
+        self._A = None
+
+    def create(self, stream=None):
+        _check(lib().b200_eps_create(stream, ctypes.byref(self.handle)))
+        return self
+
+    def setOperators(self, A, B=None):
+        if B is not None:
+            raise B200Error(1, "only standard problems (B = None) are supported")
+        self._A = A
+        _check(lib().b200_eps_set_operators(self.handle, A.handle))
+
+    def setProblemType(self, ptype):
+        if ptype != EPS.ProblemType.HEP:
+            raise B200Error(1, "only EPS_HEP is supported")
+
+    def setDimensions(self, nev=1, ncv=0, mpd=0):
+        _check(lib().b200_eps_set_dimensions(self.handle, nev, ncv or 0, mpd or 0))
+
+    def setTolerances(self, tol=0.0, max_it=0):
+        _check(lib().b200_eps_set_tolerances(self.handle, tol or 0.0, max_it or 0))
+
+    def setWhichEigenpairs(self, which):
+        _check(lib().b200_eps_set_which_eigenpairs(self.handle, which))
+
+    def setKrylovSchurRestart(self, keep):
+        _check(lib().b200_eps_krylovschur_set_restart(self.handle, keep))
+
+    def setInitialSpace(self, v0):
+        v0 = np.ascontiguousarray(v0, dtype=np.float64)
+        _check(lib().b200_eps_set_initial_space(self.handle, _d(v0)))
+
+    def setInitialSpaceDevice(self, v0_ptr):
+        _check(lib().b200_eps_set_initial_space_device(self.handle, v0_ptr))
+
+    def setMaxRestarts(self, r):
+        _check(lib().b200_eps_set_max_restarts(self.handle, r))
+
+    def setTiming(self, on):
+        _check(lib().b200_eps_set_timing(self.handle, 1 if on else 0))
+
+    def solve(self):
+        _check(lib().b200_eps_solve(self.handle))
+
+    def getConverged(self):
+        v = ctypes.c_int()
+        _check(lib().b200_eps_get_converged(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def getIterationNumber(self):
+        v = ctypes.c_int()
+        _check(lib().b200_eps_get_iteration_number(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def getConvergedReason(self):
+        v = ctypes.c_int()
+        _check(lib().b200_eps_get_converged_reason(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def getEigenpair(self, i, want_vector=True):
+        lam = ctypes.c_double()
+        x = np.empty(self._A.n) if want_vector else None
+        _check(lib().b200_eps_get_eigenpair(self.handle, i, ctypes.byref(lam), _d(x) if want_vector else None))
+        return (lam.value, x) if want_vector else lam.value
+
+    def getEigenvalue(self, i):
+        return self.getEigenpair(i, want_vector=False)
+
+    def getEigenvectorPointer(self, i):
+        p = ctypes.c_void_p()
+        _check(lib().b200_eps_get_eigenvector_device(self.handle, i, ctypes.byref(p)))
+        return p.value
+
+    def getErrorEstimate(self, i):
+        v = ctypes.c_double()
+        _check(lib().b200_eps_get_error_estimate(self.handle, i, ctypes.byref(v)))
+        return v.value
+
+    def computeError(self, i, etype=ERROR_RELATIVE):
+        v = ctypes.c_double()
+        _check(lib().b200_eps_compute_error(self.handle, i, etype, ctypes.byref(v)))
+        return v.value
+
+    def getStats(self):
+        s = EPSStats()
+        _check(lib().b200_eps_get_stats(self.handle, ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in EPSStats._fields_}
+
+    def destroy(self):
+        if self.handle:
+            lib().b200_eps_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def solve_csr_host(csr, v0, nev, ncv, tol=1e-8, which=LARGEST_MAGNITUDE, mpd=0, max_it=0, want_vectors=True,
+                   stream=None):
+    """One call from host CSR arrays to host eigenpairs (b200_eps_solve_csr_host)."""
+    rowptr, colind, vals = (np.ascontiguousarray(csr[0], dtype=np.int32), np.ascontiguousarray(csr[1], dtype=np.int32),
+                            np.ascontiguousarray(csr[2], dtype=np.float64))
+    n = len(rowptr) - 1
+    v0 = np.ascontiguousarray(v0, dtype=np.float64)
+    evals = np.zeros(ncv + 1)
+    errest = np.zeros(ncv + 1)
+    X = np.zeros((ncv + 1, n)) if want_vectors else None
+    info = np.zeros(8, dtype=np.int32)
+    _check(lib().b200_eps_solve_csr_host(n, int(rowptr[-1]), _i(rowptr), _i(colind), _d(vals), _d(v0), nev, ncv, mpd,
+                                         tol, max_it, which, _d(evals), _d(X) if want_vectors else None, _d(errest),
+                                         _i(info), stream))
+    nconv = int(info[0])
+    return {"evals": evals[:nconv].copy(), "X": X[:nconv].T.copy() if want_vectors else None,
+            "errest": errest[:nconv].copy(), "nconv": nconv, "its": int(info[1]), "reason": int(info[2]),
+            "lanczos_steps": int(info[3]), "restarts": int(info[4])}

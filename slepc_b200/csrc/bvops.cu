@@ -1,0 +1,378 @@
+// Dense tall-skinny BV operations in FP64 for sm_100a.
+//
+//   multinplace  BVMultInPlace   (src/sys/classes/bv/interface/bvops.c:220-245;
+//                                 GPU reference bvcuda.cu:65-112: cudaMalloc of an
+//                                 n x (e-s) temporary, cuBLAS DGEMM, cudaMemcpy2D back)
+//                Here: a persistent row-blocked kernel.  Each CTA keeps Q(l:k,s:e) in
+//                shared memory, loads a 64-row panel of V(:,l:k) into shared memory,
+//                computes the 64 x (e-s) product with a register tile, and writes it
+//                back over V(:,s:e) of the same rows.  Rows are disjoint across CTAs and
+//                a panel is read completely before any of its rows is written, so the
+//                update is safely in place with no temporary.
+//   mult         BVMult          (bvops.c:47-85)
+//   multvec      BVMultVec       (bvops.c:96-134)
+//   dot          BVDot           (bvglobal.c)
+//   sumsq        BVNorm(NORM_2 / NORM_FROBENIUS) building block, deterministic
+//   residual     EPSComputeResidualNorm_Private (src/eps/interface/epssolve.c:666-722):
+//                SpMV fused with r = Ax - lambda x and its sum of squares
+//   random       stand-in for BVSetRandomColumn (bvops.c:360-379)
+#include "common.h"
+#include "kernels.h"
+
+namespace b200 {
+namespace {
+
+constexpr int kRB = 64;        // rows per panel of the in-place GEMM
+constexpr int kGemmThreads = 256;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+// V(:,s:e) = V(:,l:k) * Q(l:k,s:e) ; kq = k-l, nc = e-s; MAXJ = ceil(nc/16) <= 8.
+// Q points at element (l,s) of the coefficient matrix (leading dimension ldq).
+template <int MAXJ>
+__global__ void __launch_bounds__(kGemmThreads) multinplace_kernel(double *V, int ld, int n, int l, int kq,
+                                                                   const double *__restrict__ Q, int ldq, int s,
+                                                                   int nc) {
+  extern __shared__ __align__(16) double sm[];
+  double *Qs = sm;                          // [kq][nc] row-major by c: Qs[c*nc + j]
+  double *As = sm + (size_t)kq * nc;        // [max(kq,nc)][kRB]: input panel As[c*kRB + r], then output tile
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < kq * nc; idx += kGemmThreads) {
+    const int c = idx / nc, j = idx - c * nc;
+    Qs[idx] = Q[(size_t)c + (size_t)j * ldq];
+  }
+  const int cg = tid & 15;   // column group: columns cg + 16*jj
+  const int rg = tid >> 4;   // row group: rows rg + 16*ii
+  const int npanels = (n + kRB - 1) / kRB;
+  for (int pnl = blockIdx.x; pnl < npanels; pnl += gridDim.x) {
+    const long long r0 = (long long)pnl * kRB;
+    const int rows = (int)min((long long)kRB, (long long)n - r0);
+    __syncthreads();
+    for (int idx = tid; idx < kq * kRB; idx += kGemmThreads) {
+      const int c = idx / kRB, r = idx - c * kRB;
+      As[idx] = (r < rows) ? V[(size_t)(l + c) * ld + r0 + r] : 0.0;
+    }
+    __syncthreads();
+    double acc[4][MAXJ];
+#pragma unroll
+    for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < MAXJ; ++jj) acc[ii][jj] = 0.0;
+    for (int c = 0; c < kq; ++c) {
+      double a[4], q[MAXJ];
+#pragma unroll
+      for (int ii = 0; ii < 4; ++ii) a[ii] = As[c * kRB + rg + 16 * ii];
+#pragma unroll
+      for (int jj = 0; jj < MAXJ; ++jj) {
+        const int j = cg + 16 * jj;
+        q[jj] = (j < nc) ? Qs[c * nc + j] : 0.0;
+      }
+#pragma unroll
+      for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+        for (int jj = 0; jj < MAXJ; ++jj) acc[ii][jj] = fma(a[ii], q[jj], acc[ii][jj]);
+    }
+    __syncthreads();  // panel fully consumed: reuse As as the output tile [nc][kRB]
+#pragma unroll
+    for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < MAXJ; ++jj) {
+        const int j = cg + 16 * jj;
+        if (j < nc) As[j * kRB + rg + 16 * ii] = acc[ii][jj];
+      }
+    __syncthreads();
+    for (int idx = tid; idx < nc * kRB; idx += kGemmThreads) {
+      const int j = idx / kRB, r = idx - j * kRB;
+      if (r < rows) V[(size_t)(s + j) * ld + r0 + r] = As[idx];
+    }
+  }
+}
+
+// Y(:,j) = alpha * X(:,0:nx) Q(0:nx,j) + beta * Y(:,j), one thread per row, Q column in registers-free loop.
+__global__ void mult_kernel(double *Y, int ldy, const double *__restrict__ X, int ldx, int n, int nx, int ny,
+                            const double *__restrict__ Q, int ldq, double alpha, double beta) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (r >= n) return;
+  double acc = 0.0;
+  for (int c = 0; c < nx; ++c) acc = fma(X[(size_t)c * ldx + r], Q[c + (size_t)j * ldq], acc);
+  double *y = Y + (size_t)j * ldy + r;
+  *y = (beta == 0.0) ? alpha * acc : alpha * acc + beta * (*y);
+}
+
+__global__ void multvec_kernel(const double *__restrict__ X, int ldx, int n, int k, const double *__restrict__ q,
+                               double alpha, double beta, double *y) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  double acc = 0.0;
+  for (int c = 0; c < k; ++c) acc = fma(X[(size_t)c * ldx + r], q[c], acc);
+  y[r] = (beta == 0.0) ? alpha * acc : beta * y[r] + alpha * acc;
+}
+
+// partial[blk * (nx*ny) + (i + j*ny)] over a persistent row split; one output pair per warp iteration.
+__global__ void dot_partial_kernel(const double *__restrict__ X, int ldx, int nx, const double *__restrict__ Y,
+                                   int ldy, int ny, int n, double *partial) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const long long rows_per = (n + gridDim.x - 1) / gridDim.x;
+  const long long r0 = (long long)blockIdx.x * rows_per;
+  const long long r1 = min((long long)n, r0 + rows_per);
+  const int npairs = nx * ny;
+  for (int pr = warp; pr < npairs; pr += nw) {
+    const int i = pr % ny, j = pr / ny;
+    const double *y = Y + (size_t)i * ldy, *x = X + (size_t)j * ldx;
+    double acc = 0.0;
+    for (long long r = r0 + lane; r < r1; r += 32) acc = fma(y[r], x[r], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) partial[(size_t)blockIdx.x * npairs + pr] = acc;
+  }
+}
+
+__global__ void dot_final_kernel(const double *__restrict__ partial, int nblocks, int nx, int ny, double *M, int ldm) {
+  const int npairs = nx * ny;
+  for (int pr = blockIdx.x * blockDim.x + threadIdx.x; pr < npairs; pr += gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int b = 0; b < nblocks; ++b) acc += partial[(size_t)b * npairs + pr];
+    const int i = pr % ny, j = pr / ny;
+    M[i + (size_t)j * ldm] = acc;
+  }
+}
+
+__global__ void scale_kernel(double *x, long long len, double alpha) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x)
+    x[i] *= alpha;
+}
+
+__global__ void copy_kernel(double *dst, const double *__restrict__ src, long long len) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+__global__ void sumsq_partial_kernel(const double *__restrict__ x, long long len, double *partial) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x)
+    acc = fma(x[i], x[i], acc);
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    partial[blockIdx.x] = s;
+  }
+}
+
+__global__ void sum_final_kernel(const double *__restrict__ partial, int nblocks, double *out) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) acc += partial[b];
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    out[0] = s;
+  }
+}
+
+template <int LPR>
+__global__ void __launch_bounds__(256) residual_partial_kernel(int n, const int *__restrict__ rowptr,
+                                                               const int *__restrict__ colind,
+                                                               const double *__restrict__ vals,
+                                                               const double *__restrict__ x, double lambda,
+                                                               double *partial) {
+  __shared__ double red[8];
+  constexpr int kRowsPerWarp = 32 / LPR;
+  const int lane = threadIdx.x & (LPR - 1);
+  const int sub = (threadIdx.x & 31) / LPR;
+  const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double acc = 0.0;
+  for (long long base = (long long)warp_global * kRowsPerWarp; base < n; base += (long long)nwarps * kRowsPerWarp) {
+    const long long row = base + sub;
+    double sum = 0.0;
+    if (row < n) {
+      const int rs = rowptr[row], re = rowptr[row + 1];
+      for (int p = rs + lane; p < re; p += LPR) sum = fma(vals[p], x[colind[p]], sum);
+    }
+#pragma unroll
+    for (int off = LPR / 2; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off, LPR);
+    if (lane == 0 && row < n) {
+      const double r = sum - lambda * x[row];
+      acc = fma(r, r, acc);
+    }
+  }
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < 8; ++w) s += red[w];
+    partial[blockIdx.x] = s;
+  }
+}
+
+__device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+
+__global__ void random_kernel(double *x, int n, uint64_t seed, uint64_t stream_id) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const uint64_t z = splitmix64(seed ^ splitmix64(stream_id * 0x100000001B3ULL + (uint64_t)i));
+    x[i] = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+  }
+}
+
+int num_sms() {
+  static int cached[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && cached[dev]) return cached[dev];
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+  if (v <= 0) v = 1;
+  if (dev < 64) cached[dev] = v;
+  return v;
+}
+
+unsigned grid_for(long long len, int threads) {
+  long long b = (len + threads - 1) / threads;
+  const long long cap = (long long)num_sms() * 8;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
+}  // namespace
+
+cudaError_t multinplace_launch(double *V, int ld, int n, int l, int k, const double *Q, int ldq, int s, int e,
+                               cudaStream_t stream) {
+  const int kq = k - l, nc = e - s;
+  if (nc <= 0 || kq <= 0 || n <= 0) return cudaSuccess;
+  if (nc > 16 * 8 || kq > kMaxCols) return cudaErrorInvalidValue;
+  const size_t smem = sizeof(double) * ((size_t)kq * nc + (size_t)(kq > nc ? kq : nc) * kRB);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  const int maxj = (nc + 15) / 16;
+  const int npanels = (n + kRB - 1) / kRB;
+  int grid = num_sms() * 2;
+  if (grid > npanels) grid = npanels;
+  cudaError_t err = cudaSuccess;
+  switch (maxj) {
+#define B200_MIP_CASE(J)                                                                                         \
+  case J:                                                                                                        \
+    err = cudaFuncSetAttribute(multinplace_kernel<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024); \
+    if (err != cudaSuccess) return err;                                                                          \
+    multinplace_kernel<J><<<grid, kGemmThreads, smem, stream>>>(V, ld, n, l, kq, Q, ldq, s, nc);                 \
+    break;
+    B200_MIP_CASE(1)
+    B200_MIP_CASE(2)
+    B200_MIP_CASE(3)
+    B200_MIP_CASE(4)
+    B200_MIP_CASE(5)
+    B200_MIP_CASE(6)
+    B200_MIP_CASE(7)
+    B200_MIP_CASE(8)
+#undef B200_MIP_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t mult_launch(double *Y, int ldy, const double *X, int ldx, int n, int nx, int ny, const double *Q, int ldq,
+                        double alpha, double beta, cudaStream_t stream) {
+  if (n <= 0 || ny <= 0) return cudaSuccess;
+  dim3 grid((unsigned)((n + 255) / 256), (unsigned)ny);
+  mult_kernel<<<grid, 256, 0, stream>>>(Y, ldy, X, ldx, n, nx, ny, Q, ldq, alpha, beta);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t multvec_launch(const double *X, int ldx, int n, int k, const double *q, double alpha, double beta, double *y,
+                           cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  multvec_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(X, ldx, n, k, q, alpha, beta, y);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t dot_launch(const double *X, int ldx, int nx, const double *Y, int ldy, int ny, int n, double *M, int ldm,
+                       double *work, int work_len, cudaStream_t stream) {
+  if (nx <= 0 || ny <= 0) return cudaSuccess;
+  const int npairs = nx * ny;
+  int blocks = num_sms();
+  if (blocks * npairs > work_len) blocks = work_len / npairs;
+  if (blocks < 1) return cudaErrorInvalidValue;
+  dot_partial_kernel<<<blocks, 256, 0, stream>>>(X, ldx, nx, Y, ldy, ny, n, work);
+  count_launch();
+  dot_final_kernel<<<(npairs + 255) / 256, 256, 0, stream>>>(work, blocks, nx, ny, M, ldm);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t scale_launch(double *x, long long len, double alpha, cudaStream_t stream) {
+  if (len <= 0) return cudaSuccess;
+  scale_kernel<<<grid_for(len, 256), 256, 0, stream>>>(x, len, alpha);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t copy_launch(double *dst, const double *src, long long len, cudaStream_t stream) {
+  if (len <= 0) return cudaSuccess;
+  copy_kernel<<<grid_for(len, 256), 256, 0, stream>>>(dst, src, len);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t sumsq_launch(const double *x, long long len, double *out, double *work, int work_len, cudaStream_t stream) {
+  int blocks = (int)grid_for(len, 256);
+  if (blocks > work_len) blocks = work_len;
+  sumsq_partial_kernel<<<blocks, 256, 0, stream>>>(x, len, work);
+  count_launch();
+  sum_final_kernel<<<1, 256, 0, stream>>>(work, blocks, out);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t residual_launch(int n, const int *rowptr, const int *colind, const double *vals, const double *x,
+                            double lambda, double *out, double *work, int work_len, int lanes, cudaStream_t stream) {
+  int blocks = num_sms() * 4;
+  if (blocks > work_len) blocks = work_len;
+  switch (lanes) {
+#define B200_RES_CASE(L)                                                                                    \
+  case L:                                                                                                   \
+    residual_partial_kernel<L><<<blocks, 256, 0, stream>>>(n, rowptr, colind, vals, x, lambda, work); \
+    break;
+    B200_RES_CASE(1)
+    B200_RES_CASE(2)
+    B200_RES_CASE(4)
+    B200_RES_CASE(8)
+    B200_RES_CASE(16)
+    B200_RES_CASE(32)
+#undef B200_RES_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+  count_launch();
+  sum_final_kernel<<<1, 256, 0, stream>>>(work, blocks, out);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t random_launch(double *x, int n, uint64_t seed, uint64_t stream_id, cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  random_kernel<<<grid_for(n, 256), 256, 0, stream>>>(x, n, seed, stream_id);
+  count_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace b200

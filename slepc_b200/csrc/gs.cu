@@ -1,0 +1,439 @@
+// Fused classical Gram-Schmidt with DGKS refinement for sm_100a.
+//
+// Replaces the BV Gram-Schmidt path of SLEPc:
+//   BVOrthogonalizeGS (src/sys/classes/bv/interface/bvorthog.c:145-217)
+//   BVOrthogonalizeCGS1 (bvorthog.c:91-132) with BVDotColumnInc (:32-47),
+//   BVMultColumn (bvops.c:165), BV_SquareRoot / BV_SquareSum / BV_AddCoefficients
+//   (include/slepc/private/bvimpl.h:121-141, 289-415)
+// whose GPU form (bvcuda.cu:204-264, 45-60, 420-548) issues a cuBLAS gemv per
+// half-pass plus 2-4 synchronous device-to-host scalar copies per pass.
+//
+// Here one kernel, gs_pass_kernel, performs any combination of
+//   UPDATE  w <- w - V(:,0:jb) coef      (the second half of CGS pass p)
+//   SCALE   w <- w * scale               (BVOrthonormalizeColumn's 1/norm)
+//   DOT     c <- [V(:,0:jb) w', w'^T w'] (the first half of CGS pass p+1)
+// in one streaming read of V: each CTA of a persistent grid (one per SM)
+// pulls row chunks of all jb columns plus w into shared memory with
+// cp.async.bulk copies completing on an mbarrier (two stages, so the next
+// chunk is in flight while the current one is computed), applies the update
+// row-wise and the dot column-wise from shared memory, and accumulates
+// per-CTA column sums.  The last CTA to finish (atomic ticket) reduces the
+// per-CTA sums in a fixed order (deterministic result), then runs the DGKS
+// decision of BVOrthogonalizeGS on the device and writes the action of the
+// next pass.  The host enqueues a fixed sequence of passes without waiting;
+// passes the device decides against return immediately.
+//
+// A CGS pass of the reference reads V twice (dot, then update); fusing the
+// update of pass p with the dot of pass p+1 reads V three times per column
+// with one DGKS refinement instead of four, and no host round trip.
+#include "common.h"
+#include "kernels.h"
+
+namespace b200 {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kStages = 2;
+constexpr size_t kStageBudget = 100 * 1024;  // bytes of one pipeline stage
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n"
+      " .reg .pred p;\n"
+      " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n"
+      "}\n"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Bounded wait: returns false if the phase did not complete within kSpinLimit polls.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  for (long long it = 0; it < kSpinLimit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+struct PassParams {
+  GsPassArgs a;
+  GsState *st;
+  double *coef;
+  double *cnew;
+  double *partials;
+  int first;       // first pass of a column: action = DOT, coefficients start from zero
+  int plain_dot;   // plain BVDotVec: DOT only, no decision
+  int chunk;       // rows per chunk (multiple of 32)
+  int nchunks;
+  int G;           // CTAs in the grid
+};
+
+// Shared scalars of the decision step.
+struct DecideShared {
+  int stage, pass, action, cont, lindep, err;
+  double onrm, nrm, scale;
+  double red[kWarps];
+};
+
+// BVOrthogonalizeGS's "finish a pass" logic (bvorthog.c:176-187, 209-214), run by thread 0.
+__device__ void finish_pass(DecideShared &d, const PassParams &p, double onrm, double nrm, bool have_next) {
+  const GsState *st = p.st;
+  const GsPassArgs &a = p.a;
+  const bool refine = d.pass < 3 && nrm != 0.0 && fabs(nrm) < st->eta * fabs(onrm);
+  if (refine) {
+    if (have_next) {
+      // The dot just reduced is already the dot of the next pass.
+      d.stage = kStageDotOfPass;
+      d.cont = 1;
+    } else {
+      d.action = kActUpdate | kActDot;
+      d.stage = kStageDotOfPass;
+      d.cont = 0;
+    }
+    return;
+  }
+  const int lindep = !(nrm != 0.0 && fabs(nrm) >= st->eta * fabs(onrm));
+  d.lindep = lindep;
+  d.nrm = nrm;
+  d.scale = (a.normalize && nrm != 1.0 && nrm != 0.0) ? 1.0 / nrm : 1.0;
+  d.action = (have_next ? 0 : kActUpdate) | (d.scale != 1.0 ? kActScale : 0);
+  d.stage = kStageDone;
+  d.cont = 0;
+  if (a.hacc) a.hacc[a.jb] = lindep ? 0.0 : nrm;  // BV_SetValue(bv,k,k,h,...)
+  if (a.T) {
+    a.T[a.step] = (a.jb > 0) ? a.hacc[a.jb - 1] : 0.0;
+    a.T[a.ldt + a.step] = lindep ? 0.0 : nrm;
+  }
+}
+
+// DGKS decision on the reduced dot (cnew_s), run by the whole last CTA.
+__device__ void decide(const PassParams &p, const double *cnew_s, DecideShared &d) {
+  const GsPassArgs &a = p.a;
+  GsState *st = p.st;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    d.stage = p.first ? kStageDotOfPass : st->stage;
+    d.pass = p.first ? 0 : st->pass;
+    d.onrm = st->onrm;
+    d.action = kActNone;
+    d.lindep = 0;
+    d.err = 0;
+    d.nrm = 0.0;
+    d.scale = 1.0;
+  }
+  __syncthreads();
+  bool fresh = p.first != 0;
+  for (int iter = 0; iter < 4; ++iter) {
+    if (d.stage == kStageDotOfPass) {
+      // Coefficients of this pass: applied by the next UPDATE and accumulated (BV_AddCoefficients).
+      double local = 0.0;
+      for (int i = tid; i < a.jb; i += kThreads) {
+        const double c = cnew_s[i];
+        p.coef[i] = c;
+        if (a.hacc) a.hacc[i] = fresh ? c : a.hacc[i] + c;
+        local = fma(c, c, local);
+      }
+      local = warp_sum(local);
+      if (lane == 0) d.red[warp] = local;
+      __syncthreads();
+      if (tid == 0) {
+        double sum = 0.0;
+        for (int w = 0; w < kWarps; ++w) sum += d.red[w];  // BV_SquareSum
+        d.pass += 1;
+        const double self = cnew_s[a.jb];
+        if (a.column && !(self > -st->deftol)) d.err |= kDevErrInnerProduct;  // BV_SafeSqrt
+        const double onrm = (self < 0.0) ? 0.0 : sqrt(self);
+        const double t = onrm * onrm - sum;  // estimate |v'| from |v| (bvorthog.c:124-127)
+        if (t > 0.0) {
+          finish_pass(d, p, onrm, sqrt(t), false);
+        } else {
+          d.onrm = onrm;
+          d.action = kActUpdate | kActDot;  // explicit norm of the updated vector next
+          d.stage = kStageExplicitNorm;
+          d.cont = 0;
+        }
+      }
+    } else if (d.stage == kStageExplicitNorm) {
+      if (tid == 0) {
+        const double self = cnew_s[a.jb];
+        finish_pass(d, p, d.onrm, (self < 0.0) ? 0.0 : sqrt(self), true);  // BV_NormVecOrColumn
+      }
+    } else {
+      if (tid == 0) d.cont = 0;
+    }
+    fresh = false;
+    __syncthreads();
+    if (!d.cont) break;
+    __syncthreads();
+  }
+  if (tid == 0) {
+    st->action = d.action;
+    st->stage = d.stage;
+    st->pass = d.pass;
+    st->onrm = d.onrm;
+    st->err |= d.err;
+    if (d.stage == kStageDone) {
+      st->nrm = d.nrm;
+      st->scale = d.scale;
+      st->beta_out = d.nrm;
+      st->lindep = d.lindep;
+      if (d.lindep && a.step >= 0) {
+        st->halt = 1;
+        st->halt_step = a.step;
+      }
+    } else {
+      st->scale = 1.0;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  GsState *st = p.st;
+  const GsPassArgs &a = p.a;
+  if (a.step >= 0 && st->halt && st->halt_step < a.step) return;
+  const int action = (p.first || p.plain_dot) ? (int)kActDot : st->action;
+  if (action == kActNone) return;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int CH = p.chunk;
+  const int jb = a.jb;
+  const bool do_update = (action & kActUpdate) != 0;
+  const bool do_dot = (action & kActDot) != 0;
+  const bool do_scale = (action & kActScale) != 0;
+  const int ncl = (do_update || do_dot) ? jb : 0;  // basis columns streamed
+  const double scale = do_scale ? st->scale : 1.0;
+
+  // shared memory carve-up
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+  double *coef_s = reinterpret_cast<double *>(smem_raw + 128);
+  double *cacc = coef_s + kMaxCols;           // [kMaxCols + 1]
+  DecideShared *dsh = reinterpret_cast<DecideShared *>(cacc + kMaxCols + 1);
+  __shared__ int is_last;
+  const size_t head = 128 + sizeof(double) * (2 * kMaxCols + 1) + ((sizeof(DecideShared) + 127) / 128) * 128;
+  double *stage_base = reinterpret_cast<double *>(smem_raw + ((head + 127) / 128) * 128);
+  const size_t stage_elems = (size_t)CH * (jb + 1);
+
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  for (int i = tid; i < jb; i += kThreads) coef_s[i] = do_update ? p.coef[i] : 0.0;
+  for (int i = tid; i <= jb; i += kThreads) cacc[i] = 0.0;
+  __syncthreads();
+
+  const int G = p.G;
+  const int nmine = (p.nchunks > (int)blockIdx.x) ? (p.nchunks - 1 - (int)blockIdx.x) / G + 1 : 0;
+  const double *Vw = a.V + (size_t)a.wcol * a.ld;
+  double *Vw_out = a.V + (size_t)a.wcol * a.ld;
+
+  auto issue = [&](int i, int s) {
+    const long long q = (long long)blockIdx.x + (long long)i * G;
+    const long long r0 = q * CH;
+    const int rows = (int)min((long long)CH, (long long)a.n - r0);
+    const uint32_t bytes = (uint32_t)(((rows * 8) + 15) & ~15);
+    double *buf = stage_base + (size_t)s * stage_elems;
+    mbar_arrive_expect_tx(&bars[s], bytes * (uint32_t)(ncl + 1));
+    bulk_load(buf, Vw + r0, bytes, &bars[s]);
+    for (int c = 0; c < ncl; ++c) bulk_load(buf + (size_t)(c + 1) * CH, a.V + (size_t)c * a.ld + r0, bytes, &bars[s]);
+  };
+
+  if (tid == 0) {
+    for (int s = 0; s < kStages && s < nmine; ++s) issue(s, s);
+  }
+
+  bool timed_out = false;
+  for (int i = 0; i < nmine; ++i) {
+    const int s = i % kStages;
+    const uint32_t parity = (uint32_t)((i / kStages) & 1);
+    // every thread waits (bounded); the block then agrees on one outcome
+    const bool ok = mbar_wait_bounded(&bars[s], parity);
+    if (__syncthreads_or(!ok)) {
+      timed_out = true;
+      break;
+    }
+    const long long r0 = ((long long)blockIdx.x + (long long)i * G) * CH;
+    const int rows = (int)min((long long)CH, (long long)a.n - r0);
+    double *ws = stage_base + (size_t)s * stage_elems;
+    const double *Vs = ws + CH;  // column c at Vs + c*CH
+
+    if (do_update || do_scale) {
+      for (int r = tid; r < rows; r += kThreads) {
+        double wv = ws[r];
+        if (do_update) {
+          double acc = 0.0;
+          for (int c = 0; c < jb; ++c) acc = fma(Vs[(size_t)c * CH + r], coef_s[c], acc);
+          wv -= acc;
+        }
+        if (do_scale) wv *= scale;
+        ws[r] = wv;
+        Vw_out[r0 + r] = wv;
+      }
+      __syncthreads();
+    }
+    if (do_dot) {
+      for (int c = warp; c <= jb; c += kWarps) {
+        const double *col = (c == jb) ? ws : Vs + (size_t)c * CH;
+        double sacc = 0.0;
+        for (int r = lane; r < rows; r += 32) sacc = fma(col[r], ws[r], sacc);
+        sacc = warp_sum(sacc);
+        if (lane == 0) cacc[c] += sacc;
+      }
+    }
+    __syncthreads();
+    if (tid == 0 && i + kStages < nmine) {
+      fence_proxy_async();
+      issue(i + kStages, s);
+    }
+  }
+  if (timed_out) {
+    // Drain copies still in flight on either stage (bounded), report, and leave.
+    if (tid == 0) {
+      atomicOr(&st->err, (int)kDevErrTimeout);
+      for (int s = 0; s < kStages; ++s) (void)mbar_wait_bounded(&bars[s], 0), (void)mbar_wait_bounded(&bars[s], 1);
+    }
+    __syncthreads();
+    return;
+  }
+  // per-CTA column sums -> partials[c * G + cta]
+  if (do_dot)
+    for (int c = tid; c <= jb; c += kThreads) p.partials[(size_t)c * G + blockIdx.x] = cacc[c];
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) is_last = (atomicAdd(&st->ticket, 1u) == (unsigned)(G - 1));
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  if (tid == 0) {
+    // algorithmic traffic of this pass: streamed columns + w read, w written back if changed
+    st->bytes += (unsigned long long)a.n * 8ull * (unsigned long long)(ncl + 1 + ((do_update || do_scale) ? 1 : 0));
+    st->passes += 1;
+  }
+  if (!do_dot) {
+    // The final UPDATE/SCALE of a column is done: later follow-up launches idle.
+    if (tid == 0) {
+      st->ticket = 0u;
+      st->action = kActNone;
+    }
+    return;
+  }
+
+  // Fixed-order reduction across CTAs: lane b sums CTAs b, b+32, ...; then a fixed shuffle tree.
+  double *cnew_s = cacc;  // reuse
+  for (int c = warp; c <= jb; c += kWarps) {
+    double sacc = 0.0;
+    for (int b = lane; b < G; b += 32) sacc += __ldcg(p.partials + (size_t)c * G + b);
+    sacc = warp_sum(sacc);
+    if (lane == 0) {
+      cnew_s[c] = sacc;
+      p.cnew[c] = sacc;
+    }
+  }
+  __syncthreads();
+  if (tid == 0) st->ticket = 0u;
+  if (p.plain_dot) return;
+  decide(p, cnew_s, *dsh);
+}
+
+size_t pass_smem_bytes(int jb, int CH) {
+  const size_t head = 128 + sizeof(double) * (2 * kMaxCols + 1) + ((sizeof(DecideShared) + 127) / 128) * 128;
+  return ((head + 127) / 128) * 128 + (size_t)kStages * CH * (jb + 1) * sizeof(double);
+}
+
+int pass_chunk_rows(int jb) {
+  size_t ch = kStageBudget / ((size_t)(jb + 1) * sizeof(double));
+  ch = (ch / 32) * 32;
+  if (ch < 32) ch = 32;
+  if (ch > 2048) ch = 2048;
+  return (int)ch;
+}
+
+cudaError_t launch_pass(const GsPassArgs &a, const GsWork &w, int first, int plain_dot, cudaStream_t stream) {
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr_set[dev]) {
+    cudaError_t e = cudaFuncSetAttribute(gs_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e != cudaSuccess) return e;
+    attr_set[dev] = true;
+  }
+  PassParams p;
+  p.a = a;
+  p.st = w.st;
+  p.coef = w.coef;
+  p.cnew = w.cnew;
+  p.partials = w.partials;
+  p.first = first;
+  p.plain_dot = plain_dot;
+  p.chunk = pass_chunk_rows(a.jb);
+  p.nchunks = (a.n + p.chunk - 1) / p.chunk;
+  int G = w.num_sms;
+  if (G > w.max_ctas) G = w.max_ctas;
+  if (G > p.nchunks) G = p.nchunks;
+  if (G < 1) G = 1;
+  p.G = G;
+  const size_t smem = pass_smem_bytes(a.jb, p.chunk);
+  gs_pass_kernel<<<G, kThreads, smem, stream>>>(p);
+  count_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+namespace {
+__global__ void gs_reset_kernel(GsState *st, double eta) {
+  GsState h;
+  memset(&h, 0, sizeof(h));
+  h.eta = eta;
+  h.deftol = 10.0 * 2.220446049250313e-16;  // BV deftol = 10*PETSC_MACHINE_EPSILON (bvfunc.c:184)
+  h.halt_step = -1;
+  h.scale = 1.0;
+  *st = h;
+}
+}  // namespace
+
+cudaError_t gs_state_reset(const GsWork &w, double eta, cudaStream_t stream) {
+  gs_reset_kernel<<<1, 1, 0, stream>>>(w.st, eta);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t gs_orthogonalize_launch(const GsPassArgs &a, const GsWork &w, cudaStream_t stream) {
+  if (a.jb < 0 || a.jb >= kMaxCols) return cudaErrorInvalidValue;
+  cudaError_t e = launch_pass(a, w, 1, 0, stream);
+  // Worst case: three passes whose norm estimates all need the explicit norm,
+  // then a final scale: four follow-up launches (idle ones return at once).
+  for (int k = 0; k < 4 && e == cudaSuccess; ++k) e = launch_pass(a, w, 0, 0, stream);
+  return e;
+}
+
+cudaError_t gs_dot_launch(const GsPassArgs &a, const GsWork &w, cudaStream_t stream) {
+  if (a.jb < 0 || a.jb >= kMaxCols) return cudaErrorInvalidValue;
+  return launch_pass(a, w, 0, 1, stream);
+}
+
+}  // namespace b200

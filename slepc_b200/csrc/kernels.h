@@ -1,0 +1,73 @@
+// Launch wrappers of the device kernels (internal to the library).
+#pragma once
+
+#include "common.h"
+
+namespace b200 {
+
+void count_launch();
+uint64_t launch_count();
+
+// ---- SpMV (spmv.cu)
+int spmv_choose_lanes(int n, int64_t nnz);
+// st/step: when st is given, the launch is skipped on the device if a
+// Lanczos run halted (breakdown) at an earlier step.
+cudaError_t spmv_launch(int n, const int *rowptr, const int *colind, const double *vals, const double *x, double *y,
+                        int lanes, cudaStream_t stream, const GsState *st = nullptr, int step = 0);
+
+// ---- Fused Gram-Schmidt passes (gs.cu)
+// Device workspace of one BV for the Gram-Schmidt kernels.
+struct GsWork {
+  GsState *st;        // control block
+  double *coef;       // [kMaxCols] coefficients applied by the next UPDATE
+  double *cnew;       // [kMaxCols+1] result of the last reduced dot
+  double *partials;   // [(kMaxCols+1) * max_ctas] per-CTA partial dots
+  int max_ctas;
+  int num_sms;
+};
+
+struct GsPassArgs {
+  double *V;      // basis, column-major
+  int ld, n;
+  int jb;         // basis columns 0..jb-1
+  int wcol;       // column holding the vector being orthogonalised
+  double *hacc;   // accumulated coefficients (jb + 1 entries: coefficients then norm)
+  double *T;      // optional Lanczos output: T[step] = alpha, T[ldt+step] = beta
+  int ldt;
+  int step;       // Lanczos step index (halt gating), or -1
+  int normalize;  // scale by 1/norm at the end
+  int column;     // 1: column variant (BV_SafeSqrt check on w^T w)
+};
+
+// Enqueue the full CGS + DGKS("if needed") orthogonalisation of one column:
+// a first dot pass plus the follow-up passes the device decides on.
+cudaError_t gs_orthogonalize_launch(const GsPassArgs &a, const GsWork &w, cudaStream_t stream);
+// Initialise the control block (eta, deftol, clears halt/err) -- once per run.
+cudaError_t gs_state_reset(const GsWork &w, double eta, cudaStream_t stream);
+// Plain dots q = V(:,0:jb)^T w (no decision), result in w.cnew.
+cudaError_t gs_dot_launch(const GsPassArgs &a, const GsWork &w, cudaStream_t stream);
+
+// ---- Dense tall-skinny operations (bvops.cu)
+// V(:,s:e) = V(:,l:k) * Q(l:k,s:e), row-blocked, in place; Q points at element (l,s).
+cudaError_t multinplace_launch(double *V, int ld, int n, int l, int k, const double *Q, int ldq, int s, int e,
+                               cudaStream_t stream);
+// Y(:,0:ny) = alpha * X(:,0:nx) * Q(0:nx,0:ny) + beta * Y(:,0:ny)   (X != Y storage)
+cudaError_t mult_launch(double *Y, int ldy, const double *X, int ldx, int n, int nx, int ny, const double *Q, int ldq,
+                        double alpha, double beta, cudaStream_t stream);
+// y = beta*y + alpha*X(:,0:k) q
+cudaError_t multvec_launch(const double *X, int ldx, int n, int k, const double *q, double alpha, double beta, double *y,
+                           cudaStream_t stream);
+// M(0:ny,0:nx) = Y(:,0:ny)^T X(:,0:nx), M column-major ldm (device), deterministic.
+cudaError_t dot_launch(const double *X, int ldx, int nx, const double *Y, int ldy, int ny, int n, double *M, int ldm,
+                       double *work, int work_len, cudaStream_t stream);
+cudaError_t scale_launch(double *x, long long len, double alpha, cudaStream_t stream);
+cudaError_t copy_launch(double *dst, const double *src, long long len, cudaStream_t stream);
+// Sum of squares of x (len) into out[0] (device), deterministic two-level reduction.
+cudaError_t sumsq_launch(const double *x, long long len, double *out, double *work, int work_len, cudaStream_t stream);
+// out[0] = ||A x - lambda x||^2 (fused SpMV + residual), deterministic.
+cudaError_t residual_launch(int n, const int *rowptr, const int *colind, const double *vals, const double *x,
+                            double lambda, double *out, double *work, int work_len, int lanes, cudaStream_t stream);
+// Counter-based uniform [0,1) column (stands in for PETSc's VecSetRandom).
+cudaError_t random_launch(double *x, int n, uint64_t seed, uint64_t stream_id, cudaStream_t stream);
+
+}  // namespace b200

@@ -1,0 +1,1084 @@
+// Host objects (Mat, BV, EPS), the Krylov-Schur driver and the C ABI.
+//
+// The driver restates EPSSolve_KrylovSchur_Default
+// (src/eps/impls/krylov/krylovschur/krylovschur.c:227-348) for Hermitian
+// problems with Ritz extraction and locking, together with EPSSetUp's
+// defaults (krylovschur.c:93-194, src/eps/interface/epssetup.c:669-713),
+// EPSGetStartVector (epssolve.c:841-870), EPSKrylovConvergence
+// (src/eps/impls/krylov/epskrylov.c:207-295), EPSConvergedRelative and
+// EPSStoppingBasic (epsdefault.c:224-232, 290-305), and SlepcSortEigenvalues
+// (src/sys/slepcsc.c:89-149).  All vector work runs on the GPU; a Lanczos
+// run of BVMatLanczos (bvkrylov.c:165-226) is enqueued as one asynchronous
+// sequence of kernels with a single host synchronisation at its end.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.h"
+#include "ds_hep.h"
+#include "kernels.h"
+
+using namespace b200;
+
+// --------------------------------------------------------------- errors ---
+static thread_local std::string g_last_error;
+static std::atomic<uint64_t> g_launches{0};
+
+extern "C" void b200_set_last_error(const char *file, int line, const char *msg) {
+  const char *base = strrchr(file, '/');
+  g_last_error = std::string(msg) + " (" + (base ? base + 1 : file) + ":" + std::to_string(line) + ")";
+}
+extern "C" const char *b200_last_error(void) { return g_last_error.c_str(); }
+extern "C" const char *b200_version(void) { return "slepc_b200 0.1 (sm_100a, FP64 Krylov-Schur)"; }
+extern "C" uint64_t b200_kernel_launch_count(void) { return g_launches.load(); }
+
+namespace b200 {
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+uint64_t launch_count() { return g_launches.load(); }
+int num_sms_host() {
+  int dev = 0, v = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+  return v > 0 ? v : 1;
+}
+}  // namespace b200
+
+#define B200_DEV_ERR(msg)                             \
+  do {                                                \
+    b200_set_last_error(__FILE__, __LINE__, msg);     \
+    return B200_ERR_DEVICE;                           \
+  } while (0)
+
+// ------------------------------------------------------------------ Mat ---
+struct b200_mat_s {
+  int n = 0;
+  int64_t nnz = 0;
+  int *rowptr = nullptr, *colind = nullptr;
+  double *vals = nullptr;
+  int lanes = 8;
+  cudaStream_t stream = nullptr;
+};
+
+static b200_status mat_alloc(int n, int64_t nnz, cudaStream_t stream, b200_mat *A) {
+  b200_mat M = new b200_mat_s;
+  M->n = n;
+  M->nnz = nnz;
+  M->stream = stream;
+  M->lanes = spmv_choose_lanes(n, nnz);
+  if (cudaMalloc(&M->rowptr, sizeof(int) * ((size_t)n + 1)) != cudaSuccess ||
+      cudaMalloc(&M->colind, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)) != cudaSuccess ||
+      cudaMalloc(&M->vals, sizeof(double) * (size_t)(nnz > 0 ? nnz : 1)) != cudaSuccess) {
+    cudaFree(M->rowptr);
+    cudaFree(M->colind);
+    cudaFree(M->vals);
+    delete M;
+    b200_set_last_error(__FILE__, __LINE__, "cudaMalloc failed for the CSR arrays");
+    return B200_ERR_NOMEM;
+  }
+  *A = M;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_mat_create_csr(int n, int64_t nnz, const int *rowptr, const int *colind, const double *vals,
+                                           void *stream, b200_mat *A) {
+  B200_ARG_CHECK(A && n > 0 && nnz >= 0 && rowptr && (nnz == 0 || (colind && vals)), "invalid CSR arguments");
+  B200_ARG_CHECK(rowptr[0] == 0 && rowptr[n] == nnz, "rowptr must start at 0 and end at nnz");
+  B200_ARG_CHECK(nnz <= 0x7fffffff, "nnz must fit a 32-bit index (PETSc default int size)");
+  b200_mat M;
+  B200_CHECK(mat_alloc(n, nnz, (cudaStream_t)stream, &M));
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(M->rowptr, rowptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && nnz)
+    e = cudaMemcpyAsync(M->colind, colind, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(M->vals, vals, sizeof(double) * (size_t)nnz, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    b200_mat_destroy(M);
+    b200_set_last_error(__FILE__, __LINE__, cudaGetErrorString(e));
+    return B200_ERR_CUDA;
+  }
+  *A = M;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_mat_create_csr_device(int n, int64_t nnz, const int *rowptr, const int *colind,
+                                                  const double *vals, void *stream, b200_mat *A) {
+  B200_ARG_CHECK(A && n > 0 && nnz >= 0 && rowptr && (nnz == 0 || (colind && vals)), "invalid CSR arguments");
+  B200_ARG_CHECK(nnz <= 0x7fffffff, "nnz must fit a 32-bit index");
+  b200_mat M;
+  B200_CHECK(mat_alloc(n, nnz, (cudaStream_t)stream, &M));
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(M->rowptr, rowptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess && nnz)
+    e = cudaMemcpyAsync(M->colind, colind, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess && nnz)
+    e = cudaMemcpyAsync(M->vals, vals, sizeof(double) * (size_t)nnz, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    b200_mat_destroy(M);
+    b200_set_last_error(__FILE__, __LINE__, cudaGetErrorString(e));
+    return B200_ERR_CUDA;
+  }
+  *A = M;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_mat_mult(b200_mat A, const double *x, double *y) {
+  B200_ARG_CHECK(A && x && y, "null argument");
+  B200_CUDA_CHECK(spmv_launch(A->n, A->rowptr, A->colind, A->vals, x, y, A->lanes, A->stream));
+  return B200_OK;
+}
+
+extern "C" b200_status b200_mat_get_size(b200_mat A, int *n, int64_t *nnz) {
+  B200_ARG_CHECK(A, "null matrix");
+  if (n) *n = A->n;
+  if (nnz) *nnz = A->nnz;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_mat_get_lanes(b200_mat A, int *lanes) {
+  B200_ARG_CHECK(A && lanes, "null argument");
+  *lanes = A->lanes;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_mat_destroy(b200_mat A) {
+  if (!A) return B200_OK;
+  cudaFree(A->rowptr);
+  cudaFree(A->colind);
+  cudaFree(A->vals);
+  delete A;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_csr_spmv(int n, const int *rowptr, const int *colind, const double *vals, const double *x,
+                                     double *y, int lanes, void *stream) {
+  B200_ARG_CHECK(n >= 0 && rowptr && colind && vals && x && y, "null argument");
+  B200_ARG_CHECK(lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32,
+                 "lanes must be a power of two in [1,32]");
+  B200_CUDA_CHECK(spmv_launch(n, rowptr, colind, vals, x, y, lanes, (cudaStream_t)stream));
+  return B200_OK;
+}
+
+// ------------------------------------------------------------------- BV ---
+struct b200_bv_s {
+  int n = 0, m = 0, ld = 0;   // m user columns; column m is an internal work column
+  double *V = nullptr;
+  int l = 0, k = 0;
+  double eta = 0.7071;        // bvfunc.c:178
+  cudaStream_t stream = nullptr;
+  GsWork gs{};
+  double *coefbuf = nullptr;  // (m+1) x (m+1): column j = coefficients of column j (BVGetBufferVec)
+  int ldc = 0;
+  double *hvec = nullptr;     // coefficients of the vector variant
+  double *T = nullptr;        // Lanczos alpha (T[j]) and beta (T[ldt+j])
+  int ldt = 0;
+  double *red = nullptr;      // reduction workspace
+  int red_len = 0;
+  double *scal = nullptr;     // device scalars
+  double *qbuf = nullptr;     // device staging of coefficient matrices
+  size_t qbuf_len = 0;
+  double *hpin = nullptr;     // pinned host staging
+  size_t hpin_len = 0;
+  uint64_t seed = 0x5eedULL, nrand = 0;
+};
+
+static void bv_free(b200_bv bv) {
+  if (!bv) return;
+  cudaFree(bv->V);
+  cudaFree(bv->gs.st);
+  cudaFree(bv->gs.coef);
+  cudaFree(bv->gs.cnew);
+  cudaFree(bv->gs.partials);
+  cudaFree(bv->coefbuf);
+  cudaFree(bv->hvec);
+  cudaFree(bv->T);
+  cudaFree(bv->red);
+  cudaFree(bv->scal);
+  cudaFree(bv->qbuf);
+  cudaFreeHost(bv->hpin);
+  delete bv;
+}
+
+extern "C" b200_status b200_bv_create(int n, int m, void *stream, b200_bv *out) {
+  B200_ARG_CHECK(out && n > 0 && m > 0, "invalid BV sizes");
+  B200_ARG_CHECK(m + 1 < kMaxCols, "too many BV columns for the Gram-Schmidt kernels (m <= 253)");
+  b200_bv bv = new b200_bv_s;
+  bv->n = n;
+  bv->m = m;
+  bv->ld = ((n + 31) / 32) * 32;
+  bv->k = m;
+  bv->stream = (cudaStream_t)stream;
+  bv->ldc = m + 1;
+  bv->ldt = m + 1;
+  const int sms = num_sms_host();
+  bv->gs.num_sms = sms;
+  bv->gs.max_ctas = sms;
+  bv->red_len = sms * 8 > 4096 ? sms * 8 : 4096;
+  bv->qbuf_len = (size_t)(m + 1) * (m + 1);
+  bv->hpin_len = (size_t)(m + 1) * (m + 1) + 4 * (size_t)(m + 1) + 64;
+  bool ok = true;
+  // one spare chunk of rows past the last column: the bulk copies of a ragged
+  // final chunk round up to 16 bytes
+  ok = ok && cudaMalloc(&bv->V, sizeof(double) * ((size_t)bv->ld * (m + 1) + 32)) == cudaSuccess;
+  ok = ok && cudaMalloc(&bv->gs.st, sizeof(GsState)) == cudaSuccess;
+  ok = ok && cudaMalloc(&bv->gs.coef, sizeof(double) * kMaxCols) == cudaSuccess;
+  ok = ok && cudaMalloc(&bv->gs.cnew, sizeof(double) * (kMaxCols + 1)) == cudaSuccess;
+  ok = ok && cudaMalloc(&bv->gs.partials, sizeof(double) * (size_t)(kMaxCols + 1) * sms) == cudaSuccess;
+  ok = ok && cudaMalloc(&bv->coefbuf, sizeof(double) * (size_t)bv->ldc * (m + 1)) == cudaSuccess;
+  ok = ok && cudaMalloc(&bv->hvec, sizeof(double) * (kMaxCols + 1)) == cudaSuccess;
+  ok = ok && cudaMalloc(&bv->T, sizeof(double) * 2 * (size_t)bv->ldt) == cudaSuccess;
+  ok = ok && cudaMalloc(&bv->red, sizeof(double) * (size_t)bv->red_len) == cudaSuccess;
+  ok = ok && cudaMalloc(&bv->scal, sizeof(double) * 16) == cudaSuccess;
+  ok = ok && cudaMalloc(&bv->qbuf, sizeof(double) * bv->qbuf_len) == cudaSuccess;
+  ok = ok && cudaMallocHost(&bv->hpin, sizeof(double) * bv->hpin_len) == cudaSuccess;
+  if (!ok) {
+    bv_free(bv);
+    b200_set_last_error(__FILE__, __LINE__, "device allocation failed for the BV");
+    return B200_ERR_NOMEM;
+  }
+  cudaError_t e = cudaMemsetAsync(bv->V, 0, sizeof(double) * ((size_t)bv->ld * (m + 1) + 32), bv->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bv->coefbuf, 0, sizeof(double) * (size_t)bv->ldc * (m + 1), bv->stream);
+  if (e == cudaSuccess) e = gs_state_reset(bv->gs, bv->eta, bv->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(bv->stream);
+  if (e != cudaSuccess) {
+    bv_free(bv);
+    b200_set_last_error(__FILE__, __LINE__, cudaGetErrorString(e));
+    return B200_ERR_CUDA;
+  }
+  *out = bv;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_destroy(b200_bv bv) {
+  bv_free(bv);
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_get_sizes(b200_bv bv, int *n, int *m, int *ld) {
+  B200_ARG_CHECK(bv, "null BV");
+  if (n) *n = bv->n;
+  if (m) *m = bv->m;
+  if (ld) *ld = bv->ld;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_get_array(b200_bv bv, double **V) {
+  B200_ARG_CHECK(bv && V, "null argument");
+  *V = bv->V;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_set_active_columns(b200_bv bv, int l, int k) {
+  B200_ARG_CHECK(bv && 0 <= k && k <= bv->m && 0 <= l && l <= k, "active columns out of range");
+  bv->l = l;
+  bv->k = k;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_get_active_columns(b200_bv bv, int *l, int *k) {
+  B200_ARG_CHECK(bv, "null BV");
+  if (l) *l = bv->l;
+  if (k) *k = bv->k;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_set_orthog_eta(b200_bv bv, double eta) {
+  B200_ARG_CHECK(bv && eta > 0.0, "eta must be positive");
+  bv->eta = eta;
+  return B200_OK;
+}
+
+static inline double *col(b200_bv bv, int j) { return bv->V + (size_t)j * bv->ld; }
+
+extern "C" b200_status b200_bv_set_column(b200_bv bv, int j, const double *x) {
+  B200_ARG_CHECK(bv && x && j >= 0 && j < bv->m, "column index out of range");
+  B200_CUDA_CHECK(cudaMemcpyAsync(col(bv, j), x, sizeof(double) * bv->n, cudaMemcpyHostToDevice, bv->stream));
+  B200_CUDA_CHECK(cudaStreamSynchronize(bv->stream));
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_get_column(b200_bv bv, int j, double *x) {
+  B200_ARG_CHECK(bv && x && j >= 0 && j < bv->m, "column index out of range");
+  B200_CUDA_CHECK(cudaMemcpyAsync(x, col(bv, j), sizeof(double) * bv->n, cudaMemcpyDeviceToHost, bv->stream));
+  B200_CUDA_CHECK(cudaStreamSynchronize(bv->stream));
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_copy_vec(b200_bv bv, int j, double *x) {
+  B200_ARG_CHECK(bv && x && j >= 0 && j < bv->m, "column index out of range");
+  B200_CUDA_CHECK(copy_launch(x, col(bv, j), bv->n, bv->stream));
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_insert_vec(b200_bv bv, int j, const double *x) {
+  B200_ARG_CHECK(bv && x && j >= 0 && j < bv->m, "column index out of range");
+  B200_CUDA_CHECK(copy_launch(col(bv, j), x, bv->n, bv->stream));
+  return B200_OK;
+}
+
+// Read back the control block after a synchronisation; map device errors.
+static b200_status bv_read_state(b200_bv bv, GsState *out) {
+  GsState *h = reinterpret_cast<GsState *>(bv->hpin);
+  B200_CUDA_CHECK(cudaMemcpyAsync(h, bv->gs.st, sizeof(GsState), cudaMemcpyDeviceToHost, bv->stream));
+  B200_CUDA_CHECK(cudaStreamSynchronize(bv->stream));
+  *out = *h;
+  if (out->err & kDevErrInnerProduct) {
+    b200_set_last_error(__FILE__, __LINE__, "invalid inner product (negative self dot product)");
+    return B200_ERR_INNER;
+  }
+  if (out->err) B200_DEV_ERR("a Gram-Schmidt kernel reported a device-side error (bounded wait expired)");
+  return B200_OK;
+}
+
+// Orthogonalise column j against columns 0..j-1 (column variant).
+static b200_status bv_orth_column(b200_bv bv, int j, int normalize, double *H, double *norm, int *lindep) {
+  B200_CUDA_CHECK(gs_state_reset(bv->gs, bv->eta, bv->stream));
+  GsPassArgs a{};
+  a.V = bv->V;
+  a.ld = bv->ld;
+  a.n = bv->n;
+  a.jb = j;
+  a.wcol = j;
+  a.hacc = bv->coefbuf + (size_t)j * bv->ldc;
+  a.T = nullptr;
+  a.ldt = 0;
+  a.step = -1;
+  a.normalize = normalize;
+  a.column = 1;
+  B200_CUDA_CHECK(gs_orthogonalize_launch(a, bv->gs, bv->stream));
+  if (H) {
+    B200_CUDA_CHECK(cudaMemcpyAsync(bv->hpin + 64, a.hacc, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, bv->stream));
+  }
+  GsState st;
+  B200_CHECK(bv_read_state(bv, &st));
+  if (H) memcpy(H, bv->hpin + 64, sizeof(double) * (j + 1));
+  if (norm) *norm = st.beta_out;
+  if (lindep) *lindep = st.lindep;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_orthogonalize_column(b200_bv bv, int j, double *H, double *norm, int *lindep) {
+  B200_ARG_CHECK(bv && j >= 0 && j < bv->m, "column index out of range");
+  return bv_orth_column(bv, j, 0, H, norm, lindep);
+}
+
+extern "C" b200_status b200_bv_orthonormalize_column(b200_bv bv, int j, double *norm, int *lindep) {
+  B200_ARG_CHECK(bv && j >= 0 && j < bv->m, "column index out of range");
+  return bv_orth_column(bv, j, 1, nullptr, norm, lindep);
+}
+
+extern "C" b200_status b200_bv_orthogonalize_vec(b200_bv bv, double *v, double *H, double *norm, int *lindep) {
+  B200_ARG_CHECK(bv && v, "null argument");
+  const int k = bv->k;
+  // the vector is staged in the work column (column m) so every bulk copy stays inside the BV storage
+  B200_CUDA_CHECK(copy_launch(col(bv, bv->m), v, bv->n, bv->stream));
+  B200_CUDA_CHECK(gs_state_reset(bv->gs, bv->eta, bv->stream));
+  GsPassArgs a{};
+  a.V = bv->V;
+  a.ld = bv->ld;
+  a.n = bv->n;
+  a.jb = k;
+  a.wcol = bv->m;
+  a.hacc = bv->hvec;
+  a.step = -1;
+  a.normalize = 0;
+  a.column = 0;
+  B200_CUDA_CHECK(gs_orthogonalize_launch(a, bv->gs, bv->stream));
+  B200_CUDA_CHECK(copy_launch(v, col(bv, bv->m), bv->n, bv->stream));
+  if (H && k > 0)
+    B200_CUDA_CHECK(cudaMemcpyAsync(bv->hpin + 64, bv->hvec, sizeof(double) * k, cudaMemcpyDeviceToHost, bv->stream));
+  GsState st;
+  B200_CHECK(bv_read_state(bv, &st));
+  if (H && k > 0) memcpy(H, bv->hpin + 64, sizeof(double) * k);
+  if (norm) *norm = st.beta_out;
+  if (lindep) *lindep = st.lindep;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_scale_column(b200_bv bv, int j, double alpha) {
+  B200_ARG_CHECK(bv && j < bv->m, "column index out of range");
+  if (j < 0) {
+    for (int c = bv->l; c < bv->k; ++c) B200_CUDA_CHECK(scale_launch(col(bv, c), bv->n, alpha, bv->stream));
+  } else if (alpha != 1.0) {
+    B200_CUDA_CHECK(scale_launch(col(bv, j), bv->n, alpha, bv->stream));
+  }
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_orthogonalize(b200_bv bv, double *R, int ldr) {
+  B200_ARG_CHECK(bv && (!R || ldr >= bv->k), "R leading dimension too small");
+  for (int j = bv->l; j < bv->k; ++j) {
+    double norm = 0.0;
+    std::vector<double> H(j + 1);
+    B200_CHECK(bv_orth_column(bv, j, 0, R ? H.data() : nullptr, &norm, nullptr));
+    if (norm == 0.0) {
+      b200_set_last_error(__FILE__, __LINE__, "breakdown in BVOrthogonalize due to a linearly dependent column");
+      return B200_ERR_BREAKDOWN;
+    }
+    if (R) {
+      for (int i = 0; i < j; ++i) R[i + (size_t)j * ldr] = H[i];
+      R[j + (size_t)j * ldr] = norm;
+    }
+    B200_CHECK(b200_bv_scale_column(bv, j, 1.0 / norm));
+  }
+  return B200_OK;
+}
+
+static b200_status bv_multinplace_dev(b200_bv bv, const double *Qdev_ls, int ldq, int s, int e) {
+  if (s >= e || bv->k <= bv->l) return B200_OK;
+  B200_CUDA_CHECK(multinplace_launch(bv->V, bv->ld, bv->n, bv->l, bv->k, Qdev_ls, ldq, s, e, bv->stream));
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_mult_inplace(b200_bv bv, const double *Q, int ldq, int s, int e) {
+  B200_ARG_CHECK(bv && Q && ldq >= bv->k, "invalid Q");
+  B200_ARG_CHECK(s >= bv->l && s <= bv->m && e >= bv->l && e <= bv->m, "s/e out of range");
+  if (s >= e) return B200_OK;
+  const int kq = bv->k - bv->l, nc = e - s;
+  B200_ARG_CHECK((size_t)kq * nc <= bv->qbuf_len && (size_t)kq * nc <= bv->hpin_len, "Q block too large");
+  // pack Q(l:k, s:e) into pinned memory, then one host-to-device copy
+  B200_CUDA_CHECK(cudaStreamSynchronize(bv->stream));
+  for (int j = 0; j < nc; ++j)
+    memcpy(bv->hpin + (size_t)j * kq, Q + (size_t)bv->l + (size_t)(s + j) * ldq, sizeof(double) * kq);
+  B200_CUDA_CHECK(
+      cudaMemcpyAsync(bv->qbuf, bv->hpin, sizeof(double) * (size_t)kq * nc, cudaMemcpyHostToDevice, bv->stream));
+  return bv_multinplace_dev(bv, bv->qbuf, kq, s, e);
+}
+
+extern "C" b200_status b200_bv_mult_inplace_device(b200_bv bv, const double *Q, int ldq, int s, int e) {
+  B200_ARG_CHECK(bv && Q && ldq >= bv->k, "invalid Q");
+  B200_ARG_CHECK(s >= bv->l && s <= bv->m && e >= bv->l && e <= bv->m, "s/e out of range");
+  return bv_multinplace_dev(bv, Q + (size_t)bv->l + (size_t)s * ldq, ldq, s, e);
+}
+
+extern "C" b200_status b200_bv_mult(b200_bv Y, double alpha, double beta, b200_bv X, const double *Q, int ldq) {
+  B200_ARG_CHECK(X && Y && X != Y && Q && X->n == Y->n, "invalid BVMult arguments");
+  const int nx = X->k - X->l, ny = Y->k - Y->l;
+  B200_ARG_CHECK(ldq >= X->k, "Q leading dimension too small");
+  if (ny <= 0) return B200_OK;
+  B200_ARG_CHECK((size_t)nx * ny <= Y->qbuf_len && (size_t)nx * ny <= Y->hpin_len, "Q block too large");
+  B200_CUDA_CHECK(cudaStreamSynchronize(Y->stream));
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) Y->hpin[i + (size_t)j * nx] = Q[(size_t)(X->l + i) + (size_t)(Y->l + j) * ldq];
+  B200_CUDA_CHECK(
+      cudaMemcpyAsync(Y->qbuf, Y->hpin, sizeof(double) * (size_t)nx * ny, cudaMemcpyHostToDevice, Y->stream));
+  B200_CUDA_CHECK(mult_launch(col(Y, Y->l), Y->ld, col(X, X->l), X->ld, X->n, nx, ny, Y->qbuf, nx, alpha, beta, Y->stream));
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_mult_vec(b200_bv X, double alpha, double beta, double *y, const double *q) {
+  B200_ARG_CHECK(X && y && (q || X->k == X->l), "null argument");
+  const int k = X->k - X->l;
+  B200_CUDA_CHECK(cudaStreamSynchronize(X->stream));
+  if (k > 0) memcpy(X->hpin, q, sizeof(double) * k);
+  B200_CUDA_CHECK(cudaMemcpyAsync(X->scal, X->hpin, sizeof(double) * (k > 0 ? k : 1), cudaMemcpyHostToDevice, X->stream));
+  if (k > 16) {
+    B200_ARG_CHECK((size_t)k <= X->qbuf_len, "too many columns");
+    B200_CUDA_CHECK(cudaMemcpyAsync(X->qbuf, X->hpin, sizeof(double) * k, cudaMemcpyHostToDevice, X->stream));
+  }
+  B200_CUDA_CHECK(multvec_launch(col(X, X->l), X->ld, X->n, k, k > 16 ? X->qbuf : X->scal, alpha, beta, y, X->stream));
+  B200_CUDA_CHECK(cudaStreamSynchronize(X->stream));
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_dot(b200_bv X, b200_bv Y, double *M, int ldm) {
+  B200_ARG_CHECK(X && Y && M && X->n == Y->n, "invalid BVDot arguments");
+  const int nx = X->k - X->l, ny = Y->k - Y->l;
+  B200_ARG_CHECK(ldm >= Y->k, "M leading dimension too small");
+  if (nx <= 0 || ny <= 0) return B200_OK;
+  B200_ARG_CHECK((size_t)nx * ny <= X->qbuf_len && (size_t)nx * ny <= X->hpin_len, "result too large");
+  B200_CUDA_CHECK(dot_launch(col(X, X->l), X->ld, nx, col(Y, Y->l), Y->ld, ny, X->n, X->qbuf, ny, X->red, X->red_len,
+                             X->stream));
+  B200_CUDA_CHECK(
+      cudaMemcpyAsync(X->hpin, X->qbuf, sizeof(double) * (size_t)nx * ny, cudaMemcpyDeviceToHost, X->stream));
+  B200_CUDA_CHECK(cudaStreamSynchronize(X->stream));
+  for (int j = 0; j < nx; ++j)
+    for (int i = 0; i < ny; ++i) M[(size_t)(Y->l + i) + (size_t)(X->l + j) * ldm] = X->hpin[i + (size_t)j * ny];
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_dot_vec(b200_bv X, const double *y, double *q) {
+  B200_ARG_CHECK(X && y && q, "null argument");
+  const int k = X->k - X->l;
+  if (k <= 0) return B200_OK;
+  B200_CUDA_CHECK(copy_launch(col(X, X->m), y, X->n, X->stream));
+  GsPassArgs a{};
+  a.V = col(X, X->l);
+  a.ld = X->ld;
+  a.n = X->n;
+  a.jb = k;
+  a.wcol = X->m - X->l;
+  a.step = -1;
+  B200_CUDA_CHECK(gs_dot_launch(a, X->gs, X->stream));
+  B200_CUDA_CHECK(cudaMemcpyAsync(X->hpin, X->gs.cnew, sizeof(double) * k, cudaMemcpyDeviceToHost, X->stream));
+  B200_CUDA_CHECK(cudaStreamSynchronize(X->stream));
+  memcpy(q, X->hpin, sizeof(double) * k);
+  return B200_OK;
+}
+
+static b200_status bv_sumsq(b200_bv bv, const double *x, long long len, double *out) {
+  B200_CUDA_CHECK(sumsq_launch(x, len, bv->scal, bv->red, bv->red_len, bv->stream));
+  B200_CUDA_CHECK(cudaMemcpyAsync(bv->hpin, bv->scal, sizeof(double), cudaMemcpyDeviceToHost, bv->stream));
+  B200_CUDA_CHECK(cudaStreamSynchronize(bv->stream));
+  *out = bv->hpin[0];
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_norm_column(b200_bv bv, int j, double *nrm) {
+  B200_ARG_CHECK(bv && nrm && j >= 0 && j < bv->m, "column index out of range");
+  double s = 0.0;
+  B200_CHECK(bv_sumsq(bv, col(bv, j), bv->n, &s));
+  *nrm = std::sqrt(s);
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_norm(b200_bv bv, double *nrm) {
+  B200_ARG_CHECK(bv && nrm, "null argument");
+  double tot = 0.0;
+  for (int c = bv->l; c < bv->k; ++c) {
+    double s = 0.0;
+    B200_CHECK(bv_sumsq(bv, col(bv, c), bv->n, &s));
+    tot += s;
+  }
+  *nrm = std::sqrt(tot);
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_copy_column(b200_bv bv, int j, int i) {
+  B200_ARG_CHECK(bv && j >= 0 && j < bv->m && i >= 0 && i < bv->m, "column index out of range");
+  if (i == j) return B200_OK;
+  B200_CUDA_CHECK(copy_launch(col(bv, i), col(bv, j), bv->n, bv->stream));
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_mat_mult_column(b200_bv bv, b200_mat A, int j) {
+  B200_ARG_CHECK(bv && A && A->n == bv->n && j >= 0 && j + 1 < bv->m, "invalid BVMatMultColumn arguments");
+  B200_CUDA_CHECK(spmv_launch(A->n, A->rowptr, A->colind, A->vals, col(bv, j), col(bv, j + 1), A->lanes, bv->stream));
+  return B200_OK;
+}
+
+// Timing of a Lanczos run (optional): event pairs around each SpMV and each column orthogonalisation.
+struct RunTimer {
+  bool on = false;
+  std::vector<cudaEvent_t> ev;
+  size_t used = 0;
+  double ms_spmv = 0.0, ms_orth = 0.0;
+  void reserve(size_t count) {
+    while (ev.size() < count) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) break;
+      ev.push_back(e);
+    }
+  }
+  cudaEvent_t next() { return used < ev.size() ? ev[used++] : nullptr; }
+  ~RunTimer() {
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+};
+
+// BVMatLanczos: steps j = k..m-1 enqueued back to back; one synchronisation at the end.
+static b200_status bv_lanczos(b200_bv bv, b200_mat A, int k, int *m, double *alpha, double *beta_h, double *beta,
+                              int *breakdown, RunTimer *timer, GsState *st_out) {
+  const int m0 = *m;
+  B200_CUDA_CHECK(gs_state_reset(bv->gs, bv->eta, bv->stream));
+  const bool timing = timer && timer->on;
+  if (timing) {
+    timer->reserve((size_t)4 * (m0 - k) + 4);
+    timer->used = 0;
+  }
+  for (int j = k; j < m0; ++j) {
+    cudaEvent_t e0 = timing ? timer->next() : nullptr, e1 = timing ? timer->next() : nullptr;
+    cudaEvent_t e2 = timing ? timer->next() : nullptr, e3 = timing ? timer->next() : nullptr;
+    if (e0) cudaEventRecord(e0, bv->stream);
+    B200_CUDA_CHECK(
+        spmv_launch(A->n, A->rowptr, A->colind, A->vals, col(bv, j), col(bv, j + 1), A->lanes, bv->stream, bv->gs.st, j));
+    if (e1) cudaEventRecord(e1, bv->stream);
+    GsPassArgs a{};
+    a.V = bv->V;
+    a.ld = bv->ld;
+    a.n = bv->n;
+    a.jb = j + 1;
+    a.wcol = j + 1;
+    a.hacc = bv->coefbuf + (size_t)(j + 1) * bv->ldc;
+    a.T = bv->T;
+    a.ldt = bv->ldt;
+    a.step = j;
+    a.normalize = 1;
+    a.column = 1;
+    if (e2) cudaEventRecord(e2, bv->stream);
+    B200_CUDA_CHECK(gs_orthogonalize_launch(a, bv->gs, bv->stream));
+    if (e3) cudaEventRecord(e3, bv->stream);
+  }
+  // one device-to-host copy of T and of the control block
+  double *hT = bv->hpin + 64;
+  B200_CUDA_CHECK(cudaMemcpyAsync(hT, bv->T, sizeof(double) * 2 * (size_t)bv->ldt, cudaMemcpyDeviceToHost, bv->stream));
+  GsState st;
+  B200_CHECK(bv_read_state(bv, &st));
+  if (st_out) *st_out = st;
+  int mm = m0;
+  int bd = 0;
+  if (st.halt) {
+    mm = st.halt_step + 1;
+    bd = 1;
+  }
+  for (int j = k; j < mm; ++j) {
+    if (alpha) alpha[j] = hT[j];
+    if (beta_h) beta_h[j] = hT[bv->ldt + j];
+  }
+  *m = mm;
+  if (beta) *beta = st.beta_out;
+  if (breakdown) *breakdown = bd;
+  if (timing) {
+    for (int j = k; j < m0; ++j) {
+      const size_t base = (size_t)4 * (j - k);
+      if (base + 3 >= timer->ev.size()) break;
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, timer->ev[base], timer->ev[base + 1]) == cudaSuccess) timer->ms_spmv += t;
+      if (cudaEventElapsedTime(&t, timer->ev[base + 2], timer->ev[base + 3]) == cudaSuccess) timer->ms_orth += t;
+    }
+  }
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_mat_lanczos(b200_bv bv, b200_mat A, int k, int *m, double *alpha, double *beta_h,
+                                           double *beta, int *breakdown) {
+  B200_ARG_CHECK(bv && A && m && A->n == bv->n, "invalid BVMatLanczos arguments");
+  B200_ARG_CHECK(k >= 0 && *m > k && *m < bv->m, "k/m out of range (need k < m < columns)");
+  return bv_lanczos(bv, A, k, m, alpha, beta_h, beta, breakdown, nullptr, nullptr);
+}
+
+// ------------------------------------------------------------------ EPS ---
+struct b200_eps_s {
+  cudaStream_t stream = nullptr;
+  b200_mat A = nullptr;
+  int nev = 1, ncv = 0, mpd = 0;
+  double tol = 0.0;
+  int max_it = 0;
+  int which = B200_LARGEST_MAGNITUDE;
+  double keep = 0.5;  // krylovschur.c:122
+  std::vector<double> v0;
+  const double *v0_dev = nullptr;
+  int nini = 0;
+  int max_restarts = 0;
+  b200_bv V = nullptr;
+  DsHep ds;
+  std::vector<double> eigr, errest;
+  std::vector<int> perm;
+  int nconv = 0, its = 0, reason = 0;
+  bool solved = false;
+  int timing = 0;
+  b200_eps_stats stats{};
+  // effective values after setup
+  int n_ = 0, ncv_ = 0, mpd_ = 0, max_it_ = 0;
+  double tol_ = 1e-8;
+  double *resid_buf = nullptr;
+};
+
+extern "C" b200_status b200_eps_create(void *stream, b200_eps *eps) {
+  B200_ARG_CHECK(eps, "null argument");
+  b200_eps E = new b200_eps_s;
+  E->stream = (cudaStream_t)stream;
+  *eps = E;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_destroy(b200_eps eps) {
+  if (!eps) return B200_OK;
+  b200_bv_destroy(eps->V);
+  cudaFree(eps->resid_buf);
+  delete eps;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_set_operators(b200_eps eps, b200_mat A) {
+  B200_ARG_CHECK(eps && A, "null argument");
+  eps->A = A;
+  eps->solved = false;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_set_dimensions(b200_eps eps, int nev, int ncv, int mpd) {
+  B200_ARG_CHECK(eps && nev > 0, "nev must be positive");
+  eps->nev = nev;
+  eps->ncv = ncv;
+  eps->mpd = mpd;
+  eps->solved = false;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_set_tolerances(b200_eps eps, double tol, int max_it) {
+  B200_ARG_CHECK(eps, "null argument");
+  eps->tol = tol;
+  eps->max_it = max_it;
+  eps->solved = false;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_set_which_eigenpairs(b200_eps eps, int which) {
+  B200_ARG_CHECK(eps && which >= B200_LARGEST_MAGNITUDE && which <= B200_SMALLEST_REAL, "unsupported which");
+  eps->which = which;
+  eps->solved = false;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_krylovschur_set_restart(b200_eps eps, double keep) {
+  B200_ARG_CHECK(eps && keep >= 0.1 && keep <= 0.9, "keep must be in [0.1,0.9]");
+  eps->keep = keep;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_set_initial_space(b200_eps eps, const double *v0) {
+  B200_ARG_CHECK(eps && v0 && eps->A, "set the operator before the initial space");
+  eps->v0.assign(v0, v0 + eps->A->n);
+  eps->v0_dev = nullptr;
+  eps->nini = 1;
+  eps->solved = false;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_set_initial_space_device(b200_eps eps, const double *v0) {
+  B200_ARG_CHECK(eps && v0 && eps->A, "set the operator before the initial space");
+  eps->v0.clear();
+  eps->v0_dev = v0;
+  eps->nini = 1;
+  eps->solved = false;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_set_max_restarts(b200_eps eps, int max_restarts) {
+  B200_ARG_CHECK(eps && max_restarts >= 0, "invalid argument");
+  eps->max_restarts = max_restarts;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_set_timing(b200_eps eps, int on) {
+  B200_ARG_CHECK(eps, "null argument");
+  eps->timing = on;
+  return B200_OK;
+}
+
+// EPSSetDimensions_Default (epssetup.c:669-713) + EPSSetUp_KrylovSchur checks (krylovschur.c:105-112).
+static b200_status eps_setup(b200_eps eps) {
+  B200_ARG_CHECK(eps->A, "EPSSetOperators must be called first");
+  const int n = eps->A->n;
+  int nev = eps->nev, ncv = eps->ncv, mpd = eps->mpd;
+  if (ncv > 0) {
+    B200_ARG_CHECK(ncv >= nev + 1 || (ncv == nev && ncv == n), "the value of ncv must be at least nev+1");
+  } else if (mpd > 0) {
+    ncv = std::min(n, nev + mpd);
+  } else {
+    if (nev < 500) ncv = std::min(n, std::max(2 * nev, nev + 15));
+    else {
+      mpd = 500;
+      ncv = std::min(n, nev + mpd);
+    }
+  }
+  if (mpd <= 0) mpd = ncv;
+  B200_ARG_CHECK(ncv <= nev + mpd, "the value of ncv must not be larger than nev+mpd");
+  B200_ARG_CHECK(ncv <= n, "ncv cannot exceed the problem size");
+  B200_ARG_CHECK(ncv + 2 < kMaxCols, "ncv too large for this build (ncv <= 251)");
+  eps->n_ = n;
+  eps->ncv_ = ncv;
+  eps->mpd_ = mpd;
+  eps->max_it_ = eps->max_it > 0 ? eps->max_it : std::max(100, 2 * n / ncv);
+  eps->tol_ = eps->tol > 0.0 ? eps->tol : 1e-8;  // SLEPC_DEFAULT_TOL (slepcmath.h:25)
+  if (eps->V) {
+    int bn, bm, bld;
+    b200_bv_get_sizes(eps->V, &bn, &bm, &bld);
+    if (bn != n || bm != ncv + 1 || eps->V->stream != eps->stream) {
+      b200_bv_destroy(eps->V);
+      eps->V = nullptr;
+    }
+  }
+  if (!eps->V) B200_CHECK(b200_bv_create(n, ncv + 1, eps->stream, &eps->V));  // EPSAllocateSolution(eps,1)
+  eps->ds.allocate(ncv + 1);  // DSAllocate(ds, ncv+1)
+  eps->ds.set_which(eps->which);
+  eps->eigr.assign(ncv + 1, 0.0);
+  eps->errest.assign(ncv + 1, 0.0);
+  eps->perm.assign(ncv + 1, 0);
+  for (int i = 0; i <= ncv; ++i) eps->perm[i] = i;
+  if (!eps->resid_buf) B200_CUDA_CHECK(cudaMalloc(&eps->resid_buf, sizeof(double) * 8));
+  return B200_OK;
+}
+
+// EPSGetStartVector (epssolve.c:841-870): column i, random unless i == 0 and an initial vector exists.
+static b200_status eps_start_vector(b200_eps eps, int i, int *breakdown) {
+  b200_bv bv = eps->V;
+  if (i > 0 || eps->nini == 0) B200_CUDA_CHECK(random_launch(col(bv, i), bv->n, bv->seed, bv->nrand++, bv->stream));
+  double norm = 0.0;
+  int lindep = 0;
+  B200_CHECK(bv_orth_column(bv, i, 0, nullptr, &norm, &lindep));
+  if (breakdown) *breakdown = lindep;
+  else if (lindep || norm == 0.0) {
+    b200_set_last_error(__FILE__, __LINE__,
+                        i ? "unable to generate more start vectors" : "initial vector is zero or in the deflation space");
+    return B200_ERR_BREAKDOWN;
+  }
+  if (norm != 0.0) B200_CHECK(b200_bv_scale_column(bv, i, 1.0 / norm));
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_solve(b200_eps eps) {
+  B200_ARG_CHECK(eps, "null argument");
+  B200_CHECK(eps_setup(eps));
+  b200_bv V = eps->V;
+  DsHep &ds = eps->ds;
+  const int ncv = eps->ncv_, mpd = eps->mpd_, nev = eps->nev;
+  const double tol = eps->tol_;
+  memset(&eps->stats, 0, sizeof(eps->stats));
+  const uint64_t launches0 = launch_count();
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  cudaEventRecord(t0, eps->stream);
+  RunTimer timer;
+  timer.on = eps->timing != 0;
+  double ms_restart = 0.0;
+  cudaEvent_t r0 = nullptr, r1 = nullptr;
+  if (timer.on) {
+    cudaEventCreate(&r0);
+    cudaEventCreate(&r1);
+  }
+
+  eps->nconv = 0;
+  eps->its = 0;
+  eps->reason = B200_CONVERGED_ITERATING;
+  eps->solved = false;
+  V->nrand = 0;
+  b200_bv_set_active_columns(V, 0, V->m);
+
+  // EPSSetUp: BVInsertVecs(V,0,&k,IS,TRUE) (epssetup.c:424, bvfunc.c:331-374)
+  if (eps->nini) {
+    if (eps->v0_dev) B200_CUDA_CHECK(copy_launch(col(V, 0), eps->v0_dev, V->n, V->stream));
+    else
+      B200_CUDA_CHECK(
+          cudaMemcpyAsync(col(V, 0), eps->v0.data(), sizeof(double) * V->n, cudaMemcpyHostToDevice, V->stream));
+    double norm = 0.0;
+    int lindep = 0;
+    B200_CHECK(bv_orth_column(V, 0, 0, nullptr, &norm, &lindep));
+    if (norm == 0.0 || lindep) {
+      b200_set_last_error(__FILE__, __LINE__, "the initial vector is zero");
+      return B200_ERR_BREAKDOWN;
+    }
+    B200_CHECK(b200_bv_scale_column(V, 0, 1.0 / norm));
+  }
+  B200_CHECK(eps_start_vector(eps, 0, nullptr));
+
+  int l = 0;
+  double beta = 0.0;
+  while (eps->reason == B200_CONVERGED_ITERATING) {
+    eps->its++;
+    int nv = std::min(eps->nconv + mpd, ncv);
+    ds.set_dimensions(nv, eps->nconv, eps->nconv + l);
+    int breakdown = 0;
+    GsState st{};
+    B200_CHECK(bv_lanczos(V, eps->A, eps->nconv + l, &nv, ds.d(), ds.e(), &beta, &breakdown, &timer, &st));
+    eps->stats.lanczos_steps += nv - (eps->nconv + l);
+    for (int j = eps->nconv + l; j < nv; ++j) eps->stats.column_visits += j + 2;
+    eps->stats.gs_passes += st.passes;
+    eps->stats.gs_bytes += (int64_t)st.bytes;
+    ds.set_dimensions(nv, eps->nconv, eps->nconv + l);
+    ds.set_state(l ? DsHep::kRaw : DsHep::kIntermediate);
+    b200_bv_set_active_columns(V, eps->nconv, nv);
+
+    B200_CHECK(ds.solve(eps->eigr.data()));
+    ds.sort(eps->eigr.data());
+    ds.update_extra_row();
+
+    // EPSKrylovConvergence: errest_i = beta*|Q(n-1,i)| / |theta_i|, stop at the first failure
+    int k = nv;
+    for (int kk = eps->nconv; kk < nv; ++kk) {
+      const double re = eps->eigr[kk];
+      const double resnorm = std::fabs(ds.Q()[ds.n() - 1 + (size_t)kk * ds.ld()]) * beta;
+      const double w = std::fabs(re);
+      eps->errest[kk] = (w != 0.0) ? resnorm / w : 1.79769313486231571e+308;
+      if (eps->errest[kk] >= tol) {
+        k = kk;
+        break;
+      }
+    }
+    // EPSStoppingBasic
+    if (k >= nev) eps->reason = B200_CONVERGED_TOL;
+    else if (eps->its >= eps->max_it_) eps->reason = B200_DIVERGED_ITS;
+
+    if (eps->reason != B200_CONVERGED_ITERATING || breakdown || k == nv) l = 0;
+    else l = std::max(1, (int)((nv - k) * eps->keep));
+
+    if (eps->reason == B200_CONVERGED_ITERATING) {
+      if (breakdown || k == nv) {
+        if (k < nev) {
+          int bd = 0;
+          B200_CHECK(eps_start_vector(eps, k, &bd));
+          if (bd) eps->reason = B200_DIVERGED_BREAKDOWN;
+        }
+      } else {
+        ds.truncate(k + l);
+      }
+    }
+    // BVMultInPlace(V,Q,nconv,k+l) over the active columns [nconv,nv)
+    if (timer.on) cudaEventRecord(r0, V->stream);
+    B200_CHECK(b200_bv_mult_inplace(V, ds.Q(), ds.ld(), eps->nconv, k + l));
+    if (timer.on) cudaEventRecord(r1, V->stream);
+    if (eps->reason == B200_CONVERGED_ITERATING && !breakdown) B200_CHECK(b200_bv_copy_column(V, nv, k + l));
+    if (timer.on) {
+      cudaEventSynchronize(r1);
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, r0, r1) == cudaSuccess) ms_restart += t;
+    }
+    eps->nconv = k;
+    eps->stats.restarts++;
+    if (eps->max_restarts > 0 && eps->stats.restarts >= eps->max_restarts &&
+        eps->reason == B200_CONVERGED_ITERATING)
+      break;
+  }
+  B200_CUDA_CHECK(cudaStreamSynchronize(V->stream));
+  // SlepcSortEigenvalues (slepcsc.c:89-149) over the converged pairs
+  for (int i = 0; i <= ncv; ++i) eps->perm[i] = i;
+  for (int i = eps->nconv - 1; i >= 0; --i) {
+    const double re = eps->eigr[eps->perm[i]];
+    int j = i + 1;
+    while (j < eps->nconv) {
+      if (DsHep::compare(eps->which, re, eps->eigr[eps->perm[j]]) <= 0) break;
+      std::swap(eps->perm[j - 1], eps->perm[j]);
+      ++j;
+    }
+  }
+  cudaEventRecord(t1, eps->stream);
+  cudaEventSynchronize(t1);
+  float total = 0.f;
+  cudaEventElapsedTime(&total, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  if (r0) cudaEventDestroy(r0);
+  if (r1) cudaEventDestroy(r1);
+  eps->stats.ms_total = total;
+  eps->stats.ms_spmv = timer.ms_spmv;
+  eps->stats.ms_orth = timer.ms_orth;
+  eps->stats.ms_restart = ms_restart;
+  eps->stats.kernel_launches = (int64_t)(launch_count() - launches0);
+  eps->solved = true;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_get_converged(b200_eps eps, int *nconv) {
+  B200_ARG_CHECK(eps && nconv, "null argument");
+  if (!eps->solved) {
+    b200_set_last_error(__FILE__, __LINE__, "EPSSolve must be called first");
+    return B200_ERR_STATE;
+  }
+  *nconv = eps->nconv;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_get_iteration_number(b200_eps eps, int *its) {
+  B200_ARG_CHECK(eps && its, "null argument");
+  *its = eps->its;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_get_converged_reason(b200_eps eps, int *reason) {
+  B200_ARG_CHECK(eps && reason, "null argument");
+  *reason = eps->reason;
+  return B200_OK;
+}
+
+static b200_status eps_check_index(b200_eps eps, int i) {
+  if (!eps->solved) {
+    b200_set_last_error(__FILE__, __LINE__, "EPSSolve must be called first");
+    return B200_ERR_STATE;
+  }
+  B200_ARG_CHECK(i >= 0 && i < eps->nconv, "eigenpair index out of range");
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_get_eigenpair(b200_eps eps, int i, double *eigr, double *x) {
+  B200_ARG_CHECK(eps, "null argument");
+  B200_CHECK(eps_check_index(eps, i));
+  const int p = eps->perm[i];
+  if (eigr) *eigr = eps->eigr[p];
+  if (x) {
+    B200_CUDA_CHECK(
+        cudaMemcpyAsync(x, col(eps->V, p), sizeof(double) * eps->n_, cudaMemcpyDeviceToHost, eps->V->stream));
+    B200_CUDA_CHECK(cudaStreamSynchronize(eps->V->stream));
+  }
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_get_eigenvector_device(b200_eps eps, int i, const double **x) {
+  B200_ARG_CHECK(eps && x, "null argument");
+  B200_CHECK(eps_check_index(eps, i));
+  *x = col(eps->V, eps->perm[i]);
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_get_error_estimate(b200_eps eps, int i, double *errest) {
+  B200_ARG_CHECK(eps && errest, "null argument");
+  B200_CHECK(eps_check_index(eps, i));
+  *errest = eps->errest[eps->perm[i]];
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_compute_error(b200_eps eps, int i, int type, double *error) {
+  B200_ARG_CHECK(eps && error, "null argument");
+  B200_CHECK(eps_check_index(eps, i));
+  const int p = eps->perm[i];
+  const double lam = eps->eigr[p];
+  b200_mat A = eps->A;
+  b200_bv V = eps->V;
+  // ||A x - lambda x||_2, with the shift skipped for |lambda| <= eps (epssolve.c:689-694)
+  const double shift = (std::fabs(lam) > 2.220446049250313e-16) ? lam : 0.0;
+  B200_CUDA_CHECK(
+      residual_launch(A->n, A->rowptr, A->colind, A->vals, col(V, p), shift, eps->resid_buf, V->red, V->red_len, A->lanes,
+                      V->stream));
+  B200_CUDA_CHECK(cudaMemcpyAsync(V->hpin, eps->resid_buf, sizeof(double), cudaMemcpyDeviceToHost, V->stream));
+  B200_CUDA_CHECK(cudaStreamSynchronize(V->stream));
+  double r = std::sqrt(V->hpin[0]);
+  if (type == B200_ERROR_RELATIVE) r /= std::fabs(lam);
+  *error = r;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_get_stats(b200_eps eps, b200_eps_stats *stats) {
+  B200_ARG_CHECK(eps && stats, "null argument");
+  *stats = eps->stats;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_solve_csr_host(int n, int64_t nnz, const int *rowptr, const int *colind,
+                                               const double *vals, const double *v0, int nev, int ncv, int mpd,
+                                               double tol, int max_it, int which, double *evals, double *X,
+                                               double *errest, int *info, void *stream) {
+  b200_mat A = nullptr;
+  b200_eps E = nullptr;
+  B200_CHECK(b200_mat_create_csr(n, nnz, rowptr, colind, vals, stream, &A));
+  b200_status s = b200_eps_create(stream, &E);
+  if (s == B200_OK) s = b200_eps_set_operators(E, A);
+  if (s == B200_OK) s = b200_eps_set_dimensions(E, nev, ncv, mpd);
+  if (s == B200_OK) s = b200_eps_set_tolerances(E, tol, max_it);
+  if (s == B200_OK) s = b200_eps_set_which_eigenpairs(E, which);
+  if (s == B200_OK && v0) s = b200_eps_set_initial_space(E, v0);
+  if (s == B200_OK) s = b200_eps_solve(E);
+  if (s == B200_OK) {
+    for (int i = 0; i < E->nconv && s == B200_OK; ++i) {
+      double lam = 0.0;
+      s = b200_eps_get_eigenpair(E, i, &lam, X ? X + (size_t)i * n : nullptr);
+      if (evals) evals[i] = lam;
+      if (errest) errest[i] = E->errest[E->perm[i]];
+    }
+    if (info) {
+      info[0] = E->nconv;
+      info[1] = E->its;
+      info[2] = E->reason;
+      info[3] = (int)E->stats.lanczos_steps;
+      info[4] = (int)E->stats.restarts;
+    }
+  }
+  b200_eps_destroy(E);
+  b200_mat_destroy(A);
+  return s;
+}

@@ -1,0 +1,88 @@
+"""Synthetic operators and start vectors for the Krylov-Schur workloads.
+
+All matrices are returned as CSR triples (rowptr int32, colind int32,
+values float64) with column indices sorted inside each row, which is what
+PETSc's MatAssembly produces for MATSEQAIJ.
+"""
+import numpy as np
+
+
+def laplacian_2d(n, m=None):
+    """2-D 5-point Dirichlet Laplacian on an n x m grid in the ordering of
+    SLEPc's ``src/eps/tutorials/ex2.c:46-53``: row II has i = II // n,
+    j = II - i*n, diagonal 4 and -1 at II-n, II-1, II+1, II+n (when inside)."""
+    m = n if m is None else m
+    N = n * m
+    II = np.arange(N, dtype=np.int64)
+    i = II // n
+    j = II - i * n
+    cols, vals = [], []
+    # sorted column order: II-n < II-1 < II < II+1 < II+n
+    cols.append(np.where(i > 0, II - n, -1)); vals.append(-1.0)
+    cols.append(np.where(j > 0, II - 1, -1)); vals.append(-1.0)
+    cols.append(II); vals.append(4.0)
+    cols.append(np.where(j < n - 1, II + 1, -1)); vals.append(-1.0)
+    cols.append(np.where(i < m - 1, II + n, -1)); vals.append(-1.0)
+    return _stack(N, cols, vals)
+
+
+def laplacian_3d(nx, ny=None, nz=None):
+    """3-D 7-point Dirichlet Laplacian on an nx x ny x nz grid, lexicographic
+    ordering (x fastest): diagonal 6, -1 at +-1, +-nx, +-nx*ny."""
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    N = nx * ny * nz
+    II = np.arange(N, dtype=np.int64)
+    x = II % nx
+    y = (II // nx) % ny
+    z = II // (nx * ny)
+    sxy = nx * ny
+    cols, vals = [], []
+    cols.append(np.where(z > 0, II - sxy, -1)); vals.append(-1.0)
+    cols.append(np.where(y > 0, II - nx, -1)); vals.append(-1.0)
+    cols.append(np.where(x > 0, II - 1, -1)); vals.append(-1.0)
+    cols.append(II); vals.append(6.0)
+    cols.append(np.where(x < nx - 1, II + 1, -1)); vals.append(-1.0)
+    cols.append(np.where(y < ny - 1, II + nx, -1)); vals.append(-1.0)
+    cols.append(np.where(z < nz - 1, II + sxy, -1)); vals.append(-1.0)
+    return _stack(N, cols, vals)
+
+
+def _stack(N, cols, vals):
+    C = np.stack(cols, axis=1)
+    Vv = np.broadcast_to(np.asarray(vals, dtype=np.float64), C.shape)
+    mask = C >= 0
+    counts = mask.sum(axis=1)
+    rowptr = np.zeros(N + 1, dtype=np.int64)
+    np.cumsum(counts, out=rowptr[1:])
+    colind = C[mask].astype(np.int32)
+    values = np.ascontiguousarray(Vv[mask], dtype=np.float64)
+    return rowptr.astype(np.int32), colind, values
+
+
+def laplacian_2d_eigs(n, m=None):
+    m = n if m is None else m
+    a = 2 - 2 * np.cos(np.pi * np.arange(1, n + 1) / (n + 1))
+    b = 2 - 2 * np.cos(np.pi * np.arange(1, m + 1) / (m + 1))
+    return (a[:, None] + b[None, :]).ravel()
+
+
+def laplacian_3d_eigs(nx, ny=None, nz=None):
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    a = [2 - 2 * np.cos(np.pi * np.arange(1, k + 1) / (k + 1)) for k in (nx, ny, nz)]
+    return (a[0][:, None, None] + a[1][None, :, None] + a[2][None, None, :]).ravel()
+
+
+def start_vector(n, seed=0):
+    """Seeded N(0,1) start vector (the EPSSetInitialSpace vector shared by the
+    GPU path and the oracle)."""
+    return np.random.default_rng(seed).standard_normal(n)
+
+
+def to_scipy(csr, n=None):
+    import scipy.sparse as sp
+
+    rowptr, colind, vals = csr
+    n = len(rowptr) - 1 if n is None else n
+    return sp.csr_matrix((vals, colind, rowptr), shape=(n, n))

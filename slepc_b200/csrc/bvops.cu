@@ -259,7 +259,7 @@ cudaError_t multinplace_launch(double *V, int ld, int n, int l, int k, const dou
   if (nc <= 0 || kq <= 0 || n <= 0) return cudaSuccess;
   if (nc > 16 * 8 || kq > kMaxCols) return cudaErrorInvalidValue;
   const size_t smem = sizeof(double) * ((size_t)kq * nc + (size_t)(kq > nc ? kq : nc) * kRB);
-  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  if (smem + 1024 > max_dynamic_smem()) return cudaErrorInvalidValue;
   const int maxj = (nc + 15) / 16;
   const int npanels = (n + kRB - 1) / kRB;
   int grid = num_sms() * 2;
@@ -268,7 +268,7 @@ cudaError_t multinplace_launch(double *V, int ld, int n, int l, int k, const dou
   switch (maxj) {
 #define B200_MIP_CASE(J)                                                                                         \
   case J:                                                                                                        \
-    err = cudaFuncSetAttribute(multinplace_kernel<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024); \
+    err = allow_max_dynamic_smem(multinplace_kernel<J>);                                                        \
     if (err != cudaSuccess) return err;                                                                          \
     multinplace_kernel<J><<<grid, kGemmThreads, smem, stream>>>(V, ld, n, l, kq, Q, ldq, s, nc);                 \
     break;

@@ -211,6 +211,8 @@ __device__ void decide(const PassParams &p, const double *cnew_s, DecideShared &
   }
 }
 
+// MAXCPW: largest number of dot columns one warp owns (columns warp, warp+8, ...).
+template <int MAXCPW>
 __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   GsState *st = p.st;
@@ -220,7 +222,7 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p) {
   if (action == kActNone) return;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int CH = p.chunk;
+  const int CH = p.chunk;  // power of two, 32..2048
   const int jb = a.jb;
   const bool do_update = (action & kActUpdate) != 0;
   const bool do_dot = (action & kActDot) != 0;
@@ -234,6 +236,7 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p) {
   double *cacc = coef_s + kMaxCols;           // [kMaxCols + 1]
   DecideShared *dsh = reinterpret_cast<DecideShared *>(cacc + kMaxCols + 1);
   __shared__ int is_last;
+  __shared__ double upd[kThreads];            // partial row sums of the update (several threads per row)
   const size_t head = 128 + sizeof(double) * (2 * kMaxCols + 1) + ((sizeof(DecideShared) + 127) / 128) * 128;
   double *stage_base = reinterpret_cast<double *>(smem_raw + ((head + 127) / 128) * 128);
   const size_t stage_elems = (size_t)CH * (jb + 1);
@@ -243,28 +246,40 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p) {
     fence_mbar_init();
   }
   for (int i = tid; i < jb; i += kThreads) coef_s[i] = do_update ? p.coef[i] : 0.0;
-  for (int i = tid; i <= jb; i += kThreads) cacc[i] = 0.0;
   __syncthreads();
 
   const int G = p.G;
   const int nmine = (p.nchunks > (int)blockIdx.x) ? (p.nchunks - 1 - (int)blockIdx.x) / G + 1 : 0;
-  const double *Vw = a.V + (size_t)a.wcol * a.ld;
-  double *Vw_out = a.V + (size_t)a.wcol * a.ld;
+  double *Vw = a.V + (size_t)a.wcol * a.ld;
 
+  // warp 0 issues a chunk: lane 0 arms the barrier, the 32 lanes issue the column copies in parallel
   auto issue = [&](int i, int s) {
-    const long long q = (long long)blockIdx.x + (long long)i * G;
-    const long long r0 = q * CH;
+    const long long r0 = ((long long)blockIdx.x + (long long)i * G) * CH;
     const int rows = (int)min((long long)CH, (long long)a.n - r0);
     const uint32_t bytes = (uint32_t)(((rows * 8) + 15) & ~15);
     double *buf = stage_base + (size_t)s * stage_elems;
-    mbar_arrive_expect_tx(&bars[s], bytes * (uint32_t)(ncl + 1));
-    bulk_load(buf, Vw + r0, bytes, &bars[s]);
-    for (int c = 0; c < ncl; ++c) bulk_load(buf + (size_t)(c + 1) * CH, a.V + (size_t)c * a.ld + r0, bytes, &bars[s]);
+    if (lane == 0) mbar_arrive_expect_tx(&bars[s], bytes * (uint32_t)(ncl + 1));
+    __syncwarp();
+    for (int c = lane - 1; c < ncl; c += 32) {
+      if (c < 0) bulk_load(buf, Vw + r0, bytes, &bars[s]);
+      else bulk_load(buf + (size_t)(c + 1) * CH, a.V + (size_t)c * a.ld + r0, bytes, &bars[s]);
+    }
   };
 
-  if (tid == 0) {
+  if (warp == 0) {
     for (int s = 0; s < kStages && s < nmine; ++s) issue(s, s);
   }
+
+  // dot accumulators: lane-private partial sums of the columns this warp owns, across all chunks
+  double acc[MAXCPW];
+#pragma unroll
+  for (int t = 0; t < MAXCPW; ++t) acc[t] = 0.0;
+
+  // update mapping: TPR threads per row when a chunk has fewer rows than threads
+  const int TPR = (CH >= kThreads) ? 1 : kThreads / CH;
+  const int part = (TPR > 1) ? tid / CH : 0;
+  const int rbase = (TPR > 1) ? tid % CH : tid;
+  const int rstride = (TPR > 1) ? CH : kThreads;
 
   bool timed_out = false;
   for (int i = 0; i < nmine; ++i) {
@@ -282,33 +297,54 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p) {
     const double *Vs = ws + CH;  // column c at Vs + c*CH
 
     if (do_update || do_scale) {
-      for (int r = tid; r < rows; r += kThreads) {
-        double wv = ws[r];
-        if (do_update) {
-          double acc = 0.0;
-          for (int c = 0; c < jb; ++c) acc = fma(Vs[(size_t)c * CH + r], coef_s[c], acc);
-          wv -= acc;
+      for (int r = rbase; r < CH; r += rstride) {
+        double sum = 0.0;
+        if (do_update && r < rows) {
+          double a0 = 0.0, a1 = 0.0;
+          int c = part;
+          for (; c + TPR < jb; c += 2 * TPR) {
+            a0 = fma(Vs[(size_t)c * CH + r], coef_s[c], a0);
+            a1 = fma(Vs[(size_t)(c + TPR) * CH + r], coef_s[c + TPR], a1);
+          }
+          if (c < jb) a0 = fma(Vs[(size_t)c * CH + r], coef_s[c], a0);
+          sum = a0 + a1;
         }
-        if (do_scale) wv *= scale;
-        ws[r] = wv;
-        Vw_out[r0 + r] = wv;
+        if (TPR > 1) {
+          upd[tid] = sum;
+        } else if (r < rows) {
+          double wv = ws[r] - sum;
+          if (do_scale) wv *= scale;
+          ws[r] = wv;
+          Vw[r0 + r] = wv;
+        }
+      }
+      if (TPR > 1) {
+        __syncthreads();
+        if (part == 0 && rbase < rows) {
+          double tot = 0.0;
+          for (int q = 0; q < TPR; ++q) tot += upd[q * CH + rbase];
+          double wv = ws[rbase] - tot;
+          if (do_scale) wv *= scale;
+          ws[rbase] = wv;
+          Vw[r0 + rbase] = wv;
+        }
       }
       __syncthreads();
     }
     if (do_dot) {
-      for (int c = warp; c <= jb; c += kWarps) {
-        const double *col = (c == jb) ? ws : Vs + (size_t)c * CH;
-        double sacc = 0.0;
-        for (int r = lane; r < rows; r += 32) sacc = fma(col[r], ws[r], sacc);
-        sacc = warp_sum(sacc);
-        if (lane == 0) cacc[c] += sacc;
+      for (int r = lane; r < rows; r += 32) {
+        const double wr = ws[r];
+#pragma unroll
+        for (int t = 0; t < MAXCPW; ++t) {
+          const int c = warp + kWarps * t;
+          if (c < jb) acc[t] = fma(Vs[(size_t)c * CH + r], wr, acc[t]);
+          else if (c == jb) acc[t] = fma(wr, wr, acc[t]);
+        }
       }
     }
+    fence_proxy_async();  // generic-proxy smem accesses ordered before the next bulk copy into this stage
     __syncthreads();
-    if (tid == 0 && i + kStages < nmine) {
-      fence_proxy_async();
-      issue(i + kStages, s);
-    }
+    if (warp == 0 && i + kStages < nmine) issue(i + kStages, s);
   }
   if (timed_out) {
     // Drain copies still in flight on either stage (bounded), report, and leave.
@@ -319,9 +355,16 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p) {
     __syncthreads();
     return;
   }
+
   // per-CTA column sums -> partials[c * G + cta]
-  if (do_dot)
-    for (int c = tid; c <= jb; c += kThreads) p.partials[(size_t)c * G + blockIdx.x] = cacc[c];
+  if (do_dot) {
+#pragma unroll
+    for (int t = 0; t < MAXCPW; ++t) {
+      const int c = warp + kWarps * t;
+      const double v = warp_sum(acc[t]);
+      if (lane == 0 && c <= jb) p.partials[(size_t)c * G + blockIdx.x] = v;
+    }
+  }
   __threadfence();
   __syncthreads();
   if (tid == 0) is_last = (atomicAdd(&st->ticket, 1u) == (unsigned)(G - 1));
@@ -343,7 +386,7 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p) {
   }
 
   // Fixed-order reduction across CTAs: lane b sums CTAs b, b+32, ...; then a fixed shuffle tree.
-  double *cnew_s = cacc;  // reuse
+  double *cnew_s = cacc;
   for (int c = warp; c <= jb; c += kWarps) {
     double sacc = 0.0;
     for (int b = lane; b < G; b += 32) sacc += __ldcg(p.partials + (size_t)c * G + b);
@@ -365,22 +408,27 @@ size_t pass_smem_bytes(int jb, int CH) {
 }
 
 int pass_chunk_rows(int jb) {
-  size_t ch = kStageBudget / ((size_t)(jb + 1) * sizeof(double));
-  ch = (ch / 32) * 32;
-  if (ch < 32) ch = 32;
-  if (ch > 2048) ch = 2048;
-  return (int)ch;
+  const size_t budget = kStageBudget / ((size_t)(jb + 1) * sizeof(double));
+  int ch = 32;
+  while (ch < 2048 && (size_t)(2 * ch) <= budget) ch *= 2;
+  return ch;
 }
 
-cudaError_t launch_pass(const GsPassArgs &a, const GsWork &w, int first, int plain_dot, cudaStream_t stream) {
+template <int M>
+cudaError_t launch_pass_t(const PassParams &p, size_t smem, cudaStream_t stream) {
   static bool attr_set[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !attr_set[dev]) {
-    cudaError_t e = cudaFuncSetAttribute(gs_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaError_t e = allow_max_dynamic_smem(gs_pass_kernel<M>);
     if (e != cudaSuccess) return e;
     attr_set[dev] = true;
   }
+  gs_pass_kernel<M><<<p.G, kThreads, smem, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pass(const GsPassArgs &a, const GsWork &w, int first, int plain_dot, cudaStream_t stream) {
   PassParams p;
   p.a = a;
   p.st = w.st;
@@ -397,9 +445,18 @@ cudaError_t launch_pass(const GsPassArgs &a, const GsWork &w, int first, int pla
   if (G < 1) G = 1;
   p.G = G;
   const size_t smem = pass_smem_bytes(a.jb, p.chunk);
-  gs_pass_kernel<<<G, kThreads, smem, stream>>>(p);
+  if (smem + 4096 > max_dynamic_smem()) return cudaErrorInvalidValue;
+  const int cpw = (a.jb + 1 + kWarps - 1) / kWarps;  // dot columns per warp (basis + self)
+  cudaError_t e;
+  if (cpw <= 2) e = launch_pass_t<2>(p, smem, stream);
+  else if (cpw <= 4) e = launch_pass_t<4>(p, smem, stream);
+  else if (cpw <= 8) e = launch_pass_t<8>(p, smem, stream);
+  else if (cpw <= 12) e = launch_pass_t<12>(p, smem, stream);
+  else if (cpw <= 16) e = launch_pass_t<16>(p, smem, stream);
+  else if (cpw <= 32) e = launch_pass_t<32>(p, smem, stream);
+  else return cudaErrorInvalidValue;
   count_launch();
-  return cudaGetLastError();
+  return e;
 }
 
 }  // namespace

@@ -1,19 +1,50 @@
 // Launch wrappers of the device kernels (internal to the library).
 #pragma once
 
+#include <vector>
+
 #include "common.h"
 
 namespace b200 {
+
+// Allow a kernel the largest dynamic shared memory the device grants per
+// block (the opt-in maximum less the kernel's static shared memory).
+template <typename K>
+cudaError_t allow_max_dynamic_smem(K kernel) {
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa;
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kernel);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+  return e;
+}
+
+// Largest dynamic shared memory a block may request on the current device.
+inline size_t max_dynamic_smem() {
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return (size_t)optin;
+}
 
 void count_launch();
 uint64_t launch_count();
 
 // ---- SpMV (spmv.cu)
+constexpr int kTileNnz = 4096;   // nonzeros staged per CTA of the row-block SpMV
+constexpr int kTileRows = 1024;  // rows per CTA of the row-block SpMV
 int spmv_choose_lanes(int n, int64_t nnz);
+// Row blocks for the row-block SpMV: block b covers rows [b[i], b[i+1]).
+std::vector<int> spmv_row_blocks(int n, const int *rowptr_host);
 // st/step: when st is given, the launch is skipped on the device if a
 // Lanczos run halted (breakdown) at an earlier step.
+cudaError_t spmv_rowblock_launch(int nblocks, const int *blocks, const int *rowptr, const int *colind,
+                                 const double *vals, const double *x, double *y, cudaStream_t stream,
+                                 const GsState *st = nullptr, int step = 0);
 cudaError_t spmv_launch(int n, const int *rowptr, const int *colind, const double *vals, const double *x, double *y,
-                        int lanes, cudaStream_t stream, const GsState *st = nullptr, int step = 0);
+                        int lanes, cudaStream_t stream);
 
 // ---- Fused Gram-Schmidt passes (gs.cu)
 // Device workspace of one BV for the Gram-Schmidt kernels.

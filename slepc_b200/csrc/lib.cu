@@ -60,8 +60,25 @@ struct b200_mat_s {
   int *rowptr = nullptr, *colind = nullptr;
   double *vals = nullptr;
   int lanes = 8;
+  int *blocks = nullptr;  // row blocks of the row-block SpMV (nblocks + 1 entries)
+  int nblocks = 0;
   cudaStream_t stream = nullptr;
 };
+
+// Row blocks from a host copy of rowptr, uploaded to the device.
+static b200_status mat_set_blocks(b200_mat M, const int *rowptr_host) {
+  std::vector<int> b = spmv_row_blocks(M->n, rowptr_host);
+  M->nblocks = (int)b.size() - 1;
+  B200_CUDA_CHECK(cudaMalloc(&M->blocks, sizeof(int) * b.size()));
+  B200_CUDA_CHECK(cudaMemcpyAsync(M->blocks, b.data(), sizeof(int) * b.size(), cudaMemcpyHostToDevice, M->stream));
+  B200_CUDA_CHECK(cudaStreamSynchronize(M->stream));
+  return B200_OK;
+}
+
+static cudaError_t mat_spmv(b200_mat A, const double *x, double *y, cudaStream_t stream, const GsState *st = nullptr,
+                            int step = 0) {
+  return spmv_rowblock_launch(A->nblocks, A->blocks, A->rowptr, A->colind, A->vals, x, y, stream, st, step);
+}
 
 static b200_status mat_alloc(int n, int64_t nnz, cudaStream_t stream, b200_mat *A) {
   b200_mat M = new b200_mat_s;
@@ -101,6 +118,11 @@ extern "C" b200_status b200_mat_create_csr(int n, int64_t nnz, const int *rowptr
     b200_set_last_error(__FILE__, __LINE__, cudaGetErrorString(e));
     return B200_ERR_CUDA;
   }
+  b200_status st = mat_set_blocks(M, rowptr);
+  if (st != B200_OK) {
+    b200_mat_destroy(M);
+    return st;
+  }
   *A = M;
   return B200_OK;
 }
@@ -117,11 +139,24 @@ extern "C" b200_status b200_mat_create_csr_device(int n, int64_t nnz, const int 
     e = cudaMemcpyAsync(M->colind, colind, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToDevice, s);
   if (e == cudaSuccess && nnz)
     e = cudaMemcpyAsync(M->vals, vals, sizeof(double) * (size_t)nnz, cudaMemcpyDeviceToDevice, s);
+  std::vector<int> hrow((size_t)n + 1);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(hrow.data(), rowptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     b200_mat_destroy(M);
     b200_set_last_error(__FILE__, __LINE__, cudaGetErrorString(e));
     return B200_ERR_CUDA;
+  }
+  if (hrow[0] != 0 || hrow[n] != nnz) {
+    b200_mat_destroy(M);
+    b200_set_last_error(__FILE__, __LINE__, "rowptr must start at 0 and end at nnz");
+    return B200_ERR_ARG;
+  }
+  b200_status st = mat_set_blocks(M, hrow.data());
+  if (st != B200_OK) {
+    b200_mat_destroy(M);
+    return st;
   }
   *A = M;
   return B200_OK;
@@ -129,7 +164,7 @@ extern "C" b200_status b200_mat_create_csr_device(int n, int64_t nnz, const int 
 
 extern "C" b200_status b200_mat_mult(b200_mat A, const double *x, double *y) {
   B200_ARG_CHECK(A && x && y, "null argument");
-  B200_CUDA_CHECK(spmv_launch(A->n, A->rowptr, A->colind, A->vals, x, y, A->lanes, A->stream));
+  B200_CUDA_CHECK(mat_spmv(A, x, y, A->stream));
   return B200_OK;
 }
 
@@ -151,6 +186,7 @@ extern "C" b200_status b200_mat_destroy(b200_mat A) {
   cudaFree(A->rowptr);
   cudaFree(A->colind);
   cudaFree(A->vals);
+  cudaFree(A->blocks);
   delete A;
   return B200_OK;
 }
@@ -558,7 +594,7 @@ extern "C" b200_status b200_bv_copy_column(b200_bv bv, int j, int i) {
 
 extern "C" b200_status b200_bv_mat_mult_column(b200_bv bv, b200_mat A, int j) {
   B200_ARG_CHECK(bv && A && A->n == bv->n && j >= 0 && j + 1 < bv->m, "invalid BVMatMultColumn arguments");
-  B200_CUDA_CHECK(spmv_launch(A->n, A->rowptr, A->colind, A->vals, col(bv, j), col(bv, j + 1), A->lanes, bv->stream));
+  B200_CUDA_CHECK(mat_spmv(A, col(bv, j), col(bv, j + 1), bv->stream));
   return B200_OK;
 }
 
@@ -595,8 +631,7 @@ static b200_status bv_lanczos(b200_bv bv, b200_mat A, int k, int *m, double *alp
     cudaEvent_t e0 = timing ? timer->next() : nullptr, e1 = timing ? timer->next() : nullptr;
     cudaEvent_t e2 = timing ? timer->next() : nullptr, e3 = timing ? timer->next() : nullptr;
     if (e0) cudaEventRecord(e0, bv->stream);
-    B200_CUDA_CHECK(
-        spmv_launch(A->n, A->rowptr, A->colind, A->vals, col(bv, j), col(bv, j + 1), A->lanes, bv->stream, bv->gs.st, j));
+    B200_CUDA_CHECK(mat_spmv(A, col(bv, j), col(bv, j + 1), bv->stream, bv->gs.st, j));
     if (e1) cudaEventRecord(e1, bv->stream);
     GsPassArgs a{};
     a.V = bv->V;

@@ -1,24 +1,96 @@
 // CSR sparse matrix-vector product y = A x in FP64 for sm_100a.
 //
 // Replaces PETSc's MATAIJCUSPARSE MatMult behind BVMatMultColumn
-// (src/sys/classes/bv/interface/bvops.c:862-890).  Scheduling: a group of
-// LPR lanes (1..32, a power of two chosen from the mean row length) owns one
-// row; consecutive groups own consecutive rows, so a warp streams one
-// contiguous range of the value/column arrays.  Values and column indices
-// are read once with streaming (evict-first) loads; x goes through the
-// read-only path because every entry is reused by its neighbouring rows.
+// (src/sys/classes/bv/interface/bvops.c:862-890) and STApply
+// (src/sys/classes/st/interface/stsolve.c:45-60).
+//
+// Two schedules:
+//  * spmv_rowblock_kernel (used by b200_mat): rows are grouped on the host
+//    into blocks of at most kTileNnz nonzeros and kTileRows rows.  A CTA
+//    streams its block's values and column indices with coalesced,
+//    independent loads (many in flight per thread), multiplies by the
+//    gathered x (read-only path: neighbouring rows reuse x), keeps the
+//    rounded products in shared memory, then sums every row in index order
+//    with plain adds -- the order of PETSc's MatMult_SeqAIJ, so short rows
+//    give the same bits as a sequential CPU loop.  A row longer than
+//    kTileNnz gets a block of its own and a CTA-wide tree reduction.
+//  * spmv_csr_kernel (the stateless b200_csr_spmv entry): LPR lanes per row.
 #include "common.h"
 #include "kernels.h"
 
 namespace b200 {
 
+namespace {
+
+constexpr int kSpmvThreads = 256;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+__global__ void __launch_bounds__(kSpmvThreads) spmv_rowblock_kernel(const int *__restrict__ blocks,
+                                                                     const int *__restrict__ rowptr,
+                                                                     const int *__restrict__ colind,
+                                                                     const double *__restrict__ vals,
+                                                                     const double *__restrict__ x,
+                                                                     double *__restrict__ y,
+                                                                     const GsState *__restrict__ st, int step) {
+  if (st && st->halt && st->halt_step < step) return;
+  __shared__ double prod[kTileNnz];
+  __shared__ int rp[kTileRows + 1];
+  __shared__ double red[kSpmvThreads / 32];
+  const int tid = threadIdx.x;
+  const int r0 = blocks[blockIdx.x], r1 = blocks[blockIdx.x + 1];
+  const int nrows = r1 - r0;
+  const int p0 = rowptr[r0], p1 = rowptr[r1];
+  const int cnt = p1 - p0;
+  if (cnt > kTileNnz) {
+    // one long row: strided partial sums, then a fixed-order tree
+    double s = 0.0;
+    for (int p = p0 + tid; p < p1; p += kSpmvThreads) s = __dadd_rn(s, __dmul_rn(__ldcs(vals + p), __ldg(x + __ldcs(colind + p))));
+    s = warp_sum(s);
+    if ((tid & 31) == 0) red[tid >> 5] = s;
+    __syncthreads();
+    if (tid == 0) {
+      double t = 0.0;
+      for (int w = 0; w < kSpmvThreads / 32; ++w) t += red[w];
+      y[r0] = t;
+    }
+    return;
+  }
+  for (int r = tid; r <= nrows; r += kSpmvThreads) rp[r] = rowptr[r0 + r] - p0;
+  // stream the block's nonzeros: four independent (value, index, x) loads per thread in flight
+  int p = tid;
+  for (; p + 3 * kSpmvThreads < cnt; p += 4 * kSpmvThreads) {
+    double a[4];
+    int c[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a[u] = __ldcs(vals + p0 + p + u * kSpmvThreads);
+      c[u] = __ldcs(colind + p0 + p + u * kSpmvThreads);
+    }
+    double xv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) xv[u] = __ldg(x + c[u]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) prod[p + u * kSpmvThreads] = __dmul_rn(a[u], xv[u]);
+  }
+  for (; p < cnt; p += kSpmvThreads) prod[p] = __dmul_rn(__ldcs(vals + p0 + p), __ldg(x + __ldcs(colind + p0 + p)));
+  __syncthreads();
+  for (int r = tid; r < nrows; r += kSpmvThreads) {
+    double s = 0.0;
+    for (int q = rp[r]; q < rp[r + 1]; ++q) s = __dadd_rn(s, prod[q]);
+    y[r0 + r] = s;
+  }
+}
+
 template <int LPR>
 __global__ void __launch_bounds__(256) spmv_csr_kernel(int n, const int *__restrict__ rowptr,
                                                        const int *__restrict__ colind,
                                                        const double *__restrict__ vals,
-                                                       const double *__restrict__ x, double *__restrict__ y,
-                                                       const GsState *__restrict__ st, int step) {
-  if (st && st->halt && st->halt_step < step) return;
+                                                       const double *__restrict__ x, double *__restrict__ y) {
   constexpr int kRowsPerWarp = 32 / LPR;
   const int lane = threadIdx.x & (LPR - 1);
   const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -42,6 +114,8 @@ __global__ void __launch_bounds__(256) spmv_csr_kernel(int n, const int *__restr
   }
 }
 
+}  // namespace
+
 int spmv_choose_lanes(int n, int64_t nnz) {
   if (n <= 0) return 1;
   const double avg = (double)nnz / (double)n;
@@ -50,17 +124,41 @@ int spmv_choose_lanes(int n, int64_t nnz) {
   return lanes;
 }
 
+std::vector<int> spmv_row_blocks(int n, const int *rowptr) {
+  std::vector<int> b;
+  b.reserve(n / 64 + 2);
+  int r = 0;
+  b.push_back(0);
+  while (r < n) {
+    const int start = r;
+    const int base = rowptr[start];
+    while (r < n && r - start < kTileRows && rowptr[r + 1] - base <= kTileNnz) ++r;
+    if (r == start) ++r;  // a single row longer than the tile: a block of its own
+    b.push_back(r);
+  }
+  return b;
+}
+
+cudaError_t spmv_rowblock_launch(int nblocks, const int *blocks, const int *rowptr, const int *colind,
+                                 const double *vals, const double *x, double *y, cudaStream_t stream,
+                                 const GsState *st, int step) {
+  if (nblocks <= 0) return cudaSuccess;
+  spmv_rowblock_kernel<<<nblocks, kSpmvThreads, 0, stream>>>(blocks, rowptr, colind, vals, x, y, st, step);
+  count_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t spmv_launch(int n, const int *rowptr, const int *colind, const double *vals, const double *x, double *y,
-                        int lanes, cudaStream_t stream, const GsState *st, int step) {
+                        int lanes, cudaStream_t stream) {
   if (n <= 0) return cudaSuccess;
   const int threads = 256;
   const long long rows_per_block = threads / lanes;
   long long blocks = (n + rows_per_block - 1) / rows_per_block;
   if (blocks > (1ll << 20)) blocks = 1ll << 20;
   switch (lanes) {
-#define B200_SPMV_CASE(L)                                                                                 \
-  case L:                                                                                                 \
-    spmv_csr_kernel<L><<<(unsigned)blocks, threads, 0, stream>>>(n, rowptr, colind, vals, x, y, st, step); \
+#define B200_SPMV_CASE(L)                                                                         \
+  case L:                                                                                         \
+    spmv_csr_kernel<L><<<(unsigned)blocks, threads, 0, stream>>>(n, rowptr, colind, vals, x, y); \
     break;
     B200_SPMV_CASE(1)
     B200_SPMV_CASE(2)

@@ -74,6 +74,41 @@ def laplacian_3d_eigs(nx, ny=None, nz=None):
     return (a[0][:, None, None] + a[1][None, :, None] + a[2][None, None, :]).ravel()
 
 
+def laplacian_2d_eigenspace(lam, n, m=None, rtol=1e-10):
+    """Orthonormal basis of the exact eigenspace of laplacian_2d(n, m) for eigenvalue lam
+    (products of sines; entry II = i*n + j with j the fast index)."""
+    m = n if m is None else m
+    a = 2 - 2 * np.cos(np.pi * np.arange(1, n + 1) / (n + 1))
+    b = 2 - 2 * np.cos(np.pi * np.arange(1, m + 1) / (m + 1))
+    idx = np.argwhere(np.abs(a[:, None] + b[None, :] - lam) <= rtol * abs(lam))
+    j = np.arange(n)
+    i = np.arange(m)
+    cols = []
+    for p, q in idx:
+        v = np.outer(np.sin(np.pi * (q + 1) * (i + 1) / (m + 1)), np.sin(np.pi * (p + 1) * (j + 1) / (n + 1))).ravel()
+        cols.append(v / np.linalg.norm(v))
+    return np.stack(cols, axis=1) if cols else np.zeros((n * m, 0))
+
+
+def laplacian_3d_eigenspace(lam, nx, ny=None, nz=None, rtol=1e-10):
+    """Orthonormal basis of the exact eigenspace of laplacian_3d for eigenvalue lam
+    (products of sines; x is the fastest index)."""
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    dims = (nx, ny, nz)
+    ev = [2 - 2 * np.cos(np.pi * np.arange(1, k + 1) / (k + 1)) for k in dims]
+    tot = ev[0][:, None, None] + ev[1][None, :, None] + ev[2][None, None, :]
+    idx = np.argwhere(np.abs(tot - lam) <= rtol * abs(lam))
+    cols = []
+    for a, b, c in idx:
+        sx = np.sin(np.pi * (a + 1) * np.arange(1, nx + 1) / (nx + 1))
+        sy = np.sin(np.pi * (b + 1) * np.arange(1, ny + 1) / (ny + 1))
+        sz = np.sin(np.pi * (c + 1) * np.arange(1, nz + 1) / (nz + 1))
+        v = (sz[:, None, None] * sy[None, :, None] * sx[None, None, :]).ravel()
+        cols.append(v / np.linalg.norm(v))
+    return np.stack(cols, axis=1) if cols else np.zeros((nx * ny * nz, 0))
+
+
 def start_vector(n, seed=0):
     """Seeded N(0,1) start vector (the EPSSetInitialSpace vector shared by the
     GPU path and the oracle)."""

@@ -26,16 +26,23 @@
 // A CGS pass of the reference reads V twice (dot, then update); fusing the
 // update of pass p with the dot of pass p+1 reads V three times per column
 // with one DGKS refinement instead of four, and no host round trip.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "common.h"
 #include "kernels.h"
 
 namespace b200 {
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kConsumerWarps = 8;                     // warps that compute
+constexpr int kConsumers = kConsumerWarps * 32;        // 256 consumer threads
+constexpr int kThreads = kConsumers + 32;              // + one producer warp issuing the bulk copies
 constexpr int kWarps = kThreads / 32;
-constexpr int kStages = 2;
-constexpr size_t kStageBudget = 100 * 1024;  // bytes of one pipeline stage
+constexpr int kMaxStages = 8;
+constexpr int kMaxChunk = 256;                         // rows per chunk (tile box limit)
+constexpr size_t kStageTarget = 64 * 1024;            // bytes of one pipeline stage (target)
+constexpr size_t kStageBudget = 196 * 1024;           // bytes of all stages together
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -70,7 +77,33 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// 2-D tile load through a tensor map: box at (x = first row, y = first column).
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *tmap, int x, int y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// Barrier 1 over the consumer warps only (the producer warp never joins it), with an OR-vote:
+// true on every consumer thread if any passed true.
+__device__ __forceinline__ bool consumer_sync_or(bool v) {
+  uint32_t out;
+  asm volatile(
+      "{\n"
+      " .reg .pred pi, po;\n"
+      " setp.ne.u32 pi, %1, 0;\n"
+      " bar.red.or.pred po, 1, %2, pi;\n"
+      " selp.u32 %0, 1, 0, po;\n"
+      "}\n"
+      : "=r"(out)
+      : "r"((uint32_t)v), "n"(kConsumers)
+      : "memory");
+  return out != 0;
+}
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -87,7 +120,9 @@ struct PassParams {
   double *partials;
   int first;       // first pass of a column: action = DOT, coefficients start from zero
   int plain_dot;   // plain BVDotVec: DOT only, no decision
-  int chunk;       // rows per chunk (multiple of 32)
+  int chunk;       // rows per chunk (power of two, 32..256)
+  int stages;      // pipeline stages (2..kMaxStages)
+  int box_cols;    // columns fetched by the 2-D tile load (jb, or jb+1 when w is column jb)
   int nchunks;
   int G;           // CTAs in the grid
 };
@@ -211,9 +246,16 @@ __device__ void decide(const PassParams &p, const double *cnew_s, DecideShared &
   }
 }
 
-// MAXCPW: largest number of dot columns one warp owns (columns warp, warp+8, ...).
+// MAXCPW: largest number of dot columns one consumer warp owns (columns warp, warp+8, ...).
+//
+// Warp roles: warps 0..7 consume (update, scale, dot), warp 8 produces.  The
+// producer streams row chunks (w and the jb basis columns, one bulk copy per
+// column) into `stages` shared-memory stages; full[s] completes when a
+// stage's bytes have landed, empty[s] when the 8 consumer warps are done with
+// it.  Consumers synchronise among themselves only between the update (which
+// rewrites w) and the dot (which reads the new w).
 template <int MAXCPW>
-__global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p) {
+__global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, const __grid_constant__ CUtensorMap tmap) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   GsState *st = p.st;
   const GsPassArgs &a = p.a;
@@ -222,7 +264,9 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p) {
   if (action == kActNone) return;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int CH = p.chunk;  // power of two, 32..2048
+  const bool producer = (warp == kConsumerWarps);
+  const int CH = p.chunk;
+  const int S = p.stages;
   const int jb = a.jb;
   const bool do_update = (action & kActUpdate) != 0;
   const bool do_dot = (action & kActDot) != 0;
@@ -231,19 +275,25 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p) {
   const double scale = do_scale ? st->scale : 1.0;
 
   // shared memory carve-up
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw);
+  uint64_t *empty = full + kMaxStages;
   double *coef_s = reinterpret_cast<double *>(smem_raw + 128);
   double *cacc = coef_s + kMaxCols;           // [kMaxCols + 1]
   DecideShared *dsh = reinterpret_cast<DecideShared *>(cacc + kMaxCols + 1);
-  __shared__ int is_last;
-  __shared__ double upd[kThreads];            // partial row sums of the update (several threads per row)
+  __shared__ int is_last, timed_out, n_issued;
+  __shared__ double wbuf[2 * kMaxChunk];      // updated w, double-buffered by chunk parity
   const size_t head = 128 + sizeof(double) * (2 * kMaxCols + 1) + ((sizeof(DecideShared) + 127) / 128) * 128;
   double *stage_base = reinterpret_cast<double *>(smem_raw + ((head + 127) / 128) * 128);
   const size_t stage_elems = (size_t)CH * (jb + 1);
 
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kConsumerWarps);
+    }
     fence_mbar_init();
+    timed_out = 0;
+    n_issued = 0;
   }
   for (int i = tid; i < jb; i += kThreads) coef_s[i] = do_update ? p.coef[i] : 0.0;
   __syncthreads();
@@ -251,116 +301,112 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p) {
   const int G = p.G;
   const int nmine = (p.nchunks > (int)blockIdx.x) ? (p.nchunks - 1 - (int)blockIdx.x) / G + 1 : 0;
   double *Vw = a.V + (size_t)a.wcol * a.ld;
-
-  // warp 0 issues a chunk: lane 0 arms the barrier, the 32 lanes issue the column copies in parallel
-  auto issue = [&](int i, int s) {
-    const long long r0 = ((long long)blockIdx.x + (long long)i * G) * CH;
-    const int rows = (int)min((long long)CH, (long long)a.n - r0);
-    const uint32_t bytes = (uint32_t)(((rows * 8) + 15) & ~15);
-    double *buf = stage_base + (size_t)s * stage_elems;
-    if (lane == 0) mbar_arrive_expect_tx(&bars[s], bytes * (uint32_t)(ncl + 1));
-    __syncwarp();
-    for (int c = lane - 1; c < ncl; c += 32) {
-      if (c < 0) bulk_load(buf, Vw + r0, bytes, &bars[s]);
-      else bulk_load(buf + (size_t)(c + 1) * CH, a.V + (size_t)c * a.ld + r0, bytes, &bars[s]);
-    }
-  };
-
-  if (warp == 0) {
-    for (int s = 0; s < kStages && s < nmine; ++s) issue(s, s);
-  }
+  int consumed = 0;
 
   // dot accumulators: lane-private partial sums of the columns this warp owns, across all chunks
   double acc[MAXCPW];
 #pragma unroll
   for (int t = 0; t < MAXCPW; ++t) acc[t] = 0.0;
 
-  // update mapping: TPR threads per row when a chunk has fewer rows than threads
-  const int TPR = (CH >= kThreads) ? 1 : kThreads / CH;
-  const int part = (TPR > 1) ? tid / CH : 0;
-  const int rbase = (TPR > 1) ? tid % CH : tid;
-  const int rstride = (TPR > 1) ? CH : kThreads;
-
-  bool timed_out = false;
-  for (int i = 0; i < nmine; ++i) {
-    const int s = i % kStages;
-    const uint32_t parity = (uint32_t)((i / kStages) & 1);
-    // every thread waits (bounded); the block then agrees on one outcome
-    const bool ok = mbar_wait_bounded(&bars[s], parity);
-    if (__syncthreads_or(!ok)) {
-      timed_out = true;
-      break;
+  if (producer) {
+    for (int i = 0; i < nmine; ++i) {
+      const int s = i % S;
+      if (i >= S) {
+        const bool ok = mbar_wait_bounded(&empty[s], (uint32_t)(((i / S) - 1) & 1));
+        if (!__all_sync(0xffffffffu, ok)) {
+          if (lane == 0) timed_out = 1;
+          break;
+        }
+      }
+      const long long r0 = ((long long)blockIdx.x + (long long)i * G) * CH;
+      const int rows = (int)min((long long)CH, (long long)a.n - r0);
+      double *buf = stage_base + (size_t)s * stage_elems;
+      if (lane == 0) {
+        // one tile load brings the basis columns (and w when it is column jb); rows past n read as zeros
+        const bool tile = ncl > 0;
+        const bool w_in_tile = tile && p.box_cols == jb + 1;
+        const uint32_t wbytes = w_in_tile ? 0u : (uint32_t)(((rows * 8) + 15) & ~15);
+        const uint32_t tbytes = tile ? (uint32_t)CH * 8u * (uint32_t)p.box_cols : 0u;
+        mbar_arrive_expect_tx(&full[s], tbytes + wbytes);
+        if (tile) tma_load_2d(buf, &tmap, (int)r0, 0, &full[s]);
+        if (!w_in_tile) bulk_load(buf + (size_t)jb * CH, Vw + r0, wbytes, &full[s]);
+        n_issued = i + 1;
+      }
+      __syncwarp();
     }
-    const long long r0 = ((long long)blockIdx.x + (long long)i * G) * CH;
-    const int rows = (int)min((long long)CH, (long long)a.n - r0);
-    double *ws = stage_base + (size_t)s * stage_elems;
-    const double *Vs = ws + CH;  // column c at Vs + c*CH
-
-    if (do_update || do_scale) {
-      for (int r = rbase; r < CH; r += rstride) {
-        double sum = 0.0;
-        if (do_update && r < rows) {
-          double a0 = 0.0, a1 = 0.0;
-          int c = part;
-          for (; c + TPR < jb; c += 2 * TPR) {
-            a0 = fma(Vs[(size_t)c * CH + r], coef_s[c], a0);
-            a1 = fma(Vs[(size_t)(c + TPR) * CH + r], coef_s[c + TPR], a1);
+  } else {
+    for (int i = 0; i < nmine; ++i) {
+      const int s = i % S;
+      const bool ok = mbar_wait_bounded(&full[s], (uint32_t)((i / S) & 1));
+      const long long r0 = ((long long)blockIdx.x + (long long)i * G) * CH;
+      const int rows = (int)min((long long)CH, (long long)a.n - r0);
+      const double *Vs = stage_base + (size_t)s * stage_elems;  // column c at Vs + c*CH, w after the basis
+      const double *wsrc = Vs + (size_t)jb * CH;
+      double *wnew = wbuf + (i & 1) * kMaxChunk;  // updated w of this chunk (never a bulk-copy target)
+      if (do_update || do_scale) {
+        // one thread per row, four independent partial sums
+        if (ok) {
+          for (int r = tid; r < rows; r += kConsumers) {
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            if (do_update) {
+              int c = 0;
+              for (; c + 3 < jb; c += 4) {
+                s0 = fma(Vs[(size_t)c * CH + r], coef_s[c], s0);
+                s1 = fma(Vs[(size_t)(c + 1) * CH + r], coef_s[c + 1], s1);
+                s2 = fma(Vs[(size_t)(c + 2) * CH + r], coef_s[c + 2], s2);
+                s3 = fma(Vs[(size_t)(c + 3) * CH + r], coef_s[c + 3], s3);
+              }
+              for (; c < jb; ++c) s0 = fma(Vs[(size_t)c * CH + r], coef_s[c], s0);
+            }
+            double wv = wsrc[r] - ((s0 + s1) + (s2 + s3));
+            if (do_scale) wv *= scale;
+            wnew[r] = wv;
+            Vw[r0 + r] = wv;
           }
-          if (c < jb) a0 = fma(Vs[(size_t)c * CH + r], coef_s[c], a0);
-          sum = a0 + a1;
         }
-        if (TPR > 1) {
-          upd[tid] = sum;
-        } else if (r < rows) {
-          double wv = ws[r] - sum;
-          if (do_scale) wv *= scale;
-          ws[r] = wv;
-          Vw[r0 + r] = wv;
+        // the dot reads the whole updated chunk; the barrier also agrees on a timed-out wait
+        if (do_dot) {
+          if (consumer_sync_or(!ok)) break;
+        } else if (!ok) {
+          break;
         }
+      } else if (!ok) {
+        break;
       }
-      if (TPR > 1) {
-        __syncthreads();
-        if (part == 0 && rbase < rows) {
-          double tot = 0.0;
-          for (int q = 0; q < TPR; ++q) tot += upd[q * CH + rbase];
-          double wv = ws[rbase] - tot;
-          if (do_scale) wv *= scale;
-          ws[rbase] = wv;
-          Vw[r0 + rbase] = wv;
-        }
-      }
-      __syncthreads();
-    }
-    if (do_dot) {
-      for (int r = lane; r < rows; r += 32) {
-        const double wr = ws[r];
+      if (do_dot) {
+        const double *wd = (do_update || do_scale) ? wnew : wsrc;
+        for (int r = lane; r < rows; r += 32) {
+          const double wr = wd[r];
 #pragma unroll
-        for (int t = 0; t < MAXCPW; ++t) {
-          const int c = warp + kWarps * t;
-          if (c < jb) acc[t] = fma(Vs[(size_t)c * CH + r], wr, acc[t]);
-          else if (c == jb) acc[t] = fma(wr, wr, acc[t]);
+          for (int t = 0; t < MAXCPW; ++t) {
+            const int c = warp + kConsumerWarps * t;
+            if (c < jb) acc[t] = fma(Vs[(size_t)c * CH + r], wr, acc[t]);
+            else if (c == jb) acc[t] = fma(wr, wr, acc[t]);
+          }
         }
       }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);  // stage only read here: the next bulk copy may overwrite it
+      consumed = i + 1;
     }
-    fence_proxy_async();  // generic-proxy smem accesses ordered before the next bulk copy into this stage
-    __syncthreads();
-    if (warp == 0 && i + kStages < nmine) issue(i + kStages, s);
+    if (lane == 0 && consumed < nmine) timed_out = 1;
   }
+  __syncthreads();
   if (timed_out) {
-    // Drain copies still in flight on either stage (bounded), report, and leave.
+    // Drain the copies still in flight (bounded), report, and leave.
     if (tid == 0) {
       atomicOr(&st->err, (int)kDevErrTimeout);
-      for (int s = 0; s < kStages; ++s) (void)mbar_wait_bounded(&bars[s], 0), (void)mbar_wait_bounded(&bars[s], 1);
+      for (int i = consumed; i < n_issued; ++i) (void)mbar_wait_bounded(&full[i % S], (uint32_t)((i / S) & 1));
     }
     __syncthreads();
     return;
   }
 
   // per-CTA column sums -> partials[c * G + cta]
-  if (do_dot) {
+  if (do_dot && !producer) {
 #pragma unroll
     for (int t = 0; t < MAXCPW; ++t) {
-      const int c = warp + kWarps * t;
+      const int c = warp + kConsumerWarps * t;
       const double v = warp_sum(acc[t]);
       if (lane == 0 && c <= jb) p.partials[(size_t)c * G + blockIdx.x] = v;
     }
@@ -402,20 +448,56 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p) {
   decide(p, cnew_s, *dsh);
 }
 
-size_t pass_smem_bytes(int jb, int CH) {
+size_t pass_smem_bytes(int jb, int CH, int stages) {
   const size_t head = 128 + sizeof(double) * (2 * kMaxCols + 1) + ((sizeof(DecideShared) + 127) / 128) * 128;
-  return ((head + 127) / 128) * 128 + (size_t)kStages * CH * (jb + 1) * sizeof(double);
+  return ((head + 127) / 128) * 128 + (size_t)stages * CH * (jb + 1) * sizeof(double);
 }
 
+// Rows per chunk: the largest power of two (32..256, the tile box limit) whose stage fits the target size.
 int pass_chunk_rows(int jb) {
-  const size_t budget = kStageBudget / ((size_t)(jb + 1) * sizeof(double));
+  const size_t rows = kStageTarget / ((size_t)(jb + 1) * sizeof(double));
   int ch = 32;
-  while (ch < 2048 && (size_t)(2 * ch) <= budget) ch *= 2;
+  while (ch < kMaxChunk && (size_t)(2 * ch) <= rows) ch *= 2;
   return ch;
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void *ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+  }
+  return fn;
+}
+
+// Tensor map over the basis: dim 0 = rows (n, contiguous), dim 1 = columns (stride ld), box CH x box_cols.
+cudaError_t make_tmap(CUtensorMap *tm, const GsPassArgs &a, int CH, int box_cols, int total_cols) {
+  memset(tm, 0, sizeof(*tm));
+  if (box_cols <= 0) return cudaSuccess;  // no tile load in this pass
+  PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+  if (!enc) return cudaErrorNotSupported;
+  const cuuint64_t dims[2] = {(cuuint64_t)a.n, (cuuint64_t)total_cols};
+  const cuuint64_t strides[1] = {(cuuint64_t)a.ld * sizeof(double)};
+  const cuuint32_t box[2] = {(cuuint32_t)CH, (cuuint32_t)box_cols};
+  const cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void *)a.V, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+int pass_stages(int jb, int CH) {
+  const size_t stage = (size_t)CH * (jb + 1) * sizeof(double);
+  size_t s = kStageBudget / stage;
+  if (s > (size_t)kMaxStages) s = kMaxStages;
+  return (int)s;
+}
+
 template <int M>
-cudaError_t launch_pass_t(const PassParams &p, size_t smem, cudaStream_t stream) {
+cudaError_t launch_pass_t(const PassParams &p, const CUtensorMap &tm, size_t smem, cudaStream_t stream) {
   static bool attr_set[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -424,7 +506,7 @@ cudaError_t launch_pass_t(const PassParams &p, size_t smem, cudaStream_t stream)
     if (e != cudaSuccess) return e;
     attr_set[dev] = true;
   }
-  gs_pass_kernel<M><<<p.G, kThreads, smem, stream>>>(p);
+  gs_pass_kernel<M><<<p.G, kThreads, smem, stream>>>(p, tm);
   return cudaGetLastError();
 }
 
@@ -438,22 +520,28 @@ cudaError_t launch_pass(const GsPassArgs &a, const GsWork &w, int first, int pla
   p.first = first;
   p.plain_dot = plain_dot;
   p.chunk = pass_chunk_rows(a.jb);
+  p.stages = pass_stages(a.jb, p.chunk);
+  if (p.stages < 2) return cudaErrorInvalidValue;
   p.nchunks = (a.n + p.chunk - 1) / p.chunk;
   int G = w.num_sms;
   if (G > w.max_ctas) G = w.max_ctas;
   if (G > p.nchunks) G = p.nchunks;
   if (G < 1) G = 1;
   p.G = G;
-  const size_t smem = pass_smem_bytes(a.jb, p.chunk);
+  const size_t smem = pass_smem_bytes(a.jb, p.chunk, p.stages);
   if (smem + 4096 > max_dynamic_smem()) return cudaErrorInvalidValue;
-  const int cpw = (a.jb + 1 + kWarps - 1) / kWarps;  // dot columns per warp (basis + self)
-  cudaError_t e;
-  if (cpw <= 2) e = launch_pass_t<2>(p, smem, stream);
-  else if (cpw <= 4) e = launch_pass_t<4>(p, smem, stream);
-  else if (cpw <= 8) e = launch_pass_t<8>(p, smem, stream);
-  else if (cpw <= 12) e = launch_pass_t<12>(p, smem, stream);
-  else if (cpw <= 16) e = launch_pass_t<16>(p, smem, stream);
-  else if (cpw <= 32) e = launch_pass_t<32>(p, smem, stream);
+  // w is column jb in the column variant: one box covers basis and w
+  p.box_cols = (a.wcol == a.jb) ? a.jb + 1 : a.jb;
+  CUtensorMap tm;
+  cudaError_t e = make_tmap(&tm, a, p.chunk, p.box_cols, a.total_cols);
+  if (e != cudaSuccess) return e;
+  const int cpw = (a.jb + 1 + kConsumerWarps - 1) / kConsumerWarps;  // dot columns per consumer warp (basis + self)
+  if (cpw <= 2) e = launch_pass_t<2>(p, tm, smem, stream);
+  else if (cpw <= 4) e = launch_pass_t<4>(p, tm, smem, stream);
+  else if (cpw <= 8) e = launch_pass_t<8>(p, tm, smem, stream);
+  else if (cpw <= 12) e = launch_pass_t<12>(p, tm, smem, stream);
+  else if (cpw <= 16) e = launch_pass_t<16>(p, tm, smem, stream);
+  else if (cpw <= 32) e = launch_pass_t<32>(p, tm, smem, stream);
   else return cudaErrorInvalidValue;
   count_launch();
   return e;

@@ -68,6 +68,7 @@ struct GsPassArgs {
   int step;       // Lanczos step index (halt gating), or -1
   int normalize;  // scale by 1/norm at the end
   int column;     // 1: column variant (BV_SafeSqrt check on w^T w)
+  int total_cols; // columns allocated from V (bounds of the tile loads)
 };
 
 // Enqueue the full CGS + DGKS("if needed") orthogonalisation of one column:

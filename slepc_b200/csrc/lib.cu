@@ -377,6 +377,7 @@ static b200_status bv_orth_column(b200_bv bv, int j, int normalize, double *H, d
   GsPassArgs a{};
   a.V = bv->V;
   a.ld = bv->ld;
+  a.total_cols = bv->m + 1;
   a.n = bv->n;
   a.jb = j;
   a.wcol = j;
@@ -417,6 +418,7 @@ extern "C" b200_status b200_bv_orthogonalize_vec(b200_bv bv, double *v, double *
   GsPassArgs a{};
   a.V = bv->V;
   a.ld = bv->ld;
+  a.total_cols = bv->m + 1;
   a.n = bv->n;
   a.jb = k;
   a.wcol = bv->m;
@@ -546,6 +548,7 @@ extern "C" b200_status b200_bv_dot_vec(b200_bv X, const double *y, double *q) {
   GsPassArgs a{};
   a.V = col(X, X->l);
   a.ld = X->ld;
+  a.total_cols = X->m + 1 - X->l;
   a.n = X->n;
   a.jb = k;
   a.wcol = X->m - X->l;
@@ -636,6 +639,7 @@ static b200_status bv_lanczos(b200_bv bv, b200_mat A, int k, int *m, double *alp
     GsPassArgs a{};
     a.V = bv->V;
     a.ld = bv->ld;
+    a.total_cols = bv->m + 1;
     a.n = bv->n;
     a.jb = j + 1;
     a.wcol = j + 1;

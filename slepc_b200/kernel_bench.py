@@ -1,0 +1,141 @@
+"""Single-kernel timing at the 3-D 128^3 Laplacian size (n = 2,097,152) through the C ABI.
+
+Used to produce the kernel profiles (run it under ncu with -k/-s/-c) and to
+time one kernel family in isolation with CUDA events:
+
+  python slepc_b200/kernel_bench.py gs --j 20 60    # one column orthogonalisation against j columns
+  python slepc_b200/kernel_bench.py spmv             # CSR SpMV of the 7-point Laplacian
+  python slepc_b200/kernel_bench.py multinplace      # restart GEMM V(:,0:56) = V(:,0:80) Q
+
+Prints one JSON line per kernel family: average ms per call and algorithmic GB/s.
+"""
+import argparse
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+import slepc_b200 as S  # noqa: E402
+from slepc_b200 import problems as P  # noqa: E402
+
+
+def gs(args, torch):
+    n, j = args.n, args.j
+    bv = S.BV().create(n, args.m)
+    rng = np.random.default_rng(0)
+    # an orthonormal basis of j columns built by the library itself, then a vector with large components on it
+    for c in range(j):
+        bv.setColumn(c, rng.standard_normal(n))
+        bv.orthonormalizeColumn(c)
+    # components along the basis much larger than the rest, as for A*v_j in Lanczos: the first CGS pass
+    # leaves |w'| < eta*|w| and the DGKS refinement runs (three streamed passes)
+    coeff = 1.0e3 * rng.standard_normal(j)
+    base = torch.from_numpy(rng.standard_normal(n)).cuda()
+    _, _, ld = bv.getSizes()
+    w = base.clone()
+    for c in range(0, j, 16):  # w = base + V(:,0:j) coeff, built with BVMultVec on device
+        bv.setActiveColumns(c, min(j, c + 16))
+        bv.multVec(1.0, 1.0, w.data_ptr(), coeff[c:min(j, c + 16)])
+    bv.setActiveColumns(0, args.m)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lib = S.lib()
+    for _ in range(args.warmup):
+        lib.b200_bv_insert_vec(bv.handle, j, w.data_ptr())
+        bv.orthonormalizeColumn(j)
+    ms = 0.0
+    for _ in range(args.reps):
+        lib.b200_bv_insert_vec(bv.handle, j, w.data_ptr())
+        torch.cuda.synchronize()
+        e0.record()
+        nrm, _ = bv.orthonormalizeColumn(j)
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+    ms /= args.reps
+    # three streamed passes (dot; update+dot; update+scale) of j basis columns plus w, and two writes of w
+    algo = 8 * n * (3 * (j + 1) + 2)
+    return {"kernel": "gs_pass_kernel x3 (one column, DGKS refined)", "n": n, "j": j, "ms": ms,
+            "algorithmic_bytes": algo, "GBps": algo / (ms * 1e-3) / 1e9, "norm": nrm, "ld": ld}
+
+
+def spmv(args, torch):
+    csr = P.laplacian_3d(args.grid)
+    n = len(csr[0]) - 1
+    nnz = int(csr[0][-1])
+    A = S.Mat().createAIJ(csr)
+    x = torch.from_numpy(P.start_vector(n, 0)).cuda()
+    y = torch.empty(n, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")
+    for _ in range(args.warmup):
+        A.mult(x.data_ptr(), y.data_ptr())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = 0.0
+    for _ in range(args.reps):
+        flush.fill_(1.0)  # evict x and the CSR arrays from L2 between calls
+        e0.record()
+        A.mult(x.data_ptr(), y.data_ptr())
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+    ms /= args.reps
+    algo = nnz * 12 + (n + 1) * 4 + 2 * n * 8
+    return {"kernel": "spmv_rowblock_kernel", "n": n, "nnz": nnz, "ms": ms, "algorithmic_bytes": algo,
+            "GBps": algo / (ms * 1e-3) / 1e9}
+
+
+def multinplace(args, torch):
+    n, k, e = args.n, 80, 56
+    bv = S.BV().create(n, 81)
+    rng = np.random.default_rng(1)
+    for c in range(k):
+        bv.setColumn(c, rng.standard_normal(n))
+    Q = np.asfortranarray(rng.standard_normal((81, 81)))
+    bv.setActiveColumns(0, k)
+    for _ in range(args.warmup):
+        bv.multInPlace(Q, 0, e)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = 0.0
+    for _ in range(args.reps):
+        torch.cuda.synchronize()
+        e0.record()
+        bv.multInPlace(Q, 0, e)
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+    ms /= args.reps
+    algo = 8 * n * (k + e) + 8 * k * e
+    flops = 2.0 * n * k * e
+    return {"kernel": "multinplace_kernel", "n": n, "k": k, "e-s": e, "ms": ms, "algorithmic_bytes": algo,
+            "GBps": algo / (ms * 1e-3) / 1e9, "TFLOPs": flops / (ms * 1e-3) / 1e12}
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("kernel", choices=["gs", "spmv", "multinplace", "all"])
+    p.add_argument("--n", type=int, default=128 ** 3)
+    p.add_argument("--grid", type=int, default=128)
+    p.add_argument("--j", type=int, nargs="+", default=[60])
+    p.add_argument("--m", type=int, default=82)
+    p.add_argument("--reps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=2)
+    args = p.parse_args()
+    import torch
+
+    todo = ["gs", "spmv", "multinplace"] if args.kernel == "all" else [args.kernel]
+    js = list(args.j)
+    for k in todo:
+        if k == "gs":
+            for j in js:
+                args.j = j
+                print(json.dumps(gs(args, torch)), flush=True)
+        else:
+            print(json.dumps({"spmv": spmv, "multinplace": multinplace}[k](args, torch)), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -68,7 +68,7 @@ def _distinct(vals, rtol=1e-9):
     return np.array([lam for lam, _ in H.clusters(np.sort(vals)[::-1], rtol)])
 
 
-def check_parity(csr, g, o, oracle_mod, tol, exact_vals, exact_space, key):
+def check_parity(csr, g, o, oracle_mod, tol, exact_vals, exact_space, key, nev, compare_sets=True):
     """GPU result g vs oracle result o.  exact_space(lam) returns an orthonormal basis of the
     exact eigenspace; key(lam) is larger for the eigenvalues wanted first."""
     As = P.to_scipy(csr)
@@ -76,11 +76,14 @@ def check_parity(csr, g, o, oracle_mod, tol, exact_vals, exact_space, key):
     # (1) every computed value lies on the exact spectrum
     assert H.eig_set_match(g["evals"], exact_vals, 0) < 1e-10
     assert H.eig_set_match(o.evals, exact_vals, 0) < 1e-10
-    # (2) the distinct values agree inside the window both runs cover
-    thr = max(key(g["evals"]).min(), key(o.evals).min())
-    dg = _distinct(g["evals"][key(g["evals"]) >= thr])
-    do = _distinct(o.evals[key(o.evals) >= thr])
-    assert H.eig_set_match(dg, do, 0) < 1e-10 and H.eig_set_match(do, dg, 0) < 1e-10, (dg, do)
+    # (2) the distinct values of the requested pairs agree inside the window both runs cover
+    if compare_sets:
+        gv, ov = g["evals"][:nev], o.evals[:nev]
+        thr = max(key(gv).min(), key(ov).min())
+        thr -= 1e-9 * abs(thr)  # the two runs compute the cut-off eigenvalue to rounding, not bit for bit
+        dg = _distinct(gv[key(gv) >= thr])
+        do = _distinct(ov[key(ov) >= thr])
+        assert H.eig_set_match(dg, do, 0) < 1e-10 and H.eig_set_match(do, dg, 0) < 1e-10, (dg, do)
     # (3) residuals in FP64 on the host, and the device's EPSComputeError agrees
     res = np.array([oracle_mod.residual(As, g["X"][:, i], g["evals"][i]) for i in range(g["nconv"])])
     assert res.max() <= tol, res.max()
@@ -131,7 +134,7 @@ def test_ex2_golden_gpu(oracle_mod):
     assert got in [o["values"] for o in gold["outputs"].values()]
     o = oracle_mod.eps_solve(P.to_scipy(csr), v0, nev=4, ncv=20, which=oracle_mod.LARGEST_MAGNITUDE)
     rep = check_parity(csr, g, o, oracle_mod, 1e-8, P.laplacian_2d_eigs(72),
-                       lambda lam: P.laplacian_2d_eigenspace(lam, 72), LM)
+                       lambda lam: P.laplacian_2d_eigenspace(lam, 72), LM, 4)
     _report("ex2_72", **rep)
     assert abs(g["its"] - o.its) <= 2
 
@@ -145,7 +148,7 @@ def test_config1_2d_laplacian_100(oracle_mod):
     o = oracle_mod.eps_solve(P.to_scipy(csr), v0, nev=10, ncv=32, which=oracle_mod.LARGEST_MAGNITUDE)
     assert g["nconv"] >= 10
     rep = check_parity(csr, g, o, oracle_mod, 1e-8, P.laplacian_2d_eigs(100),
-                       lambda lam: P.laplacian_2d_eigenspace(lam, 100), LM)
+                       lambda lam: P.laplacian_2d_eigenspace(lam, 100), LM, 10)
     _report("config1_2d_100", **rep)
 
 
@@ -159,7 +162,7 @@ def test_3d_laplacian_nev32_ncv80(oracle_mod, N, seed):
     o = oracle_mod.eps_solve(P.to_scipy(csr), v0, nev=32, ncv=80, which=oracle_mod.LARGEST_REAL)
     assert g["nconv"] >= 32
     rep = check_parity(csr, g, o, oracle_mod, 1e-8, P.laplacian_3d_eigs(N),
-                       lambda lam: P.laplacian_3d_eigenspace(lam, N), LR)
+                       lambda lam: P.laplacian_3d_eigenspace(lam, N), LR, 32)
     _report(f"3d_{N}", **rep)
 
 
@@ -185,7 +188,9 @@ def test_random_sparse_vs_dense_eigh(oracle_mod):
         top = ev[np.argsort(order(ev), kind="stable")][:6]
         np.testing.assert_allclose(g["evals"][:6], top, rtol=1e-10)
         o = oracle_mod.eps_solve(A, v0, nev=6, ncv=30, which=which)
-        rep = check_parity(csr, g, o, oracle_mod, 1e-8, ev, space, key)
+        # the GPU's six pairs equal dense LAPACK's (checked above); the oracle may lock a smaller
+        # eigenvalue of this clustered spectrum first, so its set is not compared
+        rep = check_parity(csr, g, o, oracle_mod, 1e-8, ev, space, key, 6, compare_sets=False)
         _report(f"random_sparse_which{which}", **rep)
 
 

@@ -118,6 +118,24 @@ b200_status b200_bv_orthogonalize_column(b200_bv bv, int j, double *H_host, doub
 b200_status b200_bv_orthonormalize_column(b200_bv bv, int j, double *norm, int *lindep);
 /* BVOrthogonalizeVec (bvorthog.c:238-262): a device vector against the k active columns. */
 b200_status b200_bv_orthogonalize_vec(b200_bv bv, double *v_dev, double *H_host, double *norm, int *lindep);
+/* Allocation-free variant of b200_bv_orthogonalize_column; it has no
+ * counterpart in SLEPc.  For callers that cannot call cudaMalloc -- for
+ * example a host whose device memory is all owned by its own pool
+ * allocator, or a plugin that must not grow the process's device footprint
+ * after start-up.  V_dev is a caller-owned column-major basis (n rows,
+ * leading dimension ld, even and >= n, ncols columns, 16-byte aligned);
+ * column j is orthogonalised in place against columns 0..j-1 with the same
+ * CGS + DGKS passes.  H_dev (device, j+1 doubles) receives the coefficients
+ * and then the norm; norm and lindep (host, nullable) are read back, so the
+ * call synchronises the stream.  All working memory comes from one fixed
+ * array of about 330 KB compiled into the library, which every GPU that
+ * loads the library holds until the process exits; j at most 253, otherwise
+ * B200_ERR_ARG.  The first call on a device looks the array's address up
+ * and should come before any stream capture on that device.  Calls share
+ * the array: calls whose work overlaps on the GPU race and must be
+ * serialised by the caller. */
+b200_status b200_orthogonalize_column_noalloc(int n, int ld, int ncols, double *V_dev, int j, double *H_dev,
+                                              double *norm, int *lindep, void *stream);
 /* BVOrthogonalize with BV_ORTHOG_BLOCK_GS (bvorthog.c:505-560, :726-767):
  * columns l..k-1 one by one; R_host (nullable, ldr >= k) receives R. */
 b200_status b200_bv_orthogonalize(b200_bv bv, double *R_host, int ldr);

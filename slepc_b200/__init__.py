@@ -72,6 +72,8 @@ _SIGS = {
     "b200_bv_orthonormalize_column": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _ip]),
     "b200_bv_orthogonalize_vec": (ctypes.c_int, [_vp, _vp, _dp, _dp, _ip]),
     "b200_bv_orthogonalize": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
+    "b200_orthogonalize_column_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
+                                                         ctypes.c_int, _vp, _dp, _ip, _vp]),
     "b200_bv_mult_inplace": (ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "b200_bv_mult_inplace_device": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "b200_bv_mult": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _vp, _dp, ctypes.c_int]),
@@ -441,6 +443,15 @@ class EPS:
             self.destroy()
         except Exception:
             pass
+
+
+def orthogonalize_column_noalloc(n, ld, ncols, V_ptr, j, H_ptr, stream=None):
+    """Allocation-free column orthogonalisation on caller-owned device memory
+    (b200_orthogonalize_column_noalloc): returns (norm, lindep)."""
+    nrm, lnd = ctypes.c_double(), ctypes.c_int()
+    _check(lib().b200_orthogonalize_column_noalloc(n, ld, ncols, V_ptr, j, H_ptr, ctypes.byref(nrm),
+                                                   ctypes.byref(lnd), stream))
+    return nrm.value, bool(lnd.value)
 
 
 def solve_csr_host(csr, v0, nev, ncv, tol=1e-8, which=LARGEST_MAGNITUDE, mpd=0, max_it=0, want_vectors=True,

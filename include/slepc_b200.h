@@ -78,6 +78,13 @@ b200_status b200_mat_create_csr_device(int n, int64_t nnz, const int *rowptr_dev
 /* y = A x on device vectors (MatMult). */
 b200_status b200_mat_mult(b200_mat A, const double *x_dev, double *y_dev);
 b200_status b200_mat_get_size(b200_mat A, int *n, int64_t *nnz);
+/* CSR SpMV schedule of a matrix (a MatSetOption-style knob):
+ *   B200_SPMV_WARPTILE (default) -- warp tiles of <= 32 rows / <= 256 nonzeros;
+ *   B200_SPMV_ROWBLOCK           -- CTA row blocks of <= 1024 rows / <= 4096 nonzeros.
+ * Both sum each row in index order (rows within a tile give the bits of a sequential loop). */
+#define B200_SPMV_ROWBLOCK 0
+#define B200_SPMV_WARPTILE 1
+b200_status b200_mat_set_spmv_schedule(b200_mat A, int schedule);
 /* Lanes per row chosen for the SpMV (1..32), for tests and reports. */
 b200_status b200_mat_get_lanes(b200_mat A, int *lanes);
 b200_status b200_mat_destroy(b200_mat A);

@@ -55,6 +55,7 @@ _SIGS = {
     "b200_mat_mult": (ctypes.c_int, [_vp, _vp, _vp]),
     "b200_mat_get_size": (ctypes.c_int, [_vp, _ip, ctypes.POINTER(ctypes.c_int64)]),
     "b200_mat_get_lanes": (ctypes.c_int, [_vp, _ip]),
+    "b200_mat_set_spmv_schedule": (ctypes.c_int, [_vp, ctypes.c_int]),
     "b200_mat_destroy": (ctypes.c_int, [_vp]),
     "b200_csr_spmv": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
     "b200_bv_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp]),
@@ -175,6 +176,11 @@ class Mat:
 
     def mult(self, x_ptr, y_ptr):
         _check(lib().b200_mat_mult(self.handle, x_ptr, y_ptr))
+
+    ROWBLOCK, WARPTILE = 0, 1
+
+    def setSpMVSchedule(self, schedule):
+        _check(lib().b200_mat_set_spmv_schedule(self.handle, schedule))
 
     def getLanes(self):
         v = ctypes.c_int()

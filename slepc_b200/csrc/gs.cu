@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
   double *cacc = coef_s + kMaxCols;           // [kMaxCols + 1]
   DecideShared *dsh = reinterpret_cast<DecideShared *>(cacc + kMaxCols + 1);
   __shared__ int is_last, timed_out, n_issued;
-  __shared__ double wbuf[2 * kMaxChunk];      // updated w, double-buffered by chunk parity
+  __shared__ double upd[2 * kConsumers];      // partial update sums (TPR*CH = 256 per chunk), by chunk parity
   const size_t head = 128 + sizeof(double) * (2 * kMaxCols + 1) + ((sizeof(DecideShared) + 127) / 128) * 128;
   double *stage_base = reinterpret_cast<double *>(smem_raw + ((head + 127) / 128) * 128);
   const size_t stage_elems = (size_t)CH * (jb + 1);
@@ -335,6 +335,15 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
       __syncwarp();
     }
   } else {
+    // Update mapping: the chunk's rows form CH/32 groups of 32; the 8 consumer warps split into
+    // TPR = 8/(CH/32) parts, warp w taking row group w % (CH/32) and columns part, part+TPR, ...
+    // (one column, 32 consecutive rows per instruction: no bank conflicts).  Partial sums meet
+    // in upd[part][row] behind the chunk's barrier; each warp then folds them into w' while it
+    // runs the dot, and warp g writes row group g of w' back to global memory.
+    const int groups = CH / 32;  // 1..8
+    const int TPR = kConsumerWarps / groups;
+    const int part = warp / groups;
+    const int urow = (warp % groups) * 32 + lane;
     for (int i = 0; i < nmine; ++i) {
       const int s = i % S;
       const bool ok = mbar_wait_bounded(&full[s], (uint32_t)((i / S) & 1));
@@ -342,41 +351,41 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
       const int rows = (int)min((long long)CH, (long long)a.n - r0);
       const double *Vs = stage_base + (size_t)s * stage_elems;  // column c at Vs + c*CH, w after the basis
       const double *wsrc = Vs + (size_t)jb * CH;
-      double *wnew = wbuf + (i & 1) * kMaxChunk;  // updated w of this chunk (never a bulk-copy target)
-      if (do_update || do_scale) {
-        // one thread per row, four independent partial sums
-        if (ok) {
-          for (int r = tid; r < rows; r += kConsumers) {
-            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-            if (do_update) {
-              int c = 0;
-              for (; c + 3 < jb; c += 4) {
-                s0 = fma(Vs[(size_t)c * CH + r], coef_s[c], s0);
-                s1 = fma(Vs[(size_t)(c + 1) * CH + r], coef_s[c + 1], s1);
-                s2 = fma(Vs[(size_t)(c + 2) * CH + r], coef_s[c + 2], s2);
-                s3 = fma(Vs[(size_t)(c + 3) * CH + r], coef_s[c + 3], s3);
-              }
-              for (; c < jb; ++c) s0 = fma(Vs[(size_t)c * CH + r], coef_s[c], s0);
-            }
-            double wv = wsrc[r] - ((s0 + s1) + (s2 + s3));
-            if (do_scale) wv *= scale;
-            wnew[r] = wv;
-            Vw[r0 + r] = wv;
+      double *up = upd + (i & 1) * kConsumers;  // partial update sums of this chunk
+      const bool rewrite = do_update || do_scale;
+      if (rewrite) {
+        if (ok && do_update) {
+          double s0 = 0.0, s1 = 0.0;
+          int c = part;
+          for (; c + TPR < jb; c += 2 * TPR) {
+            s0 = fma(Vs[(size_t)c * CH + urow], coef_s[c], s0);
+            s1 = fma(Vs[(size_t)(c + TPR) * CH + urow], coef_s[c + TPR], s1);
           }
+          if (c < jb) s0 = fma(Vs[(size_t)c * CH + urow], coef_s[c], s0);
+          up[part * CH + urow] = s0 + s1;
         }
-        // the dot reads the whole updated chunk; the barrier also agrees on a timed-out wait
-        if (do_dot) {
-          if (consumer_sync_or(!ok)) break;
-        } else if (!ok) {
-          break;
-        }
+        if (consumer_sync_or(!ok)) break;  // partial sums complete (and a timed-out wait is agreed on)
       } else if (!ok) {
         break;
       }
+      // w' = w - sum of the parts (fixed order), scaled; used by the dot, written by one warp
+      auto wprime = [&](int r) -> double {
+        double wv = wsrc[r];
+        if (do_update) {
+          double tot = 0.0;
+          for (int q = 0; q < TPR; ++q) tot += up[q * CH + r];
+          wv -= tot;
+        }
+        if (do_scale) wv *= scale;
+        return wv;
+      };
+      if (rewrite && warp < groups) {
+        const int r = warp * 32 + lane;
+        if (r < rows) Vw[r0 + r] = wprime(r);
+      }
       if (do_dot) {
-        const double *wd = (do_update || do_scale) ? wnew : wsrc;
         for (int r = lane; r < rows; r += 32) {
-          const double wr = wd[r];
+          const double wr = rewrite ? wprime(r) : wsrc[r];
 #pragma unroll
           for (int t = 0; t < MAXCPW; ++t) {
             const int c = warp + kConsumerWarps * t;

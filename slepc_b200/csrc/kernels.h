@@ -36,8 +36,14 @@ uint64_t launch_count();
 constexpr int kTileNnz = 4096;   // nonzeros staged per CTA of the row-block SpMV
 constexpr int kTileRows = 1024;  // rows per CTA of the row-block SpMV
 int spmv_choose_lanes(int n, int64_t nnz);
+constexpr int kWarpTileNnz = 256;  // nonzeros staged per warp tile of the warp-tile SpMV
 // Row blocks for the row-block SpMV: block b covers rows [b[i], b[i+1]).
 std::vector<int> spmv_row_blocks(int n, const int *rowptr_host);
+// Warp tiles (<= 32 rows, <= kWarpTileNnz nonzeros) for the warp-tile SpMV.
+std::vector<int> spmv_warp_tiles(int n, const int *rowptr_host);
+cudaError_t spmv_warptile_launch(int ntiles, const int *tiles, const int *rowptr, const int *colind,
+                                 const double *vals, const double *x, double *y, cudaStream_t stream,
+                                 const GsState *st = nullptr, int step = 0);
 // st/step: when st is given, the launch is skipped on the device if a
 // Lanczos run halted (breakdown) at an earlier step.
 cudaError_t spmv_rowblock_launch(int nblocks, const int *blocks, const int *rowptr, const int *colind,

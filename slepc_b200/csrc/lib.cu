@@ -62,22 +62,31 @@ struct b200_mat_s {
   int lanes = 8;
   int *blocks = nullptr;  // row blocks of the row-block SpMV (nblocks + 1 entries)
   int nblocks = 0;
+  int *tiles = nullptr;   // warp tiles of the warp-tile SpMV (ntiles + 1 entries)
+  int ntiles = 0;
+  int schedule = B200_SPMV_WARPTILE;
   cudaStream_t stream = nullptr;
 };
 
-// Row blocks from a host copy of rowptr, uploaded to the device.
+// Row blocks and warp tiles from a host copy of rowptr, uploaded to the device.
 static b200_status mat_set_blocks(b200_mat M, const int *rowptr_host) {
   std::vector<int> b = spmv_row_blocks(M->n, rowptr_host);
+  std::vector<int> t = spmv_warp_tiles(M->n, rowptr_host);
   M->nblocks = (int)b.size() - 1;
+  M->ntiles = (int)t.size() - 1;
   B200_CUDA_CHECK(cudaMalloc(&M->blocks, sizeof(int) * b.size()));
+  B200_CUDA_CHECK(cudaMalloc(&M->tiles, sizeof(int) * t.size()));
   B200_CUDA_CHECK(cudaMemcpyAsync(M->blocks, b.data(), sizeof(int) * b.size(), cudaMemcpyHostToDevice, M->stream));
+  B200_CUDA_CHECK(cudaMemcpyAsync(M->tiles, t.data(), sizeof(int) * t.size(), cudaMemcpyHostToDevice, M->stream));
   B200_CUDA_CHECK(cudaStreamSynchronize(M->stream));
   return B200_OK;
 }
 
 static cudaError_t mat_spmv(b200_mat A, const double *x, double *y, cudaStream_t stream, const GsState *st = nullptr,
                             int step = 0) {
-  return spmv_rowblock_launch(A->nblocks, A->blocks, A->rowptr, A->colind, A->vals, x, y, stream, st, step);
+  if (A->schedule == B200_SPMV_ROWBLOCK)
+    return spmv_rowblock_launch(A->nblocks, A->blocks, A->rowptr, A->colind, A->vals, x, y, stream, st, step);
+  return spmv_warptile_launch(A->ntiles, A->tiles, A->rowptr, A->colind, A->vals, x, y, stream, st, step);
 }
 
 static b200_status mat_alloc(int n, int64_t nnz, cudaStream_t stream, b200_mat *A) {
@@ -175,6 +184,12 @@ extern "C" b200_status b200_mat_get_size(b200_mat A, int *n, int64_t *nnz) {
   return B200_OK;
 }
 
+extern "C" b200_status b200_mat_set_spmv_schedule(b200_mat A, int schedule) {
+  B200_ARG_CHECK(A && (schedule == B200_SPMV_ROWBLOCK || schedule == B200_SPMV_WARPTILE), "unknown SpMV schedule");
+  A->schedule = schedule;
+  return B200_OK;
+}
+
 extern "C" b200_status b200_mat_get_lanes(b200_mat A, int *lanes) {
   B200_ARG_CHECK(A && lanes, "null argument");
   *lanes = A->lanes;
@@ -187,6 +202,7 @@ extern "C" b200_status b200_mat_destroy(b200_mat A) {
   cudaFree(A->colind);
   cudaFree(A->vals);
   cudaFree(A->blocks);
+  cudaFree(A->tiles);
   delete A;
   return B200_OK;
 }

@@ -86,6 +86,63 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_rowblock_kernel(const int *
   }
 }
 
+// Warp tiles: a tile is <= 32 rows and <= kWarpTileNnz nonzeros (a longer row is a tile of
+// its own).  Lane i of the owning warp streams nonzeros i, i+32, ... (kWarpTileNnz/32 value,
+// index and x loads in flight per lane), keeps the rounded products in warp-private shared
+// memory, and after a __syncwarp sums row i of the tile in index order.  No CTA barrier.
+__global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles, const int *__restrict__ tiles,
+                                                                     const int *__restrict__ rowptr,
+                                                                     const int *__restrict__ colind,
+                                                                     const double *__restrict__ vals,
+                                                                     const double *__restrict__ x,
+                                                                     double *__restrict__ y,
+                                                                     const GsState *__restrict__ st, int step) {
+  if (st && st->halt && st->halt_step < step) return;
+  __shared__ double prod_all[kSpmvThreads / 32][kWarpTileNnz];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double *prod = prod_all[wib];
+  const int nwarps = gridDim.x * (kSpmvThreads / 32);
+  for (int t = blockIdx.x * (kSpmvThreads / 32) + wib; t < ntiles; t += nwarps) {
+    const int r0 = __ldg(tiles + t), r1 = __ldg(tiles + t + 1);
+    const int nrows = r1 - r0;  // 1..32
+    const int myrow_start = (lane < nrows) ? __ldg(rowptr + r0 + lane) : 0;
+    const int p0 = __shfl_sync(0xffffffffu, myrow_start, 0);
+    const int p1 = __ldg(rowptr + r1);
+    const int next = __shfl_down_sync(0xffffffffu, myrow_start, 1);
+    const int myrow_end = (lane + 1 < nrows) ? next : p1;
+    const int cnt = p1 - p0;
+    if (cnt > kWarpTileNnz) {
+      // one long row: strided partial sums, fixed-order warp tree
+      double sacc = 0.0;
+      for (int p = p0 + lane; p < p1; p += 32)
+        sacc = __dadd_rn(sacc, __dmul_rn(__ldcs(vals + p), __ldg(x + __ldcs(colind + p))));
+      sacc = warp_sum(sacc);
+      if (lane == 0) y[r0] = sacc;
+      continue;
+    }
+    double a[kWarpTileNnz / 32];
+    int c[kWarpTileNnz / 32];
+#pragma unroll
+    for (int u = 0; u < kWarpTileNnz / 32; ++u) {
+      const int q = lane + 32 * u;
+      a[u] = (q < cnt) ? __ldcs(vals + p0 + q) : 0.0;
+      c[u] = (q < cnt) ? __ldcs(colind + p0 + q) : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < kWarpTileNnz / 32; ++u) {
+      const int q = lane + 32 * u;
+      if (q < cnt) prod[q] = __dmul_rn(a[u], __ldg(x + c[u]));
+    }
+    __syncwarp();
+    if (lane < nrows) {
+      double sacc = 0.0;
+      for (int q = myrow_start - p0; q < myrow_end - p0; ++q) sacc = __dadd_rn(sacc, prod[q]);
+      y[r0 + lane] = sacc;
+    }
+    __syncwarp();
+  }
+}
+
 template <int LPR>
 __global__ void __launch_bounds__(256) spmv_csr_kernel(int n, const int *__restrict__ rowptr,
                                                        const int *__restrict__ colind,
@@ -137,6 +194,41 @@ std::vector<int> spmv_row_blocks(int n, const int *rowptr) {
     b.push_back(r);
   }
   return b;
+}
+
+std::vector<int> spmv_warp_tiles(int n, const int *rowptr) {
+  std::vector<int> b;
+  b.reserve(n / 16 + 2);
+  int r = 0;
+  b.push_back(0);
+  while (r < n) {
+    const int start = r;
+    const int base = rowptr[start];
+    while (r < n && r - start < 32 && rowptr[r + 1] - base <= kWarpTileNnz) ++r;
+    if (r == start) ++r;  // a single row longer than the tile: a tile of its own
+    b.push_back(r);
+  }
+  return b;
+}
+
+cudaError_t spmv_warptile_launch(int ntiles, const int *tiles, const int *rowptr, const int *colind,
+                                 const double *vals, const double *x, double *y, cudaStream_t stream,
+                                 const GsState *st, int step) {
+  if (ntiles <= 0) return cudaSuccess;
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 1;
+  }
+  const int warps_per_cta = kSpmvThreads / 32;
+  int grid = (ntiles + warps_per_cta - 1) / warps_per_cta;
+  const int cap = sms * 8;  // persistent: 8 CTAs (64 warps) per SM
+  if (grid > cap) grid = cap;
+  spmv_warptile_kernel<<<grid, kSpmvThreads, 0, stream>>>(ntiles, tiles, rowptr, colind, vals, x, y, st, step);
+  count_launch();
+  return cudaGetLastError();
 }
 
 cudaError_t spmv_rowblock_launch(int nblocks, const int *blocks, const int *rowptr, const int *colind,

@@ -68,6 +68,7 @@ def spmv(args, torch):
     n = len(csr[0]) - 1
     nnz = int(csr[0][-1])
     A = S.Mat().createAIJ(csr)
+    A.setSpMVSchedule(args.schedule)
     x = torch.from_numpy(P.start_vector(n, 0)).cuda()
     y = torch.empty(n, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")
@@ -84,7 +85,7 @@ def spmv(args, torch):
         ms += e0.elapsed_time(e1)
     ms /= args.reps
     algo = nnz * 12 + (n + 1) * 4 + 2 * n * 8
-    return {"kernel": "spmv_rowblock_kernel", "n": n, "nnz": nnz, "ms": ms, "algorithmic_bytes": algo,
+    return {"kernel": ["spmv_rowblock_kernel", "spmv_warptile_kernel"][args.schedule], "n": n, "nnz": nnz, "ms": ms, "algorithmic_bytes": algo,
             "GBps": algo / (ms * 1e-3) / 1e9}
 
 
@@ -122,6 +123,7 @@ def main():
     p.add_argument("--j", type=int, nargs="+", default=[60])
     p.add_argument("--m", type=int, default=82)
     p.add_argument("--reps", type=int, default=5)
+    p.add_argument("--schedule", type=int, default=1, help="SpMV schedule: 0 row blocks, 1 warp tiles")
     p.add_argument("--warmup", type=int, default=2)
     args = p.parse_args()
     import torch

@@ -49,13 +49,15 @@ def test_spmv_all_lane_widths_vs_oracle(b200, oracle_mod, lanes):
     np.testing.assert_allclose(yd.cpu().numpy(), ref, rtol=1e-13, atol=1e-13 * np.abs(ref).max())
 
 
-def test_spmv_laplacian_via_mat_bit_exact(b200, oracle_mod):
-    """Row-block SpMV of the Mat type: rows summed in index order, so it matches the
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_spmv_laplacian_via_mat_bit_exact(b200, oracle_mod, schedule):
+    """Mat SpMV (row blocks / warp tiles): rows summed in index order, so it matches the
     oracle's sequential row loop bit for bit."""
     torch = _torch()
     csr = P.laplacian_3d(40, 33, 29)
     n = len(csr[0]) - 1
     A = b200.Mat().createAIJ(csr)
+    A.setSpMVSchedule(schedule)
     assert A.getLanes() == 8
     x = P.start_vector(n, 4)
     xd = torch.from_numpy(x).cuda()
@@ -65,8 +67,9 @@ def test_spmv_laplacian_via_mat_bit_exact(b200, oracle_mod):
     np.testing.assert_array_equal(yd.cpu().numpy(), oracle_mod.spmv(P.to_scipy(csr), x))
 
 
-def test_spmv_mat_ragged_long_rows(b200, oracle_mod):
-    """Empty rows, short rows, and rows longer than one CTA's tile (4096 nonzeros)."""
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_spmv_mat_ragged_long_rows(b200, oracle_mod, schedule):
+    """Empty rows, short rows, and rows longer than a tile (4096 / 256 nonzeros)."""
     torch = _torch()
     rng = np.random.default_rng(3)
     n = 20011
@@ -79,6 +82,7 @@ def test_spmv_mat_ragged_long_rows(b200, oracle_mod):
     vals = rng.standard_normal(int(rowptr[-1]))
     csr = (rowptr.astype(np.int32), colind, vals)
     A = b200.Mat().createAIJ(csr)
+    A.setSpMVSchedule(schedule)
     x = rng.standard_normal(n)
     xd = torch.from_numpy(x).cuda()
     yd = torch.full((n,), np.nan, dtype=torch.float64, device="cuda")
@@ -86,7 +90,7 @@ def test_spmv_mat_ragged_long_rows(b200, oracle_mod):
     torch.cuda.synchronize()
     ref = oracle_mod.spmv(P.to_scipy(csr), x)
     y = yd.cpu().numpy()
-    short = lens <= 4096
+    short = lens <= (4096 if schedule == 0 else 256)
     np.testing.assert_array_equal(y[short], ref[short])
     np.testing.assert_allclose(y[~short], ref[~short], rtol=1e-12, atol=1e-12 * np.abs(ref).max())
 

@@ -35,7 +35,7 @@ from slepc_b200 import problems as P  # noqa: E402
 # Column visits (sum over Lanczos steps j of j+2) of a full solve of this
 # workload, measured by the GPU arm (stats.column_visits); the reference arm
 # uses it to extrapolate its bounded CPU sample to a full solve.
-FULL_SOLVE_COLUMN_VISITS = {128: None}
+FULL_SOLVE_COLUMN_VISITS = {128: 219668}
 
 SPMV_BYTES_PER_NNZ = 12  # 8-byte value + 4-byte column index
 
@@ -49,7 +49,7 @@ def parse():
     p.add_argument("--grid", type=int, default=128)
     p.add_argument("--nev", type=int, default=32)
     p.add_argument("--ncv", type=int, default=80)
-    p.add_argument("--cpu-restarts", type=int, default=2, help="restarts in the bounded CPU sample")
+    p.add_argument("--cpu-restarts", type=int, default=4, help="restarts in the bounded CPU sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
 

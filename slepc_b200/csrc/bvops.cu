@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(kGemmThreads) multinplace_kernel(double *V, in
                                                                    int nc) {
   extern __shared__ __align__(16) double sm[];
   double *Qs = sm;                          // [kq][nc] row-major by c: Qs[c*nc + j]
-  double *As = sm + (size_t)kq * nc;        // [max(kq,nc)][kRB]: input panel As[c*kRB + r], then output tile
+  double *As = sm + (size_t)kq * nc;        // input panel As[c*kRB + r]; then output tile Os[j*(kRB+1) + r]
   const int tid = threadIdx.x;
   for (int idx = tid; idx < kq * nc; idx += kGemmThreads) {
     const int c = idx / nc, j = idx - c * nc;
@@ -76,18 +76,18 @@ __global__ void __launch_bounds__(kGemmThreads) multinplace_kernel(double *V, in
 #pragma unroll
         for (int jj = 0; jj < MAXJ; ++jj) acc[ii][jj] = fma(a[ii], q[jj], acc[ii][jj]);
     }
-    __syncthreads();  // panel fully consumed: reuse As as the output tile [nc][kRB]
+    __syncthreads();  // panel fully consumed: reuse its space as the output tile, padded to kRB+1 per column
 #pragma unroll
     for (int ii = 0; ii < 4; ++ii)
 #pragma unroll
       for (int jj = 0; jj < MAXJ; ++jj) {
         const int j = cg + 16 * jj;
-        if (j < nc) As[j * kRB + rg + 16 * ii] = acc[ii][jj];
+        if (j < nc) As[j * (kRB + 1) + rg + 16 * ii] = acc[ii][jj];
       }
     __syncthreads();
     for (int idx = tid; idx < nc * kRB; idx += kGemmThreads) {
       const int j = idx / kRB, r = idx - j * kRB;
-      if (r < rows) V[(size_t)(s + j) * ld + r0 + r] = As[idx];
+      if (r < rows) V[(size_t)(s + j) * ld + r0 + r] = As[j * (kRB + 1) + r];
     }
   }
 }
@@ -258,7 +258,7 @@ cudaError_t multinplace_launch(double *V, int ld, int n, int l, int k, const dou
   const int kq = k - l, nc = e - s;
   if (nc <= 0 || kq <= 0 || n <= 0) return cudaSuccess;
   if (nc > 16 * 8 || kq > kMaxCols) return cudaErrorInvalidValue;
-  const size_t smem = sizeof(double) * ((size_t)kq * nc + (size_t)(kq > nc ? kq : nc) * kRB);
+  const size_t smem = sizeof(double) * ((size_t)kq * nc + (size_t)(kq > nc ? kq : nc) * (kRB + 1));
   if (smem + 1024 > max_dynamic_smem()) return cudaErrorInvalidValue;
   const int maxj = (nc + 15) / 16;
   const int npanels = (n + kRB - 1) / kRB;

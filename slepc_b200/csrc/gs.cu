@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
   double *cacc = coef_s + kMaxCols;           // [kMaxCols + 1]
   DecideShared *dsh = reinterpret_cast<DecideShared *>(cacc + kMaxCols + 1);
   __shared__ int is_last, timed_out, n_issued;
-  __shared__ double upd[2 * kConsumers];      // partial update sums (TPR*CH = 256 per chunk), by chunk parity
+  __shared__ double upd[2 * kConsumers];      // partial update sums (TPR*CH = kConsumers per chunk), by chunk parity
   const size_t head = 128 + sizeof(double) * (2 * kMaxCols + 1) + ((sizeof(DecideShared) + 127) / 128) * 128;
   double *stage_base = reinterpret_cast<double *>(smem_raw + ((head + 127) / 128) * 128);
   const size_t stage_elems = (size_t)CH * (jb + 1);

@@ -1,5 +1,7 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 Krylov-Schur eigensolver on the 3-D 128^3 Laplacian.
+"""Benchmark of the B200 Krylov-Schur eigensolver on the 3-D 128^3 Laplacian
+(default), or of the SVD cross solver on a power-law rectangular matrix
+(--workload cross).
 
 Workload (one "step" = one full EPSSolve from the seeded start vector):
   3-D 7-point Dirichlet Laplacian on a 128^3 grid (n = 2,097,152, 14,581,760
@@ -36,6 +38,8 @@ from slepc_b200 import problems as P  # noqa: E402
 # workload, measured by the GPU arm (stats.column_visits); the reference arm
 # uses it to extrapolate its bounded CPU sample to a full solve.
 FULL_SOLVE_COLUMN_VISITS = {128: 219668}
+# Lanczos steps of a full solve of the SVD cross workload (rows, cols, nsv, ncv), measured by the GPU arm.
+FULL_SOLVE_LANCZOS_STEPS_CROSS = {}
 
 SPMV_BYTES_PER_NNZ = 12  # 8-byte value + 4-byte column index
 
@@ -51,6 +55,14 @@ def parse():
     p.add_argument("--ncv", type=int, default=80)
     p.add_argument("--cpu-restarts", type=int, default=4, help="restarts in the bounded CPU sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", choices=["laplacian3d", "cross"], default="laplacian3d",
+                   help="laplacian3d: the EPS headline case; cross: largest singular triplets of the "
+                        "2,000,000 x 500,000 power-law matrix through A^T A")
+    p.add_argument("--rows", type=int, default=2_000_000, help="cross workload: rows of A")
+    p.add_argument("--cols", type=int, default=500_000, help="cross workload: columns of A")
+    p.add_argument("--nsv", type=int, default=32, help="cross workload: singular triplets")
+    p.add_argument("--svd-ncv", type=int, default=96, help="cross workload: ncv")
+    p.add_argument("--svd-dtype", choices=["f32", "f64"], default="f32", help="cross workload: value storage")
     return p.parse_args()
 
 
@@ -328,8 +340,205 @@ def run_b200(args):
     return 0
 
 
+# ------------------------------------------------------------------ SVD cross workload
+SVD_TOL = 1e-7
+
+
+def cross_workload(args):
+    csr = P.powerlaw_rect(args.rows, args.cols, 20, 1.8, seed=0)
+    return csr, P.start_vector(min(args.rows, args.cols), 0)
+
+
+def cross_config(args, nnz, extra=None):
+    d = {"workload": f"largest {args.nsv} singular triplets of a {args.rows} x {args.cols} sparse matrix "
+                     f"(20 distinct columns per row, column index power law exponent 1.8, N(0,1) values stored "
+                     f"{'FP32' if args.svd_dtype == 'f32' else 'FP64'}), SVD cross: Krylov-Schur on A^T A, "
+                     f"ncv={args.svd_ncv}, tol={SVD_TOL:g}",
+         "m": args.rows, "n": args.cols, "nnz": nnz, "nsv": args.nsv, "ncv": args.svd_ncv, "tol": SVD_TOL,
+         "start_vector": "N(0,1) seed 0",
+         "l2": "inputs larger than L2: A and its transpose %.0f MB, basis %.2f GB (L2 = 126 MB)"
+               % (2 * nnz * (8 if args.svd_dtype == "f32" else 12) / 1e6, args.cols * (args.svd_ncv + 1) * 8 / 1e9),
+         "parallelism": "replicas" if args.gpus > 1 else "single GPU"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+def cross_cpu_sample(csr, v0, args, threads):
+    import oracle
+
+    oracle.set_threads(threads)
+    t0 = time.perf_counter()
+    r = oracle.svd_cross(csr[0], csr[1], csr[2].astype(np.float64), (args.rows, args.cols), v0, args.nsv,
+                         args.svd_ncv, tol=SVD_TOL, max_restarts=args.cpu_restarts)
+    return time.perf_counter() - t0, r
+
+
+def run_reference_cross(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return 0
+    csr, v0 = cross_workload(args)
+    threads = os.cpu_count() or 1
+    full_steps = FULL_SOLVE_LANCZOS_STEPS_CROSS.get((args.rows, args.cols, args.nsv, args.svd_ncv))
+    if full_steps is None:
+        print(json.dumps({"impl": "reference", "unavailable": "no full-solve Lanczos step count recorded"}))
+        return 0
+    for _ in range(args.warmup):
+        cross_cpu_sample(csr, v0, args, threads)
+    times, steps = [], None
+    for _ in range(args.steps):
+        t, r = cross_cpu_sample(csr, v0, args, threads)
+        times.append(t)
+        steps = r.lanczos_steps
+    value = statistics.mean(times) / steps * full_steps
+    sample = (f"first {args.cpu_restarts} restart(s) of the solve ({steps} Lanczos steps, "
+              f"{statistics.mean(times):.1f} s), extrapolated to the {full_steps} Lanczos steps of a full solve")
+    line = {"impl": "reference", "metric": "time_to_all_residuals_le_1e-7", "value": value, "unit": "s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": statistics.mean(times) * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded power-law matrix and start vector)",
+            "config": cross_config(args, int(csr[0][-1])),
+            "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_b200_cross(args):
+    import torch
+
+    import slepc_b200 as S
+
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    m, n = args.rows, args.cols
+    csr, v0 = cross_workload(args)
+    nnz = int(csr[0][-1])
+    dt = np.float32 if args.svd_dtype == "f32" else np.float64
+    vals = csr[2].astype(dt)
+    A = S.Mat().createAIJ((csr[0], csr[1], vals), size=(m, n), dtype=dt)
+    E = S.SVD().create()
+    E.setOperators(A)
+    E.setDimensions(args.nsv, args.svd_ncv)
+    E.setTolerances(SVD_TOL)
+    E.setInitialSpace(v0)
+
+    def step():
+        E.solve()
+        E.getVectorPointers(0)  # SVDComputeVectors: U = A V, orthogonalised
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    launches0 = S.kernel_launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        step()
+    ev1.record()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = S.kernel_launch_count() - launches0
+    ms_per_step = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+    nconv = E.getConverged()
+    reason = E.getConvergedReason()
+    errs = [E.computeError(i) for i in range(min(nconv, args.nsv))]
+    stats = E.getStats()
+
+    E.setTiming(True)
+    step()
+    tstats = E.getStats()
+    E.setTiming(False)
+    peak, peak_kind = measured_peaks()
+    vb = 4 if dt == np.float32 else 8
+    # one application of A^T A: both CSR operands once, x and w read once and written once
+    op_bytes = 2 * nnz * (vb + 4) + (m + 1 + n + 1) * 4 + 2 * (m + n) * 8
+    spmv_gbs = (op_bytes * tstats["lanczos_steps"] / (tstats["ms_spmv"] * 1e-3) / 1e9
+                if tstats["ms_spmv"] > 0 else None)
+    gs_gbs = tstats["gs_bytes"] / (tstats["ms_orth"] * 1e-3) / 1e9 if tstats["ms_orth"] > 0 else None
+
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    h_csr = (pin(csr[0]), pin(csr[1]), pin(vals))
+    h_v0 = pin(v0)
+    barrier()
+    t0 = time.perf_counter()
+    e2e_last = None
+    for _ in range(args.steps):
+        e2e_last = S.svd_solve_aij_host(h_csr, (m, n), h_v0, args.nsv, args.svd_ncv, tol=SVD_TOL, dtype=dt)
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
+    h2d = csr[0].nbytes + csr[1].nbytes + vals.nbytes + v0.nbytes
+    d2h = e2e_last["nconv"] * ((m + n) * 8 + 16)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        t, r = cross_cpu_sample(csr, v0, args, threads)
+        value = t / r.lanczos_steps * stats["lanczos_steps"]
+        cpu = {"value": value, "unit": "s", "cores": threads, "kind": "port",
+               "sample": (f"first {args.cpu_restarts} restart(s) of the same solve on {threads} host threads "
+                          f"({r.lanczos_steps} Lanczos steps in {t:.1f} s), extrapolated to the "
+                          f"{stats['lanczos_steps']} Lanczos steps of the full GPU solve")}
+    if rank == 0:
+        line = {"metric": "time_to_all_residuals_le_1e-7", "value": ms_per_step / 1e3, "unit": "s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded power-law matrix, seeded N(0,1) start vector)",
+                "config": cross_config(args, nnz, {
+                    "restarts": stats["restarts"], "lanczos_steps": stats["lanczos_steps"],
+                    "column_visits": stats["column_visits"], "nconv": nconv, "reason": reason,
+                    "max_rel_error": max(errs) if errs else None}),
+                "roofline": {"kernel": "cross operator A^T A (warp-tile SpMV of A, segmented SpMV of A^T)",
+                             "bound": "hbm", "achieved": spmv_gbs, "peak": peak, "unit": "GB/s",
+                             "frac": (spmv_gbs / peak) if spmv_gbs else None, "peak_kind": peak_kind,
+                             "traffic": None, "gs_achieved": gs_gbs,
+                             "share_orth": tstats["ms_orth"] / tstats["ms_total"] if tstats["ms_total"] else None,
+                             "share_spmv": tstats["ms_spmv"] / tstats["ms_total"] if tstats["ms_total"] else None,
+                             "share_restart": tstats["ms_restart"] / tstats["ms_total"] if tstats["ms_total"] else None},
+                "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+                "gpu_launches": int(launches),
+                "clocks": clk,
+                "cpu_baseline": cpu}
+        print(json.dumps(line))
+    E.destroy()
+    A.destroy()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "cross":
+        if args.impl == "reference":
+            return run_reference_cross(args)
+        return run_b200_cross(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

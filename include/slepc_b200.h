@@ -5,13 +5,15 @@
  * (passed as void*) and an int status.  Every entry point names the SLEPc
  * interface it replaces (paths relative to the SLEPc 3.22 source tree).
  *
- * Three object kinds mirror SLEPc's:
+ * Four object kinds mirror SLEPc's:
  *   b200_mat  -- a CSR matrix resident in HBM with a hand-written SpMV
- *                (the new Mat SpMV type, in place of MATAIJCUSPARSE's MatMult)
+ *                (the new Mat SpMV type, in place of MATAIJCUSPARSE's MatMult),
+ *                or the cross-product shell A^T A of the SVD cross solver
  *   b200_bv   -- a column-major basis of vectors resident in HBM
  *                (the new BV type: the BVOps table of bvimpl.h:25-61)
  *   b200_eps  -- the Hermitian Krylov-Schur solver that drives them
  *                (EPSSolve with EPSKRYLOVSCHUR, problem type EPS_HEP)
+ *   b200_svd  -- the SVD cross solver (SVDCROSS): Krylov-Schur on A^T A
  *
  * Pointers marked _dev are device (HBM) addresses; pointers marked _host are
  * host addresses.  All work is ordered on the object's stream; entry points
@@ -37,6 +39,7 @@ typedef int b200_status;
 #define B200_ERR_NOMEM 6      /* device allocation failed */
 #define B200_ERR_STATE 7      /* call out of order (e.g. EPSGetEigenpair before EPSSolve) */
 #define B200_ERR_DEVICE 8     /* a kernel reported a device-side error (bounded wait expired, NaN) */
+#define B200_ERR_FP 9         /* floating-point failure (PETSC_ERR_FP: negative eigenvalue of A^T A) */
 
 /* Which eigenpairs (EPSWhich, include/slepceps.h; comparators src/sys/slepcsc.c:152-210). */
 #define B200_LARGEST_MAGNITUDE 1
@@ -54,9 +57,22 @@ typedef int b200_status;
 #define B200_ERROR_ABSOLUTE 0
 #define B200_ERROR_RELATIVE 1
 
+/* Storage types of matrix values (PETSc's MatScalar: double, or single with
+ * --with-precision=single).  Products and sums are FP64 for both. */
+#define B200_SCALAR_F64 0
+#define B200_SCALAR_F32 1
+
+/* Which singular triplets (SVDWhich, include/slepcsvd.h). */
+#define B200_SVD_LARGEST 0
+#define B200_SVD_SMALLEST 1
+
+/* Error type for b200_svd_compute_error in addition to ABSOLUTE/RELATIVE (SVD_ERROR_NORM). */
+#define B200_ERROR_NORM 2
+
 typedef struct b200_mat_s *b200_mat;
 typedef struct b200_bv_s *b200_bv;
 typedef struct b200_eps_s *b200_eps;
+typedef struct b200_svd_s *b200_svd;
 
 /* Library information and the last error message (thread-local). */
 const char *b200_version(void);
@@ -75,9 +91,29 @@ b200_status b200_mat_create_csr(int n, int64_t nnz, const int *rowptr_host, cons
 /* Same, from arrays already in HBM (copied device to device). */
 b200_status b200_mat_create_csr_device(int n, int64_t nnz, const int *rowptr_dev, const int *colind_dev,
                                        const double *vals_dev, void *stream, b200_mat *A);
-/* y = A x on device vectors (MatMult). */
+/* Create a general m x n CSR matrix from host arrays (copied), values stored
+ * as B200_SCALAR_F64 (double *) or B200_SCALAR_F32 (float *).  The explicit
+ * transpose is built on the host at creation and kept in HBM beside A, the
+ * transpose SVDSetUp builds with MatHermitianTranspose
+ * (src/svd/interface/svdsetup.c:300-314); rows of A longer than 256 nonzeros
+ * (and of A^T: the power-law columns of A) are split into segments whose
+ * partial sums are added in a fixed order. */
+b200_status b200_mat_create_aij(int m, int n, int64_t nnz, const int *rowptr_host, const int *colind_host,
+                                const void *vals_host, int scalar_type, void *stream, b200_mat *A);
+/* The shell C = A^T A of SVDCROSS (MatMult_Cross, src/svd/impls/cross/cross.c:31-41):
+ * y = A^T (A x) through a device work vector of length m.  A must be created by
+ * b200_mat_create_aij and outlive C.  C is the EPS operator of the cross solver. */
+b200_status b200_mat_create_cross(b200_mat A, b200_mat *C);
+/* y = A x on device vectors (MatMult); for a cross shell y = A^T A x. */
 b200_status b200_mat_mult(b200_mat A, const double *x_dev, double *y_dev);
+/* y = A^T x (MatMultTranspose) for a matrix from b200_mat_create_aij. */
+b200_status b200_mat_mult_transpose(b200_mat A, const double *x_dev, double *y_dev);
+/* Number of columns (the operator dimension of a square or cross operator) and nonzeros. */
 b200_status b200_mat_get_size(b200_mat A, int *n, int64_t *nnz);
+/* MatGetSize: rows and columns. */
+b200_status b200_mat_get_sizes(b200_mat A, int *m, int *n);
+/* MatNorm(NORM_INFINITY), known for matrices created from host arrays. */
+b200_status b200_mat_norm_inf(b200_mat A, double *nrm);
 /* CSR SpMV schedule of a matrix (a MatSetOption-style knob):
  *   B200_SPMV_WARPTILE (default) -- warp tiles of <= 32 rows / <= 256 nonzeros;
  *   B200_SPMV_ROWBLOCK           -- CTA row blocks of <= 1024 rows / <= 4096 nonzeros.
@@ -236,6 +272,57 @@ b200_status b200_eps_solve_csr_host(int n, int64_t nnz, const int *rowptr_host, 
                                     const double *vals_host, const double *v0_host, int nev, int ncv, int mpd,
                                     double tol, int max_it, int which, double *evals_host, double *X_host,
                                     double *errest_host, int *info_host, void *stream);
+
+/* ------------------------------------------------------------------ SVD --- */
+
+/* The SVD cross solver (SVDCROSS, src/svd/impls/cross/cross.c) for a standard
+ * problem: Krylov-Schur (the b200_eps solver above) on the shell A^T A of
+ * b200_mat_create_cross, sigma = sqrt(lambda), left vectors U = A V
+ * orthogonalised by Gram-Schmidt.  A comes from b200_mat_create_aij; when A
+ * has fewer rows than columns the operator is A A^T and the roles of U and V
+ * are exchanged, as SVDSetUp does (src/svd/interface/svdsetup.c:300-343).
+ * SVDCreate / SVDDestroy / SVDSetOperators(svd,A,NULL). */
+b200_status b200_svd_create(void *stream, b200_svd *svd);
+b200_status b200_svd_destroy(b200_svd svd);
+b200_status b200_svd_set_operator(b200_svd svd, b200_mat A);
+/* SVDSetDimensions (ncv, mpd <= 0: the EPS defaults). */
+b200_status b200_svd_set_dimensions(b200_svd svd, int nsv, int ncv, int mpd);
+/* SVDSetTolerances (tol <= 0: 1e-8, and the EPS runs with 1e-9 as
+ * SVDSetUp_Cross chooses, cross.c:217; max_it <= 0: the EPS default). */
+b200_status b200_svd_set_tolerances(b200_svd svd, double tol, int max_it);
+/* SVDSetWhichSingularTriplets: B200_SVD_LARGEST or B200_SVD_SMALLEST. */
+b200_status b200_svd_set_which_singular_triplets(b200_svd svd, int which);
+/* SVDSetInitialSpaces with one vector, of the operator's dimension: the
+ * columns of A, or its rows when A has fewer rows than columns (the spaces
+ * are swapped with the matrix, svdsetup.c:333-338). */
+b200_status b200_svd_set_initial_space(b200_svd svd, const double *v0_host);
+/* Per-phase CUDA-event timing of the inner eigensolve (b200_eps_set_timing). */
+b200_status b200_svd_set_timing(b200_svd svd, int on);
+/* SVDSolve (src/svd/interface/svdsolve.c) with SVDSolve_Cross (cross.c:256-285). */
+b200_status b200_svd_solve(b200_svd svd);
+b200_status b200_svd_get_converged(b200_svd svd, int *nconv);
+b200_status b200_svd_get_iteration_number(b200_svd svd, int *its);
+b200_status b200_svd_get_converged_reason(b200_svd svd, int *reason);
+/* SVDGetSingularTriplet: sigma_i and (nullable) host copies of u_i (length m)
+ * and v_i (length n).  The singular vectors are computed on first request
+ * (SVDComputeVectors_Cross, cross.c:287-355). */
+b200_status b200_svd_get_singular_triplet(b200_svd svd, int i, double *sigma, double *u_host, double *v_host);
+/* Device addresses of u_i and v_i, valid until the next solve or destroy. */
+b200_status b200_svd_get_singular_vectors_device(b200_svd svd, int i, const double **u_dev, const double **v_dev);
+/* SVDComputeError (svdsolve.c:485-580): sqrt(||A v - sigma u||^2 + ||A^T u - sigma v||^2),
+ * divided by sigma*sqrt(2) (B200_ERROR_RELATIVE) or ||A||_inf*sqrt(2) (B200_ERROR_NORM). */
+b200_status b200_svd_compute_error(b200_svd svd, int i, int type, double *error);
+/* Statistics of the inner Krylov-Schur solve. */
+b200_status b200_svd_get_stats(b200_svd svd, b200_eps_stats *stats);
+
+/* One call from host CSR to host singular triplets, largest first:
+ * sigma_host (nconv values), U_host (m x nconv, column-major), V_host
+ * (n x nconv), rel_error_host (relative errors), all nullable; info_host[0..4]
+ * = nconv, its, reason, lanczos steps, restarts. */
+b200_status b200_svd_solve_aij_host(int m, int n, int64_t nnz, const int *rowptr_host, const int *colind_host,
+                                    const void *vals_host, int scalar_type, const double *v0_host, int nsv, int ncv,
+                                    double tol, int max_it, double *sigma_host, double *U_host, double *V_host,
+                                    double *rel_error_host, int *info_host, void *stream);
 
 #ifdef __cplusplus
 }

@@ -41,6 +41,11 @@ def lib():
         L.oracle_residual.argtypes = [ctypes.c_int, _ip, _ip, _dp, _dp, ctypes.c_double]
         L.oracle_spmv.argtypes = [ctypes.c_int, _ip, _ip, _dp, _dp, _dp]
         L.oracle_set_threads.argtypes = [ctypes.c_int]
+        L.oracle_csr_transpose.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, _ip, _ip, _dp]
+        L.oracle_svd_cross.restype = ctypes.c_int
+        L.oracle_svd_cross.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, _ip, _ip, _dp, _dp,
+                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, _ip]
         L.oracle_random_entry.restype = ctypes.c_double
         L.oracle_random_entry.argtypes = [ctypes.c_uint64] * 3
         _lib = L
@@ -152,3 +157,58 @@ def residual(A, x, lam):
 
 def random_entry(seed, stream, i):
     return lib().oracle_random_entry(seed, stream, i)
+
+
+def csr_transpose(rowptr, colind, vals, shape):
+    """Explicit transpose (MatTranspose_SeqAIJ order) of CSR arrays; returns (rowptr_t, colind_t, vals_t)."""
+    m, n = shape
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+    colind = np.ascontiguousarray(colind, dtype=np.int32)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    nnz = int(rowptr[m])
+    rt = np.zeros(n + 1, dtype=np.int32)
+    ct = np.zeros(max(nnz, 1), dtype=np.int32)
+    vt = np.zeros(max(nnz, 1))
+    lib().oracle_csr_transpose(m, n, _i(rowptr), _i(colind), _d(vals), _i(rt), _i(ct), _d(vt))
+    return rt, ct[:nnz], vt[:nnz]
+
+
+class SVDResult:
+    def __init__(self, sigma, U, V, rel_error, nconv, its, reason, lanczos_steps, restarts, column_visits):
+        self.sigma, self.U, self.V, self.rel_error = sigma, U, V, rel_error
+        self.nconv, self.its, self.reason = nconv, its, reason
+        self.lanczos_steps, self.restarts, self.column_visits = lanczos_steps, restarts, column_visits
+
+
+def svd_cross(rowptr, colind, vals, shape, v0, nsv, ncv, tol=0.0, largest=True, mpd=0, max_it=0, max_restarts=0):
+    """SVDSolve with SVDCROSS on an m x n CSR matrix (values as float64; FP32-stored
+    matrices pass their float32 values widened).  For m < n the transpose is
+    solved and U, V swapped back, as SVDSetUp / SVDGetSingularTriplet do; v0 then
+    has length m."""
+    m, n = shape
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+    colind = np.ascontiguousarray(colind, dtype=np.int32)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    rt, ct, vt = csr_transpose(rowptr, colind, vals, shape)
+    swapped = m < n
+    if swapped:
+        rowptr, colind, vals, rt, ct, vt = rt, ct, vt, rowptr, colind, vals
+        m, n = n, m
+    v0 = np.ascontiguousarray(v0, dtype=np.float64)
+    assert v0.shape == (n,)
+    sig = np.zeros(ncv + 1)
+    U = np.zeros((ncv + 1, m))
+    V = np.zeros((ncv + 1, n))
+    err = np.zeros(ncv + 1)
+    info = np.zeros(8, dtype=np.int32)
+    st = lib().oracle_svd_cross(m, n, _i(rowptr), _i(colind), _d(vals), _i(rt), _i(ct), _d(vt), _d(v0), nsv, ncv,
+                                mpd, tol, max_it, 0 if largest else 1, max_restarts, _d(sig), _d(U), _d(V),
+                                _d(err), _i(info))
+    if st:
+        raise RuntimeError(f"oracle_svd_cross failed with status {st}")
+    k = int(info[0])
+    U, V = U[:k].T.copy(), V[:k].T.copy()
+    if swapped:
+        U, V = V, U
+    return SVDResult(sig[:k].copy(), U, V, err[:k].copy(), k, int(info[1]), int(info[2]), int(info[3]),
+                     int(info[4]), int(info[5]))

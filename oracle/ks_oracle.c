@@ -84,6 +84,62 @@ void oracle_spmv(int n, const int *rowptr, const int *colind, const double *vals
   }
 }
 
+/* CSR with the same row-order sums for a rectangular matrix (rows x any) */
+static void csr_mult(int rows, const int *rowptr, const int *colind, const double *vals, const double *x, double *y)
+{
+  oracle_spmv(rows, rowptr, colind, vals, x, y);
+}
+
+/*
+ * Explicit transpose, MatTranspose_SeqAIJ semantics: row c of A^T lists the
+ * rows i of A with a nonzero in column c in ascending i, so its sum runs in
+ * that order.  rowptr_t has cols+1 entries; colind_t / vals_t have nnz.
+ */
+void oracle_csr_transpose(int rows, int cols, const int *rowptr, const int *colind, const double *vals,
+                          int *rowptr_t, int *colind_t, double *vals_t)
+{
+  int i, c, p;
+  int *next = (int *)malloc(sizeof(int) * ((size_t)cols + 1));
+  for (c = 0; c <= cols; c++) rowptr_t[c] = 0;
+  for (p = 0; p < rowptr[rows]; p++) rowptr_t[colind[p] + 1]++;
+  for (c = 0; c < cols; c++) rowptr_t[c + 1] += rowptr_t[c];
+  for (c = 0; c < cols; c++) next[c] = rowptr_t[c];
+  for (i = 0; i < rows; i++)
+    for (p = rowptr[i]; p < rowptr[i + 1]; p++) {
+      int q = next[colind[p]]++;
+      colind_t[q] = i;
+      vals_t[q] = vals[p];
+    }
+  free(next);
+}
+
+/*
+ * The operator of the eigensolver: a square CSR matrix, or the shell
+ * C = A^T A of the SVD cross solver, applied as w = A x then y = A^T w
+ * (MatMult_Cross, src/svd/impls/cross/cross.c:31-41, explicit transpose as
+ * SVDSetUp builds by default, src/svd/interface/svdsetup.c:300-305).
+ */
+typedef struct {
+  int n;                    /* operator dimension */
+  int cross;                /* 0: y = A x (A n x n); 1: y = A^T (A x) (A m x n) */
+  int m;                    /* rows of A (cross) */
+  const int *rp, *ci;       /* A */
+  const double *va;
+  const int *rpt, *cit;     /* A^T (cross) */
+  const double *vat;
+  double *w;                /* m entries (cross) */
+} orc_op;
+
+static void op_apply(const orc_op *op, const double *x, double *y)
+{
+  if (!op->cross) {
+    oracle_spmv(op->n, op->rp, op->ci, op->va, x, y);
+    return;
+  }
+  csr_mult(op->m, op->rp, op->ci, op->va, x, op->w);
+  csr_mult(op->n, op->rpt, op->cit, op->vat, op->w, y);
+}
+
 static double nrm2(int n, const double *x)
 {
   /* plain two-norm; PETSc VecNorm(NORM_2) -> BLASnrm2 */
@@ -417,10 +473,10 @@ static int get_start_vector(obv *bv, int i, int *breakdown)
  * X (n x nconv, ld = n) the converged Ritz vectors sorted by SlepcSortEigenvalues,
  * evals (nconv) sorted values; info.
  */
-int oracle_eps_solve(int n, const int *rowptr, const int *colind, const double *vals, const double *v0,
-                     int nev, int ncv, int mpd, double tol, int max_it, int which, int max_restarts,
-                     double *evals, double *X, double *errest_out, int *info_out)
+static int eps_solve_op(const orc_op *op, const double *v0, int nev, int ncv, int mpd, double tol, int max_it,
+                        int which, int max_restarts, double *evals, double *X, double *errest_out, int *info_out)
 {
+  const int n = op->n;
   obv bv;
   ods ds;
   orc_info info;
@@ -471,7 +527,7 @@ int oracle_eps_solve(int n, const int *rowptr, const int *colind, const double *
     m = nv;
     breakdown = 0;
     for (j = k; j < m; j++) {
-      oracle_spmv(n, rowptr, colind, vals, bv.V + (size_t)j * bv.ld, bv.V + (size_t)(j + 1) * bv.ld);
+      op_apply(op, bv.V + (size_t)j * bv.ld, bv.V + (size_t)(j + 1) * bv.ld);
       if ((st = orthonormalize_column(&bv, j + 1, &beta, &lindep))) goto done;
       info.lanczos_steps++;
       info.column_visits += j + 2;
@@ -586,6 +642,117 @@ done:
   free(bv.V); free(bv.buf); free(bv.hvec); free(bv.cvec);
   free(ds.d); free(ds.Q); free(ds.rwork); free(ds.perm);
   free(eigr); free(errest); free(perm);
+  return st;
+}
+
+int oracle_eps_solve(int n, const int *rowptr, const int *colind, const double *vals, const double *v0,
+                     int nev, int ncv, int mpd, double tol, int max_it, int which, int max_restarts,
+                     double *evals, double *X, double *errest_out, int *info_out)
+{
+  orc_op op;
+  memset(&op, 0, sizeof(op));
+  op.n = n; op.rp = rowptr; op.ci = colind; op.va = vals;
+  return eps_solve_op(&op, v0, nev, ncv, mpd, tol, max_it, which, max_restarts, evals, X, errest_out, info_out);
+}
+
+/*
+ * oracle_svd_cross: SVDSolve with SVDCROSS for a standard problem whose
+ * matrix A (m x n, m >= n; a caller with m < n passes the transpose, as
+ * SVDSetUp swaps A and A^T, svdsetup.c:300-314) is given with its explicit
+ * transpose.  Follows
+ *   SVDSetUp_Cross (cross.c:160-250): EPS_HEP on C = A^T A, which =
+ *     largest (smallest) magnitude for the largest (smallest) triplets,
+ *     EPS tol = svd tol (1e-9 = SLEPC_DEFAULT_TOL/10 when tol <= 0);
+ *   SVDSolve_Cross (cross.c:256-285): sigma_i = sqrt(lambda_i), a negative
+ *     lambda > -10 eps reset to 0, below that an error;
+ *   SVDSolve's sort (svdsolve.c): ascending sort, reversed for the largest;
+ *   SVDComputeVectors_Cross + SVDComputeVectors_Left (cross.c:346-352,
+ *     svdsolve.c:21-75): V_i = eigenvector i, U = A V, BVOrthogonalize(U)
+ *     by Gram-Schmidt column after column (bvorthog.c:507-548);
+ *   SVDComputeError (svdsolve.c:485-580) relative: sqrt(n1^2 + n2^2) /
+ *     (sigma sqrt(2)), n1 = ||A v - sigma u||, n2 = ||A^T u - sigma v||.
+ * which_svd: 0 largest, 1 smallest.  Outputs (in SVD order, nconv entries):
+ * sigma, U (m x nconv), V (n x nconv), rel_error; info as oracle_eps_solve.
+ */
+int oracle_svd_cross(int m, int n, const int *rowptr, const int *colind, const double *vals, const int *rowptr_t,
+                     const int *colind_t, const double *vals_t, const double *v0, int nsv, int ncv, int mpd,
+                     double tol, int max_it, int which_svd, int max_restarts, double *sigma_out, double *U_out,
+                     double *V_out, double *rel_error, int *info_out)
+{
+  orc_op op;
+  obv bu;
+  int st, i, j, nconv, lindep, *perm;
+  double *lam, *X, *sig, norm;
+  if (m < n || n <= 0) return ORC_ERR_ARG;
+  memset(&op, 0, sizeof(op));
+  op.n = n; op.cross = 1; op.m = m;
+  op.rp = rowptr; op.ci = colind; op.va = vals;
+  op.rpt = rowptr_t; op.cit = colind_t; op.vat = vals_t;
+  op.w = (double *)malloc(sizeof(double) * (size_t)m);
+  lam = (double *)calloc((size_t)ncv + 1, sizeof(double));
+  sig = (double *)calloc((size_t)ncv + 1, sizeof(double));
+  perm = (int *)calloc((size_t)ncv + 1, sizeof(int));
+  X = (double *)calloc((size_t)n * (ncv + 1), sizeof(double));
+  if (tol <= 0.0) tol = 1e-9;
+  st = eps_solve_op(&op, v0, nsv, ncv, mpd, tol, max_it,
+                    which_svd == 0 ? ORC_LARGEST_MAGNITUDE : ORC_SMALLEST_MAGNITUDE, max_restarts, lam, X, NULL,
+                    info_out);
+  if (st) goto done;
+  nconv = info_out ? info_out[0] : 0;
+  for (i = 0; i < nconv; i++) {
+    double s = lam[i];
+    if (s <= -10 * ORC_MACHINE_EPS) { st = ORC_ERR_ARG; goto done; }
+    if (s < 0.0) s = 0.0;
+    sig[i] = sqrt(s);
+  }
+  /* sort: insertion sort ascending (stable), reversed for the largest */
+  for (i = 0; i < nconv; i++) perm[i] = i;
+  for (i = 1; i < nconv; i++) {
+    int t = perm[i];
+    j = i - 1;
+    while (j >= 0 && sig[perm[j]] > sig[t]) { perm[j + 1] = perm[j]; j--; }
+    perm[j + 1] = t;
+  }
+  if (which_svd == 0)
+    for (i = 0; i < nconv / 2; i++) { int t = perm[i]; perm[i] = perm[nconv - 1 - i]; perm[nconv - 1 - i] = t; }
+
+  /* U = A V, then Gram-Schmidt over the columns in order */
+  bu.n = m; bu.m = nconv > 0 ? nconv : 1; bu.ld = m;
+  bu.V = (double *)calloc((size_t)m * bu.m, sizeof(double));
+  bu.buf = (double *)calloc((size_t)bu.m * bu.m, sizeof(double));
+  bu.hvec = (double *)calloc(bu.m, sizeof(double));
+  bu.cvec = (double *)calloc(bu.m, sizeof(double));
+  bu.eta = 0.7071; bu.deftol = 10 * ORC_MACHINE_EPS; bu.seed = 0x5eedULL; bu.nrand = 0;
+  for (j = 0; j < nconv; j++) csr_mult(m, rowptr, colind, vals, X + (size_t)j * n, bu.V + (size_t)j * m);
+  for (j = 0; j < nconv && !st; j++) {
+    if ((st = orthogonalize_gs(&bu, j, NULL, &norm, &lindep))) break;
+    if (norm == 0.0) { st = ORC_ERR_BREAKDOWN; break; }
+    scale_column(&bu, j, 1.0 / norm);
+  }
+  if (!st) {
+    double *r1 = (double *)malloc(sizeof(double) * (size_t)m), *r2 = (double *)malloc(sizeof(double) * (size_t)n);
+    for (i = 0; i < nconv; i++) {
+      const int p = perm[i];
+      const double s = sig[p], *u = bu.V + (size_t)p * m, *v = X + (size_t)p * n;
+      if (sigma_out) sigma_out[i] = s;
+      if (U_out) memcpy(U_out + (size_t)i * m, u, sizeof(double) * (size_t)m);
+      if (V_out) memcpy(V_out + (size_t)i * n, v, sizeof(double) * (size_t)n);
+      if (rel_error) {
+        double n1, n2;
+        csr_mult(m, rowptr, colind, vals, v, r1);
+        for (j = 0; j < m; j++) r1[j] -= s * u[j];
+        csr_mult(n, rowptr_t, colind_t, vals_t, u, r2);
+        for (j = 0; j < n; j++) r2[j] -= s * v[j];
+        n1 = nrm2(m, r1);
+        n2 = nrm2(n, r2);
+        rel_error[i] = hypot(n1, n2) / (s * sqrt(2.0));
+      }
+    }
+    free(r1); free(r2);
+  }
+  free(bu.V); free(bu.buf); free(bu.hvec); free(bu.cvec);
+done:
+  free(op.w); free(lam); free(sig); free(perm); free(X);
   return st;
 }
 

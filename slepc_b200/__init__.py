@@ -21,11 +21,14 @@ LIB_PATH = os.path.join(_HERE, "libslepc_b200.so")
 LARGEST_MAGNITUDE, SMALLEST_MAGNITUDE, LARGEST_REAL, SMALLEST_REAL = 1, 2, 3, 4
 # EPSConvergedReason
 CONVERGED_TOL, CONVERGED_ITERATING, DIVERGED_ITS, DIVERGED_BREAKDOWN = 1, 0, -1, -2
-# EPSErrorType
-ERROR_ABSOLUTE, ERROR_RELATIVE = 0, 1
+# EPSErrorType / SVDErrorType
+ERROR_ABSOLUTE, ERROR_RELATIVE, ERROR_NORM = 0, 1, 2
+# MatScalar storage of matrix values
+SCALAR_F64, SCALAR_F32 = 0, 1
 
 _STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "LAPACK error", 4: "invalid inner product",
-           5: "breakdown", 6: "out of device memory", 7: "wrong call order", 8: "device-side error"}
+           5: "breakdown", 6: "out of device memory", 7: "wrong call order", 8: "device-side error",
+           9: "floating-point error"}
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -57,6 +60,32 @@ _SIGS = {
     "b200_mat_get_lanes": (ctypes.c_int, [_vp, _ip]),
     "b200_mat_set_spmv_schedule": (ctypes.c_int, [_vp, ctypes.c_int]),
     "b200_mat_destroy": (ctypes.c_int, [_vp]),
+    "b200_mat_create_aij": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int64, _ip, _ip, _vp, ctypes.c_int,
+                                           _vp, _vp]),
+    "b200_mat_create_cross": (ctypes.c_int, [_vp, _vp]),
+    "b200_mat_mult_transpose": (ctypes.c_int, [_vp, _vp, _vp]),
+    "b200_mat_get_sizes": (ctypes.c_int, [_vp, _ip, _ip]),
+    "b200_mat_norm_inf": (ctypes.c_int, [_vp, _dp]),
+    "b200_svd_create": (ctypes.c_int, [_vp, _vp]),
+    "b200_svd_destroy": (ctypes.c_int, [_vp]),
+    "b200_svd_set_operator": (ctypes.c_int, [_vp, _vp]),
+    "b200_svd_set_dimensions": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "b200_svd_set_tolerances": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int]),
+    "b200_svd_set_which_singular_triplets": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_svd_set_initial_space": (ctypes.c_int, [_vp, _dp]),
+    "b200_svd_set_timing": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_svd_solve": (ctypes.c_int, [_vp]),
+    "b200_svd_get_converged": (ctypes.c_int, [_vp, _ip]),
+    "b200_svd_get_iteration_number": (ctypes.c_int, [_vp, _ip]),
+    "b200_svd_get_converged_reason": (ctypes.c_int, [_vp, _ip]),
+    "b200_svd_get_singular_triplet": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp, _dp]),
+    "b200_svd_get_singular_vectors_device": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                                            ctypes.POINTER(ctypes.c_void_p)]),
+    "b200_svd_compute_error": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _dp]),
+    "b200_svd_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(EPSStats)]),
+    "b200_svd_solve_aij_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int64, _ip, _ip, _vp,
+                                               ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                               ctypes.c_int, _dp, _dp, _dp, _dp, _ip, _vp]),
     "b200_csr_spmv": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
     "b200_bv_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "b200_bv_destroy": (ctypes.c_int, [_vp]),
@@ -150,23 +179,63 @@ def kernel_launch_count():
 
 
 class Mat:
-    """CSR matrix resident in HBM (the new Mat SpMV type)."""
+    """CSR matrix resident in HBM (the new Mat SpMV type), or the cross shell A^T A."""
 
     def __init__(self):
         self.handle = ctypes.c_void_p()
+        self.m = 0
         self.n = 0
         self.nnz = 0
+        self._base = None
 
-    def createAIJ(self, csr, stream=None):
+    def createAIJ(self, csr, size=None, dtype=None, stream=None):
+        """Square FP64 CSR (size None, dtype None), or a general m x n matrix
+        (size=(m, n)) with values stored as float64 or float32 (dtype); the
+        general form also keeps the explicit transpose in HBM."""
         rowptr, colind, vals = csr
         rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
         colind = np.ascontiguousarray(colind, dtype=np.int32)
-        vals = np.ascontiguousarray(vals, dtype=np.float64)
-        n = len(rowptr) - 1
-        _check(lib().b200_mat_create_csr(n, int(rowptr[-1]), _i(rowptr), _i(colind), _d(vals), stream,
-                                         ctypes.byref(self.handle)))
-        self.n, self.nnz = n, int(rowptr[-1])
+        m = len(rowptr) - 1
+        nnz = int(rowptr[-1])
+        if size is None and dtype is None:
+            vals = np.ascontiguousarray(vals, dtype=np.float64)
+            _check(lib().b200_mat_create_csr(m, nnz, _i(rowptr), _i(colind), _d(vals), stream,
+                                             ctypes.byref(self.handle)))
+            self.m = self.n = m
+        else:
+            m, n = size if size is not None else (m, m)
+            dt = np.dtype(dtype or np.float64)
+            if dt not in (np.dtype(np.float32), np.dtype(np.float64)):
+                raise B200Error(1, "values must be float32 or float64")
+            vals = np.ascontiguousarray(vals, dtype=dt)
+            st = SCALAR_F32 if dt == np.float32 else SCALAR_F64
+            _check(lib().b200_mat_create_aij(m, n, nnz, _i(rowptr), _i(colind), vals.ctypes.data, st, stream,
+                                             ctypes.byref(self.handle)))
+            self.m, self.n = m, n
+        self.nnz = nnz
         return self
+
+    def createCross(self, A):
+        """The shell A^T A (MatMult_Cross); A must outlive it."""
+        _check(lib().b200_mat_create_cross(A.handle, ctypes.byref(self.handle)))
+        self.m = self.n = A.n
+        self.nnz = A.nnz
+        self._base = A
+        return self
+
+    def getSizes(self):
+        m, n = ctypes.c_int(), ctypes.c_int()
+        _check(lib().b200_mat_get_sizes(self.handle, ctypes.byref(m), ctypes.byref(n)))
+        return m.value, n.value
+
+    def multTranspose(self, x_ptr, y_ptr):
+        _check(lib().b200_mat_mult_transpose(self.handle, x_ptr, y_ptr))
+
+    def norm(self):
+        """MatNorm(NORM_INFINITY)."""
+        v = ctypes.c_double()
+        _check(lib().b200_mat_norm_inf(self.handle, ctypes.byref(v)))
+        return v.value
 
     def createAIJDevice(self, n, nnz, rowptr_ptr, colind_ptr, vals_ptr, stream=None):
         _check(lib().b200_mat_create_csr_device(n, nnz, rowptr_ptr, colind_ptr, vals_ptr, stream,
@@ -478,3 +547,124 @@ def solve_csr_host(csr, v0, nev, ncv, tol=1e-8, which=LARGEST_MAGNITUDE, mpd=0, 
     return {"evals": evals[:nconv].copy(), "X": X[:nconv].T.copy() if want_vectors else None,
             "errest": errest[:nconv].copy(), "nconv": nconv, "its": int(info[1]), "reason": int(info[2]),
             "lanczos_steps": int(info[3]), "restarts": int(info[4])}
+
+
+class SVD:
+    """SVD cross solver (SVDCROSS): Krylov-Schur on A^T A."""
+
+    class Which:
+        LARGEST, SMALLEST = 0, 1
+
+    class ErrorType:
+        ABSOLUTE, RELATIVE, NORM = 0, 1, 2
+
+    def __init__(self):
+        self.handle = ctypes.c_void_p()
+        self._A = None
+
+    def create(self, stream=None):
+        _check(lib().b200_svd_create(stream, ctypes.byref(self.handle)))
+        return self
+
+    def setOperators(self, A, B=None):
+        if B is not None:
+            raise B200Error(1, "only standard problems (B = None) are supported")
+        self._A = A
+        _check(lib().b200_svd_set_operator(self.handle, A.handle))
+
+    def setDimensions(self, nsv=1, ncv=0, mpd=0):
+        _check(lib().b200_svd_set_dimensions(self.handle, nsv, ncv or 0, mpd or 0))
+
+    def setTolerances(self, tol=0.0, max_it=0):
+        _check(lib().b200_svd_set_tolerances(self.handle, tol or 0.0, max_it or 0))
+
+    def setWhichSingularTriplets(self, which):
+        _check(lib().b200_svd_set_which_singular_triplets(self.handle, which))
+
+    def setInitialSpace(self, v0):
+        v0 = np.ascontiguousarray(v0, dtype=np.float64)
+        _check(lib().b200_svd_set_initial_space(self.handle, _d(v0)))
+
+    def setTiming(self, on):
+        _check(lib().b200_svd_set_timing(self.handle, 1 if on else 0))
+
+    def solve(self):
+        _check(lib().b200_svd_solve(self.handle))
+
+    def getConverged(self):
+        v = ctypes.c_int()
+        _check(lib().b200_svd_get_converged(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def getIterationNumber(self):
+        v = ctypes.c_int()
+        _check(lib().b200_svd_get_iteration_number(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def getConvergedReason(self):
+        v = ctypes.c_int()
+        _check(lib().b200_svd_get_converged_reason(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def getValue(self, i):
+        s = ctypes.c_double()
+        _check(lib().b200_svd_get_singular_triplet(self.handle, i, ctypes.byref(s), None, None))
+        return s.value
+
+    def getSingularTriplet(self, i):
+        """(sigma, u, v) with u of length m and v of length n."""
+        s = ctypes.c_double()
+        u = np.empty(self._A.m)
+        v = np.empty(self._A.n)
+        _check(lib().b200_svd_get_singular_triplet(self.handle, i, ctypes.byref(s), _d(u), _d(v)))
+        return s.value, u, v
+
+    def getVectorPointers(self, i):
+        u, v = ctypes.c_void_p(), ctypes.c_void_p()
+        _check(lib().b200_svd_get_singular_vectors_device(self.handle, i, ctypes.byref(u), ctypes.byref(v)))
+        return u.value, v.value
+
+    def computeError(self, i, etype=ERROR_RELATIVE):
+        v = ctypes.c_double()
+        _check(lib().b200_svd_compute_error(self.handle, i, etype, ctypes.byref(v)))
+        return v.value
+
+    def getStats(self):
+        st = EPSStats()
+        _check(lib().b200_svd_get_stats(self.handle, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in EPSStats._fields_}
+
+    def destroy(self):
+        if self.handle:
+            lib().b200_svd_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def svd_solve_aij_host(csr, size, v0, nsv, ncv, tol=0.0, max_it=0, dtype=np.float64, want_vectors=True,
+                       stream=None):
+    """One call from host CSR arrays to host singular triplets (b200_svd_solve_aij_host)."""
+    m, n = size
+    rowptr = np.ascontiguousarray(csr[0], dtype=np.int32)
+    colind = np.ascontiguousarray(csr[1], dtype=np.int32)
+    dt = np.dtype(dtype)
+    vals = np.ascontiguousarray(csr[2], dtype=dt)
+    st = SCALAR_F32 if dt == np.float32 else SCALAR_F64
+    v0 = np.ascontiguousarray(v0, dtype=np.float64)
+    sig = np.zeros(ncv + 1)
+    err = np.zeros(ncv + 1)
+    U = np.zeros((ncv + 1, m)) if want_vectors else None
+    V = np.zeros((ncv + 1, n)) if want_vectors else None
+    info = np.zeros(8, dtype=np.int32)
+    _check(lib().b200_svd_solve_aij_host(m, n, int(rowptr[-1]), _i(rowptr), _i(colind), vals.ctypes.data, st, _d(v0),
+                                         nsv, ncv, tol, max_it, _d(sig), _d(U) if want_vectors else None,
+                                         _d(V) if want_vectors else None, _d(err), _i(info), stream))
+    k = int(info[0])
+    return {"sigma": sig[:k].copy(), "U": U[:k].T.copy() if want_vectors else None,
+            "V": V[:k].T.copy() if want_vectors else None, "rel_error": err[:k].copy(), "nconv": k,
+            "its": int(info[1]), "reason": int(info[2]), "lanczos_steps": int(info[3]), "restarts": int(info[4])}

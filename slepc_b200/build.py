@@ -43,6 +43,18 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+GEN_SRC = os.path.join(HERE, "gen_powerlaw.c")
+GEN_LIB = os.path.join(HERE, "libgen_powerlaw.so")
+
+
+def build_generator(force=False):
+    """Host-side generator of the power-law test matrix (gcc + OpenMP)."""
+    if force or _stale(GEN_LIB, [GEN_SRC]):
+        subprocess.check_call(["gcc", "-O2", "-fopenmp", "-fPIC", "-shared", "-std=c11", "-Wall", GEN_SRC, "-o",
+                               GEN_LIB, "-lm"])
+    return GEN_LIB
+
+
 def build(force=False, verbose=False):
     os.makedirs(BUILD, exist_ok=True)
     headers = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
@@ -67,3 +79,4 @@ def build(force=False, verbose=False):
 
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    print(build_generator(force="--force" in sys.argv))

@@ -166,6 +166,24 @@ __global__ void sumsq_partial_kernel(const double *__restrict__ x, long long len
   }
 }
 
+__global__ void diff_sumsq_partial_kernel(const double *__restrict__ y, const double *__restrict__ x, double alpha,
+                                          long long len, double *partial) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x) {
+    const double r = y[i] - alpha * x[i];
+    acc = fma(r, r, acc);
+  }
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    partial[blockIdx.x] = s;
+  }
+}
+
 __global__ void sum_final_kernel(const double *__restrict__ partial, int nblocks, double *out) {
   __shared__ double red[32];
   double acc = 0.0;
@@ -337,6 +355,17 @@ cudaError_t sumsq_launch(const double *x, long long len, double *out, double *wo
   int blocks = (int)grid_for(len, 256);
   if (blocks > work_len) blocks = work_len;
   sumsq_partial_kernel<<<blocks, 256, 0, stream>>>(x, len, work);
+  count_launch();
+  sum_final_kernel<<<1, 256, 0, stream>>>(work, blocks, out);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t diff_sumsq_launch(const double *y, const double *x, double alpha, long long len, double *out, double *work,
+                              int work_len, cudaStream_t stream) {
+  int blocks = (int)grid_for(len, 256);
+  if (blocks > work_len) blocks = work_len;
+  diff_sumsq_partial_kernel<<<blocks, 256, 0, stream>>>(y, x, alpha, len, work);
   count_launch();
   sum_final_kernel<<<1, 256, 0, stream>>>(work, blocks, out);
   count_launch();

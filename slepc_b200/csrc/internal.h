@@ -1,0 +1,13 @@
+// Entry points shared between the object layer (lib.cu) and the SVD solver (svd.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "slepc_b200.h"
+
+namespace b200 {
+// The cross shell of A: A^T A, or A A^T when swapped (the m < n case, which
+// SVDSetUp handles by exchanging A and A^T, src/svd/interface/svdsetup.c:300-314).
+b200_status mat_create_cross_ex(b200_mat A, bool swapped, b200_mat *C);
+// y = A x, or y = A^T x (transpose; matrices from b200_mat_create_aij), on the given stream.
+cudaError_t mat_apply(b200_mat A, const double *x, double *y, cudaStream_t stream, bool transpose);
+}  // namespace b200

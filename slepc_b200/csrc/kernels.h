@@ -36,14 +36,25 @@ uint64_t launch_count();
 constexpr int kTileNnz = 4096;   // nonzeros staged per CTA of the row-block SpMV
 constexpr int kTileRows = 1024;  // rows per CTA of the row-block SpMV
 int spmv_choose_lanes(int n, int64_t nnz);
-constexpr int kWarpTileNnz = 256;  // nonzeros staged per warp tile of the warp-tile SpMV
+constexpr int kWarpTileNnz = 256;   // nonzeros staged per warp tile of the warp-tile SpMV
+constexpr int kSegmentNnz = 4096;   // nonzeros per segment of a row longer than a warp tile
 // Row blocks for the row-block SpMV: block b covers rows [b[i], b[i+1]).
 std::vector<int> spmv_row_blocks(int n, const int *rowptr_host);
-// Warp tiles (<= 32 rows, <= kWarpTileNnz nonzeros) for the warp-tile SpMV.
-std::vector<int> spmv_warp_tiles(int n, const int *rowptr_host);
-cudaError_t spmv_warptile_launch(int ntiles, const int *tiles, const int *rowptr, const int *colind,
-                                 const double *vals, const double *x, double *y, cudaStream_t stream,
-                                 const GsState *st = nullptr, int step = 0);
+// Warp tiles for the warp-tile SpMV: {r0, r1, 0, 0} for up to 32 short rows, or a segment
+// {row, -(slot+1), p_begin, p_end} of a long row; longrows = {row, first slot, slot count}.
+struct WarpTiles {
+  std::vector<int4> tiles;
+  std::vector<int3> longrows;
+  int nslots = 0;
+};
+WarpTiles spmv_warp_tiles(int n, const int *rowptr_host);
+cudaError_t spmv_warptile_launch(int ntiles, const int4 *tiles, int nlong, const int3 *longrows, double *partials,
+                                 const int *rowptr, const int *colind, const double *vals, const double *x, double *y,
+                                 cudaStream_t stream, const GsState *st = nullptr, int step = 0);
+// Same with FP32 stored values (products and sums in FP64).
+cudaError_t spmv_warptile_launch_f32(int ntiles, const int4 *tiles, int nlong, const int3 *longrows, double *partials,
+                                     const int *rowptr, const int *colind, const float *vals, const double *x,
+                                     double *y, cudaStream_t stream, const GsState *st = nullptr, int step = 0);
 // st/step: when st is given, the launch is skipped on the device if a
 // Lanczos run halted (breakdown) at an earlier step.
 cudaError_t spmv_rowblock_launch(int nblocks, const int *blocks, const int *rowptr, const int *colind,
@@ -102,6 +113,9 @@ cudaError_t scale_launch(double *x, long long len, double alpha, cudaStream_t st
 cudaError_t copy_launch(double *dst, const double *src, long long len, cudaStream_t stream);
 // Sum of squares of x (len) into out[0] (device), deterministic two-level reduction.
 cudaError_t sumsq_launch(const double *x, long long len, double *out, double *work, int work_len, cudaStream_t stream);
+// out[0] = ||y - alpha x||^2, deterministic two-level reduction.
+cudaError_t diff_sumsq_launch(const double *y, const double *x, double alpha, long long len, double *out, double *work,
+                              int work_len, cudaStream_t stream);
 // out[0] = ||A x - lambda x||^2 (fused SpMV + residual), deterministic.
 cudaError_t residual_launch(int n, const int *rowptr, const int *colind, const double *vals, const double *x,
                             double lambda, double *out, double *work, int work_len, int lanes, cudaStream_t stream);

@@ -20,6 +20,7 @@
 
 #include "common.h"
 #include "ds_hep.h"
+#include "internal.h"
 #include "kernels.h"
 
 using namespace b200;
@@ -54,59 +55,164 @@ int num_sms_host() {
   } while (0)
 
 // ------------------------------------------------------------------ Mat ---
-struct b200_mat_s {
-  int n = 0;
+// One CSR operand in HBM with its SpMV schedules.  Values are FP64, or FP32
+// (B200_SCALAR_F32: half the value traffic; products and sums stay FP64).
+struct CsrPart {
+  int rows = 0, cols = 0;
   int64_t nnz = 0;
   int *rowptr = nullptr, *colind = nullptr;
-  double *vals = nullptr;
+  void *vals = nullptr;
+  bool f32 = false;
   int lanes = 8;
-  int *blocks = nullptr;  // row blocks of the row-block SpMV (nblocks + 1 entries)
+  int *blocks = nullptr;       // row blocks of the row-block SpMV (nblocks + 1 entries), FP64 only
   int nblocks = 0;
-  int *tiles = nullptr;   // warp tiles of the warp-tile SpMV (ntiles + 1 entries)
+  int4 *tiles = nullptr;       // warp tiles and long-row segments of the warp-tile SpMV
   int ntiles = 0;
+  int3 *longrows = nullptr;    // rows longer than a warp tile: {row, first slot, slot count}
+  int nlong = 0;
+  double *partials = nullptr;  // one slot per long-row segment
+};
+
+enum MatKind { kMatCsr = 0, kMatCross = 1 };
+
+// kMatCsr: the matrix A (m x n) with, for a rectangular AIJ matrix, its explicit
+// transpose.  kMatCross: the shell C = A^T A (n x n) of MatMult_Cross
+// (src/svd/impls/cross/cross.c:31-41) over a kMatCsr matrix it does not own.
+struct b200_mat_s {
+  int kind = kMatCsr;
+  int m = 0, n = 0;          // rows and columns of the operator
+  int64_t nnz = 0;
+  CsrPart a;                 // A
+  CsrPart at;                // A^T (rectangular AIJ matrices; rows == 0 otherwise)
+  b200_mat base = nullptr;   // kMatCross: the matrix A of A^T A
+  bool swapped = false;      // kMatCross: the operator is A A^T (SVDSetUp's swap for m < n)
+  double *work = nullptr;    // kMatCross: w = A x (base->m entries; base->n when swapped)
+  double norm_inf = -1.0;    // max_i sum_j |a_ij| when known (computed from the host arrays)
   int schedule = B200_SPMV_WARPTILE;
   cudaStream_t stream = nullptr;
 };
 
-// Row blocks and warp tiles from a host copy of rowptr, uploaded to the device.
-static b200_status mat_set_blocks(b200_mat M, const int *rowptr_host) {
-  std::vector<int> b = spmv_row_blocks(M->n, rowptr_host);
-  std::vector<int> t = spmv_warp_tiles(M->n, rowptr_host);
-  M->nblocks = (int)b.size() - 1;
-  M->ntiles = (int)t.size() - 1;
-  B200_CUDA_CHECK(cudaMalloc(&M->blocks, sizeof(int) * b.size()));
-  B200_CUDA_CHECK(cudaMalloc(&M->tiles, sizeof(int) * t.size()));
-  B200_CUDA_CHECK(cudaMemcpyAsync(M->blocks, b.data(), sizeof(int) * b.size(), cudaMemcpyHostToDevice, M->stream));
-  B200_CUDA_CHECK(cudaMemcpyAsync(M->tiles, t.data(), sizeof(int) * t.size(), cudaMemcpyHostToDevice, M->stream));
-  B200_CUDA_CHECK(cudaStreamSynchronize(M->stream));
-  return B200_OK;
+static void part_free(CsrPart &P) {
+  cudaFree(P.rowptr);
+  cudaFree(P.colind);
+  cudaFree(P.vals);
+  cudaFree(P.blocks);
+  cudaFree(P.tiles);
+  cudaFree(P.longrows);
+  cudaFree(P.partials);
+  P = CsrPart{};
 }
 
-static cudaError_t mat_spmv(b200_mat A, const double *x, double *y, cudaStream_t stream, const GsState *st = nullptr,
-                            int step = 0) {
-  if (A->schedule == B200_SPMV_ROWBLOCK)
-    return spmv_rowblock_launch(A->nblocks, A->blocks, A->rowptr, A->colind, A->vals, x, y, stream, st, step);
-  return spmv_warptile_launch(A->ntiles, A->tiles, A->rowptr, A->colind, A->vals, x, y, stream, st, step);
-}
-
-static b200_status mat_alloc(int n, int64_t nnz, cudaStream_t stream, b200_mat *A) {
-  b200_mat M = new b200_mat_s;
-  M->n = n;
-  M->nnz = nnz;
-  M->stream = stream;
-  M->lanes = spmv_choose_lanes(n, nnz);
-  if (cudaMalloc(&M->rowptr, sizeof(int) * ((size_t)n + 1)) != cudaSuccess ||
-      cudaMalloc(&M->colind, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)) != cudaSuccess ||
-      cudaMalloc(&M->vals, sizeof(double) * (size_t)(nnz > 0 ? nnz : 1)) != cudaSuccess) {
-    cudaFree(M->rowptr);
-    cudaFree(M->colind);
-    cudaFree(M->vals);
-    delete M;
+static b200_status part_alloc(CsrPart &P, int rows, int cols, int64_t nnz, bool f32) {
+  P.rows = rows;
+  P.cols = cols;
+  P.nnz = nnz;
+  P.f32 = f32;
+  P.lanes = spmv_choose_lanes(rows, nnz);
+  const size_t vsz = f32 ? sizeof(float) : sizeof(double);
+  if (cudaMalloc(&P.rowptr, sizeof(int) * ((size_t)rows + 1)) != cudaSuccess ||
+      cudaMalloc(&P.colind, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)) != cudaSuccess ||
+      cudaMalloc(&P.vals, vsz * (size_t)(nnz > 0 ? nnz : 1)) != cudaSuccess) {
+    part_free(P);
     b200_set_last_error(__FILE__, __LINE__, "cudaMalloc failed for the CSR arrays");
     return B200_ERR_NOMEM;
   }
-  *A = M;
   return B200_OK;
+}
+
+static b200_status part_upload(CsrPart &P, const int *rowptr, const int *colind, const void *vals, cudaMemcpyKind kind,
+                               cudaStream_t s) {
+  const size_t vsz = P.f32 ? sizeof(float) : sizeof(double);
+  cudaError_t e = cudaMemcpyAsync(P.rowptr, rowptr, sizeof(int) * ((size_t)P.rows + 1), kind, s);
+  if (e == cudaSuccess && P.nnz) e = cudaMemcpyAsync(P.colind, colind, sizeof(int) * (size_t)P.nnz, kind, s);
+  if (e == cudaSuccess && P.nnz) e = cudaMemcpyAsync(P.vals, vals, vsz * (size_t)P.nnz, kind, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    b200_set_last_error(__FILE__, __LINE__, cudaGetErrorString(e));
+    return B200_ERR_CUDA;
+  }
+  return B200_OK;
+}
+
+// Row blocks (FP64 only) and warp tiles from a host copy of rowptr, uploaded to the device.
+static b200_status part_set_schedules(CsrPart &P, const int *rowptr_host, cudaStream_t s) {
+  if (!P.f32) {
+    std::vector<int> b = spmv_row_blocks(P.rows, rowptr_host);
+    P.nblocks = (int)b.size() - 1;
+    B200_CUDA_CHECK(cudaMalloc(&P.blocks, sizeof(int) * b.size()));
+    B200_CUDA_CHECK(cudaMemcpyAsync(P.blocks, b.data(), sizeof(int) * b.size(), cudaMemcpyHostToDevice, s));
+  }
+  WarpTiles wt = spmv_warp_tiles(P.rows, rowptr_host);
+  P.ntiles = (int)wt.tiles.size();
+  P.nlong = (int)wt.longrows.size();
+  B200_CUDA_CHECK(cudaMalloc(&P.tiles, sizeof(int4) * (wt.tiles.empty() ? 1 : wt.tiles.size())));
+  if (P.ntiles)
+    B200_CUDA_CHECK(
+        cudaMemcpyAsync(P.tiles, wt.tiles.data(), sizeof(int4) * wt.tiles.size(), cudaMemcpyHostToDevice, s));
+  if (P.nlong) {
+    B200_CUDA_CHECK(cudaMalloc(&P.longrows, sizeof(int3) * wt.longrows.size()));
+    B200_CUDA_CHECK(cudaMalloc(&P.partials, sizeof(double) * (size_t)wt.nslots));
+    B200_CUDA_CHECK(cudaMemcpyAsync(P.longrows, wt.longrows.data(), sizeof(int3) * wt.longrows.size(),
+                                    cudaMemcpyHostToDevice, s));
+  }
+  B200_CUDA_CHECK(cudaStreamSynchronize(s));
+  return B200_OK;
+}
+
+static cudaError_t part_spmv(const CsrPart &P, int schedule, const double *x, double *y, cudaStream_t stream,
+                             const GsState *st, int step) {
+  if (P.f32)
+    return spmv_warptile_launch_f32(P.ntiles, P.tiles, P.nlong, P.longrows, P.partials, P.rowptr, P.colind,
+                                    static_cast<const float *>(P.vals), x, y, stream, st, step);
+  if (schedule == B200_SPMV_ROWBLOCK)
+    return spmv_rowblock_launch(P.nblocks, P.blocks, P.rowptr, P.colind, static_cast<const double *>(P.vals), x, y,
+                                stream, st, step);
+  return spmv_warptile_launch(P.ntiles, P.tiles, P.nlong, P.longrows, P.partials, P.rowptr, P.colind,
+                              static_cast<const double *>(P.vals), x, y, stream, st, step);
+}
+
+// y = Op x for the operator of A (the EPS operator: A itself, or A^T A).
+static cudaError_t mat_spmv(b200_mat A, const double *x, double *y, cudaStream_t stream, const GsState *st = nullptr,
+                            int step = 0) {
+  if (A->kind == kMatCross) {
+    const CsrPart &first = A->swapped ? A->base->at : A->base->a;
+    const CsrPart &second = A->swapped ? A->base->a : A->base->at;
+    cudaError_t e = part_spmv(first, A->base->schedule, x, A->work, stream, st, step);
+    if (e != cudaSuccess) return e;
+    return part_spmv(second, A->base->schedule, A->work, y, stream, st, step);
+  }
+  return part_spmv(A->a, A->schedule, x, y, stream, st, step);
+}
+
+// Explicit transpose on the host, each row of A^T in ascending row order of A
+// (the layout MatTranspose_SeqAIJ produces, so a row of A^T is summed in that order).
+template <typename VT>
+static void csr_transpose_host(int rows, int cols, const int *rowptr, const int *colind, const VT *vals,
+                               std::vector<int> &rp, std::vector<int> &ci, std::vector<VT> &va) {
+  const int64_t nnz = rowptr[rows];
+  rp.assign((size_t)cols + 1, 0);
+  ci.resize((size_t)nnz);
+  va.resize((size_t)nnz);
+  for (int64_t p = 0; p < nnz; ++p) rp[(size_t)colind[p] + 1]++;
+  for (int c = 0; c < cols; ++c) rp[(size_t)c + 1] += rp[c];
+  std::vector<int> next(rp.begin(), rp.end() - 1);
+  for (int i = 0; i < rows; ++i)
+    for (int p = rowptr[i]; p < rowptr[i + 1]; ++p) {
+      const int q = next[colind[p]]++;
+      ci[q] = i;
+      va[q] = vals[p];
+    }
+}
+
+template <typename VT>
+static double csr_norm_inf_host(int rows, const int *rowptr, const VT *vals) {
+  double nrm = 0.0;
+  for (int i = 0; i < rows; ++i) {
+    double sacc = 0.0;
+    for (int p = rowptr[i]; p < rowptr[i + 1]; ++p) sacc += std::fabs((double)vals[p]);
+    if (sacc > nrm) nrm = sacc;
+  }
+  return nrm;
 }
 
 extern "C" b200_status b200_mat_create_csr(int n, int64_t nnz, const int *rowptr, const int *colind, const double *vals,
@@ -114,24 +220,19 @@ extern "C" b200_status b200_mat_create_csr(int n, int64_t nnz, const int *rowptr
   B200_ARG_CHECK(A && n > 0 && nnz >= 0 && rowptr && (nnz == 0 || (colind && vals)), "invalid CSR arguments");
   B200_ARG_CHECK(rowptr[0] == 0 && rowptr[n] == nnz, "rowptr must start at 0 and end at nnz");
   B200_ARG_CHECK(nnz <= 0x7fffffff, "nnz must fit a 32-bit index (PETSc default int size)");
-  b200_mat M;
-  B200_CHECK(mat_alloc(n, nnz, (cudaStream_t)stream, &M));
   cudaStream_t s = (cudaStream_t)stream;
-  cudaError_t e = cudaMemcpyAsync(M->rowptr, rowptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess && nnz)
-    e = cudaMemcpyAsync(M->colind, colind, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(M->vals, vals, sizeof(double) * (size_t)nnz, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) {
-    b200_mat_destroy(M);
-    b200_set_last_error(__FILE__, __LINE__, cudaGetErrorString(e));
-    return B200_ERR_CUDA;
-  }
-  b200_status st = mat_set_blocks(M, rowptr);
+  b200_mat M = new b200_mat_s;
+  M->m = M->n = n;
+  M->nnz = nnz;
+  M->stream = s;
+  b200_status st = part_alloc(M->a, n, n, nnz, false);
+  if (st == B200_OK) st = part_upload(M->a, rowptr, colind, vals, cudaMemcpyHostToDevice, s);
+  if (st == B200_OK) st = part_set_schedules(M->a, rowptr, s);
   if (st != B200_OK) {
     b200_mat_destroy(M);
     return st;
   }
+  M->norm_inf = csr_norm_inf_host(n, rowptr, vals);
   *A = M;
   return B200_OK;
 }
@@ -140,29 +241,18 @@ extern "C" b200_status b200_mat_create_csr_device(int n, int64_t nnz, const int 
                                                   const double *vals, void *stream, b200_mat *A) {
   B200_ARG_CHECK(A && n > 0 && nnz >= 0 && rowptr && (nnz == 0 || (colind && vals)), "invalid CSR arguments");
   B200_ARG_CHECK(nnz <= 0x7fffffff, "nnz must fit a 32-bit index");
-  b200_mat M;
-  B200_CHECK(mat_alloc(n, nnz, (cudaStream_t)stream, &M));
   cudaStream_t s = (cudaStream_t)stream;
-  cudaError_t e = cudaMemcpyAsync(M->rowptr, rowptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyDeviceToDevice, s);
-  if (e == cudaSuccess && nnz)
-    e = cudaMemcpyAsync(M->colind, colind, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToDevice, s);
-  if (e == cudaSuccess && nnz)
-    e = cudaMemcpyAsync(M->vals, vals, sizeof(double) * (size_t)nnz, cudaMemcpyDeviceToDevice, s);
   std::vector<int> hrow((size_t)n + 1);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(hrow.data(), rowptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) {
-    b200_mat_destroy(M);
-    b200_set_last_error(__FILE__, __LINE__, cudaGetErrorString(e));
-    return B200_ERR_CUDA;
-  }
-  if (hrow[0] != 0 || hrow[n] != nnz) {
-    b200_mat_destroy(M);
-    b200_set_last_error(__FILE__, __LINE__, "rowptr must start at 0 and end at nnz");
-    return B200_ERR_ARG;
-  }
-  b200_status st = mat_set_blocks(M, hrow.data());
+  B200_CUDA_CHECK(cudaMemcpyAsync(hrow.data(), rowptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyDeviceToHost, s));
+  B200_CUDA_CHECK(cudaStreamSynchronize(s));
+  B200_ARG_CHECK(hrow[0] == 0 && hrow[n] == nnz, "rowptr must start at 0 and end at nnz");
+  b200_mat M = new b200_mat_s;
+  M->m = M->n = n;
+  M->nnz = nnz;
+  M->stream = s;
+  b200_status st = part_alloc(M->a, n, n, nnz, false);
+  if (st == B200_OK) st = part_upload(M->a, rowptr, colind, vals, cudaMemcpyDeviceToDevice, s);
+  if (st == B200_OK) st = part_set_schedules(M->a, hrow.data(), s);
   if (st != B200_OK) {
     b200_mat_destroy(M);
     return st;
@@ -171,9 +261,85 @@ extern "C" b200_status b200_mat_create_csr_device(int n, int64_t nnz, const int 
   return B200_OK;
 }
 
+template <typename VT>
+static b200_status mat_create_aij(int m, int n, int64_t nnz, const int *rowptr, const int *colind, const VT *vals,
+                                  cudaStream_t s, b200_mat *A) {
+  for (int64_t p = 0; p < nnz; ++p)
+    B200_ARG_CHECK(colind[p] >= 0 && colind[p] < n, "column index out of range");
+  for (int i = 0; i < m; ++i) B200_ARG_CHECK(rowptr[i] <= rowptr[i + 1], "rowptr must be nondecreasing");
+  const bool f32 = sizeof(VT) == sizeof(float);
+  std::vector<int> rp, ci;
+  std::vector<VT> va;
+  csr_transpose_host(m, n, rowptr, colind, vals, rp, ci, va);
+  b200_mat M = new b200_mat_s;
+  M->m = m;
+  M->n = n;
+  M->nnz = nnz;
+  M->stream = s;
+  b200_status st = part_alloc(M->a, m, n, nnz, f32);
+  if (st == B200_OK) st = part_upload(M->a, rowptr, colind, vals, cudaMemcpyHostToDevice, s);
+  if (st == B200_OK) st = part_set_schedules(M->a, rowptr, s);
+  if (st == B200_OK) st = part_alloc(M->at, n, m, nnz, f32);
+  if (st == B200_OK) st = part_upload(M->at, rp.data(), ci.data(), va.data(), cudaMemcpyHostToDevice, s);
+  if (st == B200_OK) st = part_set_schedules(M->at, rp.data(), s);
+  if (st != B200_OK) {
+    b200_mat_destroy(M);
+    return st;
+  }
+  M->norm_inf = csr_norm_inf_host(m, rowptr, vals);
+  *A = M;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_mat_create_aij(int m, int n, int64_t nnz, const int *rowptr, const int *colind,
+                                           const void *vals, int scalar_type, void *stream, b200_mat *A) {
+  B200_ARG_CHECK(A && m > 0 && n > 0 && nnz >= 0 && rowptr && (nnz == 0 || (colind && vals)), "invalid CSR arguments");
+  B200_ARG_CHECK(rowptr[0] == 0 && rowptr[m] == nnz, "rowptr must start at 0 and end at nnz");
+  B200_ARG_CHECK(nnz <= 0x7fffffff, "nnz must fit a 32-bit index (PETSc default int size)");
+  B200_ARG_CHECK(scalar_type == B200_SCALAR_F64 || scalar_type == B200_SCALAR_F32, "unknown scalar type");
+  if (scalar_type == B200_SCALAR_F32)
+    return mat_create_aij(m, n, nnz, rowptr, colind, static_cast<const float *>(vals), (cudaStream_t)stream, A);
+  return mat_create_aij(m, n, nnz, rowptr, colind, static_cast<const double *>(vals), (cudaStream_t)stream, A);
+}
+
+namespace b200 {
+b200_status mat_create_cross_ex(b200_mat A, bool swapped, b200_mat *C) {
+  B200_ARG_CHECK(A && C && A->kind == kMatCsr && A->at.rows == A->n, "A must be a matrix from b200_mat_create_aij");
+  b200_mat M = new b200_mat_s;
+  M->kind = kMatCross;
+  M->swapped = swapped;
+  M->m = M->n = swapped ? A->m : A->n;
+  M->nnz = A->nnz;
+  M->base = A;
+  M->stream = A->stream;
+  const int wlen = swapped ? A->n : A->m;
+  if (cudaMalloc(&M->work, sizeof(double) * (size_t)wlen) != cudaSuccess) {
+    delete M;
+    b200_set_last_error(__FILE__, __LINE__, "cudaMalloc failed for the cross-product work vector");
+    return B200_ERR_NOMEM;
+  }
+  *C = M;
+  return B200_OK;
+}
+
+cudaError_t mat_apply(b200_mat A, const double *x, double *y, cudaStream_t stream, bool transpose) {
+  if (!transpose) return mat_spmv(A, x, y, stream);
+  return part_spmv(A->at, A->schedule, x, y, stream, nullptr, 0);
+}
+}  // namespace b200
+
+extern "C" b200_status b200_mat_create_cross(b200_mat A, b200_mat *C) { return mat_create_cross_ex(A, false, C); }
+
 extern "C" b200_status b200_mat_mult(b200_mat A, const double *x, double *y) {
   B200_ARG_CHECK(A && x && y, "null argument");
   B200_CUDA_CHECK(mat_spmv(A, x, y, A->stream));
+  return B200_OK;
+}
+
+extern "C" b200_status b200_mat_mult_transpose(b200_mat A, const double *x, double *y) {
+  B200_ARG_CHECK(A && x && y, "null argument");
+  B200_ARG_CHECK(A->kind == kMatCsr && A->at.rows == A->n, "only a rectangular AIJ matrix stores its transpose");
+  B200_CUDA_CHECK(part_spmv(A->at, A->schedule, x, y, A->stream, nullptr, 0));
   return B200_OK;
 }
 
@@ -184,25 +350,39 @@ extern "C" b200_status b200_mat_get_size(b200_mat A, int *n, int64_t *nnz) {
   return B200_OK;
 }
 
+extern "C" b200_status b200_mat_get_sizes(b200_mat A, int *m, int *n) {
+  B200_ARG_CHECK(A, "null matrix");
+  if (m) *m = A->m;
+  if (n) *n = A->n;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_mat_norm_inf(b200_mat A, double *nrm) {
+  B200_ARG_CHECK(A && nrm, "null argument");
+  B200_ARG_CHECK(A->norm_inf >= 0.0, "the infinity norm is known only for matrices created from host arrays");
+  *nrm = A->norm_inf;
+  return B200_OK;
+}
+
 extern "C" b200_status b200_mat_set_spmv_schedule(b200_mat A, int schedule) {
   B200_ARG_CHECK(A && (schedule == B200_SPMV_ROWBLOCK || schedule == B200_SPMV_WARPTILE), "unknown SpMV schedule");
+  B200_ARG_CHECK(schedule == B200_SPMV_WARPTILE || (A->kind == kMatCsr && !A->a.f32),
+                 "the row-block schedule is available for FP64 CSR matrices only");
   A->schedule = schedule;
   return B200_OK;
 }
 
 extern "C" b200_status b200_mat_get_lanes(b200_mat A, int *lanes) {
   B200_ARG_CHECK(A && lanes, "null argument");
-  *lanes = A->lanes;
+  *lanes = A->kind == kMatCross ? A->base->a.lanes : A->a.lanes;
   return B200_OK;
 }
 
 extern "C" b200_status b200_mat_destroy(b200_mat A) {
   if (!A) return B200_OK;
-  cudaFree(A->rowptr);
-  cudaFree(A->colind);
-  cudaFree(A->vals);
-  cudaFree(A->blocks);
-  cudaFree(A->tiles);
+  part_free(A->a);
+  part_free(A->at);
+  cudaFree(A->work);
   delete A;
   return B200_OK;
 }
@@ -732,6 +912,7 @@ struct b200_eps_s {
   int n_ = 0, ncv_ = 0, mpd_ = 0, max_it_ = 0;
   double tol_ = 1e-8;
   double *resid_buf = nullptr;
+  double *op_buf = nullptr;  // Op x for residuals of operators without a fused residual kernel
 };
 
 extern "C" b200_status b200_eps_create(void *stream, b200_eps *eps) {
@@ -746,12 +927,16 @@ extern "C" b200_status b200_eps_destroy(b200_eps eps) {
   if (!eps) return B200_OK;
   b200_bv_destroy(eps->V);
   cudaFree(eps->resid_buf);
+  cudaFree(eps->op_buf);
   delete eps;
   return B200_OK;
 }
 
 extern "C" b200_status b200_eps_set_operators(b200_eps eps, b200_mat A) {
   B200_ARG_CHECK(eps && A, "null argument");
+  B200_ARG_CHECK(A->m == A->n, "the operator of an eigenproblem must be square");
+  cudaFree(eps->op_buf);
+  eps->op_buf = nullptr;
   eps->A = A;
   eps->solved = false;
   return B200_OK;
@@ -1087,9 +1272,15 @@ extern "C" b200_status b200_eps_compute_error(b200_eps eps, int i, int type, dou
   b200_bv V = eps->V;
   // ||A x - lambda x||_2, with the shift skipped for |lambda| <= eps (epssolve.c:689-694)
   const double shift = (std::fabs(lam) > 2.220446049250313e-16) ? lam : 0.0;
-  B200_CUDA_CHECK(
-      residual_launch(A->n, A->rowptr, A->colind, A->vals, col(V, p), shift, eps->resid_buf, V->red, V->red_len, A->lanes,
-                      V->stream));
+  if (A->kind == kMatCsr && !A->a.f32) {
+    B200_CUDA_CHECK(residual_launch(A->n, A->a.rowptr, A->a.colind, static_cast<const double *>(A->a.vals), col(V, p),
+                                    shift, eps->resid_buf, V->red, V->red_len, A->a.lanes, V->stream));
+  } else {
+    if (!eps->op_buf) B200_CUDA_CHECK(cudaMalloc(&eps->op_buf, sizeof(double) * (size_t)A->n));
+    B200_CUDA_CHECK(mat_spmv(A, col(V, p), eps->op_buf, V->stream));
+    B200_CUDA_CHECK(diff_sumsq_launch(eps->op_buf, col(V, p), shift, A->n, eps->resid_buf, V->red, V->red_len,
+                                      V->stream));
+  }
   B200_CUDA_CHECK(cudaMemcpyAsync(V->hpin, eps->resid_buf, sizeof(double), cudaMemcpyDeviceToHost, V->stream));
   B200_CUDA_CHECK(cudaStreamSynchronize(V->stream));
   double r = std::sqrt(V->hpin[0]);

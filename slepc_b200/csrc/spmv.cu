@@ -86,16 +86,22 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_rowblock_kernel(const int *
   }
 }
 
-// Warp tiles: a tile is <= 32 rows and <= kWarpTileNnz nonzeros (a longer row is a tile of
-// its own).  Lane i of the owning warp streams nonzeros i, i+32, ... (kWarpTileNnz/32 value,
-// index and x loads in flight per lane), keeps the rounded products in warp-private shared
-// memory, and after a __syncwarp sums row i of the tile in index order.  No CTA barrier.
-__global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles, const int *__restrict__ tiles,
+// Warp tiles.  A tile {r0, r1, -, -} is <= 32 rows and <= kWarpTileNnz nonzeros; lane i of the
+// owning warp streams nonzeros i, i+32, ... (kWarpTileNnz/32 value, index and x loads in flight
+// per lane), keeps the rounded products in warp-private shared memory, and after a __syncwarp
+// sums row i of the tile in index order (the order of a sequential CSR loop).  A row with
+// more than kWarpTileNnz nonzeros becomes segment tiles {row, -(slot+1), p_begin, p_end} of at
+// most kSegmentNnz nonzeros each; a segment's warp writes its partial sum (fixed-order warp
+// tree) to partials[slot], and spmv_fixup_kernel adds a long row's partials in slot order.
+// VT is the stored value type (double, or float for FP32 storage); products and sums are FP64.
+template <typename VT>
+__global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles, const int4 *__restrict__ tiles,
                                                                      const int *__restrict__ rowptr,
                                                                      const int *__restrict__ colind,
-                                                                     const double *__restrict__ vals,
+                                                                     const VT *__restrict__ vals,
                                                                      const double *__restrict__ x,
                                                                      double *__restrict__ y,
+                                                                     double *__restrict__ partials,
                                                                      const GsState *__restrict__ st, int step) {
   if (st && st->halt && st->halt_step < step) return;
   __shared__ double prod_all[kSpmvThreads / 32][kWarpTileNnz];
@@ -103,7 +109,17 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles,
   double *prod = prod_all[wib];
   const int nwarps = gridDim.x * (kSpmvThreads / 32);
   for (int t = blockIdx.x * (kSpmvThreads / 32) + wib; t < ntiles; t += nwarps) {
-    const int r0 = __ldg(tiles + t), r1 = __ldg(tiles + t + 1);
+    const int4 tile = tiles[t];
+    if (tile.y < 0) {
+      // segment of a long row
+      double sacc = 0.0;
+      for (int p = tile.z + lane; p < tile.w; p += 32)
+        sacc = __dadd_rn(sacc, __dmul_rn((double)__ldcs(vals + p), __ldg(x + __ldcs(colind + p))));
+      sacc = warp_sum(sacc);
+      if (lane == 0) partials[-tile.y - 1] = sacc;
+      continue;
+    }
+    const int r0 = tile.x, r1 = tile.y;
     const int nrows = r1 - r0;  // 1..32
     const int myrow_start = (lane < nrows) ? __ldg(rowptr + r0 + lane) : 0;
     const int p0 = __shfl_sync(0xffffffffu, myrow_start, 0);
@@ -111,21 +127,12 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles,
     const int next = __shfl_down_sync(0xffffffffu, myrow_start, 1);
     const int myrow_end = (lane + 1 < nrows) ? next : p1;
     const int cnt = p1 - p0;
-    if (cnt > kWarpTileNnz) {
-      // one long row: strided partial sums, fixed-order warp tree
-      double sacc = 0.0;
-      for (int p = p0 + lane; p < p1; p += 32)
-        sacc = __dadd_rn(sacc, __dmul_rn(__ldcs(vals + p), __ldg(x + __ldcs(colind + p))));
-      sacc = warp_sum(sacc);
-      if (lane == 0) y[r0] = sacc;
-      continue;
-    }
     double a[kWarpTileNnz / 32];
     int c[kWarpTileNnz / 32];
 #pragma unroll
     for (int u = 0; u < kWarpTileNnz / 32; ++u) {
       const int q = lane + 32 * u;
-      a[u] = (q < cnt) ? __ldcs(vals + p0 + q) : 0.0;
+      a[u] = (q < cnt) ? (double)__ldcs(vals + p0 + q) : 0.0;
       c[u] = (q < cnt) ? __ldcs(colind + p0 + q) : 0;
     }
 #pragma unroll
@@ -141,6 +148,18 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles,
     }
     __syncwarp();
   }
+}
+
+// y[row] of every long row = sum of its segment partials in slot order.  longrows[i] = {row, first, count}.
+__global__ void spmv_fixup_kernel(int nlong, const int3 *__restrict__ longrows, const double *__restrict__ partials,
+                                  double *__restrict__ y, const GsState *__restrict__ st, int step) {
+  if (st && st->halt && st->halt_step < step) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nlong) return;
+  const int3 lr = longrows[i];
+  double sacc = 0.0;
+  for (int k = 0; k < lr.z; ++k) sacc += partials[lr.y + k];
+  y[lr.x] = sacc;
 }
 
 template <int LPR>
@@ -196,24 +215,36 @@ std::vector<int> spmv_row_blocks(int n, const int *rowptr) {
   return b;
 }
 
-std::vector<int> spmv_warp_tiles(int n, const int *rowptr) {
-  std::vector<int> b;
-  b.reserve(n / 16 + 2);
+WarpTiles spmv_warp_tiles(int n, const int *rowptr) {
+  WarpTiles wt;
+  wt.tiles.reserve(n / 16 + 2);
   int r = 0;
-  b.push_back(0);
   while (r < n) {
     const int start = r;
     const int base = rowptr[start];
     while (r < n && r - start < 32 && rowptr[r + 1] - base <= kWarpTileNnz) ++r;
-    if (r == start) ++r;  // a single row longer than the tile: a tile of its own
-    b.push_back(r);
+    if (r > start) {
+      wt.tiles.push_back({start, r, 0, 0});
+      continue;
+    }
+    // a single row longer than a tile: segments of kSegmentNnz nonzeros
+    const int p0 = rowptr[r], p1 = rowptr[r + 1];
+    const int first = wt.nslots;
+    for (int p = p0; p < p1; p += kSegmentNnz) {
+      const int pe = (p1 - p > kSegmentNnz) ? p + kSegmentNnz : p1;
+      wt.tiles.push_back({r, -(wt.nslots + 1), p, pe});
+      ++wt.nslots;
+    }
+    wt.longrows.push_back({r, first, wt.nslots - first});
+    ++r;
   }
-  return b;
+  return wt;
 }
 
-cudaError_t spmv_warptile_launch(int ntiles, const int *tiles, const int *rowptr, const int *colind,
-                                 const double *vals, const double *x, double *y, cudaStream_t stream,
-                                 const GsState *st, int step) {
+template <typename VT>
+cudaError_t spmv_warptile_launch_t(int ntiles, const int4 *tiles, int nlong, const int3 *longrows, double *partials,
+                                   const int *rowptr, const int *colind, const VT *vals, const double *x, double *y,
+                                   cudaStream_t stream, const GsState *st, int step) {
   if (ntiles <= 0) return cudaSuccess;
   static int sms = 0;
   if (!sms) {
@@ -226,9 +257,28 @@ cudaError_t spmv_warptile_launch(int ntiles, const int *tiles, const int *rowptr
   int grid = (ntiles + warps_per_cta - 1) / warps_per_cta;
   const int cap = sms * 8;  // persistent: 8 CTAs (64 warps) per SM
   if (grid > cap) grid = cap;
-  spmv_warptile_kernel<<<grid, kSpmvThreads, 0, stream>>>(ntiles, tiles, rowptr, colind, vals, x, y, st, step);
+  spmv_warptile_kernel<VT><<<grid, kSpmvThreads, 0, stream>>>(ntiles, tiles, rowptr, colind, vals, x, y, partials, st,
+                                                              step);
   count_launch();
+  if (nlong > 0) {
+    spmv_fixup_kernel<<<(nlong + 127) / 128, 128, 0, stream>>>(nlong, longrows, partials, y, st, step);
+    count_launch();
+  }
   return cudaGetLastError();
+}
+
+cudaError_t spmv_warptile_launch(int ntiles, const int4 *tiles, int nlong, const int3 *longrows, double *partials,
+                                 const int *rowptr, const int *colind, const double *vals, const double *x, double *y,
+                                 cudaStream_t stream, const GsState *st, int step) {
+  return spmv_warptile_launch_t<double>(ntiles, tiles, nlong, longrows, partials, rowptr, colind, vals, x, y, stream,
+                                        st, step);
+}
+
+cudaError_t spmv_warptile_launch_f32(int ntiles, const int4 *tiles, int nlong, const int3 *longrows, double *partials,
+                                     const int *rowptr, const int *colind, const float *vals, const double *x,
+                                     double *y, cudaStream_t stream, const GsState *st, int step) {
+  return spmv_warptile_launch_t<float>(ntiles, tiles, nlong, longrows, partials, rowptr, colind, vals, x, y, stream,
+                                       st, step);
 }
 
 cudaError_t spmv_rowblock_launch(int nblocks, const int *blocks, const int *rowptr, const int *colind,

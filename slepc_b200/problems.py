@@ -121,3 +121,89 @@ def to_scipy(csr, n=None):
     rowptr, colind, vals = csr
     n = len(rowptr) - 1 if n is None else n
     return sp.csr_matrix((vals, colind, rowptr), shape=(n, n))
+
+
+# ---------------------------------------------------------------- power-law rectangular matrix
+_gen = None
+
+
+def _genlib():
+    global _gen
+    if _gen is None:
+        import ctypes
+
+        from . import build as _b
+
+        L = ctypes.CDLL(_b.build_generator())
+        L.gen_powerlaw.restype = ctypes.c_int
+        L.gen_powerlaw.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_uint64,
+                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.gen_uniform.restype = ctypes.c_double
+        L.gen_uniform.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_int64, ctypes.c_int64]
+        L.gen_normal.restype = ctypes.c_double
+        L.gen_normal.argtypes = [ctypes.c_uint64, ctypes.c_int64, ctypes.c_int64]
+        _gen = L
+    return _gen
+
+
+def powerlaw_rect(m, n, nnz_row=20, alpha=1.8, seed=0):
+    """m x n CSR matrix with nnz_row distinct columns per row drawn from a power
+    law with exponent alpha in the column index (few columns appear in almost
+    every row) and N(0,1) values stored as float32: (rowptr, colind, vals)."""
+    k = min(nnz_row, n)
+    rowptr = np.empty(m + 1, dtype=np.int32)
+    colind = np.empty(m * k, dtype=np.int32)
+    vals = np.empty(m * k, dtype=np.float32)
+    st = _genlib().gen_powerlaw(m, n, nnz_row, float(alpha), seed, rowptr.ctypes.data, colind.ctypes.data,
+                                vals.ctypes.data)
+    if st:
+        raise ValueError("invalid power-law matrix parameters")
+    return rowptr, colind, vals
+
+
+def _mix(z):
+    M = (1 << 64) - 1
+    z = (z + 0x9E3779B97F4A7C15) & M
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
+    return z ^ (z >> 31)
+
+
+def powerlaw_rect_py(m, n, nnz_row=20, alpha=1.8, seed=0):
+    """Pure-Python restatement of powerlaw_rect for small sizes (checks the C generator)."""
+    import math
+
+    M = (1 << 64) - 1
+
+    def bits(stream, row, t):
+        return _mix(_mix((seed * 4 + stream) & M) ^ ((row << 24) ^ t))
+
+    def uniform(stream, row, t):
+        return (bits(stream, row, t) >> 11) * (1.0 / 9007199254740992.0)
+
+    k = min(nnz_row, n)
+    a1 = alpha - 1.0
+    tail = 1.0 - math.pow(n + 1.0, -a1)
+    rowptr = np.arange(m + 1, dtype=np.int32) * k
+    colind = np.empty(m * k, dtype=np.int32)
+    vals = np.empty(m * k, dtype=np.float32)
+    for i in range(m):
+        cols = []
+        t = 0
+        while len(cols) < k and t < (1 << 24):
+            x = math.pow(1.0 - uniform(0, i, t) * tail, -1.0 / a1)
+            c = min(max(int(math.floor(x)) - 1, 0), n - 1)
+            if c not in cols:
+                cols.append(c)
+            t += 1
+        c = 0
+        while len(cols) < k and c < n:
+            if c not in cols:
+                cols.append(c)
+            c += 1
+        colind[i * k:(i + 1) * k] = sorted(cols)
+        for j in range(k):
+            u1 = ((bits(1, i, 2 * j) >> 11) + 1.0) * (1.0 / 9007199254740992.0)
+            u2 = uniform(1, i, 2 * j + 1)
+            vals[i * k + j] = np.float32(math.sqrt(-2.0 * math.log(u1)) * math.cos(6.283185307179586 * u2))
+    return rowptr, colind, vals

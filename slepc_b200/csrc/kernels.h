@@ -37,24 +37,35 @@ constexpr int kTileNnz = 4096;   // nonzeros staged per CTA of the row-block SpM
 constexpr int kTileRows = 1024;  // rows per CTA of the row-block SpMV
 int spmv_choose_lanes(int n, int64_t nnz);
 constexpr int kWarpTileNnz = 256;   // nonzeros staged per warp tile of the warp-tile SpMV
-constexpr int kSegmentNnz = 4096;   // nonzeros per segment of a row longer than a warp tile
+constexpr int kSegmentNnz = 1024;   // nonzeros per segment of a row longer than a warp tile
 // Row blocks for the row-block SpMV: block b covers rows [b[i], b[i+1]).
 std::vector<int> spmv_row_blocks(int n, const int *rowptr_host);
-// Warp tiles for the warp-tile SpMV: {r0, r1, 0, 0} for up to 32 short rows, or a segment
-// {row, -(slot+1), p_begin, p_end} of a long row; longrows = {row, first slot, slot count}.
+// Warp tiles for the warp-tile SpMV: {r0, r1} for up to 32 short rows; a row longer than
+// kWarpTileNnz becomes segments {p_begin, p_end} of at most kSegmentNnz nonzeros, and
+// longrows = {row, first segment, segment count}.
 struct WarpTiles {
-  std::vector<int4> tiles;
+  std::vector<int2> tiles;
+  std::vector<int2> segs;
   std::vector<int3> longrows;
-  int nslots = 0;
 };
 WarpTiles spmv_warp_tiles(int n, const int *rowptr_host);
-cudaError_t spmv_warptile_launch(int ntiles, const int4 *tiles, int nlong, const int3 *longrows, double *partials,
-                                 const int *rowptr, const int *colind, const double *vals, const double *x, double *y,
-                                 cudaStream_t stream, const GsState *st = nullptr, int step = 0);
+// Device copies of a WarpTiles plan plus one partial-sum slot per segment.
+struct SpmvTiles {
+  int2 *tiles = nullptr;
+  int ntiles = 0;
+  int2 *segs = nullptr;
+  int nsegs = 0;
+  int3 *longrows = nullptr;
+  int nlong = 0;
+  double *partials = nullptr;
+};
+cudaError_t spmv_warptile_launch(const SpmvTiles &T, const int *rowptr, const int *colind, const double *vals,
+                                 const double *x, double *y, cudaStream_t stream, const GsState *st = nullptr,
+                                 int step = 0);
 // Same with FP32 stored values (products and sums in FP64).
-cudaError_t spmv_warptile_launch_f32(int ntiles, const int4 *tiles, int nlong, const int3 *longrows, double *partials,
-                                     const int *rowptr, const int *colind, const float *vals, const double *x,
-                                     double *y, cudaStream_t stream, const GsState *st = nullptr, int step = 0);
+cudaError_t spmv_warptile_launch_f32(const SpmvTiles &T, const int *rowptr, const int *colind, const float *vals,
+                                     const double *x, double *y, cudaStream_t stream, const GsState *st = nullptr,
+                                     int step = 0);
 // st/step: when st is given, the launch is skipped on the device if a
 // Lanczos run halted (breakdown) at an earlier step.
 cudaError_t spmv_rowblock_launch(int nblocks, const int *blocks, const int *rowptr, const int *colind,
@@ -95,6 +106,12 @@ cudaError_t gs_orthogonalize_launch(const GsPassArgs &a, const GsWork &w, cudaSt
 cudaError_t gs_state_reset(const GsWork &w, double eta, cudaStream_t stream);
 // Plain dots q = V(:,0:jb)^T w (no decision), result in w.cnew.
 cudaError_t gs_dot_launch(const GsPassArgs &a, const GsWork &w, cudaStream_t stream);
+
+// Explicit transpose of a device CSR matrix (transpose.cu): rowptr_t (cols+1), colind_t and
+// vals_t (nnz) in HBM, each row of A^T in ascending row order of A.  Synchronises the stream.
+cudaError_t csr_transpose_device(int rows, int cols, long long nnz, const int *rowptr, const int *colind,
+                                 const void *vals, bool f32, int *rowptr_t, int *colind_t, void *vals_t,
+                                 cudaStream_t s);
 
 // ---- Dense tall-skinny operations (bvops.cu)
 // V(:,s:e) = V(:,l:k) * Q(l:k,s:e), row-blocked, in place; Q points at element (l,s).

@@ -66,11 +66,7 @@ struct CsrPart {
   int lanes = 8;
   int *blocks = nullptr;       // row blocks of the row-block SpMV (nblocks + 1 entries), FP64 only
   int nblocks = 0;
-  int4 *tiles = nullptr;       // warp tiles and long-row segments of the warp-tile SpMV
-  int ntiles = 0;
-  int3 *longrows = nullptr;    // rows longer than a warp tile: {row, first slot, slot count}
-  int nlong = 0;
-  double *partials = nullptr;  // one slot per long-row segment
+  SpmvTiles wt;                // warp tiles, long-row segments and their partial-sum slots
 };
 
 enum MatKind { kMatCsr = 0, kMatCross = 1 };
@@ -97,9 +93,10 @@ static void part_free(CsrPart &P) {
   cudaFree(P.colind);
   cudaFree(P.vals);
   cudaFree(P.blocks);
-  cudaFree(P.tiles);
-  cudaFree(P.longrows);
-  cudaFree(P.partials);
+  cudaFree(P.wt.tiles);
+  cudaFree(P.wt.segs);
+  cudaFree(P.wt.longrows);
+  cudaFree(P.wt.partials);
   P = CsrPart{};
 }
 
@@ -143,16 +140,21 @@ static b200_status part_set_schedules(CsrPart &P, const int *rowptr_host, cudaSt
     B200_CUDA_CHECK(cudaMemcpyAsync(P.blocks, b.data(), sizeof(int) * b.size(), cudaMemcpyHostToDevice, s));
   }
   WarpTiles wt = spmv_warp_tiles(P.rows, rowptr_host);
-  P.ntiles = (int)wt.tiles.size();
-  P.nlong = (int)wt.longrows.size();
-  B200_CUDA_CHECK(cudaMalloc(&P.tiles, sizeof(int4) * (wt.tiles.empty() ? 1 : wt.tiles.size())));
-  if (P.ntiles)
+  P.wt.ntiles = (int)wt.tiles.size();
+  P.wt.nsegs = (int)wt.segs.size();
+  P.wt.nlong = (int)wt.longrows.size();
+  if (P.wt.ntiles) {
+    B200_CUDA_CHECK(cudaMalloc(&P.wt.tiles, sizeof(int2) * wt.tiles.size()));
     B200_CUDA_CHECK(
-        cudaMemcpyAsync(P.tiles, wt.tiles.data(), sizeof(int4) * wt.tiles.size(), cudaMemcpyHostToDevice, s));
-  if (P.nlong) {
-    B200_CUDA_CHECK(cudaMalloc(&P.longrows, sizeof(int3) * wt.longrows.size()));
-    B200_CUDA_CHECK(cudaMalloc(&P.partials, sizeof(double) * (size_t)wt.nslots));
-    B200_CUDA_CHECK(cudaMemcpyAsync(P.longrows, wt.longrows.data(), sizeof(int3) * wt.longrows.size(),
+        cudaMemcpyAsync(P.wt.tiles, wt.tiles.data(), sizeof(int2) * wt.tiles.size(), cudaMemcpyHostToDevice, s));
+  }
+  if (P.wt.nsegs) {
+    B200_CUDA_CHECK(cudaMalloc(&P.wt.segs, sizeof(int2) * wt.segs.size()));
+    B200_CUDA_CHECK(cudaMalloc(&P.wt.partials, sizeof(double) * wt.segs.size()));
+    B200_CUDA_CHECK(cudaMalloc(&P.wt.longrows, sizeof(int3) * wt.longrows.size()));
+    B200_CUDA_CHECK(
+        cudaMemcpyAsync(P.wt.segs, wt.segs.data(), sizeof(int2) * wt.segs.size(), cudaMemcpyHostToDevice, s));
+    B200_CUDA_CHECK(cudaMemcpyAsync(P.wt.longrows, wt.longrows.data(), sizeof(int3) * wt.longrows.size(),
                                     cudaMemcpyHostToDevice, s));
   }
   B200_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -162,13 +164,12 @@ static b200_status part_set_schedules(CsrPart &P, const int *rowptr_host, cudaSt
 static cudaError_t part_spmv(const CsrPart &P, int schedule, const double *x, double *y, cudaStream_t stream,
                              const GsState *st, int step) {
   if (P.f32)
-    return spmv_warptile_launch_f32(P.ntiles, P.tiles, P.nlong, P.longrows, P.partials, P.rowptr, P.colind,
-                                    static_cast<const float *>(P.vals), x, y, stream, st, step);
+    return spmv_warptile_launch_f32(P.wt, P.rowptr, P.colind, static_cast<const float *>(P.vals), x, y, stream, st,
+                                    step);
   if (schedule == B200_SPMV_ROWBLOCK)
     return spmv_rowblock_launch(P.nblocks, P.blocks, P.rowptr, P.colind, static_cast<const double *>(P.vals), x, y,
                                 stream, st, step);
-  return spmv_warptile_launch(P.ntiles, P.tiles, P.nlong, P.longrows, P.partials, P.rowptr, P.colind,
-                              static_cast<const double *>(P.vals), x, y, stream, st, step);
+  return spmv_warptile_launch(P.wt, P.rowptr, P.colind, static_cast<const double *>(P.vals), x, y, stream, st, step);
 }
 
 // y = Op x for the operator of A (the EPS operator: A itself, or A^T A).
@@ -182,26 +183,6 @@ static cudaError_t mat_spmv(b200_mat A, const double *x, double *y, cudaStream_t
     return part_spmv(second, A->base->schedule, A->work, y, stream, st, step);
   }
   return part_spmv(A->a, A->schedule, x, y, stream, st, step);
-}
-
-// Explicit transpose on the host, each row of A^T in ascending row order of A
-// (the layout MatTranspose_SeqAIJ produces, so a row of A^T is summed in that order).
-template <typename VT>
-static void csr_transpose_host(int rows, int cols, const int *rowptr, const int *colind, const VT *vals,
-                               std::vector<int> &rp, std::vector<int> &ci, std::vector<VT> &va) {
-  const int64_t nnz = rowptr[rows];
-  rp.assign((size_t)cols + 1, 0);
-  ci.resize((size_t)nnz);
-  va.resize((size_t)nnz);
-  for (int64_t p = 0; p < nnz; ++p) rp[(size_t)colind[p] + 1]++;
-  for (int c = 0; c < cols; ++c) rp[(size_t)c + 1] += rp[c];
-  std::vector<int> next(rp.begin(), rp.end() - 1);
-  for (int i = 0; i < rows; ++i)
-    for (int p = rowptr[i]; p < rowptr[i + 1]; ++p) {
-      const int q = next[colind[p]]++;
-      ci[q] = i;
-      va[q] = vals[p];
-    }
 }
 
 template <typename VT>
@@ -268,9 +249,6 @@ static b200_status mat_create_aij(int m, int n, int64_t nnz, const int *rowptr, 
     B200_ARG_CHECK(colind[p] >= 0 && colind[p] < n, "column index out of range");
   for (int i = 0; i < m; ++i) B200_ARG_CHECK(rowptr[i] <= rowptr[i + 1], "rowptr must be nondecreasing");
   const bool f32 = sizeof(VT) == sizeof(float);
-  std::vector<int> rp, ci;
-  std::vector<VT> va;
-  csr_transpose_host(m, n, rowptr, colind, vals, rp, ci, va);
   b200_mat M = new b200_mat_s;
   M->m = m;
   M->n = n;
@@ -279,8 +257,21 @@ static b200_status mat_create_aij(int m, int n, int64_t nnz, const int *rowptr, 
   b200_status st = part_alloc(M->a, m, n, nnz, f32);
   if (st == B200_OK) st = part_upload(M->a, rowptr, colind, vals, cudaMemcpyHostToDevice, s);
   if (st == B200_OK) st = part_set_schedules(M->a, rowptr, s);
+  // the explicit transpose, built in HBM from the uploaded A
   if (st == B200_OK) st = part_alloc(M->at, n, m, nnz, f32);
-  if (st == B200_OK) st = part_upload(M->at, rp.data(), ci.data(), va.data(), cudaMemcpyHostToDevice, s);
+  std::vector<int> rp;
+  if (st == B200_OK) {
+    cudaError_t e = csr_transpose_device(m, n, nnz, M->a.rowptr, M->a.colind, M->a.vals, f32, M->at.rowptr,
+                                         M->at.colind, M->at.vals, s);
+    rp.resize((size_t)n + 1);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(rp.data(), M->at.rowptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      b200_set_last_error(__FILE__, __LINE__, cudaGetErrorString(e));
+      st = e == cudaErrorMemoryAllocation ? B200_ERR_NOMEM : B200_ERR_CUDA;
+    }
+  }
   if (st == B200_OK) st = part_set_schedules(M->at, rp.data(), s);
   if (st != B200_OK) {
     b200_mat_destroy(M);

@@ -86,22 +86,19 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_rowblock_kernel(const int *
   }
 }
 
-// Warp tiles.  A tile {r0, r1, -, -} is <= 32 rows and <= kWarpTileNnz nonzeros; lane i of the
-// owning warp streams nonzeros i, i+32, ... (kWarpTileNnz/32 value, index and x loads in flight
-// per lane), keeps the rounded products in warp-private shared memory, and after a __syncwarp
-// sums row i of the tile in index order (the order of a sequential CSR loop).  A row with
-// more than kWarpTileNnz nonzeros becomes segment tiles {row, -(slot+1), p_begin, p_end} of at
-// most kSegmentNnz nonzeros each; a segment's warp writes its partial sum (fixed-order warp
-// tree) to partials[slot], and spmv_fixup_kernel adds a long row's partials in slot order.
+// Warp tiles.  A tile {r0, r1} is <= 32 rows and <= kWarpTileNnz nonzeros; lane i of the owning
+// warp streams nonzeros i, i+32, ... (kWarpTileNnz/32 value, index and x loads in flight per
+// lane), keeps the rounded products in warp-private shared memory, and after a __syncwarp sums
+// row i of the tile in index order (the order of a sequential CSR loop).  Full occupancy (2048
+// threads per SM): the short loads of many warps hide the gather latency.
 // VT is the stored value type (double, or float for FP32 storage); products and sums are FP64.
 template <typename VT>
-__global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles, const int4 *__restrict__ tiles,
+__global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles, const int2 *__restrict__ tiles,
                                                                      const int *__restrict__ rowptr,
                                                                      const int *__restrict__ colind,
                                                                      const VT *__restrict__ vals,
                                                                      const double *__restrict__ x,
                                                                      double *__restrict__ y,
-                                                                     double *__restrict__ partials,
                                                                      const GsState *__restrict__ st, int step) {
   if (st && st->halt && st->halt_step < step) return;
   __shared__ double prod_all[kSpmvThreads / 32][kWarpTileNnz];
@@ -109,16 +106,7 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles,
   double *prod = prod_all[wib];
   const int nwarps = gridDim.x * (kSpmvThreads / 32);
   for (int t = blockIdx.x * (kSpmvThreads / 32) + wib; t < ntiles; t += nwarps) {
-    const int4 tile = tiles[t];
-    if (tile.y < 0) {
-      // segment of a long row
-      double sacc = 0.0;
-      for (int p = tile.z + lane; p < tile.w; p += 32)
-        sacc = __dadd_rn(sacc, __dmul_rn((double)__ldcs(vals + p), __ldg(x + __ldcs(colind + p))));
-      sacc = warp_sum(sacc);
-      if (lane == 0) partials[-tile.y - 1] = sacc;
-      continue;
-    }
+    const int2 tile = tiles[t];
     const int r0 = tile.x, r1 = tile.y;
     const int nrows = r1 - r0;  // 1..32
     const int myrow_start = (lane < nrows) ? __ldg(rowptr + r0 + lane) : 0;
@@ -127,18 +115,18 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles,
     const int next = __shfl_down_sync(0xffffffffu, myrow_start, 1);
     const int myrow_end = (lane + 1 < nrows) ? next : p1;
     const int cnt = p1 - p0;
-    double a[kWarpTileNnz / 32];
+    VT a[kWarpTileNnz / 32];  // kept in the stored type until the multiply (fewer registers for FP32)
     int c[kWarpTileNnz / 32];
 #pragma unroll
     for (int u = 0; u < kWarpTileNnz / 32; ++u) {
       const int q = lane + 32 * u;
-      a[u] = (q < cnt) ? (double)__ldcs(vals + p0 + q) : 0.0;
+      a[u] = (q < cnt) ? __ldcs(vals + p0 + q) : VT(0);
       c[u] = (q < cnt) ? __ldcs(colind + p0 + q) : 0;
     }
 #pragma unroll
     for (int u = 0; u < kWarpTileNnz / 32; ++u) {
       const int q = lane + 32 * u;
-      if (q < cnt) prod[q] = __dmul_rn(a[u], __ldg(x + c[u]));
+      if (q < cnt) prod[q] = __dmul_rn((double)a[u], __ldg(x + c[u]));
     }
     __syncwarp();
     if (lane < nrows) {
@@ -150,16 +138,82 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles,
   }
 }
 
-// y[row] of every long row = sum of its segment partials in slot order.  longrows[i] = {row, first, count}.
-__global__ void spmv_fixup_kernel(int nlong, const int3 *__restrict__ longrows, const double *__restrict__ partials,
-                                  double *__restrict__ y, const GsState *__restrict__ st, int step) {
+// Segments of rows longer than a warp tile: segs[s] = {p_begin, p_end} (at most kSegmentNnz
+// nonzeros).  A warp streams its segment in chunks of kWarpTileNnz nonzeros with 8 independent
+// value/index loads and then 8 x gathers in flight per lane, adds each lane's products in a
+// fixed order, reduces the warp with a fixed shuffle tree and writes partials[s].  Half
+// occupancy buys the registers for the loads in flight; long dense-like rows (the power-law
+// columns of a transposed matrix) stream at full width.
+template <typename VT>
+__global__ void __launch_bounds__(kSpmvThreads, sizeof(VT) == 4 ? 4 : 3) spmv_segment_kernel(int nsegs, const int2 *__restrict__ segs,
+                                                                       const int *__restrict__ colind,
+                                                                       const VT *__restrict__ vals,
+                                                                       const double *__restrict__ x,
+                                                                       double *__restrict__ partials,
+                                                                       const GsState *__restrict__ st, int step) {
   if (st && st->halt && st->halt_step < step) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = gridDim.x * (kSpmvThreads / 32);
+  for (int sg = blockIdx.x * (kSpmvThreads / 32) + (threadIdx.x >> 5); sg < nsegs; sg += nwarps) {
+    const int2 seg = segs[sg];
+    constexpr int U = kWarpTileNnz / 32;
+    double sacc = 0.0;
+    const int nfull = (seg.y - seg.x) / kWarpTileNnz;
+    VT a[U];
+    int c[U];
+    if (nfull > 0) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        a[u] = __ldcs(vals + seg.x + lane + 32 * u);
+        c[u] = __ldcs(colind + seg.x + lane + 32 * u);
+      }
+    }
+    // software pipeline: the values and indices of chunk k+1 are in flight while chunk k gathers x
+    for (int k = 0; k < nfull; ++k) {
+      double xv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) xv[u] = __ldg(x + c[u]);
+      VT an[U];
+      int cn[U];
+      if (k + 1 < nfull) {
+        const int pn = seg.x + (k + 1) * kWarpTileNnz + lane;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          an[u] = __ldcs(vals + pn + 32 * u);
+          cn[u] = __ldcs(colind + pn + 32 * u);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) sacc = __dadd_rn(sacc, __dmul_rn((double)a[u], xv[u]));
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        a[u] = an[u];
+        c[u] = cn[u];
+      }
+    }
+    const int p = seg.x + nfull * kWarpTileNnz;
+    for (int q = p + lane; q < seg.y; q += 32)
+      sacc = __dadd_rn(sacc, __dmul_rn((double)__ldcs(vals + q), __ldg(x + __ldcs(colind + q))));
+    sacc = warp_sum(sacc);
+    if (lane == 0) partials[sg] = sacc;
+  }
+}
+
+// y[row] of every long row from its segment partials: one warp per row, lane l adds partials
+// l, l+32, ... in order, then a fixed shuffle tree.  longrows[i] = {row, first slot, slot count}.
+__global__ void __launch_bounds__(256) spmv_fixup_kernel(int nlong, const int3 *__restrict__ longrows,
+                                                         const double *__restrict__ partials,
+                                                         double *__restrict__ y, const GsState *__restrict__ st,
+                                                         int step) {
+  if (st && st->halt && st->halt_step < step) return;
+  const int lane = threadIdx.x & 31;
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= nlong) return;
   const int3 lr = longrows[i];
   double sacc = 0.0;
-  for (int k = 0; k < lr.z; ++k) sacc += partials[lr.y + k];
-  y[lr.x] = sacc;
+  for (int k = lane; k < lr.z; k += 32) sacc += partials[lr.y + k];
+  sacc = warp_sum(sacc);
+  if (lane == 0) y[lr.x] = sacc;
 }
 
 template <int LPR>
@@ -224,61 +278,64 @@ WarpTiles spmv_warp_tiles(int n, const int *rowptr) {
     const int base = rowptr[start];
     while (r < n && r - start < 32 && rowptr[r + 1] - base <= kWarpTileNnz) ++r;
     if (r > start) {
-      wt.tiles.push_back({start, r, 0, 0});
+      wt.tiles.push_back({start, r});
       continue;
     }
     // a single row longer than a tile: segments of kSegmentNnz nonzeros
     const int p0 = rowptr[r], p1 = rowptr[r + 1];
-    const int first = wt.nslots;
-    for (int p = p0; p < p1; p += kSegmentNnz) {
-      const int pe = (p1 - p > kSegmentNnz) ? p + kSegmentNnz : p1;
-      wt.tiles.push_back({r, -(wt.nslots + 1), p, pe});
-      ++wt.nslots;
-    }
-    wt.longrows.push_back({r, first, wt.nslots - first});
+    const int first = (int)wt.segs.size();
+    for (int p = p0; p < p1; p += kSegmentNnz) wt.segs.push_back({p, (p1 - p > kSegmentNnz) ? p + kSegmentNnz : p1});
+    wt.longrows.push_back({r, first, (int)wt.segs.size() - first});
     ++r;
   }
   return wt;
 }
 
 template <typename VT>
-cudaError_t spmv_warptile_launch_t(int ntiles, const int4 *tiles, int nlong, const int3 *longrows, double *partials,
-                                   const int *rowptr, const int *colind, const VT *vals, const double *x, double *y,
-                                   cudaStream_t stream, const GsState *st, int step) {
-  if (ntiles <= 0) return cudaSuccess;
-  static int sms = 0;
+cudaError_t spmv_warptile_launch_t(const SpmvTiles &T, const int *rowptr, const int *colind, const VT *vals,
+                                   const double *x, double *y, cudaStream_t stream, const GsState *st, int step) {
+  static int sms = 0, tile_per_sm = 0, seg_per_sm = 0;
   if (!sms) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (sms <= 0) sms = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tile_per_sm, spmv_warptile_kernel<VT>, kSpmvThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&seg_per_sm, spmv_segment_kernel<VT>, kSpmvThreads, 0);
+    if (tile_per_sm <= 0) tile_per_sm = 1;
+    if (seg_per_sm <= 0) seg_per_sm = 1;
   }
   const int warps_per_cta = kSpmvThreads / 32;
-  int grid = (ntiles + warps_per_cta - 1) / warps_per_cta;
-  const int cap = sms * 8;  // persistent: 8 CTAs (64 warps) per SM
-  if (grid > cap) grid = cap;
-  spmv_warptile_kernel<VT><<<grid, kSpmvThreads, 0, stream>>>(ntiles, tiles, rowptr, colind, vals, x, y, partials, st,
-                                                              step);
-  count_launch();
-  if (nlong > 0) {
-    spmv_fixup_kernel<<<(nlong + 127) / 128, 128, 0, stream>>>(nlong, longrows, partials, y, st, step);
+  // persistent grids: every CTA resident at once
+  if (T.nsegs > 0) {
+    int grid = (T.nsegs + warps_per_cta - 1) / warps_per_cta;
+    if (grid > sms * seg_per_sm) grid = sms * seg_per_sm;
+    spmv_segment_kernel<VT><<<grid, kSpmvThreads, 0, stream>>>(T.nsegs, T.segs, colind, vals, x, T.partials, st,
+                                                               step);
+    count_launch();
+  }
+  if (T.ntiles > 0) {
+    int grid = (T.ntiles + warps_per_cta - 1) / warps_per_cta;
+    if (grid > sms * tile_per_sm) grid = sms * tile_per_sm;
+    spmv_warptile_kernel<VT><<<grid, kSpmvThreads, 0, stream>>>(T.ntiles, T.tiles, rowptr, colind, vals, x, y, st,
+                                                                step);
+    count_launch();
+  }
+  if (T.nlong > 0) {
+    spmv_fixup_kernel<<<(T.nlong * 32 + 255) / 256, 256, 0, stream>>>(T.nlong, T.longrows, T.partials, y, st, step);
     count_launch();
   }
   return cudaGetLastError();
 }
 
-cudaError_t spmv_warptile_launch(int ntiles, const int4 *tiles, int nlong, const int3 *longrows, double *partials,
-                                 const int *rowptr, const int *colind, const double *vals, const double *x, double *y,
-                                 cudaStream_t stream, const GsState *st, int step) {
-  return spmv_warptile_launch_t<double>(ntiles, tiles, nlong, longrows, partials, rowptr, colind, vals, x, y, stream,
-                                        st, step);
+cudaError_t spmv_warptile_launch(const SpmvTiles &T, const int *rowptr, const int *colind, const double *vals,
+                                 const double *x, double *y, cudaStream_t stream, const GsState *st, int step) {
+  return spmv_warptile_launch_t<double>(T, rowptr, colind, vals, x, y, stream, st, step);
 }
 
-cudaError_t spmv_warptile_launch_f32(int ntiles, const int4 *tiles, int nlong, const int3 *longrows, double *partials,
-                                     const int *rowptr, const int *colind, const float *vals, const double *x,
-                                     double *y, cudaStream_t stream, const GsState *st, int step) {
-  return spmv_warptile_launch_t<float>(ntiles, tiles, nlong, longrows, partials, rowptr, colind, vals, x, y, stream,
-                                       st, step);
+cudaError_t spmv_warptile_launch_f32(const SpmvTiles &T, const int *rowptr, const int *colind, const float *vals,
+                                     const double *x, double *y, cudaStream_t stream, const GsState *st, int step) {
+  return spmv_warptile_launch_t<float>(T, rowptr, colind, vals, x, y, stream, st, step);
 }
 
 cudaError_t spmv_rowblock_launch(int nblocks, const int *blocks, const int *rowptr, const int *colind,

@@ -6,6 +6,7 @@ time one kernel family in isolation with CUDA events:
   python slepc_b200/kernel_bench.py gs --j 20 60    # one column orthogonalisation against j columns
   python slepc_b200/kernel_bench.py spmv             # CSR SpMV of the 7-point Laplacian
   python slepc_b200/kernel_bench.py multinplace      # restart GEMM V(:,0:56) = V(:,0:80) Q
+  python slepc_b200/kernel_bench.py cross            # A x, A^T z, A^T A x of the 2M x 500k power-law matrix
 
 Prints one JSON line per kernel family: average ms per call and algorithmic GB/s.
 """
@@ -89,6 +90,47 @@ def spmv(args, torch):
             "GBps": algo / (ms * 1e-3) / 1e9}
 
 
+def cross(args, torch):
+    """A x and A^T z of the power-law rectangular matrix (FP32 values), each timed alone with L2
+    flushed, plus the A^T A shell."""
+    m, n = args.rows, args.cols
+    rowptr, colind, vals = P.powerlaw_rect(m, n, 20, 1.8, seed=0)
+    nnz = int(rowptr[-1])
+    A = S.Mat().createAIJ((rowptr, colind, vals), size=(m, n), dtype=np.float32)
+    C = S.Mat().createCross(A)
+    x = torch.from_numpy(P.start_vector(n, 0)).cuda()
+    z = torch.from_numpy(P.start_vector(m, 1)).cuda()
+    y = torch.empty(m, dtype=torch.float64, device="cuda")
+    yt = torch.empty(n, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        ms = 0.0
+        for _ in range(args.reps):
+            flush.fill_(1.0)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        return ms / args.reps
+
+    ms_a = timed(lambda: A.mult(x.data_ptr(), y.data_ptr()))
+    ms_at = timed(lambda: A.multTranspose(z.data_ptr(), yt.data_ptr()))
+    ms_c = timed(lambda: C.mult(x.data_ptr(), yt.data_ptr()))
+    part = lambda rows, cols: nnz * 8 + (rows + 1) * 4 + cols * 8 + rows * 8
+    out = []
+    for name, ms, algo in [("A x (warp tiles, 20 nonzeros per row)", ms_a, part(m, n)),
+                           ("A^T z (segments of the power-law columns)", ms_at, part(n, m)),
+                           ("A^T (A x) shell", ms_c, part(m, n) + part(n, m))]:
+        out.append({"kernel": name, "m": m, "n": n, "nnz": nnz, "ms": ms, "algorithmic_bytes": algo,
+                    "GBps": algo / (ms * 1e-3) / 1e9})
+    return out
+
+
 def multinplace(args, torch):
     n, k, e = args.n, 80, 56
     bv = S.BV().create(n, 81)
@@ -117,7 +159,9 @@ def multinplace(args, torch):
 
 def main():
     p = argparse.ArgumentParser()
-    p.add_argument("kernel", choices=["gs", "spmv", "multinplace", "all"])
+    p.add_argument("kernel", choices=["gs", "spmv", "multinplace", "cross", "all"])
+    p.add_argument("--rows", type=int, default=2_000_000)
+    p.add_argument("--cols", type=int, default=500_000)
     p.add_argument("--n", type=int, default=128 ** 3)
     p.add_argument("--grid", type=int, default=128)
     p.add_argument("--j", type=int, nargs="+", default=[60])
@@ -135,6 +179,9 @@ def main():
             for j in js:
                 args.j = j
                 print(json.dumps(gs(args, torch)), flush=True)
+        elif k == "cross":
+            for line in cross(args, torch):
+                print(json.dumps(line), flush=True)
         else:
             print(json.dumps({"spmv": spmv, "multinplace": multinplace}[k](args, torch)), flush=True)
 

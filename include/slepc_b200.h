@@ -40,6 +40,7 @@ typedef int b200_status;
 #define B200_ERR_STATE 7      /* call out of order (e.g. EPSGetEigenpair before EPSSolve) */
 #define B200_ERR_DEVICE 8     /* a kernel reported a device-side error (bounded wait expired, NaN) */
 #define B200_ERR_FP 9         /* floating-point failure (PETSC_ERR_FP: negative eigenvalue of A^T A) */
+#define B200_ERR_IO 10        /* file read/write failure or malformed binary file (PETSC_ERR_FILE_READ / _UNEXPECTED) */
 
 /* Which eigenpairs (EPSWhich, include/slepceps.h; comparators src/sys/slepcsc.c:152-210). */
 #define B200_LARGEST_MAGNITUDE 1
@@ -69,6 +70,16 @@ typedef int b200_status;
 /* Error type for b200_svd_compute_error in addition to ABSOLUTE/RELATIVE (SVD_ERROR_NORM). */
 #define B200_ERROR_NORM 2
 
+/* PETSc binary files (PetscViewerBinary): class ids of the objects and file modes. */
+#define B200_MAT_FILE_CLASSID 1211216
+#define B200_VEC_FILE_CLASSID 1211214
+#define B200_FILE_MODE_READ 0
+#define B200_FILE_MODE_WRITE 1
+#define B200_FILE_MODE_APPEND 2
+/* b200_mat_load storage: a square CSR operator (b200_mat_create_csr), else a scalar type of b200_mat_create_aij. */
+#define B200_MAT_OPERATOR (-1)
+
+typedef struct b200_viewer_s *b200_viewer;
 typedef struct b200_mat_s *b200_mat;
 typedef struct b200_bv_s *b200_bv;
 typedef struct b200_eps_s *b200_eps;
@@ -272,6 +283,30 @@ b200_status b200_eps_solve_csr_host(int n, int64_t nnz, const int *rowptr_host, 
                                     const double *vals_host, const double *v0_host, int nev, int ncv, int mpd,
                                     double tol, int max_it, int which, double *evals_host, double *X_host,
                                     double *errest_host, int *info_host, void *stream);
+
+/* ----------------------------------------------------- PETSc binary I/O --- */
+
+/* The PETSc binary format of MatView/VecView and MatLoad/VecLoad
+ * (PetscViewerBinaryOpen as used by src/eps/tutorials/ex4.c:45-48 and
+ * ex31.c:551-562): big-endian, 32-bit PetscInt, real double PetscScalar.
+ *   Mat: int32 classid 1211216, M, N, nz, row lengths[M], column indices[nz], float64 values[nz]
+ *   Vec: int32 classid 1211214, N, float64 values[N]
+ * Objects follow one another in a file.  PetscViewerBinaryOpen / PetscViewerDestroy: */
+b200_status b200_viewer_binary_open(const char *path, int mode, b200_viewer *v);
+b200_status b200_viewer_destroy(b200_viewer v);
+/* Header of the next object without consuming it: classid, and M, N, nz for a
+ * Mat or N, 1, N for a Vec.  B200_ERR_IO at the end of the file. */
+b200_status b200_viewer_peek(b200_viewer v, int *classid, int *m, int *n, int64_t *nnz);
+/* Read the next Mat into host CSR arrays (rowptr M+1, colind/vals nz, sizes from peek). */
+b200_status b200_mat_read_csr(b200_viewer v, int *rowptr_host, int *colind_host, double *vals_host);
+b200_status b200_mat_write_csr(b200_viewer v, int m, int n, int64_t nnz, const int *rowptr_host,
+                               const int *colind_host, const double *vals_host);
+/* VecLoad / VecView of host arrays (nmax: capacity of x_host; n: length read). */
+b200_status b200_vec_read(b200_viewer v, int nmax, int *n, double *x_host);
+b200_status b200_vec_write(b200_viewer v, int n, const double *x_host);
+/* MatLoad into HBM (storage B200_MAT_OPERATOR, B200_SCALAR_F64 or B200_SCALAR_F32) and MatView. */
+b200_status b200_mat_load(b200_viewer v, int storage, void *stream, b200_mat *A);
+b200_status b200_mat_view(b200_mat A, b200_viewer v);
 
 /* ------------------------------------------------------------------ SVD --- */
 

@@ -28,7 +28,12 @@ SCALAR_F64, SCALAR_F32 = 0, 1
 
 _STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "LAPACK error", 4: "invalid inner product",
            5: "breakdown", 6: "out of device memory", 7: "wrong call order", 8: "device-side error",
-           9: "floating-point error"}
+           9: "floating-point error", 10: "file error"}
+
+# PETSc binary files
+MAT_FILE_CLASSID, VEC_FILE_CLASSID = 1211216, 1211214
+FILE_MODE_READ, FILE_MODE_WRITE, FILE_MODE_APPEND = 0, 1, 2
+MAT_OPERATOR = -1
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -66,6 +71,15 @@ _SIGS = {
     "b200_mat_mult_transpose": (ctypes.c_int, [_vp, _vp, _vp]),
     "b200_mat_get_sizes": (ctypes.c_int, [_vp, _ip, _ip]),
     "b200_mat_norm_inf": (ctypes.c_int, [_vp, _dp]),
+    "b200_viewer_binary_open": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _vp]),
+    "b200_viewer_destroy": (ctypes.c_int, [_vp]),
+    "b200_viewer_peek": (ctypes.c_int, [_vp, _ip, _ip, _ip, ctypes.POINTER(ctypes.c_int64)]),
+    "b200_mat_read_csr": (ctypes.c_int, [_vp, _ip, _ip, _dp]),
+    "b200_mat_write_csr": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int64, _ip, _ip, _dp]),
+    "b200_vec_read": (ctypes.c_int, [_vp, ctypes.c_int, _ip, _dp]),
+    "b200_vec_write": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    "b200_mat_load": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
+    "b200_mat_view": (ctypes.c_int, [_vp, _vp]),
     "b200_svd_create": (ctypes.c_int, [_vp, _vp]),
     "b200_svd_destroy": (ctypes.c_int, [_vp]),
     "b200_svd_set_operator": (ctypes.c_int, [_vp, _vp]),
@@ -178,6 +192,71 @@ def kernel_launch_count():
     return int(lib().b200_kernel_launch_count())
 
 
+class Viewer:
+    """PETSc binary file (PetscViewerBinary) holding Mat and Vec objects in sequence."""
+
+    class Mode:
+        READ, WRITE, APPEND = 0, 1, 2
+
+    def __init__(self):
+        self.handle = ctypes.c_void_p()
+
+    def createBinary(self, name, mode=0):
+        _check(lib().b200_viewer_binary_open(os.fsencode(name), mode, ctypes.byref(self.handle)))
+        return self
+
+    def peek(self):
+        """(classid, m, n, nnz) of the next object, without consuming it."""
+        c, m, n, z = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int64()
+        _check(lib().b200_viewer_peek(self.handle, ctypes.byref(c), ctypes.byref(m), ctypes.byref(n),
+                                      ctypes.byref(z)))
+        return c.value, m.value, n.value, z.value
+
+    def readCSR(self):
+        """The next Mat as host arrays (rowptr, colind, vals) and its shape."""
+        _, m, n, nnz = self.peek()
+        rowptr = np.zeros(m + 1, dtype=np.int32)
+        colind = np.zeros(max(nnz, 1), dtype=np.int32)
+        vals = np.zeros(max(nnz, 1))
+        _check(lib().b200_mat_read_csr(self.handle, _i(rowptr), _i(colind), _d(vals)))
+        return (rowptr, colind[:nnz], vals[:nnz]), (m, n)
+
+    def writeCSR(self, csr, shape):
+        rowptr = np.ascontiguousarray(csr[0], dtype=np.int32)
+        colind = np.ascontiguousarray(csr[1], dtype=np.int32)
+        vals = np.ascontiguousarray(csr[2], dtype=np.float64)
+        _check(lib().b200_mat_write_csr(self.handle, shape[0], shape[1], int(rowptr[-1]), _i(rowptr), _i(colind),
+                                        _d(vals)))
+
+    def readVec(self):
+        _, n, _, _ = self.peek()
+        x = np.zeros(max(n, 1))
+        got = ctypes.c_int()
+        _check(lib().b200_vec_read(self.handle, len(x), ctypes.byref(got), _d(x)))
+        return x[:got.value]
+
+    def writeVec(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        _check(lib().b200_vec_write(self.handle, len(x), _d(x)))
+
+    def destroy(self):
+        if self.handle:
+            _check(lib().b200_viewer_destroy(self.handle))
+            self.handle = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
 class Mat:
     """CSR matrix resident in HBM (the new Mat SpMV type), or the cross shell A^T A."""
 
@@ -214,6 +293,18 @@ class Mat:
             self.m, self.n = m, n
         self.nnz = nnz
         return self
+
+    def load(self, viewer, storage=MAT_OPERATOR, stream=None):
+        """MatLoad: the next Mat of a PETSc binary file, as a square operator
+        (MAT_OPERATOR) or a general matrix stored SCALAR_F64 / SCALAR_F32."""
+        _, m, n, nnz = viewer.peek()
+        _check(lib().b200_mat_load(viewer.handle, storage, stream, ctypes.byref(self.handle)))
+        self.m, self.n, self.nnz = m, n, nnz
+        return self
+
+    def view(self, viewer):
+        """MatView to a PETSc binary file."""
+        _check(lib().b200_mat_view(self.handle, viewer.handle))
 
     def createCross(self, A):
         """The shell A^T A (MatMult_Cross); A must outlive it."""
@@ -507,6 +598,12 @@ class EPS:
         s = EPSStats()
         _check(lib().b200_eps_get_stats(self.handle, ctypes.byref(s)))
         return {f: getattr(s, f) for f, _ in EPSStats._fields_}
+
+    def viewEigenvectors(self, viewer):
+        """Append the converged eigenvectors to a PETSc binary file as Vecs, in order (a warm
+        start for a later solve: read one back and pass it to setInitialSpace)."""
+        for i in range(self.getConverged()):
+            viewer.writeVec(self.getEigenpair(i)[1])
 
     def destroy(self):
         if self.handle:

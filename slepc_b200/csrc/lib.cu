@@ -369,6 +369,55 @@ extern "C" b200_status b200_mat_get_lanes(b200_mat A, int *lanes) {
   return B200_OK;
 }
 
+// MatLoad: the next Mat object of a PETSc binary file as a square CSR operator
+// (storage B200_MAT_OPERATOR) or as a general AIJ matrix with its transpose
+// (storage B200_SCALAR_F64 / B200_SCALAR_F32).
+extern "C" b200_status b200_mat_load(b200_viewer v, int storage, void *stream, b200_mat *A) {
+  B200_ARG_CHECK(v && A, "null argument");
+  B200_ARG_CHECK(storage == B200_MAT_OPERATOR || storage == B200_SCALAR_F64 || storage == B200_SCALAR_F32,
+                 "unknown storage");
+  int classid = 0, m = 0, n = 0;
+  int64_t nnz = 0;
+  B200_CHECK(b200_viewer_peek(v, &classid, &m, &n, &nnz));
+  B200_ARG_CHECK(classid == B200_MAT_FILE_CLASSID, "the next object in the file is not a Mat");
+  B200_ARG_CHECK(storage != B200_MAT_OPERATOR || m == n, "an operator must be square");
+  std::vector<int> rp((size_t)m + 1), ci((size_t)(nnz > 0 ? nnz : 1));
+  std::vector<double> va((size_t)(nnz > 0 ? nnz : 1));
+  B200_CHECK(b200_mat_read_csr(v, rp.data(), ci.data(), va.data()));
+  if (storage == B200_MAT_OPERATOR) return b200_mat_create_csr(n, nnz, rp.data(), ci.data(), va.data(), stream, A);
+  if (storage == B200_SCALAR_F32) {
+    std::vector<float> vf(va.begin(), va.end());
+    return b200_mat_create_aij(m, n, nnz, rp.data(), ci.data(), vf.data(), B200_SCALAR_F32, stream, A);
+  }
+  return b200_mat_create_aij(m, n, nnz, rp.data(), ci.data(), va.data(), B200_SCALAR_F64, stream, A);
+}
+
+// MatView to a PETSc binary file (FP32-stored values are written widened to double).
+extern "C" b200_status b200_mat_view(b200_mat A, b200_viewer v) {
+  B200_ARG_CHECK(A && v, "null argument");
+  B200_ARG_CHECK(A->kind == kMatCsr, "a cross shell has no stored entries to view");
+  const CsrPart &P = A->a;
+  std::vector<int> rp((size_t)P.rows + 1), ci((size_t)(P.nnz > 0 ? P.nnz : 1));
+  std::vector<double> va((size_t)(P.nnz > 0 ? P.nnz : 1));
+  B200_CUDA_CHECK(cudaMemcpyAsync(rp.data(), P.rowptr, sizeof(int) * rp.size(), cudaMemcpyDeviceToHost, A->stream));
+  if (P.nnz) {
+    B200_CUDA_CHECK(
+        cudaMemcpyAsync(ci.data(), P.colind, sizeof(int) * (size_t)P.nnz, cudaMemcpyDeviceToHost, A->stream));
+    if (P.f32) {
+      std::vector<float> vf((size_t)P.nnz);
+      B200_CUDA_CHECK(
+          cudaMemcpyAsync(vf.data(), P.vals, sizeof(float) * (size_t)P.nnz, cudaMemcpyDeviceToHost, A->stream));
+      B200_CUDA_CHECK(cudaStreamSynchronize(A->stream));
+      for (size_t i = 0; i < vf.size(); ++i) va[i] = vf[i];
+    } else {
+      B200_CUDA_CHECK(
+          cudaMemcpyAsync(va.data(), P.vals, sizeof(double) * (size_t)P.nnz, cudaMemcpyDeviceToHost, A->stream));
+    }
+  }
+  B200_CUDA_CHECK(cudaStreamSynchronize(A->stream));
+  return b200_mat_write_csr(v, P.rows, P.cols, P.nnz, rp.data(), ci.data(), va.data());
+}
+
 extern "C" b200_status b200_mat_destroy(b200_mat A) {
   if (!A) return B200_OK;
   part_free(A->a);

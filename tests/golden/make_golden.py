@@ -13,6 +13,7 @@ Sources:
   src/sys/classes/bv/tests/output/test2_1.out         (test2.c, n=20 k=8, CGS)
   src/sys/classes/ds/tests/output/test2_1.out         (test2.c, DSHEP n=12, ld=n+2)
   src/sys/classes/bv/tests/output/test1_1_bv_type-svec.out (test1.c, n=10 k=5 l=3, -verbose)
+  src/eps/tutorials/X.bin, Ybus.bin                    (PETSc binary Vec and Mat read by ex31.c)
 """
 import json
 import os
@@ -103,9 +104,33 @@ def bv_test1(root):
             "X_after_multinplace_scale2": _vec_blocks(after_mip), "norm2_X0": n2, "norm_fro": fro}
 
 
+def petsc_binary(root):
+    """The two PETSc binary files of ex31 (a Vec and an AIJ Mat), decoded with the published
+    layout (big-endian int32 header and indices, float64 values; values kept exactly as hex)."""
+    import struct
+
+    out = {}
+    raw = open(os.path.join(root, "src/eps/tutorials/X.bin"), "rb").read()
+    cid, n = struct.unpack(">ii", raw[:8])
+    vals = struct.unpack(">%dd" % n, raw[8:8 + 8 * n])
+    out["X.bin"] = {"classid": cid, "n": n, "values_hex": [v.hex() for v in vals], "bytes": len(raw)}
+    raw = open(os.path.join(root, "src/eps/tutorials/Ybus.bin"), "rb").read()
+    cid, m, ncol, nz = struct.unpack(">iiii", raw[:16])
+    off = 16
+    lens = struct.unpack(">%di" % m, raw[off:off + 4 * m])
+    off += 4 * m
+    cols = struct.unpack(">%di" % nz, raw[off:off + 4 * nz])
+    off += 4 * nz
+    vals = struct.unpack(">%dd" % nz, raw[off:off + 8 * nz])
+    out["Ybus.bin"] = {"classid": cid, "m": m, "n": ncol, "nz": nz, "row_lengths": list(lens),
+                       "colind": list(cols), "values_hex": [v.hex() for v in vals], "bytes": len(raw)}
+    return {"source": "src/eps/tutorials/X.bin, Ybus.bin (read by ex31.c:551-562 with VecLoad / MatLoad)",
+            "files": out}
+
+
 def main(root):
     fixtures = {"ex2_1.json": ex2(root), "bv_test2.json": bv_test2(root), "ds_test2.json": ds_test2(root),
-                "bv_test1.json": bv_test1(root)}
+                "bv_test1.json": bv_test1(root), "petsc_binary.json": petsc_binary(root)}
     for name, obj in fixtures.items():
         with open(os.path.join(HERE, name), "w") as f:
             json.dump(obj, f, indent=1)

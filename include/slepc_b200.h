@@ -246,6 +246,25 @@ b200_status b200_eps_set_initial_space_device(b200_eps eps, const double *v0_dev
 /* Stop after this many restarts (0 = no cap; used to time bounded samples). */
 b200_status b200_eps_set_max_restarts(b200_eps eps, int max_restarts);
 /* EPSSolve (src/eps/interface/epssolve.c:119-229 -> EPSSolve_KrylovSchur_Default, krylovschur.c:227-348). */
+/* EPSSetType: B200_EPS_KRYLOVSCHUR (default) or B200_EPS_LOBPCG. */
+#define B200_EPS_KRYLOVSCHUR 0
+#define B200_EPS_LOBPCG 1
+b200_status b200_eps_set_type(b200_eps eps, int type);
+/* EPSLOBPCGSetBlockSize (bs <= 0: min(16, nev)), EPSLOBPCGSetRestart (in [0.1, 1]),
+ * EPSLOBPCGSetLocking (src/eps/impls/cg/lobpcg/lobpcg.c). */
+b200_status b200_eps_lobpcg_set_block_size(b200_eps eps, int bs);
+b200_status b200_eps_lobpcg_set_restart(b200_eps eps, double restart);
+b200_status b200_eps_lobpcg_set_locking(b200_eps eps, int lock);
+/* Preconditioner of a preconditioned eigensolver: STPRECOND with KSPPREONLY and
+ * PCNONE (identity) or PCJACOBI (diag(A)^{-1}, a zero diagonal entry counts as 1). */
+#define B200_PC_NONE 0
+#define B200_PC_JACOBI 1
+b200_status b200_eps_set_preconditioner(b200_eps eps, int pc);
+/* EPSSetInitialSpace with k vectors (host, n x k column-major): inserted and
+ * orthonormalised as BVInsertVecs does, linearly dependent ones dropped
+ * (src/sys/classes/bv/interface/bvfunc.c:331-374).  Krylov-Schur starts from
+ * the first; LOBPCG uses the block. */
+b200_status b200_eps_set_initial_space_block(b200_eps eps, int k, const double *X_host);
 b200_status b200_eps_solve(b200_eps eps);
 b200_status b200_eps_get_converged(b200_eps eps, int *nconv);
 b200_status b200_eps_get_iteration_number(b200_eps eps, int *its);

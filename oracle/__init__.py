@@ -41,6 +41,10 @@ def lib():
         L.oracle_residual.argtypes = [ctypes.c_int, _ip, _ip, _dp, _dp, ctypes.c_double]
         L.oracle_spmv.argtypes = [ctypes.c_int, _ip, _ip, _dp, _dp, _dp]
         L.oracle_set_threads.argtypes = [ctypes.c_int]
+        L.oracle_lobpcg.restype = ctypes.c_int
+        L.oracle_lobpcg.argtypes = [ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_double, _dp, ctypes.c_int, _dp, _dp, _dp, _ip]
         L.oracle_csr_transpose.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, _ip, _ip, _dp]
         L.oracle_svd_cross.restype = ctypes.c_int
         L.oracle_svd_cross.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, _ip, _ip, _dp, _dp,
@@ -212,3 +216,28 @@ def svd_cross(rowptr, colind, vals, shape, v0, nsv, ncv, tol=0.0, largest=True, 
         U, V = V, U
     return SVDResult(sig[:k].copy(), U, V, err[:k].copy(), k, int(info[1]), int(info[2]), int(info[3]),
                      int(info[4]), int(info[5]))
+
+
+def lobpcg(A, nev, bs=0, ncv=0, tol=1e-8, max_it=0, which=SMALLEST_REAL, pc="jacobi", lock=True, restart=0.9,
+           X0=None):
+    """EPSSolve with EPSLOBPCG on a symmetric scipy CSR matrix; X0 (n x k) an initial space."""
+    n = A.shape[0]
+    rowptr, colind, vals = _csr(A)
+    cap = max(ncv, 3 * max(bs, min(16, nev)), ((nev - 1) // max(bs or min(16, nev), 1) + 3) * max(bs or min(16, nev), 1)) + 48
+    evals = np.zeros(cap)
+    errest = np.zeros(cap)
+    X = np.zeros((cap, n))
+    info = np.zeros(8, dtype=np.int32)
+    nini = 0
+    x0p = None
+    if X0 is not None:
+        X0 = np.asfortranarray(X0, dtype=np.float64)
+        nini = X0.shape[1]
+        x0p = _d(X0)
+    st = lib().oracle_lobpcg(n, _i(rowptr), _i(colind), _d(vals), nev, bs, ncv, tol, max_it, which,
+                             {"none": 0, "jacobi": 1}[pc], 1 if lock else 0, restart, x0p, nini, _d(evals), _d(X),
+                             _d(errest), _i(info))
+    if st:
+        raise RuntimeError(f"oracle_lobpcg failed with status {st}")
+    k = int(info[0])
+    return SolveResult(evals[:k].copy(), X[:k].T.copy(), errest[:k].copy(), k, int(info[1]), int(info[2]), 0, 0, 0)

@@ -448,11 +448,11 @@ typedef struct {
 } orc_info;
 
 /* EPSGetStartVector, epssolve.c:841-870 (i > 0 uses a random vector) */
-static int get_start_vector(obv *bv, int i, int *breakdown)
+static int get_start_vector(obv *bv, int i, int nini, int *breakdown)
 {
   double norm;
   int lindep, st;
-  if (i > 0) set_random_column(bv, i);
+  if (i > 0 || nini == 0) set_random_column(bv, i);   /* epssolve.c:852 */
   if ((st = orthogonalize_gs(bv, i, NULL, &norm, &lindep))) return st;
   if (breakdown) *breakdown = lindep;
   else if (lindep || norm == 0.0) return ORC_ERR_BREAKDOWN;
@@ -507,13 +507,18 @@ static int eps_solve_op(const orc_op *op, const double *v0, int nev, int ncv, in
   errest = (double *)calloc(ds.ld, sizeof(double));
   perm = (int *)calloc(ds.ld, sizeof(int));
 
-  /* EPSSetUp: BVInsertVecs(V,0,&k,IS,TRUE) (epssetup.c:424, bvfunc.c:331-374) */
-  memcpy(bv.V, v0, sizeof(double) * (size_t)n);
-  if ((st = orthogonalize_gs(&bv, 0, NULL, &norm, &lindep))) goto done;
-  if (norm == 0.0 || lindep) { st = ORC_ERR_BREAKDOWN; goto done; }
-  scale_column(&bv, 0, 1.0 / norm);
-  /* EPSGetStartVector(eps,0,NULL) with nini = 1 */
-  if ((st = get_start_vector(&bv, 0, NULL))) goto done;
+  /* EPSSetUp: BVInsertVecs(V,0,&k,IS,TRUE) (epssetup.c:421-427, bvfunc.c:331-374): a zero or
+   * dependent initial vector is dropped and the start vector is then random */
+  {
+    int nini = 0;
+    if (v0) {
+      memcpy(bv.V, v0, sizeof(double) * (size_t)n);
+      if ((st = orthogonalize_gs(&bv, 0, NULL, &norm, &lindep))) goto done;
+      if (!(norm == 0.0 || lindep)) { scale_column(&bv, 0, 1.0 / norm); nini = 1; }
+    }
+    /* EPSGetStartVector(eps,0,NULL) */
+    if ((st = get_start_vector(&bv, 0, nini, NULL))) goto done;
+  }
 
   l = 0;
   info.reason = ORC_ITERATING;
@@ -577,7 +582,7 @@ static int eps_solve_op(const orc_op *op, const double *v0, int nev, int ncv, in
       if (breakdown || k == nv) {
         if (k < nev) {
           int bd = 0;
-          if ((st = get_start_vector(&bv, k, &bd))) goto done;
+          if ((st = get_start_vector(&bv, k, 1, &bd))) goto done;
           if (bd) info.reason = ORC_DIVERGED_BREAKDOWN;
         }
       } else {
@@ -889,4 +894,424 @@ double oracle_residual(int n, const int *rowptr, const int *colind, const double
   r = nrm2(n, u);
   free(u);
   return r / fabs(lambda);
+}
+
+/* ======================================================================
+ * LOBPCG: EPSSolve_LOBPCG (src/eps/impls/cg/lobpcg/lobpcg.c:86-398) with
+ * EPSSetUp_LOBPCG / EPSSetDimensions_LOBPCG (:40-84), soft and hard locking,
+ * a standard symmetric problem (B = NULL), and the preconditioner of
+ * STPRECOND + KSPPREONLY: PCNONE (identity) or PCJACOBI (w = diag(A)^{-1} r,
+ * zero diagonal entries replaced by 1).  The block operations follow the BV
+ * interface with active columns [l,k):
+ *   BVCopy (bvbasic.c:1779, BVCopy_Svec svec.c:233-247), BVMatMult
+ *   (bvops.c), BVMatProject_MatMult / _Dot (bvglobal.c:902-1060), BVDot and
+ *   BVMult (BLAS gemm, bvblas.c), BVMultInPlace (64-row blocked gemm),
+ *   BVOrthogonalize_GS (bvorthog.c:507-548: each column against ALL previous
+ *   columns, leading ones included), BVOrthogonalizeVec (:238-262),
+ *   BVInsertVecs (bvfunc.c:331-374);
+ * DSGHEP: LAPACK dsygvd itype 1 "V" "U" (dsghep.c:96-148), DSSort_GHEP
+ * (:75-94, insertion sort with SlepcCompareSmallestReal; the spectrum is
+ * flipped for the largest), DSVectors_GHEP (X = Q).
+ * ====================================================================== */
+extern void scipy_dsygvd_(const int *, const char *, const char *, const int *, double *, const int *, double *,
+                          const int *, double *, double *, const int *, int *, const int *, int *, size_t, size_t);
+
+typedef struct {
+  obv b;     /* storage and Gram-Schmidt scratch */
+  int l, k;  /* active columns */
+} oblk;
+
+#define BCOL(B, j) ((B)->b.V + (size_t)(j) * (B)->b.ld)
+
+static void blk_init(oblk *B, int n, int m)
+{
+  B->b.n = n; B->b.m = m; B->b.ld = n;
+  B->b.V = (double *)calloc((size_t)n * m, sizeof(double));
+  B->b.buf = (double *)calloc((size_t)m * m, sizeof(double));
+  B->b.hvec = (double *)calloc((size_t)m + 1, sizeof(double));
+  B->b.cvec = (double *)calloc((size_t)m + 1, sizeof(double));
+  B->b.eta = 0.7071; B->b.deftol = 10 * ORC_MACHINE_EPS; B->b.seed = 0x5eedULL; B->b.nrand = 0;
+  B->l = 0; B->k = m;
+}
+
+static void blk_free(oblk *B)
+{
+  free(B->b.V); free(B->b.buf); free(B->b.hvec); free(B->b.cvec);
+}
+
+static void blk_active(oblk *B, int l, int k) { B->l = l; B->k = k; }
+
+static void blk_copy(const oblk *src, oblk *dst)
+{
+  for (int j = 0; j < src->k - src->l; j++)
+    memcpy(BCOL(dst, dst->l + j), BCOL(src, src->l + j), sizeof(double) * (size_t)src->b.n);
+}
+
+static void blk_copy_column(oblk *B, int j, int i)
+{
+  memcpy(BCOL(B, i), BCOL(B, j), sizeof(double) * (size_t)B->b.n);
+}
+
+static void blk_matmult(const orc_op *op, const oblk *X, oblk *Y)
+{
+  for (int j = 0; j < X->k - X->l; j++) op_apply(op, BCOL(X, X->l + j), BCOL(Y, Y->l + j));
+}
+
+/* M(Y.l+i, X.l+j) = Y(:,Y.l+i)' X(:,X.l+j) (BVDot: M = Y^H X on active columns) */
+static void blk_dot(const oblk *X, const oblk *Y, double *M, int ldm)
+{
+  const int nx = X->k - X->l, ny = Y->k - Y->l, n = X->b.n;
+  const double one = 1.0, zero = 0.0;
+  if (nx <= 0 || ny <= 0) return;
+  scipy_dgemm_("T", "N", &ny, &nx, &n, &one, BCOL(Y, Y->l), &Y->b.ld, BCOL(X, X->l), &X->b.ld, &zero,
+               M + Y->l + (size_t)X->l * ldm, &ldm, 1, 1);
+}
+
+/* BVMult: Y(:,Y.l:Y.k) = beta Y + alpha X(:,X.l:X.k) Q(X.l:X.k, Y.l:Y.k) */
+static void blk_mult(oblk *Y, double alpha, double beta, const oblk *X, const double *Q, int ldq)
+{
+  const int nx = X->k - X->l, ny = Y->k - Y->l, n = X->b.n;
+  if (ny <= 0) return;
+  if (nx <= 0) { for (int j = 0; j < ny; j++) for (int i = 0; i < n; i++) BCOL(Y, Y->l + j)[i] *= beta; return; }
+  scipy_dgemm_("N", "N", &n, &ny, &nx, &alpha, BCOL(X, X->l), &X->b.ld, Q + X->l + (size_t)Y->l * ldq, &ldq, &beta,
+               BCOL(Y, Y->l), &Y->b.ld, 1, 1);
+}
+
+/* BVMultInPlace(V,Q,s,e): V(:,s:e) = V(:,l:k) Q(l:k,s:e), 64-row blocks (bvblas.c:74-106) */
+static void blk_multinplace(oblk *V, const double *Q, int ldq, int s, int e)
+{
+  int ncols = e - s, kq = V->k - V->l, bs = 64, rr, j, n = V->b.n;
+  const double one = 1.0, zero = 0.0;
+  if (ncols <= 0 || kq <= 0) return;
+  double *work = (double *)malloc(sizeof(double) * (size_t)bs * ncols);
+  const double *pb = Q + V->l + (size_t)s * ldq;
+  double *A = BCOL(V, V->l);
+  int r0 = n % bs;
+  if (r0) {
+    scipy_dgemm_("N", "N", &r0, &ncols, &kq, &one, A, &V->b.ld, pb, &ldq, &zero, work, &r0, 1, 1);
+    for (j = 0; j < ncols; j++) memcpy(BCOL(V, s + j), work + (size_t)j * r0, sizeof(double) * r0);
+  }
+  for (rr = r0; rr < n; rr += bs) {
+    scipy_dgemm_("N", "N", &bs, &ncols, &kq, &one, A + rr, &V->b.ld, pb, &ldq, &zero, work, &bs, 1, 1);
+    for (j = 0; j < ncols; j++) memcpy(BCOL(V, s + j) + rr, work + (size_t)j * bs, sizeof(double) * bs);
+  }
+  free(work);
+}
+
+/* BVOrthogonalize with BV_ORTHOG_BLOCK_GS */
+static int blk_orthogonalize(oblk *B)
+{
+  double norm;
+  int lindep, st;
+  for (int j = B->l; j < B->k; j++) {
+    if ((st = orthogonalize_gs(&B->b, j, NULL, &norm, &lindep))) return st;
+    if (norm == 0.0) return ORC_ERR_BREAKDOWN;
+    scale_column(&B->b, j, 1.0 / norm);
+  }
+  return ORC_OK;
+}
+
+/* DSSolve_GHEP + DSSort_GHEP + DSVectors_GHEP on an nv x nv pencil (A, B), ld x ld.
+ * On return wr holds the sorted eigenvalues and X (ld x ld) the eigenvectors. */
+static int ds_ghep(int nv, int ld, double *A, double *B, double *wr, double *X, int *perm)
+{
+  int itype = 1, info = 0, n1 = nv, lwork = 2 * nv * nv + 6 * nv + 1, liwork = 5 * nv + 3, i, j, p, k;
+  double *work = (double *)malloc(sizeof(double) * (size_t)lwork), rtmp;
+  int *iwork = (int *)malloc(sizeof(int) * (size_t)liwork);
+  scipy_dsygvd_(&itype, "V", "U", &n1, A, &ld, B, &ld, wr, work, &lwork, iwork, &liwork, &info, 1, 1);
+  free(work); free(iwork);
+  if (info) return ORC_ERR_LAPACK;
+  memset(X, 0, sizeof(double) * (size_t)ld * ld);
+  for (i = 0; i < nv; i++) memcpy(X + (size_t)i * ld, A + (size_t)i * ld, sizeof(double) * nv);
+  /* insertion sort, smallest real first */
+  for (i = 0; i < nv; i++) perm[i] = i;
+  for (i = 1; i < nv; i++) {
+    double re = wr[perm[i]];
+    j = i - 1;
+    int result = sc_compare(ORC_SMALLEST_REAL, re, wr[perm[j]]);
+    while (result < 0 && j >= 0) {
+      int tmp = perm[j]; perm[j] = perm[j + 1]; perm[j + 1] = tmp; j--;
+      if (j >= 0) result = sc_compare(ORC_SMALLEST_REAL, re, wr[perm[j]]);
+    }
+  }
+  {
+    double *w2 = (double *)malloc(sizeof(double) * (size_t)nv);
+    for (i = 0; i < nv; i++) w2[i] = wr[perm[i]];
+    memcpy(wr, w2, sizeof(double) * (size_t)nv);
+    free(w2);
+  }
+  for (i = 0; i < nv; i++) {
+    p = perm[i];
+    if (p != i) {
+      j = i + 1;
+      while (perm[j] != i) j++;
+      perm[j] = p; perm[i] = i;
+      for (k = 0; k < nv; k++) {
+        rtmp = X[k + (size_t)p * ld]; X[k + (size_t)p * ld] = X[k + (size_t)i * ld]; X[k + (size_t)i * ld] = rtmp;
+      }
+    }
+  }
+  return ORC_OK;
+}
+
+/* W(:,j) = dinv .* R(:,j) on active columns (PCApply_Jacobi: pointwise product with the inverse diagonal) */
+static void precond_apply(const double *dinv, oblk *R)
+{
+  if (!dinv) return;
+  for (int j = R->l; j < R->k; j++) {
+    double *w = BCOL(R, j);
+    for (int i = 0; i < R->b.n; i++) w[i] = dinv[i] * w[i];
+  }
+}
+
+/*
+ * oracle_lobpcg: EPSSolve with EPSLOBPCG on a symmetric CSR matrix.
+ *   which: ORC_SMALLEST_REAL or ORC_LARGEST_REAL; bs <= 0: min(16, nev);
+ *   ncv <= 0: the LOBPCG default; restart 0.9; lock 1; max_it <= 0: max(100, 2n/ncv);
+ *   pc: 0 none, 1 Jacobi; X0 (n x nini, column-major) the initial space (may be NULL).
+ * Outputs sorted eigenvalues (nconv), eigenvectors X (n x nconv), error estimates,
+ * info[0..3] = nconv, its, reason, iterations of the inner loop.
+ */
+int oracle_lobpcg(int n, const int *rowptr, const int *colind, const double *vals, int nev, int bs, int ncv,
+                  double tol, int max_it, int which, int pc, int lock, double restart, const double *X0, int nini,
+                  double *evals, double *Xout, double *errest_out, int *info)
+{
+  orc_op op;
+  oblk V, Z, X, R, P, AX, Y;
+  int st = ORC_OK, i, j, k, nv, ini, nconv, locked, its, guard, flip, useY, mpd, eps_its = 0, eps_nconv = 0;
+  int reason = ORC_ITERATING;
+  double *eigr, *errest, *dinv = NULL, *MA, *MB, *Q, *wr, norm;
+  int *dsperm, *perm;
+  memset(&op, 0, sizeof(op));
+  op.n = n; op.rp = rowptr; op.ci = colind; op.va = vals;
+  if (which != ORC_SMALLEST_REAL && which != ORC_LARGEST_REAL) return ORC_ERR_ARG;
+  if (bs <= 0) bs = nev < 16 ? nev : 16;
+  k = 3 * bs > ((nev - 1) / bs + 3) * bs ? 3 * bs : ((nev - 1) / bs + 3) * bs;
+  if (ncv <= 0) ncv = k;
+  else if (ncv < k) return ORC_ERR_ARG;
+  mpd = 3 * bs;
+  if (n < 5 * bs) return ORC_ERR_ARG;
+  if (max_it <= 0) max_it = (2 * n / ncv > 100) ? 2 * n / ncv : 100;
+  if (tol <= 0.0) tol = 1e-8;
+  if (restart <= 0.0) restart = 0.9;
+  guard = bs == 1 ? 0 : (int)((1.0 - restart) * bs + 0.45);
+  if (guard > bs - 1) guard = bs - 1;
+  flip = which == ORC_LARGEST_REAL;
+  useY = nev > bs - guard;
+
+  blk_init(&V, n, ncv);
+  blk_init(&Z, n, 3 * bs); blk_init(&X, n, bs); blk_init(&R, n, bs); blk_init(&P, n, bs); blk_init(&AX, n, bs);
+  blk_init(&Y, n, useY ? nev : 1);
+  blk_active(&Y, 0, 0);
+  eigr = (double *)calloc((size_t)ncv + 3 * bs, sizeof(double));
+  errest = (double *)calloc((size_t)ncv + 3 * bs, sizeof(double));
+  perm = (int *)calloc((size_t)ncv, sizeof(int));
+  MA = (double *)calloc((size_t)mpd * mpd, sizeof(double));
+  MB = (double *)calloc((size_t)mpd * mpd, sizeof(double));
+  Q = (double *)calloc((size_t)mpd * mpd, sizeof(double));
+  wr = (double *)calloc((size_t)mpd, sizeof(double));
+  dsperm = (int *)calloc((size_t)mpd, sizeof(int));
+  if (pc == 1) {
+    dinv = (double *)malloc(sizeof(double) * (size_t)n);
+    for (i = 0; i < n; i++) {
+      double d = 0.0;
+      for (int p = rowptr[i]; p < rowptr[i + 1]; p++)
+        if (colind[p] == i) d += vals[p];
+      dinv[i] = 1.0 / (d != 0.0 ? d : 1.0);
+    }
+  }
+
+  /* EPSSetUp: BVInsertVecs(V,0,&nini,IS,TRUE) */
+  {
+    int ndep = 0, lindep;
+    for (i = 0; i < nini; i++) {
+      memcpy(BCOL(&V, i - ndep), X0 + (size_t)i * n, sizeof(double) * (size_t)n);
+      if ((st = orthogonalize_gs(&V.b, i - ndep, NULL, &norm, &lindep))) goto done;
+      if (norm == 0.0 || lindep) ndep++;
+      else scale_column(&V.b, i - ndep, 1.0 / norm);
+    }
+    nini -= ndep;
+  }
+  /* 2-3: more initial vectors */
+  for (k = nini; k < ncv - bs; k++) {
+    set_random_column(&V.b, k);
+    if ((st = orthonormalize_column(&V.b, k, NULL, NULL))) goto done;
+  }
+  nv = bs;
+  blk_active(&V, 0, nv); blk_active(&Z, 0, nv);
+  blk_copy(&V, &Z);
+  blk_copy(&Z, &X);
+
+  /* 4. initial Ritz vectors */
+#define LOBPCG_RAYLEIGH_RITZ_X()                                                         \
+  do {                                                                                   \
+    blk_matmult(&op, &X, &AX);                                                           \
+    memset(MA, 0, sizeof(double) * (size_t)mpd * mpd);                                   \
+    blk_dot(&AX, &X, MA, mpd);                                                           \
+    if (flip) for (i = 0; i < mpd * mpd; i++) MA[i] = -MA[i];                            \
+    memset(MB, 0, sizeof(double) * (size_t)mpd * mpd);                                   \
+    for (i = 0; i < nv; i++) MB[i + (size_t)i * mpd] = 1.0;                              \
+    if ((st = ds_ghep(nv, mpd, MA, MB, wr, Q, dsperm))) goto done;                       \
+    for (j = 0; j < nv; j++) if (locked + j < ncv) eigr[locked + j] = flip ? -wr[j] : wr[j]; \
+    blk_multinplace(&X, Q, mpd, 0, nv);                                                  \
+    blk_multinplace(&AX, Q, mpd, 0, nv);                                                 \
+  } while (0)
+  locked = 0;
+  LOBPCG_RAYLEIGH_RITZ_X();
+
+  /* 5 */
+  nconv = 0;
+  its = 0;
+
+  /* 6. main loop */
+  while (reason == ORC_ITERATING) {
+    if (lock) { blk_active(&R, nconv, bs); blk_active(&AX, nconv, bs); }
+    /* 7. residuals */
+    ini = lock ? nconv : 0;
+    blk_copy(&AX, &R);
+    for (j = ini; j < bs; j++) {
+      double *r = BCOL(&R, j), *x = BCOL(&X, j), lam = eigr[locked + j];
+      for (i = 0; i < n; i++) r[i] -= lam * x[i];   /* VecAXPY */
+    }
+    /* 8. residual norms, active set */
+    k = ini;
+    {
+      int countc = 1;
+      for (j = ini; j < bs; j++) {
+        i = locked + j;
+        norm = nrm2(n, BCOL(&R, j));
+        errest[i] = (eigr[i] != 0.0) ? norm / fabs(eigr[i]) : DBL_MAX;   /* EPSConvergedRelative */
+        if (countc) {
+          if (errest[i] < tol) k++;
+          else countc = 0;
+        }
+        if (!countc) break;
+      }
+    }
+    nconv = k;
+    eps_nconv = locked + nconv;
+    /* EPSStoppingBasic */
+    if (eps_nconv >= nev) reason = ORC_CONVERGED_TOL;
+    else if (eps_its + its >= max_it) reason = ORC_DIVERGED_ITS;
+    if (reason != ORC_ITERATING || nconv >= bs - guard) {
+      blk_active(&V, locked, eps_nconv);
+      blk_active(&X, 0, nconv);
+      blk_copy(&X, &V);
+    }
+    if (reason != ORC_ITERATING) break;
+    else if (nconv >= bs - guard) { eps_its += its - 1; its = 0; }
+    else its++;
+
+    if (nconv >= bs - guard) {  /* hard locking */
+      int lindep;
+      blk_active(&Y, locked, locked + nconv);
+      blk_copy(&X, &Y);
+      blk_active(&Y, 0, locked + nconv);
+      for (j = nconv; j < bs; j++) {
+        blk_copy_column(&X, j, j - nconv);
+        blk_copy_column(&R, j, j - nconv);
+        blk_copy_column(&P, j, j - nconv);
+        blk_copy_column(&AX, j, j - nconv);
+      }
+      blk_active(&V, locked + bs, locked + bs + nconv);
+      blk_active(&X, bs - nconv, bs);
+      blk_copy(&V, &X);
+      for (j = bs - nconv; j < bs; j++) {
+        double *v = BCOL(&X, j);
+        if ((st = orthogonalize_gs(&Y.b, Y.k, v, &norm, &lindep))) goto done;
+        if (norm > 0.0 && !lindep) for (i = 0; i < n; i++) v[i] *= 1.0 / norm;   /* VecScale */
+        else { reason = ORC_DIVERGED_BREAKDOWN; goto diverged; }
+      }
+      locked += nconv;
+      nconv = 0;
+      blk_active(&X, nconv, bs);
+      if ((st = blk_orthogonalize(&X))) goto done;
+      blk_active(&Z, nconv, bs);
+      blk_active(&AX, nconv, bs);
+      blk_copy(&X, &Z);
+      nv = bs;
+      LOBPCG_RAYLEIGH_RITZ_X();
+      continue;
+    }
+
+    ini = lock ? nconv : 0;
+    if (lock) { blk_active(&R, nconv, bs); blk_active(&P, nconv, bs); blk_active(&AX, nconv, bs); }
+
+    /* 9. preconditioner */
+    precond_apply(dinv, &R);
+    if (locked > 0) {
+      int lindep;
+      for (j = ini; j < bs; j++) {
+        double *w = BCOL(&R, j);
+        if ((st = orthogonalize_gs(&Y.b, Y.k, w, &norm, &lindep))) goto done;
+        if (norm > 0.0 && !lindep) for (i = 0; i < n; i++) w[i] *= 1.0 / norm;
+        if (norm <= 0.0 || lindep) { reason = ORC_DIVERGED_BREAKDOWN; goto diverged; }
+      }
+    }
+    /* 11 */
+    if ((st = blk_orthogonalize(&R))) goto done;
+    /* 13-16 */
+    if (its > 1 && (st = blk_orthogonalize(&P))) goto done;
+    /* 17-23 */
+    blk_active(&Z, 0, bs); blk_active(&X, 0, bs);
+    blk_copy(&X, &Z);
+    blk_active(&Z, bs, 2 * bs - ini);
+    blk_copy(&R, &Z);
+    if (its > 1) {
+      blk_active(&Z, 2 * bs - ini, 3 * bs - 2 * ini);
+      blk_copy(&P, &Z);
+    }
+    nv = its > 1 ? 3 * bs - 2 * ini : 2 * bs - ini;
+    blk_active(&Z, 0, nv);
+    {
+      oblk W;   /* BVMatProject_MatMult: W = A Z, M = Z' W */
+      blk_init(&W, n, nv);
+      blk_matmult(&op, &Z, &W);
+      memset(MA, 0, sizeof(double) * (size_t)mpd * mpd);
+      blk_dot(&W, &Z, MA, mpd);
+      blk_free(&W);
+    }
+    if (flip) for (i = 0; i < mpd * mpd; i++) MA[i] = -MA[i];
+    memset(MB, 0, sizeof(double) * (size_t)mpd * mpd);
+    blk_dot(&Z, &Z, MB, mpd);   /* BVMatProject_Dot */
+    /* 24 */
+    if ((st = ds_ghep(nv, mpd, MA, MB, wr, Q, dsperm))) goto done;
+    for (j = 0; j < nv; j++) if (locked + j < ncv) eigr[locked + j] = flip ? -wr[j] : wr[j];
+    /* 25-33 */
+    blk_active(&Z, bs, nv);
+    if (lock) blk_active(&P, 0, bs);
+    blk_mult(&P, 1.0, 0.0, &Z, Q, mpd);
+    blk_active(&X, 0, bs);
+    blk_copy(&P, &X);
+    if (lock) blk_active(&P, nconv, bs);
+    blk_active(&Z, 0, bs);
+    blk_mult(&X, 1.0, 1.0, &Z, Q, mpd);
+    if (lock) blk_active(&X, nconv, bs);
+    blk_matmult(&op, &X, &AX);
+  }
+
+diverged:
+  eps_its += its;
+  /* EPSSolve post-processing: SlepcSortEigenvalues */
+  for (i = 0; i < eps_nconv; i++) perm[i] = i;
+  for (i = eps_nconv - 1; i >= 0; i--) {
+    double re = eigr[perm[i]];
+    j = i + 1;
+    while (j < eps_nconv) {
+      if (sc_compare(which, re, eigr[perm[j]]) <= 0) break;
+      int tmp = perm[j - 1]; perm[j - 1] = perm[j]; perm[j] = tmp;
+      j++;
+    }
+  }
+  for (i = 0; i < eps_nconv; i++) {
+    if (evals) evals[i] = eigr[perm[i]];
+    if (errest_out) errest_out[i] = errest[perm[i]];
+    if (Xout) memcpy(Xout + (size_t)i * n, BCOL(&V, perm[i]), sizeof(double) * (size_t)n);
+  }
+done:
+#undef LOBPCG_RAYLEIGH_RITZ_X
+  if (info) { info[0] = eps_nconv; info[1] = eps_its; info[2] = reason; info[3] = ncv; }
+  blk_free(&V); blk_free(&Z); blk_free(&X); blk_free(&R); blk_free(&P); blk_free(&AX); blk_free(&Y);
+  free(eigr); free(errest); free(perm); free(MA); free(MB); free(Q); free(wr); free(dsperm); free(dinv);
+  return st;
 }

@@ -71,6 +71,12 @@ _SIGS = {
     "b200_mat_mult_transpose": (ctypes.c_int, [_vp, _vp, _vp]),
     "b200_mat_get_sizes": (ctypes.c_int, [_vp, _ip, _ip]),
     "b200_mat_norm_inf": (ctypes.c_int, [_vp, _dp]),
+    "b200_eps_set_type": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_eps_lobpcg_set_block_size": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_eps_lobpcg_set_restart": (ctypes.c_int, [_vp, ctypes.c_double]),
+    "b200_eps_lobpcg_set_locking": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_eps_set_preconditioner": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_eps_set_initial_space_block": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     "b200_viewer_binary_open": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _vp]),
     "b200_viewer_destroy": (ctypes.c_int, [_vp]),
     "b200_viewer_peek": (ctypes.c_int, [_vp, _ip, _ip, _ip, ctypes.POINTER(ctypes.c_int64)]),
@@ -509,6 +515,12 @@ class EPS:
     class ProblemType:
         HEP = 1
 
+    class Type:
+        KRYLOVSCHUR, LOBPCG = 0, 1
+
+    class PCType:
+        NONE, JACOBI = 0, 1
+
     def __init__(self):
         self.handle = ctypes.c_void_p()
         self._A = None
@@ -540,8 +552,30 @@ class EPS:
         _check(lib().b200_eps_krylovschur_set_restart(self.handle, keep))
 
     def setInitialSpace(self, v0):
-        v0 = np.ascontiguousarray(v0, dtype=np.float64)
+        """One vector (length n) or a block (n x k array, columns are the vectors)."""
+        v0 = np.asarray(v0, dtype=np.float64)
+        if v0.ndim == 2:
+            X = np.asfortranarray(v0)
+            _check(lib().b200_eps_set_initial_space_block(self.handle, X.shape[1], _d(X)))
+            return
+        v0 = np.ascontiguousarray(v0)
         _check(lib().b200_eps_set_initial_space(self.handle, _d(v0)))
+
+    def setType(self, t):
+        _check(lib().b200_eps_set_type(self.handle, t))
+
+    def setLOBPCGBlockSize(self, bs):
+        _check(lib().b200_eps_lobpcg_set_block_size(self.handle, bs))
+
+    def setLOBPCGRestart(self, restart):
+        _check(lib().b200_eps_lobpcg_set_restart(self.handle, restart))
+
+    def setLOBPCGLocking(self, lock):
+        _check(lib().b200_eps_lobpcg_set_locking(self.handle, 1 if lock else 0))
+
+    def setPreconditioner(self, pc):
+        """STPRECOND with KSPPREONLY and PCNONE / PCJACOBI (EPS.PCType)."""
+        _check(lib().b200_eps_set_preconditioner(self.handle, pc))
 
     def setInitialSpaceDevice(self, v0_ptr):
         _check(lib().b200_eps_set_initial_space_device(self.handle, v0_ptr))

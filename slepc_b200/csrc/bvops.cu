@@ -184,6 +184,32 @@ __global__ void diff_sumsq_partial_kernel(const double *__restrict__ y, const do
   }
 }
 
+// y -= alpha x (VecAXPY with -alpha), product and difference rounded separately
+__global__ void axmy_kernel(double *y, const double *__restrict__ x, double alpha, long long len) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x)
+    y[i] = __dsub_rn(y[i], __dmul_rn(alpha, x[i]));
+}
+
+// columns c of V(:, 0:ncols): V(i,c) = d(i) * V(i,c)  (PCApply_Jacobi: pointwise product with diag^{-1})
+__global__ void diag_scale_kernel(double *V, int ld, int n, int ncols, const double *__restrict__ d) {
+  const long long total = (long long)n * ncols;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t / n), i = (int)(t % n);
+    V[i + (size_t)c * ld] = __dmul_rn(d[i], V[i + (size_t)c * ld]);
+  }
+}
+
+// dinv(i) = 1 / a_ii (entries on the diagonal summed in index order; a zero diagonal counts as 1)
+__global__ void inverse_diagonal_kernel(int n, const int *__restrict__ rowptr, const int *__restrict__ colind,
+                                        const double *__restrict__ vals, double *dinv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double d = 0.0;
+    for (int p = rowptr[i]; p < rowptr[i + 1]; ++p)
+      if (colind[p] == i) d = __dadd_rn(d, vals[p]);
+    dinv[i] = 1.0 / (d != 0.0 ? d : 1.0);
+  }
+}
+
 __global__ void sum_final_kernel(const double *__restrict__ partial, int nblocks, double *out) {
   __shared__ double red[32];
   double acc = 0.0;
@@ -393,6 +419,28 @@ cudaError_t residual_launch(int n, const int *rowptr, const int *colind, const d
   }
   count_launch();
   sum_final_kernel<<<1, 256, 0, stream>>>(work, blocks, out);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t axmy_launch(double *y, const double *x, double alpha, long long len, cudaStream_t stream) {
+  if (len <= 0) return cudaSuccess;
+  axmy_kernel<<<grid_for(len, 256), 256, 0, stream>>>(y, x, alpha, len);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t diag_scale_launch(double *V, int ld, int n, int ncols, const double *d, cudaStream_t stream) {
+  if (ncols <= 0 || n <= 0) return cudaSuccess;
+  diag_scale_kernel<<<grid_for((long long)n * ncols, 256), 256, 0, stream>>>(V, ld, n, ncols, d);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t inverse_diagonal_launch(int n, const int *rowptr, const int *colind, const double *vals, double *dinv,
+                                    cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  inverse_diagonal_kernel<<<grid_for(n, 256), 256, 0, stream>>>(n, rowptr, colind, vals, dinv);
   count_launch();
   return cudaGetLastError();
 }

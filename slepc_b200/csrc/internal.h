@@ -10,4 +10,10 @@ namespace b200 {
 b200_status mat_create_cross_ex(b200_mat A, bool swapped, b200_mat *C);
 // y = A x, or y = A^T x (transpose; matrices from b200_mat_create_aij), on the given stream.
 cudaError_t mat_apply(b200_mat A, const double *x, double *y, cudaStream_t stream, bool transpose);
+// BVOrthogonalizeColumn / BVOrthonormalizeColumn (normalize = 1) of column j against columns 0..j-1.
+b200_status bv_orth_column(b200_bv bv, int j, int normalize, double *H, double *norm, int *lindep);
+// EPSSetUp's BVInsertVecs of the initial space into columns 0..k-1 (sets eps->nini_eff).
+b200_status eps_insert_initial_space(b200_eps eps, b200_bv V, int max_cols);
+// EPSSolve with EPSLOBPCG (lobpcg.cu).
+b200_status lobpcg_solve(b200_eps eps);
 }  // namespace b200

@@ -136,6 +136,13 @@ cudaError_t diff_sumsq_launch(const double *y, const double *x, double alpha, lo
 // out[0] = ||A x - lambda x||^2 (fused SpMV + residual), deterministic.
 cudaError_t residual_launch(int n, const int *rowptr, const int *colind, const double *vals, const double *x,
                             double lambda, double *out, double *work, int work_len, int lanes, cudaStream_t stream);
+// y -= alpha x, with the product and the difference rounded separately (VecAXPY(y,-alpha,x)).
+cudaError_t axmy_launch(double *y, const double *x, double alpha, long long len, cudaStream_t stream);
+// V(i,c) = d(i) V(i,c) for columns 0..ncols-1 (Jacobi preconditioner application).
+cudaError_t diag_scale_launch(double *V, int ld, int n, int ncols, const double *d, cudaStream_t stream);
+// dinv(i) = 1 / a_ii of a square FP64 CSR matrix (1 where the diagonal is zero).
+cudaError_t inverse_diagonal_launch(int n, const int *rowptr, const int *colind, const double *vals, double *dinv,
+                                    cudaStream_t stream);
 // Counter-based uniform [0,1) column (stands in for PETSc's VecSetRandom).
 cudaError_t random_launch(double *x, int n, uint64_t seed, uint64_t stream_id, cudaStream_t stream);
 

@@ -22,6 +22,7 @@
 #include "ds_hep.h"
 #include "internal.h"
 #include "kernels.h"
+#include "objects.h"
 
 using namespace b200;
 
@@ -55,39 +56,6 @@ int num_sms_host() {
   } while (0)
 
 // ------------------------------------------------------------------ Mat ---
-// One CSR operand in HBM with its SpMV schedules.  Values are FP64, or FP32
-// (B200_SCALAR_F32: half the value traffic; products and sums stay FP64).
-struct CsrPart {
-  int rows = 0, cols = 0;
-  int64_t nnz = 0;
-  int *rowptr = nullptr, *colind = nullptr;
-  void *vals = nullptr;
-  bool f32 = false;
-  int lanes = 8;
-  int *blocks = nullptr;       // row blocks of the row-block SpMV (nblocks + 1 entries), FP64 only
-  int nblocks = 0;
-  SpmvTiles wt;                // warp tiles, long-row segments and their partial-sum slots
-};
-
-enum MatKind { kMatCsr = 0, kMatCross = 1 };
-
-// kMatCsr: the matrix A (m x n) with, for a rectangular AIJ matrix, its explicit
-// transpose.  kMatCross: the shell C = A^T A (n x n) of MatMult_Cross
-// (src/svd/impls/cross/cross.c:31-41) over a kMatCsr matrix it does not own.
-struct b200_mat_s {
-  int kind = kMatCsr;
-  int m = 0, n = 0;          // rows and columns of the operator
-  int64_t nnz = 0;
-  CsrPart a;                 // A
-  CsrPart at;                // A^T (rectangular AIJ matrices; rows == 0 otherwise)
-  b200_mat base = nullptr;   // kMatCross: the matrix A of A^T A
-  bool swapped = false;      // kMatCross: the operator is A A^T (SVDSetUp's swap for m < n)
-  double *work = nullptr;    // kMatCross: w = A x (base->m entries; base->n when swapped)
-  double norm_inf = -1.0;    // max_i sum_j |a_ij| when known (computed from the host arrays)
-  int schedule = B200_SPMV_WARPTILE;
-  cudaStream_t stream = nullptr;
-};
-
 static void part_free(CsrPart &P) {
   cudaFree(P.rowptr);
   cudaFree(P.colind);
@@ -437,28 +405,6 @@ extern "C" b200_status b200_csr_spmv(int n, const int *rowptr, const int *colind
 }
 
 // ------------------------------------------------------------------- BV ---
-struct b200_bv_s {
-  int n = 0, m = 0, ld = 0;   // m user columns; column m is an internal work column
-  double *V = nullptr;
-  int l = 0, k = 0;
-  double eta = 0.7071;        // bvfunc.c:178
-  cudaStream_t stream = nullptr;
-  GsWork gs{};
-  double *coefbuf = nullptr;  // (m+1) x (m+1): column j = coefficients of column j (BVGetBufferVec)
-  int ldc = 0;
-  double *hvec = nullptr;     // coefficients of the vector variant
-  double *T = nullptr;        // Lanczos alpha (T[j]) and beta (T[ldt+j])
-  int ldt = 0;
-  double *red = nullptr;      // reduction workspace
-  int red_len = 0;
-  double *scal = nullptr;     // device scalars
-  double *qbuf = nullptr;     // device staging of coefficient matrices
-  size_t qbuf_len = 0;
-  double *hpin = nullptr;     // pinned host staging
-  size_t hpin_len = 0;
-  uint64_t seed = 0x5eedULL, nrand = 0;
-};
-
 static void bv_free(b200_bv bv) {
   if (!bv) return;
   cudaFree(bv->V);
@@ -474,6 +420,37 @@ static void bv_free(b200_bv bv) {
   cudaFree(bv->qbuf);
   cudaFreeHost(bv->hpin);
   delete bv;
+}
+
+// Grow the coefficient staging (device qbuf, pinned hpin) to hold q doubles and the reduction
+// workspace to hold red doubles; block operations between BVs of different widths need more
+// than a BV's own (m+1)^2.
+static b200_status bv_reserve(b200_bv bv, size_t q, size_t red) {
+  if (q > bv->qbuf_len || q + 64 > bv->hpin_len) {
+    B200_CUDA_CHECK(cudaStreamSynchronize(bv->stream));
+    double *nq = nullptr, *nh = nullptr;
+    B200_CUDA_CHECK(cudaMalloc(&nq, sizeof(double) * q));
+    if (cudaMallocHost(&nh, sizeof(double) * (q + 64)) != cudaSuccess) {
+      cudaFree(nq);
+      b200_set_last_error(__FILE__, __LINE__, "pinned host allocation failed");
+      return B200_ERR_NOMEM;
+    }
+    cudaFree(bv->qbuf);
+    cudaFreeHost(bv->hpin);
+    bv->qbuf = nq;
+    bv->hpin = nh;
+    bv->qbuf_len = q;
+    bv->hpin_len = q + 64;
+  }
+  if (red > (size_t)bv->red_len) {
+    B200_CUDA_CHECK(cudaStreamSynchronize(bv->stream));
+    double *nr = nullptr;
+    B200_CUDA_CHECK(cudaMalloc(&nr, sizeof(double) * red));
+    cudaFree(bv->red);
+    bv->red = nr;
+    bv->red_len = (int)red;
+  }
+  return B200_OK;
 }
 
 extern "C" b200_status b200_bv_create(int n, int m, void *stream, b200_bv *out) {
@@ -565,7 +542,6 @@ extern "C" b200_status b200_bv_set_orthog_eta(b200_bv bv, double eta) {
   return B200_OK;
 }
 
-static inline double *col(b200_bv bv, int j) { return bv->V + (size_t)j * bv->ld; }
 
 extern "C" b200_status b200_bv_set_column(b200_bv bv, int j, const double *x) {
   B200_ARG_CHECK(bv && x && j >= 0 && j < bv->m, "column index out of range");
@@ -608,7 +584,7 @@ static b200_status bv_read_state(b200_bv bv, GsState *out) {
 }
 
 // Orthogonalise column j against columns 0..j-1 (column variant).
-static b200_status bv_orth_column(b200_bv bv, int j, int normalize, double *H, double *norm, int *lindep) {
+b200_status b200::bv_orth_column(b200_bv bv, int j, int normalize, double *H, double *norm, int *lindep) {
   B200_CUDA_CHECK(gs_state_reset(bv->gs, bv->eta, bv->stream));
   GsPassArgs a{};
   a.V = bv->V;
@@ -714,7 +690,7 @@ extern "C" b200_status b200_bv_mult_inplace(b200_bv bv, const double *Q, int ldq
   B200_ARG_CHECK(s >= bv->l && s <= bv->m && e >= bv->l && e <= bv->m, "s/e out of range");
   if (s >= e) return B200_OK;
   const int kq = bv->k - bv->l, nc = e - s;
-  B200_ARG_CHECK((size_t)kq * nc <= bv->qbuf_len && (size_t)kq * nc <= bv->hpin_len, "Q block too large");
+  B200_CHECK(bv_reserve(bv, (size_t)kq * nc, 0));
   // pack Q(l:k, s:e) into pinned memory, then one host-to-device copy
   B200_CUDA_CHECK(cudaStreamSynchronize(bv->stream));
   for (int j = 0; j < nc; ++j)
@@ -735,7 +711,7 @@ extern "C" b200_status b200_bv_mult(b200_bv Y, double alpha, double beta, b200_b
   const int nx = X->k - X->l, ny = Y->k - Y->l;
   B200_ARG_CHECK(ldq >= X->k, "Q leading dimension too small");
   if (ny <= 0) return B200_OK;
-  B200_ARG_CHECK((size_t)nx * ny <= Y->qbuf_len && (size_t)nx * ny <= Y->hpin_len, "Q block too large");
+  B200_CHECK(bv_reserve(Y, (size_t)nx * ny, 0));
   B200_CUDA_CHECK(cudaStreamSynchronize(Y->stream));
   for (int j = 0; j < ny; ++j)
     for (int i = 0; i < nx; ++i) Y->hpin[i + (size_t)j * nx] = Q[(size_t)(X->l + i) + (size_t)(Y->l + j) * ldq];
@@ -765,7 +741,7 @@ extern "C" b200_status b200_bv_dot(b200_bv X, b200_bv Y, double *M, int ldm) {
   const int nx = X->k - X->l, ny = Y->k - Y->l;
   B200_ARG_CHECK(ldm >= Y->k, "M leading dimension too small");
   if (nx <= 0 || ny <= 0) return B200_OK;
-  B200_ARG_CHECK((size_t)nx * ny <= X->qbuf_len && (size_t)nx * ny <= X->hpin_len, "result too large");
+  B200_CHECK(bv_reserve(X, (size_t)nx * ny, (size_t)nx * ny * num_sms_host()));
   B200_CUDA_CHECK(dot_launch(col(X, X->l), X->ld, nx, col(Y, Y->l), Y->ld, ny, X->n, X->qbuf, ny, X->red, X->red_len,
                              X->stream));
   B200_CUDA_CHECK(
@@ -928,33 +904,6 @@ extern "C" b200_status b200_bv_mat_lanczos(b200_bv bv, b200_mat A, int k, int *m
 }
 
 // ------------------------------------------------------------------ EPS ---
-struct b200_eps_s {
-  cudaStream_t stream = nullptr;
-  b200_mat A = nullptr;
-  int nev = 1, ncv = 0, mpd = 0;
-  double tol = 0.0;
-  int max_it = 0;
-  int which = B200_LARGEST_MAGNITUDE;
-  double keep = 0.5;  // krylovschur.c:122
-  std::vector<double> v0;
-  const double *v0_dev = nullptr;
-  int nini = 0;
-  int max_restarts = 0;
-  b200_bv V = nullptr;
-  DsHep ds;
-  std::vector<double> eigr, errest;
-  std::vector<int> perm;
-  int nconv = 0, its = 0, reason = 0;
-  bool solved = false;
-  int timing = 0;
-  b200_eps_stats stats{};
-  // effective values after setup
-  int n_ = 0, ncv_ = 0, mpd_ = 0, max_it_ = 0;
-  double tol_ = 1e-8;
-  double *resid_buf = nullptr;
-  double *op_buf = nullptr;  // Op x for residuals of operators without a fused residual kernel
-};
-
 extern "C" b200_status b200_eps_create(void *stream, b200_eps *eps) {
   B200_ARG_CHECK(eps, "null argument");
   b200_eps E = new b200_eps_s;
@@ -968,6 +917,7 @@ extern "C" b200_status b200_eps_destroy(b200_eps eps) {
   b200_bv_destroy(eps->V);
   cudaFree(eps->resid_buf);
   cudaFree(eps->op_buf);
+  cudaFree(eps->dinv);
   delete eps;
   return B200_OK;
 }
@@ -1002,6 +952,7 @@ extern "C" b200_status b200_eps_set_tolerances(b200_eps eps, double tol, int max
 extern "C" b200_status b200_eps_set_which_eigenpairs(b200_eps eps, int which) {
   B200_ARG_CHECK(eps && which >= B200_LARGEST_MAGNITUDE && which <= B200_SMALLEST_REAL, "unsupported which");
   eps->which = which;
+  eps->which_set = true;
   eps->solved = false;
   return B200_OK;
 }
@@ -1016,6 +967,8 @@ extern "C" b200_status b200_eps_set_initial_space(b200_eps eps, const double *v0
   B200_ARG_CHECK(eps && v0 && eps->A, "set the operator before the initial space");
   eps->v0.assign(v0, v0 + eps->A->n);
   eps->v0_dev = nullptr;
+  eps->X0.clear();
+  eps->nini_block = 0;
   eps->nini = 1;
   eps->solved = false;
   return B200_OK;
@@ -1025,8 +978,77 @@ extern "C" b200_status b200_eps_set_initial_space_device(b200_eps eps, const dou
   B200_ARG_CHECK(eps && v0 && eps->A, "set the operator before the initial space");
   eps->v0.clear();
   eps->v0_dev = v0;
+  eps->X0.clear();
+  eps->nini_block = 0;
   eps->nini = 1;
   eps->solved = false;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_set_initial_space_block(b200_eps eps, int k, const double *X) {
+  B200_ARG_CHECK(eps && eps->A && k >= 0 && (k == 0 || X), "set the operator before the initial space");
+  eps->v0.clear();
+  eps->v0_dev = nullptr;
+  eps->X0.assign(X, X + (size_t)k * eps->A->n);
+  eps->nini_block = k;
+  eps->nini = k;
+  eps->solved = false;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_set_type(b200_eps eps, int type) {
+  B200_ARG_CHECK(eps && (type == B200_EPS_KRYLOVSCHUR || type == B200_EPS_LOBPCG), "unknown EPS type");
+  eps->type = type;
+  eps->solved = false;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_lobpcg_set_block_size(b200_eps eps, int bs) {
+  B200_ARG_CHECK(eps && bs >= 0, "the block size must be positive");
+  eps->lobpcg_bs = bs;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_lobpcg_set_restart(b200_eps eps, double restart) {
+  B200_ARG_CHECK(eps && restart >= 0.1 && restart <= 1.0, "the restart argument must be in [0.1,1.0]");
+  eps->lobpcg_restart = restart;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_lobpcg_set_locking(b200_eps eps, int lock) {
+  B200_ARG_CHECK(eps, "null argument");
+  eps->lobpcg_lock = lock ? 1 : 0;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_set_preconditioner(b200_eps eps, int pc) {
+  B200_ARG_CHECK(eps && (pc == B200_PC_NONE || pc == B200_PC_JACOBI), "unknown preconditioner");
+  eps->pc = pc;
+  return B200_OK;
+}
+
+// EPSSetUp's BVInsertVecs(V,0,&k,IS,TRUE) (epssetup.c:421-427, bvfunc.c:331-374): the initial
+// space into columns 0..k-1, orthonormalised, linearly dependent vectors dropped.
+b200_status b200::eps_insert_initial_space(b200_eps eps, b200_bv V, int max_cols) {
+  const int nin = eps->nini_block > 0 ? eps->nini_block : (eps->nini ? 1 : 0);
+  B200_ARG_CHECK(nin <= max_cols, "the number of initial vectors is larger than ncv");
+  int ndep = 0;
+  for (int i = 0; i < nin; ++i) {
+    double *dst = col(V, i - ndep);
+    if (eps->nini_block > 0)
+      B200_CUDA_CHECK(cudaMemcpyAsync(dst, eps->X0.data() + (size_t)i * V->n, sizeof(double) * V->n,
+                                      cudaMemcpyHostToDevice, V->stream));
+    else if (eps->v0_dev)
+      B200_CUDA_CHECK(copy_launch(dst, eps->v0_dev, V->n, V->stream));
+    else
+      B200_CUDA_CHECK(cudaMemcpyAsync(dst, eps->v0.data(), sizeof(double) * V->n, cudaMemcpyHostToDevice, V->stream));
+    double norm = 0.0;
+    int lindep = 0;
+    B200_CHECK(bv_orth_column(V, i - ndep, 0, nullptr, &norm, &lindep));
+    if (norm == 0.0 || lindep) ++ndep;
+    else B200_CHECK(b200_bv_scale_column(V, i - ndep, 1.0 / norm));
+  }
+  eps->nini_eff = nin - ndep;
   return B200_OK;
 }
 
@@ -1089,7 +1111,7 @@ static b200_status eps_setup(b200_eps eps) {
 // EPSGetStartVector (epssolve.c:841-870): column i, random unless i == 0 and an initial vector exists.
 static b200_status eps_start_vector(b200_eps eps, int i, int *breakdown) {
   b200_bv bv = eps->V;
-  if (i > 0 || eps->nini == 0) B200_CUDA_CHECK(random_launch(col(bv, i), bv->n, bv->seed, bv->nrand++, bv->stream));
+  if (i > 0 || eps->nini_eff == 0) B200_CUDA_CHECK(random_launch(col(bv, i), bv->n, bv->seed, bv->nrand++, bv->stream));
   double norm = 0.0;
   int lindep = 0;
   B200_CHECK(bv_orth_column(bv, i, 0, nullptr, &norm, &lindep));
@@ -1105,6 +1127,7 @@ static b200_status eps_start_vector(b200_eps eps, int i, int *breakdown) {
 
 extern "C" b200_status b200_eps_solve(b200_eps eps) {
   B200_ARG_CHECK(eps, "null argument");
+  if (eps->type == B200_EPS_LOBPCG) return lobpcg_solve(eps);
   B200_CHECK(eps_setup(eps));
   b200_bv V = eps->V;
   DsHep &ds = eps->ds;
@@ -1132,21 +1155,8 @@ extern "C" b200_status b200_eps_solve(b200_eps eps) {
   V->nrand = 0;
   b200_bv_set_active_columns(V, 0, V->m);
 
-  // EPSSetUp: BVInsertVecs(V,0,&k,IS,TRUE) (epssetup.c:424, bvfunc.c:331-374)
-  if (eps->nini) {
-    if (eps->v0_dev) B200_CUDA_CHECK(copy_launch(col(V, 0), eps->v0_dev, V->n, V->stream));
-    else
-      B200_CUDA_CHECK(
-          cudaMemcpyAsync(col(V, 0), eps->v0.data(), sizeof(double) * V->n, cudaMemcpyHostToDevice, V->stream));
-    double norm = 0.0;
-    int lindep = 0;
-    B200_CHECK(bv_orth_column(V, 0, 0, nullptr, &norm, &lindep));
-    if (norm == 0.0 || lindep) {
-      b200_set_last_error(__FILE__, __LINE__, "the initial vector is zero");
-      return B200_ERR_BREAKDOWN;
-    }
-    B200_CHECK(b200_bv_scale_column(V, 0, 1.0 / norm));
-  }
+  // EPSSetUp: BVInsertVecs(V,0,&k,IS,TRUE); then EPSGetStartVector(eps,0,NULL)
+  B200_CHECK(eps_insert_initial_space(eps, V, ncv));
   B200_CHECK(eps_start_vector(eps, 0, nullptr));
 
   int l = 0;

@@ -207,3 +207,60 @@ def powerlaw_rect_py(m, n, nnz_row=20, alpha=1.8, seed=0):
             u2 = uniform(1, i, 2 * j + 1)
             vals[i * k + j] = np.float32(math.sqrt(-2.0 * math.log(u1)) * math.cos(6.283185307179586 * u2))
     return rowptr, colind, vals
+
+
+# ---------------------------------------------------------------- anisotropic diffusion (learned warm start workload)
+def gaussian_random_field(N, corr_len, seed, variance=1.0):
+    """N x N samples on the cell centres of the unit square of a stationary Gaussian field with
+    squared-exponential covariance variance * exp(-r^2 / (2 corr_len^2)): white noise filtered
+    spectrally on a 2N x 2N periodic grid (so the wrap-around correlation stays outside the
+    square), then shifted and scaled to mean 0 and the given variance."""
+    rng = np.random.default_rng(seed)
+    M = 2 * N
+    xi = rng.standard_normal((M, M))
+    k = np.fft.fftfreq(M, d=1.0 / N)  # cycles per unit length
+    k2 = k[:, None] ** 2 + k[None, :] ** 2
+    field = np.fft.ifft2(np.fft.fft2(xi) * np.exp(-np.pi ** 2 * corr_len ** 2 * k2)).real[:N, :N]
+    field = field - field.mean()
+    return field * np.sqrt(variance) / field.std()
+
+
+def diffusion_fv(kappa):
+    """5-point finite-volume matrix of -div(kappa grad u) on the N x N cell grid of the unit
+    square with u = 0 on the boundary, multiplied by h^2: face coefficients are harmonic means
+    of the two cell values, a boundary face contributes 2 kappa_cell.  Row-major cell
+    ordering; returns (rowptr, colind, vals)."""
+    kap = np.asarray(kappa, dtype=np.float64)
+    N = kap.shape[0]
+    idx = np.arange(N * N).reshape(N, N)
+    hx = 2.0 * kap[:, :-1] * kap[:, 1:] / (kap[:, :-1] + kap[:, 1:])   # faces between (i,j) and (i,j+1)
+    hy = 2.0 * kap[:-1, :] * kap[1:, :] / (kap[:-1, :] + kap[1:, :])   # faces between (i,j) and (i+1,j)
+    diag = np.zeros((N, N))
+    diag[:, :-1] += hx
+    diag[:, 1:] += hx
+    diag[:-1, :] += hy
+    diag[1:, :] += hy
+    diag[:, 0] += 2 * kap[:, 0]
+    diag[:, -1] += 2 * kap[:, -1]
+    diag[0, :] += 2 * kap[0, :]
+    diag[-1, :] += 2 * kap[-1, :]
+    rows = [idx.ravel(), idx[:, :-1].ravel(), idx[:, 1:].ravel(), idx[:-1, :].ravel(), idx[1:, :].ravel()]
+    cols = [idx.ravel(), idx[:, 1:].ravel(), idx[:, :-1].ravel(), idx[1:, :].ravel(), idx[:-1, :].ravel()]
+    vals = [diag.ravel(), -hx.ravel(), -hx.ravel(), -hy.ravel(), -hy.ravel()]
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    v = np.concatenate(vals)
+    order = np.lexsort((c, r))
+    r, c, v = r[order], c[order], v[order]
+    rowptr = np.zeros(N * N + 1, dtype=np.int32)
+    np.cumsum(np.bincount(r, minlength=N * N), out=rowptr[1:])
+    return rowptr, c.astype(np.int32), v
+
+
+def diffusion_problem(N, seed):
+    """kappa = exp(GRF) with variance 1 and a correlation length drawn uniformly from
+    [0.05, 0.2] (from the seed), and its finite-volume matrix: (csr, kappa, corr_len)."""
+    rng = np.random.default_rng([seed, 0x4b])
+    corr_len = float(rng.uniform(0.05, 0.2))
+    kappa = np.exp(gaussian_random_field(N, corr_len, [seed, 0x47]))
+    return diffusion_fv(kappa), kappa, corr_len

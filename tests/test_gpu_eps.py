@@ -218,16 +218,20 @@ def test_max_iterations_and_restart_cap():
     assert E.getConvergedReason() == S.DIVERGED_ITS and E.getIterationNumber() == 3
 
 
-def test_zero_initial_vector_is_an_error():
+def test_zero_initial_vector_falls_back_to_a_random_start(oracle_mod):
+    """BVInsertVecs drops a zero initial vector (bvfunc.c:331-374), so EPSGetStartVector draws a
+    random one (epssolve.c:852): the solve proceeds, from the same random vector as the oracle."""
     csr = P.laplacian_2d(20)
     A = S.Mat().createAIJ(csr)
     E = S.EPS().create()
     E.setOperators(A)
     E.setDimensions(2, 10)
     E.setInitialSpace(np.zeros(A.n))
-    with pytest.raises(S.B200Error) as ei:
-        E.solve()
-    assert ei.value.status == 5
+    E.solve()
+    assert E.getConvergedReason() == S.CONVERGED_TOL and E.getConverged() >= 2
+    ref = oracle_mod.eps_solve(P.to_scipy(csr), np.zeros(A.n), nev=2, ncv=10)
+    assert E.getIterationNumber() == ref.its
+    np.testing.assert_allclose([E.getEigenvalue(i) for i in range(2)], ref.evals[:2], rtol=1e-10)
 
 
 def test_invariant_subspace_start_vector_still_converges():

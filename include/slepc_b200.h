@@ -84,6 +84,7 @@ typedef struct b200_mat_s *b200_mat;
 typedef struct b200_bv_s *b200_bv;
 typedef struct b200_eps_s *b200_eps;
 typedef struct b200_svd_s *b200_svd;
+typedef struct b200_batch_s *b200_batch;
 
 /* Library information and the last error message (thread-local). */
 const char *b200_version(void);
@@ -377,6 +378,43 @@ b200_status b200_svd_solve_aij_host(int m, int n, int64_t nnz, const int *rowptr
                                     const void *vals_host, int scalar_type, const double *v0_host, int nsv, int ncv,
                                     double tol, int max_it, double *sigma_host, double *U_host, double *V_host,
                                     double *rel_error_host, int *info_host, void *stream);
+
+/* -------------------------------------------------------------- batched --- */
+
+/* Many independent small Hermitian eigenproblems solved by Krylov-Schur in one
+ * persistent launch (no SLEPc counterpart as one call: it stands for a loop
+ * of EPSSolve over the problems).  Each CTA of the launch takes a problem
+ * from a work queue (largest first) and runs the whole solve for it on the
+ * device: Lanczos with CGS+DGKS, the projected problem (implicit QL in place
+ * of LAPACK dsteqr), sort, convergence test, truncation and the restart.
+ * The launch is captured in a CUDA graph and replayed; the CTA size is
+ * chosen by an autotuner unless set.
+ *   rowptr: the problems' row pointers one after another (ns[p]+1 local
+ *   offsets each); colind (local indices) and vals: their nonzeros one after
+ *   another; rows of at most 256 nonzeros.  Copied to HBM. */
+b200_status b200_batch_create(int nprob, const int *ns_host, const int *rowptr_host, const int *colind_host,
+                              const double *vals_host, void *stream, b200_batch *B);
+b200_status b200_batch_destroy(b200_batch B);
+/* EPSSetDimensions for every problem (ncv <= 31; ncv <= the smallest n). */
+b200_status b200_batch_set_dimensions(b200_batch B, int nev, int ncv, int mpd);
+b200_status b200_batch_set_tolerances(b200_batch B, double tol, int max_it);
+b200_status b200_batch_set_which_eigenpairs(b200_batch B, int which);
+/* Start vectors, one after another (sum of ns doubles); all zero by default,
+ * which means random starts (a zero initial vector is dropped). */
+b200_status b200_batch_set_initial_vectors(b200_batch B, const double *v0_host);
+/* CTA size per problem: 128, 256, 512, or 0 for the autotuner (default). */
+b200_status b200_batch_set_threads(b200_batch B, int threads);
+/* Times each CTA size on the largest problems and keeps the fastest. */
+b200_status b200_batch_autotune(b200_batch B, int *threads);
+b200_status b200_batch_solve(b200_batch B);
+/* Results of problem p: converged count, restarts, reason, Lanczos steps, and the
+ * sorted eigenvalues / error estimates (nconv values each, nullable). */
+b200_status b200_batch_get_solution(b200_batch B, int p, int *nconv, int *its, int *reason, int *lanczos_steps,
+                                    double *evals_host, double *errest_host);
+b200_status b200_batch_get_eigenvector(b200_batch B, int p, int i, double *x_host);
+/* All results at once: evals_host (nprob x ncv), info_host (nprob x 8: nconv, its, reason,
+ * steps, device error), and the device time of the last solve in ms. */
+b200_status b200_batch_get_all(b200_batch B, double *evals_host, int *info_host, float *ms);
 
 #ifdef __cplusplus
 }

@@ -45,6 +45,9 @@ def lib():
         L.oracle_lobpcg.argtypes = [ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_double, _dp, ctypes.c_int, _dp, _dp, _dp, _ip]
+        L.oracle_eps_solve_batch.restype = ctypes.c_int
+        L.oracle_eps_solve_batch.argtypes = [ctypes.c_int, _ip, _ip, _ip, _dp, _dp, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_double, ctypes.c_int, _dp, _ip]
         L.oracle_csr_transpose.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, _ip, _ip, _dp]
         L.oracle_svd_cross.restype = ctypes.c_int
         L.oracle_svd_cross.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, _ip, _ip, _dp, _dp,
@@ -241,3 +244,21 @@ def lobpcg(A, nev, bs=0, ncv=0, tol=1e-8, max_it=0, which=SMALLEST_REAL, pc="jac
         raise RuntimeError(f"oracle_lobpcg failed with status {st}")
     k = int(info[0])
     return SolveResult(evals[:k].copy(), X[:k].T.copy(), errest[:k].copy(), k, int(info[1]), int(info[2]), 0, 0, 0)
+
+
+def eps_solve_batch(ns, rowptr, colind, vals, v0, nev, ncv, tol=1e-8, which=LARGEST_REAL, threads=0):
+    """oracle_eps_solve on every problem of a batch in parallel over problems: (evals (nprob x ncv), info (nprob x 6))."""
+    ns = np.ascontiguousarray(ns, dtype=np.int32)
+    nprob = len(ns)
+    evals = np.zeros((nprob, ncv))
+    info = np.zeros((nprob, 6), dtype=np.int32)
+    if threads:
+        set_threads(threads)
+    bad = lib().oracle_eps_solve_batch(nprob, _i(ns), _i(np.ascontiguousarray(rowptr, dtype=np.int32)),
+                                       _i(np.ascontiguousarray(colind, dtype=np.int32)),
+                                       _d(np.ascontiguousarray(vals, dtype=np.float64)),
+                                       _d(np.ascontiguousarray(v0, dtype=np.float64)), nev, ncv, tol, which,
+                                       _d(evals), _i(info))
+    if bad:
+        raise RuntimeError(f"{bad} oracle batch problems failed")
+    return evals, info

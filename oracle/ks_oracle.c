@@ -1315,3 +1315,42 @@ done:
   free(eigr); free(errest); free(perm); free(MA); free(MB); free(Q); free(wr); free(dsperm); free(dinv);
   return st;
 }
+
+/*
+ * oracle_eps_solve_batch: oracle_eps_solve on every problem of a batch, the
+ * problems spread over the host threads (each problem single-threaded).
+ * rowptr: the problems' local row pointers one after another (ns[p]+1 each);
+ * colind/vals: their nonzeros one after another; v0: start vectors one after
+ * another.  Outputs per problem p: evals[p*ncv ...] (nconv sorted values),
+ * info[p*6 ...] as oracle_eps_solve.  Returns the number of failed problems.
+ */
+int oracle_eps_solve_batch(int nprob, const int *ns, const int *rowptr, const int *colind, const double *vals,
+                           const double *v0, int nev, int ncv, double tol, int which, double *evals, int *info)
+{
+  long long *rp_off = (long long *)malloc(sizeof(long long) * (size_t)(nprob + 1));
+  long long *nz_off = (long long *)malloc(sizeof(long long) * (size_t)(nprob + 1));
+  long long *x_off = (long long *)malloc(sizeof(long long) * (size_t)(nprob + 1));
+  int p, bad = 0;
+  rp_off[0] = nz_off[0] = x_off[0] = 0;
+  for (p = 0; p < nprob; p++) {
+    rp_off[p + 1] = rp_off[p] + ns[p] + 1;
+    nz_off[p + 1] = nz_off[p] + rowptr[rp_off[p] + ns[p]];
+    x_off[p + 1] = x_off[p] + ns[p];
+  }
+#ifdef _OPENMP
+  int levels = omp_get_max_active_levels();
+  omp_set_max_active_levels(1);
+#endif
+  scipy_openblas_set_num_threads(1);
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : bad)
+  for (p = 0; p < nprob; p++) {
+    int st = oracle_eps_solve(ns[p], rowptr + rp_off[p], colind + nz_off[p], vals + nz_off[p], v0 + x_off[p], nev, ncv,
+                              0, tol, 0, which, 0, evals + (size_t)p * ncv, NULL, NULL, info + (size_t)p * 6);
+    if (st) bad++;
+  }
+#ifdef _OPENMP
+  omp_set_max_active_levels(levels);
+#endif
+  free(rp_off); free(nz_off); free(x_off);
+  return bad;
+}

@@ -86,6 +86,18 @@ _SIGS = {
     "b200_vec_write": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     "b200_mat_load": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     "b200_mat_view": (ctypes.c_int, [_vp, _vp]),
+    "b200_batch_create": (ctypes.c_int, [ctypes.c_int, _ip, _ip, _ip, _dp, _vp, _vp]),
+    "b200_batch_destroy": (ctypes.c_int, [_vp]),
+    "b200_batch_set_dimensions": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "b200_batch_set_tolerances": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int]),
+    "b200_batch_set_which_eigenpairs": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_batch_set_initial_vectors": (ctypes.c_int, [_vp, _dp]),
+    "b200_batch_set_threads": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_batch_autotune": (ctypes.c_int, [_vp, _ip]),
+    "b200_batch_solve": (ctypes.c_int, [_vp]),
+    "b200_batch_get_solution": (ctypes.c_int, [_vp, ctypes.c_int, _ip, _ip, _ip, _ip, _dp, _dp]),
+    "b200_batch_get_eigenvector": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _dp]),
+    "b200_batch_get_all": (ctypes.c_int, [_vp, _dp, _ip, ctypes.POINTER(ctypes.c_float)]),
     "b200_svd_create": (ctypes.c_int, [_vp, _vp]),
     "b200_svd_destroy": (ctypes.c_int, [_vp]),
     "b200_svd_set_operator": (ctypes.c_int, [_vp, _vp]),
@@ -799,3 +811,81 @@ def svd_solve_aij_host(csr, size, v0, nsv, ncv, tol=0.0, max_it=0, dtype=np.floa
     return {"sigma": sig[:k].copy(), "U": U[:k].T.copy() if want_vectors else None,
             "V": V[:k].T.copy() if want_vectors else None, "rel_error": err[:k].copy(), "nconv": k,
             "its": int(info[1]), "reason": int(info[2]), "lanczos_steps": int(info[3]), "restarts": int(info[4])}
+
+
+class BatchEPS:
+    """Many independent small Hermitian eigenproblems by Krylov-Schur in one persistent launch."""
+
+    def __init__(self):
+        self.handle = ctypes.c_void_p()
+        self.ns = None
+        self.ncv = 0
+
+    def create(self, ns, rowptr, colind, vals, stream=None):
+        """ns: problem sizes; rowptr: local row pointers one after another; colind/vals: nonzeros."""
+        self.ns = np.ascontiguousarray(ns, dtype=np.int32)
+        self._keep = (np.ascontiguousarray(rowptr, dtype=np.int32), np.ascontiguousarray(colind, dtype=np.int32),
+                      np.ascontiguousarray(vals, dtype=np.float64))
+        _check(lib().b200_batch_create(len(self.ns), _i(self.ns), _i(self._keep[0]), _i(self._keep[1]),
+                                       _d(self._keep[2]), stream, ctypes.byref(self.handle)))
+        self._keep = None
+        return self
+
+    def setDimensions(self, nev, ncv=0, mpd=0):
+        _check(lib().b200_batch_set_dimensions(self.handle, nev, ncv, mpd))
+        self.nev = nev
+        self.ncv = ncv or max(2 * nev, nev + 15)
+
+    def setTolerances(self, tol=0.0, max_it=0):
+        _check(lib().b200_batch_set_tolerances(self.handle, tol, max_it))
+
+    def setWhichEigenpairs(self, which):
+        _check(lib().b200_batch_set_which_eigenpairs(self.handle, which))
+
+    def setInitialVectors(self, v0):
+        v0 = np.ascontiguousarray(v0, dtype=np.float64)
+        _check(lib().b200_batch_set_initial_vectors(self.handle, _d(v0)))
+
+    def setThreads(self, threads):
+        _check(lib().b200_batch_set_threads(self.handle, threads))
+
+    def autotune(self):
+        t = ctypes.c_int()
+        _check(lib().b200_batch_autotune(self.handle, ctypes.byref(t)))
+        return t.value
+
+    def solve(self):
+        _check(lib().b200_batch_solve(self.handle))
+
+    def getSolution(self, p):
+        nconv, its, reason, steps = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        ev = np.zeros(max(self.ncv, 1))
+        er = np.zeros(max(self.ncv, 1))
+        _check(lib().b200_batch_get_solution(self.handle, p, ctypes.byref(nconv), ctypes.byref(its),
+                                             ctypes.byref(reason), ctypes.byref(steps), _d(ev), _d(er)))
+        k = nconv.value
+        return {"nconv": k, "its": its.value, "reason": reason.value, "lanczos_steps": steps.value,
+                "evals": ev[:k].copy(), "errest": er[:k].copy()}
+
+    def getEigenvector(self, p, i):
+        x = np.zeros(int(self.ns[p]))
+        _check(lib().b200_batch_get_eigenvector(self.handle, p, i, _d(x)))
+        return x
+
+    def getAll(self):
+        ev = np.zeros((len(self.ns), self.ncv))
+        info = np.zeros((len(self.ns), 8), dtype=np.int32)
+        ms = ctypes.c_float()
+        _check(lib().b200_batch_get_all(self.handle, _d(ev), _i(info), ctypes.byref(ms)))
+        return ev, info, ms.value
+
+    def destroy(self):
+        if self.handle:
+            lib().b200_batch_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

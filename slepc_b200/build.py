@@ -43,15 +43,15 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-GEN_SRC = os.path.join(HERE, "gen_powerlaw.c")
-GEN_LIB = os.path.join(HERE, "libgen_powerlaw.so")
+GEN_SRCS = [os.path.join(HERE, "gen_powerlaw.c"), os.path.join(HERE, "gen_knn.c")]
+GEN_LIB = os.path.join(HERE, "libproblem_gen.so")
 
 
 def build_generator(force=False):
-    """Host-side generator of the power-law test matrix (gcc + OpenMP)."""
-    if force or _stale(GEN_LIB, [GEN_SRC]):
-        subprocess.check_call(["gcc", "-O2", "-fopenmp", "-fPIC", "-shared", "-std=c11", "-Wall", GEN_SRC, "-o",
-                               GEN_LIB, "-lm"])
+    """Host-side generators of the test matrices (power-law rectangular, k-NN graph batches; gcc + OpenMP)."""
+    if force or _stale(GEN_LIB, GEN_SRCS):
+        subprocess.check_call(["gcc", "-O2", "-fopenmp", "-fPIC", "-shared", "-std=c11", "-Wall"] + GEN_SRCS +
+                              ["-o", GEN_LIB, "-lm"])
     return GEN_LIB
 
 

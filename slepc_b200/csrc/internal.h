@@ -14,6 +14,8 @@ cudaError_t mat_apply(b200_mat A, const double *x, double *y, cudaStream_t strea
 b200_status bv_orth_column(b200_bv bv, int j, int normalize, double *H, double *norm, int *lindep);
 // EPSSetUp's BVInsertVecs of the initial space into columns 0..k-1 (sets eps->nini_eff).
 b200_status eps_insert_initial_space(b200_eps eps, b200_bv V, int max_cols);
+// Streaming multiprocessors of the current device.
+int num_sms_host();
 // EPSSolve with EPSLOBPCG (lobpcg.cu).
 b200_status lobpcg_solve(b200_eps eps);
 }  // namespace b200

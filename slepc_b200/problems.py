@@ -264,3 +264,90 @@ def diffusion_problem(N, seed):
     corr_len = float(rng.uniform(0.05, 0.2))
     kappa = np.exp(gaussian_random_field(N, corr_len, [seed, 0x47]))
     return diffusion_fv(kappa), kappa, corr_len
+
+
+# ---------------------------------------------------------------- k-NN graph batches (batched workload)
+def _knnlib():
+    import ctypes
+
+    L = _genlib()
+    if not hasattr(L, "_knn_ready"):
+        L.knn_build.restype = ctypes.c_int64
+        L.knn_build.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int64, ctypes.c_void_p,
+                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
+        L.knn_points.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_int64, ctypes.c_void_p]
+        L.knn_build_batch.restype = ctypes.c_int
+        L.knn_build_batch.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p]
+        L._knn_ready = True
+    return L
+
+
+def knn_operator(n, k=8, seed=0, problem=0):
+    """2I - L_norm of the symmetrised k-NN graph of n random points (problem `problem` of the
+    batch with this seed): (rowptr, colind, vals)."""
+    L = _knnlib()
+    cap = n * (4 * k + 2)
+    while True:
+        rowptr = np.empty(n + 1, dtype=np.int32)
+        colind = np.empty(cap, dtype=np.int32)
+        vals = np.empty(cap)
+        nnz = L.knn_build(n, k, seed, problem, rowptr.ctypes.data, colind.ctypes.data, vals.ctypes.data, cap)
+        if nnz < 0:
+            raise ValueError("invalid k-NN parameters")
+        if nnz <= cap:
+            return rowptr, colind[:nnz].copy(), vals[:nnz].copy()
+        cap = int(nnz)
+
+
+def knn_points(n, seed=0, problem=0):
+    xy = np.empty(2 * n)
+    _knnlib().knn_points(n, seed, problem, xy.ctypes.data)
+    return xy.reshape(n, 2)
+
+
+def batch_sizes(nprob, seed=0, lo=500, hi=20000):
+    """Problem sizes n ~ U[lo, hi] (integers, inclusive) from the seed."""
+    return np.random.default_rng([seed, 0x5a]).integers(lo, hi + 1, size=nprob).astype(np.int32)
+
+
+class Batch:
+    """Concatenated CSR of a batch: problem p has rows [row_off[p], row_off[p] + ns[p]) of the
+    batch, its own row pointer at rowptr[row_off[p] + p : row_off[p] + p + ns[p] + 1] (local
+    offsets from nnz_off[p]) and local column indices."""
+
+    def __init__(self, ns, rowptr, colind, vals, row_off, nnz_off):
+        self.ns, self.rowptr, self.colind, self.vals = ns, rowptr, colind, vals
+        self.row_off, self.nnz_off = row_off, nnz_off
+
+    @property
+    def nprob(self):
+        return len(self.ns)
+
+    def problem(self, p):
+        r0 = int(self.row_off[p]) + p
+        n = int(self.ns[p])
+        z0, z1 = int(self.nnz_off[p]), int(self.nnz_off[p + 1])
+        return self.rowptr[r0:r0 + n + 1].copy(), self.colind[z0:z1].copy(), self.vals[z0:z1].copy()
+
+
+def knn_batch(ns, k=8, seed=0):
+    """The batch of k-NN operators for sizes ns (OpenMP over problems)."""
+    L = _knnlib()
+    ns = np.ascontiguousarray(ns, dtype=np.int32)
+    nprob = len(ns)
+    counts = np.zeros(nprob, dtype=np.int64)
+    if L.knn_build_batch(nprob, ns.ctypes.data, k, seed, counts.ctypes.data, None, None, None, None, None):
+        raise ValueError("invalid k-NN parameters")
+    row_off = np.zeros(nprob + 1, dtype=np.int64)
+    np.cumsum(ns, out=row_off[1:])
+    nnz_off = np.zeros(nprob + 1, dtype=np.int64)
+    np.cumsum(counts, out=nnz_off[1:])
+    rowptr = np.zeros(int(row_off[-1]) + nprob, dtype=np.int32)
+    colind = np.zeros(int(nnz_off[-1]), dtype=np.int32)
+    vals = np.zeros(int(nnz_off[-1]))
+    if L.knn_build_batch(nprob, ns.ctypes.data, k, seed, counts.ctypes.data, row_off.ctypes.data, nnz_off.ctypes.data,
+                         rowptr.ctypes.data, colind.ctypes.data, vals.ctypes.data):
+        raise RuntimeError("k-NN batch build failed")
+    return Batch(ns, rowptr, colind, vals, row_off, nnz_off)

@@ -20,7 +20,9 @@
 // Determinism: every reduction is a fixed tree (per-thread row order, fixed
 // shuffle tree, warps summed in order), the QL and sort run redundantly on
 // the lanes of one warp (each lane owns one row of Q), so a batch gives the
-// same bits run to run.
+// same bits run to run.  The basis is written and re-read by the same CTA
+// between barriers; its loads go through L2 (ld.global.cg) so that they
+// always see the CTA's own stores.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -59,8 +61,10 @@ struct BParams {
 
 template <int T>
 struct BShared {
-  double red[T / 32][kBCols + 1];
-  double c[kBCols + 1];
+  double red[T / 32][kBCols + 8];
+  double c[kBCols + 8];
+  double scal[8];    // scalars decided by thread 0 and read by every thread
+  int flag[8];
   double d[kBLd], e[kBLd], Q[kBLd * kBLd], eigr[kBLd], errest[kBLd], wr[kBLd];
   double prod[T / 32][kWarpTileNnz];
   int perm[kBLd];
@@ -99,7 +103,7 @@ __device__ void cta_spmv(const BProblem &P, const int *__restrict__ rowptr, cons
     const int nxt = __shfl_down_sync(0xffffffffu, mystart, 1);
     const int myend = (lane + 1 < nrows) ? nxt : p1;
     const int cnt = p1 - p0;
-    for (int q = lane; q < cnt; q += 32) prod[q] = __dmul_rn(va[p0 + q], x[ci[p0 + q]]);
+    for (int q = lane; q < cnt; q += 32) prod[q] = __dmul_rn(va[p0 + q], __ldcg(x + ci[p0 + q]));
     __syncwarp();
     if (lane < nrows) {
       double s = 0.0;
@@ -111,31 +115,34 @@ __device__ void cta_spmv(const BProblem &P, const int *__restrict__ rowptr, cons
   __syncthreads();
 }
 
-// sh.c[i] = V(:,c0+i)' w for i < ncols (deterministic); w may be one of the columns
+// sh.c[i] = V(:,c0+i)' w for i < ncols (deterministic); w may be one of the columns.  Columns
+// go in groups of 8: per-thread partial sums in row order, a fixed shuffle tree per warp, the
+// warps added in order.
 template <int T>
 __device__ void cta_dots(const double *V, int ld, int n, int c0, int ncols, const double *w, BShared<T> &sh) {
-  double acc[kBCols + 1];
-#pragma unroll
-  for (int i = 0; i <= kBCols; ++i) acc[i] = 0.0;
-  for (int r = threadIdx.x; r < n; r += T) {
-    const double wr = w[r];
-#pragma unroll
-    for (int i = 0; i <= kBCols; ++i)
-      if (i < ncols) acc[i] = fma(V[r + (size_t)(c0 + i) * ld], wr, acc[i]);
-  }
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  for (int g0 = 0; g0 < ncols; g0 += 8) {
+    const int gn = min(8, ncols - g0);
+    double acc[8];
 #pragma unroll
-  for (int i = 0; i <= kBCols; ++i) {
-    if (i < ncols) {
+    for (int i = 0; i < 8; ++i) acc[i] = 0.0;
+    for (int r = threadIdx.x; r < n; r += T) {
+      const double wr = __ldcg(w + r);
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+        if (i < gn) acc[i] = fma(__ldcg(V + r + (size_t)(c0 + g0 + i) * ld), wr, acc[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
       const double v = bwarp_sum(acc[i]);
-      if (lane == 0) sh.red[wib][i] = v;
+      if (lane == 0) sh.red[wib][g0 + i] = v;
     }
   }
   __syncthreads();
   if (threadIdx.x < ncols) {
-    double s = 0.0;
-    for (int w2 = 0; w2 < T / 32; ++w2) s += sh.red[w2][threadIdx.x];
-    sh.c[threadIdx.x] = s;
+    double sacc = 0.0;
+    for (int w2 = 0; w2 < T / 32; ++w2) sacc += sh.red[w2][threadIdx.x];
+    sh.c[threadIdx.x] = sacc;
   }
   __syncthreads();
 }
@@ -145,21 +152,21 @@ template <int T>
 __device__ void cta_update(const double *V, int ld, int n, int ncols, const double *coef, double *w) {
   for (int r = threadIdx.x; r < n; r += T) {
     double acc = 0.0;
-    for (int i = 0; i < ncols; ++i) acc = fma(V[r + (size_t)i * ld], coef[i], acc);
-    w[r] = w[r] - acc;
+    for (int i = 0; i < ncols; ++i) acc = fma(__ldcg(V + r + (size_t)i * ld), coef[i], acc);
+    w[r] = __ldcg(w + r) - acc;
   }
   __syncthreads();
 }
 
 template <int T>
 __device__ void cta_scale(double *w, int n, double alpha) {
-  for (int r = threadIdx.x; r < n; r += T) w[r] *= alpha;
+  for (int r = threadIdx.x; r < n; r += T) w[r] = __ldcg(w + r) * alpha;
   __syncthreads();
 }
 
 template <int T>
 __device__ void cta_copy(double *dst, const double *src, int n) {
-  for (int r = threadIdx.x; r < n; r += T) dst[r] = src[r];
+  for (int r = threadIdx.x; r < n; r += T) dst[r] = __ldcg(src + r);
   __syncthreads();
 }
 
@@ -181,32 +188,47 @@ __device__ void cta_orthonormalize(double *V, int ld, int n, int j, double eta, 
                                    int *err, BShared<T> &sh) {
   double *w = V + (size_t)j * ld;
   for (int i = 0; i < j; ++i) h[i] = 0.0;
-  double onrm = 0.0, nrm = 0.0;
-  int passes = 0;
-  double cl[kBCols + 1];
-  do {
+  int more = 1, passes = 0;
+  while (more) {
     cta_dots<T>(V, ld, n, 0, j + 1, w, sh);  // includes w against itself
-    for (int i = 0; i <= j; ++i) cl[i] = sh.c[i];
-    const double self = cl[j];
-    if (self < 0.0) *err = 1;
-    onrm = sqrt(self < 0.0 ? 0.0 : self);
+    for (int i = 0; i < j; ++i) h[i] += sh.c[i];
     cta_update<T>(V, ld, n, j, sh.c, w);
-    double sum = 0.0;
-    for (int i = 0; i < j; ++i) sum += cl[i] * cl[i];
-    double est = onrm * onrm - sum;
-    if (est <= 0.0) {
-      cta_dots<T>(V, ld, n, j, 1, w, sh);  // explicit norm
-      est = sqrt(sh.c[0]);
-    } else {
-      est = sqrt(est);
+    // thread 0: the Pythagorean estimate of the new norm (bvorthog.c:124-127)
+    if (threadIdx.x == 0) {
+      const double self = sh.c[j];
+      if (self < 0.0) sh.flag[2] = 1;
+      const double onrm = sqrt(self < 0.0 ? 0.0 : self);
+      double sum = 0.0;
+      for (int i = 0; i < j; ++i) sum += sh.c[i] * sh.c[i];
+      const double est = onrm * onrm - sum;
+      sh.scal[0] = onrm;
+      sh.scal[1] = est;
+      sh.flag[0] = est <= 0.0;
     }
-    nrm = est;
-    for (int i = 0; i < j; ++i) h[i] += cl[i];
-    ++passes;
     __syncthreads();
-  } while (passes < 3 && nrm != 0.0 && fabs(nrm) < eta * fabs(onrm));
-  *lindep = !(nrm != 0.0 && fabs(nrm) >= eta * fabs(onrm));
+    double nrm;
+    if (sh.flag[0]) {
+      cta_dots<T>(V, ld, n, j, 1, w, sh);  // explicit norm
+      nrm = sqrt(sh.c[0]);
+    } else {
+      nrm = sqrt(sh.scal[1]);
+    }
+    ++passes;
+    if (threadIdx.x == 0) {
+      const double onrm = sh.scal[0];
+      sh.scal[2] = nrm;
+      sh.flag[1] = (passes < 3 && nrm != 0.0 && fabs(nrm) < eta * fabs(onrm));
+      sh.flag[3] = !(nrm != 0.0 && fabs(nrm) >= eta * fabs(onrm));
+    }
+    __syncthreads();
+    more = sh.flag[1];
+    __syncthreads();
+  }
+  const double nrm = sh.scal[2];
+  *lindep = sh.flag[3];
+  if (sh.flag[2]) *err = 1;
   *norm = nrm;
+  __syncthreads();
   if (nrm != 1.0 && nrm != 0.0) cta_scale<T>(w, n, 1.0 / nrm);
 }
 
@@ -403,7 +425,7 @@ __device__ void cta_multinplace(double *V, int ld, int n, int l, int k, const do
     double row[kBCols];
 #pragma unroll
     for (int c = 0; c < kBCols; ++c)
-      if (c < k - l) row[c] = V[r + (size_t)(l + c) * ld];
+      if (c < k - l) row[c] = __ldcg(V + r + (size_t)(l + c) * ld);
     for (int j = s; j < e; ++j) {
       double acc = 0.0;
 #pragma unroll
@@ -420,7 +442,7 @@ __global__ void __launch_bounds__(T) batched_ks_kernel(int nprob, const BProblem
                                                        const int *__restrict__ order, int *__restrict__ next,
                                                        const int *__restrict__ rowptr, const int *__restrict__ colind,
                                                        const double *__restrict__ vals, const int2 *__restrict__ tiles,
-                                                       const double *__restrict__ v0, double *__restrict__ Vall,
+                                                       const double *__restrict__ v0, double *Vall,
                                                        BParams prm, double *__restrict__ evals,
                                                        double *__restrict__ errest_out, int *__restrict__ vcol,
                                                        int *__restrict__ info) {
@@ -442,6 +464,8 @@ __global__ void __launch_bounds__(T) batched_ks_kernel(int nprob, const BProblem
     const int max_it = prm.max_it_user > 0 ? prm.max_it_user : max(100, 2 * n / ncv);
     int err = 0;
     uint64_t nrand = 0;
+    if (threadIdx.x < 8) sh.flag[threadIdx.x] = 0;
+    __syncthreads();
     BDs ds{0, 0, 0, 0, 0};
     double h[kBCols + 1];
     // EPSSetUp: BVInsertVecs of the start vector (dropped if zero), then EPSGetStartVector(0)
@@ -590,6 +614,9 @@ __global__ void __launch_bounds__(T) batched_ks_kernel(int nprob, const BProblem
       inf[2] = reason;
       inf[3] = (int)steps;
       inf[4] = err;
+      inf[5] = nini;
+      inf[6] = 0;
+      inf[7] = 0;
     }
     __syncthreads();
   }
@@ -644,6 +671,9 @@ cudaError_t launch_batched(b200_batch B, const b200::BParams &prm, int nprob, cu
   int grid = sms * per_sm;
   if (grid > nprob) grid = nprob;
   cudaError_t e = cudaMemsetAsync(B->next, 0, sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  // every info entry -1 until its problem is solved
+  e = cudaMemsetAsync(B->info, 0xff, sizeof(int) * 8 * (size_t)B->nprob, s);
   if (e != cudaSuccess) return e;
   batched_ks_kernel<T><<<grid, T, 0, s>>>(nprob, B->probs, B->order, B->next, B->rowptr, B->colind, B->vals,
                                           B->tiles, B->v0, B->V, prm, B->evals, B->errest, B->vcol, B->info);
@@ -948,12 +978,17 @@ extern "C" b200_status b200_batch_solve(b200_batch B) {
   B200_CUDA_CHECK(
       cudaMemcpyAsync(B->h_info.data(), B->info, sizeof(int) * B->h_info.size(), cudaMemcpyDeviceToHost, B->stream));
   B200_CUDA_CHECK(cudaStreamSynchronize(B->stream));
-  for (int p = 0; p < B->nprob; ++p)
-    if (B->h_info[(size_t)p * 8 + 4]) {
-      b200_set_last_error(__FILE__, __LINE__, "a batched problem reported a device-side error");
-      B->solved = true;
+  B->solved = true;
+  for (int p = 0; p < B->nprob; ++p) {
+    if (B->h_info[(size_t)p * 8] < 0) {
+      b200_set_last_error(__FILE__, __LINE__, "a batched problem was not solved by the launch");
       return B200_ERR_DEVICE;
     }
+    if (B->h_info[(size_t)p * 8 + 4]) {
+      b200_set_last_error(__FILE__, __LINE__, "a batched problem reported a device-side error");
+      return B200_ERR_DEVICE;
+    }
+  }
   B->solved = true;
   return B200_OK;
 }

@@ -415,6 +415,9 @@ b200_status b200_batch_get_eigenvector(b200_batch B, int p, int i, double *x_hos
 /* All results at once: evals_host (nprob x ncv), info_host (nprob x 8: nconv, its, reason,
  * steps, device error), and the device time of the last solve in ms. */
 b200_status b200_batch_get_all(b200_batch B, double *evals_host, int *info_host, float *ms);
+/* Algorithmic bytes the last solve moved (SpMV: 12 per nonzero plus the vectors; Gram-Schmidt
+ * dots and updates: 8 per row and column touched; restarts), summed over the problems. */
+b200_status b200_batch_get_bytes(b200_batch B, double *bytes);
 
 #ifdef __cplusplus
 }

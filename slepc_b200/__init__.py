@@ -98,6 +98,7 @@ _SIGS = {
     "b200_batch_get_solution": (ctypes.c_int, [_vp, ctypes.c_int, _ip, _ip, _ip, _ip, _dp, _dp]),
     "b200_batch_get_eigenvector": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _dp]),
     "b200_batch_get_all": (ctypes.c_int, [_vp, _dp, _ip, ctypes.POINTER(ctypes.c_float)]),
+    "b200_batch_get_bytes": (ctypes.c_int, [_vp, _dp]),
     "b200_svd_create": (ctypes.c_int, [_vp, _vp]),
     "b200_svd_destroy": (ctypes.c_int, [_vp]),
     "b200_svd_set_operator": (ctypes.c_int, [_vp, _vp]),
@@ -878,6 +879,12 @@ class BatchEPS:
         ms = ctypes.c_float()
         _check(lib().b200_batch_get_all(self.handle, _d(ev), _i(info), ctypes.byref(ms)))
         return ev, info, ms.value
+
+    def getBytes(self):
+        """Algorithmic bytes moved by the last solve (for the HBM roofline)."""
+        v = ctypes.c_double()
+        _check(lib().b200_batch_get_bytes(self.handle, ctypes.byref(v)))
+        return v.value
 
     def destroy(self):
         if self.handle:

@@ -50,6 +50,7 @@ struct BProblem {
   long long v_off;     // start of its basis: ld x (ncv + 1) doubles
   long long tile_off;  // first warp tile (int2 local rows [r0, r1))
   long long x_off;     // start of its rows in the start-vector / output arrays
+  long long nnz;       // its nonzeros
   int n, ld, ntiles, index;
 };
 
@@ -69,6 +70,7 @@ struct BShared {
   double prod[T / 32][kWarpTileNnz];
   int perm[kBLd];
   int problem;
+  unsigned long long bytes;  // algorithmic bytes moved for the current problem
 };
 
 __device__ __forceinline__ double bwarp_sum(double v) {
@@ -121,6 +123,7 @@ __device__ void cta_spmv(const BProblem &P, const int *__restrict__ rowptr, cons
 template <int T>
 __device__ void cta_dots(const double *V, int ld, int n, int c0, int ncols, const double *w, BShared<T> &sh) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  if (threadIdx.x == 0) sh.bytes += 8ull * n * (ncols + 1);
   for (int g0 = 0; g0 < ncols; g0 += 8) {
     const int gn = min(8, ncols - g0);
     double acc[8];
@@ -193,6 +196,7 @@ __device__ void cta_orthonormalize(double *V, int ld, int n, int j, double eta, 
     cta_dots<T>(V, ld, n, 0, j + 1, w, sh);  // includes w against itself
     for (int i = 0; i < j; ++i) h[i] += sh.c[i];
     cta_update<T>(V, ld, n, j, sh.c, w);
+    if (threadIdx.x == 0 && j > 0) sh.bytes += 8ull * n * (j + 2);
     // thread 0: the Pythagorean estimate of the new norm (bvorthog.c:124-127)
     if (threadIdx.x == 0) {
       const double self = sh.c[j];
@@ -229,7 +233,10 @@ __device__ void cta_orthonormalize(double *V, int ld, int n, int j, double eta, 
   if (sh.flag[2]) *err = 1;
   *norm = nrm;
   __syncthreads();
-  if (nrm != 1.0 && nrm != 0.0) cta_scale<T>(w, n, 1.0 / nrm);
+  if (nrm != 1.0 && nrm != 0.0) {
+    cta_scale<T>(w, n, 1.0 / nrm);
+    if (threadIdx.x == 0) sh.bytes += 16ull * n;
+  }
 }
 
 // plane rotation [c s; -s c] [f; g] = [r; 0] with r carrying the sign of f
@@ -445,7 +452,7 @@ __global__ void __launch_bounds__(T) batched_ks_kernel(int nprob, const BProblem
                                                        const double *__restrict__ v0, double *Vall,
                                                        BParams prm, double *__restrict__ evals,
                                                        double *__restrict__ errest_out, int *__restrict__ vcol,
-                                                       int *__restrict__ info) {
+                                                       int *__restrict__ info, double *__restrict__ bytes_out) {
   __shared__ BShared<T> sh;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   for (;;) {
@@ -465,6 +472,7 @@ __global__ void __launch_bounds__(T) batched_ks_kernel(int nprob, const BProblem
     int err = 0;
     uint64_t nrand = 0;
     if (threadIdx.x < 8) sh.flag[threadIdx.x] = 0;
+    if (threadIdx.x == 0) sh.bytes = 0;
     __syncthreads();
     BDs ds{0, 0, 0, 0, 0};
     double h[kBCols + 1];
@@ -500,6 +508,7 @@ __global__ void __launch_bounds__(T) batched_ks_kernel(int nprob, const BProblem
       int m = nv, breakdown = 0;
       for (int j = k0; j < m; ++j) {
         cta_spmv<T>(P, rowptr, colind, vals, tiles, V + (size_t)j * ld, V + (size_t)(j + 1) * ld, sh);
+        if (threadIdx.x == 0) sh.bytes += 12ull * P.nnz + 4ull * (n + 1) + 16ull * n;
         double nrm;
         int lindep;
         cta_orthonormalize<T>(V, ld, n, j + 1, prm.eta, h, &nrm, &lindep, &err, sh);
@@ -581,6 +590,7 @@ __global__ void __launch_bounds__(T) batched_ks_kernel(int nprob, const BProblem
         if (e > s) {
           // Q restricted to rows [nconv, nv): V(:, s:e) = V(:, nconv:nv) Q(nconv:nv, s:e)
           cta_multinplace<T>(V, ld, n, nconv, nv, sh.Q, s, e);
+          if (threadIdx.x == 0) sh.bytes += 8ull * n * ((nv - nconv) + (e - s));
         }
       }
       if (reason == 0 && !breakdown) cta_copy<T>(V + (size_t)(k + lnew) * ld, V + (size_t)nv * ld, n);
@@ -615,8 +625,7 @@ __global__ void __launch_bounds__(T) batched_ks_kernel(int nprob, const BProblem
       inf[3] = (int)steps;
       inf[4] = err;
       inf[5] = nini;
-      inf[6] = 0;
-      inf[7] = 0;
+      bytes_out[pidx] = (double)sh.bytes;
     }
     __syncthreads();
   }
@@ -642,6 +651,7 @@ struct b200_batch_s {
   int *next = nullptr;    // work-queue counter
   double *evals = nullptr, *errest = nullptr;
   int *vcol = nullptr, *info = nullptr;
+  double *bytes = nullptr;  // algorithmic bytes per problem of the last solve
   long long total_rows = 0;
   // parameters
   int nev = 1, ncv = 0, mpd = 0, max_it = 0, which = B200_LARGEST_REAL;
@@ -650,6 +660,7 @@ struct b200_batch_s {
   // results on the host
   std::vector<double> h_evals, h_errest;
   std::vector<int> h_vcol, h_info;
+  std::vector<double> h_bytes;
   bool solved = false;
   // captured launch
   cudaGraph_t graph = nullptr;
@@ -664,7 +675,7 @@ namespace b200 {
 namespace {
 
 template <int T>
-cudaError_t launch_batched(b200_batch B, const b200::BParams &prm, int nprob, cudaStream_t s) {
+cudaError_t launch_batched(b200_batch B, const b200::BParams &prm, int nprob, cudaStream_t s, bool count) {
   int sms = num_sms_host(), per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_ks_kernel<T>, T, 0);
   if (per_sm < 1) per_sm = 1;
@@ -676,16 +687,17 @@ cudaError_t launch_batched(b200_batch B, const b200::BParams &prm, int nprob, cu
   e = cudaMemsetAsync(B->info, 0xff, sizeof(int) * 8 * (size_t)B->nprob, s);
   if (e != cudaSuccess) return e;
   batched_ks_kernel<T><<<grid, T, 0, s>>>(nprob, B->probs, B->order, B->next, B->rowptr, B->colind, B->vals,
-                                          B->tiles, B->v0, B->V, prm, B->evals, B->errest, B->vcol, B->info);
-  count_launch();
+                                          B->tiles, B->v0, B->V, prm, B->evals, B->errest, B->vcol, B->info,
+                                          B->bytes);
+  if (count) count_launch();
   return cudaGetLastError();
 }
 
-cudaError_t launch_any(b200_batch B, int threads, const b200::BParams &prm, int nprob, cudaStream_t s) {
+cudaError_t launch_any(b200_batch B, int threads, const b200::BParams &prm, int nprob, cudaStream_t s, bool count) {
   switch (threads) {
-    case 128: return launch_batched<128>(B, prm, nprob, s);
-    case 256: return launch_batched<256>(B, prm, nprob, s);
-    default: return launch_batched<512>(B, prm, nprob, s);
+    case 128: return launch_batched<128>(B, prm, nprob, s, count);
+    case 256: return launch_batched<256>(B, prm, nprob, s, count);
+    default: return launch_batched<512>(B, prm, nprob, s, count);
   }
 }
 
@@ -748,6 +760,7 @@ extern "C" b200_status b200_batch_create(int nprob, const int *ns, const int *ro
     P.nnz_off = nz;
     P.tile_off = (long long)tiles.size();
     P.x_off = rows;
+    P.nnz = r[n];
     P.n = n;
     P.ld = (n + 3) & ~3;
     P.ntiles = (int)wt.tiles.size();
@@ -770,7 +783,8 @@ extern "C" b200_status b200_batch_create(int nprob, const int *ns, const int *ro
             cudaMalloc(&B->order, sizeof(int) * nprob) == cudaSuccess &&
             cudaMalloc(&B->next, sizeof(int)) == cudaSuccess &&
             cudaMalloc(&B->probs, sizeof(b200::BProblem) * nprob) == cudaSuccess &&
-            cudaMalloc(&B->info, sizeof(int) * 8 * nprob) == cudaSuccess;
+            cudaMalloc(&B->info, sizeof(int) * 8 * nprob) == cudaSuccess &&
+            cudaMalloc(&B->bytes, sizeof(double) * nprob) == cudaSuccess;
   if (ok) {
     ok = cudaMemcpyAsync(B->rowptr, rowptr, sizeof(int) * rp, cudaMemcpyHostToDevice, s) == cudaSuccess &&
          (nz == 0 || cudaMemcpyAsync(B->colind, colind, sizeof(int) * nz, cudaMemcpyHostToDevice, s) == cudaSuccess) &&
@@ -808,6 +822,7 @@ extern "C" b200_status b200_batch_destroy(b200_batch B) {
   cudaFree(B->errest);
   cudaFree(B->vcol);
   cudaFree(B->info);
+  cudaFree(B->bytes);
   delete B;
   return B200_OK;
 }
@@ -905,7 +920,7 @@ extern "C" b200_status b200_batch_autotune(b200_batch B, int *threads_out) {
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_ks_kernel<512>, 512, 0);
     const int sample = std::min(B->nprob, 2 * num_sms_host() * std::max(per_sm, 1));
     B200_CUDA_CHECK(cudaEventRecord(e0, B->stream));
-    B200_CUDA_CHECK(launch_any(B, t, prm, sample, B->stream));
+    B200_CUDA_CHECK(launch_any(B, t, prm, sample, B->stream, true));
     B200_CUDA_CHECK(cudaEventRecord(e1, B->stream));
     B200_CUDA_CHECK(cudaEventSynchronize(e1));
     float ms = 0.0f;
@@ -944,7 +959,7 @@ extern "C" b200_status b200_batch_solve(b200_batch B) {
     cudaStream_t cap = nullptr;
     B200_CUDA_CHECK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     B200_CUDA_CHECK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = launch_any(B, B->threads, prm, B->nprob, cap);
+    cudaError_t e = launch_any(B, B->threads, prm, B->nprob, cap, false);  // counted at each replay
     cudaGraph_t g = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(cap, &g);
     cudaStreamDestroy(cap);
@@ -960,6 +975,7 @@ extern "C" b200_status b200_batch_solve(b200_batch B) {
   B200_CUDA_CHECK(cudaEventCreate(&e1));
   B200_CUDA_CHECK(cudaEventRecord(e0, B->stream));
   B200_CUDA_CHECK(cudaGraphLaunch(B->exec, B->stream));
+  count_launch();  // the graph holds one kernel
   B200_CUDA_CHECK(cudaEventRecord(e1, B->stream));
   B200_CUDA_CHECK(cudaEventSynchronize(e1));
   cudaEventElapsedTime(&B->last_ms, e0, e1);
@@ -977,6 +993,9 @@ extern "C" b200_status b200_batch_solve(b200_batch B) {
       cudaMemcpyAsync(B->h_vcol.data(), B->vcol, sizeof(int) * B->h_vcol.size(), cudaMemcpyDeviceToHost, B->stream));
   B200_CUDA_CHECK(
       cudaMemcpyAsync(B->h_info.data(), B->info, sizeof(int) * B->h_info.size(), cudaMemcpyDeviceToHost, B->stream));
+  B->h_bytes.resize(B->nprob);
+  B200_CUDA_CHECK(cudaMemcpyAsync(B->h_bytes.data(), B->bytes, sizeof(double) * B->nprob, cudaMemcpyDeviceToHost,
+                                  B->stream));
   B200_CUDA_CHECK(cudaStreamSynchronize(B->stream));
   B->solved = true;
   for (int p = 0; p < B->nprob; ++p) {
@@ -1037,5 +1056,17 @@ extern "C" b200_status b200_batch_get_all(b200_batch B, double *evals_host, int 
   if (evals_host) memcpy(evals_host, B->h_evals.data(), sizeof(double) * B->h_evals.size());
   if (info_host) memcpy(info_host, B->h_info.data(), sizeof(int) * B->h_info.size());
   if (ms) *ms = B->last_ms;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_batch_get_bytes(b200_batch B, double *bytes) {
+  B200_ARG_CHECK(B && bytes, "null argument");
+  if (!B->solved) {
+    b200_set_last_error(__FILE__, __LINE__, "b200_batch_solve has not been called");
+    return B200_ERR_STATE;
+  }
+  double t = 0.0;
+  for (double b : B->h_bytes) t += b;
+  *bytes = t;
   return B200_OK;
 }

@@ -127,11 +127,19 @@ b200_status b200_mat_get_sizes(b200_mat A, int *m, int *n);
 /* MatNorm(NORM_INFINITY), known for matrices created from host arrays. */
 b200_status b200_mat_norm_inf(b200_mat A, double *nrm);
 /* CSR SpMV schedule of a matrix (a MatSetOption-style knob):
- *   B200_SPMV_WARPTILE (default) -- warp tiles of <= 32 rows / <= 256 nonzeros;
- *   B200_SPMV_ROWBLOCK           -- CTA row blocks of <= 1024 rows / <= 4096 nonzeros.
- * Both sum each row in index order (rows within a tile give the bits of a sequential loop). */
+ *   B200_SPMV_SELL (default)  -- sliced ELL, 32-row slices, one row per lane (rows <= 32 nonzeros;
+ *                                longer rows by warp tiles and segments);
+ *   B200_SPMV_WARPTILE        -- warp tiles of <= 32 rows / <= 256 nonzeros;
+ *   B200_SPMV_PIPELINED       -- the warp tiles with the next tile's loads in flight;
+ *   B200_SPMV_ROWBLOCK        -- CTA row blocks of <= 1024 rows / <= 4096 nonzeros (FP64 only).
+ * All sum each row of at most 256 nonzeros in index order (the bits of a sequential loop). */
 #define B200_SPMV_ROWBLOCK 0
 #define B200_SPMV_WARPTILE 1
+/* warp tiles with a two-tile software pipeline (next tile's loads in flight; same bits) */
+#define B200_SPMV_PIPELINED 2
+/* sliced ELL, 32-row slices, one row per lane, for rows of at most 32 nonzeros (longer rows:
+ * warp tiles / segments); a second copy of the entries in HBM; same bits */
+#define B200_SPMV_SELL 3
 b200_status b200_mat_set_spmv_schedule(b200_mat A, int schedule);
 /* Lanes per row chosen for the SpMV (1..32), for tests and reports. */
 b200_status b200_mat_get_lanes(b200_mat A, int *lanes);

@@ -356,7 +356,7 @@ class Mat:
     def mult(self, x_ptr, y_ptr):
         _check(lib().b200_mat_mult(self.handle, x_ptr, y_ptr))
 
-    ROWBLOCK, WARPTILE = 0, 1
+    ROWBLOCK, WARPTILE, PIPELINED, SELL = 0, 1, 2, 3
 
     def setSpMVSchedule(self, schedule):
         _check(lib().b200_mat_set_spmv_schedule(self.handle, schedule))

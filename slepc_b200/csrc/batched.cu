@@ -48,7 +48,7 @@ struct BProblem {
   long long rp_off;    // start of the problem's row pointer (n+1 local offsets)
   long long nnz_off;   // start of its nonzeros
   long long v_off;     // start of its basis: ld x (ncv + 1) doubles
-  long long tile_off;  // first warp tile (int2 local rows [r0, r1))
+  long long tile_off;  // first warp tile ({r0, r1, p0, p1} in local rows and nonzeros)
   long long x_off;     // start of its rows in the start-vector / output arrays
   long long nnz;       // its nonzeros
   int n, ld, ntiles, index;
@@ -89,7 +89,7 @@ __device__ __forceinline__ uint64_t bsplitmix(uint64_t z) {
 // y = A x for one problem: warps walk its tiles (<= 32 rows, <= kWarpTileNnz nonzeros)
 template <int T>
 __device__ void cta_spmv(const BProblem &P, const int *__restrict__ rowptr, const int *__restrict__ colind,
-                         const double *__restrict__ vals, const int2 *__restrict__ tiles, const double *x, double *y,
+                         const double *__restrict__ vals, const int4 *__restrict__ tiles, const double *x, double *y,
                          BShared<T> &sh) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   double *prod = sh.prod[wib];
@@ -97,11 +97,9 @@ __device__ void cta_spmv(const BProblem &P, const int *__restrict__ rowptr, cons
   const int *ci = colind + P.nnz_off;
   const double *va = vals + P.nnz_off;
   for (int t = wib; t < P.ntiles; t += T / 32) {
-    const int2 tile = tiles[P.tile_off + t];
-    const int r0 = tile.x, r1 = tile.y, nrows = r1 - r0;
+    const int4 tile = tiles[P.tile_off + t];
+    const int r0 = tile.x, r1 = tile.y, nrows = r1 - r0, p0 = tile.z, p1 = tile.w;
     const int mystart = (lane < nrows) ? rp[r0 + lane] : 0;
-    const int p0 = __shfl_sync(0xffffffffu, mystart, 0);
-    const int p1 = rp[r1];
     const int nxt = __shfl_down_sync(0xffffffffu, mystart, 1);
     const int myend = (lane + 1 < nrows) ? nxt : p1;
     const int cnt = p1 - p0;
@@ -448,7 +446,7 @@ template <int T>
 __global__ void __launch_bounds__(T) batched_ks_kernel(int nprob, const BProblem *__restrict__ probs,
                                                        const int *__restrict__ order, int *__restrict__ next,
                                                        const int *__restrict__ rowptr, const int *__restrict__ colind,
-                                                       const double *__restrict__ vals, const int2 *__restrict__ tiles,
+                                                       const double *__restrict__ vals, const int4 *__restrict__ tiles,
                                                        const double *__restrict__ v0, double *Vall,
                                                        BParams prm, double *__restrict__ evals,
                                                        double *__restrict__ errest_out, int *__restrict__ vcol,
@@ -643,7 +641,7 @@ struct b200_batch_s {
   b200::BProblem *probs = nullptr;
   int *rowptr = nullptr, *colind = nullptr;
   double *vals = nullptr;
-  int2 *tiles = nullptr;
+  int4 *tiles = nullptr;
   double *v0 = nullptr;   // concatenated start vectors
   double *V = nullptr;    // concatenated bases
   size_t v_total = 0;
@@ -726,7 +724,7 @@ extern "C" b200_status b200_batch_create(int nprob, const int *ns, const int *ro
   B->nprob = nprob;
   B->ns.assign(ns, ns + nprob);
   // host plan: offsets and warp tiles of every problem
-  std::vector<int2> tiles;
+  std::vector<int4> tiles;
   long long rp = 0, nz = 0, rows = 0;
   B->hprobs.resize(nprob);
   for (int p = 0; p < nprob; ++p) {
@@ -778,7 +776,7 @@ extern "C" b200_status b200_batch_create(int nprob, const int *ns, const int *ro
   bool ok = cudaMalloc(&B->rowptr, sizeof(int) * rp) == cudaSuccess &&
             cudaMalloc(&B->colind, sizeof(int) * (nz > 0 ? nz : 1)) == cudaSuccess &&
             cudaMalloc(&B->vals, sizeof(double) * (nz > 0 ? nz : 1)) == cudaSuccess &&
-            cudaMalloc(&B->tiles, sizeof(int2) * (tiles.empty() ? 1 : tiles.size())) == cudaSuccess &&
+            cudaMalloc(&B->tiles, sizeof(int4) * (tiles.empty() ? 1 : tiles.size())) == cudaSuccess &&
             cudaMalloc(&B->v0, sizeof(double) * rows) == cudaSuccess &&
             cudaMalloc(&B->order, sizeof(int) * nprob) == cudaSuccess &&
             cudaMalloc(&B->next, sizeof(int)) == cudaSuccess &&
@@ -790,7 +788,7 @@ extern "C" b200_status b200_batch_create(int nprob, const int *ns, const int *ro
          (nz == 0 || cudaMemcpyAsync(B->colind, colind, sizeof(int) * nz, cudaMemcpyHostToDevice, s) == cudaSuccess) &&
          (nz == 0 || cudaMemcpyAsync(B->vals, vals, sizeof(double) * nz, cudaMemcpyHostToDevice, s) == cudaSuccess) &&
          (tiles.empty() ||
-          cudaMemcpyAsync(B->tiles, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice, s) ==
+          cudaMemcpyAsync(B->tiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, s) ==
               cudaSuccess) &&
          cudaMemcpyAsync(B->order, order.data(), sizeof(int) * nprob, cudaMemcpyHostToDevice, s) == cudaSuccess &&
          cudaMemsetAsync(B->v0, 0, sizeof(double) * rows, s) == cudaSuccess &&

@@ -40,18 +40,19 @@ constexpr int kWarpTileNnz = 256;   // nonzeros staged per warp tile of the warp
 constexpr int kSegmentNnz = 1024;   // nonzeros per segment of a row longer than a warp tile
 // Row blocks for the row-block SpMV: block b covers rows [b[i], b[i+1]).
 std::vector<int> spmv_row_blocks(int n, const int *rowptr_host);
-// Warp tiles for the warp-tile SpMV: {r0, r1} for up to 32 short rows; a row longer than
+// Warp tiles for the warp-tile SpMV: {r0, r1, p0, p1} (rows and their nonzeros) for up to 32
+// short rows; a row longer than
 // kWarpTileNnz becomes segments {p_begin, p_end} of at most kSegmentNnz nonzeros, and
 // longrows = {row, first segment, segment count}.
 struct WarpTiles {
-  std::vector<int2> tiles;
+  std::vector<int4> tiles;
   std::vector<int2> segs;
   std::vector<int3> longrows;
 };
 WarpTiles spmv_warp_tiles(int n, const int *rowptr_host);
 // Device copies of a WarpTiles plan plus one partial-sum slot per segment.
 struct SpmvTiles {
-  int2 *tiles = nullptr;
+  int4 *tiles = nullptr;
   int ntiles = 0;
   int2 *segs = nullptr;
   int nsegs = 0;
@@ -59,13 +60,43 @@ struct SpmvTiles {
   int nlong = 0;
   double *partials = nullptr;
 };
+// Sliced ELL with 32-row slices for rows of at most kSellMaxRow nonzeros; the other rows go to
+// warp tiles and segments (rest).
+constexpr int kSellMaxRow = 32;
+struct SellPlan {
+  std::vector<long long> off;
+  std::vector<int> width;
+  std::vector<unsigned> mask;
+  long long entries = 0;
+  WarpTiles rest;
+};
+SellPlan spmv_sell_plan(int n, const int *rowptr_host);
+struct SpmvSell {
+  int nslices = 0;
+  long long *off = nullptr;
+  int *width = nullptr;
+  unsigned *mask = nullptr;
+  void *vals = nullptr;  // double or float, like the matrix
+  int *cols = nullptr;
+  SpmvTiles rest;
+};
+cudaError_t spmv_sell_launch(const SpmvSell &S, int n, const SpmvTiles &rest, const int *rowptr, const int *colind,
+                             const double *vals, const double *x, double *y, cudaStream_t stream,
+                             const GsState *st = nullptr, int step = 0);
+cudaError_t spmv_sell_launch_f32(const SpmvSell &S, int n, const SpmvTiles &rest, const int *rowptr,
+                                 const int *colind, const float *vals, const double *x, double *y,
+                                 cudaStream_t stream, const GsState *st = nullptr, int step = 0);
+// The slices' columns and values from the CSR arrays in HBM (S.off/width/mask already on the device).
+cudaError_t sell_gather(int n, const SpmvSell &S, const int *rowptr, const int *colind, const void *vals, bool f32,
+                        cudaStream_t stream);
+// pipelined: the two-tile software-pipelined variant of the tile kernel (same result bits).
 cudaError_t spmv_warptile_launch(const SpmvTiles &T, const int *rowptr, const int *colind, const double *vals,
                                  const double *x, double *y, cudaStream_t stream, const GsState *st = nullptr,
-                                 int step = 0);
+                                 int step = 0, bool pipelined = false);
 // Same with FP32 stored values (products and sums in FP64).
 cudaError_t spmv_warptile_launch_f32(const SpmvTiles &T, const int *rowptr, const int *colind, const float *vals,
                                      const double *x, double *y, cudaStream_t stream, const GsState *st = nullptr,
-                                     int step = 0);
+                                     int step = 0, bool pipelined = false);
 // st/step: when st is given, the launch is skipped on the device if a
 // Lanczos run halted (breakdown) at an earlier step.
 cudaError_t spmv_rowblock_launch(int nblocks, const int *blocks, const int *rowptr, const int *colind,

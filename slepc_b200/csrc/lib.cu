@@ -65,6 +65,15 @@ static void part_free(CsrPart &P) {
   cudaFree(P.wt.segs);
   cudaFree(P.wt.longrows);
   cudaFree(P.wt.partials);
+  cudaFree(P.sell.off);
+  cudaFree(P.sell.width);
+  cudaFree(P.sell.mask);
+  cudaFree(P.sell.vals);
+  cudaFree(P.sell.cols);
+  cudaFree(P.sell.rest.tiles);
+  cudaFree(P.sell.rest.segs);
+  cudaFree(P.sell.rest.longrows);
+  cudaFree(P.sell.rest.partials);
   P = CsrPart{};
 }
 
@@ -99,7 +108,10 @@ static b200_status part_upload(CsrPart &P, const int *rowptr, const int *colind,
   return B200_OK;
 }
 
-// Row blocks (FP64 only) and warp tiles from a host copy of rowptr, uploaded to the device.
+static b200_status part_build_sell(CsrPart &P, const int *rowptr_host, cudaStream_t s);
+
+// Row blocks (FP64 only), warp tiles and the sliced-ELL copy (the default schedule) from a host
+// copy of rowptr, uploaded to the device.
 static b200_status part_set_schedules(CsrPart &P, const int *rowptr_host, cudaStream_t s) {
   if (!P.f32) {
     std::vector<int> b = spmv_row_blocks(P.rows, rowptr_host);
@@ -112,9 +124,9 @@ static b200_status part_set_schedules(CsrPart &P, const int *rowptr_host, cudaSt
   P.wt.nsegs = (int)wt.segs.size();
   P.wt.nlong = (int)wt.longrows.size();
   if (P.wt.ntiles) {
-    B200_CUDA_CHECK(cudaMalloc(&P.wt.tiles, sizeof(int2) * wt.tiles.size()));
+    B200_CUDA_CHECK(cudaMalloc(&P.wt.tiles, sizeof(int4) * wt.tiles.size()));
     B200_CUDA_CHECK(
-        cudaMemcpyAsync(P.wt.tiles, wt.tiles.data(), sizeof(int2) * wt.tiles.size(), cudaMemcpyHostToDevice, s));
+        cudaMemcpyAsync(P.wt.tiles, wt.tiles.data(), sizeof(int4) * wt.tiles.size(), cudaMemcpyHostToDevice, s));
   }
   if (P.wt.nsegs) {
     B200_CUDA_CHECK(cudaMalloc(&P.wt.segs, sizeof(int2) * wt.segs.size()));
@@ -126,18 +138,75 @@ static b200_status part_set_schedules(CsrPart &P, const int *rowptr_host, cudaSt
                                     cudaMemcpyHostToDevice, s));
   }
   B200_CUDA_CHECK(cudaStreamSynchronize(s));
+  return part_build_sell(P, rowptr_host, s);
+}
+
+// Sliced-ELL copy of a CSR operand, built in HBM from the device CSR arrays.
+static b200_status part_build_sell(CsrPart &P, const int *rowptr_host, cudaStream_t s) {
+  if (P.sell_ready) return B200_OK;
+  std::vector<int> rp;
+  if (!rowptr_host) {
+    rp.resize((size_t)P.rows + 1);
+    B200_CUDA_CHECK(cudaMemcpyAsync(rp.data(), P.rowptr, sizeof(int) * rp.size(), cudaMemcpyDeviceToHost, s));
+    B200_CUDA_CHECK(cudaStreamSynchronize(s));
+    rowptr_host = rp.data();
+  }
+  SellPlan sp = spmv_sell_plan(P.rows, rowptr_host);
+  SpmvSell &S = P.sell;
+  S.nslices = (int)sp.off.size();
+  const size_t vsz = P.f32 ? sizeof(float) : sizeof(double);
+  B200_CUDA_CHECK(cudaMalloc(&S.off, sizeof(long long) * (S.nslices ? S.nslices : 1)));
+  B200_CUDA_CHECK(cudaMalloc(&S.width, sizeof(int) * (S.nslices ? S.nslices : 1)));
+  B200_CUDA_CHECK(cudaMalloc(&S.mask, sizeof(unsigned) * (S.nslices ? S.nslices : 1)));
+  B200_CUDA_CHECK(cudaMalloc(&S.vals, vsz * (size_t)(sp.entries ? sp.entries : 1)));
+  B200_CUDA_CHECK(cudaMalloc(&S.cols, sizeof(int) * (size_t)(sp.entries ? sp.entries : 1)));
+  if (S.nslices) {
+    B200_CUDA_CHECK(cudaMemcpyAsync(S.off, sp.off.data(), sizeof(long long) * S.nslices, cudaMemcpyHostToDevice, s));
+    B200_CUDA_CHECK(cudaMemcpyAsync(S.width, sp.width.data(), sizeof(int) * S.nslices, cudaMemcpyHostToDevice, s));
+    B200_CUDA_CHECK(cudaMemcpyAsync(S.mask, sp.mask.data(), sizeof(unsigned) * S.nslices, cudaMemcpyHostToDevice, s));
+    B200_CUDA_CHECK(sell_gather(P.rows, S, P.rowptr, P.colind, P.vals, P.f32, s));
+  }
+  WarpTiles &wt = sp.rest;
+  S.rest.ntiles = (int)wt.tiles.size();
+  S.rest.nsegs = (int)wt.segs.size();
+  S.rest.nlong = (int)wt.longrows.size();
+  if (S.rest.ntiles) {
+    B200_CUDA_CHECK(cudaMalloc(&S.rest.tiles, sizeof(int4) * wt.tiles.size()));
+    B200_CUDA_CHECK(
+        cudaMemcpyAsync(S.rest.tiles, wt.tiles.data(), sizeof(int4) * wt.tiles.size(), cudaMemcpyHostToDevice, s));
+  }
+  if (S.rest.nsegs) {
+    B200_CUDA_CHECK(cudaMalloc(&S.rest.segs, sizeof(int2) * wt.segs.size()));
+    B200_CUDA_CHECK(cudaMalloc(&S.rest.partials, sizeof(double) * wt.segs.size()));
+    B200_CUDA_CHECK(cudaMalloc(&S.rest.longrows, sizeof(int3) * wt.longrows.size()));
+    B200_CUDA_CHECK(
+        cudaMemcpyAsync(S.rest.segs, wt.segs.data(), sizeof(int2) * wt.segs.size(), cudaMemcpyHostToDevice, s));
+    B200_CUDA_CHECK(cudaMemcpyAsync(S.rest.longrows, wt.longrows.data(), sizeof(int3) * wt.longrows.size(),
+                                    cudaMemcpyHostToDevice, s));
+  }
+  B200_CUDA_CHECK(cudaStreamSynchronize(s));
+  P.sell_ready = true;
   return B200_OK;
 }
 
 static cudaError_t part_spmv(const CsrPart &P, int schedule, const double *x, double *y, cudaStream_t stream,
                              const GsState *st, int step) {
+  if (schedule == B200_SPMV_SELL && P.sell_ready) {
+    if (P.f32)
+      return spmv_sell_launch_f32(P.sell, P.rows, P.sell.rest, P.rowptr, P.colind, static_cast<const float *>(P.vals),
+                                  x, y, stream, st, step);
+    return spmv_sell_launch(P.sell, P.rows, P.sell.rest, P.rowptr, P.colind, static_cast<const double *>(P.vals), x,
+                            y, stream, st, step);
+  }
+  const bool pipelined = schedule == B200_SPMV_PIPELINED;
   if (P.f32)
     return spmv_warptile_launch_f32(P.wt, P.rowptr, P.colind, static_cast<const float *>(P.vals), x, y, stream, st,
-                                    step);
+                                    step, pipelined);
   if (schedule == B200_SPMV_ROWBLOCK)
     return spmv_rowblock_launch(P.nblocks, P.blocks, P.rowptr, P.colind, static_cast<const double *>(P.vals), x, y,
                                 stream, st, step);
-  return spmv_warptile_launch(P.wt, P.rowptr, P.colind, static_cast<const double *>(P.vals), x, y, stream, st, step);
+  return spmv_warptile_launch(P.wt, P.rowptr, P.colind, static_cast<const double *>(P.vals), x, y, stream, st, step,
+                              pipelined);
 }
 
 // y = Op x for the operator of A (the EPS operator: A itself, or A^T A).
@@ -324,9 +393,16 @@ extern "C" b200_status b200_mat_norm_inf(b200_mat A, double *nrm) {
 }
 
 extern "C" b200_status b200_mat_set_spmv_schedule(b200_mat A, int schedule) {
-  B200_ARG_CHECK(A && (schedule == B200_SPMV_ROWBLOCK || schedule == B200_SPMV_WARPTILE), "unknown SpMV schedule");
-  B200_ARG_CHECK(schedule == B200_SPMV_WARPTILE || (A->kind == kMatCsr && !A->a.f32),
+  B200_ARG_CHECK(A && (schedule == B200_SPMV_ROWBLOCK || schedule == B200_SPMV_WARPTILE ||
+                       schedule == B200_SPMV_PIPELINED || schedule == B200_SPMV_SELL),
+                 "unknown SpMV schedule");
+  B200_ARG_CHECK(schedule != B200_SPMV_ROWBLOCK || (A->kind == kMatCsr && !A->a.f32),
                  "the row-block schedule is available for FP64 CSR matrices only");
+  B200_ARG_CHECK(A->kind == kMatCsr, "set the schedule on the matrix of a cross shell");
+  if (schedule == B200_SPMV_SELL) {
+    B200_CHECK(part_build_sell(A->a, nullptr, A->stream));
+    if (A->at.rows) B200_CHECK(part_build_sell(A->at, nullptr, A->stream));
+  }
   A->schedule = schedule;
   return B200_OK;
 }

@@ -22,6 +22,8 @@ struct CsrPart {
   int *blocks = nullptr;       // row blocks of the row-block SpMV (nblocks + 1 entries), FP64 only
   int nblocks = 0;
   b200::SpmvTiles wt;                // warp tiles, long-row segments and their partial-sum slots
+  b200::SpmvSell sell;               // sliced-ELL copy (built when that schedule is selected)
+  bool sell_ready = false;
 };
 
 enum MatKind { kMatCsr = 0, kMatCross = 1 };
@@ -39,7 +41,7 @@ struct b200_mat_s {
   bool swapped = false;      // kMatCross: the operator is A A^T (SVDSetUp's swap for m < n)
   double *work = nullptr;    // kMatCross: w = A x (base->m entries; base->n when swapped)
   double norm_inf = -1.0;    // max_i sum_j |a_ij| when known (computed from the host arrays)
-  int schedule = B200_SPMV_WARPTILE;
+  int schedule = B200_SPMV_SELL;
   cudaStream_t stream = nullptr;
 };
 

@@ -86,14 +86,14 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_rowblock_kernel(const int *
   }
 }
 
-// Warp tiles.  A tile {r0, r1} is <= 32 rows and <= kWarpTileNnz nonzeros; lane i of the owning
+// Warp tiles.  A tile {r0, r1, p0, p1} is <= 32 rows and <= kWarpTileNnz nonzeros; lane i of the owning
 // warp streams nonzeros i, i+32, ... (kWarpTileNnz/32 value, index and x loads in flight per
 // lane), keeps the rounded products in warp-private shared memory, and after a __syncwarp sums
 // row i of the tile in index order (the order of a sequential CSR loop).  Full occupancy (2048
 // threads per SM): the short loads of many warps hide the gather latency.
 // VT is the stored value type (double, or float for FP32 storage); products and sums are FP64.
 template <typename VT>
-__global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles, const int2 *__restrict__ tiles,
+__global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles, const int4 *__restrict__ tiles,
                                                                      const int *__restrict__ rowptr,
                                                                      const int *__restrict__ colind,
                                                                      const VT *__restrict__ vals,
@@ -106,15 +106,15 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles,
   double *prod = prod_all[wib];
   const int nwarps = gridDim.x * (kSpmvThreads / 32);
   for (int t = blockIdx.x * (kSpmvThreads / 32) + wib; t < ntiles; t += nwarps) {
-    const int2 tile = tiles[t];
-    const int r0 = tile.x, r1 = tile.y;
+    const int4 tile = tiles[t];
+    const int r0 = tile.x, r1 = tile.y, p0 = tile.z, p1 = tile.w;
     const int nrows = r1 - r0;  // 1..32
+    const int cnt = p1 - p0;
+    // the nonzero range comes with the tile, so the value and index loads below do not wait
+    // for the row pointer; the row boundaries are needed only for the sums
     const int myrow_start = (lane < nrows) ? __ldg(rowptr + r0 + lane) : 0;
-    const int p0 = __shfl_sync(0xffffffffu, myrow_start, 0);
-    const int p1 = __ldg(rowptr + r1);
     const int next = __shfl_down_sync(0xffffffffu, myrow_start, 1);
     const int myrow_end = (lane + 1 < nrows) ? next : p1;
-    const int cnt = p1 - p0;
     VT a[kWarpTileNnz / 32];  // kept in the stored type until the multiply (fewer registers for FP32)
     int c[kWarpTileNnz / 32];
 #pragma unroll
@@ -135,6 +135,111 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles,
       y[r0 + lane] = sacc;
     }
     __syncwarp();
+  }
+}
+
+// The same warp tiles with a two-tile software pipeline: while a warp gathers x for tile t it
+// already has the values and column indices of its next tile in flight (half occupancy, twice
+// the loads in flight per warp).  Same sums in the same order as spmv_warptile_kernel.
+template <typename VT>
+__global__ void __launch_bounds__(kSpmvThreads, sizeof(VT) == 4 ? 4 : 3)
+    spmv_warptile_pipelined_kernel(int ntiles, const int4 *__restrict__ tiles, const int *__restrict__ rowptr,
+                                   const int *__restrict__ colind, const VT *__restrict__ vals,
+                                   const double *__restrict__ x, double *__restrict__ y,
+                                   const GsState *__restrict__ st, int step) {
+  if (st && st->halt && st->halt_step < step) return;
+  __shared__ double prod_all[kSpmvThreads / 32][kWarpTileNnz];
+  constexpr int U = kWarpTileNnz / 32;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double *prod = prod_all[wib];
+  const int nwarps = gridDim.x * (kSpmvThreads / 32);
+  int t = blockIdx.x * (kSpmvThreads / 32) + wib;
+  if (t >= ntiles) return;
+  int4 tile = tiles[t];
+  VT a[U];
+  int c[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int q = lane + 32 * u;
+    a[u] = (q < tile.w - tile.z) ? __ldcs(vals + tile.z + q) : VT(0);
+    c[u] = (q < tile.w - tile.z) ? __ldcs(colind + tile.z + q) : 0;
+  }
+  while (true) {
+    const int tn = t + nwarps;
+    int4 ntile = make_int4(0, 0, 0, 0);
+    VT an[U];
+    int cn[U];
+    if (tn < ntiles) {
+      ntile = tiles[tn];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int q = lane + 32 * u;
+        an[u] = (q < ntile.w - ntile.z) ? __ldcs(vals + ntile.z + q) : VT(0);
+        cn[u] = (q < ntile.w - ntile.z) ? __ldcs(colind + ntile.z + q) : 0;
+      }
+    }
+    const int r0 = tile.x, nrows = tile.y - tile.x, p0 = tile.z, p1 = tile.w, cnt = p1 - p0;
+    const int myrow_start = (lane < nrows) ? __ldg(rowptr + r0 + lane) : 0;
+    const int nextb = __shfl_down_sync(0xffffffffu, myrow_start, 1);
+    const int myrow_end = (lane + 1 < nrows) ? nextb : p1;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int q = lane + 32 * u;
+      if (q < cnt) prod[q] = __dmul_rn((double)a[u], __ldg(x + c[u]));
+    }
+    __syncwarp();
+    if (lane < nrows) {
+      double sacc = 0.0;
+      for (int q = myrow_start - p0; q < myrow_end - p0; ++q) sacc = __dadd_rn(sacc, prod[q]);
+      y[r0 + lane] = sacc;
+    }
+    __syncwarp();
+    if (tn >= ntiles) break;
+    t = tn;
+    tile = ntile;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      a[u] = an[u];
+      c[u] = cn[u];
+    }
+  }
+}
+
+// Sliced ELL (32-row slices): slice s stores its rows column-major in kSellWidth-padded chunks,
+// entry (row 32s+i, k) at off[s] + 32k + i, column -1 for padding; lane i of the owning warp sums
+// row 32s+i in index order (the same bits as a sequential CSR loop) with loads of 32 consecutive
+// entries per instruction.  Rows with more than kSellMaxRow nonzeros are not in the slices
+// (their mask bit is 0) and are computed by the tile or segment kernels.
+template <typename VT>
+__global__ void __launch_bounds__(kSpmvThreads) spmv_sell_kernel(int nslices, int n, const long long *__restrict__ off,
+                                                                 const int *__restrict__ width,
+                                                                 const unsigned *__restrict__ mask,
+                                                                 const VT *__restrict__ sval,
+                                                                 const int *__restrict__ scol,
+                                                                 const double *__restrict__ x, double *__restrict__ y,
+                                                                 const GsState *__restrict__ st, int step) {
+  if (st && st->halt && st->halt_step < step) return;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = gridDim.x * (kSpmvThreads / 32);
+  for (int sl = blockIdx.x * (kSpmvThreads / 32) + (threadIdx.x >> 5); sl < nslices; sl += nwarps) {
+    const long long base = off[sl] + lane;
+    const int w = width[sl];
+    double sacc = 0.0;
+    for (int k0 = 0; k0 < w; k0 += 8) {
+      VT a[8];
+      int c[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const bool in = k0 + u < w;
+        c[u] = in ? __ldcs(scol + base + 32ll * (k0 + u)) : -1;
+        a[u] = in ? __ldcs(sval + base + 32ll * (k0 + u)) : VT(0);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (c[u] >= 0) sacc = __dadd_rn(sacc, __dmul_rn((double)a[u], __ldg(x + c[u])));
+    }
+    const int r = 32 * sl + lane;
+    if (r < n && ((mask[sl] >> lane) & 1u)) y[r] = sacc;
   }
 }
 
@@ -269,6 +374,53 @@ std::vector<int> spmv_row_blocks(int n, const int *rowptr) {
   return b;
 }
 
+SellPlan spmv_sell_plan(int n, const int *rowptr) {
+  SellPlan sp;
+  const int nslices = (n + 31) / 32;
+  sp.off.resize(nslices);
+  sp.width.resize(nslices);
+  sp.mask.resize(nslices);
+  long long total = 0;
+  for (int sl = 0; sl < nslices; ++sl) {
+    int w = 0;
+    unsigned m = 0;
+    for (int i = 0; i < 32 && 32 * sl + i < n; ++i) {
+      const int r = 32 * sl + i, len = rowptr[r + 1] - rowptr[r];
+      if (len <= kSellMaxRow) {
+        m |= 1u << i;
+        if (len > w) w = len;
+      }
+    }
+    sp.off[sl] = total;
+    sp.width[sl] = w;
+    sp.mask[sl] = m;
+    total += 32ll * w;
+  }
+  sp.entries = total;
+  // warp tiles and segments for the rows left out of the slices
+  for (int r = 0; r < n;) {
+    if (rowptr[r + 1] - rowptr[r] <= kSellMaxRow) {
+      ++r;
+      continue;
+    }
+    const int start = r;
+    const int base = rowptr[start];
+    while (r < n && r - start < 32 && rowptr[r + 1] - rowptr[r] > kSellMaxRow && rowptr[r + 1] - base <= kWarpTileNnz)
+      ++r;
+    if (r > start) {
+      sp.rest.tiles.push_back({start, r, rowptr[start], rowptr[r]});
+      continue;
+    }
+    const int p0 = rowptr[r], p1 = rowptr[r + 1];
+    const int first = (int)sp.rest.segs.size();
+    for (int p = p0; p < p1; p += kSegmentNnz)
+      sp.rest.segs.push_back({p, (p1 - p > kSegmentNnz) ? p + kSegmentNnz : p1});
+    sp.rest.longrows.push_back({r, first, (int)sp.rest.segs.size() - first});
+    ++r;
+  }
+  return sp;
+}
+
 WarpTiles spmv_warp_tiles(int n, const int *rowptr) {
   WarpTiles wt;
   wt.tiles.reserve(n / 16 + 2);
@@ -278,7 +430,7 @@ WarpTiles spmv_warp_tiles(int n, const int *rowptr) {
     const int base = rowptr[start];
     while (r < n && r - start < 32 && rowptr[r + 1] - base <= kWarpTileNnz) ++r;
     if (r > start) {
-      wt.tiles.push_back({start, r});
+      wt.tiles.push_back({start, r, rowptr[start], rowptr[r]});
       continue;
     }
     // a single row longer than a tile: segments of kSegmentNnz nonzeros
@@ -293,8 +445,9 @@ WarpTiles spmv_warp_tiles(int n, const int *rowptr) {
 
 template <typename VT>
 cudaError_t spmv_warptile_launch_t(const SpmvTiles &T, const int *rowptr, const int *colind, const VT *vals,
-                                   const double *x, double *y, cudaStream_t stream, const GsState *st, int step) {
-  static int sms = 0, tile_per_sm = 0, seg_per_sm = 0;
+                                   const double *x, double *y, cudaStream_t stream, const GsState *st, int step,
+                                   bool pipelined) {
+  static int sms = 0, tile_per_sm = 0, seg_per_sm = 0, pipe_per_sm = 0;
   if (!sms) {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -302,8 +455,10 @@ cudaError_t spmv_warptile_launch_t(const SpmvTiles &T, const int *rowptr, const 
     if (sms <= 0) sms = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tile_per_sm, spmv_warptile_kernel<VT>, kSpmvThreads, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&seg_per_sm, spmv_segment_kernel<VT>, kSpmvThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pipe_per_sm, spmv_warptile_pipelined_kernel<VT>, kSpmvThreads, 0);
     if (tile_per_sm <= 0) tile_per_sm = 1;
     if (seg_per_sm <= 0) seg_per_sm = 1;
+    if (pipe_per_sm <= 0) pipe_per_sm = 1;
   }
   const int warps_per_cta = kSpmvThreads / 32;
   // persistent grids: every CTA resident at once
@@ -316,9 +471,15 @@ cudaError_t spmv_warptile_launch_t(const SpmvTiles &T, const int *rowptr, const 
   }
   if (T.ntiles > 0) {
     int grid = (T.ntiles + warps_per_cta - 1) / warps_per_cta;
-    if (grid > sms * tile_per_sm) grid = sms * tile_per_sm;
-    spmv_warptile_kernel<VT><<<grid, kSpmvThreads, 0, stream>>>(T.ntiles, T.tiles, rowptr, colind, vals, x, y, st,
-                                                                step);
+    if (pipelined) {
+      if (grid > sms * pipe_per_sm) grid = sms * pipe_per_sm;
+      spmv_warptile_pipelined_kernel<VT><<<grid, kSpmvThreads, 0, stream>>>(T.ntiles, T.tiles, rowptr, colind, vals,
+                                                                            x, y, st, step);
+    } else {
+      if (grid > sms * tile_per_sm) grid = sms * tile_per_sm;
+      spmv_warptile_kernel<VT><<<grid, kSpmvThreads, 0, stream>>>(T.ntiles, T.tiles, rowptr, colind, vals, x, y,
+                                                                  st, step);
+    }
     count_launch();
   }
   if (T.nlong > 0) {
@@ -328,14 +489,92 @@ cudaError_t spmv_warptile_launch_t(const SpmvTiles &T, const int *rowptr, const 
   return cudaGetLastError();
 }
 
+// one thread per row: entries k < width of row 32s+i at off[s] + 32k + i, padding (-1, 0) past the
+// row's end and for rows outside the slices
+template <typename VT>
+__global__ void sell_gather_kernel(int n, int nslices, const long long *__restrict__ off, const int *__restrict__ width,
+                                   const unsigned *__restrict__ mask, const int *__restrict__ rowptr,
+                                   const int *__restrict__ colind, const VT *__restrict__ vals, int *__restrict__ scol,
+                                   VT *__restrict__ sval) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < 32ll * nslices;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int sl = (int)(t >> 5), i = (int)(t & 31), r = 32 * sl + i;
+    const bool in = r < n && ((mask[sl] >> i) & 1u);
+    const int p0 = in ? rowptr[r] : 0, len = in ? rowptr[r + 1] - p0 : 0;
+    const long long base = off[sl] + i;
+    for (int k = 0; k < width[sl]; ++k) {
+      scol[base + 32ll * k] = k < len ? colind[p0 + k] : -1;
+      sval[base + 32ll * k] = k < len ? vals[p0 + k] : VT(0);
+    }
+  }
+}
+
+cudaError_t sell_gather(int n, const SpmvSell &S, const int *rowptr, const int *colind, const void *vals, bool f32,
+                        cudaStream_t stream) {
+  if (S.nslices <= 0) return cudaSuccess;
+  long long g = (32ll * S.nslices + 255) / 256;
+  if (g > 148 * 32) g = 148 * 32;
+  if (f32)
+    sell_gather_kernel<float><<<(unsigned)g, 256, 0, stream>>>(n, S.nslices, S.off, S.width, S.mask, rowptr, colind,
+                                                               static_cast<const float *>(vals), S.cols,
+                                                               static_cast<float *>(S.vals));
+  else
+    sell_gather_kernel<double><<<(unsigned)g, 256, 0, stream>>>(n, S.nslices, S.off, S.width, S.mask, rowptr, colind,
+                                                                static_cast<const double *>(vals), S.cols,
+                                                                static_cast<double *>(S.vals));
+  count_launch();
+  return cudaGetLastError();
+}
+
+template <typename VT>
+cudaError_t spmv_sell_launch_t(const SpmvSell &S, int n, const SpmvTiles &rest, const int *rowptr, const int *colind,
+                               const VT *vals, const double *x, double *y, cudaStream_t stream, const GsState *st,
+                               int step) {
+  static int sms = 0, per_sm = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spmv_sell_kernel<VT>, kSpmvThreads, 0);
+    if (per_sm <= 0) per_sm = 1;
+  }
+  if (S.nslices > 0) {
+    int grid = (S.nslices + kSpmvThreads / 32 - 1) / (kSpmvThreads / 32);
+    if (grid > sms * per_sm) grid = sms * per_sm;
+    spmv_sell_kernel<VT><<<grid, kSpmvThreads, 0, stream>>>(S.nslices, n, S.off, S.width, S.mask,
+                                                            static_cast<const VT *>(S.vals), S.cols, x, y, st, step);
+    count_launch();
+  }
+  if (rest.ntiles > 0 || rest.nsegs > 0) {
+    cudaError_t e = spmv_warptile_launch_t<VT>(rest, rowptr, colind, vals, x, y, stream, st, step, false);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t spmv_sell_launch(const SpmvSell &S, int n, const SpmvTiles &rest, const int *rowptr, const int *colind,
+                             const double *vals, const double *x, double *y, cudaStream_t stream, const GsState *st,
+                             int step) {
+  return spmv_sell_launch_t<double>(S, n, rest, rowptr, colind, vals, x, y, stream, st, step);
+}
+
+cudaError_t spmv_sell_launch_f32(const SpmvSell &S, int n, const SpmvTiles &rest, const int *rowptr,
+                                 const int *colind, const float *vals, const double *x, double *y,
+                                 cudaStream_t stream, const GsState *st, int step) {
+  return spmv_sell_launch_t<float>(S, n, rest, rowptr, colind, vals, x, y, stream, st, step);
+}
+
 cudaError_t spmv_warptile_launch(const SpmvTiles &T, const int *rowptr, const int *colind, const double *vals,
-                                 const double *x, double *y, cudaStream_t stream, const GsState *st, int step) {
-  return spmv_warptile_launch_t<double>(T, rowptr, colind, vals, x, y, stream, st, step);
+                                 const double *x, double *y, cudaStream_t stream, const GsState *st, int step,
+                                 bool pipelined) {
+  return spmv_warptile_launch_t<double>(T, rowptr, colind, vals, x, y, stream, st, step, pipelined);
 }
 
 cudaError_t spmv_warptile_launch_f32(const SpmvTiles &T, const int *rowptr, const int *colind, const float *vals,
-                                     const double *x, double *y, cudaStream_t stream, const GsState *st, int step) {
-  return spmv_warptile_launch_t<float>(T, rowptr, colind, vals, x, y, stream, st, step);
+                                     const double *x, double *y, cudaStream_t stream, const GsState *st, int step,
+                                     bool pipelined) {
+  return spmv_warptile_launch_t<float>(T, rowptr, colind, vals, x, y, stream, st, step, pipelined);
 }
 
 cudaError_t spmv_rowblock_launch(int nblocks, const int *blocks, const int *rowptr, const int *colind,

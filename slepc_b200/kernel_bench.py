@@ -86,7 +86,7 @@ def spmv(args, torch):
         ms += e0.elapsed_time(e1)
     ms /= args.reps
     algo = nnz * 12 + (n + 1) * 4 + 2 * n * 8
-    return {"kernel": ["spmv_rowblock_kernel", "spmv_warptile_kernel"][args.schedule], "n": n, "nnz": nnz, "ms": ms, "algorithmic_bytes": algo,
+    return {"kernel": ["spmv_rowblock_kernel", "spmv_warptile_kernel", "spmv_warptile_pipelined_kernel", "spmv_sell_kernel"][args.schedule], "n": n, "nnz": nnz, "ms": ms, "algorithmic_bytes": algo,
             "GBps": algo / (ms * 1e-3) / 1e9}
 
 

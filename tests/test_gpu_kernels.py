@@ -49,7 +49,7 @@ def test_spmv_all_lane_widths_vs_oracle(b200, oracle_mod, lanes):
     np.testing.assert_allclose(yd.cpu().numpy(), ref, rtol=1e-13, atol=1e-13 * np.abs(ref).max())
 
 
-@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("schedule", [0, 1, 2, 3])
 def test_spmv_laplacian_via_mat_bit_exact(b200, oracle_mod, schedule):
     """Mat SpMV (row blocks / warp tiles): rows summed in index order, so it matches the
     oracle's sequential row loop bit for bit."""
@@ -67,7 +67,7 @@ def test_spmv_laplacian_via_mat_bit_exact(b200, oracle_mod, schedule):
     np.testing.assert_array_equal(yd.cpu().numpy(), oracle_mod.spmv(P.to_scipy(csr), x))
 
 
-@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("schedule", [0, 1, 2, 3])
 def test_spmv_mat_ragged_long_rows(b200, oracle_mod, schedule):
     """Empty rows, short rows, and rows longer than a tile (4096 / 256 nonzeros)."""
     torch = _torch()
@@ -76,6 +76,7 @@ def test_spmv_mat_ragged_long_rows(b200, oracle_mod, schedule):
     lens = rng.integers(0, 12, size=n)
     lens[::13] = 0
     lens[[5, 777, 20010]] = [5000, 9000, 4097]
+    lens[[100, 101, 102, 9000, 9031]] = [40, 200, 33, 256, 32]  # tile rows beside sliced-ELL rows
     rowptr = np.zeros(n + 1, dtype=np.int64)
     np.cumsum(lens, out=rowptr[1:])
     colind = np.concatenate([np.sort(rng.choice(n, size=l, replace=False)) for l in lens]).astype(np.int32)

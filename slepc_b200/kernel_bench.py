@@ -7,6 +7,7 @@ time one kernel family in isolation with CUDA events:
   python slepc_b200/kernel_bench.py spmv             # CSR SpMV of the 7-point Laplacian
   python slepc_b200/kernel_bench.py multinplace      # restart GEMM V(:,0:56) = V(:,0:80) Q
   python slepc_b200/kernel_bench.py cross            # A x, A^T z, A^T A x of the 2M x 500k power-law matrix
+  python slepc_b200/kernel_bench.py batched          # the batched Krylov-Schur launch on a small k-NN batch
 
 Prints one JSON line per kernel family: average ms per call and algorithmic GB/s.
 """
@@ -131,6 +132,28 @@ def cross(args, torch):
     return out
 
 
+def batched(args, torch):
+    """The batched Krylov-Schur launch on a small k-NN batch (n ~ U[500, 3000]); device time per solve
+    and the device-counted algorithmic bytes."""
+    ns = P.batch_sizes(args.nprob, 1, 500, 3000)
+    B = P.knn_batch(ns, 8, 1)
+    v0 = np.concatenate([P.start_vector(int(n), p) for p, n in enumerate(ns)])
+    E = S.BatchEPS().create(B.ns, B.rowptr, B.colind, B.vals)
+    E.setDimensions(8, 24)
+    E.setInitialVectors(v0)
+    E.setThreads(args.threads)
+    for _ in range(args.warmup):
+        E.solve()
+    ms = 0.0
+    for _ in range(args.reps):
+        E.solve()
+        ms += E.getAll()[2]
+    ms /= args.reps
+    algo = E.getBytes()
+    return {"kernel": "batched_ks_kernel", "nprob": args.nprob, "rows": int(ns.sum()), "threads": args.threads,
+            "ms": ms, "algorithmic_bytes": algo, "GBps": algo / (ms * 1e-3) / 1e9}
+
+
 def multinplace(args, torch):
     n, k, e = args.n, 80, 56
     bv = S.BV().create(n, 81)
@@ -159,7 +182,9 @@ def multinplace(args, torch):
 
 def main():
     p = argparse.ArgumentParser()
-    p.add_argument("kernel", choices=["gs", "spmv", "multinplace", "cross", "all"])
+    p.add_argument("kernel", choices=["gs", "spmv", "multinplace", "cross", "batched", "all"])
+    p.add_argument("--nprob", type=int, default=64)
+    p.add_argument("--threads", type=int, default=512)
     p.add_argument("--rows", type=int, default=2_000_000)
     p.add_argument("--cols", type=int, default=500_000)
     p.add_argument("--n", type=int, default=128 ** 3)
@@ -179,6 +204,8 @@ def main():
             for j in js:
                 args.j = j
                 print(json.dumps(gs(args, torch)), flush=True)
+        elif k == "batched":
+            print(json.dumps(batched(args, torch)), flush=True)
         elif k == "cross":
             for line in cross(args, torch):
                 print(json.dumps(line), flush=True)

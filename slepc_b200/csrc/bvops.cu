@@ -131,6 +131,58 @@ __global__ void dot_partial_kernel(const double *__restrict__ X, int ldx, int nx
   }
 }
 
+// Gram block M = Y^T X for up to 64 x 64 column pairs per CTA row (blockIdx.y, blockIdx.z select the
+// 64-column blocks of Y and X): the CTA's rows are staged in 32-row panels in shared memory and
+// thread (ty, tx) of a 16 x 16 layout accumulates the 4 x 4 pairs (4ty+a, 4tx+b) in row order.
+// partial[blk * (nx*ny) + (i + j*ny)] as dot_partial_kernel writes it.
+constexpr int kGramRows = 32;
+__global__ void __launch_bounds__(256) gram_partial_kernel(const double *__restrict__ X, int ldx, int nx,
+                                                           const double *__restrict__ Y, int ldy, int ny, int n,
+                                                           double *partial) {
+  __shared__ double Xs[kGramRows][64 + 1], Ys[kGramRows][64 + 1];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int y0 = blockIdx.y * 64, x0 = blockIdx.z * 64;
+  const int cy = min(64, ny - y0), cx = min(64, nx - x0);
+  const long long rows_per = (n + gridDim.x - 1) / gridDim.x;
+  const long long r0 = (long long)blockIdx.x * rows_per;
+  const long long r1 = min((long long)n, r0 + rows_per);
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (long long p0 = r0; p0 < r1; p0 += kGramRows) {
+    const int pr = (int)min((long long)kGramRows, r1 - p0);
+    // column-major loads: 32 consecutive rows of one column per warp
+    for (int e = threadIdx.x; e < kGramRows * 64; e += 256) {
+      const int r = e % kGramRows, c = e / kGramRows;
+      Xs[r][c] = (r < pr && c < cx) ? X[(size_t)(x0 + c) * ldx + p0 + r] : 0.0;
+      Ys[r][c] = (r < pr && c < cy) ? Y[(size_t)(y0 + c) * ldy + p0 + r] : 0.0;
+    }
+    __syncthreads();
+    for (int r = 0; r < pr; ++r) {
+      double yv[4], xv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) yv[a] = Ys[r][4 * ty + a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) xv[b] = Xs[r][4 * tx + b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(yv[a], xv[b], acc[a][b]);
+    }
+    __syncthreads();
+  }
+  const int npairs = nx * ny;
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = 4 * ty + a, j = 4 * tx + b;
+      if (i < cy && j < cx) partial[(size_t)blockIdx.x * npairs + (y0 + i) + (size_t)(x0 + j) * ny] = acc[a][b];
+    }
+}
+
 __global__ void dot_final_kernel(const double *__restrict__ partial, int nblocks, int nx, int ny, double *M, int ldm) {
   const int npairs = nx * ny;
   for (int pr = blockIdx.x * blockDim.x + threadIdx.x; pr < npairs; pr += gridDim.x * blockDim.x) {
@@ -208,6 +260,33 @@ __global__ void inverse_diagonal_kernel(int n, const int *__restrict__ rowptr, c
       if (colind[p] == i) d = __dadd_rn(d, vals[p]);
     dinv[i] = 1.0 / (d != 0.0 ? d : 1.0);
   }
+}
+
+// partial[c * gridDim.x + b] = sum of squares of column c over the block's row range
+__global__ void colnorm_partial_kernel(const double *__restrict__ X, int ldx, int n, double *partial) {
+  __shared__ double red[32];
+  const int c = blockIdx.y;
+  const long long rows_per = (n + gridDim.x - 1) / gridDim.x;
+  const long long r0 = (long long)blockIdx.x * rows_per, r1 = min((long long)n, r0 + rows_per);
+  const double *x = X + (size_t)c * ldx;
+  double acc = 0.0;
+  for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) acc = fma(x[r], x[r], acc);
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    partial[(size_t)c * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+__global__ void colnorm_final_kernel(const double *__restrict__ partial, int nblocks, int k, double *out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= k) return;
+  double s = 0.0;
+  for (int b = 0; b < nblocks; ++b) s += partial[(size_t)c * nblocks + b];
+  out[c] = sqrt(s);
 }
 
 __global__ void sum_final_kernel(const double *__restrict__ partial, int nblocks, double *out) {
@@ -356,7 +435,13 @@ cudaError_t dot_launch(const double *X, int ldx, int nx, const double *Y, int ld
   int blocks = num_sms();
   if (blocks * npairs > work_len) blocks = work_len / npairs;
   if (blocks < 1) return cudaErrorInvalidValue;
-  dot_partial_kernel<<<blocks, 256, 0, stream>>>(X, ldx, nx, Y, ldy, ny, n, work);
+  if (npairs >= 64) {
+    // register-tiled Gram blocks: both blocks of columns read once per CTA row range
+    const dim3 grid(blocks, (ny + 63) / 64, (nx + 63) / 64);
+    gram_partial_kernel<<<grid, 256, 0, stream>>>(X, ldx, nx, Y, ldy, ny, n, work);
+  } else {
+    dot_partial_kernel<<<blocks, 256, 0, stream>>>(X, ldx, nx, Y, ldy, ny, n, work);
+  }
   count_launch();
   dot_final_kernel<<<(npairs + 255) / 256, 256, 0, stream>>>(work, blocks, nx, ny, M, ldm);
   count_launch();
@@ -373,6 +458,19 @@ cudaError_t scale_launch(double *x, long long len, double alpha, cudaStream_t st
 cudaError_t copy_launch(double *dst, const double *src, long long len, cudaStream_t stream) {
   if (len <= 0) return cudaSuccess;
   copy_kernel<<<grid_for(len, 256), 256, 0, stream>>>(dst, src, len);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t colnorm_launch(const double *X, int ldx, int n, int k, double *out, double *work, int work_len,
+                           cudaStream_t stream) {
+  if (k <= 0) return cudaSuccess;
+  int blocks = num_sms();
+  if (blocks * k > work_len) blocks = work_len / k;
+  if (blocks < 1) return cudaErrorInvalidValue;
+  colnorm_partial_kernel<<<dim3(blocks, k), 256, 0, stream>>>(X, ldx, n, work);
+  count_launch();
+  colnorm_final_kernel<<<(k + 127) / 128, 128, 0, stream>>>(work, blocks, k, out);
   count_launch();
   return cudaGetLastError();
 }

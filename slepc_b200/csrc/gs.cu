@@ -585,6 +585,20 @@ cudaError_t gs_orthogonalize_launch(const GsPassArgs &a, const GsWork &w, cudaSt
   return e;
 }
 
+// out[0] = the norm, out[1] = the lindep flag, out[2] = the device error bits of the last column
+// orthogonalisation (read back once for a block of columns)
+__global__ void gs_record_kernel(const GsState *__restrict__ st, double *out) {
+  out[0] = st->beta_out;
+  out[1] = (double)st->lindep;
+  out[2] = (double)st->err;
+}
+
+cudaError_t gs_record_launch(const GsWork &w, double *out, cudaStream_t stream) {
+  gs_record_kernel<<<1, 1, 0, stream>>>(w.st, out);
+  count_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t gs_dot_launch(const GsPassArgs &a, const GsWork &w, cudaStream_t stream) {
   if (a.jb < 0 || a.jb >= kMaxCols) return cudaErrorInvalidValue;
   return launch_pass(a, w, 0, 1, stream);

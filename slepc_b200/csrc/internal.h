@@ -14,6 +14,12 @@ cudaError_t mat_apply(b200_mat A, const double *x, double *y, cudaStream_t strea
 b200_status bv_orth_column(b200_bv bv, int j, int normalize, double *H, double *norm, int *lindep);
 // EPSSetUp's BVInsertVecs of the initial space into columns 0..k-1 (sets eps->nini_eff).
 b200_status eps_insert_initial_space(b200_eps eps, b200_bv V, int max_cols);
+// BVOrthogonalize (no R) with one host synchronisation for the whole block.
+b200_status bv_orthogonalize_block(b200_bv bv);
+// BVOrthogonalizeVec + scale by 1/norm for several device vectors, one synchronisation.
+b200_status bv_orthonormalize_vecs(b200_bv bv, double *const *vecs, int count, int *breakdown);
+// Column norms of the active columns, one synchronisation.
+b200_status bv_column_norms(b200_bv bv, double *nrm);
 // Streaming multiprocessors of the current device.
 int num_sms_host();
 // EPSSolve with EPSLOBPCG (lobpcg.cu).

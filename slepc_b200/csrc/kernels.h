@@ -135,6 +135,8 @@ struct GsPassArgs {
 cudaError_t gs_orthogonalize_launch(const GsPassArgs &a, const GsWork &w, cudaStream_t stream);
 // Initialise the control block (eta, deftol, clears halt/err) -- once per run.
 cudaError_t gs_state_reset(const GsWork &w, double eta, cudaStream_t stream);
+// out[0..2] = norm, lindep flag and error bits of the last orthogonalisation (no host sync).
+cudaError_t gs_record_launch(const GsWork &w, double *out, cudaStream_t stream);
 // Plain dots q = V(:,0:jb)^T w (no decision), result in w.cnew.
 cudaError_t gs_dot_launch(const GsPassArgs &a, const GsWork &w, cudaStream_t stream);
 
@@ -159,6 +161,9 @@ cudaError_t dot_launch(const double *X, int ldx, int nx, const double *Y, int ld
                        double *work, int work_len, cudaStream_t stream);
 cudaError_t scale_launch(double *x, long long len, double alpha, cudaStream_t stream);
 cudaError_t copy_launch(double *dst, const double *src, long long len, cudaStream_t stream);
+// out[c] = ||X(:,c)||_2 for c < k (device), deterministic (fixed row split, fixed order).
+cudaError_t colnorm_launch(const double *X, int ldx, int n, int k, double *out, double *work, int work_len,
+                           cudaStream_t stream);
 // Sum of squares of x (len) into out[0] (device), deterministic two-level reduction.
 cudaError_t sumsq_launch(const double *x, long long len, double *out, double *work, int work_len, cudaStream_t stream);
 // out[0] = ||y - alpha x||^2, deterministic two-level reduction.

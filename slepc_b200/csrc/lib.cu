@@ -736,8 +736,97 @@ extern "C" b200_status b200_bv_scale_column(b200_bv bv, int j, double alpha) {
   return B200_OK;
 }
 
+// BVOrthogonalize_GS without R: every column of [l,k) orthogonalised against all previous columns
+// and scaled by 1/norm on the device, the norms recorded on the device and read back once.
+b200_status b200::bv_orthogonalize_block(b200_bv bv) {
+  const int nc = bv->k - bv->l;
+  if (nc <= 0) return B200_OK;
+  B200_CHECK(bv_reserve(bv, (size_t)3 * nc, 0));
+  for (int j = bv->l; j < bv->k; ++j) {
+    B200_CUDA_CHECK(gs_state_reset(bv->gs, bv->eta, bv->stream));
+    GsPassArgs a{};
+    a.V = bv->V;
+    a.ld = bv->ld;
+    a.total_cols = bv->m + 1;
+    a.n = bv->n;
+    a.jb = j;
+    a.wcol = j;
+    a.hacc = bv->coefbuf + (size_t)j * bv->ldc;
+    a.step = -1;
+    a.normalize = 1;
+    a.column = 1;
+    B200_CUDA_CHECK(gs_orthogonalize_launch(a, bv->gs, bv->stream));
+    B200_CUDA_CHECK(gs_record_launch(bv->gs, bv->qbuf + 3 * (size_t)(j - bv->l), bv->stream));
+  }
+  B200_CUDA_CHECK(
+      cudaMemcpyAsync(bv->hpin, bv->qbuf, sizeof(double) * 3 * (size_t)nc, cudaMemcpyDeviceToHost, bv->stream));
+  B200_CUDA_CHECK(cudaStreamSynchronize(bv->stream));
+  for (int c = 0; c < nc; ++c) {
+    const int err = (int)bv->hpin[3 * c + 2];
+    if (err & kDevErrInnerProduct) {
+      b200_set_last_error(__FILE__, __LINE__, "invalid inner product (negative self dot product)");
+      return B200_ERR_INNER;
+    }
+    if (err) B200_DEV_ERR("a Gram-Schmidt kernel reported a device-side error");
+    if (bv->hpin[3 * c] == 0.0) {
+      b200_set_last_error(__FILE__, __LINE__, "breakdown in BVOrthogonalize due to a linearly dependent column");
+      return B200_ERR_BREAKDOWN;
+    }
+  }
+  return B200_OK;
+}
+
+// BVOrthogonalizeVec of `count` device vectors against the active columns of bv, each scaled by
+// 1/norm on the device; one read-back at the end.  *breakdown: some vector had norm 0 or was
+// linearly dependent (the caller stops, as LOBPCG does).
+b200_status b200::bv_orthonormalize_vecs(b200_bv bv, double *const *vecs, int count, int *breakdown) {
+  *breakdown = 0;
+  if (count <= 0) return B200_OK;
+  B200_CHECK(bv_reserve(bv, (size_t)3 * count, 0));
+  for (int i = 0; i < count; ++i) {
+    B200_CUDA_CHECK(copy_launch(col(bv, bv->m), vecs[i], bv->n, bv->stream));
+    B200_CUDA_CHECK(gs_state_reset(bv->gs, bv->eta, bv->stream));
+    GsPassArgs a{};
+    a.V = bv->V;
+    a.ld = bv->ld;
+    a.total_cols = bv->m + 1;
+    a.n = bv->n;
+    a.jb = bv->k;
+    a.wcol = bv->m;
+    a.hacc = bv->hvec;
+    a.step = -1;
+    a.normalize = 1;
+    a.column = 0;
+    B200_CUDA_CHECK(gs_orthogonalize_launch(a, bv->gs, bv->stream));
+    B200_CUDA_CHECK(copy_launch(vecs[i], col(bv, bv->m), bv->n, bv->stream));
+    B200_CUDA_CHECK(gs_record_launch(bv->gs, bv->qbuf + 3 * (size_t)i, bv->stream));
+  }
+  B200_CUDA_CHECK(
+      cudaMemcpyAsync(bv->hpin, bv->qbuf, sizeof(double) * 3 * (size_t)count, cudaMemcpyDeviceToHost, bv->stream));
+  B200_CUDA_CHECK(cudaStreamSynchronize(bv->stream));
+  for (int i = 0; i < count; ++i) {
+    const int err = (int)bv->hpin[3 * i + 2];
+    if (err) B200_DEV_ERR("a Gram-Schmidt kernel reported a device-side error");
+    if (!(bv->hpin[3 * i] > 0.0) || bv->hpin[3 * i + 1] != 0.0) *breakdown = 1;
+  }
+  return B200_OK;
+}
+
+// Norms of columns [l,k) into host nrm[0..k-l), one reduction and one read-back.
+b200_status b200::bv_column_norms(b200_bv bv, double *nrm) {
+  const int nc = bv->k - bv->l;
+  if (nc <= 0) return B200_OK;
+  B200_CHECK(bv_reserve(bv, (size_t)nc, (size_t)nc * num_sms_host()));
+  B200_CUDA_CHECK(colnorm_launch(col(bv, bv->l), bv->ld, bv->n, nc, bv->qbuf, bv->red, bv->red_len, bv->stream));
+  B200_CUDA_CHECK(cudaMemcpyAsync(bv->hpin, bv->qbuf, sizeof(double) * nc, cudaMemcpyDeviceToHost, bv->stream));
+  B200_CUDA_CHECK(cudaStreamSynchronize(bv->stream));
+  memcpy(nrm, bv->hpin, sizeof(double) * nc);
+  return B200_OK;
+}
+
 extern "C" b200_status b200_bv_orthogonalize(b200_bv bv, double *R, int ldr) {
   B200_ARG_CHECK(bv && (!R || ldr >= bv->k), "R leading dimension too small");
+  if (!R) return bv_orthogonalize_block(bv);
   for (int j = bv->l; j < bv->k; ++j) {
     double norm = 0.0;
     std::vector<double> H(j + 1);

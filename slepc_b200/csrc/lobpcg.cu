@@ -245,10 +245,12 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
     // 8. residual norms and the active set
     int k = ini;
     bool countc = true;
+    std::vector<double> rnorm(bs);
+    active(R, ini, bs);
+    B200_CHECK(bv_column_norms(R, rnorm.data()));  // all residual norms, one synchronisation
     for (int j = ini; j < bs; ++j) {
       const int i = locked + j;
-      double nrm = 0.0;
-      B200_CHECK(b200_bv_norm_column(R, j, &nrm));
+      const double nrm = rnorm[j - ini];
       errest[i] = (eigr[i] != 0.0) ? nrm / std::fabs(eigr[i]) : 1.7976931348623157e308;
       if (countc) {
         if (errest[i] < tol) ++k;
@@ -286,16 +288,12 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
       active(V, locked + bs, locked + bs + nconv);
       active(X, bs - nconv, bs);
       B200_CUDA_CHECK(bv_copy(V, X));
-      for (int j = bs - nconv; j < bs; ++j) {
-        double nrm = 0.0;
-        int lindep = 0;
-        B200_CHECK(b200_bv_orthogonalize_vec(Y, col(X, j), nullptr, &nrm, &lindep));
-        if (nrm > 0.0 && !lindep) {
-          B200_CHECK(b200_bv_scale_column(X, j, 1.0 / nrm));
-        } else {
-          reason = B200_DIVERGED_BREAKDOWN;
-          break;
-        }
+      {
+        std::vector<double *> vs;
+        for (int j = bs - nconv; j < bs; ++j) vs.push_back(col(X, j));
+        int bd = 0;
+        B200_CHECK(bv_orthonormalize_vecs(Y, vs.data(), (int)vs.size(), &bd));
+        if (bd) reason = B200_DIVERGED_BREAKDOWN;
       }
       if (reason != B200_CONVERGED_ITERATING) break;
       locked += nconv;
@@ -320,17 +318,14 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
     if (eps->pc == B200_PC_JACOBI)
       B200_CUDA_CHECK(diag_scale_launch(col(R, ini), R->ld, n, bs - ini, eps->dinv, R->stream));
     if (locked > 0) {
-      for (int j = ini; j < bs; ++j) {
-        double nrm = 0.0;
-        int lindep = 0;
-        B200_CHECK(b200_bv_orthogonalize_vec(Y, col(R, j), nullptr, &nrm, &lindep));
-        if (nrm > 0.0 && !lindep) B200_CHECK(b200_bv_scale_column(R, j, 1.0 / nrm));
-        if (nrm <= 0.0 || lindep) {
-          reason = B200_DIVERGED_BREAKDOWN;
-          break;
-        }
+      std::vector<double *> vs;
+      for (int j = ini; j < bs; ++j) vs.push_back(col(R, j));
+      int bd = 0;
+      B200_CHECK(bv_orthonormalize_vecs(Y, vs.data(), (int)vs.size(), &bd));
+      if (bd) {
+        reason = B200_DIVERGED_BREAKDOWN;
+        break;
       }
-      if (reason != B200_CONVERGED_ITERATING) break;
     }
     // 11. orthonormalise the preconditioned residuals; 13-16 the conjugate directions
     B200_CHECK(b200_bv_orthogonalize(R, nullptr, 0));

@@ -255,6 +255,29 @@ b200_status b200_eps_set_initial_space_device(b200_eps eps, const double *v0_dev
 /* Stop after this many restarts (0 = no cap; used to time bounded samples). */
 b200_status b200_eps_set_max_restarts(b200_eps eps, int max_restarts);
 /* EPSSolve (src/eps/interface/epssolve.c:119-229 -> EPSSolve_KrylovSchur_Default, krylovschur.c:227-348). */
+/* Arithmetic of the Krylov-Schur solve (no SLEPc counterpart: SLEPc computes
+ * in the one precision PETSc was configured with).
+ *   B200_PRECISION_FP64 (default): the drop-in path, FP64 throughout.
+ *   B200_PRECISION_MIXED: two phases.  (1) Krylov-Schur with the basis stored
+ *   in FP32 and the matrix values in FP32 (every product, sum, DGKS
+ *   correction, Rayleigh quotient and projected problem in FP64), run to a
+ *   loose tolerance: half the HBM traffic of the FP64 basis.  (2) FP64
+ *   refinement of the block of nev + guard Ritz vectors by Chebyshev-filtered
+ *   subspace iteration with an FP64 Rayleigh-Ritz step (block SpMV with the
+ *   FP64 matrix, CholQR2 orthonormalisation, host dsyevd), until every wanted
+ *   residual ||Ax - theta x|| / |theta| computed in FP64 is below tol.
+ *   Needs a square CSR operator and which = largest/smallest real, largest
+ *   algebraic/magnitude or smallest algebraic. */
+#define B200_PRECISION_FP64 0
+#define B200_PRECISION_MIXED 1
+b200_status b200_eps_set_precision(b200_eps eps, int precision);
+/* Mixed-form parameters (0 or a negative value keeps the default): tol_low,
+ * the phase-1 tolerance (default 1e-6, never below tol); degree, the
+ * Chebyshev filter degree per sweep (default 24); guard, columns of the
+ * refinement block beyond nev (default max(8, nev/2)); max_sweeps (default
+ * 40). */
+b200_status b200_eps_set_mixed_options(b200_eps eps, double tol_low, int degree, int guard, int max_sweeps);
+
 /* EPSSetType: B200_EPS_KRYLOVSCHUR (default) or B200_EPS_LOBPCG. */
 #define B200_EPS_KRYLOVSCHUR 0
 #define B200_EPS_LOBPCG 1
@@ -297,6 +320,14 @@ typedef struct {
   double ms_spmv, ms_orth, ms_restart, ms_total;
   int64_t gs_bytes;
   int64_t column_visits;  /* sum over Lanczos steps j of (j+2): basis columns one CGS pass reads */
+  /* mixed precision (zero otherwise): refinement sweeps, Chebyshev degree, block columns,
+   * restarts of the FP32-basis phase, device time of the two phases, block SpMV columns */
+  int64_t filter_sweeps;
+  int64_t filter_degree;
+  int64_t block_size;
+  int64_t phase1_restarts;
+  double ms_phase1, ms_phase2;
+  int64_t spmm_columns;
 } b200_eps_stats;
 b200_status b200_eps_get_stats(b200_eps eps, b200_eps_stats *stats);
 /* Enable per-phase CUDA-event timing (adds events around each phase). */

@@ -51,7 +51,10 @@ class EPSStats(ctypes.Structure):
     _fields_ = [("lanczos_steps", ctypes.c_int64), ("gs_passes", ctypes.c_int64), ("restarts", ctypes.c_int64),
                 ("kernel_launches", ctypes.c_int64), ("ms_spmv", ctypes.c_double), ("ms_orth", ctypes.c_double),
                 ("ms_restart", ctypes.c_double), ("ms_total", ctypes.c_double), ("gs_bytes", ctypes.c_int64),
-                ("column_visits", ctypes.c_int64)]
+                ("column_visits", ctypes.c_int64), ("filter_sweeps", ctypes.c_int64),
+                ("filter_degree", ctypes.c_int64), ("block_size", ctypes.c_int64),
+                ("phase1_restarts", ctypes.c_int64), ("ms_phase1", ctypes.c_double), ("ms_phase2", ctypes.c_double),
+                ("spmm_columns", ctypes.c_int64)]
 
 
 _SIGS = {
@@ -72,6 +75,8 @@ _SIGS = {
     "b200_mat_get_sizes": (ctypes.c_int, [_vp, _ip, _ip]),
     "b200_mat_norm_inf": (ctypes.c_int, [_vp, _dp]),
     "b200_eps_set_type": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_eps_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_eps_set_mixed_options": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "b200_eps_lobpcg_set_block_size": (ctypes.c_int, [_vp, ctypes.c_int]),
     "b200_eps_lobpcg_set_restart": (ctypes.c_int, [_vp, ctypes.c_double]),
     "b200_eps_lobpcg_set_locking": (ctypes.c_int, [_vp, ctypes.c_int]),
@@ -531,6 +536,10 @@ class EPS:
     class Type:
         KRYLOVSCHUR, LOBPCG = 0, 1
 
+    class Precision:
+        FP64 = 0
+        MIXED = 1
+
     class PCType:
         NONE, JACOBI = 0, 1
 
@@ -589,6 +598,16 @@ class EPS:
     def setPreconditioner(self, pc):
         """STPRECOND with KSPPREONLY and PCNONE / PCJACOBI (EPS.PCType)."""
         _check(lib().b200_eps_set_preconditioner(self.handle, pc))
+
+    def setPrecision(self, precision):
+        """EPS.Precision.FP64 (default, the drop-in path) or EPS.Precision.MIXED: Krylov-Schur
+        on an FP32 basis with FP32 matrix values to a loose tolerance, then FP64
+        Chebyshev-filtered Rayleigh-Ritz refinement of the block of leading Ritz vectors."""
+        _check(lib().b200_eps_set_precision(self.handle, precision))
+
+    def setMixedOptions(self, tol_low=0.0, degree=0, guard=-1, max_sweeps=0):
+        """Parameters of the mixed form; 0 (or -1 for guard) keeps the default."""
+        _check(lib().b200_eps_set_mixed_options(self.handle, tol_low, degree, guard, max_sweeps))
 
     def setInitialSpaceDevice(self, v0_ptr):
         _check(lib().b200_eps_set_initial_space_device(self.handle, v0_ptr))

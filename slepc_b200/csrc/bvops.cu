@@ -31,12 +31,13 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// V(:,s:e) = V(:,l:k) * Q(l:k,s:e) ; kq = k-l, nc = e-s; MAXJ = ceil(nc/16) <= 8.
-// Q points at element (l,s) of the coefficient matrix (leading dimension ldq).
-template <int MAXJ>
-__global__ void __launch_bounds__(kGemmThreads) multinplace_kernel(double *V, int ld, int n, int l, int kq,
-                                                                   const double *__restrict__ Q, int ldq, int s,
-                                                                   int nc) {
+// Y(:,0:nc) = X(:,0:kq) * Q(0:kq,0:nc) ; MAXJ = ceil(nc/16) <= 8.  X and Y may overlap (the
+// in-place V(:,s:e) = V(:,l:k) Q(l:k,s:e) of BVMultInPlace): a panel of X is read completely before
+// any of its rows is written.  TI / TO are the stored types of X and Y (double, or float for the
+// FP32 basis of the mixed-precision solver); products and sums are FP64.
+template <int MAXJ, typename TI, typename TO>
+__global__ void __launch_bounds__(kGemmThreads) panel_gemm_kernel(const TI *X, int ldx, TO *Y, int ldy, int n, int kq,
+                                                                  const double *__restrict__ Q, int ldq, int nc) {
   extern __shared__ __align__(16) double sm[];
   double *Qs = sm;                          // [kq][nc] row-major by c: Qs[c*nc + j]
   double *As = sm + (size_t)kq * nc;        // input panel As[c*kRB + r]; then output tile Os[j*(kRB+1) + r]
@@ -54,7 +55,7 @@ __global__ void __launch_bounds__(kGemmThreads) multinplace_kernel(double *V, in
     __syncthreads();
     for (int idx = tid; idx < kq * kRB; idx += kGemmThreads) {
       const int c = idx / kRB, r = idx - c * kRB;
-      As[idx] = (r < rows) ? V[(size_t)(l + c) * ld + r0 + r] : 0.0;
+      As[idx] = (r < rows) ? (double)X[(size_t)c * ldx + r0 + r] : 0.0;
     }
     __syncthreads();
     double acc[4][MAXJ];
@@ -87,7 +88,7 @@ __global__ void __launch_bounds__(kGemmThreads) multinplace_kernel(double *V, in
     __syncthreads();
     for (int idx = tid; idx < nc * kRB; idx += kGemmThreads) {
       const int j = idx / kRB, r = idx - j * kRB;
-      if (r < rows) V[(size_t)(s + j) * ld + r0 + r] = As[j * (kRB + 1) + r];
+      if (r < rows) Y[(size_t)j * ldy + r0 + r] = (TO)As[j * (kRB + 1) + r];
     }
   }
 }
@@ -289,6 +290,83 @@ __global__ void colnorm_final_kernel(const double *__restrict__ partial, int nbl
   out[c] = sqrt(s);
 }
 
+// partial[c * gridDim.x + b] = sum over the block's rows of (AX(r,c) - theta[c] X(r,c))^2
+__global__ void colresid_partial_kernel(const double *__restrict__ AX, const double *__restrict__ X, int ld, int n,
+                                        const double *__restrict__ theta, double *partial) {
+  __shared__ double red[32];
+  const int c = blockIdx.y;
+  const long long rows_per = (n + gridDim.x - 1) / gridDim.x;
+  const long long r0 = (long long)blockIdx.x * rows_per, r1 = min((long long)n, r0 + rows_per);
+  const double *ax = AX + (size_t)c * ld, *x = X + (size_t)c * ld;
+  const double th = theta[c];
+  double acc = 0.0;
+  for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+    const double d = ax[r] - th * x[r];
+    acc = fma(d, d, acc);
+  }
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    partial[(size_t)c * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+__global__ void to_f32_kernel(float *dst, const double *__restrict__ src, long long len) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = __double2float_rn(src[i]);
+}
+
+// Gershgorin discs: partial[2b] = min_i (a_ii - sum_{j!=i} |a_ij|), partial[2b+1] = max_i (a_ii + ...)
+// over the rows of block b (grid-stride).
+template <typename VT>
+__global__ void gershgorin_partial_kernel(int n, const int *__restrict__ rowptr, const int *__restrict__ colind,
+                                          const VT *__restrict__ vals, double *partial) {
+  __shared__ double rlo[32], rhi[32];
+  double lo = 1.79769313486231571e+308, hi = -1.79769313486231571e+308;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double d = 0.0, rad = 0.0;
+    for (int p = rowptr[i]; p < rowptr[i + 1]; ++p) {
+      const double a = (double)vals[p];
+      if (colind[p] == i) d += a;
+      else rad += fabs(a);
+    }
+    lo = fmin(lo, d - rad);
+    hi = fmax(hi, d + rad);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, off));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    rlo[threadIdx.x >> 5] = lo;
+    rhi[threadIdx.x >> 5] = hi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+      lo = fmin(lo, rlo[w]);
+      hi = fmax(hi, rhi[w]);
+    }
+    partial[2 * blockIdx.x] = lo;
+    partial[2 * blockIdx.x + 1] = hi;
+  }
+}
+
+__global__ void gershgorin_final_kernel(const double *__restrict__ partial, int nblocks, double *out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double lo = 1.79769313486231571e+308, hi = -1.79769313486231571e+308;
+  for (int b = 0; b < nblocks; ++b) {
+    lo = fmin(lo, partial[2 * b]);
+    hi = fmax(hi, partial[2 * b + 1]);
+  }
+  out[0] = lo;
+  out[1] = hi;
+}
+
 __global__ void sum_final_kernel(const double *__restrict__ partial, int nblocks, double *out) {
   __shared__ double red[32];
   double acc = 0.0;
@@ -376,9 +454,9 @@ unsigned grid_for(long long len, int threads) {
 
 }  // namespace
 
-cudaError_t multinplace_launch(double *V, int ld, int n, int l, int k, const double *Q, int ldq, int s, int e,
-                               cudaStream_t stream) {
-  const int kq = k - l, nc = e - s;
+template <typename TI, typename TO>
+cudaError_t panel_gemm_launch(const TI *X, int ldx, TO *Y, int ldy, int n, int kq, const double *Q, int ldq, int nc,
+                              cudaStream_t stream) {
   if (nc <= 0 || kq <= 0 || n <= 0) return cudaSuccess;
   if (nc > 16 * 8 || kq > kMaxCols) return cudaErrorInvalidValue;
   const size_t smem = sizeof(double) * ((size_t)kq * nc + (size_t)(kq > nc ? kq : nc) * (kRB + 1));
@@ -389,11 +467,11 @@ cudaError_t multinplace_launch(double *V, int ld, int n, int l, int k, const dou
   if (grid > npanels) grid = npanels;
   cudaError_t err = cudaSuccess;
   switch (maxj) {
-#define B200_MIP_CASE(J)                                                                                         \
-  case J:                                                                                                        \
-    err = allow_max_dynamic_smem(multinplace_kernel<J>);                                                        \
-    if (err != cudaSuccess) return err;                                                                          \
-    multinplace_kernel<J><<<grid, kGemmThreads, smem, stream>>>(V, ld, n, l, kq, Q, ldq, s, nc);                 \
+#define B200_MIP_CASE(J)                                                                                   \
+  case J:                                                                                                  \
+    err = allow_max_dynamic_smem(panel_gemm_kernel<J, TI, TO>);                                            \
+    if (err != cudaSuccess) return err;                                                                    \
+    panel_gemm_kernel<J, TI, TO><<<grid, kGemmThreads, smem, stream>>>(X, ldx, Y, ldy, n, kq, Q, ldq, nc); \
     break;
     B200_MIP_CASE(1)
     B200_MIP_CASE(2)
@@ -407,6 +485,65 @@ cudaError_t multinplace_launch(double *V, int ld, int n, int l, int k, const dou
     default:
       return cudaErrorInvalidValue;
   }
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t multinplace_launch(double *V, int ld, int n, int l, int k, const double *Q, int ldq, int s, int e,
+                               cudaStream_t stream) {
+  return panel_gemm_launch<double, double>(V + (size_t)l * ld, ld, V + (size_t)s * ld, ld, n, k - l, Q, ldq, e - s,
+                                           stream);
+}
+
+cudaError_t multinplace_launch_f32(float *V, int ld, int n, int l, int k, const double *Q, int ldq, int s, int e,
+                                   cudaStream_t stream) {
+  return panel_gemm_launch<float, float>(V + (size_t)l * ld, ld, V + (size_t)s * ld, ld, n, k - l, Q, ldq, e - s,
+                                         stream);
+}
+
+cudaError_t panel_mult_launch(double *Y, int ldy, const double *X, int ldx, int n, int nx, int ny, const double *Q,
+                              int ldq, cudaStream_t stream) {
+  return panel_gemm_launch<double, double>(X, ldx, Y, ldy, n, nx, Q, ldq, ny, stream);
+}
+
+cudaError_t panel_mult_launch_f32(double *Y, int ldy, const float *X, int ldx, int n, int nx, int ny, const double *Q,
+                                  int ldq, cudaStream_t stream) {
+  return panel_gemm_launch<float, double>(X, ldx, Y, ldy, n, nx, Q, ldq, ny, stream);
+}
+
+cudaError_t colresid_launch(const double *AX, const double *X, int ld, int n, int k, const double *theta, double *out,
+                            double *work, int work_len, cudaStream_t stream) {
+  if (k <= 0) return cudaSuccess;
+  int blocks = num_sms();
+  if (blocks * k > work_len) blocks = work_len / k;
+  if (blocks < 1) return cudaErrorInvalidValue;
+  colresid_partial_kernel<<<dim3(blocks, k), 256, 0, stream>>>(AX, X, ld, n, theta, work);
+  count_launch();
+  colnorm_final_kernel<<<(k + 127) / 128, 128, 0, stream>>>(work, blocks, k, out);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t to_f32_launch(float *dst, const double *src, long long len, cudaStream_t stream) {
+  if (len <= 0) return cudaSuccess;
+  to_f32_kernel<<<grid_for(len, 256), 256, 0, stream>>>(dst, src, len);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t gershgorin_launch(int n, const int *rowptr, const int *colind, const void *vals, bool f32, double *out,
+                              double *work, int work_len, cudaStream_t stream) {
+  int blocks = (int)grid_for(n, 256);
+  if (2 * blocks > work_len) blocks = work_len / 2;
+  if (blocks < 1) return cudaErrorInvalidValue;
+  if (f32)
+    gershgorin_partial_kernel<float><<<blocks, 256, 0, stream>>>(n, rowptr, colind, static_cast<const float *>(vals),
+                                                                  work);
+  else
+    gershgorin_partial_kernel<double><<<blocks, 256, 0, stream>>>(n, rowptr, colind,
+                                                                   static_cast<const double *>(vals), work);
+  count_launch();
+  gershgorin_final_kernel<<<1, 32, 0, stream>>>(work, blocks, out);
   count_launch();
   return cudaGetLastError();
 }

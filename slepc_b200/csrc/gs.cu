@@ -123,6 +123,7 @@ struct PassParams {
   int chunk;       // rows per chunk (power of two, 32..256)
   int stages;      // pipeline stages (2..kMaxStages)
   int box_cols;    // columns fetched by the 2-D tile load (jb, or jb+1 when w is column jb)
+  int stage_bytes; // bytes of one stage: CH rows of the jb basis columns (stored type) and of w (FP64)
   int nchunks;
   int G;           // CTAs in the grid
 };
@@ -254,7 +255,10 @@ __device__ void decide(const PassParams &p, const double *cnew_s, DecideShared &
 // stage's bytes have landed, empty[s] when the 8 consumer warps are done with
 // it.  Consumers synchronise among themselves only between the update (which
 // rewrites w) and the dot (which reads the new w).
-template <int MAXCPW>
+//
+// TS is the stored type of the basis: double, or float for the FP32 basis of the mixed-precision
+// solver (w, the coefficients and every product and sum stay FP64).
+template <int MAXCPW, typename TS>
 __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, const __grid_constant__ CUtensorMap tmap) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   GsState *st = p.st;
@@ -283,8 +287,9 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
   __shared__ int is_last, timed_out, n_issued;
   __shared__ double upd[2 * kConsumers];      // partial update sums (TPR*CH = kConsumers per chunk), by chunk parity
   const size_t head = 128 + sizeof(double) * (2 * kMaxCols + 1) + ((sizeof(DecideShared) + 127) / 128) * 128;
-  double *stage_base = reinterpret_cast<double *>(smem_raw + ((head + 127) / 128) * 128);
-  const size_t stage_elems = (size_t)CH * (jb + 1);
+  unsigned char *stage_base = smem_raw + ((head + 127) / 128) * 128;
+  const size_t stage_bytes = (size_t)p.stage_bytes;
+  const size_t w_offset = (size_t)CH * jb * sizeof(TS);  // w follows the basis columns in a stage
 
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
@@ -300,7 +305,7 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
 
   const int G = p.G;
   const int nmine = (p.nchunks > (int)blockIdx.x) ? (p.nchunks - 1 - (int)blockIdx.x) / G + 1 : 0;
-  double *Vw = a.V + (size_t)a.wcol * a.ld;
+  double *Vw = a.wvec ? a.wvec : a.V + (size_t)a.wcol * a.ld;
   int consumed = 0;
 
   // dot accumulators: lane-private partial sums of the columns this warp owns, across all chunks
@@ -320,16 +325,16 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
       }
       const long long r0 = ((long long)blockIdx.x + (long long)i * G) * CH;
       const int rows = (int)min((long long)CH, (long long)a.n - r0);
-      double *buf = stage_base + (size_t)s * stage_elems;
+      unsigned char *buf = stage_base + (size_t)s * stage_bytes;
       if (lane == 0) {
         // one tile load brings the basis columns (and w when it is column jb); rows past n read as zeros
         const bool tile = ncl > 0;
         const bool w_in_tile = tile && p.box_cols == jb + 1;
         const uint32_t wbytes = w_in_tile ? 0u : (uint32_t)(((rows * 8) + 15) & ~15);
-        const uint32_t tbytes = tile ? (uint32_t)CH * 8u * (uint32_t)p.box_cols : 0u;
+        const uint32_t tbytes = tile ? (uint32_t)CH * (uint32_t)sizeof(TS) * (uint32_t)p.box_cols : 0u;
         mbar_arrive_expect_tx(&full[s], tbytes + wbytes);
         if (tile) tma_load_2d(buf, &tmap, (int)r0, 0, &full[s]);
-        if (!w_in_tile) bulk_load(buf + (size_t)jb * CH, Vw + r0, wbytes, &full[s]);
+        if (!w_in_tile) bulk_load(buf + w_offset, Vw + r0, wbytes, &full[s]);
         n_issued = i + 1;
       }
       __syncwarp();
@@ -349,8 +354,9 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
       const bool ok = mbar_wait_bounded(&full[s], (uint32_t)((i / S) & 1));
       const long long r0 = ((long long)blockIdx.x + (long long)i * G) * CH;
       const int rows = (int)min((long long)CH, (long long)a.n - r0);
-      const double *Vs = stage_base + (size_t)s * stage_elems;  // column c at Vs + c*CH, w after the basis
-      const double *wsrc = Vs + (size_t)jb * CH;
+      const unsigned char *sbuf = stage_base + (size_t)s * stage_bytes;
+      const TS *Vs = reinterpret_cast<const TS *>(sbuf);  // column c at Vs + c*CH, w after the basis
+      const double *wsrc = reinterpret_cast<const double *>(sbuf + w_offset);
       double *up = upd + (i & 1) * kConsumers;  // partial update sums of this chunk
       const bool rewrite = do_update || do_scale;
       if (rewrite) {
@@ -358,10 +364,10 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
           double s0 = 0.0, s1 = 0.0;
           int c = part;
           for (; c + TPR < jb; c += 2 * TPR) {
-            s0 = fma(Vs[(size_t)c * CH + urow], coef_s[c], s0);
-            s1 = fma(Vs[(size_t)(c + TPR) * CH + urow], coef_s[c + TPR], s1);
+            s0 = fma((double)Vs[(size_t)c * CH + urow], coef_s[c], s0);
+            s1 = fma((double)Vs[(size_t)(c + TPR) * CH + urow], coef_s[c + TPR], s1);
           }
-          if (c < jb) s0 = fma(Vs[(size_t)c * CH + urow], coef_s[c], s0);
+          if (c < jb) s0 = fma((double)Vs[(size_t)c * CH + urow], coef_s[c], s0);
           up[part * CH + urow] = s0 + s1;
         }
         if (consumer_sync_or(!ok)) break;  // partial sums complete (and a timed-out wait is agreed on)
@@ -389,7 +395,7 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
 #pragma unroll
           for (int t = 0; t < MAXCPW; ++t) {
             const int c = warp + kConsumerWarps * t;
-            if (c < jb) acc[t] = fma(Vs[(size_t)c * CH + r], wr, acc[t]);
+            if (c < jb) acc[t] = fma((double)Vs[(size_t)c * CH + r], wr, acc[t]);
             else if (c == jb) acc[t] = fma(wr, wr, acc[t]);
           }
         }
@@ -428,7 +434,8 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
   __threadfence();
   if (tid == 0) {
     // algorithmic traffic of this pass: streamed columns + w read, w written back if changed
-    st->bytes += (unsigned long long)a.n * 8ull * (unsigned long long)(ncl + 1 + ((do_update || do_scale) ? 1 : 0));
+    st->bytes += (unsigned long long)a.n *
+                 ((unsigned long long)sizeof(TS) * ncl + 8ull * (1ull + ((do_update || do_scale) ? 1ull : 0ull)));
     st->passes += 1;
   }
   if (!do_dot) {
@@ -457,14 +464,17 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
   decide(p, cnew_s, *dsh);
 }
 
-size_t pass_smem_bytes(int jb, int CH, int stages) {
+// bytes of one pipeline stage: CH rows of jb basis columns of ts bytes each, then CH rows of w (FP64)
+size_t pass_stage_bytes(int jb, int CH, size_t ts) { return (size_t)CH * ((size_t)jb * ts + sizeof(double)); }
+
+size_t pass_smem_bytes(int jb, int CH, int stages, size_t ts) {
   const size_t head = 128 + sizeof(double) * (2 * kMaxCols + 1) + ((sizeof(DecideShared) + 127) / 128) * 128;
-  return ((head + 127) / 128) * 128 + (size_t)stages * CH * (jb + 1) * sizeof(double);
+  return ((head + 127) / 128) * 128 + (size_t)stages * pass_stage_bytes(jb, CH, ts);
 }
 
 // Rows per chunk: the largest power of two (32..256, the tile box limit) whose stage fits the target size.
-int pass_chunk_rows(int jb) {
-  const size_t rows = kStageTarget / ((size_t)(jb + 1) * sizeof(double));
+int pass_chunk_rows(int jb, size_t ts) {
+  const size_t rows = kStageTarget / ((size_t)jb * ts + sizeof(double));
   int ch = 32;
   while (ch < kMaxChunk && (size_t)(2 * ch) <= rows) ch *= 2;
   return ch;
@@ -484,38 +494,40 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 // Tensor map over the basis: dim 0 = rows (n, contiguous), dim 1 = columns (stride ld), box CH x box_cols.
 cudaError_t make_tmap(CUtensorMap *tm, const GsPassArgs &a, int CH, int box_cols, int total_cols) {
+  const bool f32 = a.V32 != nullptr;
   memset(tm, 0, sizeof(*tm));
   if (box_cols <= 0) return cudaSuccess;  // no tile load in this pass
   PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
   if (!enc) return cudaErrorNotSupported;
   const cuuint64_t dims[2] = {(cuuint64_t)a.n, (cuuint64_t)total_cols};
-  const cuuint64_t strides[1] = {(cuuint64_t)a.ld * sizeof(double)};
+  const cuuint64_t strides[1] = {f32 ? (cuuint64_t)a.ld32 * sizeof(float) : (cuuint64_t)a.ld * sizeof(double)};
   const cuuint32_t box[2] = {(cuuint32_t)CH, (cuuint32_t)box_cols};
   const cuuint32_t estr[2] = {1, 1};
-  CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void *)a.V, dims, strides, box, estr,
+  CUresult r = enc(tm, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2,
+                   f32 ? (void *)a.V32 : (void *)a.V, dims, strides, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-int pass_stages(int jb, int CH) {
-  const size_t stage = (size_t)CH * (jb + 1) * sizeof(double);
+int pass_stages(int jb, int CH, size_t ts) {
+  const size_t stage = pass_stage_bytes(jb, CH, ts);
   size_t s = kStageBudget / stage;
   if (s > (size_t)kMaxStages) s = kMaxStages;
   return (int)s;
 }
 
-template <int M>
+template <int M, typename TS>
 cudaError_t launch_pass_t(const PassParams &p, const CUtensorMap &tm, size_t smem, cudaStream_t stream) {
   static bool attr_set[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !attr_set[dev]) {
-    cudaError_t e = allow_max_dynamic_smem(gs_pass_kernel<M>);
+    cudaError_t e = allow_max_dynamic_smem(gs_pass_kernel<M, TS>);
     if (e != cudaSuccess) return e;
     attr_set[dev] = true;
   }
-  gs_pass_kernel<M><<<p.G, kThreads, smem, stream>>>(p, tm);
+  gs_pass_kernel<M, TS><<<p.G, kThreads, smem, stream>>>(p, tm);
   return cudaGetLastError();
 }
 
@@ -528,8 +540,12 @@ cudaError_t launch_pass(const GsPassArgs &a, const GsWork &w, int first, int pla
   p.partials = w.partials;
   p.first = first;
   p.plain_dot = plain_dot;
-  p.chunk = pass_chunk_rows(a.jb);
-  p.stages = pass_stages(a.jb, p.chunk);
+  const bool f32 = a.V32 != nullptr;
+  const size_t ts = f32 ? sizeof(float) : sizeof(double);
+  if (f32 && !a.wvec) return cudaErrorInvalidValue;  // w is FP64 and kept apart from an FP32 basis
+  p.chunk = pass_chunk_rows(a.jb, ts);
+  p.stages = pass_stages(a.jb, p.chunk, ts);
+  p.stage_bytes = (int)pass_stage_bytes(a.jb, p.chunk, ts);
   if (p.stages < 2) return cudaErrorInvalidValue;
   p.nchunks = (a.n + p.chunk - 1) / p.chunk;
   int G = w.num_sms;
@@ -537,20 +553,28 @@ cudaError_t launch_pass(const GsPassArgs &a, const GsWork &w, int first, int pla
   if (G > p.nchunks) G = p.nchunks;
   if (G < 1) G = 1;
   p.G = G;
-  const size_t smem = pass_smem_bytes(a.jb, p.chunk, p.stages);
+  const size_t smem = pass_smem_bytes(a.jb, p.chunk, p.stages, ts);
   if (smem + 4096 > max_dynamic_smem()) return cudaErrorInvalidValue;
   // w is column jb in the column variant: one box covers basis and w
-  p.box_cols = (a.wcol == a.jb) ? a.jb + 1 : a.jb;
+  p.box_cols = (a.wcol == a.jb && !a.wvec && !f32) ? a.jb + 1 : a.jb;
   CUtensorMap tm;
   cudaError_t e = make_tmap(&tm, a, p.chunk, p.box_cols, a.total_cols);
   if (e != cudaSuccess) return e;
   const int cpw = (a.jb + 1 + kConsumerWarps - 1) / kConsumerWarps;  // dot columns per consumer warp (basis + self)
-  if (cpw <= 2) e = launch_pass_t<2>(p, tm, smem, stream);
-  else if (cpw <= 4) e = launch_pass_t<4>(p, tm, smem, stream);
-  else if (cpw <= 8) e = launch_pass_t<8>(p, tm, smem, stream);
-  else if (cpw <= 12) e = launch_pass_t<12>(p, tm, smem, stream);
-  else if (cpw <= 16) e = launch_pass_t<16>(p, tm, smem, stream);
-  else if (cpw <= 32) e = launch_pass_t<32>(p, tm, smem, stream);
+  if (f32) {
+    if (cpw <= 2) e = launch_pass_t<2, float>(p, tm, smem, stream);
+    else if (cpw <= 4) e = launch_pass_t<4, float>(p, tm, smem, stream);
+    else if (cpw <= 8) e = launch_pass_t<8, float>(p, tm, smem, stream);
+    else if (cpw <= 12) e = launch_pass_t<12, float>(p, tm, smem, stream);
+    else if (cpw <= 16) e = launch_pass_t<16, float>(p, tm, smem, stream);
+    else if (cpw <= 32) e = launch_pass_t<32, float>(p, tm, smem, stream);
+    else return cudaErrorInvalidValue;
+  } else if (cpw <= 2) e = launch_pass_t<2, double>(p, tm, smem, stream);
+  else if (cpw <= 4) e = launch_pass_t<4, double>(p, tm, smem, stream);
+  else if (cpw <= 8) e = launch_pass_t<8, double>(p, tm, smem, stream);
+  else if (cpw <= 12) e = launch_pass_t<12, double>(p, tm, smem, stream);
+  else if (cpw <= 16) e = launch_pass_t<16, double>(p, tm, smem, stream);
+  else if (cpw <= 32) e = launch_pass_t<32, double>(p, tm, smem, stream);
   else return cudaErrorInvalidValue;
   count_launch();
   return e;

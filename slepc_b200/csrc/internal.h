@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include "slepc_b200.h"
+#include "kernels.h"
 
 namespace b200 {
 // The cross shell of A: A^T A, or A A^T when swapped (the m < n case, which
@@ -24,4 +25,17 @@ b200_status bv_column_norms(b200_bv bv, double *nrm);
 int num_sms_host();
 // EPSSolve with EPSLOBPCG (lobpcg.cu).
 b200_status lobpcg_solve(b200_eps eps);
+// Krylov-Schur with b200_eps_set_precision(MIXED) after the setup (mixed.cu).
+b200_status mixed_solve(b200_eps eps);
+// Read the Gram-Schmidt control block after a stream synchronisation (maps device errors).
+b200_status bv_state(b200_bv bv, GsState *out);
+// Sliced-ELL copy and FP32 value copies of a square CSR operator for the mixed solver.
+b200_status mat_mixed_prepare(b200_mat A, cudaStream_t s);
+// y = A x with FP32 values and FP32 x (products and sums FP64); gated on st/step like the SpMV.
+cudaError_t mat_spmv_x32(b200_mat A, const float *x, double *y, cudaStream_t stream, const GsState *st, int step);
+// Out(:,b) = alpha (A Y(:,b) - shift Y(:,b)) - beta X(:,b), b < nb, with the operator's own values.
+cudaError_t mat_spmm(b200_mat A, const double *Y, const double *X, double *Out, int ld, int nb, double alpha,
+                     double shift, double beta, cudaStream_t stream);
+// out[0..1] (device) = Gershgorin bounds of the spectrum of A.
+cudaError_t mat_gershgorin(b200_mat A, double *out, double *work, int work_len, cudaStream_t stream);
 }  // namespace b200

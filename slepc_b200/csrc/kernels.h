@@ -69,6 +69,7 @@ struct SellPlan {
   std::vector<unsigned> mask;
   long long entries = 0;
   WarpTiles rest;
+  std::vector<int> rest_rows;  // the rows left out of the slices, ascending
 };
 SellPlan spmv_sell_plan(int n, const int *rowptr_host);
 struct SpmvSell {
@@ -79,6 +80,10 @@ struct SpmvSell {
   void *vals = nullptr;  // double or float, like the matrix
   int *cols = nullptr;
   SpmvTiles rest;
+  long long entries = 0;     // slice entries (padding included)
+  int *rest_rows = nullptr;  // rows left out of the slices (block SpMV: one warp per row)
+  int nrest = 0;
+  float *vals32 = nullptr;   // FP32 copy of vals for the mixed-precision solver (FP64 matrices only)
 };
 cudaError_t spmv_sell_launch(const SpmvSell &S, int n, const SpmvTiles &rest, const int *rowptr, const int *colind,
                              const double *vals, const double *x, double *y, cudaStream_t stream,
@@ -86,6 +91,18 @@ cudaError_t spmv_sell_launch(const SpmvSell &S, int n, const SpmvTiles &rest, co
 cudaError_t spmv_sell_launch_f32(const SpmvSell &S, int n, const SpmvTiles &rest, const int *rowptr,
                                  const int *colind, const float *vals, const double *x, double *y,
                                  cudaStream_t stream, const GsState *st = nullptr, int step = 0);
+// FP32 values and FP32 x (the FP32 basis of the mixed-precision solver); products and sums FP64.
+// svals: the slices' FP32 values; vals: FP32 CSR values for the rows outside the slices.
+cudaError_t spmv_sell_launch_x32(const SpmvSell &S, const float *svals, int n, const SpmvTiles &rest,
+                                 const int *rowptr, const int *colind, const float *vals, const float *x, double *y,
+                                 cudaStream_t stream, const GsState *st = nullptr, int step = 0);
+// Block SpMV with a fused three-term update (block.cu), FP64:
+//   Out(:,b) = alpha * (A Y(:,b) - shift * Y(:,b)) - beta * X(:,b),  b < nb
+// (X may be null: no beta term).  Y, X and Out are column-major with leading dimension ld; Out
+// must not overlap Y or X.  The slices are read once per group of 8 columns.
+cudaError_t spmm_sell_launch(const SpmvSell &S, int n, const int *rowptr, const int *colind, const void *vals, bool f32,
+                             const double *Y, const double *X, double *Out, int ld, int nb, double alpha, double shift,
+                             double beta, cudaStream_t stream);
 // The slices' columns and values from the CSR arrays in HBM (S.off/width/mask already on the device).
 cudaError_t sell_gather(int n, const SpmvSell &S, const int *rowptr, const int *colind, const void *vals, bool f32,
                         cudaStream_t stream);
@@ -128,6 +145,12 @@ struct GsPassArgs {
   int normalize;  // scale by 1/norm at the end
   int column;     // 1: column variant (BV_SafeSqrt check on w^T w)
   int total_cols; // columns allocated from V (bounds of the tile loads)
+  // FP32 basis (mixed-precision solver): when V32 is set the basis columns are read from V32
+  // (leading dimension ld32) and the vector being orthogonalised is the FP64 vector wvec (n + 2
+  // entries allocated); wvec may also be set with an FP64 basis.
+  const float *V32;
+  int ld32;
+  double *wvec;
 };
 
 // Enqueue the full CGS + DGKS("if needed") orthogonalisation of one column:
@@ -150,6 +173,22 @@ cudaError_t csr_transpose_device(int rows, int cols, long long nnz, const int *r
 // V(:,s:e) = V(:,l:k) * Q(l:k,s:e), row-blocked, in place; Q points at element (l,s).
 cudaError_t multinplace_launch(double *V, int ld, int n, int l, int k, const double *Q, int ldq, int s, int e,
                                cudaStream_t stream);
+// The same on an FP32 basis (products and sums FP64, results rounded to FP32).
+cudaError_t multinplace_launch_f32(float *V, int ld, int n, int l, int k, const double *Q, int ldq, int s, int e,
+                                   cudaStream_t stream);
+// Y(:,0:ny) = X(:,0:nx) Q(0:nx,0:ny) with the row-panel kernel (ny <= 128, X and Y distinct).
+cudaError_t panel_mult_launch(double *Y, int ldy, const double *X, int ldx, int n, int nx, int ny, const double *Q,
+                              int ldq, cudaStream_t stream);
+cudaError_t panel_mult_launch_f32(double *Y, int ldy, const float *X, int ldx, int n, int nx, int ny, const double *Q,
+                                  int ldq, cudaStream_t stream);
+// out[c] = ||AX(:,c) - theta[c] X(:,c)||_2 for c < k (theta and out on the device), deterministic.
+cudaError_t colresid_launch(const double *AX, const double *X, int ld, int n, int k, const double *theta, double *out,
+                            double *work, int work_len, cudaStream_t stream);
+// dst = src rounded to FP32.
+cudaError_t to_f32_launch(float *dst, const double *src, long long len, cudaStream_t stream);
+// out[0], out[1] = the smallest left and largest right end of the Gershgorin discs (device).
+cudaError_t gershgorin_launch(int n, const int *rowptr, const int *colind, const void *vals, bool f32, double *out,
+                              double *work, int work_len, cudaStream_t stream);
 // Y(:,0:ny) = alpha * X(:,0:nx) * Q(0:nx,0:ny) + beta * Y(:,0:ny)   (X != Y storage)
 cudaError_t mult_launch(double *Y, int ldy, const double *X, int ldx, int n, int nx, int ny, const double *Q, int ldq,
                         double alpha, double beta, cudaStream_t stream);

@@ -74,6 +74,9 @@ static void part_free(CsrPart &P) {
   cudaFree(P.sell.rest.segs);
   cudaFree(P.sell.rest.longrows);
   cudaFree(P.sell.rest.partials);
+  cudaFree(P.sell.rest_rows);
+  cudaFree(P.sell.vals32);
+  cudaFree(P.vals32);
   P = CsrPart{};
 }
 
@@ -165,6 +168,13 @@ static b200_status part_build_sell(CsrPart &P, const int *rowptr_host, cudaStrea
     B200_CUDA_CHECK(cudaMemcpyAsync(S.width, sp.width.data(), sizeof(int) * S.nslices, cudaMemcpyHostToDevice, s));
     B200_CUDA_CHECK(cudaMemcpyAsync(S.mask, sp.mask.data(), sizeof(unsigned) * S.nslices, cudaMemcpyHostToDevice, s));
     B200_CUDA_CHECK(sell_gather(P.rows, S, P.rowptr, P.colind, P.vals, P.f32, s));
+  }
+  S.entries = sp.entries;
+  S.nrest = (int)sp.rest_rows.size();
+  if (S.nrest) {
+    B200_CUDA_CHECK(cudaMalloc(&S.rest_rows, sizeof(int) * sp.rest_rows.size()));
+    B200_CUDA_CHECK(cudaMemcpyAsync(S.rest_rows, sp.rest_rows.data(), sizeof(int) * sp.rest_rows.size(),
+                                    cudaMemcpyHostToDevice, s));
   }
   WarpTiles &wt = sp.rest;
   S.rest.ntiles = (int)wt.tiles.size();
@@ -357,6 +367,41 @@ cudaError_t mat_apply(b200_mat A, const double *x, double *y, cudaStream_t strea
 }  // namespace b200
 
 extern "C" b200_status b200_mat_create_cross(b200_mat A, b200_mat *C) { return mat_create_cross_ex(A, false, C); }
+
+// The sliced-ELL copy of a square CSR operator and, for FP64 values, FP32 copies of its values
+// (CSR and slices) for the FP32 phase of the mixed-precision solver.
+b200_status b200::mat_mixed_prepare(b200_mat A, cudaStream_t s) {
+  B200_ARG_CHECK(A->kind == kMatCsr && A->m == A->n, "the mixed-precision solver needs a square CSR operator");
+  CsrPart &P = A->a;
+  B200_CHECK(part_build_sell(P, nullptr, s));
+  if (!P.f32 && !P.vals32) {
+    B200_CUDA_CHECK(cudaMalloc(&P.vals32, sizeof(float) * (size_t)(P.nnz > 0 ? P.nnz : 1)));
+    B200_CUDA_CHECK(cudaMalloc(&P.sell.vals32, sizeof(float) * (size_t)(P.sell.entries > 0 ? P.sell.entries : 1)));
+    B200_CUDA_CHECK(to_f32_launch(P.vals32, static_cast<const double *>(P.vals), P.nnz, s));
+    B200_CUDA_CHECK(to_f32_launch(P.sell.vals32, static_cast<const double *>(P.sell.vals), P.sell.entries, s));
+  }
+  return B200_OK;
+}
+
+cudaError_t b200::mat_spmv_x32(b200_mat A, const float *x, double *y, cudaStream_t stream, const GsState *st,
+                               int step) {
+  const CsrPart &P = A->a;
+  const float *svals = P.f32 ? static_cast<const float *>(P.sell.vals) : P.sell.vals32;
+  const float *cvals = P.f32 ? static_cast<const float *>(P.vals) : P.vals32;
+  return spmv_sell_launch_x32(P.sell, svals, P.rows, P.sell.rest, P.rowptr, P.colind, cvals, x, y, stream, st, step);
+}
+
+cudaError_t b200::mat_spmm(b200_mat A, const double *Y, const double *X, double *Out, int ld, int nb, double alpha,
+                           double shift, double beta, cudaStream_t stream) {
+  const CsrPart &P = A->a;
+  return spmm_sell_launch(P.sell, P.rows, P.rowptr, P.colind, P.vals, P.f32, Y, X, Out, ld, nb, alpha, shift, beta,
+                          stream);
+}
+
+cudaError_t b200::mat_gershgorin(b200_mat A, double *out, double *work, int work_len, cudaStream_t stream) {
+  const CsrPart &P = A->a;
+  return gershgorin_launch(P.rows, P.rowptr, P.colind, P.vals, P.f32, out, work, work_len, stream);
+}
 
 extern "C" b200_status b200_mat_mult(b200_mat A, const double *x, double *y) {
   B200_ARG_CHECK(A && x && y, "null argument");
@@ -658,6 +703,8 @@ static b200_status bv_read_state(b200_bv bv, GsState *out) {
   if (out->err) B200_DEV_ERR("a Gram-Schmidt kernel reported a device-side error (bounded wait expired)");
   return B200_OK;
 }
+
+b200_status b200::bv_state(b200_bv bv, GsState *out) { return bv_read_state(bv, out); }
 
 // Orthogonalise column j against columns 0..j-1 (column variant).
 b200_status b200::bv_orth_column(b200_bv bv, int j, int normalize, double *H, double *norm, int *lindep) {
@@ -1083,6 +1130,10 @@ extern "C" b200_status b200_eps_destroy(b200_eps eps) {
   cudaFree(eps->resid_buf);
   cudaFree(eps->op_buf);
   cudaFree(eps->dinv);
+  cudaFree(eps->V32);
+  cudaFree(eps->wv);
+  cudaFree(eps->blk);
+  cudaFree(eps->mred);
   delete eps;
   return B200_OK;
 }
@@ -1158,6 +1209,24 @@ extern "C" b200_status b200_eps_set_initial_space_block(b200_eps eps, int k, con
   eps->nini_block = k;
   eps->nini = k;
   eps->solved = false;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_set_precision(b200_eps eps, int precision) {
+  B200_ARG_CHECK(eps, "null argument");
+  B200_ARG_CHECK(precision == B200_PRECISION_FP64 || precision == B200_PRECISION_MIXED, "unknown precision");
+  eps->precision = precision;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_set_mixed_options(b200_eps eps, double tol_low, int degree, int guard,
+                                                  int max_sweeps) {
+  B200_ARG_CHECK(eps, "null argument");
+  B200_ARG_CHECK(degree <= 4096 && max_sweeps <= 100000, "degree or max_sweeps too large");
+  eps->mixed_tol_low = tol_low > 0.0 ? tol_low : 0.0;
+  eps->mixed_degree = degree > 0 ? degree : 0;
+  eps->mixed_guard = guard >= 0 ? guard : -1;
+  eps->mixed_max_sweeps = max_sweeps > 0 ? max_sweeps : 0;
   return B200_OK;
 }
 
@@ -1294,6 +1363,7 @@ extern "C" b200_status b200_eps_solve(b200_eps eps) {
   B200_ARG_CHECK(eps, "null argument");
   if (eps->type == B200_EPS_LOBPCG) return lobpcg_solve(eps);
   B200_CHECK(eps_setup(eps));
+  if (eps->precision == B200_PRECISION_MIXED) return mixed_solve(eps);
   b200_bv V = eps->V;
   DsHep &ds = eps->ds;
   const int ncv = eps->ncv_, mpd = eps->mpd_, nev = eps->nev;

@@ -24,6 +24,7 @@ struct CsrPart {
   b200::SpmvTiles wt;                // warp tiles, long-row segments and their partial-sum slots
   b200::SpmvSell sell;               // sliced-ELL copy (built when that schedule is selected)
   bool sell_ready = false;
+  float *vals32 = nullptr;           // FP32 copy of FP64 values for the mixed-precision solver
 };
 
 enum MatKind { kMatCsr = 0, kMatCross = 1 };
@@ -106,5 +107,20 @@ struct b200_eps_s {
   int nini_eff = 0;  // initial vectors kept by BVInsertVecs in the last setup
   double *dinv = nullptr;  // device inverse diagonal for the Jacobi preconditioner
   const void *dinv_of = nullptr;
+  // mixed-precision Krylov-Schur (b200_eps_set_precision): parameters and device buffers
+  int precision = B200_PRECISION_FP64;
+  double mixed_tol_low = 0.0;  // phase-1 tolerance (0: default)
+  int mixed_degree = 0;        // Chebyshev degree (0: default)
+  int mixed_guard = -1;        // guard columns of the refinement block (-1: default)
+  int mixed_max_sweeps = 0;    // refinement sweeps (0: default)
+  float *V32 = nullptr;        // FP32 basis, ld32 x (ncv + 1)
+  size_t V32_cap = 0;
+  int ld32 = 0;
+  double *wv = nullptr;        // FP64 vector being orthogonalised (n + 2)
+  size_t wv_cap = 0;
+  double *blk = nullptr;       // 5 FP64 blocks of ldb x kb for the refinement phase
+  size_t blk_cap = 0;
+  double *mred = nullptr;      // reductions and small device matrices of the refinement phase
+  size_t mred_cap = 0;
 };
 

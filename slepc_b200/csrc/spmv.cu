@@ -92,12 +92,12 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_rowblock_kernel(const int *
 // row i of the tile in index order (the order of a sequential CSR loop).  Full occupancy (2048
 // threads per SM): the short loads of many warps hide the gather latency.
 // VT is the stored value type (double, or float for FP32 storage); products and sums are FP64.
-template <typename VT>
+template <typename VT, typename XT>
 __global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles, const int4 *__restrict__ tiles,
                                                                      const int *__restrict__ rowptr,
                                                                      const int *__restrict__ colind,
                                                                      const VT *__restrict__ vals,
-                                                                     const double *__restrict__ x,
+                                                                     const XT *__restrict__ x,
                                                                      double *__restrict__ y,
                                                                      const GsState *__restrict__ st, int step) {
   if (st && st->halt && st->halt_step < step) return;
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles,
 #pragma unroll
     for (int u = 0; u < kWarpTileNnz / 32; ++u) {
       const int q = lane + 32 * u;
-      if (q < cnt) prod[q] = __dmul_rn((double)a[u], __ldg(x + c[u]));
+      if (q < cnt) prod[q] = __dmul_rn((double)a[u], (double)__ldg(x + c[u]));
     }
     __syncwarp();
     if (lane < nrows) {
@@ -141,11 +141,11 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_warptile_kernel(int ntiles,
 // The same warp tiles with a two-tile software pipeline: while a warp gathers x for tile t it
 // already has the values and column indices of its next tile in flight (half occupancy, twice
 // the loads in flight per warp).  Same sums in the same order as spmv_warptile_kernel.
-template <typename VT>
+template <typename VT, typename XT>
 __global__ void __launch_bounds__(kSpmvThreads, sizeof(VT) == 4 ? 4 : 3)
     spmv_warptile_pipelined_kernel(int ntiles, const int4 *__restrict__ tiles, const int *__restrict__ rowptr,
                                    const int *__restrict__ colind, const VT *__restrict__ vals,
-                                   const double *__restrict__ x, double *__restrict__ y,
+                                   const XT *__restrict__ x, double *__restrict__ y,
                                    const GsState *__restrict__ st, int step) {
   if (st && st->halt && st->halt_step < step) return;
   __shared__ double prod_all[kSpmvThreads / 32][kWarpTileNnz];
@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(kSpmvThreads, sizeof(VT) == 4 ? 4 : 3)
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int q = lane + 32 * u;
-      if (q < cnt) prod[q] = __dmul_rn((double)a[u], __ldg(x + c[u]));
+      if (q < cnt) prod[q] = __dmul_rn((double)a[u], (double)__ldg(x + c[u]));
     }
     __syncwarp();
     if (lane < nrows) {
@@ -210,13 +210,13 @@ __global__ void __launch_bounds__(kSpmvThreads, sizeof(VT) == 4 ? 4 : 3)
 // row 32s+i in index order (the same bits as a sequential CSR loop) with loads of 32 consecutive
 // entries per instruction.  Rows with more than kSellMaxRow nonzeros are not in the slices
 // (their mask bit is 0) and are computed by the tile or segment kernels.
-template <typename VT>
+template <typename VT, typename XT>
 __global__ void __launch_bounds__(kSpmvThreads) spmv_sell_kernel(int nslices, int n, const long long *__restrict__ off,
                                                                  const int *__restrict__ width,
                                                                  const unsigned *__restrict__ mask,
                                                                  const VT *__restrict__ sval,
                                                                  const int *__restrict__ scol,
-                                                                 const double *__restrict__ x, double *__restrict__ y,
+                                                                 const XT *__restrict__ x, double *__restrict__ y,
                                                                  const GsState *__restrict__ st, int step) {
   if (st && st->halt && st->halt_step < step) return;
   const int lane = threadIdx.x & 31;
@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_sell_kernel(int nslices, in
       }
 #pragma unroll
       for (int u = 0; u < 8; ++u)
-        if (c[u] >= 0) sacc = __dadd_rn(sacc, __dmul_rn((double)a[u], __ldg(x + c[u])));
+        if (c[u] >= 0) sacc = __dadd_rn(sacc, __dmul_rn((double)a[u], (double)__ldg(x + c[u])));
     }
     const int r = 32 * sl + lane;
     if (r < n && ((mask[sl] >> lane) & 1u)) y[r] = sacc;
@@ -249,11 +249,11 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_sell_kernel(int nslices, in
 // fixed order, reduces the warp with a fixed shuffle tree and writes partials[s].  Half
 // occupancy buys the registers for the loads in flight; long dense-like rows (the power-law
 // columns of a transposed matrix) stream at full width.
-template <typename VT>
+template <typename VT, typename XT>
 __global__ void __launch_bounds__(kSpmvThreads, sizeof(VT) == 4 ? 4 : 3) spmv_segment_kernel(int nsegs, const int2 *__restrict__ segs,
                                                                        const int *__restrict__ colind,
                                                                        const VT *__restrict__ vals,
-                                                                       const double *__restrict__ x,
+                                                                       const XT *__restrict__ x,
                                                                        double *__restrict__ partials,
                                                                        const GsState *__restrict__ st, int step) {
   if (st && st->halt && st->halt_step < step) return;
@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(kSpmvThreads, sizeof(VT) == 4 ? 4 : 3) spmv_se
     for (int k = 0; k < nfull; ++k) {
       double xv[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u) xv[u] = __ldg(x + c[u]);
+      for (int u = 0; u < U; ++u) xv[u] = (double)__ldg(x + c[u]);
       VT an[U];
       int cn[U];
       if (k + 1 < nfull) {
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(kSpmvThreads, sizeof(VT) == 4 ? 4 : 3) spmv_se
     }
     const int p = seg.x + nfull * kWarpTileNnz;
     for (int q = p + lane; q < seg.y; q += 32)
-      sacc = __dadd_rn(sacc, __dmul_rn((double)__ldcs(vals + q), __ldg(x + __ldcs(colind + q))));
+      sacc = __dadd_rn(sacc, __dmul_rn((double)__ldcs(vals + q), (double)__ldg(x + __ldcs(colind + q))));
     sacc = warp_sum(sacc);
     if (lane == 0) partials[sg] = sacc;
   }
@@ -389,6 +389,8 @@ SellPlan spmv_sell_plan(int n, const int *rowptr) {
       if (len <= kSellMaxRow) {
         m |= 1u << i;
         if (len > w) w = len;
+      } else {
+        sp.rest_rows.push_back(r);
       }
     }
     sp.off[sl] = total;
@@ -443,9 +445,9 @@ WarpTiles spmv_warp_tiles(int n, const int *rowptr) {
   return wt;
 }
 
-template <typename VT>
+template <typename VT, typename XT>
 cudaError_t spmv_warptile_launch_t(const SpmvTiles &T, const int *rowptr, const int *colind, const VT *vals,
-                                   const double *x, double *y, cudaStream_t stream, const GsState *st, int step,
+                                   const XT *x, double *y, cudaStream_t stream, const GsState *st, int step,
                                    bool pipelined) {
   static int sms = 0, tile_per_sm = 0, seg_per_sm = 0, pipe_per_sm = 0;
   if (!sms) {
@@ -453,9 +455,9 @@ cudaError_t spmv_warptile_launch_t(const SpmvTiles &T, const int *rowptr, const 
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (sms <= 0) sms = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tile_per_sm, spmv_warptile_kernel<VT>, kSpmvThreads, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&seg_per_sm, spmv_segment_kernel<VT>, kSpmvThreads, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pipe_per_sm, spmv_warptile_pipelined_kernel<VT>, kSpmvThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tile_per_sm, spmv_warptile_kernel<VT, XT>, kSpmvThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&seg_per_sm, spmv_segment_kernel<VT, XT>, kSpmvThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pipe_per_sm, spmv_warptile_pipelined_kernel<VT, XT>, kSpmvThreads, 0);
     if (tile_per_sm <= 0) tile_per_sm = 1;
     if (seg_per_sm <= 0) seg_per_sm = 1;
     if (pipe_per_sm <= 0) pipe_per_sm = 1;
@@ -465,7 +467,7 @@ cudaError_t spmv_warptile_launch_t(const SpmvTiles &T, const int *rowptr, const 
   if (T.nsegs > 0) {
     int grid = (T.nsegs + warps_per_cta - 1) / warps_per_cta;
     if (grid > sms * seg_per_sm) grid = sms * seg_per_sm;
-    spmv_segment_kernel<VT><<<grid, kSpmvThreads, 0, stream>>>(T.nsegs, T.segs, colind, vals, x, T.partials, st,
+    spmv_segment_kernel<VT, XT><<<grid, kSpmvThreads, 0, stream>>>(T.nsegs, T.segs, colind, vals, x, T.partials, st,
                                                                step);
     count_launch();
   }
@@ -473,11 +475,11 @@ cudaError_t spmv_warptile_launch_t(const SpmvTiles &T, const int *rowptr, const 
     int grid = (T.ntiles + warps_per_cta - 1) / warps_per_cta;
     if (pipelined) {
       if (grid > sms * pipe_per_sm) grid = sms * pipe_per_sm;
-      spmv_warptile_pipelined_kernel<VT><<<grid, kSpmvThreads, 0, stream>>>(T.ntiles, T.tiles, rowptr, colind, vals,
+      spmv_warptile_pipelined_kernel<VT, XT><<<grid, kSpmvThreads, 0, stream>>>(T.ntiles, T.tiles, rowptr, colind, vals,
                                                                             x, y, st, step);
     } else {
       if (grid > sms * tile_per_sm) grid = sms * tile_per_sm;
-      spmv_warptile_kernel<VT><<<grid, kSpmvThreads, 0, stream>>>(T.ntiles, T.tiles, rowptr, colind, vals, x, y,
+      spmv_warptile_kernel<VT, XT><<<grid, kSpmvThreads, 0, stream>>>(T.ntiles, T.tiles, rowptr, colind, vals, x, y,
                                                                   st, step);
     }
     count_launch();
@@ -526,28 +528,28 @@ cudaError_t sell_gather(int n, const SpmvSell &S, const int *rowptr, const int *
   return cudaGetLastError();
 }
 
-template <typename VT>
-cudaError_t spmv_sell_launch_t(const SpmvSell &S, int n, const SpmvTiles &rest, const int *rowptr, const int *colind,
-                               const VT *vals, const double *x, double *y, cudaStream_t stream, const GsState *st,
-                               int step) {
+template <typename VT, typename XT>
+cudaError_t spmv_sell_launch_t(const SpmvSell &S, const VT *svals, int n, const SpmvTiles &rest, const int *rowptr,
+                               const int *colind, const VT *vals, const XT *x, double *y, cudaStream_t stream,
+                               const GsState *st, int step) {
   static int sms = 0, per_sm = 0;
   if (!sms) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (sms <= 0) sms = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spmv_sell_kernel<VT>, kSpmvThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spmv_sell_kernel<VT, XT>, kSpmvThreads, 0);
     if (per_sm <= 0) per_sm = 1;
   }
   if (S.nslices > 0) {
     int grid = (S.nslices + kSpmvThreads / 32 - 1) / (kSpmvThreads / 32);
     if (grid > sms * per_sm) grid = sms * per_sm;
-    spmv_sell_kernel<VT><<<grid, kSpmvThreads, 0, stream>>>(S.nslices, n, S.off, S.width, S.mask,
-                                                            static_cast<const VT *>(S.vals), S.cols, x, y, st, step);
+    spmv_sell_kernel<VT, XT><<<grid, kSpmvThreads, 0, stream>>>(S.nslices, n, S.off, S.width, S.mask, svals, S.cols, x,
+                                                                y, st, step);
     count_launch();
   }
   if (rest.ntiles > 0 || rest.nsegs > 0) {
-    cudaError_t e = spmv_warptile_launch_t<VT>(rest, rowptr, colind, vals, x, y, stream, st, step, false);
+    cudaError_t e = spmv_warptile_launch_t<VT, XT>(rest, rowptr, colind, vals, x, y, stream, st, step, false);
     if (e != cudaSuccess) return e;
   }
   return cudaGetLastError();
@@ -556,25 +558,33 @@ cudaError_t spmv_sell_launch_t(const SpmvSell &S, int n, const SpmvTiles &rest, 
 cudaError_t spmv_sell_launch(const SpmvSell &S, int n, const SpmvTiles &rest, const int *rowptr, const int *colind,
                              const double *vals, const double *x, double *y, cudaStream_t stream, const GsState *st,
                              int step) {
-  return spmv_sell_launch_t<double>(S, n, rest, rowptr, colind, vals, x, y, stream, st, step);
+  return spmv_sell_launch_t<double, double>(S, static_cast<const double *>(S.vals), n, rest, rowptr, colind, vals, x,
+                                            y, stream, st, step);
 }
 
 cudaError_t spmv_sell_launch_f32(const SpmvSell &S, int n, const SpmvTiles &rest, const int *rowptr,
                                  const int *colind, const float *vals, const double *x, double *y,
                                  cudaStream_t stream, const GsState *st, int step) {
-  return spmv_sell_launch_t<float>(S, n, rest, rowptr, colind, vals, x, y, stream, st, step);
+  return spmv_sell_launch_t<float, double>(S, static_cast<const float *>(S.vals), n, rest, rowptr, colind, vals, x, y,
+                                           stream, st, step);
+}
+
+cudaError_t spmv_sell_launch_x32(const SpmvSell &S, const float *svals, int n, const SpmvTiles &rest,
+                                 const int *rowptr, const int *colind, const float *vals, const float *x, double *y,
+                                 cudaStream_t stream, const GsState *st, int step) {
+  return spmv_sell_launch_t<float, float>(S, svals, n, rest, rowptr, colind, vals, x, y, stream, st, step);
 }
 
 cudaError_t spmv_warptile_launch(const SpmvTiles &T, const int *rowptr, const int *colind, const double *vals,
                                  const double *x, double *y, cudaStream_t stream, const GsState *st, int step,
                                  bool pipelined) {
-  return spmv_warptile_launch_t<double>(T, rowptr, colind, vals, x, y, stream, st, step, pipelined);
+  return spmv_warptile_launch_t<double, double>(T, rowptr, colind, vals, x, y, stream, st, step, pipelined);
 }
 
 cudaError_t spmv_warptile_launch_f32(const SpmvTiles &T, const int *rowptr, const int *colind, const float *vals,
                                      const double *x, double *y, cudaStream_t stream, const GsState *st, int step,
                                      bool pipelined) {
-  return spmv_warptile_launch_t<float>(T, rowptr, colind, vals, x, y, stream, st, step, pipelined);
+  return spmv_warptile_launch_t<float, double>(T, rowptr, colind, vals, x, y, stream, st, step, pipelined);
 }
 
 cudaError_t spmv_rowblock_launch(int nblocks, const int *blocks, const int *rowptr, const int *colind,

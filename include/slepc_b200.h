@@ -224,6 +224,12 @@ b200_status b200_bv_norm_column(b200_bv bv, int j, double *nrm);
 b200_status b200_bv_norm(b200_bv bv, double *nrm);
 /* BVCopyColumn (bvops.c): column i <- column j. */
 b200_status b200_bv_copy_column(b200_bv bv, int j, int i);
+/* BVMatMult (bvops.c:692-730; matrix-product path of BVMatMult_Svec, svec.c:203-219):
+ * Y(:, Y.l + j) = A V(:, V.l + j) for the active columns of V (Y has as many
+ * active columns).  A square CSR operator is applied to all columns at once
+ * (block SpMV: the matrix is read once, FP64 products and sums in index
+ * order per row); other operators column by column. */
+b200_status b200_bv_mat_mult(b200_bv V, b200_mat A, b200_bv Y);
 /* BVMatMultColumn (bvops.c:862-890): column j+1 <- A * column j. */
 b200_status b200_bv_mat_mult_column(b200_bv bv, b200_mat A, int j);
 /* BVMatLanczos (src/sys/classes/bv/interface/bvkrylov.c:165-226): Lanczos
@@ -273,10 +279,16 @@ b200_status b200_eps_set_max_restarts(b200_eps eps, int max_restarts);
 b200_status b200_eps_set_precision(b200_eps eps, int precision);
 /* Mixed-form parameters (0 or a negative value keeps the default): tol_low,
  * the phase-1 tolerance (default 1e-6, never below tol); degree, the
- * Chebyshev filter degree per sweep (default 24); guard, columns of the
+ * Chebyshev filter degree per sweep (default 64; a sweep uses less when the
+ * amplification of the leading Ritz value would exceed 1e6, which keeps the
+ * block well conditioned for its Cholesky QR); guard, columns of the
  * refinement block beyond nev (default max(8, nev/2)); max_sweeps (default
- * 40). */
-b200_status b200_eps_set_mixed_options(b200_eps eps, double tol_low, int degree, int guard, int max_sweeps);
+ * 40); fp32_first_pass: 1 runs the first Gram-Schmidt pass of every column
+ * (its projections and the update that applies them) in FP32 arithmetic and
+ * always takes the FP64 DGKS correction pass, 0 (default) keeps every pass in
+ * FP64 arithmetic on the FP32 basis. */
+b200_status b200_eps_set_mixed_options(b200_eps eps, double tol_low, int degree, int guard, int max_sweeps,
+                                       int fp32_first_pass);
 
 /* EPSSetType: B200_EPS_KRYLOVSCHUR (default) or B200_EPS_LOBPCG. */
 #define B200_EPS_KRYLOVSCHUR 0

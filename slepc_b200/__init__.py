@@ -76,7 +76,8 @@ _SIGS = {
     "b200_mat_norm_inf": (ctypes.c_int, [_vp, _dp]),
     "b200_eps_set_type": (ctypes.c_int, [_vp, ctypes.c_int]),
     "b200_eps_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
-    "b200_eps_set_mixed_options": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "b200_eps_set_mixed_options": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_int]),
     "b200_eps_lobpcg_set_block_size": (ctypes.c_int, [_vp, ctypes.c_int]),
     "b200_eps_lobpcg_set_restart": (ctypes.c_int, [_vp, ctypes.c_double]),
     "b200_eps_lobpcg_set_locking": (ctypes.c_int, [_vp, ctypes.c_int]),
@@ -153,6 +154,7 @@ _SIGS = {
     "b200_bv_norm": (ctypes.c_int, [_vp, _dp]),
     "b200_bv_copy_column": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
     "b200_bv_mat_mult_column": (ctypes.c_int, [_vp, _vp, ctypes.c_int]),
+    "b200_bv_mat_mult": (ctypes.c_int, [_vp, _vp, _vp]),
     "b200_bv_mat_lanczos": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _ip, _dp, _dp, _dp, _ip]),
     "b200_eps_create": (ctypes.c_int, [_vp, _vp]),
     "b200_eps_destroy": (ctypes.c_int, [_vp]),
@@ -503,6 +505,10 @@ class BV:
     def matMultColumn(self, A, j):
         _check(lib().b200_bv_mat_mult_column(self.handle, A.handle, j))
 
+    def matMult(self, A, Y):
+        """BVMatMult: Y(:, Y.l+j) = A V(:, V.l+j) over the active columns."""
+        _check(lib().b200_bv_mat_mult(self.handle, A.handle, Y.handle))
+
     def matLanczos(self, A, k, m):
         """BVMatLanczos: returns (alpha, beta_vec, m, beta, breakdown)."""
         mm = ctypes.c_int(m)
@@ -605,9 +611,10 @@ class EPS:
         Chebyshev-filtered Rayleigh-Ritz refinement of the block of leading Ritz vectors."""
         _check(lib().b200_eps_set_precision(self.handle, precision))
 
-    def setMixedOptions(self, tol_low=0.0, degree=0, guard=-1, max_sweeps=0):
+    def setMixedOptions(self, tol_low=0.0, degree=0, guard=-1, max_sweeps=0, fp32_first_pass=False):
         """Parameters of the mixed form; 0 (or -1 for guard) keeps the default."""
-        _check(lib().b200_eps_set_mixed_options(self.handle, tol_low, degree, guard, max_sweeps))
+        _check(lib().b200_eps_set_mixed_options(self.handle, tol_low, degree, guard, max_sweeps,
+                                                int(bool(fp32_first_pass))))
 
     def setInitialSpaceDevice(self, v0_ptr):
         _check(lib().b200_eps_set_initial_space_device(self.handle, v0_ptr))

@@ -566,10 +566,10 @@ cudaError_t multvec_launch(const double *X, int ldx, int n, int k, const double 
 }
 
 cudaError_t dot_launch(const double *X, int ldx, int nx, const double *Y, int ldy, int ny, int n, double *M, int ldm,
-                       double *work, int work_len, cudaStream_t stream) {
+                       double *work, int work_len, cudaStream_t stream, int ctas_per_sm) {
   if (nx <= 0 || ny <= 0) return cudaSuccess;
   const int npairs = nx * ny;
-  int blocks = num_sms();
+  int blocks = num_sms() * (ctas_per_sm > 0 ? ctas_per_sm : 1);
   if (blocks * npairs > work_len) blocks = work_len / npairs;
   if (blocks < 1) return cudaErrorInvalidValue;
   if (npairs >= 64) {

@@ -43,6 +43,12 @@ constexpr int kMaxStages = 8;
 constexpr int kMaxChunk = 256;                         // rows per chunk (tile box limit)
 constexpr size_t kStageTarget = 64 * 1024;            // bytes of one pipeline stage (target)
 constexpr size_t kStageBudget = 196 * 1024;           // bytes of all stages together
+// FP32 basis: two CTAs per SM (twice the consumer warps for the same bytes), each with about half
+// the stage budget; chunks of 128 rows (512-byte runs per column) whenever two stages fit, which
+// measured well ahead of 64 rows with more stages
+constexpr size_t kStageBudget32 = 100 * 1024;
+template <typename TS>
+constexpr int ctas_per_sm() { return sizeof(TS) == sizeof(float) ? 2 : 1; }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -139,7 +145,9 @@ struct DecideShared {
 __device__ void finish_pass(DecideShared &d, const PassParams &p, double onrm, double nrm, bool have_next) {
   const GsState *st = p.st;
   const GsPassArgs &a = p.a;
-  const bool refine = d.pass < 3 && nrm != 0.0 && fabs(nrm) < st->eta * fabs(onrm);
+  // fast32: the first pass ran in FP32 arithmetic, so the FP64 correction pass is always taken
+  const bool refine =
+      d.pass < 3 && nrm != 0.0 && (fabs(nrm) < st->eta * fabs(onrm) || (a.fast32 && d.pass == 1));
   if (refine) {
     if (have_next) {
       // The dot just reduced is already the dot of the next pass.
@@ -259,7 +267,8 @@ __device__ void decide(const PassParams &p, const double *cnew_s, DecideShared &
 // TS is the stored type of the basis: double, or float for the FP32 basis of the mixed-precision
 // solver (w, the coefficients and every product and sum stay FP64).
 template <int MAXCPW, typename TS>
-__global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, const __grid_constant__ CUtensorMap tmap) {
+__global__ void __launch_bounds__(kThreads, ctas_per_sm<TS>()) gs_pass_kernel(PassParams p,
+                                                                             const __grid_constant__ CUtensorMap tmap) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   GsState *st = p.st;
   const GsPassArgs &a = p.a;
@@ -277,6 +286,11 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
   const bool do_scale = (action & kActScale) != 0;
   const int ncl = (do_update || do_dot) ? jb : 0;  // basis columns streamed
   const double scale = do_scale ? st->scale : 1.0;
+  // FP32 basis with fast32: the dot of the first pass and the update that applies its coefficients
+  // run in FP32 arithmetic (products and sums), the correction pass in FP64
+  const int passno = p.first ? 0 : st->pass;
+  const bool fast_dot = sizeof(TS) == sizeof(float) && a.fast32 && p.first && do_dot;
+  const bool fast_update = sizeof(TS) == sizeof(float) && a.fast32 && do_update && passno == 1;
 
   // shared memory carve-up
   uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw);
@@ -286,6 +300,7 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
   DecideShared *dsh = reinterpret_cast<DecideShared *>(cacc + kMaxCols + 1);
   __shared__ int is_last, timed_out, n_issued;
   __shared__ double upd[2 * kConsumers];      // partial update sums (TPR*CH = kConsumers per chunk), by chunk parity
+  __shared__ float coef32_s[sizeof(TS) == sizeof(float) ? kMaxCols : 1];  // FP32 coefficients (fast update)
   const size_t head = 128 + sizeof(double) * (2 * kMaxCols + 1) + ((sizeof(DecideShared) + 127) / 128) * 128;
   unsigned char *stage_base = smem_raw + ((head + 127) / 128) * 128;
   const size_t stage_bytes = (size_t)p.stage_bytes;
@@ -301,6 +316,9 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
     n_issued = 0;
   }
   for (int i = tid; i < jb; i += kThreads) coef_s[i] = do_update ? p.coef[i] : 0.0;
+  if constexpr (sizeof(TS) == sizeof(float))
+    if (fast_update)
+      for (int i = tid; i < jb; i += kThreads) coef32_s[i] = __double2float_rn(p.coef[i]);
   __syncthreads();
 
   const int G = p.G;
@@ -361,14 +379,39 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
       const bool rewrite = do_update || do_scale;
       if (rewrite) {
         if (ok && do_update) {
-          double s0 = 0.0, s1 = 0.0;
-          int c = part;
-          for (; c + TPR < jb; c += 2 * TPR) {
-            s0 = fma((double)Vs[(size_t)c * CH + urow], coef_s[c], s0);
-            s1 = fma((double)Vs[(size_t)(c + TPR) * CH + urow], coef_s[c + TPR], s1);
+          if constexpr (sizeof(TS) == sizeof(double)) {
+            double s0 = 0.0, s1 = 0.0;
+            int c = part;
+            for (; c + TPR < jb; c += 2 * TPR) {
+              s0 = fma(Vs[(size_t)c * CH + urow], coef_s[c], s0);
+              s1 = fma(Vs[(size_t)(c + TPR) * CH + urow], coef_s[c + TPR], s1);
+            }
+            if (c < jb) s0 = fma(Vs[(size_t)c * CH + urow], coef_s[c], s0);
+            up[part * CH + urow] = s0 + s1;
+          } else if (fast_update) {
+            float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+            int c = part;
+            for (; c + 3 * TPR < jb; c += 4 * TPR) {
+              s0 = fmaf((float)Vs[(size_t)c * CH + urow], coef32_s[c], s0);
+              s1 = fmaf((float)Vs[(size_t)(c + TPR) * CH + urow], coef32_s[c + TPR], s1);
+              s2 = fmaf((float)Vs[(size_t)(c + 2 * TPR) * CH + urow], coef32_s[c + 2 * TPR], s2);
+              s3 = fmaf((float)Vs[(size_t)(c + 3 * TPR) * CH + urow], coef32_s[c + 3 * TPR], s3);
+            }
+            for (; c < jb; c += TPR) s0 = fmaf((float)Vs[(size_t)c * CH + urow], coef32_s[c], s0);
+            up[part * CH + urow] = (double)((s0 + s1) + (s2 + s3));
+          } else {
+            // four independent chains: the FP32 basis doubles the columns a chunk holds per byte
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            int c = part;
+            for (; c + 3 * TPR < jb; c += 4 * TPR) {
+              s0 = fma((double)Vs[(size_t)c * CH + urow], coef_s[c], s0);
+              s1 = fma((double)Vs[(size_t)(c + TPR) * CH + urow], coef_s[c + TPR], s1);
+              s2 = fma((double)Vs[(size_t)(c + 2 * TPR) * CH + urow], coef_s[c + 2 * TPR], s2);
+              s3 = fma((double)Vs[(size_t)(c + 3 * TPR) * CH + urow], coef_s[c + 3 * TPR], s3);
+            }
+            for (; c < jb; c += TPR) s0 = fma((double)Vs[(size_t)c * CH + urow], coef_s[c], s0);
+            up[part * CH + urow] = (s0 + s1) + (s2 + s3);
           }
-          if (c < jb) s0 = fma((double)Vs[(size_t)c * CH + urow], coef_s[c], s0);
-          up[part * CH + urow] = s0 + s1;
         }
         if (consumer_sync_or(!ok)) break;  // partial sums complete (and a timed-out wait is agreed on)
       } else if (!ok) {
@@ -389,7 +432,23 @@ __global__ void __launch_bounds__(kThreads, 1) gs_pass_kernel(PassParams p, cons
         const int r = warp * 32 + lane;
         if (r < rows) Vw[r0 + r] = wprime(r);
       }
-      if (do_dot) {
+      if (do_dot && fast_dot) {
+        // FP32 products summed in FP32 over the chunk's rows of this lane, then added in FP64
+        float facc[MAXCPW];
+#pragma unroll
+        for (int t = 0; t < MAXCPW; ++t) facc[t] = 0.f;
+        for (int r = lane; r < rows; r += 32) {
+          const float wr = __double2float_rn(rewrite ? wprime(r) : wsrc[r]);
+#pragma unroll
+          for (int t = 0; t < MAXCPW; ++t) {
+            const int c = warp + kConsumerWarps * t;
+            if (c < jb) facc[t] = fmaf((float)Vs[(size_t)c * CH + r], wr, facc[t]);
+            else if (c == jb) facc[t] = fmaf(wr, wr, facc[t]);
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < MAXCPW; ++t) acc[t] += (double)facc[t];
+      } else if (do_dot) {
         for (int r = lane; r < rows; r += 32) {
           const double wr = rewrite ? wprime(r) : wsrc[r];
 #pragma unroll
@@ -474,6 +533,11 @@ size_t pass_smem_bytes(int jb, int CH, int stages, size_t ts) {
 
 // Rows per chunk: the largest power of two (32..256, the tile box limit) whose stage fits the target size.
 int pass_chunk_rows(int jb, size_t ts) {
+  if (ts == sizeof(float)) {
+    int ch = kMaxChunk / 2;
+    while (ch > 32 && 2 * pass_stage_bytes(jb, ch, ts) > kStageBudget32) ch /= 2;
+    return ch;
+  }
   const size_t rows = kStageTarget / ((size_t)jb * ts + sizeof(double));
   int ch = 32;
   while (ch < kMaxChunk && (size_t)(2 * ch) <= rows) ch *= 2;
@@ -512,7 +576,7 @@ cudaError_t make_tmap(CUtensorMap *tm, const GsPassArgs &a, int CH, int box_cols
 
 int pass_stages(int jb, int CH, size_t ts) {
   const size_t stage = pass_stage_bytes(jb, CH, ts);
-  size_t s = kStageBudget / stage;
+  size_t s = (ts == sizeof(double) ? kStageBudget : kStageBudget32) / stage;
   if (s > (size_t)kMaxStages) s = kMaxStages;
   return (int)s;
 }
@@ -548,7 +612,7 @@ cudaError_t launch_pass(const GsPassArgs &a, const GsWork &w, int first, int pla
   p.stage_bytes = (int)pass_stage_bytes(a.jb, p.chunk, ts);
   if (p.stages < 2) return cudaErrorInvalidValue;
   p.nchunks = (a.n + p.chunk - 1) / p.chunk;
-  int G = w.num_sms;
+  int G = w.num_sms * (f32 ? ctas_per_sm<float>() : 1);
   if (G > w.max_ctas) G = w.max_ctas;
   if (G > p.nchunks) G = p.nchunks;
   if (G < 1) G = 1;

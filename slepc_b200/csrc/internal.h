@@ -25,6 +25,8 @@ b200_status bv_column_norms(b200_bv bv, double *nrm);
 int num_sms_host();
 // EPSSolve with EPSLOBPCG (lobpcg.cu).
 b200_status lobpcg_solve(b200_eps eps);
+// BVMatMult: Y(:, Y.l+j) = A V(:, V.l+j) over the active columns (block SpMV for square CSR).
+b200_status bv_mat_mult(b200_bv V, b200_mat A, b200_bv Y);
 // Krylov-Schur with b200_eps_set_precision(MIXED) after the setup (mixed.cu).
 b200_status mixed_solve(b200_eps eps);
 // Read the Gram-Schmidt control block after a stream synchronisation (maps device errors).

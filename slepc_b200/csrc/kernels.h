@@ -99,7 +99,7 @@ cudaError_t spmv_sell_launch_x32(const SpmvSell &S, const float *svals, int n, c
 // Block SpMV with a fused three-term update (block.cu), FP64:
 //   Out(:,b) = alpha * (A Y(:,b) - shift * Y(:,b)) - beta * X(:,b),  b < nb
 // (X may be null: no beta term).  Y, X and Out are column-major with leading dimension ld; Out
-// must not overlap Y or X.  The slices are read once per group of 8 columns.
+// must not overlap Y or X.  The slices are read once per block.
 cudaError_t spmm_sell_launch(const SpmvSell &S, int n, const int *rowptr, const int *colind, const void *vals, bool f32,
                              const double *Y, const double *X, double *Out, int ld, int nb, double alpha, double shift,
                              double beta, cudaStream_t stream);
@@ -151,6 +151,9 @@ struct GsPassArgs {
   const float *V32;
   int ld32;
   double *wvec;
+  // with V32: the first CGS pass (its dot and the update applying its coefficients) in FP32
+  // arithmetic, and the FP64 DGKS correction pass always taken
+  int fast32;
 };
 
 // Enqueue the full CGS + DGKS("if needed") orthogonalisation of one column:
@@ -195,9 +198,10 @@ cudaError_t mult_launch(double *Y, int ldy, const double *X, int ldx, int n, int
 // y = beta*y + alpha*X(:,0:k) q
 cudaError_t multvec_launch(const double *X, int ldx, int n, int k, const double *q, double alpha, double beta, double *y,
                            cudaStream_t stream);
-// M(0:ny,0:nx) = Y(:,0:ny)^T X(:,0:nx), M column-major ldm (device), deterministic.
+// M(0:ny,0:nx) = Y(:,0:ny)^T X(:,0:nx), M column-major ldm (device), deterministic for a given
+// ctas_per_sm (row blocks per SM of the partial sums).
 cudaError_t dot_launch(const double *X, int ldx, int nx, const double *Y, int ldy, int ny, int n, double *M, int ldm,
-                       double *work, int work_len, cudaStream_t stream);
+                       double *work, int work_len, cudaStream_t stream, int ctas_per_sm = 1);
 cudaError_t scale_launch(double *x, long long len, double alpha, cudaStream_t stream);
 cudaError_t copy_launch(double *dst, const double *src, long long len, cudaStream_t stream);
 // out[c] = ||X(:,c)||_2 for c < k (device), deterministic (fixed row split, fixed order).

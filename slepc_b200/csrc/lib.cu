@@ -587,7 +587,7 @@ extern "C" b200_status b200_bv_create(int n, int m, void *stream, b200_bv *out) 
   bv->ldt = m + 1;
   const int sms = num_sms_host();
   bv->gs.num_sms = sms;
-  bv->gs.max_ctas = sms;
+  bv->gs.max_ctas = 2 * sms;  // the FP32-basis passes of the mixed solver run two CTAs per SM
   bv->red_len = sms * 8 > 4096 ? sms * 8 : 4096;
   bv->qbuf_len = (size_t)(m + 1) * (m + 1);
   bv->hpin_len = (size_t)(m + 1) * (m + 1) + 4 * (size_t)(m + 1) + 64;
@@ -598,7 +598,7 @@ extern "C" b200_status b200_bv_create(int n, int m, void *stream, b200_bv *out) 
   ok = ok && cudaMalloc(&bv->gs.st, sizeof(GsState)) == cudaSuccess;
   ok = ok && cudaMalloc(&bv->gs.coef, sizeof(double) * kMaxCols) == cudaSuccess;
   ok = ok && cudaMalloc(&bv->gs.cnew, sizeof(double) * (kMaxCols + 1)) == cudaSuccess;
-  ok = ok && cudaMalloc(&bv->gs.partials, sizeof(double) * (size_t)(kMaxCols + 1) * sms) == cudaSuccess;
+  ok = ok && cudaMalloc(&bv->gs.partials, sizeof(double) * (size_t)(kMaxCols + 1) * 2 * sms) == cudaSuccess;
   ok = ok && cudaMalloc(&bv->coefbuf, sizeof(double) * (size_t)bv->ldc * (m + 1)) == cudaSuccess;
   ok = ok && cudaMalloc(&bv->hvec, sizeof(double) * (kMaxCols + 1)) == cudaSuccess;
   ok = ok && cudaMalloc(&bv->T, sizeof(double) * 2 * (size_t)bv->ldt) == cudaSuccess;
@@ -1025,6 +1025,29 @@ extern "C" b200_status b200_bv_mat_mult_column(b200_bv bv, b200_mat A, int j) {
   return B200_OK;
 }
 
+// BVMatMult (bvops.c:692-730) with the matrix-product path of BVMatMult_Svec (svec.c:203-219):
+// Y(:, Y.l + j) = A V(:, V.l + j) for the active columns.  A square CSR operator takes the block
+// SpMV (the matrix read once for all columns); other operators go column by column.
+b200_status b200::bv_mat_mult(b200_bv V, b200_mat A, b200_bv Y) {
+  const int nc = V->k - V->l;
+  if (nc <= 0) return B200_OK;
+  if (A->kind == kMatCsr && A->m == A->n && V->ld == Y->ld && A->a.sell_ready) {
+    const CsrPart &P = A->a;
+    B200_CUDA_CHECK(spmm_sell_launch(P.sell, P.rows, P.rowptr, P.colind, P.vals, P.f32, col(V, V->l), nullptr,
+                                     col(Y, Y->l), V->ld, nc, 1.0, 0.0, 0.0, Y->stream));
+    return B200_OK;
+  }
+  for (int j = 0; j < nc; ++j) B200_CUDA_CHECK(mat_spmv(A, col(V, V->l + j), col(Y, Y->l + j), Y->stream));
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_mat_mult(b200_bv V, b200_mat A, b200_bv Y) {
+  B200_ARG_CHECK(V && A && Y && V != Y, "invalid BVMatMult arguments (V and Y must differ)");
+  B200_ARG_CHECK(A->n == V->n && A->m == Y->n, "mismatching dimensions of A, V and Y");
+  B200_ARG_CHECK(V->k - V->l == Y->k - Y->l, "V and Y must have the same number of active columns");
+  return bv_mat_mult(V, A, Y);
+}
+
 // Timing of a Lanczos run (optional): event pairs around each SpMV and each column orthogonalisation.
 struct RunTimer {
   bool on = false;
@@ -1220,13 +1243,14 @@ extern "C" b200_status b200_eps_set_precision(b200_eps eps, int precision) {
 }
 
 extern "C" b200_status b200_eps_set_mixed_options(b200_eps eps, double tol_low, int degree, int guard,
-                                                  int max_sweeps) {
+                                                  int max_sweeps, int fp32_first_pass) {
   B200_ARG_CHECK(eps, "null argument");
   B200_ARG_CHECK(degree <= 4096 && max_sweeps <= 100000, "degree or max_sweeps too large");
   eps->mixed_tol_low = tol_low > 0.0 ? tol_low : 0.0;
   eps->mixed_degree = degree > 0 ? degree : 0;
   eps->mixed_guard = guard >= 0 ? guard : -1;
   eps->mixed_max_sweeps = max_sweeps > 0 ? max_sweeps : 0;
+  eps->mixed_fp32_pass = fp32_first_pass ? 1 : 0;
   return B200_OK;
 }
 

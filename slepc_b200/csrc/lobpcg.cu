@@ -50,15 +50,6 @@ cudaError_t bv_copy_column(b200_bv bv, int j, int i) {
   return cudaMemcpyAsync(col(bv, i), col(bv, j), sizeof(double) * bv->n, cudaMemcpyDeviceToDevice, bv->stream);
 }
 
-// BVMatMult: Y(:, Y.l + j) = A X(:, X.l + j)
-cudaError_t bv_matmult(b200_mat A, b200_bv X, b200_bv Y) {
-  for (int j = 0; j < X->k - X->l; ++j) {
-    cudaError_t e = mat_apply(A, col(X, X->l + j), col(Y, Y->l + j), Y->stream, false);
-    if (e != cudaSuccess) return e;
-  }
-  return cudaSuccess;
-}
-
 // DSSolve_GHEP + DSSort_GHEP + DSVectors_GHEP on the nv x nv pencil (A, B) with leading
 // dimension ld; wr gets the sorted eigenvalues and X (ld x ld) the eigenvectors.
 b200_status ds_ghep(int nv, int ld, std::vector<double> &A, std::vector<double> &B, std::vector<double> &wr,
@@ -215,7 +206,7 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
 
   // 4. Rayleigh-Ritz on X alone (also after hard locking)
   auto rayleigh_ritz_x = [&]() -> b200_status {
-    B200_CUDA_CHECK(bv_matmult(A, X, AX));
+    B200_CHECK(bv_mat_mult(X, A, AX));
     eps->stats.lanczos_steps += X->k - X->l;
     std::fill(MA.begin(), MA.end(), 0.0);
     B200_CHECK(b200_bv_dot(AX, X, MA.data(), mpd));  // BVMatProject(AX,NULL,X,M): M = X^T AX
@@ -343,7 +334,7 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
     nv = its > 1 ? 3 * bs - 2 * ini : 2 * bs - ini;
     active(Z, 0, nv);
     active(W, 0, nv);
-    B200_CUDA_CHECK(bv_matmult(A, Z, W));  // BVMatProject_MatMult: W = A Z, M = Z^T W
+    B200_CHECK(bv_mat_mult(Z, A, W));  // BVMatProject_MatMult: W = A Z, M = Z^T W
     eps->stats.lanczos_steps += nv;
     std::fill(MA.begin(), MA.end(), 0.0);
     B200_CHECK(b200_bv_dot(W, Z, MA.data(), mpd));
@@ -365,7 +356,7 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
     active(Z, 0, bs);
     B200_CHECK(b200_bv_mult(X, 1.0, 1.0, Z, Q.data(), mpd));
     if (lock) active(X, nconv, bs);
-    B200_CUDA_CHECK(bv_matmult(A, X, AX));
+    B200_CHECK(bv_mat_mult(X, A, AX));
     eps->stats.lanczos_steps += X->k - X->l;
   }
   eps_its += its;

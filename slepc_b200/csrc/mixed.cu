@@ -50,7 +50,7 @@ using namespace b200;
 namespace {
 
 constexpr double kDefaultTolLow = 1e-6;
-constexpr int kDefaultDegree = 24;
+constexpr int kDefaultDegree = 64;
 constexpr int kDefaultMaxSweeps = 40;
 constexpr int kMaxBlock = 128;  // columns of the refinement block (row-panel GEMM limit)
 constexpr int kBlocks = 5;      // FP64 blocks of the refinement phase
@@ -78,7 +78,15 @@ struct Mixed {
   float *V32;
   double *wv;
 
+  std::vector<cudaEvent_t> ev;  // per-step SpMV / Gram-Schmidt events when timing is on
+  double ms_spmv = 0.0, ms_orth = 0.0;
+
   float *col32(int j) const { return V32 + (size_t)j * ld32; }
+  void release_events() {
+    for (auto e : ev) cudaEventDestroy(e);
+    ev.clear();
+  }
+  ~Mixed() { release_events(); }
 
   GsPassArgs args(int jb, int step, double *T) const {
     GsPassArgs a{};
@@ -97,6 +105,7 @@ struct Mixed {
     a.step = step;
     a.normalize = 1;
     a.column = 1;
+    a.fast32 = eps->mixed_fp32_pass;
     return a;
   }
 
@@ -124,12 +133,24 @@ struct Mixed {
   // BVMatLanczos on the FP32 basis: steps k..m-1 back to back, one synchronisation at the end.
   b200_status lanczos(int k, int *m, double *alpha, double *beta_h, double *beta, int *breakdown, GsState *st_out) {
     const int m0 = *m;
+    const bool timing = eps->timing != 0;
+    if (timing)
+      while (ev.size() < (size_t)3 * (m0 - k)) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) break;
+        ev.push_back(e);
+      }
+    const bool have_ev = timing && ev.size() >= (size_t)3 * (m0 - k);
     B200_CUDA_CHECK(gs_state_reset(V->gs, V->eta, s));
     for (int j = k; j < m0; ++j) {
+      const size_t e = (size_t)3 * (j - k);
+      if (have_ev) cudaEventRecord(ev[e], s);
       B200_CUDA_CHECK(mat_spmv_x32(eps->A, col32(j), wv, s, V->gs.st, j));
+      if (have_ev) cudaEventRecord(ev[e + 1], s);
       GsPassArgs a = args(j + 1, j, V->T);
       B200_CUDA_CHECK(gs_orthogonalize_launch(a, V->gs, s));
       B200_CUDA_CHECK(to_f32_launch(col32(j + 1), wv, n, s));
+      if (have_ev) cudaEventRecord(ev[e + 2], s);
     }
     double *hT = V->hpin + 64;
     B200_CUDA_CHECK(cudaMemcpyAsync(hT, V->T, sizeof(double) * 2 * (size_t)V->ldt, cudaMemcpyDeviceToHost, s));
@@ -148,6 +169,13 @@ struct Mixed {
     *m = mm;
     *beta = st.beta_out;
     *breakdown = bd;
+    if (have_ev)
+      for (int j = k; j < m0; ++j) {
+        const size_t e = (size_t)3 * (j - k);
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, ev[e], ev[e + 1]) == cudaSuccess) ms_spmv += t;
+        if (cudaEventElapsedTime(&t, ev[e + 1], ev[e + 2]) == cudaSuccess) ms_orth += t;
+      }
     return B200_OK;
   }
 };
@@ -277,6 +305,9 @@ b200_status b200::mixed_solve(b200_eps eps) {
     eps->stats.restarts++;
   }
   eps->stats.phase1_restarts = eps->stats.restarts;
+  eps->stats.ms_spmv = M.ms_spmv;
+  eps->stats.ms_orth = M.ms_orth;  // Gram-Schmidt passes and the FP32 store of each new column
+  M.release_events();
   cudaEventRecord(t1, s);
   if (reason == B200_DIVERGED_BREAKDOWN || nv <= 0) {
     B200_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -318,7 +349,7 @@ b200_status b200::mixed_solve(b200_eps eps) {
   int lwork = 1 + 6 * kb + 2 * kb * kb, liwork = 3 + 5 * kb;
   std::vector<double> lw((size_t)lwork);
   std::vector<int> liw((size_t)liwork);
-  int sweeps = 0, done_conv = 0;
+  int sweeps = 0, done_conv = 0, used_degree = 0;
   const int wl = (int)std::min(work_len, (size_t)1 << 30);
   while (sweeps < max_sweeps) {
     ++sweeps;
@@ -338,12 +369,22 @@ b200_status b200::mixed_solve(b200_eps eps) {
     }
     const double e = 0.5 * (b - a), c = 0.5 * (b + a);
     int f = x;  // block holding the filtered vectors
-    if (e > 0.0 && best != c && std::isfinite(e) && degree > 0) {
+    // The scaled filter maps the best Ritz value to 1 and the damped interval into [-1/T, 1/T] with
+    // T = T_d(t_best): the block's condition number grows like T, so d is capped to keep T <= 1e6
+    // (Cholesky QR twice is accurate in FP64 below about 1e8).
+    int d = degree;
+    const double tb = std::fabs((best - c) / e);
+    if (tb > 1.0 && std::isfinite(tb)) {
+      const double cap = std::acosh(1e6) / std::acosh(tb);
+      if (cap < d) d = std::max(2, (int)cap);
+    }
+    used_degree = std::max(used_degree, d);
+    if (e > 0.0 && best != c && std::isfinite(e) && d > 0) {
       const double sigma1 = e / (best - c);
       int prev = x, cur = (x + 1) % kBlocks, nxt = (x + 2) % kBlocks;
       B200_CUDA_CHECK(mat_spmm(eps->A, B[prev], nullptr, B[cur], ldb, kb, sigma1 / e, c, 0.0, s));
       double sigma = sigma1;
-      for (int i = 2; i <= degree; ++i) {
+      for (int i = 2; i <= d; ++i) {
         const double sn = 1.0 / (2.0 / sigma1 - sigma);
         B200_CUDA_CHECK(mat_spmm(eps->A, B[cur], B[prev], B[nxt], ldb, kb, 2.0 * sn / e, c, sigma * sn, s));
         const int t = prev;
@@ -353,7 +394,7 @@ b200_status b200::mixed_solve(b200_eps eps) {
         sigma = sn;
       }
       f = cur;
-      eps->stats.spmm_columns += (int64_t)kb * degree;
+      eps->stats.spmm_columns += (int64_t)kb * d;
     }
     auto free_block = [&](std::initializer_list<int> used) {
       for (int i = 0; i < kBlocks; ++i)
@@ -363,7 +404,7 @@ b200_status b200::mixed_solve(b200_eps eps) {
     // CholQR2: F = Q R, G = F^T F = R^T R (Cholesky on the host), Q = F R^{-1}; twice
     int npass = 2;  // one more pass after a shifted one
     for (int pass = 0; pass < npass; ++pass) {
-      B200_CUDA_CHECK(dot_launch(B[f], ldb, kb, B[f], ldb, kb, n, Gdev, kb, work, wl, s));
+      B200_CUDA_CHECK(dot_launch(B[f], ldb, kb, B[f], ldb, kb, n, Gdev, kb, work, wl, s, 4));
       B200_CUDA_CHECK(cudaMemcpyAsync(G.data(), Gdev, sizeof(double) * G.size(), cudaMemcpyDeviceToHost, s));
       B200_CUDA_CHECK(cudaStreamSynchronize(s));
       int info = 0;
@@ -400,7 +441,7 @@ b200_status b200::mixed_solve(b200_eps eps) {
     const int aq = free_block({f});
     B200_CUDA_CHECK(mat_spmm(eps->A, B[f], nullptr, B[aq], ldb, kb, 1.0, 0.0, 0.0, s));
     eps->stats.spmm_columns += kb;
-    B200_CUDA_CHECK(dot_launch(B[aq], ldb, kb, B[f], ldb, kb, n, Gdev, kb, work, wl, s));
+    B200_CUDA_CHECK(dot_launch(B[aq], ldb, kb, B[f], ldb, kb, n, Gdev, kb, work, wl, s, 4));
     B200_CUDA_CHECK(cudaMemcpyAsync(G.data(), Gdev, sizeof(double) * G.size(), cudaMemcpyDeviceToHost, s));
     B200_CUDA_CHECK(cudaStreamSynchronize(s));
     for (int j = 0; j < kb; ++j)
@@ -439,7 +480,7 @@ b200_status b200::mixed_solve(b200_eps eps) {
     if (done_conv >= nev) break;
   }
   eps->stats.filter_sweeps = sweeps;
-  eps->stats.filter_degree = degree;
+  eps->stats.filter_degree = used_degree;  // the largest degree a sweep used
   eps->stats.block_size = kb;
 
   // results: eigenvectors in columns 0..kb-1 of the FP64 BV, values and residuals in order

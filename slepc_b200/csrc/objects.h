@@ -113,6 +113,7 @@ struct b200_eps_s {
   int mixed_degree = 0;        // Chebyshev degree (0: default)
   int mixed_guard = -1;        // guard columns of the refinement block (-1: default)
   int mixed_max_sweeps = 0;    // refinement sweeps (0: default)
+  int mixed_fp32_pass = 0;     // first Gram-Schmidt pass in FP32 arithmetic
   float *V32 = nullptr;        // FP32 basis, ld32 x (ncv + 1)
   size_t V32_cap = 0;
   int ld32 = 0;

@@ -91,6 +91,37 @@ def spmv(args, torch):
             "GBps": algo / (ms * 1e-3) / 1e9}
 
 
+def spmm(args, torch):
+    """BVMatMult of the 3-D Laplacian on a block of --nb columns (the block SpMV of the mixed
+    solver's refinement phase), L2 flushed between calls."""
+    csr = P.laplacian_3d(args.grid)
+    n = len(csr[0]) - 1
+    nnz = int(csr[0][-1])
+    A = S.Mat().createAIJ(csr)
+    nb = args.nb
+    V = S.BV().create(n, nb)
+    Y = S.BV().create(n, nb)
+    rng = np.random.default_rng(0)
+    for j in range(nb):
+        V.setColumn(j, rng.standard_normal(n))
+    flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")
+    for _ in range(args.warmup):
+        V.matMult(A, Y)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = 0.0
+    for _ in range(args.reps):
+        flush.fill_(1.0)
+        e0.record()
+        V.matMult(A, Y)
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+    ms /= args.reps
+    algo = nnz * 12 + (n + 1) * 4 + 2 * nb * n * 8
+    return {"kernel": "spmm_sell_kernel (BVMatMult)", "n": n, "nnz": nnz, "columns": nb, "ms": ms,
+            "algorithmic_bytes": algo, "GBps": algo / (ms * 1e-3) / 1e9}
+
+
 def cross(args, torch):
     """A x and A^T z of the power-law rectangular matrix (FP32 values), each timed alone with L2
     flushed, plus the A^T A shell."""
@@ -182,7 +213,8 @@ def multinplace(args, torch):
 
 def main():
     p = argparse.ArgumentParser()
-    p.add_argument("kernel", choices=["gs", "spmv", "multinplace", "cross", "batched", "all"])
+    p.add_argument("kernel", choices=["gs", "spmv", "spmm", "multinplace", "cross", "batched", "all"])
+    p.add_argument("--nb", type=int, default=48, help="columns of the BVMatMult block")
     p.add_argument("--nprob", type=int, default=64)
     p.add_argument("--threads", type=int, default=512)
     p.add_argument("--rows", type=int, default=2_000_000)
@@ -210,7 +242,7 @@ def main():
             for line in cross(args, torch):
                 print(json.dumps(line), flush=True)
         else:
-            print(json.dumps({"spmv": spmv, "multinplace": multinplace}[k](args, torch)), flush=True)
+            print(json.dumps({"spmv": spmv, "spmm": spmm, "multinplace": multinplace}[k](args, torch)), flush=True)
 
 
 if __name__ == "__main__":

@@ -96,6 +96,48 @@ def test_spmv_mat_ragged_long_rows(b200, oracle_mod, schedule):
     np.testing.assert_allclose(y[~short], ref[~short], rtol=1e-12, atol=1e-12 * np.abs(ref).max())
 
 
+@pytest.mark.parametrize("case", ["laplacian", "ragged"])
+def test_bv_mat_mult_block_vs_columns(b200, oracle_mod, case):
+    """BVMatMult (block SpMV over the active columns) against the oracle's SpMV column by column:
+    bit for bit on rows the sliced-ELL slices hold (index-order sums, products and sums rounded
+    separately), to 1e-12 relative on the rows longer than a slice."""
+    rng = np.random.default_rng(7)
+    if case == "laplacian":
+        csr = P.laplacian_3d(30, 27, 25)
+        n = len(csr[0]) - 1
+        lens = np.diff(csr[0])
+    else:
+        n = 9001
+        lens = rng.integers(0, 12, size=n)
+        lens[::11] = 0
+        lens[[3, 4000, 9000]] = [700, 33, 64]
+        rowptr = np.zeros(n + 1, dtype=np.int32)
+        np.cumsum(lens, out=rowptr[1:])
+        colind = np.concatenate([np.sort(rng.choice(n, size=l, replace=False)) for l in lens]).astype(np.int32)
+        csr = (rowptr, colind, rng.standard_normal(int(rowptr[-1])))
+    A = b200.Mat().createAIJ(csr)
+    m = 21
+    X = rng.standard_normal((n, m))
+    V = b200.BV().create(n, m)
+    Y = b200.BV().create(n, m + 1)
+    V.setColumns(X)
+    for lk in ((0, m), (2, 19)):
+        V.setActiveColumns(*lk)
+        Y.setActiveColumns(1, 1 + lk[1] - lk[0])
+        V.matMult(A, Y)
+        got = Y.getColumns()
+        As = P.to_scipy(csr)
+        short = lens <= 32
+        for j in range(lk[1] - lk[0]):
+            ref = oracle_mod.spmv(As, X[:, lk[0] + j])
+            y = got[:, 1 + j]
+            np.testing.assert_array_equal(y[short], ref[short])
+            np.testing.assert_allclose(y[~short], ref[~short], rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+    V.destroy()
+    Y.destroy()
+    A.destroy()
+
+
 def test_bv_test1_golden_ops(b200):
     """src/sys/classes/bv/tests/test1.c: BVMult, BVMultVec, BVDot, BVDotVec, BVMultInPlace, BVScale, BVNorm."""
     torch = _torch()

@@ -122,6 +122,29 @@ def spmm(args, torch):
             "algorithmic_bytes": algo, "GBps": algo / (ms * 1e-3) / 1e9}
 
 
+def mixed(args, torch):
+    """A mixed-precision solve of the 3-D Laplacian (nev 32, ncv 80) cut after --restarts restarts
+    of the FP32-basis phase and --sweeps refinement sweeps: a short, complete run of every kernel of
+    the mixed form (for profiling); prints the solver's counters."""
+    csr = P.laplacian_3d(args.grid)
+    n = len(csr[0]) - 1
+    A = S.Mat().createAIJ(csr)
+    E = S.EPS().create()
+    E.setOperators(A)
+    E.setDimensions(32, 80)
+    E.setTolerances(1e-8)
+    E.setWhichEigenpairs(S.LARGEST_REAL)
+    E.setInitialSpace(P.start_vector(n, 0))
+    E.setPrecision(S.EPS.Precision.MIXED)
+    E.setMaxRestarts(args.restarts)
+    E.setMixedOptions(tol_low=1e-6, degree=32, max_sweeps=args.sweeps)
+    E.solve()
+    st = E.getStats()
+    E.destroy()
+    A.destroy()
+    return {"kernel": "mixed solve (FP32-basis phase + refinement)", "n": n, **st}
+
+
 def cross(args, torch):
     """A x and A^T z of the power-law rectangular matrix (FP32 values), each timed alone with L2
     flushed, plus the A^T A shell."""
@@ -213,7 +236,9 @@ def multinplace(args, torch):
 
 def main():
     p = argparse.ArgumentParser()
-    p.add_argument("kernel", choices=["gs", "spmv", "spmm", "multinplace", "cross", "batched", "all"])
+    p.add_argument("kernel", choices=["gs", "spmv", "spmm", "mixed", "multinplace", "cross", "batched", "all"])
+    p.add_argument("--restarts", type=int, default=3, help="mixed: restarts of the FP32-basis phase")
+    p.add_argument("--sweeps", type=int, default=1, help="mixed: refinement sweeps")
     p.add_argument("--nb", type=int, default=48, help="columns of the BVMatMult block")
     p.add_argument("--nprob", type=int, default=64)
     p.add_argument("--threads", type=int, default=512)
@@ -242,7 +267,8 @@ def main():
             for line in cross(args, torch):
                 print(json.dumps(line), flush=True)
         else:
-            print(json.dumps({"spmv": spmv, "spmm": spmm, "multinplace": multinplace}[k](args, torch)), flush=True)
+            print(json.dumps({"spmv": spmv, "spmm": spmm, "mixed": mixed, "multinplace": multinplace}[k](args, torch)),
+                  flush=True)
 
 
 if __name__ == "__main__":

@@ -430,6 +430,40 @@ b200_status b200_svd_solve_aij_host(int m, int n, int64_t nnz, const int *rowptr
                                     double tol, int max_it, double *sigma_host, double *U_host, double *V_host,
                                     double *rel_error_host, int *info_host, void *stream);
 
+/* ---------------------------------------------------- learned warm start --- */
+
+/* A spectral neural operator that maps the coefficient field of a diffusion
+ * operator on an N x N grid to nout fields, trained to reproduce the
+ * operator's lowest eigenvectors; its output is a starting block for
+ * EPSSetInitialSpace (src/eps/interface/epssetup.c:613), the hook through
+ * which a SLEPc user supplies an initial space (no network exists in SLEPc).
+ * Forward, backward and the Adam update run in this library's own FP32
+ * kernels.  Inputs per sample: 3 x N*N features (log kappa, x, y of the cell
+ * centres, row-major); outputs nout x N*N.  Network: pointwise lift to
+ * `width` channels, `layers` layers of (Dirichlet sine-mode spectral mixing
+ * over modes x modes modes + pointwise mixing, gelu), pointwise projection
+ * through `hidden` channels.  Loss per output k: 1 - (y_k . u_k)^2 / |y_k|^2
+ * against a unit target u_k, averaged.  Parameters are one flat FP32 array
+ * (set/get from host memory; initialisation is the caller's). */
+typedef struct b200_neural_op_s *b200_neural_op;
+b200_status b200_neural_op_create(int N, int width, int modes, int layers, int hidden, int nout, void *stream,
+                                  b200_neural_op *op);
+b200_status b200_neural_op_destroy(b200_neural_op op);
+b200_status b200_neural_op_num_params(b200_neural_op op, int64_t *n);
+b200_status b200_neural_op_set_params(b200_neural_op op, const float *params_host);  /* also resets Adam */
+b200_status b200_neural_op_get_params(b200_neural_op op, float *params_host);
+/* out_dev (batch x nout x N*N) = network(features_dev (batch x 3 x N*N)), device pointers */
+b200_status b200_neural_op_forward(b200_neural_op op, int batch, const float *features_dev, float *out_dev);
+/* mean loss against targets_dev (batch x nout x N*N) */
+b200_status b200_neural_op_loss(b200_neural_op op, int batch, const float *features_dev, const float *targets_dev,
+                                float *loss);
+/* loss and its gradient with respect to every parameter (grads_host nullable, nparams floats) */
+b200_status b200_neural_op_loss_grad(b200_neural_op op, int batch, const float *features_dev,
+                                     const float *targets_dev, float *loss, float *grads_host);
+/* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the loss of one batch */
+b200_status b200_neural_op_train_step(b200_neural_op op, int batch, const float *features_dev,
+                                      const float *targets_dev, float lr, float *loss);
+
 /* -------------------------------------------------------------- batched --- */
 
 /* Many independent small Hermitian eigenproblems solved by Krylov-Schur in one

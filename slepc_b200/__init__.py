@@ -93,6 +93,16 @@ _SIGS = {
     "b200_mat_load": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     "b200_mat_view": (ctypes.c_int, [_vp, _vp]),
     "b200_batch_create": (ctypes.c_int, [ctypes.c_int, _ip, _ip, _ip, _dp, _vp, _vp]),
+    "b200_neural_op_create": (ctypes.c_int, [ctypes.c_int] * 6 + [_vp, _vp]),
+    "b200_neural_op_destroy": (ctypes.c_int, [_vp]),
+    "b200_neural_op_num_params": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+    "b200_neural_op_set_params": (ctypes.c_int, [_vp, _vp]),
+    "b200_neural_op_get_params": (ctypes.c_int, [_vp, _vp]),
+    "b200_neural_op_forward": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
+    "b200_neural_op_loss": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.POINTER(ctypes.c_float)]),
+    "b200_neural_op_loss_grad": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.POINTER(ctypes.c_float), _vp]),
+    "b200_neural_op_train_step": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_float,
+                                                 ctypes.POINTER(ctypes.c_float)]),
     "b200_batch_destroy": (ctypes.c_int, [_vp]),
     "b200_batch_set_dimensions": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "b200_batch_set_tolerances": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int]),
@@ -838,6 +848,79 @@ def svd_solve_aij_host(csr, size, v0, nsv, ncv, tol=0.0, max_it=0, dtype=np.floa
     return {"sigma": sig[:k].copy(), "U": U[:k].T.copy() if want_vectors else None,
             "V": V[:k].T.copy() if want_vectors else None, "rel_error": err[:k].copy(), "nconv": k,
             "its": int(info[1]), "reason": int(info[2]), "lanczos_steps": int(info[3]), "restarts": int(info[4])}
+
+
+class NeuralOperator:
+    """The neural-operator warm start (b200_neural_op_*): features and targets are CUDA float32
+    tensors of shape (batch, 3, N*N) and (batch, nout, N*N); parameters are a flat float32 array."""
+
+    def __init__(self):
+        self.handle = ctypes.c_void_p()
+
+    def create(self, N, width=32, modes=16, layers=4, hidden=64, nout=16, stream=None):
+        _check(lib().b200_neural_op_create(N, width, modes, layers, hidden, nout, stream, ctypes.byref(self.handle)))
+        self.dims = (N, width, modes, layers, hidden, nout)
+        return self
+
+    def destroy(self):
+        if self.handle:
+            _check(lib().b200_neural_op_destroy(self.handle))
+            self.handle = ctypes.c_void_p()
+
+    def numParams(self):
+        n = ctypes.c_int64()
+        _check(lib().b200_neural_op_num_params(self.handle, ctypes.byref(n)))
+        return n.value
+
+    def setParams(self, theta):
+        theta = np.ascontiguousarray(theta, dtype=np.float32)
+        assert theta.size == self.numParams()
+        _check(lib().b200_neural_op_set_params(self.handle, theta.ctypes.data))
+
+    def getParams(self):
+        out = np.empty(self.numParams(), dtype=np.float32)
+        _check(lib().b200_neural_op_get_params(self.handle, out.ctypes.data))
+        return out
+
+    @staticmethod
+    def _dense(t):
+        """The kernels read dense (batch, channels, N*N) float32 device memory."""
+        import torch
+
+        if not t.is_cuda:
+            raise B200Error(1, "neural-operator tensors must be on the GPU")
+        return t.to(torch.float32).contiguous()
+
+    def forward(self, features):
+        import torch
+
+        features = self._dense(features)
+        N, _, _, _, _, K = self.dims
+        out = torch.empty((features.shape[0], K, N * N), dtype=torch.float32, device=features.device)
+        _check(lib().b200_neural_op_forward(self.handle, features.shape[0], features.data_ptr(), out.data_ptr()))
+        return out
+
+    def loss(self, features, targets):
+        features, targets = self._dense(features), self._dense(targets)
+        v = ctypes.c_float()
+        _check(lib().b200_neural_op_loss(self.handle, features.shape[0], features.data_ptr(), targets.data_ptr(),
+                                         ctypes.byref(v)))
+        return v.value
+
+    def lossGrad(self, features, targets):
+        features, targets = self._dense(features), self._dense(targets)
+        v = ctypes.c_float()
+        g = np.empty(self.numParams(), dtype=np.float32)
+        _check(lib().b200_neural_op_loss_grad(self.handle, features.shape[0], features.data_ptr(),
+                                              targets.data_ptr(), ctypes.byref(v), g.ctypes.data))
+        return v.value, g
+
+    def trainStep(self, features, targets, lr):
+        features, targets = self._dense(features), self._dense(targets)
+        v = ctypes.c_float()
+        _check(lib().b200_neural_op_train_step(self.handle, features.shape[0], features.data_ptr(),
+                                               targets.data_ptr(), lr, ctypes.byref(v)))
+        return v.value
 
 
 class BatchEPS:

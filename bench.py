@@ -58,7 +58,12 @@ def parse():
     p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                    help="laplacian3d: arithmetic of the timed solve (fp64: the drop-in path; mixed: FP32 basis "
                         "then FP64 Chebyshev-filtered Rayleigh-Ritz); the fp64 line also reports the mixed form")
-    p.add_argument("--workload", choices=["laplacian3d", "cross", "batched"], default="laplacian3d",
+    p.add_argument("--learn-grid", type=int, default=64, help="learned workload: N of the N x N diffusion grid")
+    p.add_argument("--learn-nev", type=int, default=16, help="learned workload: eigenpairs (LOBPCG block)")
+    p.add_argument("--train-fields", type=int, default=256, help="learned workload: training fields")
+    p.add_argument("--eval-fields", type=int, default=16, help="learned workload: held-out fields per step")
+    p.add_argument("--epochs", type=int, default=120, help="learned workload: training epochs")
+    p.add_argument("--workload", choices=["laplacian3d", "cross", "batched", "learned"], default="laplacian3d",
                    help="laplacian3d: the EPS headline case; cross: largest singular triplets of the "
                         "2,000,000 x 500,000 power-law matrix through A^T A; batched: 4096 k-NN graph "
                         "eigenproblems in one persistent launch")
@@ -803,8 +808,135 @@ def run_b200_batched(args):
     return 0
 
 
+# ------------------------------------------------------------------ learned warm start workload
+EVAL_SEED0 = 100000
+
+
+def learned_config(args, extra=None):
+    d = {"workload": (f"{args.learn_nev} smallest eigenpairs of -div(kappa grad u) on a {args.learn_grid}^2 grid "
+                      "(5-point FV, kappa = exp(GRF), variance 1, correlation length U[0.05, 0.2]) by LOBPCG (Jacobi, "
+                      f"block {args.learn_nev}, tol 1e-8) on {args.eval_fields} held-out fields, started from the "
+                      "neural operator's block; the network (width 32, 12 x 12 modes, 4 layers) trained on the "
+                      f"plain solver's eigenvectors of {args.train_fields} fields, {args.epochs} epochs"),
+         "grid": args.learn_grid, "nev": args.learn_nev, "train_fields": args.train_fields,
+         "eval_fields": args.eval_fields, "epochs": args.epochs, "tol": 1e-8,
+         "l2": "fields of %d x %d cells; every solve is a separate operator" % (args.learn_grid, args.learn_grid),
+         "parallelism": "single GPU"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+def run_b200_learned(args):
+    import torch
+
+    import slepc_b200 as S
+    from slepc_b200 import learned as LN
+
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    N, nev = args.learn_grid, args.learn_nev
+    t0 = time.perf_counter()
+    F, T, its_train = LN.dataset(S, N, range(args.train_fields), nev)
+    t_data = time.perf_counter() - t0
+    dims = (N, 32, 12, 4, 64, nev)
+    op = S.NeuralOperator().create(*dims)
+    op.setParams(LN.init_params(*dims, seed=0))
+    Fd, Td = torch.from_numpy(F).cuda(), torch.from_numpy(T).cuda()
+    t0 = time.perf_counter()
+    hist = LN.train(op, Fd, Td, epochs=args.epochs, batch=8, lr=2e-3, lr_final=2e-4)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    seeds = list(range(EVAL_SEED0, EVAL_SEED0 + args.eval_fields))
+    probs = [P.diffusion_problem(N, sd) for sd in seeds]
+    feats = torch.from_numpy(np.stack([LN.features(k) for _, k, _ in probs])).cuda()
+    launches0 = None
+
+    def step(learned):
+        blocks = LN.predict(op, feats) if learned else None
+        out = []
+        for i, (csr, _, _) in enumerate(probs):
+            X0 = blocks[i].T.astype(np.float64) if learned else None
+            out.append(LN.solve_lowest(S, csr, nev, X0=X0))
+        return out
+
+    for _ in range(args.warmup):
+        step(True)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    launches0 = S.kernel_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        res_l = step(True)
+    ev1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = S.kernel_launch_count() - launches0
+    ms_step = ev0.elapsed_time(ev1) / args.steps
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    res_r = step(False)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_random = e0.elapsed_time(e1)
+    # end to end: host fields in, host eigenpairs out (features up, network, block down, solve, pairs down)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        hf = torch.from_numpy(np.stack([LN.features(k) for _, k, _ in probs])).pin_memory()
+        blocks = LN.predict(op, hf.cuda(non_blocking=True))
+        for i, (csr, _, _) in enumerate(probs):
+            LN.solve_lowest(S, csr, nev, X0=blocks[i].T.astype(np.float64))
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    captured = [LN.captured(r["X"], b.T.astype(np.float64)) for r, b in zip(res_r, LN.predict(op, feats))]
+    its_l = [r["its"] for r in res_l]
+    its_r = [r["its"] for r in res_r]
+    ok = all(r["nconv"] >= nev and r["max_error"] <= 1e-8 for r in res_l + res_r)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+
+        threads = os.cpu_count() or 1
+        oracle.set_threads(threads)
+        csr0 = probs[0][0]
+        t0 = time.perf_counter()
+        r = oracle.lobpcg(P.to_scipy(csr0), nev, tol=1e-8, max_it=100000)
+        tc = time.perf_counter() - t0
+        cpu = {"value": tc, "unit": "s per field", "cores": threads, "kind": "port",
+               "sample": f"oracle LOBPCG from the random block on held-out field {seeds[0]} ({r.its} iterations)"}
+    if rank == 0:
+        n = args.eval_fields
+        line = {"metric": "time_to_all_residuals_le_1e-8_per_field", "value": ms_step / 1e3 / n, "unit": "s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64 solve, f32 network",
+                "data": "synthetic (seeded Gaussian random fields)",
+                "config": learned_config(args, {"dataset_seconds": t_data, "train_seconds": t_train,
+                                                "final_train_loss": hist[-1],
+                                                "mean_train_solve_iterations": float(np.mean(its_train))}),
+                "learned_vs_random": {"s_per_field_random": ms_random / 1e3 / n, "speedup": ms_random / ms_step,
+                                      "mean_iterations_learned": float(np.mean(its_l)),
+                                      "mean_iterations_random": float(np.mean(its_r)),
+                                      "iterations_learned": its_l, "iterations_random": its_r,
+                                      "mean_captured_subspace": float(np.mean(captured)),
+                                      "all_pairs_converged_to_1e-8": ok},
+                "roofline": None,
+                "e2e": {"value": e2e_s / n, "unit": "s", "h2d_bytes_per_step": int(n * 3 * N * N * 4),
+                        "d2h_bytes_per_step": int(n * nev * N * N * 12)},
+                "gpu_launches": int(launches), "clocks": clk, "cpu_baseline": cpu}
+        print(json.dumps(line))
+    op.destroy()
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "learned":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the learned workload has no reference arm: SLEPc "
+                              "has no learned start; its CPU baseline (oracle LOBPCG) is in the b200 line"}))
+            return 0
+        return run_b200_learned(args)
     if args.workload == "batched":
         if args.impl == "reference":
             return run_reference_batched(args)

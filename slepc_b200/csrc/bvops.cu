@@ -93,6 +93,74 @@ __global__ void __launch_bounds__(kGemmThreads) panel_gemm_kernel(const TI *X, i
   }
 }
 
+// The same product on the FP64 tensor cores: Y(:,0:nc) = X(:,0:kq) Q(0:kq,0:nc) with
+// mma.sync.m8n8k4.f64 (tcgen05 has no FP64 kind).  A CTA loads a kRB-row panel of X (zero-padded to
+// a multiple of 4 columns, converted to FP64) and Q (zero-padded to NT 8-column tiles) into shared
+// memory; warp w computes rows 8w..8w+7 of the panel against all NT column tiles (lane (g, t) holds
+// A(g, t), B(t, g) and D(g, 2t..2t+1) of each 8x8x4 step); the results are staged back through the
+// panel's shared memory and written out column by column.  A panel is read completely before any of
+// its rows is written, so X and Y may overlap (in-place BVMultInPlace).  Row strides of 72 and
+// (8 mod 16) doubles keep each fragment load at two shared-memory wavefronts.
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+constexpr int kDmmaStride = kRB + 8;  // doubles between panel columns in shared memory
+
+__host__ __device__ inline int dmma_q_stride(int ncp) { return (ncp % 16) ? ncp : ncp + 8; }
+
+template <int NT, typename TI, typename TO>
+__global__ void __launch_bounds__(kGemmThreads) panel_dmma_kernel(const TI *X, int ldx, TO *Y, int ldy, int n, int kq,
+                                                                  const double *__restrict__ Q, int ldq, int nc) {
+  static_assert(kRB == 8 * (kGemmThreads / 32), "one 8-row strip per warp");
+  extern __shared__ __align__(16) double sm[];
+  const int kp = (kq + 3) & ~3;
+  constexpr int ncp = NT * 8;
+  const int SQ = dmma_q_stride(ncp);
+  double *Qs = sm;                          // kp x SQ, Qs[k*SQ + j] = Q(k, j)
+  double *Xs = sm + (size_t)kp * SQ;        // panel: Xs[c*kDmmaStride + r]; then the output tile
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  for (int idx = tid; idx < kp * ncp; idx += kGemmThreads) {
+    const int k = idx / ncp, j = idx - k * ncp;
+    Qs[k * SQ + j] = (k < kq && j < nc) ? Q[(size_t)k + (size_t)j * ldq] : 0.0;
+  }
+  const int npanels = (n + kRB - 1) / kRB;
+  for (int pnl = blockIdx.x; pnl < npanels; pnl += gridDim.x) {
+    const long long r0 = (long long)pnl * kRB;
+    const int rows = (int)min((long long)kRB, (long long)n - r0);
+    __syncthreads();  // the previous panel's output has been written out
+    for (int idx = tid; idx < kp * kRB; idx += kGemmThreads) {
+      const int c = idx / kRB, r = idx - c * kRB;
+      Xs[c * kDmmaStride + r] = (c < kq && r < rows) ? (double)X[(size_t)c * ldx + r0 + r] : 0.0;
+    }
+    __syncthreads();
+    double acc[NT][2];
+#pragma unroll
+    for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = 0.0;
+    const double *xa = Xs + t * kDmmaStride + warp * 8 + g;
+    const double *qb = Qs + t * SQ + g;
+    for (int k0 = 0; k0 < kp; k0 += 4) {
+      const double a = xa[k0 * kDmmaStride];
+#pragma unroll
+      for (int j = 0; j < NT; ++j) dmma_8x8x4(acc[j], a, qb[k0 * SQ + 8 * j]);
+    }
+    __syncthreads();  // every warp is done with the panel: its space takes the output tile
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+      Xs[(8 * j + 2 * t) * kDmmaStride + warp * 8 + g] = acc[j][0];
+      Xs[(8 * j + 2 * t + 1) * kDmmaStride + warp * 8 + g] = acc[j][1];
+    }
+    __syncthreads();
+    for (int idx = tid; idx < nc * kRB; idx += kGemmThreads) {
+      const int j = idx / kRB, r = idx - j * kRB;
+      if (r < rows) Y[(size_t)j * ldy + r0 + r] = (TO)Xs[j * kDmmaStride + r];
+    }
+  }
+}
+
 // Y(:,j) = alpha * X(:,0:nx) Q(0:nx,j) + beta * Y(:,j), one thread per row, Q column in registers-free loop.
 __global__ void mult_kernel(double *Y, int ldy, const double *__restrict__ X, int ldx, int n, int nx, int ny,
                             const double *__restrict__ Q, int ldq, double alpha, double beta) {
@@ -459,6 +527,34 @@ cudaError_t panel_gemm_launch(const TI *X, int ldx, TO *Y, int ldy, int n, int k
                               cudaStream_t stream) {
   if (nc <= 0 || kq <= 0 || n <= 0) return cudaSuccess;
   if (nc > 16 * 8 || kq > kMaxCols) return cudaErrorInvalidValue;
+  {
+    // FP64 tensor cores when the padded panel and Q fit in shared memory
+    const int kp = (kq + 3) & ~3, nt = (nc + 7) / 8, ncp = 8 * nt;
+    const size_t dsm = sizeof(double) * ((size_t)kp * dmma_q_stride(ncp) + (size_t)(kp > ncp ? kp : ncp) * kDmmaStride);
+    if (dsm + 1024 <= max_dynamic_smem()) {
+      const int npanels = (n + kRB - 1) / kRB;
+      int grid = num_sms() * 2;
+      if (grid > npanels) grid = npanels;
+      cudaError_t err = cudaSuccess;
+      switch (nt) {
+#define B200_DMMA_CASE(NT)                                                                                  \
+  case NT:                                                                                                  \
+    err = allow_max_dynamic_smem(panel_dmma_kernel<NT, TI, TO>);                                            \
+    if (err != cudaSuccess) return err;                                                                     \
+    panel_dmma_kernel<NT, TI, TO><<<grid, kGemmThreads, dsm, stream>>>(X, ldx, Y, ldy, n, kq, Q, ldq, nc);   \
+    break;
+        B200_DMMA_CASE(1) B200_DMMA_CASE(2) B200_DMMA_CASE(3) B200_DMMA_CASE(4) B200_DMMA_CASE(5)
+        B200_DMMA_CASE(6) B200_DMMA_CASE(7) B200_DMMA_CASE(8) B200_DMMA_CASE(9) B200_DMMA_CASE(10)
+        B200_DMMA_CASE(11) B200_DMMA_CASE(12) B200_DMMA_CASE(13) B200_DMMA_CASE(14) B200_DMMA_CASE(15)
+        B200_DMMA_CASE(16)
+#undef B200_DMMA_CASE
+        default:
+          return cudaErrorInvalidValue;
+      }
+      count_launch();
+      return cudaGetLastError();
+    }
+  }
   const size_t smem = sizeof(double) * ((size_t)kq * nc + (size_t)(kq > nc ? kq : nc) * (kRB + 1));
   if (smem + 1024 > max_dynamic_smem()) return cudaErrorInvalidValue;
   const int maxj = (nc + 15) / 16;

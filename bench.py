@@ -310,6 +310,8 @@ def run_b200(args):
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
     h_csr = (pin(csr[0]), pin(csr[1]), pin(csr[2]))
     h_v0 = pin(v0)
+    # the caller's page-locked output block, allocated once and reused by every call
+    h_out = torch.empty((args.ncv + 1, n), dtype=torch.float64).pin_memory().numpy()
     barrier()
     t0 = time.perf_counter()
     e2e_last = None
@@ -317,7 +319,8 @@ def run_b200(args):
         if mixed:
             e2e_last = mixed_host_solve(S, h_csr, h_v0, args)
         else:
-            e2e_last = S.solve_csr_host(h_csr, h_v0, args.nev, args.ncv, tol=1e-8, which=S.LARGEST_REAL)
+            e2e_last = S.solve_csr_host(h_csr, h_v0, args.nev, args.ncv, tol=1e-8, which=S.LARGEST_REAL,
+                                        out=h_out)
     e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
     h2d = csr[0].nbytes + csr[1].nbytes + csr[2].nbytes + v0.nbytes
     d2h = e2e_last["nconv"] * (n * 8 + 16)

@@ -710,21 +710,29 @@ def orthogonalize_column_noalloc(n, ld, ncols, V_ptr, j, H_ptr, stream=None):
 
 
 def solve_csr_host(csr, v0, nev, ncv, tol=1e-8, which=LARGEST_MAGNITUDE, mpd=0, max_it=0, want_vectors=True,
-                   stream=None):
-    """One call from host CSR arrays to host eigenpairs (b200_eps_solve_csr_host)."""
+                   stream=None, out=None):
+    """One call from host CSR arrays to host eigenpairs (b200_eps_solve_csr_host).  out: an optional
+    C-contiguous float64 array of shape (ncv + 1, n) that receives the eigenvectors (row i = vector i),
+    for callers that keep a reused (for instance page-locked) output buffer."""
     rowptr, colind, vals = (np.ascontiguousarray(csr[0], dtype=np.int32), np.ascontiguousarray(csr[1], dtype=np.int32),
                             np.ascontiguousarray(csr[2], dtype=np.float64))
     n = len(rowptr) - 1
     v0 = np.ascontiguousarray(v0, dtype=np.float64)
     evals = np.zeros(ncv + 1)
     errest = np.zeros(ncv + 1)
-    X = np.zeros((ncv + 1, n)) if want_vectors else None
+    # np.empty: only the rows the library writes (nconv of them) are ever touched
+    if want_vectors and out is not None:
+        if out.shape != (ncv + 1, n) or out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]:
+            raise B200Error(1, "out must be a C-contiguous float64 array of shape (ncv + 1, n)")
+        X = out
+    else:
+        X = np.empty((ncv + 1, n)) if want_vectors else None
     info = np.zeros(8, dtype=np.int32)
     _check(lib().b200_eps_solve_csr_host(n, int(rowptr[-1]), _i(rowptr), _i(colind), _d(vals), _d(v0), nev, ncv, mpd,
                                          tol, max_it, which, _d(evals), _d(X) if want_vectors else None, _d(errest),
                                          _i(info), stream))
     nconv = int(info[0])
-    return {"evals": evals[:nconv].copy(), "X": X[:nconv].T.copy() if want_vectors else None,
+    return {"evals": evals[:nconv].copy(), "X": X[:nconv].T if want_vectors else None,
             "errest": errest[:nconv].copy(), "nconv": nconv, "its": int(info[1]), "reason": int(info[2]),
             "lanczos_steps": int(info[3]), "restarts": int(info[4])}
 
@@ -838,15 +846,15 @@ def svd_solve_aij_host(csr, size, v0, nsv, ncv, tol=0.0, max_it=0, dtype=np.floa
     v0 = np.ascontiguousarray(v0, dtype=np.float64)
     sig = np.zeros(ncv + 1)
     err = np.zeros(ncv + 1)
-    U = np.zeros((ncv + 1, m)) if want_vectors else None
-    V = np.zeros((ncv + 1, n)) if want_vectors else None
+    U = np.empty((ncv + 1, m)) if want_vectors else None
+    V = np.empty((ncv + 1, n)) if want_vectors else None
     info = np.zeros(8, dtype=np.int32)
     _check(lib().b200_svd_solve_aij_host(m, n, int(rowptr[-1]), _i(rowptr), _i(colind), vals.ctypes.data, st, _d(v0),
                                          nsv, ncv, tol, max_it, _d(sig), _d(U) if want_vectors else None,
                                          _d(V) if want_vectors else None, _d(err), _i(info), stream))
     k = int(info[0])
-    return {"sigma": sig[:k].copy(), "U": U[:k].T.copy() if want_vectors else None,
-            "V": V[:k].T.copy() if want_vectors else None, "rel_error": err[:k].copy(), "nconv": k,
+    return {"sigma": sig[:k].copy(), "U": U[:k].T if want_vectors else None,
+            "V": V[:k].T if want_vectors else None, "rel_error": err[:k].copy(), "nconv": k,
             "its": int(info[1]), "reason": int(info[2]), "lanczos_steps": int(info[3]), "restarts": int(info[4])}
 
 

@@ -647,7 +647,9 @@ def batched_workload(args):
 def batched_config(args, B, extra=None):
     d = {"workload": f"{args.nprob} independent symmetric eigenproblems, n ~ U[500, 20000], each 2I - L_norm of a "
                      "symmetrised 8-NN graph of uniform points in the unit square, FP64 CSR, nev=8 largest real, "
-                     "ncv=24, tol=1e-8, one persistent launch under a captured CUDA graph",
+                     "ncv=24, tol=1e-8, one persistent launch under a captured CUDA graph"
+                     + (" (mixed: FP32-basis phase to 1e-6, then the FP64 solve from the phase-1 Ritz vectors, "
+                        "three launches in one graph)" if args.precision == "mixed" else ""),
          "nprob": args.nprob, "rows": int(B.ns.sum()), "nnz": int(B.vals.size), "nev": 8, "ncv": 24, "tol": 1e-8,
          "start_vector": "N(0,1), seed = problem index",
          "l2": "inputs larger than L2: CSR %.1f GB, bases %.1f GB (L2 = 126 MB)"
@@ -740,6 +742,8 @@ def run_b200_batched(args):
         E.setTolerances(1e-8)
         E.setWhichEigenpairs(S.LARGEST_REAL)
         E.setInitialVectors(v0)
+        if args.precision == "mixed":
+            E.setPrecision(S.EPS.Precision.MIXED, 1e-6)
         return E
 
     E = make()
@@ -791,7 +795,7 @@ def run_b200_batched(args):
     if rank == 0:
         line = {"metric": "time_to_all_residuals_le_1e-8", "value": ms_per_step / 1e3, "unit": "s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 basis then f64" if args.precision == "mixed" else "f64",
                 "data": "synthetic (seeded k-NN graphs, seeded N(0,1) start vectors)",
                 "config": batched_config(args, B, {
                     "threads_per_problem": threads, "all_converged": bool(np.all(info[:, 2] == 1)),

@@ -503,6 +503,15 @@ b200_status b200_batch_get_all(b200_batch B, double *evals_host, int *info_host,
 /* Algorithmic bytes the last solve moved (SpMV: 12 per nonzero plus the vectors; Gram-Schmidt
  * dots and updates: 8 per row and column touched; restarts), summed over the problems. */
 b200_status b200_batch_get_bytes(b200_batch B, double *bytes);
+/* Precision of the batched solve (no SLEPc counterpart).  B200_PRECISION_FP64 (default);
+ * B200_PRECISION_MIXED: phase 1 runs the same per-problem Krylov-Schur with every basis stored in
+ * FP32 (FP64 work vector, products and sums; half the basis bytes) to tol_low (default 1e-6);
+ * phase 2 runs the FP64 solve of each problem from the sum of its phase-1 Ritz vectors to tol.
+ * The three launches (phase 1, start vectors, phase 2) form one captured graph; the results are
+ * phase 2's.  get_bytes then counts both phases. */
+b200_status b200_batch_set_precision(b200_batch B, int precision, double tol_low);
+/* Phase-1 counters of the last mixed solve: info_host (nprob x 8, as get_all) and its bytes. */
+b200_status b200_batch_get_phase1(b200_batch B, int *info_host, double *bytes);
 
 #ifdef __cplusplus
 }

@@ -115,6 +115,8 @@ _SIGS = {
     "b200_batch_get_eigenvector": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _dp]),
     "b200_batch_get_all": (ctypes.c_int, [_vp, _dp, _ip, ctypes.POINTER(ctypes.c_float)]),
     "b200_batch_get_bytes": (ctypes.c_int, [_vp, _dp]),
+    "b200_batch_set_precision": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double]),
+    "b200_batch_get_phase1": (ctypes.c_int, [_vp, _vp, _dp]),
     "b200_svd_create": (ctypes.c_int, [_vp, _vp]),
     "b200_svd_destroy": (ctypes.c_int, [_vp]),
     "b200_svd_set_operator": (ctypes.c_int, [_vp, _vp]),
@@ -1002,6 +1004,18 @@ class BatchEPS:
         v = ctypes.c_double()
         _check(lib().b200_batch_get_bytes(self.handle, ctypes.byref(v)))
         return v.value
+
+    def setPrecision(self, precision, tol_low=0.0):
+        """EPS.Precision.FP64 (default) or EPS.Precision.MIXED: phase 1 on FP32 bases to tol_low, then
+        the FP64 solve of every problem from the sum of its phase-1 Ritz vectors."""
+        _check(lib().b200_batch_set_precision(self.handle, precision, tol_low))
+
+    def getPhase1(self):
+        """Phase-1 counters of the last mixed solve: (info (nprob x 8), algorithmic bytes)."""
+        info = np.zeros((len(self.ns), 8), dtype=np.int32)
+        v = ctypes.c_double()
+        _check(lib().b200_batch_get_phase1(self.handle, info.ctypes.data, ctypes.byref(v)))
+        return info, v.value
 
     def destroy(self):
         if self.handle:

@@ -87,9 +87,9 @@ __device__ __forceinline__ uint64_t bsplitmix(uint64_t z) {
 }
 
 // y = A x for one problem: warps walk its tiles (<= 32 rows, <= kWarpTileNnz nonzeros)
-template <int T>
+template <int T, typename XT>
 __device__ void cta_spmv(const BProblem &P, const int *__restrict__ rowptr, const int *__restrict__ colind,
-                         const double *__restrict__ vals, const int4 *__restrict__ tiles, const double *x, double *y,
+                         const double *__restrict__ vals, const int4 *__restrict__ tiles, const XT *x, double *y,
                          BShared<T> &sh) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   double *prod = sh.prod[wib];
@@ -103,7 +103,7 @@ __device__ void cta_spmv(const BProblem &P, const int *__restrict__ rowptr, cons
     const int nxt = __shfl_down_sync(0xffffffffu, mystart, 1);
     const int myend = (lane + 1 < nrows) ? nxt : p1;
     const int cnt = p1 - p0;
-    for (int q = lane; q < cnt; q += 32) prod[q] = __dmul_rn(va[p0 + q], __ldcg(x + ci[p0 + q]));
+    for (int q = lane; q < cnt; q += 32) prod[q] = __dmul_rn(va[p0 + q], (double)__ldcg(x + ci[p0 + q]));
     __syncwarp();
     if (lane < nrows) {
       double s = 0.0;
@@ -505,7 +505,7 @@ __global__ void __launch_bounds__(T) batched_ks_kernel(int nprob, const BProblem
       const int k0 = nconv + l;
       int m = nv, breakdown = 0;
       for (int j = k0; j < m; ++j) {
-        cta_spmv<T>(P, rowptr, colind, vals, tiles, V + (size_t)j * ld, V + (size_t)(j + 1) * ld, sh);
+        cta_spmv<T, double>(P, rowptr, colind, vals, tiles, V + (size_t)j * ld, V + (size_t)(j + 1) * ld, sh);
         if (threadIdx.x == 0) sh.bytes += 12ull * P.nnz + 4ull * (n + 1) + 16ull * n;
         double nrm;
         int lindep;
@@ -629,6 +629,346 @@ __global__ void __launch_bounds__(T) batched_ks_kernel(int nprob, const BProblem
   }
 }
 
+// ---- FP32 basis (phase 1 of the mixed form): the basis columns are stored as FP32, the vector
+// being orthogonalised is a separate FP64 work vector, every product and sum is FP64.
+
+// sh.c[i] = V32(:,i)' w for i < ncols and sh.c[ncols] = w' w (deterministic, groups of 8 columns)
+template <int T>
+__device__ void cta_dots32(const float *V, int ld, int n, int ncols, const double *w, BShared<T> &sh) {
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  if (threadIdx.x == 0) sh.bytes += 4ull * n * ncols + 8ull * n;
+  for (int g0 = 0; g0 < ncols || g0 == 0; g0 += 8) {
+    const int gn = min(8, ncols - g0);
+    double acc[8], self = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) acc[i] = 0.0;
+    for (int r = threadIdx.x; r < n; r += T) {
+      const double wr = __ldcg(w + r);
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+        if (i < gn) acc[i] = fma((double)__ldcg(V + r + (size_t)(g0 + i) * ld), wr, acc[i]);
+      if (g0 == 0) self = fma(wr, wr, self);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const double v = bwarp_sum(acc[i]);
+      if (lane == 0 && i < gn) sh.red[wib][g0 + i] = v;
+    }
+    if (g0 == 0) {
+      const double v = bwarp_sum(self);
+      if (lane == 0) sh.red[wib][ncols] = v;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x <= ncols) {
+    double sacc = 0.0;
+    for (int w2 = 0; w2 < T / 32; ++w2) sacc += sh.red[w2][threadIdx.x];
+    sh.c[threadIdx.x] = sacc;
+  }
+  __syncthreads();
+}
+
+// w -= V32(:,0:ncols) coef
+template <int T>
+__device__ void cta_update32(const float *V, int ld, int n, int ncols, const double *coef, double *w) {
+  for (int r = threadIdx.x; r < n; r += T) {
+    double acc = 0.0;
+    for (int i = 0; i < ncols; ++i) acc = fma((double)__ldcg(V + r + (size_t)i * ld), coef[i], acc);
+    w[r] = __ldcg(w + r) - acc;
+  }
+  __syncthreads();
+}
+
+// CGS + DGKS "if needed" of the FP64 vector w against the FP32 columns 0..j-1 (the same decisions
+// as cta_orthonormalize), w scaled by 1/norm, then rounded into column j of the basis.
+template <int T>
+__device__ void cta_orth32(float *V, int ld, int n, int j, double *w, double eta, double *h, double *norm,
+                           int *lindep, int *err, BShared<T> &sh) {
+  for (int i = 0; i < j; ++i) h[i] = 0.0;
+  int more = 1, passes = 0;
+  while (more) {
+    cta_dots32<T>(V, ld, n, j, w, sh);
+    for (int i = 0; i < j; ++i) h[i] += sh.c[i];
+    cta_update32<T>(V, ld, n, j, sh.c, w);
+    if (threadIdx.x == 0 && j > 0) sh.bytes += 4ull * n * j + 16ull * n;
+    if (threadIdx.x == 0) {
+      const double self = sh.c[j];
+      if (self < 0.0) sh.flag[2] = 1;
+      const double onrm = sqrt(self < 0.0 ? 0.0 : self);
+      double sum = 0.0;
+      for (int i = 0; i < j; ++i) sum += sh.c[i] * sh.c[i];
+      const double est = onrm * onrm - sum;
+      sh.scal[0] = onrm;
+      sh.scal[1] = est;
+      sh.flag[0] = est <= 0.0;
+    }
+    __syncthreads();
+    double nrm;
+    if (sh.flag[0]) {
+      cta_dots32<T>(V, ld, n, 0, w, sh);  // explicit norm
+      nrm = sqrt(sh.c[0]);
+    } else {
+      nrm = sqrt(sh.scal[1]);
+    }
+    ++passes;
+    if (threadIdx.x == 0) {
+      const double onrm = sh.scal[0];
+      sh.scal[2] = nrm;
+      sh.flag[1] = (passes < 3 && nrm != 0.0 && fabs(nrm) < eta * fabs(onrm));
+      sh.flag[3] = !(nrm != 0.0 && fabs(nrm) >= eta * fabs(onrm));
+    }
+    __syncthreads();
+    more = sh.flag[1];
+    __syncthreads();
+  }
+  const double nrm = sh.scal[2];
+  *lindep = sh.flag[3];
+  if (sh.flag[2]) *err = 1;
+  *norm = nrm;
+  __syncthreads();
+  const double sc = (nrm != 1.0 && nrm != 0.0) ? 1.0 / nrm : 1.0;
+  float *col = V + (size_t)j * ld;
+  for (int r = threadIdx.x; r < n; r += T) {
+    const double v = __ldcg(w + r) * sc;
+    w[r] = v;
+    col[r] = __double2float_rn(v);
+  }
+  if (threadIdx.x == 0) sh.bytes += 20ull * n;
+  __syncthreads();
+}
+
+// V32(:, s:e) = V32(:, l:k) Q(l:k, s:e) in place (FP64 sums)
+template <int T>
+__device__ void cta_multinplace32(float *V, int ld, int n, int l, int k, const double *Q, int s, int e) {
+  if (e <= s || k <= l) return;
+  for (int r = threadIdx.x; r < n; r += T) {
+    double row[kBCols];
+#pragma unroll
+    for (int c = 0; c < kBCols; ++c)
+      if (c < k - l) row[c] = (double)__ldcg(V + r + (size_t)(l + c) * ld);
+    for (int j = s; j < e; ++j) {
+      double acc = 0.0;
+#pragma unroll
+      for (int c = 0; c < kBCols; ++c)
+        if (c < k - l) acc = fma(row[c], Q[(l + c) + j * kBLd], acc);
+      V[r + (size_t)j * ld] = __double2float_rn(acc);
+    }
+  }
+  __syncthreads();
+}
+
+// Phase 1 of the batched mixed form: batched_ks_kernel's loop on an FP32 basis (same decisions,
+// same projected-problem code), stopping at prm.tol (the loose tolerance).  W holds one FP64 work
+// vector per problem (at the problem's row offset).
+template <int T>
+__global__ void __launch_bounds__(T) batched_ks32_kernel(int nprob, const BProblem *__restrict__ probs,
+                                                         const int *__restrict__ order, int *__restrict__ next,
+                                                         const int *__restrict__ rowptr,
+                                                         const int *__restrict__ colind,
+                                                         const double *__restrict__ vals,
+                                                         const int4 *__restrict__ tiles,
+                                                         const double *__restrict__ v0, float *Vall, double *Wall,
+                                                         BParams prm, double *__restrict__ evals,
+                                                         double *__restrict__ errest_out, int *__restrict__ vcol,
+                                                         int *__restrict__ info, double *__restrict__ bytes_out) {
+  __shared__ BShared<T> sh;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int q = atomicAdd(next, 1);
+      sh.problem = q < nprob ? order[q] : -1;
+    }
+    __syncthreads();
+    const int pidx = sh.problem;
+    __syncthreads();
+    if (pidx < 0) return;
+    const BProblem P = probs[pidx];
+    const int n = P.n, ld = P.ld;
+    float *V = Vall + P.v_off;
+    double *w = Wall + P.x_off;
+    const int ncv = prm.ncv, mpd = prm.mpd, nev = prm.nev;
+    const int max_it = prm.max_it_user > 0 ? prm.max_it_user : max(100, 2 * n / ncv);
+    int err = 0;
+    uint64_t nrand = 0;
+    if (threadIdx.x < 8) sh.flag[threadIdx.x] = 0;
+    if (threadIdx.x == 0) sh.bytes = 0;
+    __syncthreads();
+    BDs ds{0, 0, 0, 0, 0};
+    double h[kBCols + 1];
+    int nini = 0;
+    {
+      cta_copy<T>(w, v0 + P.x_off, n);
+      double nrm;
+      int lindep;
+      cta_orth32<T>(V, ld, n, 0, w, prm.eta, h, &nrm, &lindep, &err, sh);
+      nini = (nrm == 0.0 || lindep) ? 0 : 1;
+      if (!nini) {
+        cta_random<T>(w, n, prm.seed, nrand++);
+        cta_orth32<T>(V, ld, n, 0, w, prm.eta, h, &nrm, &lindep, &err, sh);
+      }
+      if (nrm == 0.0 || lindep) err = 2;
+    }
+    int nconv = 0, its = 0, reason = 0, l = 0;
+    long long steps = 0;
+    double beta = 0.0;
+    if (threadIdx.x < kBLd) {
+      sh.d[threadIdx.x] = 0.0;
+      sh.e[threadIdx.x] = 0.0;
+    }
+    __syncthreads();
+    while (reason == 0 && !err) {
+      ++its;
+      int nv = min(nconv + mpd, ncv);
+      ds.n = nv;
+      ds.t = nv;
+      ds.l = nconv;
+      ds.k = nconv + l;
+      const int k0 = nconv + l;
+      int m = nv, breakdown = 0;
+      for (int j = k0; j < m; ++j) {
+        cta_spmv<T, float>(P, rowptr, colind, vals, tiles, V + (size_t)j * ld, w, sh);
+        if (threadIdx.x == 0) sh.bytes += 12ull * P.nnz + 4ull * (n + 1) + 12ull * n;
+        double nrm;
+        int lindep;
+        cta_orth32<T>(V, ld, n, j + 1, w, prm.eta, h, &nrm, &lindep, &err, sh);
+        if (threadIdx.x == 0) {
+          sh.d[j] = h[j];
+          sh.e[j] = lindep ? 0.0 : nrm;
+        }
+        ++steps;
+        beta = nrm;
+        if (lindep) {
+          m = j + 1;
+          breakdown = 1;
+          break;
+        }
+      }
+      __syncthreads();
+      nv = m;
+      ds.n = nv;
+      ds.t = nv;
+      ds.l = nconv;
+      ds.k = nconv + l;
+      ds.state = l ? 0 : 1;
+      if (wib == 0) {
+        ds_solve(ds, sh.d, sh.e, sh.Q, sh.wr, lane);
+        ds_sort(ds, sh.d, sh.Q, sh.wr, sh.perm, prm.which, lane);
+        const double bt = sh.e[ds.n - 1];
+        __syncwarp();
+        if (lane < ds.n) sh.e[lane] = bt * sh.Q[ds.n - 1 + lane * kBLd];
+        __syncwarp();
+      }
+      ds.k = ds.n;
+      ds.state = 2;
+      __syncthreads();
+      int kk = nconv;
+      for (; kk < nv; ++kk) {
+        const double re = sh.wr[kk];
+        const double resnorm = fabs(sh.Q[ds.n - 1 + kk * kBLd]) * beta;
+        const double wabs = fabs(re);
+        const double est = (wabs != 0.0) ? resnorm / wabs : 1.7976931348623157e308;
+        if (threadIdx.x == 0) {
+          sh.eigr[kk] = re;
+          sh.errest[kk] = est;
+        }
+        if (est >= prm.tol) break;
+      }
+      const int k = kk;
+      if (k >= nev) reason = B200_CONVERGED_TOL;
+      else if (its >= max_it) reason = B200_DIVERGED_ITS;
+      int lnew;
+      if (reason != 0 || breakdown || k == nv) lnew = 0;
+      else {
+        lnew = (int)((nv - k) * prm.keep);
+        if (lnew < 1) lnew = 1;
+      }
+      __syncthreads();
+      if (reason == 0) {
+        if (breakdown || k == nv) {
+          if (k < nev) {
+            cta_random<T>(w, n, prm.seed, nrand++);
+            double nrm;
+            int lindep;
+            cta_orth32<T>(V, ld, n, k, w, prm.eta, h, &nrm, &lindep, &err, sh);
+            if (lindep) reason = B200_DIVERGED_BREAKDOWN;
+          }
+        } else {
+          ds.k = k + lnew;
+          ds.t = ds.n;
+          ds.n = k + lnew;
+          ds.state = 3;
+        }
+      }
+      {
+        const int s = nconv, e = k + lnew;
+        if (e > s) {
+          cta_multinplace32<T>(V, ld, n, nconv, nv, sh.Q, s, e);
+          if (threadIdx.x == 0) sh.bytes += 4ull * n * ((nv - nconv) + (e - s));
+        }
+      }
+      if (reason == 0 && !breakdown) {
+        const float *src = V + (size_t)nv * ld;
+        float *dst = V + (size_t)(k + lnew) * ld;
+        for (int r = threadIdx.x; r < n; r += T) dst[r] = __ldcg(src + r);
+        __syncthreads();
+      }
+      nconv = k;
+      l = lnew;
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      int pm[kBLd];
+      for (int i = 0; i < ncv; ++i) pm[i] = i;
+      for (int i = nconv - 1; i >= 0; --i) {
+        const double re = sh.eigr[pm[i]];
+        int j = i + 1;
+        while (j < nconv) {
+          if (bcompare(prm.which, re, sh.eigr[pm[j]]) <= 0) break;
+          const int tmp = pm[j - 1];
+          pm[j - 1] = pm[j];
+          pm[j] = tmp;
+          ++j;
+        }
+      }
+      for (int i = 0; i < ncv; ++i) {
+        evals[(size_t)pidx * ncv + i] = i < nconv ? sh.eigr[pm[i]] : 0.0;
+        errest_out[(size_t)pidx * ncv + i] = i < nconv ? sh.errest[pm[i]] : 0.0;
+        vcol[(size_t)pidx * ncv + i] = i < nconv ? pm[i] : -1;
+      }
+      int *inf = info + (size_t)pidx * 8;
+      inf[0] = nconv;
+      inf[1] = its;
+      inf[2] = reason;
+      inf[3] = (int)steps;
+      inf[4] = err;
+      inf[5] = nini;
+      bytes_out[pidx] = (double)sh.bytes;
+    }
+    __syncthreads();
+  }
+}
+
+// The start vector of phase 2 for every problem: the sum of its (up to nev) phase-1 Ritz vectors
+// in FP64, or its original start vector when phase 1 converged none; phase 1's counters are kept.
+__global__ void batched_phase2_start_kernel(int nprob, const BProblem *__restrict__ probs, int nev, int ncv,
+                                            const float *__restrict__ V32, const int *__restrict__ vcol,
+                                            const int *__restrict__ info, const double *__restrict__ bytes,
+                                            const double *__restrict__ v0, double *__restrict__ v0_next,
+                                            int *__restrict__ info1, double *__restrict__ bytes1) {
+  for (int p = blockIdx.x; p < nprob; p += gridDim.x) {
+    const BProblem P = probs[p];
+    const int nconv = min(info[(size_t)p * 8], nev);
+    const float *V = V32 + P.v_off;
+    for (int r = threadIdx.x; r < P.n; r += blockDim.x) {
+      double s = 0.0;
+      for (int i = 0; i < nconv; ++i) s += (double)V[r + (size_t)vcol[(size_t)p * ncv + i] * P.ld];
+      v0_next[P.x_off + r] = nconv > 0 ? s : v0[P.x_off + r];
+    }
+    if (threadIdx.x < 8) info1[(size_t)p * 8 + threadIdx.x] = info[(size_t)p * 8 + threadIdx.x];
+    if (threadIdx.x == 0) bytes1[p] = bytes[p];
+  }
+}
+
 }  // namespace
 }  // namespace b200
 
@@ -667,13 +1007,26 @@ struct b200_batch_s {
   b200::BParams graph_prm{};
   int alloc_ncv = 0;
   float last_ms = 0.0f;
+  // mixed precision: phase 1 on an FP32 basis to tol_low, phase 2 in FP64 from the phase-1 Ritz vectors
+  int precision = B200_PRECISION_FP64;
+  double tol_low = 1e-6;
+  float *V32 = nullptr;      // FP32 bases (same offsets as V)
+  double *W = nullptr;       // FP64 work vector per problem (row offsets)
+  double *v0_2 = nullptr;    // phase-2 start vectors
+  int *info1 = nullptr;      // phase-1 counters (nprob x 8)
+  double *bytes1 = nullptr;  // phase-1 algorithmic bytes per problem
+  std::vector<int> h_info1;
+  std::vector<double> h_bytes1;
+  int graph_precision = -1;
+  double graph_tol_low = 0.0;
 };
 
 namespace b200 {
 namespace {
 
 template <int T>
-cudaError_t launch_batched(b200_batch B, const b200::BParams &prm, int nprob, cudaStream_t s, bool count) {
+cudaError_t launch_batched(b200_batch B, const b200::BParams &prm, int nprob, cudaStream_t s, bool count,
+                           const double *v0 = nullptr) {
   int sms = num_sms_host(), per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_ks_kernel<T>, T, 0);
   if (per_sm < 1) per_sm = 1;
@@ -685,10 +1038,44 @@ cudaError_t launch_batched(b200_batch B, const b200::BParams &prm, int nprob, cu
   e = cudaMemsetAsync(B->info, 0xff, sizeof(int) * 8 * (size_t)B->nprob, s);
   if (e != cudaSuccess) return e;
   batched_ks_kernel<T><<<grid, T, 0, s>>>(nprob, B->probs, B->order, B->next, B->rowptr, B->colind, B->vals,
-                                          B->tiles, B->v0, B->V, prm, B->evals, B->errest, B->vcol, B->info,
-                                          B->bytes);
+                                          B->tiles, v0 ? v0 : B->v0, B->V, prm, B->evals, B->errest, B->vcol,
+                                          B->info, B->bytes);
   if (count) count_launch();
   return cudaGetLastError();
+}
+
+// The mixed form: phase 1 (FP32 basis, tolerance tol_low), the phase-2 start vectors, phase 2 (FP64).
+template <int T>
+cudaError_t launch_mixed(b200_batch B, const b200::BParams &prm, cudaStream_t s, bool count) {
+  int sms = num_sms_host(), per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_ks32_kernel<T>, T, 0);
+  if (per_sm < 1) per_sm = 1;
+  int grid = sms * per_sm;
+  if (grid > B->nprob) grid = B->nprob;
+  cudaError_t e = cudaMemsetAsync(B->next, 0, sizeof(int), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(B->info, 0xff, sizeof(int) * 8 * (size_t)B->nprob, s);
+  if (e != cudaSuccess) return e;
+  b200::BParams p1 = prm;
+  p1.tol = B->tol_low > prm.tol ? B->tol_low : prm.tol;
+  batched_ks32_kernel<T><<<grid, T, 0, s>>>(B->nprob, B->probs, B->order, B->next, B->rowptr, B->colind, B->vals,
+                                            B->tiles, B->v0, B->V32, B->W, p1, B->evals, B->errest, B->vcol,
+                                            B->info, B->bytes);
+  if (count) count_launch();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const int g2 = B->nprob < sms * 8 ? B->nprob : sms * 8;
+  batched_phase2_start_kernel<<<g2, 256, 0, s>>>(B->nprob, B->probs, prm.nev, prm.ncv, B->V32, B->vcol, B->info,
+                                                 B->bytes, B->v0, B->v0_2, B->info1, B->bytes1);
+  if (count) count_launch();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return launch_batched<T>(B, prm, B->nprob, s, count, B->v0_2);
+}
+
+cudaError_t launch_mixed_any(b200_batch B, int threads, const b200::BParams &prm, cudaStream_t s, bool count) {
+  switch (threads) {
+    case 128: return launch_mixed<128>(B, prm, s, count);
+    case 256: return launch_mixed<256>(B, prm, s, count);
+    default: return launch_mixed<512>(B, prm, s, count);
+  }
 }
 
 cudaError_t launch_any(b200_batch B, int threads, const b200::BParams &prm, int nprob, cudaStream_t s, bool count) {
@@ -821,7 +1208,20 @@ extern "C" b200_status b200_batch_destroy(b200_batch B) {
   cudaFree(B->vcol);
   cudaFree(B->info);
   cudaFree(B->bytes);
+  cudaFree(B->V32);
+  cudaFree(B->W);
+  cudaFree(B->v0_2);
+  cudaFree(B->info1);
+  cudaFree(B->bytes1);
   delete B;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_batch_set_precision(b200_batch B, int precision, double tol_low) {
+  B200_ARG_CHECK(B && (precision == B200_PRECISION_FP64 || precision == B200_PRECISION_MIXED), "unknown precision");
+  B->precision = precision;
+  B->tol_low = tol_low > 0.0 ? tol_low : 1e-6;
+  B->solved = false;
   return B200_OK;
 }
 
@@ -867,9 +1267,21 @@ extern "C" b200_status b200_batch_set_threads(b200_batch B, int threads) {
   return B200_OK;
 }
 
+static b200_status batch_alloc_mixed(b200_batch B) {
+  if (B->precision != B200_PRECISION_MIXED || B->V32) return B200_OK;
+  B200_CUDA_CHECK(cudaMalloc(&B->V32, sizeof(float) * (B->v_total ? B->v_total : 1)));
+  B200_CUDA_CHECK(cudaMalloc(&B->W, sizeof(double) * B->total_rows));
+  B200_CUDA_CHECK(cudaMalloc(&B->v0_2, sizeof(double) * B->total_rows));
+  B200_CUDA_CHECK(cudaMalloc(&B->info1, sizeof(int) * 8 * (size_t)B->nprob));
+  B200_CUDA_CHECK(cudaMalloc(&B->bytes1, sizeof(double) * B->nprob));
+  return B200_OK;
+}
+
 static b200_status batch_alloc(b200_batch B) {
   if (B->ncv == 0) B200_CHECK(b200_batch_set_dimensions(B, B->nev, 0, 0));
-  if (B->V && B->alloc_ncv == B->ncv) return B200_OK;
+  if (B->V && B->alloc_ncv == B->ncv) return batch_alloc_mixed(B);
+  cudaFree(B->V32);  // sized with the bases
+  B->V32 = nullptr;
   if (B->exec) cudaGraphExecDestroy(B->exec);
   if (B->graph) cudaGraphDestroy(B->graph);
   B->exec = nullptr;
@@ -896,7 +1308,7 @@ static b200_status batch_alloc(b200_batch B) {
                                   cudaMemcpyHostToDevice, B->stream));
   B200_CUDA_CHECK(cudaStreamSynchronize(B->stream));
   B->alloc_ncv = B->ncv;
-  return B200_OK;
+  return batch_alloc_mixed(B);
 }
 
 // Project-written autotuner: each candidate CTA size solves the largest problems of the batch
@@ -949,7 +1361,9 @@ extern "C" b200_status b200_batch_solve(b200_batch B) {
   const b200::BParams prm = batch_params(B);
   // one persistent launch (counter reset + kernel), captured once in a CUDA graph and replayed
   // while the launch shape, the parameters and the buffers stay the same
-  if (!B->exec || B->graph_threads != B->threads || memcmp(&B->graph_prm, &prm, sizeof(prm)) != 0) {
+  const bool mixed = B->precision == B200_PRECISION_MIXED;
+  if (!B->exec || B->graph_threads != B->threads || memcmp(&B->graph_prm, &prm, sizeof(prm)) != 0 ||
+      B->graph_precision != B->precision || B->graph_tol_low != B->tol_low) {
     if (B->exec) cudaGraphExecDestroy(B->exec);
     if (B->graph) cudaGraphDestroy(B->graph);
     B->exec = nullptr;
@@ -957,7 +1371,8 @@ extern "C" b200_status b200_batch_solve(b200_batch B) {
     cudaStream_t cap = nullptr;
     B200_CUDA_CHECK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     B200_CUDA_CHECK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = launch_any(B, B->threads, prm, B->nprob, cap, false);  // counted at each replay
+    cudaError_t e = mixed ? launch_mixed_any(B, B->threads, prm, cap, false)  // counted at each replay
+                          : launch_any(B, B->threads, prm, B->nprob, cap, false);
     cudaGraph_t g = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(cap, &g);
     cudaStreamDestroy(cap);
@@ -967,13 +1382,19 @@ extern "C" b200_status b200_batch_solve(b200_batch B) {
     B200_CUDA_CHECK(cudaGraphInstantiate(&B->exec, g, 0));
     B->graph_threads = B->threads;
     B->graph_prm = prm;
+    B->graph_precision = B->precision;
+    B->graph_tol_low = B->tol_low;
   }
   cudaEvent_t e0, e1;
   B200_CUDA_CHECK(cudaEventCreate(&e0));
   B200_CUDA_CHECK(cudaEventCreate(&e1));
   B200_CUDA_CHECK(cudaEventRecord(e0, B->stream));
   B200_CUDA_CHECK(cudaGraphLaunch(B->exec, B->stream));
-  count_launch();  // the graph holds one kernel
+  count_launch();  // the graph holds one kernel (three in the mixed form)
+  if (mixed) {
+    count_launch();
+    count_launch();
+  }
   B200_CUDA_CHECK(cudaEventRecord(e1, B->stream));
   B200_CUDA_CHECK(cudaEventSynchronize(e1));
   cudaEventElapsedTime(&B->last_ms, e0, e1);
@@ -994,6 +1415,17 @@ extern "C" b200_status b200_batch_solve(b200_batch B) {
   B->h_bytes.resize(B->nprob);
   B200_CUDA_CHECK(cudaMemcpyAsync(B->h_bytes.data(), B->bytes, sizeof(double) * B->nprob, cudaMemcpyDeviceToHost,
                                   B->stream));
+  if (mixed) {
+    B->h_info1.resize((size_t)B->nprob * 8);
+    B->h_bytes1.resize(B->nprob);
+    B200_CUDA_CHECK(cudaMemcpyAsync(B->h_info1.data(), B->info1, sizeof(int) * B->h_info1.size(),
+                                    cudaMemcpyDeviceToHost, B->stream));
+    B200_CUDA_CHECK(cudaMemcpyAsync(B->h_bytes1.data(), B->bytes1, sizeof(double) * B->nprob, cudaMemcpyDeviceToHost,
+                                    B->stream));
+  } else {
+    B->h_info1.clear();
+    B->h_bytes1.clear();
+  }
   B200_CUDA_CHECK(cudaStreamSynchronize(B->stream));
   B->solved = true;
   for (int p = 0; p < B->nprob; ++p) {
@@ -1065,6 +1497,22 @@ extern "C" b200_status b200_batch_get_bytes(b200_batch B, double *bytes) {
   }
   double t = 0.0;
   for (double b : B->h_bytes) t += b;
+  for (double b : B->h_bytes1) t += b;  // phase 1 of the mixed form
   *bytes = t;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_batch_get_phase1(b200_batch B, int *info_host, double *bytes) {
+  B200_ARG_CHECK(B, "null argument");
+  if (!B->solved || B->h_info1.empty()) {
+    b200_set_last_error(__FILE__, __LINE__, "no mixed-precision solve has run");
+    return B200_ERR_STATE;
+  }
+  if (info_host) memcpy(info_host, B->h_info1.data(), sizeof(int) * B->h_info1.size());
+  if (bytes) {
+    double t = 0.0;
+    for (double b : B->h_bytes1) t += b;
+    *bytes = t;
+  }
   return B200_OK;
 }

@@ -92,3 +92,37 @@ def test_batched_autotune_and_arguments():
         E.setDimensions(8, 40)  # ncv + 1 > 32
     with pytest.raises(S.B200Error):
         E.setThreads(100)
+
+
+@pytest.mark.parametrize("threads", [256, 512])
+def test_batched_mixed_precision_vs_oracle(oracle_mod, threads):
+    """The mixed form: phase 1 on FP32 bases to 1e-6, phase 2 in FP64 from the phase-1 Ritz vectors.
+    Eigenvalues equal the FP64 oracle's to 1e-10, residuals in FP64 below the tolerance, both phases
+    report their counters."""
+    B, v0 = _batch(48, 3, 500, 3000)
+    E = S.BatchEPS().create(B.ns, B.rowptr, B.colind, B.vals)
+    E.setDimensions(8, 24)
+    E.setTolerances(1e-8)
+    E.setWhichEigenpairs(S.LARGEST_REAL)
+    E.setInitialVectors(v0)
+    E.setThreads(threads)
+    E.setPrecision(S.EPS.Precision.MIXED, 1e-6)
+    E.solve()
+    ev, info, ms = E.getAll()
+    info1, bytes1 = E.getPhase1()
+    oev, oinfo = oracle_mod.eps_solve_batch(B.ns, B.rowptr, B.colind, B.vals, v0, 8, 24, 1e-8,
+                                            oracle_mod.LARGEST_REAL, threads=8)
+    assert ms > 0 and 0 < bytes1 < E.getBytes()
+    for p in range(B.nprob):
+        assert info[p, 2] == S.CONVERGED_TOL and info[p, 4] == 0 and info1[p, 4] == 0
+        assert info1[p, 0] >= 8 and info[p, 0] >= 8
+        np.testing.assert_allclose(ev[p, :8], oev[p, :8], rtol=1e-10)
+    assert info1[:, 3].sum() > 0 and info[:, 3].sum() > 0
+    for p in (0, 11, 40):
+        As = P.to_scipy(B.problem(p))
+        sol = E.getSolution(p)
+        for i in range(8):
+            x = E.getEigenvector(p, i)
+            r = np.linalg.norm(As @ x - sol["evals"][i] * x) / abs(sol["evals"][i])
+            assert r < 2e-8, (p, i, r)
+    E.destroy()

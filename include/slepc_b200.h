@@ -279,7 +279,7 @@ b200_status b200_eps_set_max_restarts(b200_eps eps, int max_restarts);
 b200_status b200_eps_set_precision(b200_eps eps, int precision);
 /* Mixed-form parameters (0 or a negative value keeps the default): tol_low,
  * the phase-1 tolerance (default 1e-6, never below tol); degree, the
- * Chebyshev filter degree per sweep (default 64; a sweep uses less when the
+ * Chebyshev filter degree per sweep (default 128; a sweep uses less when the
  * amplification of the leading Ritz value would exceed 1e6, which keeps the
  * block well conditioned for its Cholesky QR); guard, columns of the
  * refinement block beyond nev (default max(8, nev/2)); max_sweeps (default
@@ -289,6 +289,12 @@ b200_status b200_eps_set_precision(b200_eps eps, int precision);
  * FP64 arithmetic on the FP32 basis. */
 b200_status b200_eps_set_mixed_options(b200_eps eps, double tol_low, int degree, int guard, int max_sweeps,
                                        int fp32_first_pass);
+/* DGKS threshold eta of the FP32-basis phase (BVSetOrthogonalization's eta, bvorthog.c:176-187):
+ * a second Gram-Schmidt pass only when the norm drops below eta times the norm before the pass.
+ * 0 (default) takes one pass per column: two reads of the FP32 basis instead of three, with the
+ * same phase-1 restart count on the 3-D Laplacian; the FP64 refinement phase supplies the
+ * accuracy.  A negative value keeps the BV's 0.7071 ("if needed" refinement). */
+b200_status b200_eps_set_mixed_eta(b200_eps eps, double eta);
 
 /* EPSSetType: B200_EPS_KRYLOVSCHUR (default) or B200_EPS_LOBPCG. */
 #define B200_EPS_KRYLOVSCHUR 0

@@ -76,6 +76,7 @@ _SIGS = {
     "b200_mat_norm_inf": (ctypes.c_int, [_vp, _dp]),
     "b200_eps_set_type": (ctypes.c_int, [_vp, ctypes.c_int]),
     "b200_eps_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_eps_set_mixed_eta": (ctypes.c_int, [_vp, ctypes.c_double]),
     "b200_eps_set_mixed_options": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                   ctypes.c_int]),
     "b200_eps_lobpcg_set_block_size": (ctypes.c_int, [_vp, ctypes.c_int]),
@@ -622,6 +623,10 @@ class EPS:
         on an FP32 basis with FP32 matrix values to a loose tolerance, then FP64
         Chebyshev-filtered Rayleigh-Ritz refinement of the block of leading Ritz vectors."""
         _check(lib().b200_eps_set_precision(self.handle, precision))
+
+    def setMixedEta(self, eta):
+        """DGKS threshold of the FP32-basis phase (0, the default: one pass per column; negative: 0.7071)."""
+        _check(lib().b200_eps_set_mixed_eta(self.handle, eta))
 
     def setMixedOptions(self, tol_low=0.0, degree=0, guard=-1, max_sweeps=0, fp32_first_pass=False):
         """Parameters of the mixed form; 0 (or -1 for guard) keeps the default."""

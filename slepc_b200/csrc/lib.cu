@@ -1242,6 +1242,12 @@ extern "C" b200_status b200_eps_set_precision(b200_eps eps, int precision) {
   return B200_OK;
 }
 
+extern "C" b200_status b200_eps_set_mixed_eta(b200_eps eps, double eta) {
+  B200_ARG_CHECK(eps && eta <= 1.0, "eta must be at most 1");
+  eps->mixed_eta1 = eta;
+  return B200_OK;
+}
+
 extern "C" b200_status b200_eps_set_mixed_options(b200_eps eps, double tol_low, int degree, int guard,
                                                   int max_sweeps, int fp32_first_pass) {
   B200_ARG_CHECK(eps, "null argument");

@@ -50,7 +50,7 @@ using namespace b200;
 namespace {
 
 constexpr double kDefaultTolLow = 1e-6;
-constexpr int kDefaultDegree = 64;
+constexpr int kDefaultDegree = 128;
 constexpr int kDefaultMaxSweeps = 40;
 constexpr int kMaxBlock = 128;  // columns of the refinement block (row-panel GEMM limit)
 constexpr int kBlocks = 5;      // FP64 blocks of the refinement phase
@@ -141,7 +141,7 @@ struct Mixed {
         ev.push_back(e);
       }
     const bool have_ev = timing && ev.size() >= (size_t)3 * (m0 - k);
-    B200_CUDA_CHECK(gs_state_reset(V->gs, V->eta, s));
+    B200_CUDA_CHECK(gs_state_reset(V->gs, eps->mixed_eta1 >= 0.0 ? eps->mixed_eta1 : V->eta, s));
     for (int j = k; j < m0; ++j) {
       const size_t e = (size_t)3 * (j - k);
       if (have_ev) cudaEventRecord(ev[e], s);
@@ -349,7 +349,7 @@ b200_status b200::mixed_solve(b200_eps eps) {
   int lwork = 1 + 6 * kb + 2 * kb * kb, liwork = 3 + 5 * kb;
   std::vector<double> lw((size_t)lwork);
   std::vector<int> liw((size_t)liwork);
-  int sweeps = 0, done_conv = 0, used_degree = 0;
+  int sweeps = 0, done_conv = 0, used_degree = 0, nlock = 0;
   const int wl = (int)std::min(work_len, (size_t)1 << 30);
   while (sweeps < max_sweeps) {
     ++sweeps;
@@ -379,14 +379,19 @@ b200_status b200::mixed_solve(b200_eps eps) {
       if (cap < d) d = std::max(2, (int)cap);
     }
     used_degree = std::max(used_degree, d);
-    if (e > 0.0 && best != c && std::isfinite(e) && d > 0) {
+    // soft locking: the leading pairs that have converged keep their vectors; only columns
+    // nlock..kb-1 are filtered (CholQR2 and Rayleigh-Ritz still take the whole block)
+    const int a0 = nlock, na = kb - nlock;
+    if (e > 0.0 && best != c && std::isfinite(e) && d > 0 && na > 0) {
       const double sigma1 = e / (best - c);
+      const size_t off = (size_t)a0 * ldb;
       int prev = x, cur = (x + 1) % kBlocks, nxt = (x + 2) % kBlocks;
-      B200_CUDA_CHECK(mat_spmm(eps->A, B[prev], nullptr, B[cur], ldb, kb, sigma1 / e, c, 0.0, s));
+      B200_CUDA_CHECK(mat_spmm(eps->A, B[prev] + off, nullptr, B[cur] + off, ldb, na, sigma1 / e, c, 0.0, s));
       double sigma = sigma1;
       for (int i = 2; i <= d; ++i) {
         const double sn = 1.0 / (2.0 / sigma1 - sigma);
-        B200_CUDA_CHECK(mat_spmm(eps->A, B[cur], B[prev], B[nxt], ldb, kb, 2.0 * sn / e, c, sigma * sn, s));
+        B200_CUDA_CHECK(
+            mat_spmm(eps->A, B[cur] + off, B[prev] + off, B[nxt] + off, ldb, na, 2.0 * sn / e, c, sigma * sn, s));
         const int t = prev;
         prev = cur;
         cur = nxt;
@@ -394,7 +399,10 @@ b200_status b200::mixed_solve(b200_eps eps) {
         sigma = sn;
       }
       f = cur;
-      eps->stats.spmm_columns += (int64_t)kb * d;
+      if (f != x && a0 > 0)
+        B200_CUDA_CHECK(cudaMemcpy2DAsync(B[f], sizeof(double) * ldb, B[x], sizeof(double) * ldb, sizeof(double) * n,
+                                          a0, cudaMemcpyDeviceToDevice, s));
+      eps->stats.spmm_columns += (int64_t)na * d;
     }
     auto free_block = [&](std::initializer_list<int> used) {
       for (int i = 0; i < kBlocks; ++i)
@@ -478,6 +486,7 @@ b200_status b200::mixed_solve(b200_eps eps) {
     }
     while (done_conv < kb && rel[done_conv] < tol) ++done_conv;  // EPSConvergedRelative, leading pairs
     if (done_conv >= nev) break;
+    nlock = done_conv;
   }
   eps->stats.filter_sweeps = sweeps;
   eps->stats.filter_degree = used_degree;  // the largest degree a sweep used

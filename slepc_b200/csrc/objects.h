@@ -114,6 +114,7 @@ struct b200_eps_s {
   int mixed_guard = -1;        // guard columns of the refinement block (-1: default)
   int mixed_max_sweeps = 0;    // refinement sweeps (0: default)
   int mixed_fp32_pass = 0;     // first Gram-Schmidt pass in FP32 arithmetic
+  double mixed_eta1 = 0.0;     // DGKS threshold of the FP32-basis phase (0: one pass; < 0: the BV's 0.7071)
   float *V32 = nullptr;        // FP32 basis, ld32 x (ncv + 1)
   size_t V32_cap = 0;
   int ld32 = 0;

@@ -41,6 +41,7 @@ typedef int b200_status;
 #define B200_ERR_DEVICE 8     /* a kernel reported a device-side error (bounded wait expired, NaN) */
 #define B200_ERR_FP 9         /* floating-point failure (PETSC_ERR_FP: negative eigenvalue of A^T A) */
 #define B200_ERR_IO 10        /* file read/write failure or malformed binary file (PETSC_ERR_FILE_READ / _UNEXPECTED) */
+#define B200_ERR_SUP 11       /* an option this implementation does not provide (PETSC_ERR_SUP) */
 
 /* Which eigenpairs (EPSWhich, include/slepceps.h; comparators src/sys/slepcsc.c:152-210). */
 #define B200_LARGEST_MAGNITUDE 1
@@ -164,6 +165,16 @@ b200_status b200_bv_set_active_columns(b200_bv bv, int l, int k);
 b200_status b200_bv_get_active_columns(b200_bv bv, int *l, int *k);
 /* BVSetOrthogonalization eta (bvfunc.c:178 default 0.7071); CGS with refinement if needed. */
 b200_status b200_bv_set_orthog_eta(b200_bv bv, double eta);
+/* BVSetOrthogonalization / BVGetOrthogonalization block type (BVOrthogBlockType,
+ * include/slepcbv.h:84-88; bvbasic.c:975-987; default GS, bvfunc.c:179): the
+ * method of b200_bv_orthogonalize.  TSQR and TSQRCHOL return B200_ERR_SUP. */
+#define B200_ORTHOG_BLOCK_GS 0
+#define B200_ORTHOG_BLOCK_CHOL 1
+#define B200_ORTHOG_BLOCK_TSQR 2
+#define B200_ORTHOG_BLOCK_TSQRCHOL 3
+#define B200_ORTHOG_BLOCK_SVQB 4
+b200_status b200_bv_set_orthog_block(b200_bv bv, int type);
+b200_status b200_bv_get_orthog_block(b200_bv bv, int *type);
 /* Copy a column from/to host memory (BVGetColumn + VecGetArray / VecSetValues). */
 b200_status b200_bv_set_column(b200_bv bv, int j, const double *x_host);
 b200_status b200_bv_get_column(b200_bv bv, int j, double *x_host);
@@ -199,8 +210,13 @@ b200_status b200_bv_orthogonalize_vec(b200_bv bv, double *v_dev, double *H_host,
  * serialised by the caller. */
 b200_status b200_orthogonalize_column_noalloc(int n, int ld, int ncols, double *V_dev, int j, double *H_dev,
                                               double *norm, int *lindep, void *stream);
-/* BVOrthogonalize with BV_ORTHOG_BLOCK_GS (bvorthog.c:505-560, :726-767):
- * columns l..k-1 one by one; R_host (nullable, ldr >= k) receives R. */
+/* BVOrthogonalize (bvorthog.c:726-767) of columns l..k-1 with the BV's block
+ * type: GS column by column (BVOrthogonalize_GS, :505-560); CHOL (:595-613) and
+ * SVQB (:665-684) one Gram-Schmidt pass against columns 0..l-1, the Gram
+ * matrix of the block on the device and its Cholesky factor or scaled
+ * eigendecomposition on the host, then one in-place product.  R_host
+ * (nullable, ldr >= k) receives R with V_in = V_out R (upper triangular
+ * except for SVQB). */
 b200_status b200_bv_orthogonalize(b200_bv bv, double *R_host, int ldr);
 
 /* BVMultInPlace (bvops.c:220-245; BVMultInPlace_BLAS_CUDA bvcuda.cu:65-112):
@@ -310,6 +326,11 @@ b200_status b200_eps_lobpcg_set_locking(b200_eps eps, int lock);
 #define B200_PC_NONE 0
 #define B200_PC_JACOBI 1
 b200_status b200_eps_set_preconditioner(b200_eps eps, int pc);
+/* BVSetOrthogonalization block type of the eigensolver's basis (-bv_orthog_block),
+ * which LOBPCG's X, R and P blocks inherit (lobpcg.c:256, :331, :334 call
+ * BVOrthogonalize on them).  Krylov-Schur orthogonalises column by column and
+ * does not use it. */
+b200_status b200_eps_set_bv_orthog_block(b200_eps eps, int type);
 /* EPSSetInitialSpace with k vectors (host, n x k column-major): inserted and
  * orthonormalised as BVInsertVecs does, linearly dependent ones dropped
  * (src/sys/classes/bv/interface/bvfunc.c:331-374).  Krylov-Schur starts from

@@ -13,6 +13,7 @@ import numpy as np
 from . import build as _build
 
 LARGEST_MAGNITUDE, SMALLEST_MAGNITUDE, LARGEST_REAL, SMALLEST_REAL = 1, 2, 3, 4
+ORTHOG_BLOCK_GS, ORTHOG_BLOCK_CHOL, ORTHOG_BLOCK_SVQB = 0, 1, 4  # BVOrthogBlockType
 CONVERGED_TOL, DIVERGED_ITS, DIVERGED_BREAKDOWN, ITERATING = 1, -1, -2, 0
 
 _lib = None
@@ -44,7 +45,10 @@ def lib():
         L.oracle_lobpcg.restype = ctypes.c_int
         L.oracle_lobpcg.argtypes = [ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-                                    ctypes.c_double, _dp, ctypes.c_int, _dp, _dp, _dp, _ip]
+                                    ctypes.c_double, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, _ip]
+        L.oracle_bv_orthogonalize_block.restype = ctypes.c_int
+        L.oracle_bv_orthogonalize_block.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_int, _dp, ctypes.c_int]
         L.oracle_eps_solve_batch.restype = ctypes.c_int
         L.oracle_eps_solve_batch.argtypes = [ctypes.c_int, _ip, _ip, _ip, _dp, _dp, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_double, ctypes.c_int, _dp, _ip]
@@ -137,6 +141,18 @@ def bv_orthogonalize_vec(V, k, v):
     return v, H[:k], nrm.value, bool(lnd.value)
 
 
+def bv_orthogonalize_block(V, l, k, block_type):
+    """BVOrthogonalize of columns [l,k) of a Fortran-ordered n x m array (in place) with block
+    type ORTHOG_BLOCK_CHOL or ORTHOG_BLOCK_SVQB; returns R (k x k) with V_in = V_out R on [0,k)."""
+    assert V.flags.f_contiguous and V.dtype == np.float64
+    n = V.shape[0]
+    R = np.zeros((k, k), order="F")
+    st = lib().oracle_bv_orthogonalize_block(n, n, _d(V), l, k, block_type, _d(R), k)
+    if st:
+        raise RuntimeError(f"orthogonalize block failed {st}")
+    return R
+
+
 def bv_multinplace(V, l, k, Q, s, e):
     assert V.flags.f_contiguous and Q.flags.f_contiguous
     n = V.shape[0]
@@ -222,8 +238,9 @@ def svd_cross(rowptr, colind, vals, shape, v0, nsv, ncv, tol=0.0, largest=True, 
 
 
 def lobpcg(A, nev, bs=0, ncv=0, tol=1e-8, max_it=0, which=SMALLEST_REAL, pc="jacobi", lock=True, restart=0.9,
-           X0=None):
-    """EPSSolve with EPSLOBPCG on a symmetric scipy CSR matrix; X0 (n x k) an initial space."""
+           X0=None, orthog_block=ORTHOG_BLOCK_GS):
+    """EPSSolve with EPSLOBPCG on a symmetric scipy CSR matrix; X0 (n x k) an initial space;
+    orthog_block the BVOrthogBlockType of the blocks (ORTHOG_BLOCK_GS, _CHOL or _SVQB)."""
     n = A.shape[0]
     rowptr, colind, vals = _csr(A)
     cap = max(ncv, 3 * max(bs, min(16, nev)), ((nev - 1) // max(bs or min(16, nev), 1) + 3) * max(bs or min(16, nev), 1)) + 48
@@ -238,7 +255,8 @@ def lobpcg(A, nev, bs=0, ncv=0, tol=1e-8, max_it=0, which=SMALLEST_REAL, pc="jac
         nini = X0.shape[1]
         x0p = _d(X0)
     st = lib().oracle_lobpcg(n, _i(rowptr), _i(colind), _d(vals), nev, bs, ncv, tol, max_it, which,
-                             {"none": 0, "jacobi": 1}[pc], 1 if lock else 0, restart, x0p, nini, _d(evals), _d(X),
+                             {"none": 0, "jacobi": 1}[pc], 1 if lock else 0, restart, orthog_block, x0p, nini,
+                             _d(evals), _d(X),
                              _d(errest), _i(info))
     if st:
         raise RuntimeError(f"oracle_lobpcg failed with status {st}")

@@ -998,17 +998,129 @@ static void blk_multinplace(oblk *V, const double *Q, int ldq, int s, int e)
   free(work);
 }
 
-/* BVOrthogonalize with BV_ORTHOG_BLOCK_GS */
-static int blk_orthogonalize(oblk *B)
+/* BVOrthogBlockType (slepcbv.h:84-88) */
+#define ORC_BLOCK_GS 0
+#define ORC_BLOCK_CHOL 1
+#define ORC_BLOCK_SVQB 4
+
+extern void scipy_dpotrf_(const char *, const int *, double *, const int *, int *, size_t);
+extern void scipy_dtrtri_(const char *, const char *, const int *, double *, const int *, int *, size_t, size_t);
+extern void scipy_dsyev_(const char *, const char *, const int *, double *, const int *, double *, double *,
+                         const int *, int *, size_t, size_t);
+
+/* The Gram-matrix block orthogonalizations of the active columns [l,k):
+ *   BVOrthogonalize_Chol (bvorthog.c:595-613): BVOrthogonalize_BlockGS against
+ *   the leading columns (:492-501, V2 -= V1 (V1' V2), one pass), G = V2' V2,
+ *   BVMatCholInv_LAPACK_Private (bvlapack.c:136-213: dpotrf "U", on failure
+ *   once more with 50 eps added to the diagonal, then dtrtri "U" "N"),
+ *   BVMultInPlace(V, inv(R), l, k);
+ *   BVOrthogonalize_SVQB (bvorthog.c:665-684): BlockGS, G = V2' V2,
+ *   BVMatSVQB_LAPACK_Private (bvlapack.c:261-340: D = diag(G)^{-1/2}, dsyev
+ *   "V" "L" of D G D = U Lambda U', S = D U Lambda^{-1/2}), BVMultInPlace(V, S).
+ * R (nullable, ldr >= k): R(0:l, l:k) = V1' V2 and R(l:k, l:k) = the Cholesky
+ * factor (upper triangular) or Lambda^{1/2} U' D^{-1} (SVQB), so that
+ * V_in = V_out R.  A zero column or a non-positive eigenvalue of the SVQB Gram
+ * matrix (a numerically rank-deficient block) is reported as ORC_ERR_BREAKDOWN. */
+static int blk_orthogonalize_gram(oblk *B, int type, double *Rout, int ldr)
+{
+  const int l = B->l, nc = B->k - B->l, n = B->b.n, ld = B->b.ld;
+  const double one = 1.0, zero = 0.0, mone = -1.0;
+  int info = 0, st = ORC_OK, i, j;
+  if (nc <= 0) return ORC_OK;
+  double *C = NULL, *G = (double *)malloc(sizeof(double) * (size_t)nc * nc);
+  double *S = (double *)calloc((size_t)nc * nc, sizeof(double));
+  double *Rf = (double *)calloc((size_t)nc * nc, sizeof(double));
+  double *work = NULL, *eig = NULL, *D = NULL;
+  if (l > 0) {
+    C = (double *)malloc(sizeof(double) * (size_t)l * nc);
+    scipy_dgemm_("T", "N", &l, &nc, &n, &one, B->b.V, &ld, BCOL(B, l), &ld, &zero, C, &l, 1, 1);
+    scipy_dgemm_("N", "N", &n, &nc, &l, &mone, B->b.V, &ld, C, &l, &one, BCOL(B, l), &ld, 1, 1);
+  }
+  scipy_dgemm_("T", "N", &nc, &nc, &n, &one, BCOL(B, l), &ld, BCOL(B, l), &ld, &zero, G, &nc, 1, 1);
+  if (type == ORC_BLOCK_CHOL) {
+    memcpy(Rf, G, sizeof(double) * (size_t)nc * nc);
+    scipy_dpotrf_("U", &nc, Rf, &nc, &info, 1);
+    if (info) {
+      memcpy(Rf, G, sizeof(double) * (size_t)nc * nc);
+      for (i = 0; i < nc; i++) Rf[i + (size_t)i * nc] += 50.0 * ORC_MACHINE_EPS;
+      info = 0;
+      scipy_dpotrf_("U", &nc, Rf, &nc, &info, 1);
+      if (info) { st = ORC_ERR_LAPACK; goto out; }
+    }
+    for (j = 0; j < nc; j++)
+      for (i = j + 1; i < nc; i++) Rf[i + (size_t)j * nc] = 0.0;
+    memcpy(S, Rf, sizeof(double) * (size_t)nc * nc);
+    scipy_dtrtri_("U", "N", &nc, S, &nc, &info, 1, 1);
+    if (info) { st = ORC_ERR_LAPACK; goto out; }
+  } else {
+    int lwork = -1;
+    double q;
+    eig = (double *)malloc(sizeof(double) * (size_t)nc);
+    D = (double *)malloc(sizeof(double) * (size_t)nc);
+    scipy_dsyev_("V", "L", &nc, S, &nc, eig, &q, &lwork, &info, 1, 1);
+    lwork = (int)q;
+    work = (double *)malloc(sizeof(double) * (size_t)(lwork > 1 ? lwork : 1));
+    for (i = 0; i < nc; i++) {
+      if (!(G[i + (size_t)i * nc] > 0.0)) { st = ORC_ERR_BREAKDOWN; goto out; }
+      D[i] = 1.0 / sqrt(G[i + (size_t)i * nc]);
+    }
+    for (j = 0; j < nc; j++)
+      for (i = 0; i < nc; i++) S[i + (size_t)j * nc] = G[i + (size_t)j * nc] * D[i] * D[j];
+    scipy_dsyev_("V", "L", &nc, S, &nc, eig, work, &lwork, &info, 1, 1);
+    if (info) { st = ORC_ERR_LAPACK; goto out; }
+    for (i = 0; i < nc; i++)
+      if (!(eig[i] > 0.0)) { st = ORC_ERR_BREAKDOWN; goto out; }
+    /* R = Lambda^{1/2} U' / D, S = D U Lambda^{-1/2} */
+    for (j = 0; j < nc; j++)
+      for (i = 0; i < nc; i++) Rf[i + (size_t)j * nc] = S[j + (size_t)i * nc] * sqrt(eig[i]) / D[j];
+    for (j = 0; j < nc; j++)
+      for (i = 0; i < nc; i++) S[i + (size_t)j * nc] = S[i + (size_t)j * nc] * D[i] / sqrt(eig[j]);
+  }
+  {
+    /* BVMultInPlace(V, S, l, k): Q indexed from the active columns */
+    const int ldq = B->k;
+    double *Q = (double *)calloc((size_t)ldq * ldq, sizeof(double));
+    for (j = 0; j < nc; j++) memcpy(Q + l + (size_t)(l + j) * ldq, S + (size_t)j * nc, sizeof(double) * (size_t)nc);
+    blk_multinplace(B, Q, ldq, l, B->k);
+    free(Q);
+  }
+  if (Rout) {
+    for (j = 0; j < nc; j++) {
+      for (i = 0; i < l; i++) Rout[i + (size_t)(l + j) * ldr] = C[i + (size_t)j * l];
+      for (i = 0; i < nc; i++) Rout[l + i + (size_t)(l + j) * ldr] = Rf[i + (size_t)j * nc];
+    }
+  }
+out:
+  free(C); free(G); free(S); free(Rf); free(work); free(eig); free(D);
+  return st;
+}
+
+/* BVOrthogonalize (bvorthog.c:726-767) with the given BVOrthogBlockType; BV_ORTHOG_BLOCK_GS
+ * proceeds column by column (BVOrthogonalize_GS, :507-548). */
+static int blk_orthogonalize(oblk *B, int type)
 {
   double norm;
   int lindep, st;
+  if (type == ORC_BLOCK_CHOL || type == ORC_BLOCK_SVQB) return blk_orthogonalize_gram(B, type, NULL, 0);
+  if (type != ORC_BLOCK_GS) return ORC_ERR_ARG;
   for (int j = B->l; j < B->k; j++) {
     if ((st = orthogonalize_gs(&B->b, j, NULL, &norm, &lindep))) return st;
     if (norm == 0.0) return ORC_ERR_BREAKDOWN;
     scale_column(&B->b, j, 1.0 / norm);
   }
   return ORC_OK;
+}
+
+/* BVOrthogonalize of the columns [l,k) of V (n x k, leading dimension ld) with
+ * block type 1 (Cholesky) or 4 (SVQB); R as above (nullable). */
+int oracle_bv_orthogonalize_block(int n, int ld, double *V, int l, int k, int type, double *R, int ldr)
+{
+  oblk B;
+  if (n <= 0 || ld < n || l < 0 || k < l || (type != ORC_BLOCK_CHOL && type != ORC_BLOCK_SVQB)) return ORC_ERR_ARG;
+  memset(&B, 0, sizeof(B));
+  B.b.n = n; B.b.m = k; B.b.ld = ld; B.b.V = V;
+  B.l = l; B.k = k;
+  return blk_orthogonalize_gram(&B, type, R, ldr);
 }
 
 /* DSSolve_GHEP + DSSort_GHEP + DSVectors_GHEP on an nv x nv pencil (A, B), ld x ld.
@@ -1068,13 +1180,15 @@ static void precond_apply(const double *dinv, oblk *R)
  * oracle_lobpcg: EPSSolve with EPSLOBPCG on a symmetric CSR matrix.
  *   which: ORC_SMALLEST_REAL or ORC_LARGEST_REAL; bs <= 0: min(16, nev);
  *   ncv <= 0: the LOBPCG default; restart 0.9; lock 1; max_it <= 0: max(100, 2n/ncv);
- *   pc: 0 none, 1 Jacobi; X0 (n x nini, column-major) the initial space (may be NULL).
+ *   pc: 0 none, 1 Jacobi; orthog_block: the BVOrthogBlockType of X, R and P (0 GS, 1 Cholesky,
+ *   4 SVQB; BVSetOrthogonalization on eps->V, which the blocks inherit through BVDuplicate);
+ *   X0 (n x nini, column-major) the initial space (may be NULL).
  * Outputs sorted eigenvalues (nconv), eigenvectors X (n x nconv), error estimates,
  * info[0..3] = nconv, its, reason, iterations of the inner loop.
  */
 int oracle_lobpcg(int n, const int *rowptr, const int *colind, const double *vals, int nev, int bs, int ncv,
-                  double tol, int max_it, int which, int pc, int lock, double restart, const double *X0, int nini,
-                  double *evals, double *Xout, double *errest_out, int *info)
+                  double tol, int max_it, int which, int pc, int lock, double restart, int orthog_block,
+                  const double *X0, int nini, double *evals, double *Xout, double *errest_out, int *info)
 {
   orc_op op;
   oblk V, Z, X, R, P, AX, Y;
@@ -1085,6 +1199,8 @@ int oracle_lobpcg(int n, const int *rowptr, const int *colind, const double *val
   memset(&op, 0, sizeof(op));
   op.n = n; op.rp = rowptr; op.ci = colind; op.va = vals;
   if (which != ORC_SMALLEST_REAL && which != ORC_LARGEST_REAL) return ORC_ERR_ARG;
+  if (orthog_block != ORC_BLOCK_GS && orthog_block != ORC_BLOCK_CHOL && orthog_block != ORC_BLOCK_SVQB)
+    return ORC_ERR_ARG;
   if (bs <= 0) bs = nev < 16 ? nev : 16;
   k = 3 * bs > ((nev - 1) / bs + 3) * bs ? 3 * bs : ((nev - 1) / bs + 3) * bs;
   if (ncv <= 0) ncv = k;
@@ -1225,7 +1341,7 @@ int oracle_lobpcg(int n, const int *rowptr, const int *colind, const double *val
       locked += nconv;
       nconv = 0;
       blk_active(&X, nconv, bs);
-      if ((st = blk_orthogonalize(&X))) goto done;
+      if ((st = blk_orthogonalize(&X, orthog_block))) goto done;
       blk_active(&Z, nconv, bs);
       blk_active(&AX, nconv, bs);
       blk_copy(&X, &Z);
@@ -1249,9 +1365,9 @@ int oracle_lobpcg(int n, const int *rowptr, const int *colind, const double *val
       }
     }
     /* 11 */
-    if ((st = blk_orthogonalize(&R))) goto done;
+    if ((st = blk_orthogonalize(&R, orthog_block))) goto done;
     /* 13-16 */
-    if (its > 1 && (st = blk_orthogonalize(&P))) goto done;
+    if (its > 1 && (st = blk_orthogonalize(&P, orthog_block))) goto done;
     /* 17-23 */
     blk_active(&Z, 0, bs); blk_active(&X, 0, bs);
     blk_copy(&X, &Z);

@@ -83,6 +83,7 @@ _SIGS = {
     "b200_eps_lobpcg_set_restart": (ctypes.c_int, [_vp, ctypes.c_double]),
     "b200_eps_lobpcg_set_locking": (ctypes.c_int, [_vp, ctypes.c_int]),
     "b200_eps_set_preconditioner": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_eps_set_bv_orthog_block": (ctypes.c_int, [_vp, ctypes.c_int]),
     "b200_eps_set_initial_space_block": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     "b200_viewer_binary_open": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _vp]),
     "b200_viewer_destroy": (ctypes.c_int, [_vp]),
@@ -146,6 +147,8 @@ _SIGS = {
     "b200_bv_set_active_columns": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
     "b200_bv_get_active_columns": (ctypes.c_int, [_vp, _ip, _ip]),
     "b200_bv_set_orthog_eta": (ctypes.c_int, [_vp, ctypes.c_double]),
+    "b200_bv_set_orthog_block": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_bv_get_orthog_block": (ctypes.c_int, [_vp, _ip]),
     "b200_bv_set_column": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     "b200_bv_get_column": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     "b200_bv_copy_vec": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
@@ -401,6 +404,10 @@ class Mat:
 class BV:
     """Column-major basis of vectors resident in HBM (the new BV type)."""
 
+    class OrthogBlockType:
+        """BVOrthogBlockType (include/slepcbv.h:84-88); TSQR and TSQRCHOL are not provided."""
+        GS, CHOL, TSQR, TSQRCHOL, SVQB = 0, 1, 2, 3, 4
+
     def __init__(self):
         self.handle = ctypes.c_void_p()
 
@@ -428,6 +435,15 @@ class BV:
 
     def setOrthogonalizationEta(self, eta):
         _check(lib().b200_bv_set_orthog_eta(self.handle, eta))
+
+    def setOrthogonalizationBlock(self, block):
+        """BVSetOrthogonalization's block type (BV.OrthogBlockType), the method of orthogonalize()."""
+        _check(lib().b200_bv_set_orthog_block(self.handle, block))
+
+    def getOrthogonalizationBlock(self):
+        t = ctypes.c_int()
+        _check(lib().b200_bv_get_orthog_block(self.handle, ctypes.byref(t)))
+        return t.value
 
     def setColumn(self, j, x):
         x = np.ascontiguousarray(x, dtype=np.float64)
@@ -617,6 +633,11 @@ class EPS:
     def setPreconditioner(self, pc):
         """STPRECOND with KSPPREONLY and PCNONE / PCJACOBI (EPS.PCType)."""
         _check(lib().b200_eps_set_preconditioner(self.handle, pc))
+
+    def setBVOrthogonalizationBlock(self, block):
+        """-bv_orthog_block: the BVOrthogBlockType (BV.OrthogBlockType) of the basis, which
+        LOBPCG's blocks inherit."""
+        _check(lib().b200_eps_set_bv_orthog_block(self.handle, block))
 
     def setPrecision(self, precision):
         """EPS.Precision.FP64 (default, the drop-in path) or EPS.Precision.MIXED: Krylov-Schur

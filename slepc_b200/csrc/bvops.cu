@@ -37,7 +37,8 @@ __device__ __forceinline__ double warp_sum(double v) {
 // FP32 basis of the mixed-precision solver); products and sums are FP64.
 template <int MAXJ, typename TI, typename TO>
 __global__ void __launch_bounds__(kGemmThreads) panel_gemm_kernel(const TI *X, int ldx, TO *Y, int ldy, int n, int kq,
-                                                                  const double *__restrict__ Q, int ldq, int nc) {
+                                                                  const double *__restrict__ Q, int ldq, int nc,
+                                                                  double alpha, double beta) {
   extern __shared__ __align__(16) double sm[];
   double *Qs = sm;                          // [kq][nc] row-major by c: Qs[c*nc + j]
   double *As = sm + (size_t)kq * nc;        // input panel As[c*kRB + r]; then output tile Os[j*(kRB+1) + r]
@@ -88,7 +89,11 @@ __global__ void __launch_bounds__(kGemmThreads) panel_gemm_kernel(const TI *X, i
     __syncthreads();
     for (int idx = tid; idx < nc * kRB; idx += kGemmThreads) {
       const int j = idx / kRB, r = idx - j * kRB;
-      if (r < rows) Y[(size_t)j * ldy + r0 + r] = (TO)As[j * (kRB + 1) + r];
+      if (r < rows) {
+        TO *y = Y + (size_t)j * ldy + r0 + r;
+        const double v = As[j * (kRB + 1) + r];
+        *y = (TO)(beta == 0.0 ? alpha * v : alpha * v + beta * (double)*y);
+      }
     }
   }
 }
@@ -113,7 +118,8 @@ __host__ __device__ inline int dmma_q_stride(int ncp) { return (ncp % 16) ? ncp 
 
 template <int NT, typename TI, typename TO>
 __global__ void __launch_bounds__(kGemmThreads) panel_dmma_kernel(const TI *X, int ldx, TO *Y, int ldy, int n, int kq,
-                                                                  const double *__restrict__ Q, int ldq, int nc) {
+                                                                  const double *__restrict__ Q, int ldq, int nc,
+                                                                  double alpha, double beta) {
   static_assert(kRB == 8 * (kGemmThreads / 32), "one 8-row strip per warp");
   extern __shared__ __align__(16) double sm[];
   const int kp = (kq + 3) & ~3;
@@ -156,7 +162,11 @@ __global__ void __launch_bounds__(kGemmThreads) panel_dmma_kernel(const TI *X, i
     __syncthreads();
     for (int idx = tid; idx < nc * kRB; idx += kGemmThreads) {
       const int j = idx / kRB, r = idx - j * kRB;
-      if (r < rows) Y[(size_t)j * ldy + r0 + r] = (TO)Xs[j * kDmmaStride + r];
+      if (r < rows) {
+        TO *y = Y + (size_t)j * ldy + r0 + r;
+        const double v = Xs[j * kDmmaStride + r];
+        *y = (TO)(beta == 0.0 ? alpha * v : alpha * v + beta * (double)*y);
+      }
     }
   }
 }
@@ -524,7 +534,7 @@ unsigned grid_for(long long len, int threads) {
 
 template <typename TI, typename TO>
 cudaError_t panel_gemm_launch(const TI *X, int ldx, TO *Y, int ldy, int n, int kq, const double *Q, int ldq, int nc,
-                              cudaStream_t stream) {
+                              cudaStream_t stream, double alpha = 1.0, double beta = 0.0) {
   if (nc <= 0 || kq <= 0 || n <= 0) return cudaSuccess;
   if (nc > 16 * 8 || kq > kMaxCols) return cudaErrorInvalidValue;
   {
@@ -541,7 +551,8 @@ cudaError_t panel_gemm_launch(const TI *X, int ldx, TO *Y, int ldy, int n, int k
   case NT:                                                                                                  \
     err = allow_max_dynamic_smem(panel_dmma_kernel<NT, TI, TO>);                                            \
     if (err != cudaSuccess) return err;                                                                     \
-    panel_dmma_kernel<NT, TI, TO><<<grid, kGemmThreads, dsm, stream>>>(X, ldx, Y, ldy, n, kq, Q, ldq, nc);   \
+    panel_dmma_kernel<NT, TI, TO><<<grid, kGemmThreads, dsm, stream>>>(X, ldx, Y, ldy, n, kq, Q, ldq, nc, alpha, \
+                                                                       beta);                                  \
     break;
         B200_DMMA_CASE(1) B200_DMMA_CASE(2) B200_DMMA_CASE(3) B200_DMMA_CASE(4) B200_DMMA_CASE(5)
         B200_DMMA_CASE(6) B200_DMMA_CASE(7) B200_DMMA_CASE(8) B200_DMMA_CASE(9) B200_DMMA_CASE(10)
@@ -567,7 +578,8 @@ cudaError_t panel_gemm_launch(const TI *X, int ldx, TO *Y, int ldy, int n, int k
   case J:                                                                                                  \
     err = allow_max_dynamic_smem(panel_gemm_kernel<J, TI, TO>);                                            \
     if (err != cudaSuccess) return err;                                                                    \
-    panel_gemm_kernel<J, TI, TO><<<grid, kGemmThreads, smem, stream>>>(X, ldx, Y, ldy, n, kq, Q, ldq, nc); \
+    panel_gemm_kernel<J, TI, TO><<<grid, kGemmThreads, smem, stream>>>(X, ldx, Y, ldy, n, kq, Q, ldq, nc, alpha, \
+                                                                       beta);                                  \
     break;
     B200_MIP_CASE(1)
     B200_MIP_CASE(2)
@@ -647,6 +659,12 @@ cudaError_t gershgorin_launch(int n, const int *rowptr, const int *colind, const
 cudaError_t mult_launch(double *Y, int ldy, const double *X, int ldx, int n, int nx, int ny, const double *Q, int ldq,
                         double alpha, double beta, cudaStream_t stream) {
   if (n <= 0 || ny <= 0) return cudaSuccess;
+  // the row-panel product (X read once, FP64 tensor cores) when the block fits it; the simple
+  // kernel below reads X once per output column
+  if (nx > 0 && nx <= kMaxCols && ny <= 16 * 8) {
+    const cudaError_t err = panel_gemm_launch<double, double>(X, ldx, Y, ldy, n, nx, Q, ldq, ny, stream, alpha, beta);
+    if (err != cudaErrorInvalidValue) return err;  // otherwise the block does not fit shared memory
+  }
   dim3 grid((unsigned)((n + 255) / 256), (unsigned)ny);
   mult_kernel<<<grid, 256, 0, stream>>>(Y, ldy, X, ldx, n, nx, ny, Q, ldq, alpha, beta);
   count_launch();

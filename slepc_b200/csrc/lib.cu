@@ -12,6 +12,7 @@
 // sequence of kernels with a single host synchronisation at its end.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -29,6 +30,13 @@ using namespace b200;
 // --------------------------------------------------------------- errors ---
 static thread_local std::string g_last_error;
 static std::atomic<uint64_t> g_launches{0};
+
+// LAPACK from the OpenBLAS bundled with scipy (symbols carry a scipy_ prefix)
+extern "C" void scipy_dpotrf_(const char *uplo, const int *n, double *a, const int *lda, int *info, size_t);
+extern "C" void scipy_dtrtri_(const char *uplo, const char *diag, const int *n, double *a, const int *lda, int *info,
+                              size_t, size_t);
+extern "C" void scipy_dsyev_(const char *jobz, const char *uplo, const int *n, double *a, const int *lda, double *w,
+                             double *work, const int *lwork, int *info, size_t, size_t);
 
 extern "C" void b200_set_last_error(const char *file, int line, const char *msg) {
   const char *base = strrchr(file, '/');
@@ -663,6 +671,24 @@ extern "C" b200_status b200_bv_set_orthog_eta(b200_bv bv, double eta) {
   return B200_OK;
 }
 
+extern "C" b200_status b200_bv_set_orthog_block(b200_bv bv, int type) {
+  B200_ARG_CHECK(bv, "null BV");
+  if (type == B200_ORTHOG_BLOCK_TSQR || type == B200_ORTHOG_BLOCK_TSQRCHOL) {
+    b200_set_last_error(__FILE__, __LINE__, "the TSQR block orthogonalizations are not supported");
+    return B200_ERR_SUP;
+  }
+  B200_ARG_CHECK(type == B200_ORTHOG_BLOCK_GS || type == B200_ORTHOG_BLOCK_CHOL || type == B200_ORTHOG_BLOCK_SVQB,
+                 "unknown block orthogonalization type");
+  bv->orthog_block = type;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_bv_get_orthog_block(b200_bv bv, int *type) {
+  B200_ARG_CHECK(bv && type, "null argument");
+  *type = bv->orthog_block;
+  return B200_OK;
+}
+
 
 extern "C" b200_status b200_bv_set_column(b200_bv bv, int j, const double *x) {
   B200_ARG_CHECK(bv && x && j >= 0 && j < bv->m, "column index out of range");
@@ -871,8 +897,101 @@ b200_status b200::bv_column_norms(b200_bv bv, double *nrm) {
   return B200_OK;
 }
 
+// BVOrthogonalize_Chol (bvorthog.c:595-613) and BVOrthogonalize_SVQB (:665-684) on the active
+// columns [l,k): one Gram-Schmidt pass against the leading columns (BVOrthogonalize_BlockGS,
+// :492-501: C = V1^T V2, V2 -= V1 C), the Gram matrix G = V2^T V2 on the device, its
+// factorisation on the host in FP64 (BVMatCholInv_LAPACK_Private, bvlapack.c:136-213: dpotrf "U",
+// once more with 50 eps on the diagonal if it fails, dtrtri; BVMatSVQB_LAPACK_Private, :261-340:
+// D = diag(G)^{-1/2}, dsyev "V" "L" of D G D = U Lambda U^T, S = D U Lambda^{-1/2}), then
+// V2 := V2 S with the row-panel in-place product.  Six kernel launches and one read-back instead
+// of a Gram-Schmidt sweep per column.  R (nullable): R(0:l, l:k) = C and R(l:k, l:k) = the
+// Cholesky factor or Lambda^{1/2} U^T D^{-1}, so that V_in = V_out R.  A zero column or a
+// non-positive eigenvalue of the SVQB Gram matrix (a numerically rank-deficient block, for which
+// the reference would divide by zero or take the square root of a negative number) is reported as
+// a breakdown.
+static b200_status bv_orthogonalize_gram(b200_bv bv, double *R, int ldr) {
+  const int l = bv->l, k = bv->k, nc = k - l, n = bv->n, ld = bv->ld;
+  if (nc <= 0) return B200_OK;
+  const size_t nC = (size_t)l * nc, nG = (size_t)nc * nc;
+  B200_CHECK(bv_reserve(bv, nC + nG, std::max(nC, nG) * num_sms_host()));
+  cudaStream_t s = bv->stream;
+  double *Cdev = bv->qbuf, *Gdev = bv->qbuf + nC;
+  if (l > 0) {
+    B200_CUDA_CHECK(dot_launch(col(bv, l), ld, nc, bv->V, ld, l, n, Cdev, l, bv->red, bv->red_len, s));
+    B200_CUDA_CHECK(mult_launch(col(bv, l), ld, bv->V, ld, n, l, nc, Cdev, l, -1.0, 1.0, s));
+  }
+  B200_CUDA_CHECK(dot_launch(col(bv, l), ld, nc, col(bv, l), ld, nc, n, Gdev, nc, bv->red, bv->red_len, s));
+  B200_CUDA_CHECK(cudaMemcpyAsync(bv->hpin, bv->qbuf, sizeof(double) * (nC + nG), cudaMemcpyDeviceToHost, s));
+  B200_CUDA_CHECK(cudaStreamSynchronize(s));
+  std::vector<double> C(bv->hpin, bv->hpin + nC), G(bv->hpin + nC, bv->hpin + nC + nG), Rf(nG, 0.0), S(nG, 0.0);
+  int info = 0;
+  if (bv->orthog_block == B200_ORTHOG_BLOCK_CHOL) {
+    Rf = G;
+    scipy_dpotrf_("U", &nc, Rf.data(), &nc, &info, 1);
+    if (info) {
+      Rf = G;
+      for (int i = 0; i < nc; ++i) Rf[(size_t)i * nc + i] += 50.0 * 2.220446049250313e-16;
+      info = 0;
+      scipy_dpotrf_("U", &nc, Rf.data(), &nc, &info, 1);
+      if (info) {
+        b200_set_last_error(__FILE__, __LINE__, "LAPACK dpotrf failed in BVOrthogonalize (Cholesky)");
+        return B200_ERR_LAPACK;
+      }
+    }
+    for (int j = 0; j < nc; ++j)
+      for (int i = j + 1; i < nc; ++i) Rf[(size_t)j * nc + i] = 0.0;
+    S = Rf;
+    scipy_dtrtri_("U", "N", &nc, S.data(), &nc, &info, 1, 1);
+    if (info) {
+      b200_set_last_error(__FILE__, __LINE__, "LAPACK dtrtri failed in BVOrthogonalize (Cholesky)");
+      return B200_ERR_LAPACK;
+    }
+  } else {
+    std::vector<double> D(nc), eig(nc);
+    for (int i = 0; i < nc; ++i) {
+      if (!(G[(size_t)i * nc + i] > 0.0)) {
+        b200_set_last_error(__FILE__, __LINE__, "breakdown in BVOrthogonalize (SVQB): zero column");
+        return B200_ERR_BREAKDOWN;
+      }
+      D[i] = 1.0 / std::sqrt(G[(size_t)i * nc + i]);
+    }
+    for (int j = 0; j < nc; ++j)
+      for (int i = 0; i < nc; ++i) S[(size_t)j * nc + i] = G[(size_t)j * nc + i] * D[i] * D[j];
+    int lwork = -1;
+    double q = 0.0;
+    scipy_dsyev_("V", "L", &nc, S.data(), &nc, eig.data(), &q, &lwork, &info, 1, 1);
+    lwork = std::max(1, (int)q);
+    std::vector<double> work(lwork);
+    scipy_dsyev_("V", "L", &nc, S.data(), &nc, eig.data(), work.data(), &lwork, &info, 1, 1);
+    if (info) {
+      b200_set_last_error(__FILE__, __LINE__, "LAPACK dsyev failed in BVOrthogonalize (SVQB)");
+      return B200_ERR_LAPACK;
+    }
+    for (int i = 0; i < nc; ++i)
+      if (!(eig[i] > 0.0)) {
+        b200_set_last_error(__FILE__, __LINE__, "breakdown in BVOrthogonalize (SVQB): rank-deficient block");
+        return B200_ERR_BREAKDOWN;
+      }
+    for (int j = 0; j < nc; ++j)
+      for (int i = 0; i < nc; ++i) Rf[(size_t)j * nc + i] = S[(size_t)i * nc + j] * std::sqrt(eig[i]) / D[j];
+    for (int j = 0; j < nc; ++j)
+      for (int i = 0; i < nc; ++i) S[(size_t)j * nc + i] *= D[i] / std::sqrt(eig[j]);
+  }
+  memcpy(bv->hpin, S.data(), sizeof(double) * nG);
+  B200_CUDA_CHECK(cudaMemcpyAsync(Gdev, bv->hpin, sizeof(double) * nG, cudaMemcpyHostToDevice, s));
+  B200_CUDA_CHECK(multinplace_launch(bv->V, ld, n, l, k, Gdev, nc, l, k, s));
+  if (R) {
+    for (int j = 0; j < nc; ++j) {
+      for (int i = 0; i < l; ++i) R[i + (size_t)(l + j) * ldr] = C[i + (size_t)j * l];
+      for (int i = 0; i < nc; ++i) R[l + i + (size_t)(l + j) * ldr] = Rf[i + (size_t)j * nc];
+    }
+  }
+  return B200_OK;
+}
+
 extern "C" b200_status b200_bv_orthogonalize(b200_bv bv, double *R, int ldr) {
   B200_ARG_CHECK(bv && (!R || ldr >= bv->k), "R leading dimension too small");
+  if (bv->orthog_block != B200_ORTHOG_BLOCK_GS) return bv_orthogonalize_gram(bv, R, ldr);
   if (!R) return bv_orthogonalize_block(bv);
   for (int j = bv->l; j < bv->k; ++j) {
     double norm = 0.0;
@@ -1288,6 +1407,19 @@ extern "C" b200_status b200_eps_lobpcg_set_locking(b200_eps eps, int lock) {
 extern "C" b200_status b200_eps_set_preconditioner(b200_eps eps, int pc) {
   B200_ARG_CHECK(eps && (pc == B200_PC_NONE || pc == B200_PC_JACOBI), "unknown preconditioner");
   eps->pc = pc;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_set_bv_orthog_block(b200_eps eps, int type) {
+  B200_ARG_CHECK(eps, "null EPS");
+  if (type == B200_ORTHOG_BLOCK_TSQR || type == B200_ORTHOG_BLOCK_TSQRCHOL) {
+    b200_set_last_error(__FILE__, __LINE__, "the TSQR block orthogonalizations are not supported");
+    return B200_ERR_SUP;
+  }
+  B200_ARG_CHECK(type == B200_ORTHOG_BLOCK_GS || type == B200_ORTHOG_BLOCK_CHOL || type == B200_ORTHOG_BLOCK_SVQB,
+                 "unknown block orthogonalization type");
+  eps->orthog_block = type;
+  if (eps->V) eps->V->orthog_block = type;
   return B200_OK;
 }
 

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -141,6 +142,21 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
   eps->tol_ = tol;
   memset(&eps->stats, 0, sizeof(eps->stats));
   const uint64_t launches0 = launch_count();
+  // Optional phase timing (b200_eps_set_timing): host clock between stream synchronisations at the
+  // edges of each phase.  ms_spmv: BVMatMult; ms_orth: BVOrthogonalize and BVOrthogonalizeVec of
+  // the blocks; ms_restart: the Rayleigh-Ritz projections (BVDot, DSSolve, BVMult); ms_total: all.
+  using clk = std::chrono::steady_clock;
+  const bool timing = eps->timing != 0;
+  auto phase_begin = [&]() {
+    if (timing) cudaStreamSynchronize(eps->stream);
+    return clk::now();
+  };
+  auto phase_end = [&](clk::time_point t0, double &acc) {
+    if (!timing) return;
+    cudaStreamSynchronize(eps->stream);
+    acc += std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+  };
+  const clk::time_point t_solve = phase_begin();
 
   // EPSAllocateSolution(eps,0): V with ncv columns
   if (eps->V) {
@@ -166,6 +182,10 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
   B200_CHECK(b200_bv_create(n, 3 * bs, eps->stream, &B.W));  // A Z of BVMatProject
   for (b200_bv b : {B.Z, B.X, B.R, B.P, B.AX, B.Y, B.W})
     B200_CUDA_CHECK(cudaMemsetAsync(b->V, 0, sizeof(double) * b->ld * (size_t)(b->m + 1), b->stream));
+  // the blocks are BVDuplicateResize copies of eps->V and inherit its orthogonalization settings
+  // (BVDuplicate_Private, bvbasic.c:1619-1632)
+  V->orthog_block = eps->orthog_block;
+  for (b200_bv b : {B.Z, B.X, B.R, B.P, B.AX, B.Y, B.W}) b->orthog_block = eps->orthog_block;
   b200_bv Z = B.Z, X = B.X, R = B.R, P = B.P, AX = B.AX, Y = B.Y, W = B.W;
   active(Y, 0, 0);
   if (eps->pc == B200_PC_JACOBI) {
@@ -206,8 +226,11 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
 
   // 4. Rayleigh-Ritz on X alone (also after hard locking)
   auto rayleigh_ritz_x = [&]() -> b200_status {
+    clk::time_point t0 = phase_begin();
     B200_CHECK(bv_mat_mult(X, A, AX));
+    phase_end(t0, eps->stats.ms_spmv);
     eps->stats.lanczos_steps += X->k - X->l;
+    t0 = phase_begin();
     std::fill(MA.begin(), MA.end(), 0.0);
     B200_CHECK(b200_bv_dot(AX, X, MA.data(), mpd));  // BVMatProject(AX,NULL,X,M): M = X^T AX
     if (flip)
@@ -219,6 +242,7 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
       if (locked + j < ncv) eigr[locked + j] = flip ? -wr[j] : wr[j];
     B200_CHECK(b200_bv_mult_inplace(X, Q.data(), mpd, 0, nv));
     B200_CHECK(b200_bv_mult_inplace(AX, Q.data(), mpd, 0, nv));
+    phase_end(t0, eps->stats.ms_restart);
     return B200_OK;
   };
   B200_CHECK(rayleigh_ritz_x());
@@ -279,6 +303,7 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
       active(V, locked + bs, locked + bs + nconv);
       active(X, bs - nconv, bs);
       B200_CUDA_CHECK(bv_copy(V, X));
+      const clk::time_point t0 = phase_begin();
       {
         std::vector<double *> vs;
         for (int j = bs - nconv; j < bs; ++j) vs.push_back(col(X, j));
@@ -291,6 +316,7 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
       nconv = 0;
       active(X, nconv, bs);
       B200_CHECK(b200_bv_orthogonalize(X, nullptr, 0));
+      phase_end(t0, eps->stats.ms_orth);
       active(Z, nconv, bs);
       active(AX, nconv, bs);
       B200_CUDA_CHECK(bv_copy(X, Z));
@@ -308,6 +334,7 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
     // 9. preconditioner on the residuals, then against the locked vectors
     if (eps->pc == B200_PC_JACOBI)
       B200_CUDA_CHECK(diag_scale_launch(col(R, ini), R->ld, n, bs - ini, eps->dinv, R->stream));
+    clk::time_point t0 = phase_begin();
     if (locked > 0) {
       std::vector<double *> vs;
       for (int j = ini; j < bs; ++j) vs.push_back(col(R, j));
@@ -321,6 +348,7 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
     // 11. orthonormalise the preconditioned residuals; 13-16 the conjugate directions
     B200_CHECK(b200_bv_orthogonalize(R, nullptr, 0));
     if (its > 1) B200_CHECK(b200_bv_orthogonalize(P, nullptr, 0));
+    phase_end(t0, eps->stats.ms_orth);
     // 17-23. Z = [X R P] and the Gram matrices Z^T A Z, Z^T Z
     active(Z, 0, bs);
     active(X, 0, bs);
@@ -334,8 +362,11 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
     nv = its > 1 ? 3 * bs - 2 * ini : 2 * bs - ini;
     active(Z, 0, nv);
     active(W, 0, nv);
+    t0 = phase_begin();
     B200_CHECK(bv_mat_mult(Z, A, W));  // BVMatProject_MatMult: W = A Z, M = Z^T W
+    phase_end(t0, eps->stats.ms_spmv);
     eps->stats.lanczos_steps += nv;
+    t0 = phase_begin();
     std::fill(MA.begin(), MA.end(), 0.0);
     B200_CHECK(b200_bv_dot(W, Z, MA.data(), mpd));
     if (flip)
@@ -355,8 +386,11 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
     if (lock) active(P, nconv, bs);
     active(Z, 0, bs);
     B200_CHECK(b200_bv_mult(X, 1.0, 1.0, Z, Q.data(), mpd));
+    phase_end(t0, eps->stats.ms_restart);
     if (lock) active(X, nconv, bs);
+    t0 = phase_begin();
     B200_CHECK(bv_mat_mult(X, A, AX));
+    phase_end(t0, eps->stats.ms_spmv);
     eps->stats.lanczos_steps += X->k - X->l;
   }
   eps_its += its;
@@ -382,6 +416,7 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
   }
   active(V, 0, eps_nconv);
   B200_CUDA_CHECK(cudaStreamSynchronize(eps->stream));
+  phase_end(t_solve, eps->stats.ms_total);
   eps->stats.restarts = eps_its;
   eps->stats.kernel_launches = (int64_t)(launch_count() - launches0);
   eps->solved = true;

@@ -51,6 +51,7 @@ struct b200_bv_s {
   double *V = nullptr;
   int l = 0, k = 0;
   double eta = 0.7071;        // bvfunc.c:178
+  int orthog_block = B200_ORTHOG_BLOCK_GS;  // bvfunc.c:179
   cudaStream_t stream = nullptr;
   b200::GsWork gs{};
   double *coefbuf = nullptr;  // (m+1) x (m+1): column j = coefficients of column j (BVGetBufferVec)
@@ -102,6 +103,7 @@ struct b200_eps_s {
   double lobpcg_restart = 0.0;
   int lobpcg_lock = 1;
   int pc = B200_PC_JACOBI;
+  int orthog_block = B200_ORTHOG_BLOCK_GS;  // BVSetOrthogonalization block type of eps->V (LOBPCG blocks)
   std::vector<double> X0;  // initial space of EPSSetInitialSpace with several vectors (n x nini_block)
   int nini_block = 0;
   int nini_eff = 0;  // initial vectors kept by BVInsertVecs in the last setup

@@ -8,6 +8,7 @@ time one kernel family in isolation with CUDA events:
   python slepc_b200/kernel_bench.py multinplace      # restart GEMM V(:,0:56) = V(:,0:80) Q
   python slepc_b200/kernel_bench.py cross            # A x, A^T z, A^T A x of the 2M x 500k power-law matrix
   python slepc_b200/kernel_bench.py batched          # the batched Krylov-Schur launch on a small k-NN batch
+  python slepc_b200/kernel_bench.py lobpcg --lgrid 512   # LOBPCG per block orthogonalization type
 
 Prints one JSON line per kernel family: average ms per call and algorithmic GB/s.
 """
@@ -145,6 +146,89 @@ def mixed(args, torch):
     return {"kernel": "mixed solve (FP32-basis phase + refinement)", "n": n, **st}
 
 
+def lobpcg(args, torch):
+    """LOBPCG (smallest 16, block 16, Jacobi) on the 2-D anisotropic diffusion operator of an
+    --lgrid^2 grid, once per BVOrthogBlockType: iterations, seconds, milliseconds and kernel
+    launches per iteration, and the largest eigenvalue difference from the Gram-Schmidt run."""
+    from slepc_b200 import learned
+
+    csr = P.diffusion_problem(args.lgrid, 1)[0]
+    out, base = [], None
+    for name in args.block:
+        t = {"gs": S.BV.OrthogBlockType.GS, "chol": S.BV.OrthogBlockType.CHOL, "svqb": S.BV.OrthogBlockType.SVQB}[name]
+        learned.solve_lowest(S, csr, nev=16, max_it=3, orthog_block=t)  # warm-up: allocations, first launches
+        r = learned.solve_lowest(S, csr, nev=16, orthog_block=t, stats=True)
+        if base is None:
+            base = r["vals"]
+        its = max(r["its"], 1)
+        line = {"kernel": f"lobpcg orthog_block={name}", "n": args.lgrid ** 2, "its": r["its"],
+                "reason": r["reason"], "seconds": round(r["seconds"], 4),
+                "ms_per_iteration": round(1e3 * r["seconds"] / its, 4),
+                "launches_per_iteration": round(r["stats"]["kernel_launches"] / its, 1),
+                "max_error": r["max_error"],
+                "max_rel_diff_vs_first": float(np.max(np.abs(r["vals"] - base) / np.abs(base)))}
+        if args.phases:
+            # a second run with the phase edges synchronised: where an iteration's time goes
+            q = learned.solve_lowest(S, csr, nev=16, orthog_block=t, stats=True, timing=True)
+            st, qi = q["stats"], max(q["its"], 1)
+            line["phase_ms_per_iteration"] = {k: round(st[f"ms_{k}"] / qi, 4) for k in ("spmv", "orth", "restart",
+                                                                                          "total")}
+        out.append(line)
+    return out
+
+
+def lobpcg_ops(args, torch):
+    """The block operations of one LOBPCG iteration at n = --lgrid^2, each timed alone on the host
+    clock over --reps x 20 calls (every call ends with a read-back or a synchronisation, as in the
+    solver): BVDot of 48-column blocks, BVMult 32 -> 16 columns, BVOrthogonalize of 16 columns per
+    block type, the host generalized eigensolve of a 48 x 48 pencil, and an empty synchronisation."""
+    import time
+
+    import scipy.linalg as sl
+
+    n = args.lgrid ** 2
+    rng = np.random.default_rng(0)
+    Z = S.BV().create(n, 48)
+    W = S.BV().create(n, 48)
+    Z.setColumns(rng.standard_normal((n, 48)))
+    W.setColumns(rng.standard_normal((n, 48)))
+    P16 = S.BV().create(n, 16)
+    Q = rng.standard_normal((48, 16))
+    out = []
+
+    def timed(name, fn, calls=20):
+        fn()
+        best = None
+        for _ in range(args.reps):
+            t0 = time.perf_counter()
+            for _ in range(calls):
+                fn()
+            torch.cuda.synchronize()
+            dt = (time.perf_counter() - t0) / calls * 1e3
+            best = dt if best is None else min(best, dt)
+        out.append({"op": name, "n": n, "ms_per_call": round(best, 4)})
+
+    timed("BVDot 48 x 48", lambda: W.dot(Z))
+    Z.setActiveColumns(16, 48)
+    timed("BVMult 32 -> 16 (beta 0)", lambda: P16.mult(1.0, 0.0, Z, Q))
+    timed("BVMult 32 -> 16 (beta 1)", lambda: P16.mult(1.0, 1.0, Z, Q))
+    Z.setActiveColumns(0, 48)
+    for name, t in (("gs", S.BV.OrthogBlockType.GS), ("chol", S.BV.OrthogBlockType.CHOL),
+                    ("svqb", S.BV.OrthogBlockType.SVQB)):
+        R = S.BV().create(n, 16)
+        R.setColumns(rng.standard_normal((n, 16)))
+        R.setOrthogonalizationBlock(t)
+        timed(f"BVOrthogonalize 16 columns ({name})", lambda: R.orthogonalize(16))
+        R.destroy()
+    A = rng.standard_normal((48, 48))
+    A = A + A.T
+    B = rng.standard_normal((48, 48))
+    B = B @ B.T + 48 * np.eye(48)
+    timed("host dsygvd 48 x 48 (scipy)", lambda: sl.eigh(A, B, driver="gvd"))
+    timed("empty stream synchronisation", lambda: torch.cuda.synchronize())
+    return out
+
+
 def cross(args, torch):
     """A x and A^T z of the power-law rectangular matrix (FP32 values), each timed alone with L2
     flushed, plus the A^T A shell."""
@@ -236,7 +320,11 @@ def multinplace(args, torch):
 
 def main():
     p = argparse.ArgumentParser()
-    p.add_argument("kernel", choices=["gs", "spmv", "spmm", "mixed", "multinplace", "cross", "batched", "all"])
+    p.add_argument("kernel", choices=["gs", "spmv", "spmm", "mixed", "multinplace", "cross", "batched", "lobpcg",
+                                      "lobpcg_ops", "all"])
+    p.add_argument("--lgrid", type=int, default=512, help="lobpcg: side of the 2-D diffusion grid")
+    p.add_argument("--block", nargs="+", default=["gs", "chol", "svqb"], help="lobpcg: block orthogonalizations")
+    p.add_argument("--phases", action="store_true", help="lobpcg: also a run with per-phase times")
     p.add_argument("--restarts", type=int, default=3, help="mixed: restarts of the FP32-basis phase")
     p.add_argument("--sweeps", type=int, default=1, help="mixed: refinement sweeps")
     p.add_argument("--nb", type=int, default=48, help="columns of the BVMatMult block")
@@ -263,6 +351,9 @@ def main():
                 print(json.dumps(gs(args, torch)), flush=True)
         elif k == "batched":
             print(json.dumps(batched(args, torch)), flush=True)
+        elif k in ("lobpcg", "lobpcg_ops"):
+            for line in (lobpcg if k == "lobpcg" else lobpcg_ops)(args, torch):
+                print(json.dumps(line), flush=True)
         elif k == "cross":
             for line in cross(args, torch):
                 print(json.dumps(line), flush=True)

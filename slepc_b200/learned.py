@@ -39,11 +39,13 @@ def init_params(N, width, modes, layers, hidden, nout, seed=0):
     return np.concatenate([p.ravel() for p in parts]).astype(np.float32)
 
 
-def solve_lowest(S, csr, nev=16, tol=1e-8, X0=None, max_it=100000):
+def solve_lowest(S, csr, nev=16, tol=1e-8, X0=None, max_it=100000, orthog_block=None, stats=False, timing=False):
     """The plain solver for the family: LOBPCG, smallest real, Jacobi preconditioner, block nev,
     optional initial block X0 (n x k), iteration cap max_it (LOBPCG's default cap, max(100,
-    2n/ncv), stops long before these operators converge).  Returns values, vectors (n x nconv),
-    iterations, seconds."""
+    2n/ncv), stops long before these operators converge), optional BVOrthogBlockType of the
+    blocks (S.BV.OrthogBlockType; Gram-Schmidt when None).  Returns values, vectors (n x nconv),
+    iterations, seconds, and the solver's counters when stats is set (with per-phase times when
+    timing is set; the phase edges then synchronise the stream)."""
     A = S.Mat().createAIJ(csr)
     E = S.EPS().create()
     E.setOperators(A)
@@ -53,6 +55,10 @@ def solve_lowest(S, csr, nev=16, tol=1e-8, X0=None, max_it=100000):
     E.setDimensions(nev, 0)
     E.setTolerances(tol, max_it)
     E.setPreconditioner(S.EPS.PCType.JACOBI)
+    if orthog_block is not None:
+        E.setBVOrthogonalizationBlock(orthog_block)
+    if timing:
+        E.setTiming(True)
     if X0 is not None:
         E.setInitialSpace(X0)
     t0 = time.perf_counter()
@@ -63,6 +69,8 @@ def solve_lowest(S, csr, nev=16, tol=1e-8, X0=None, max_it=100000):
     out = {"vals": np.array([p[0] for p in pairs]), "X": np.stack([p[1] for p in pairs], axis=1) if pairs else None,
            "its": E.getIterationNumber(), "reason": E.getConvergedReason(), "nconv": nconv, "seconds": secs,
            "max_error": max((E.computeError(i) for i in range(min(nconv, nev))), default=None)}
+    if stats:
+        out["stats"] = E.getStats()
     E.destroy()
     A.destroy()
     return out

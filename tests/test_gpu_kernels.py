@@ -276,3 +276,27 @@ def test_mat_lanczos_vs_oracle_three_term(b200, oracle_mod):
     np.testing.assert_allclose(beta_v[:30], bo, rtol=1e-8)
     Vg = bv.getColumns(31)
     assert np.abs(Vg.T @ Vg - np.eye(31)).max() < 1e-13
+
+
+@pytest.mark.parametrize("nx,ny", [(48, 16), (7, 33), (250, 120)])
+def test_bv_mult_alpha_beta_vs_numpy(b200, nx, ny):
+    """BVMult Y = alpha X Q + beta Y: the row-panel tensor-core product and the column kernel it
+    falls back to when X's panel and Q do not fit shared memory (250 x 120) against numpy in FP64."""
+    rng = np.random.default_rng(nx * 1000 + ny)
+    n = 20011
+    X0 = rng.standard_normal((n, nx))
+    Y0 = rng.standard_normal((n, ny))
+    Q = rng.standard_normal((nx, ny))
+    X = b200.BV().create(n, nx)
+    Y = b200.BV().create(n, ny)
+    X.setColumns(X0)
+    Y.setColumns(Y0)
+    Y.mult(-0.7, 1.3, X, Q)
+    ref = -0.7 * X0 @ Q + 1.3 * Y0
+    got = Y.getColumns()
+    assert np.abs(got - ref).max() <= 1e-13 * np.abs(X0).max() * np.abs(Q).max() * nx
+    Y.setColumns(Y0)
+    Y.mult(1.0, 0.0, X, Q)
+    assert np.abs(Y.getColumns() - X0 @ Q).max() <= 1e-13 * np.abs(X0).max() * np.abs(Q).max() * nx
+    X.destroy()
+    Y.destroy()

@@ -210,65 +210,101 @@ __global__ void dot_partial_kernel(const double *__restrict__ X, int ldx, int nx
   }
 }
 
-// Gram block M = Y^T X for up to 64 x 64 column pairs per CTA row (blockIdx.y, blockIdx.z select the
-// 64-column blocks of Y and X): the CTA's rows are staged in 32-row panels in shared memory and
-// thread (ty, tx) of a 16 x 16 layout accumulates the 4 x 4 pairs (4ty+a, 4tx+b) in row order.
+// Gram block M = Y^T X for up to T x T column pairs per CTA row, T = 16 TM (blockIdx.y, blockIdx.z
+// select the T-column blocks of Y and X; TM is chosen from the block width so that narrow blocks do
+// not pay for padding).  The CTA's rows are staged in 32-row panels in shared memory, the next panel
+// is loaded into registers while the current one is consumed, and thread (ty, tx) of a 16 x 16 layout
+// accumulates the TM x TM pairs (TM ty + a, TM tx + b) in row order.
 // partial[blk * (nx*ny) + (i + j*ny)] as dot_partial_kernel writes it.
 constexpr int kGramRows = 32;
+template <int TM>
 __global__ void __launch_bounds__(256) gram_partial_kernel(const double *__restrict__ X, int ldx, int nx,
                                                            const double *__restrict__ Y, int ldy, int ny, int n,
                                                            double *partial) {
-  __shared__ double Xs[kGramRows][64 + 1], Ys[kGramRows][64 + 1];
+  constexpr int T = 16 * TM;
+  constexpr int kLoads = kGramRows * T / 256;  // elements of each operand a thread stages per panel
+  __shared__ double Xs[kGramRows][T + 1], Ys[kGramRows][T + 1];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int y0 = blockIdx.y * 64, x0 = blockIdx.z * 64;
-  const int cy = min(64, ny - y0), cx = min(64, nx - x0);
+  const int y0 = blockIdx.y * T, x0 = blockIdx.z * T;
+  const int cy = min(T, ny - y0), cx = min(T, nx - x0);
   const long long rows_per = (n + gridDim.x - 1) / gridDim.x;
   const long long r0 = (long long)blockIdx.x * rows_per;
   const long long r1 = min((long long)n, r0 + rows_per);
-  double acc[4][4];
+  double acc[TM][TM];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < TM; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-  for (long long p0 = r0; p0 < r1; p0 += kGramRows) {
-    const int pr = (int)min((long long)kGramRows, r1 - p0);
-    // column-major loads: 32 consecutive rows of one column per warp
-    for (int e = threadIdx.x; e < kGramRows * 64; e += 256) {
+    for (int b = 0; b < TM; ++b) acc[a][b] = 0.0;
+  double xr[kLoads], yr[kLoads];
+  // column-major loads: 32 consecutive rows of one column per warp
+  auto load = [&](long long p0, int pr) {
+#pragma unroll
+    for (int u = 0; u < kLoads; ++u) {
+      const int e = threadIdx.x + 256 * u;
       const int r = e % kGramRows, c = e / kGramRows;
-      Xs[r][c] = (r < pr && c < cx) ? X[(size_t)(x0 + c) * ldx + p0 + r] : 0.0;
-      Ys[r][c] = (r < pr && c < cy) ? Y[(size_t)(y0 + c) * ldy + p0 + r] : 0.0;
+      xr[u] = (r < pr && c < cx) ? X[(size_t)(x0 + c) * ldx + p0 + r] : 0.0;
+      yr[u] = (r < pr && c < cy) ? Y[(size_t)(y0 + c) * ldy + p0 + r] : 0.0;
+    }
+  };
+  long long p0 = r0;
+  int pr = p0 < r1 ? (int)min((long long)kGramRows, r1 - p0) : 0;
+  if (pr > 0) load(p0, pr);
+  while (pr > 0) {
+#pragma unroll
+    for (int u = 0; u < kLoads; ++u) {
+      const int e = threadIdx.x + 256 * u;
+      const int r = e % kGramRows, c = e / kGramRows;
+      Xs[r][c] = xr[u];
+      Ys[r][c] = yr[u];
     }
     __syncthreads();
+    const long long pn = p0 + kGramRows;
+    const int prn = pn < r1 ? (int)min((long long)kGramRows, r1 - pn) : 0;
+    if (prn > 0) load(pn, prn);  // in flight while this panel is consumed
     for (int r = 0; r < pr; ++r) {
-      double yv[4], xv[4];
+      double yv[TM], xv[TM];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) yv[a] = Ys[r][4 * ty + a];
+      for (int a = 0; a < TM; ++a) yv[a] = Ys[r][TM * ty + a];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) xv[b] = Xs[r][4 * tx + b];
+      for (int b = 0; b < TM; ++b) xv[b] = Xs[r][TM * tx + b];
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < TM; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(yv[a], xv[b], acc[a][b]);
+        for (int b = 0; b < TM; ++b) acc[a][b] = fma(yv[a], xv[b], acc[a][b]);
     }
     __syncthreads();
+    p0 = pn;
+    pr = prn;
   }
   const int npairs = nx * ny;
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < TM; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int i = 4 * ty + a, j = 4 * tx + b;
+    for (int b = 0; b < TM; ++b) {
+      const int i = TM * ty + a, j = TM * tx + b;
       if (i < cy && j < cx) partial[(size_t)blockIdx.x * npairs + (y0 + i) + (size_t)(x0 + j) * ny] = acc[a][b];
     }
 }
 
-__global__ void dot_final_kernel(const double *__restrict__ partial, int nblocks, int nx, int ny, double *M, int ldm) {
+// M(i, j) = the sum over the row blocks of the partial sums.  A CTA takes 32 consecutive pairs (one
+// per lane, so each load of a row block's partials is one coalesced 256-byte line); its 8 warps split
+// the row blocks (warp g sums blocks g, g + 8, ...) and the 8 sums are added in a fixed order.
+__global__ void __launch_bounds__(256) dot_final_kernel(const double *__restrict__ partial, int nblocks, int nx,
+                                                        int ny, double *M, int ldm) {
+  __shared__ double red[8][33];
   const int npairs = nx * ny;
-  for (int pr = blockIdx.x * blockDim.x + threadIdx.x; pr < npairs; pr += gridDim.x * blockDim.x) {
-    double acc = 0.0;
-    for (int b = 0; b < nblocks; ++b) acc += partial[(size_t)b * npairs + pr];
-    const int i = pr % ny, j = pr / ny;
-    M[i + (size_t)j * ldm] = acc;
+  const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+  const int pr = blockIdx.x * 32 + lane;
+  double acc = 0.0;
+  if (pr < npairs)
+    for (int b = g; b < nblocks; b += 8) acc += partial[(size_t)b * npairs + pr];
+  red[g][lane] = acc;
+  __syncthreads();
+  if (g == 0 && pr < npairs) {
+    double t = red[0][lane];
+#pragma unroll
+    for (int q = 1; q < 8; ++q) t += red[q][lane];
+    M[(pr % ny) + (size_t)(pr / ny) * ldm] = t;
   }
 }
 
@@ -688,13 +724,21 @@ cudaError_t dot_launch(const double *X, int ldx, int nx, const double *Y, int ld
   if (blocks < 1) return cudaErrorInvalidValue;
   if (npairs >= 64) {
     // register-tiled Gram blocks: both blocks of columns read once per CTA row range
-    const dim3 grid(blocks, (ny + 63) / 64, (nx + 63) / 64);
-    gram_partial_kernel<<<grid, 256, 0, stream>>>(X, ldx, nx, Y, ldy, ny, n, work);
+    const int w = nx > ny ? nx : ny;
+    const int tm = w > 48 ? 4 : (w + 15) / 16;
+    const int T = 16 * tm;
+    const dim3 grid(blocks, (ny + T - 1) / T, (nx + T - 1) / T);
+    switch (tm) {
+      case 1: gram_partial_kernel<1><<<grid, 256, 0, stream>>>(X, ldx, nx, Y, ldy, ny, n, work); break;
+      case 2: gram_partial_kernel<2><<<grid, 256, 0, stream>>>(X, ldx, nx, Y, ldy, ny, n, work); break;
+      case 3: gram_partial_kernel<3><<<grid, 256, 0, stream>>>(X, ldx, nx, Y, ldy, ny, n, work); break;
+      default: gram_partial_kernel<4><<<grid, 256, 0, stream>>>(X, ldx, nx, Y, ldy, ny, n, work); break;
+    }
   } else {
     dot_partial_kernel<<<blocks, 256, 0, stream>>>(X, ldx, nx, Y, ldy, ny, n, work);
   }
   count_launch();
-  dot_final_kernel<<<(npairs + 255) / 256, 256, 0, stream>>>(work, blocks, nx, ny, M, ldm);
+  dot_final_kernel<<<(npairs + 31) / 32, 256, 0, stream>>>(work, blocks, nx, ny, M, ldm);
   count_launch();
   return cudaGetLastError();
 }

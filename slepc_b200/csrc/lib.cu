@@ -913,14 +913,16 @@ static b200_status bv_orthogonalize_gram(b200_bv bv, double *R, int ldr) {
   const int l = bv->l, k = bv->k, nc = k - l, n = bv->n, ld = bv->ld;
   if (nc <= 0) return B200_OK;
   const size_t nC = (size_t)l * nc, nG = (size_t)nc * nc;
-  B200_CHECK(bv_reserve(bv, nC + nG, std::max(nC, nG) * num_sms_host()));
+  const int cps_c = dot_ctas_per_sm(nc, l), cps_g = dot_ctas_per_sm(nc, nc);
+  B200_CHECK(bv_reserve(bv, nC + nG, std::max(nC * cps_c, nG * cps_g) * num_sms_host()));
   cudaStream_t s = bv->stream;
   double *Cdev = bv->qbuf, *Gdev = bv->qbuf + nC;
   if (l > 0) {
-    B200_CUDA_CHECK(dot_launch(col(bv, l), ld, nc, bv->V, ld, l, n, Cdev, l, bv->red, bv->red_len, s));
+    B200_CUDA_CHECK(dot_launch(col(bv, l), ld, nc, bv->V, ld, l, n, Cdev, l, bv->red, bv->red_len, s, cps_c));
     B200_CUDA_CHECK(mult_launch(col(bv, l), ld, bv->V, ld, n, l, nc, Cdev, l, -1.0, 1.0, s));
   }
-  B200_CUDA_CHECK(dot_launch(col(bv, l), ld, nc, col(bv, l), ld, nc, n, Gdev, nc, bv->red, bv->red_len, s));
+  B200_CUDA_CHECK(
+      dot_launch(col(bv, l), ld, nc, col(bv, l), ld, nc, n, Gdev, nc, bv->red, bv->red_len, s, cps_g));
   B200_CUDA_CHECK(cudaMemcpyAsync(bv->hpin, bv->qbuf, sizeof(double) * (nC + nG), cudaMemcpyDeviceToHost, s));
   B200_CUDA_CHECK(cudaStreamSynchronize(s));
   std::vector<double> C(bv->hpin, bv->hpin + nC), G(bv->hpin + nC, bv->hpin + nC + nG), Rf(nG, 0.0), S(nG, 0.0);
@@ -1072,9 +1074,10 @@ extern "C" b200_status b200_bv_dot(b200_bv X, b200_bv Y, double *M, int ldm) {
   const int nx = X->k - X->l, ny = Y->k - Y->l;
   B200_ARG_CHECK(ldm >= Y->k, "M leading dimension too small");
   if (nx <= 0 || ny <= 0) return B200_OK;
-  B200_CHECK(bv_reserve(X, (size_t)nx * ny, (size_t)nx * ny * num_sms_host()));
+  const int cps = dot_ctas_per_sm(nx, ny);
+  B200_CHECK(bv_reserve(X, (size_t)nx * ny, (size_t)nx * ny * num_sms_host() * cps));
   B200_CUDA_CHECK(dot_launch(col(X, X->l), X->ld, nx, col(Y, Y->l), Y->ld, ny, X->n, X->qbuf, ny, X->red, X->red_len,
-                             X->stream));
+                             X->stream, cps));
   B200_CUDA_CHECK(
       cudaMemcpyAsync(X->hpin, X->qbuf, sizeof(double) * (size_t)nx * ny, cudaMemcpyDeviceToHost, X->stream));
   B200_CUDA_CHECK(cudaStreamSynchronize(X->stream));

@@ -300,3 +300,24 @@ def test_bv_mult_alpha_beta_vs_numpy(b200, nx, ny):
     assert np.abs(Y.getColumns() - X0 @ Q).max() <= 1e-13 * np.abs(X0).max() * np.abs(Q).max() * nx
     X.destroy()
     Y.destroy()
+
+
+@pytest.mark.parametrize("nx,ny", [(16, 16), (20, 9), (48, 48), (33, 40), (64, 64), (130, 70)])
+def test_bv_dot_gram_tiles_vs_numpy(b200, nx, ny):
+    """BVDot M = Y^T X through every Gram tile width (16, 32, 48, 64 columns, several tiles per
+    side) and both row-block counts against numpy in FP64."""
+    rng = np.random.default_rng(nx * 7 + ny)
+    n = 50021
+    X0 = rng.standard_normal((n, nx))
+    Y0 = rng.standard_normal((n, ny))
+    X = b200.BV().create(n, nx)
+    Y = b200.BV().create(n, ny)
+    X.setColumns(X0)
+    Y.setColumns(Y0)
+    M = X.dot(Y)
+    ref = Y0.T @ X0
+    assert M.shape == ref.shape
+    assert np.abs(M - ref).max() <= 1e-13 * n
+    np.testing.assert_array_equal(M, X.dot(Y))  # deterministic
+    X.destroy()
+    Y.destroy()

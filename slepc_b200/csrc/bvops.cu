@@ -210,37 +210,33 @@ __global__ void dot_partial_kernel(const double *__restrict__ X, int ldx, int nx
   }
 }
 
-// Gram block M = Y^T X for up to 64 x 64 column pairs per CTA row (blockIdx.y, blockIdx.z select the
-// 64-column blocks of Y and X) on the FP64 tensor cores, mma.sync.m8n8k4.f64 with the rows as the
-// reduction dimension: lane (g, t) supplies A(g, t) = Y(k + t, i0 + g) and B(t, g) = X(k + t, j0 + g)
-// from 32-row panels staged column by column in shared memory (stride 36 doubles: a half-warp's
-// fragment loads fall in distinct banks) and accumulates M(i0 + g, j0 + 2t .. 2t + 1).  The block's
-// 8 x 8 tiles are dealt to the warps; when there are fewer tiles than warps, the warps split each
-// panel's k-steps instead and their sums are added in a fixed order at the end.  The next panel is
-// loaded into registers while the current one is consumed.
+// Gram block M = Y^T X for up to T x T column pairs per CTA row, T = 16 TM (blockIdx.y, blockIdx.z
+// select the T-column blocks of Y and X; TM is chosen from the block width so that narrow blocks do
+// not pay for padding).  The CTA's rows are staged in 32-row panels in shared memory, the next panel
+// is loaded into registers while the current one is consumed, and thread (ty, tx) of a 16 x 16 layout
+// accumulates the TM x TM pairs (TM ty + a, TM tx + b) in row order.
 // partial[blk * (nx*ny) + (i + j*ny)] as dot_partial_kernel writes it.
 constexpr int kGramRows = 32;
-constexpr int kGramStride = kGramRows + 4;
-__global__ void __launch_bounds__(256) gram_dmma_kernel(const double *__restrict__ X, int ldx, int nx,
-                                                        const double *__restrict__ Y, int ldy, int ny, int n,
-                                                        double *partial) {
-  constexpr int kLoads = kGramRows * 64 / 256;  // elements of each operand a thread stages per panel
-  __shared__ __align__(16) double Xs[64 * kGramStride], Ys[64 * kGramStride];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  const int y0 = blockIdx.y * 64, x0 = blockIdx.z * 64;
-  const int cy = min(64, ny - y0), cx = min(64, nx - x0);
-  const int nty = (cy + 7) >> 3, ntx = (cx + 7) >> 3, ntiles = nty * ntx;
-  // warps per k-group (a power of two >= the tile count, at most 8) and the number of k-groups
-  const int wpg = ntiles >= 5 ? 8 : ntiles >= 3 ? 4 : ntiles == 2 ? 2 : 1;
-  const int ngrp = 8 / wpg, grp = warp / wpg, lw = warp % wpg;
+template <int TM>
+__global__ void __launch_bounds__(256) gram_partial_kernel(const double *__restrict__ X, int ldx, int nx,
+                                                           const double *__restrict__ Y, int ldy, int ny, int n,
+                                                           double *partial) {
+  constexpr int T = 16 * TM;
+  constexpr int kLoads = kGramRows * T / 256;  // elements of each operand a thread stages per panel
+  __shared__ double Xs[kGramRows][T + 1], Ys[kGramRows][T + 1];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int y0 = blockIdx.y * T, x0 = blockIdx.z * T;
+  const int cy = min(T, ny - y0), cx = min(T, nx - x0);
   const long long rows_per = (n + gridDim.x - 1) / gridDim.x;
   const long long r0 = (long long)blockIdx.x * rows_per;
   const long long r1 = min((long long)n, r0 + rows_per);
-  double acc[8][2];
+  double acc[TM][TM];
 #pragma unroll
-  for (int u = 0; u < 8; ++u) acc[u][0] = acc[u][1] = 0.0;
+  for (int a = 0; a < TM; ++a)
+#pragma unroll
+    for (int b = 0; b < TM; ++b) acc[a][b] = 0.0;
   double xr[kLoads], yr[kLoads];
+  // column-major loads: 32 consecutive rows of one column per warp
   auto load = [&](long long p0, int pr) {
 #pragma unroll
     for (int u = 0; u < kLoads; ++u) {
@@ -258,61 +254,36 @@ __global__ void __launch_bounds__(256) gram_dmma_kernel(const double *__restrict
     for (int u = 0; u < kLoads; ++u) {
       const int e = threadIdx.x + 256 * u;
       const int r = e % kGramRows, c = e / kGramRows;
-      Xs[c * kGramStride + r] = xr[u];  // rows past pr and columns past cx/cy hold zeros
-      Ys[c * kGramStride + r] = yr[u];
+      Xs[r][c] = xr[u];
+      Ys[r][c] = yr[u];
     }
     __syncthreads();
     const long long pn = p0 + kGramRows;
     const int prn = pn < r1 ? (int)min((long long)kGramRows, r1 - pn) : 0;
     if (prn > 0) load(pn, prn);  // in flight while this panel is consumed
-    for (int k0 = 4 * grp; k0 < kGramRows; k0 += 4 * ngrp) {
+    for (int r = 0; r < pr; ++r) {
+      double yv[TM], xv[TM];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int tile = lw + wpg * u;
-        if (tile < ntiles) {
-          const int ti = tile / ntx, tj = tile - ti * ntx;
-          const double a = Ys[(8 * ti + g) * kGramStride + k0 + t];
-          const double b = Xs[(8 * tj + g) * kGramStride + k0 + t];
-          dmma_8x8x4(acc[u], a, b);
-        }
-      }
+      for (int a = 0; a < TM; ++a) yv[a] = Ys[r][TM * ty + a];
+#pragma unroll
+      for (int b = 0; b < TM; ++b) xv[b] = Xs[r][TM * tx + b];
+#pragma unroll
+      for (int a = 0; a < TM; ++a)
+#pragma unroll
+        for (int b = 0; b < TM; ++b) acc[a][b] = fma(yv[a], xv[b], acc[a][b]);
     }
     __syncthreads();
     p0 = pn;
     pr = prn;
   }
   const int npairs = nx * ny;
-  auto store = [&](int tile, int e, double v) {
-    const int ti = tile / ntx, tj = tile - ti * ntx;
-    const int i = 8 * ti + g, j = 8 * tj + 2 * t + e;
-    if (i < cy && j < cx) partial[(size_t)blockIdx.x * npairs + (y0 + i) + (size_t)(x0 + j) * ny] = v;
-  };
-  if (ngrp == 1) {
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int tile = lw + wpg * u;
-      if (tile < ntiles) {
-        store(tile, 0, acc[u][0]);
-        store(tile, 1, acc[u][1]);
-      }
-    }
-    return;
-  }
-  // fewer than five tiles: one tile per warp of each k-group; add the groups' sums in order
-  double *red = Xs;  // ngrp x wpg x 64 <= 512 doubles
-  if (lw < ntiles) {
-    red[(grp * wpg + lw) * 64 + 2 * lane] = acc[0][0];
-    red[(grp * wpg + lw) * 64 + 2 * lane + 1] = acc[0][1];
-  }
-  __syncthreads();
-  if (grp == 0 && lw < ntiles) {
+  for (int a = 0; a < TM; ++a)
 #pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      double v = red[lw * 64 + 2 * lane + e];
-      for (int q = 1; q < ngrp; ++q) v += red[(q * wpg + lw) * 64 + 2 * lane + e];
-      store(lw, e, v);
+    for (int b = 0; b < TM; ++b) {
+      const int i = TM * ty + a, j = TM * tx + b;
+      if (i < cy && j < cx) partial[(size_t)blockIdx.x * npairs + (y0 + i) + (size_t)(x0 + j) * ny] = acc[a][b];
     }
-  }
 }
 
 // M(i, j) = the sum over the row blocks of the partial sums.  A CTA takes 32 consecutive pairs (one
@@ -752,9 +723,17 @@ cudaError_t dot_launch(const double *X, int ldx, int nx, const double *Y, int ld
   if (blocks * npairs > work_len) blocks = work_len / npairs;
   if (blocks < 1) return cudaErrorInvalidValue;
   if (npairs >= 64) {
-    // Gram blocks on the FP64 tensor cores: both blocks of columns read once per CTA row range
-    const dim3 grid(blocks, (ny + 63) / 64, (nx + 63) / 64);
-    gram_dmma_kernel<<<grid, 256, 0, stream>>>(X, ldx, nx, Y, ldy, ny, n, work);
+    // register-tiled Gram blocks: both blocks of columns read once per CTA row range
+    const int w = nx > ny ? nx : ny;
+    const int tm = w > 48 ? 4 : (w + 15) / 16;
+    const int T = 16 * tm;
+    const dim3 grid(blocks, (ny + T - 1) / T, (nx + T - 1) / T);
+    switch (tm) {
+      case 1: gram_partial_kernel<1><<<grid, 256, 0, stream>>>(X, ldx, nx, Y, ldy, ny, n, work); break;
+      case 2: gram_partial_kernel<2><<<grid, 256, 0, stream>>>(X, ldx, nx, Y, ldy, ny, n, work); break;
+      case 3: gram_partial_kernel<3><<<grid, 256, 0, stream>>>(X, ldx, nx, Y, ldy, ny, n, work); break;
+      default: gram_partial_kernel<4><<<grid, 256, 0, stream>>>(X, ldx, nx, Y, ldy, ny, n, work); break;
+    }
   } else {
     dot_partial_kernel<<<blocks, 256, 0, stream>>>(X, ldx, nx, Y, ldy, ny, n, work);
   }

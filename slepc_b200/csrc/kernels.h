@@ -198,11 +198,10 @@ cudaError_t mult_launch(double *Y, int ldy, const double *X, int ldx, int n, int
 // y = beta*y + alpha*X(:,0:k) q
 cudaError_t multvec_launch(const double *X, int ldx, int n, int k, const double *q, double alpha, double beta, double *y,
                            cudaStream_t stream);
-// Row blocks per SM of BVDot and the block orthogonalisations: 2 (the Gram kernel's resident CTAs
-// per SM) for blocks of up to 64 x 64 pairs, one CTA column of Gram tiles, so the rows must supply
-// the parallelism; 1 above that (the tiles do, and the partial sums would take npairs * 2 * SMs
-// doubles).
-inline int dot_ctas_per_sm(int nx, int ny) { return (long long)nx * ny <= 64 * 64 ? 2 : 1; }
+// Row blocks per SM of BVDot and the block orthogonalisations: 4 for blocks of up to 64 x 64 pairs
+// (one CTA column of Gram tiles, so the rows must supply the parallelism), 1 above that (the tiles
+// do, and the partial sums would take npairs * 4 * SMs doubles).
+inline int dot_ctas_per_sm(int nx, int ny) { return (long long)nx * ny <= 64 * 64 ? 4 : 1; }
 // M(0:ny,0:nx) = Y(:,0:ny)^T X(:,0:nx), M column-major ldm (device), deterministic for a given
 // ctas_per_sm (row blocks per SM of the partial sums).
 cudaError_t dot_launch(const double *X, int ldx, int nx, const double *Y, int ldy, int ny, int n, double *M, int ldm,

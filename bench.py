@@ -228,26 +228,12 @@ def run_b200(args):
 
     import slepc_b200 as S
 
+    from slepc_b200.ranks import Ranks
+
     rank, local_rank, world = dist_env()
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks("nccl", timeout_s=600)  # replicas: barrier and max over ranks, no data-path collective
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     csr, n, v0 = workload(args.grid)
     nnz = int(csr[0][-1])
@@ -372,8 +358,7 @@ def run_b200(args):
         print(json.dumps(line))
     E.destroy()
     A.destroy()
-    if dist is not None:
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 
@@ -513,26 +498,12 @@ def run_b200_cross(args):
 
     import slepc_b200 as S
 
+    from slepc_b200.ranks import Ranks
+
     rank, local_rank, world = dist_env()
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks("nccl", timeout_s=600)  # replicas: barrier and max over ranks, no data-path collective
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     m, n = args.rows, args.cols
     csr, v0 = cross_workload(args)
@@ -631,8 +602,7 @@ def run_b200_cross(args):
         print(json.dumps(line))
     E.destroy()
     A.destroy()
-    if dist is not None:
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 
@@ -713,26 +683,12 @@ def run_b200_batched(args):
 
     import slepc_b200 as S
 
+    from slepc_b200.ranks import Ranks
+
     rank, local_rank, world = dist_env()
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks("nccl", timeout_s=600)  # replicas: barrier and max over ranks, no data-path collective
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     B, v0 = batched_workload(args)
 
@@ -810,8 +766,7 @@ def run_b200_batched(args):
                 "cpu_baseline": cpu}
         print(json.dumps(line))
     E.destroy()
-    if dist is not None:
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 
@@ -840,8 +795,11 @@ def run_b200_learned(args):
     import slepc_b200 as S
     from slepc_b200 import learned as LN
 
+    from slepc_b200.ranks import Ranks
+
     rank, local_rank, world = dist_env()
     torch.cuda.set_device(local_rank)
+    ranks = Ranks("nccl", timeout_s=3600)  # replicas: each rank trains and evaluates its own copy
     N, nev = args.learn_grid, args.learn_nev
     t0 = time.perf_counter()
     F, T, its_train = LN.dataset(S, N, range(args.train_fields), nev)
@@ -854,7 +812,8 @@ def run_b200_learned(args):
     hist = LN.train(op, Fd, Td, epochs=args.epochs, batch=8, lr=2e-3, lr_final=2e-4)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
-    seeds = list(range(EVAL_SEED0, EVAL_SEED0 + args.eval_fields))
+    # held-out fields: each rank evaluates its own (weak scaling)
+    seeds = list(range(EVAL_SEED0 + rank * args.eval_fields, EVAL_SEED0 + (rank + 1) * args.eval_fields))
     probs = [P.diffusion_problem(N, sd) for sd in seeds]
     feats = torch.from_numpy(np.stack([LN.features(k) for _, k, _ in probs])).cuda()
     launches0 = None
@@ -870,6 +829,8 @@ def run_b200_learned(args):
     for _ in range(args.warmup):
         step(True)
     torch.cuda.synchronize()
+    ranks.barrier()
+    torch.cuda.synchronize()
     clocks = ClockSampler(local_rank)
     clocks.start()
     launches0 = S.kernel_launch_count()
@@ -879,15 +840,17 @@ def run_b200_learned(args):
         res_l = step(True)
     ev1.record()
     torch.cuda.synchronize()
+    ranks.barrier()
+    torch.cuda.synchronize()
     clk = clocks.stop()
     launches = S.kernel_launch_count() - launches0
-    ms_step = ev0.elapsed_time(ev1) / args.steps
+    ms_step = ranks.max(ev0.elapsed_time(ev1) / args.steps)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     res_r = step(False)
     e1.record()
     torch.cuda.synchronize()
-    ms_random = e0.elapsed_time(e1)
+    ms_random = ranks.max(e0.elapsed_time(e1))
     # end to end: host fields in, host eigenpairs out (features up, network, block down, solve, pairs down)
     t0 = time.perf_counter()
     for _ in range(args.steps):
@@ -895,13 +858,13 @@ def run_b200_learned(args):
         blocks = LN.predict(op, hf.cuda(non_blocking=True))
         for i, (csr, _, _) in enumerate(probs):
             LN.solve_lowest(S, csr, nev, X0=blocks[i].T.astype(np.float64))
-    e2e_s = (time.perf_counter() - t0) / args.steps
+    e2e_s = ranks.max((time.perf_counter() - t0) / args.steps)
     captured = [LN.captured(r["X"], b.T.astype(np.float64)) for r, b in zip(res_r, LN.predict(op, feats))]
     its_l = [r["its"] for r in res_l]
     its_r = [r["its"] for r in res_r]
     ok = all(r["nconv"] >= nev and r["max_error"] <= 1e-8 for r in res_l + res_r)
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle
 
         threads = os.cpu_count() or 1
@@ -933,6 +896,7 @@ def run_b200_learned(args):
                 "gpu_launches": int(launches), "clocks": clk, "cpu_baseline": cpu}
         print(json.dumps(line))
     op.destroy()
+    ranks.close()
     return 0
 
 
@@ -940,6 +904,8 @@ def main():
     args = parse()
     if args.workload == "learned":
         if args.impl == "reference":
+            if dist_env()[0] != 0:
+                return 0
             print(json.dumps({"impl": "reference", "unavailable": "the learned workload has no reference arm: SLEPc "
                               "has no learned start; its CPU baseline (oracle LOBPCG) is in the b200 line"}))
             return 0

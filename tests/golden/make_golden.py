@@ -13,6 +13,7 @@ Sources:
   src/sys/classes/bv/tests/output/test2_1.out         (test2.c, n=20 k=8, CGS)
   src/sys/classes/ds/tests/output/test2_1.out         (test2.c, DSHEP n=12, ld=n+2)
   src/sys/classes/bv/tests/output/test1_1_bv_type-svec.out (test1.c, n=10 k=5 l=3, -verbose)
+  src/sys/classes/bv/tests/output/test11_1.out, test11_6.out (test11.c, n=20 l=2 k=8, block types)
   src/eps/tutorials/X.bin, Ybus.bin                    (PETSc binary Vec and Mat read by ex31.c)
 """
 import json
@@ -104,6 +105,22 @@ def bv_test1(root):
             "X_after_multinplace_scale2": _vec_blocks(after_mip), "norm2_X0": n2, "norm_fro": fro}
 
 
+def bv_test11(root):
+    """test11.c: BVOrthogonalize of columns [0,l) and then [l,k) with each block type; the expected
+    output lists the checks that come out below 100 eps (without and with the R factor)."""
+    out = {}
+    for name, resid in (("test11_1.out", False), ("test11_6.out", True)):
+        txt = read(root, "src/sys/classes/bv/tests/output/" + name)
+        m = re.search(r"length (\d+), l=(\d+), k=(\d+)", txt)
+        out[name] = {"n": int(m.group(1)), "l": int(m.group(2)), "k": int(m.group(3)), "resid": resid,
+                     "below_100eps": re.findall(r"^\s+(.*?) < 100\*eps$", txt, flags=re.M)}
+    return {"source": "src/sys/classes/bv/tests/output/test11_1.out, test11_6.out",
+            "block_types": {"test11_1.out": ["gs", "chol", "tsqr", "tsqrchol", "svqb"],
+                            "test11_6.out": ["gs", "chol", "tsqr", "tsqrchol", "svqb"]},
+            "fixture": "X[i+j,j] = (3i+j-2)/(2(i+j+1)) for i<=n/2, i+j<n (test11.c:75-91)",
+            "outputs": out}
+
+
 def petsc_binary(root):
     """The two PETSc binary files of ex31 (a Vec and an AIJ Mat), decoded with the published
     layout (big-endian int32 header and indices, float64 values; values kept exactly as hex)."""
@@ -130,7 +147,8 @@ def petsc_binary(root):
 
 def main(root):
     fixtures = {"ex2_1.json": ex2(root), "bv_test2.json": bv_test2(root), "ds_test2.json": ds_test2(root),
-                "bv_test1.json": bv_test1(root), "petsc_binary.json": petsc_binary(root)}
+                "bv_test1.json": bv_test1(root), "petsc_binary.json": petsc_binary(root),
+                "bv_test11.json": bv_test11(root)}
     for name, obj in fixtures.items():
         with open(os.path.join(HERE, name), "w") as f:
             json.dump(obj, f, indent=1)

@@ -88,3 +88,33 @@ def test_oracle_sample_mode_stops(oracle_mod):
     r = oracle_mod.eps_solve(A, P.start_vector(A.shape[0], 0), nev=10, ncv=32,
                              which=oracle_mod.LARGEST_MAGNITUDE, max_restarts=2)
     assert r.restarts == 2 and r.reason == oracle_mod.ITERATING
+
+
+@pytest.mark.parametrize("block", ["chol", "svqb"])
+def test_bv_test11_block_orthogonalization_golden(oracle_mod, block):
+    """src/sys/classes/bv/tests/test11.c with -bv_orthog_block chol / svqb (-resid for test11_6):
+    columns [0,l) and then [l,k) orthogonalized, every check the expected output lists below
+    100 eps.  (Gram-Schmidt is pinned by test2; the TSQR types are not provided.)"""
+    g = H.golden("bv_test11.json")
+    eps = np.finfo(float).eps
+    t = {"chol": oracle_mod.ORTHOG_BLOCK_CHOL, "svqb": oracle_mod.ORTHOG_BLOCK_SVQB}[block]
+    for name, o in g["outputs"].items():
+        assert block in g["block_types"][name]
+        n, l, k = o["n"], o["l"], o["k"]
+        X = H.bv_test2_fixture(n, k)  # test11.c:75-91 fills X as test2.c does
+        Y = np.asfortranarray(X.copy())
+        R1 = oracle_mod.bv_orthogonalize_block(Y, 0, l, t)
+        R2 = oracle_mod.bv_orthogonalize_block(Y, l, k, t)
+        R = np.zeros((k, k))
+        R[:l, :l] = R1[:l, :l]
+        R[:, l:] = R2[:, l:]
+        M = Y.T @ Y - np.eye(k)
+        checks = {"Level of orthogonality of Q1": np.linalg.norm(M[:l, :l]),
+                  "Level of orthogonality of Q2": np.linalg.norm(M[l:, l:]),
+                  "Level of orthogonality of Q": np.linalg.norm(M)}
+        if o["resid"]:
+            checks["Residual ||X1-Q1*R11||"] = np.linalg.norm(X[:, :l] - Y[:, :l] @ R[:l, :l])
+            checks["Residual ||X-Q*R||"] = np.linalg.norm(X - Y @ R)
+        assert sorted(checks) == sorted(o["below_100eps"])
+        for label in o["below_100eps"]:
+            assert checks[label] < 100 * eps, (name, label, checks[label] / eps)

@@ -314,7 +314,7 @@ def multinplace(args, torch):
     ms /= args.reps
     algo = 8 * n * (k + e) + 8 * k * e
     flops = 2.0 * n * k * e
-    return {"kernel": "multinplace_kernel", "n": n, "k": k, "e-s": e, "ms": ms, "algorithmic_bytes": algo,
+    return {"kernel": "BVMultInPlace (panel_dmma_kernel)", "n": n, "k": k, "e-s": e, "ms": ms, "algorithmic_bytes": algo,
             "GBps": algo / (ms * 1e-3) / 1e9, "TFLOPs": flops / (ms * 1e-3) / 1e12}
 
 

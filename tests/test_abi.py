@@ -54,5 +54,10 @@ def test_entry_points_reject_bad_arguments(b200):
     # too many BV columns for the kernels
     assert L.b200_bv_create(100, 400, None, ctypes.byref(h)) == 1
     assert L.b200_eps_set_dimensions(None, 1, 0, 0) == 1
+    # block orthogonalization type on missing objects
+    assert L.b200_bv_set_orthog_block(None, 1) == 1
+    assert L.b200_eps_set_bv_orthog_block(None, 4) == 1
+    t = ctypes.c_int(-1)
+    assert L.b200_bv_get_orthog_block(None, ctypes.byref(t)) == 1
     with pytest.raises(b200.B200Error):
         b200._check(1)

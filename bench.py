@@ -15,8 +15,10 @@ Workload (one "step" = one full EPSSolve from the seeded start vector):
                     cores, on a bounded sample of the workload extrapolated
                     to the full solve.
 
-Multi-GPU (torchrun): every rank solves its own replica (the workload does
-not shard in this build); timings are the max over ranks.
+Multi-GPU (torchrun): every rank solves its own replica of the single-problem
+workloads; the batched workload is sharded by problem (each rank solves its
+contiguous share of the batch, no data-path collective).  Timings are the max
+over ranks.
 """
 import argparse
 import json
@@ -652,6 +654,27 @@ def batched_sample_index(args, B):
     return np.arange(0, args.nprob, step)[:args.cpu_sample]
 
 
+class BatchShard:
+    """The problems `idx` of a batch that one rank solves, with their start vectors."""
+
+    def __init__(self, B, v0, idx):
+        self.idx = list(idx)
+        self.B = B.subset(self.idx) if B is not None else None
+        self.v0 = B.rows_of(v0, self.idx) if (B is not None and v0 is not None) else None
+
+
+def batched_shard(B, v0, rank, world):
+    """Rank `rank` of `world` takes the contiguous range ranks.shard gives it (the whole batch at world 1)."""
+    from slepc_b200.ranks import shard
+
+    idx = shard(B.nprob, rank, world)
+    if world == 1:
+        s = BatchShard(None, None, idx)
+        s.B, s.v0 = B, v0
+        return s
+    return BatchShard(B, v0, idx)
+
+
 def run_reference_batched(args):
     rank, _, world = dist_env()
     if rank != 0:
@@ -683,14 +706,17 @@ def run_b200_batched(args):
 
     import slepc_b200 as S
 
-    from slepc_b200.ranks import Ranks
+    from slepc_b200.ranks import Ranks, shard
 
     rank, local_rank, world = dist_env()
     torch.cuda.set_device(local_rank)
-    ranks = Ranks("nccl", timeout_s=600)  # replicas: barrier and max over ranks, no data-path collective
+    ranks = Ranks("nccl", timeout_s=600)  # barrier, max and sum over ranks, no data-path collective
     barrier, max_over_ranks = ranks.barrier, ranks.max
 
-    B, v0 = batched_workload(args)
+    B_all, v0_all = batched_workload(args)
+    # the problems are independent: each rank solves its contiguous share of the batch
+    part = batched_shard(B_all, v0_all, rank, world)
+    B, v0 = part.B, part.v0
 
     def make():
         E = S.BatchEPS().create(B.ns, B.rowptr, B.colind, B.vals)
@@ -721,7 +747,11 @@ def run_b200_batched(args):
     launches = S.kernel_launch_count() - launches0
     ms_per_step = max_over_ranks(statistics.mean(dev_ms))
     ev, info, _ = E.getAll()
-    bytes_moved = E.getBytes()
+    bytes_moved = ranks.sum(E.getBytes())  # every rank's problems, over the slowest rank's time
+    all_converged = ranks.sum(float(np.all(info[:, 2] == 1))) == world
+    max_restarts = max_over_ranks(int(info[:, 1].max()) if len(info) else 0)
+    lanczos_total = ranks.sum(int(info[:, 3].sum()))
+    launches = int(ranks.sum(launches))
     peak, peak_kind = measured_peaks()
     achieved = bytes_moved / (ms_per_step * 1e-3) / 1e9
 
@@ -735,8 +765,8 @@ def run_b200_batched(args):
         ev2, info2, _ = E2.getAll()
         E2.destroy()
     e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
-    h2d = B.rowptr.nbytes + B.colind.nbytes + B.vals.nbytes + v0.nbytes + B.ns.nbytes
-    d2h = ev2.nbytes + info2.nbytes
+    h2d = ranks.sum(B.rowptr.nbytes + B.colind.nbytes + B.vals.nbytes + v0.nbytes + B.ns.nbytes)
+    d2h = ranks.sum(ev2.nbytes + info2.nbytes)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -751,11 +781,13 @@ def run_b200_batched(args):
     if rank == 0:
         line = {"metric": "time_to_all_residuals_le_1e-8", "value": ms_per_step / 1e3, "unit": "s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 basis then f64" if args.precision == "mixed" else "f64",
+                "higher_is_better": False, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+                "dtype": "f32 basis then f64" if args.precision == "mixed" else "f64",
                 "data": "synthetic (seeded k-NN graphs, seeded N(0,1) start vectors)",
-                "config": batched_config(args, B, {
-                    "threads_per_problem": threads, "all_converged": bool(np.all(info[:, 2] == 1)),
-                    "max_restarts": int(info[:, 1].max()), "lanczos_steps": int(info[:, 3].sum())}),
+                "config": batched_config(args, B_all, {
+                    "threads_per_problem": threads, "all_converged": bool(all_converged),
+                    "max_restarts": int(max_restarts), "lanczos_steps": int(lanczos_total),
+                    "problems_per_rank": [len(shard(B_all.nprob, r, world)) for r in range(world)]}),
                 "roofline": {"kernel": "batched_ks_kernel (whole Krylov-Schur per CTA)", "bound": "hbm",
                              "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                              "peak_kind": peak_kind, "traffic": None,

@@ -204,10 +204,12 @@ b200_status b200_bv_orthogonalize_vec(b200_bv bv, double *v_dev, double *H_host,
  * call synchronises the stream.  All working memory comes from one fixed
  * array of about 330 KB compiled into the library, which every GPU that
  * loads the library holds until the process exits; j at most 253, otherwise
- * B200_ERR_ARG.  The first call on a device looks the array's address up
- * and should come before any stream capture on that device.  Calls share
- * the array: calls whose work overlaps on the GPU race and must be
- * serialised by the caller. */
+ * B200_ERR_ARG.  The first call on a device (and in each context of it the
+ * caller makes current) looks the array's address up and should come before
+ * any stream capture there.  The address is not looked up again after
+ * cudaDeviceReset: do not call this entry point on a device after resetting
+ * it.  Calls share the array: calls whose work overlaps on the GPU race and
+ * must be serialised by the caller. */
 b200_status b200_orthogonalize_column_noalloc(int n, int ld, int ncols, double *V_dev, int j, double *H_dev,
                                               double *norm, int *lindep, void *stream);
 /* BVOrthogonalize (bvorthog.c:726-767) of columns l..k-1 with the BV's block
@@ -216,7 +218,11 @@ b200_status b200_orthogonalize_column_noalloc(int n, int ld, int ncols, double *
  * matrix of the block on the device and its Cholesky factor or scaled
  * eigendecomposition on the host, then one in-place product.  R_host
  * (nullable, ldr >= k) receives R with V_in = V_out R (upper triangular
- * except for SVQB). */
+ * except for SVQB).  On B200_ERR_BREAKDOWN (a zero or linearly dependent
+ * column) the status matches BVOrthogonalize_GS (bvorthog.c:546), but the
+ * GS type queues every column before it reads any norm back, so the columns
+ * after the dependent one have been processed too: the contents of columns
+ * l..k-1 are undefined after a breakdown. */
 b200_status b200_bv_orthogonalize(b200_bv bv, double *R_host, int ldr);
 
 /* BVMultInPlace (bvops.c:220-245; BVMultInPlace_BLAS_CUDA bvcuda.cu:65-112):

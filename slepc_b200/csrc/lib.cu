@@ -810,7 +810,10 @@ extern "C" b200_status b200_bv_scale_column(b200_bv bv, int j, double alpha) {
 }
 
 // BVOrthogonalize_GS without R: every column of [l,k) orthogonalised against all previous columns
-// and scaled by 1/norm on the device, the norms recorded on the device and read back once.
+// and scaled by 1/norm on the device, the norms recorded on the device and read back once.  A
+// dependent column is found only at that read-back, after the later columns have been
+// orthogonalised against it, so V(:,l:k) is undefined when B200_ERR_BREAKDOWN is returned (the
+// reference stops at the first zero norm, bvorthog.c:546, with the same status).
 b200_status b200::bv_orthogonalize_block(b200_bv bv) {
   const int nc = bv->k - bv->l;
   if (nc <= 0) return B200_OK;

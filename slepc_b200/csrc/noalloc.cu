@@ -11,10 +11,18 @@
 //
 // The scratch array lives in device global memory for the life of the
 // process on every GPU that loads this library.  Its address is looked up
-// once per device, on the first call made with that device current.  All
-// calls share the one array, so two calls whose work overlaps on the GPU
-// (different streams, or different host threads) overwrite each other's
-// scratch and give wrong results: serialise them.
+// once per (device, context) pair, on the first call made with that device
+// and context current: a caller that makes its own contexts with cuCtxCreate
+// gets the array of its own context, not the primary context's.  The lookup
+// is not repeated after cudaDeviceReset (the primary context keeps its
+// handle across a reset while the module, and with it the array, may be
+// reloaded elsewhere), so a process that resets a device must not call this
+// entry point on that device afterwards.  All calls share the one array, so
+// two calls whose work overlaps on the GPU (different streams, or different
+// host threads) overwrite each other's scratch and give wrong results:
+// serialise them.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "common.h"
@@ -32,28 +40,55 @@ constexpr size_t kScratchDoubles =
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
 struct ScratchView {
-  double *base = nullptr;  // device address of g_noalloc_scratch on this device
-  bool ready = false;
+  int dev = -1;
+  CUcontext ctx = nullptr;  // context the address belongs to
+  double *base = nullptr;   // device address of g_noalloc_scratch in that context
 };
 
+constexpr int kMaxViews = 64;
 std::mutex g_setup_mutex;
-ScratchView g_views[64];
+ScratchView g_views[kMaxViews];
+int g_nviews = 0;
 
-// Device address of the scratch for the current device (looked up once per device).
+using CtxGetCurrent = CUresult (*)(CUcontext *);
+
+// The calling thread's current context through the driver entry point (no link against libcuda;
+// nothing is allocated).  Null when no context is current yet.
+CUcontext current_context() {
+  static CtxGetCurrent fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<CtxGetCurrent>(p);
+  }();
+  CUcontext c = nullptr;
+  if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+  return c;
+}
+
+// Device address of the scratch for the current device and context, looked up once per pair.
 cudaError_t scratch_address(double **out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_views[dev].ready) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    g_views[dev].base = static_cast<double *>(p);
-    g_views[dev].ready = true;
-  }
-  *out = g_views[dev].base;
+  CUcontext ctx = current_context();
+  for (int i = 0; ctx && i < g_nviews; ++i)
+    if (g_views[i].dev == dev && g_views[i].ctx == ctx) {
+      *out = g_views[i].base;
+      return cudaSuccess;
+    }
+  // first call in this context (or no context current yet: the lookup makes the primary one current)
+  void *p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return e;
+  ctx = current_context();
+  bool known = false;
+  for (int i = 0; ctx && i < g_nviews; ++i) known = known || (g_views[i].dev == dev && g_views[i].ctx == ctx);
+  if (ctx && !known && g_nviews < kMaxViews) g_views[g_nviews++] = ScratchView{dev, ctx, static_cast<double *>(p)};
+  *out = static_cast<double *>(p);
   return cudaSuccess;
 }
 

@@ -331,6 +331,24 @@ class Batch:
         z0, z1 = int(self.nnz_off[p]), int(self.nnz_off[p + 1])
         return self.rowptr[r0:r0 + n + 1].copy(), self.colind[z0:z1].copy(), self.vals[z0:z1].copy()
 
+    def subset(self, idx):
+        """The batch of problems idx (in that order), with the same per-problem arrays."""
+        idx = [int(p) for p in idx]
+        ns = self.ns[idx].astype(np.int32) if idx else np.zeros(0, dtype=np.int32)
+        parts = [self.problem(p) for p in idx]
+        row_off = np.zeros(len(idx) + 1, dtype=np.int64)
+        np.cumsum(ns, out=row_off[1:])
+        nnz_off = np.zeros(len(idx) + 1, dtype=np.int64)
+        np.cumsum([len(c) for _, c, _ in parts], out=nnz_off[1:])
+        cat = (lambda xs, dt: np.concatenate(xs).astype(dt) if xs else np.zeros(0, dtype=dt))
+        return Batch(ns, cat([r for r, _, _ in parts], np.int32), cat([c for _, c, _ in parts], np.int32),
+                     cat([v for _, _, v in parts], np.float64), row_off, nnz_off)
+
+    def rows_of(self, x, idx):
+        """The slices of a batch-long vector x (sum of ns entries) that belong to problems idx."""
+        xs = [x[int(self.row_off[p]):int(self.row_off[p + 1])] for p in idx]
+        return np.concatenate(xs) if xs else np.zeros(0, dtype=x.dtype)
+
 
 def knn_batch(ns, k=8, seed=0):
     """The batch of k-NN operators for sizes ns (OpenMP over problems)."""

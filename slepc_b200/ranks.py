@@ -1,8 +1,8 @@
 """One process per GPU for replica runs.
 
 The eigensolver path is run as independent replicas, one per GPU: every rank
-solves its own copy of the problem (or its own share of independent problems)
-and no data-path collective exists.  What the ranks share is host plumbing: the
+solves its own copy of the problem, or its own share of a batch of independent
+problems (``shard``), and no data-path collective exists.  What the ranks share is host plumbing: the
 torchrun environment, a barrier on both sides of a timed region and the maximum
 of a host number (a per-rank time) over the ranks, taken on rank 0's report.
 
@@ -55,6 +55,16 @@ class Ranks:
 
         t = torch.tensor([float(x)], dtype=torch.float64, device="cuda" if self.backend == "nccl" else "cpu")
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x):
+        """The sum of the host number x over all ranks (every rank gets it)."""
+        if self.dist is None:
+            return float(x)
+        import torch
+
+        t = torch.tensor([float(x)], dtype=torch.float64, device="cuda" if self.backend == "nccl" else "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
         return float(t.item())
 
     def close(self):

@@ -38,6 +38,59 @@ def _worker(rank, world, port, out_dir, plan):
         f.write(" ".join(repr(v) for v in got))
 
 
+def _batch_worker(rank, world, port, out_dir, nprob):
+    """One rank of the sharded batched workload, with the oracle's batch solver standing in for the
+    GPU launch: the rank solves only its share of the problems and reports a sum over ranks."""
+    os.environ.update(RANK=str(rank), LOCAL_RANK=str(rank), WORLD_SIZE=str(world), MASTER_ADDR="127.0.0.1",
+                      MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    import numpy as np
+
+    import bench
+    import oracle
+    from slepc_b200 import problems as P
+
+    r = Ranks("gloo", timeout_s=60)
+    ns = P.batch_sizes(nprob, 3, lo=60, hi=200)
+    B = P.knn_batch(ns, 8, 3)
+    v0 = np.concatenate([P.start_vector(int(n), p) for p, n in enumerate(ns)])
+    part = bench.batched_shard(B, v0, rank, world)
+    ev, info = oracle.eps_solve_batch(part.B.ns, part.B.rowptr, part.B.colind, part.B.vals, part.v0, 4, 12, 1e-8,
+                                      oracle.LARGEST_REAL, threads=1)
+    total_rows = r.sum(int(part.B.ns.sum()))
+    r.close()
+    np.savez(os.path.join(out_dir, f"rank{rank}.npz"), idx=np.array(part.idx), ev=ev, info=info,
+             total_rows=total_rows)
+
+
+def test_sharded_batch_union_equals_single_rank():
+    """The batched workload split over two gloo ranks: every problem is solved by exactly one rank
+    and the union of their results equals the one-rank run of the whole batch."""
+    import numpy as np
+    import torch.multiprocessing as mp
+
+    import oracle
+    from slepc_b200 import problems as P
+
+    nprob = 7
+    with tempfile.TemporaryDirectory() as d:
+        mp.start_processes(_batch_worker, args=(2, _free_port(), d, nprob), nprocs=2, join=True,
+                           start_method="spawn")
+        parts = [np.load(os.path.join(d, f"rank{r}.npz")) for r in range(2)]
+    idx = np.concatenate([p["idx"] for p in parts])
+    assert sorted(idx.tolist()) == list(range(nprob)) and len(idx) == nprob
+    ns = P.batch_sizes(nprob, 3, lo=60, hi=200)
+    assert all(float(p["total_rows"]) == float(ns.sum()) for p in parts)
+    B = P.knn_batch(ns, 8, 3)
+    v0 = np.concatenate([P.start_vector(int(n), p) for p, n in enumerate(ns)])
+    ev, info = oracle.eps_solve_batch(B.ns, B.rowptr, B.colind, B.vals, v0, 4, 12, 1e-8, oracle.LARGEST_REAL,
+                                      threads=1)
+    got_ev = np.concatenate([p["ev"] for p in parts])
+    got_info = np.concatenate([p["info"] for p in parts])
+    np.testing.assert_array_equal(got_ev, ev[idx])
+    np.testing.assert_array_equal(got_info, info[idx])
+
+
 def test_shard_partitions_every_unit_once():
     for count in (0, 1, 5, 8, 4096, 4097):
         for world in (1, 2, 3, 8):

@@ -60,7 +60,24 @@ def test_noalloc_matches_regular_entry_point_twice():
         np.testing.assert_allclose(cn, cr, rtol=0, atol=1e-12 * np.abs(cr).max())
 
 
+def test_noalloc_matches_the_oracle():
+    import oracle
+
+    V = _case(30011, 24, 26, 3)
+    Ho, no, lo = oracle.bv_orthogonalize_column(np.asfortranarray(V.copy()), 24)
+    Hn, nn, ln, _ = _noalloc(V, 24)
+    assert ln == lo
+    np.testing.assert_allclose(nn, no, rtol=1e-12)
+    np.testing.assert_allclose(Hn, Ho, rtol=1e-11, atol=1e-13 * np.abs(Ho).max())
+
+
 def test_noalloc_rejects_sizes_beyond_the_scratch():
+    import torch
+
+    # real (small) device buffers: only the argument check may run, and it must stop the call
+    Vd = torch.zeros((300, 1000), dtype=torch.float64, device="cuda")
+    Hd = torch.zeros(261, dtype=torch.float64, device="cuda")
     with pytest.raises(S.B200Error) as ei:
-        S.orthogonalize_column_noalloc(1000, 1000, 300, 256, 260, 256)
+        S.orthogonalize_column_noalloc(1000, 1000, 300, Vd.data_ptr(), 260, Hd.data_ptr())
     assert ei.value.status == 1
+    torch.cuda.synchronize()

@@ -192,6 +192,37 @@ b200_status b200_bv_orthogonalize_column(b200_bv bv, int j, double *H_host, doub
 b200_status b200_bv_orthonormalize_column(b200_bv bv, int j, double *norm, int *lindep);
 /* BVOrthogonalizeVec (bvorthog.c:238-262): a device vector against the k active columns. */
 b200_status b200_bv_orthogonalize_vec(b200_bv bv, double *v_dev, double *H_host, double *norm, int *lindep);
+/* One classical Gram-Schmidt pass: the BV gramschmidt op
+ * (include/slepc/private/bvimpl.h:53), which BVOrthogonalizeGS's DGKS loop
+ * (src/sys/classes/bv/interface/bvorthog.c:174-203) calls 1-3 times in place
+ * of BVOrthogonalizeCGS1 (bvorthog.c:91-132).  v_dev null: column j of the BV
+ * against columns 0..j-1; otherwise the device vector v_dev against the k
+ * active columns (j ignored).  c_dev (device, nullable, jb+1 entries with jb =
+ * j or k) receives this pass's coefficients V^T w and, at position jb, w^T w;
+ * h_dev (device, nullable) accumulates h += c over the jb coefficients
+ * (BV_AddCoefficients) -- for the column variant a null h_dev accumulates
+ * into the BV's coefficient buffer column j; w <- w - V c.  onorm and norm
+ * (host, nullable) receive ||w|| before the pass and sqrt(||w||^2 - c^T c),
+ * or the explicit norm of the updated vector when that estimate is not
+ * positive (bvorthog.c:124-127); asking for either synchronises the stream.
+ * B200_ERR_INNER when w^T w < -10 eps for a column (BV_SafeSqrt). */
+b200_status b200_bv_gram_schmidt(b200_bv bv, int j, double *v_dev, double *h_dev, double *c_dev, double *onorm,
+                                 double *norm);
+/* BVResize (src/sys/classes/bv/interface/bvbasic.c:338; BVResize_Svec,
+ * impls/svec/svec.c:261): m columns of new storage, the first min(m, old m)
+ * copied when copy != 0; l and k clipped to m.  The handle stays valid. */
+b200_status b200_bv_resize(b200_bv bv, int m, int copy);
+/* BVCopy (bvbasic.c:1779; BVCopy_Svec svec.c:233): Y(:, Y.l + j) =
+ * X(:, X.l + j) for the k - l active columns of X. */
+b200_status b200_bv_copy(b200_bv X, b200_bv Y);
+/* BVNormalize (src/sys/classes/bv/interface/bvglobal.c:829) for real
+ * scalars: every active column scaled to unit 2-norm (zero columns left as
+ * they are); norms_host (nullable, k - l values) receives the norms. */
+b200_status b200_bv_normalize(b200_bv bv, double *norms_host);
+/* BVMultInPlaceHermitianTranspose (src/sys/classes/bv/interface/bvops.c:268)
+ * for real scalars: V(:,s:e) = V(:,l:k) Q(s:e, l:k)^T with Q a host
+ * column-major matrix of at least e rows (ldq >= e) and k columns. */
+b200_status b200_bv_mult_inplace_trans(b200_bv bv, const double *Q_host, int ldq, int s, int e);
 /* Allocation-free variant of b200_bv_orthogonalize_column; it has no
  * counterpart in SLEPc.  For callers that cannot call cudaMalloc -- for
  * example a host whose device memory is all owned by its own pool
@@ -283,40 +314,45 @@ b200_status b200_eps_set_initial_space_device(b200_eps eps, const double *v0_dev
 /* Stop after this many restarts (0 = no cap; used to time bounded samples). */
 b200_status b200_eps_set_max_restarts(b200_eps eps, int max_restarts);
 /* EPSSolve (src/eps/interface/epssolve.c:119-229 -> EPSSolve_KrylovSchur_Default, krylovschur.c:227-348). */
-/* Arithmetic of the Krylov-Schur solve (no SLEPc counterpart: SLEPc computes
- * in the one precision PETSc was configured with).
- *   B200_PRECISION_FP64 (default): the drop-in path, FP64 throughout.
- *   B200_PRECISION_MIXED: two phases.  (1) Krylov-Schur with the basis stored
- *   in FP32 and the matrix values in FP32 (every product, sum, DGKS
- *   correction, Rayleigh quotient and projected problem in FP64), run to a
- *   loose tolerance: half the HBM traffic of the FP64 basis.  (2) FP64
- *   refinement of the block of nev + guard Ritz vectors by Chebyshev-filtered
- *   subspace iteration with an FP64 Rayleigh-Ritz step (block SpMV with the
- *   FP64 matrix, CholQR2 orthonormalisation, host dsyevd), until every wanted
- *   residual ||Ax - theta x|| / |theta| computed in FP64 is below tol.
- *   Needs a square CSR operator and which = largest/smallest real, largest
- *   algebraic/magnitude or smallest algebraic. */
+/* Arithmetic of the Hermitian solve (no SLEPc counterpart: SLEPc computes in
+ * the one precision PETSc was configured with).
+ *   B200_PRECISION_FP64 (default): the drop-in path, Krylov-Schur in FP64
+ *   throughout, as EPSSolve_KrylovSchur_Default.
+ *   B200_PRECISION_MIXED: the same eigenpairs (every wanted residual
+ *   ||Ax - theta x|| / |theta| below tol, computed in FP64 with the FP64
+ *   matrix) by Chebyshev-filtered subspace iteration on a block of 64 or 128
+ *   vectors (nev + guard), stored row-major, in two phases.  (1) FP32: the
+ *   block and the matrix values in FP32, the filter's block SpMV accumulating
+ *   in FP32, the orthonormalisation Gram matrix X^T X on the tensor cores
+ *   (tcgen05 TF32 with FP32 accumulation) and the Rayleigh quotients X^T X,
+ *   X^T A X and the residual norms in FP64, until tol_low.  (2) FP64: the same
+ *   sweeps on the block widened to FP64 until tol.  The degree of each sweep
+ *   follows the residuals and Ritz values.  Needs a square CSR operator,
+ *   n >= 2 x block width, and which = largest/smallest real or largest
+ *   magnitude. */
 #define B200_PRECISION_FP64 0
 #define B200_PRECISION_MIXED 1
 b200_status b200_eps_set_precision(b200_eps eps, int precision);
+/* The mixed form's projection kernel, exposed for tests and benchmarks (no
+ * SLEPc counterpart as a call; it plays BVDot's role, bvglobal.c, on the
+ * block): G (bp x bp, FP64, row-major, device) = X^T Y for row-major FP32
+ * blocks of n rows and bp = 64 or 128 columns (Y null: X^T X).
+ * tensor_cores = 1: tcgen05 kind::tf32 with FP32 accumulation in TMEM (the
+ * TF32 inputs carry 10 mantissa bits); 0: FP64 products and sums on the CUDA
+ * cores.  Allocates its work arrays; synchronises the stream. */
+b200_status b200_rowblock_gram(int n, int bp, const float *X_dev, const float *Y_dev, int tensor_cores,
+                               double *G_dev, void *stream);
 /* Mixed-form parameters (0 or a negative value keeps the default): tol_low,
- * the phase-1 tolerance (default 1e-6, never below tol); degree, the
- * Chebyshev filter degree per sweep (default 128; a sweep uses less when the
- * amplification of the leading Ritz value would exceed 1e6, which keeps the
- * block well conditioned for its Cholesky QR); guard, columns of the
- * refinement block beyond nev (default max(8, nev/2)); max_sweeps (default
- * 40); fp32_first_pass: 1 runs the first Gram-Schmidt pass of every column
- * (its projections and the update that applies them) in FP32 arithmetic and
- * always takes the FP64 DGKS correction pass, 0 (default) keeps every pass in
- * FP64 arithmetic on the FP32 basis. */
+ * the tolerance of the FP32 phase (default 5e-7, never below tol; the phase
+ * also ends when a sweep no longer halves the largest wanted residual);
+ * degree, the largest Chebyshev degree of one sweep (default 160); guard,
+ * block columns beyond nev (default max(8, nev/2); the block is 64 columns
+ * when nev + guard <= 64, else 128, at most 128); max_sweeps, per phase
+ * (default 60); fp64_gram: 1 forms the FP32 phase's orthonormalisation Gram
+ * matrix in FP64 on the CUDA cores instead of on the tensor cores (0,
+ * default). */
 b200_status b200_eps_set_mixed_options(b200_eps eps, double tol_low, int degree, int guard, int max_sweeps,
-                                       int fp32_first_pass);
-/* DGKS threshold eta of the FP32-basis phase (BVSetOrthogonalization's eta, bvorthog.c:176-187):
- * a second Gram-Schmidt pass only when the norm drops below eta times the norm before the pass.
- * 0 (default) takes one pass per column: two reads of the FP32 basis instead of three, with the
- * same phase-1 restart count on the 3-D Laplacian; the FP64 refinement phase supplies the
- * accuracy.  A negative value keeps the BV's 0.7071 ("if needed" refinement). */
-b200_status b200_eps_set_mixed_eta(b200_eps eps, double eta);
+                                       int fp64_gram);
 
 /* EPSSetType: B200_EPS_KRYLOVSCHUR (default) or B200_EPS_LOBPCG. */
 #define B200_EPS_KRYLOVSCHUR 0
@@ -365,8 +401,10 @@ typedef struct {
   double ms_spmv, ms_orth, ms_restart, ms_total;
   int64_t gs_bytes;
   int64_t column_visits;  /* sum over Lanczos steps j of (j+2): basis columns one CGS pass reads */
-  /* mixed precision (zero otherwise): refinement sweeps, Chebyshev degree, block columns,
-   * restarts of the FP32-basis phase, device time of the two phases, block SpMV columns */
+  /* mixed precision (zero otherwise): sweeps of the FP64 phase, the largest Chebyshev degree of a
+   * sweep, block columns, sweeps of the FP32 phase, device time of the two phases, and block-SpMV
+   * columns (block width x block SpMVs).  In the mixed form with timing on, ms_spmv and gs_bytes
+   * hold the device time and the algorithmic bytes of the Chebyshev filters' block SpMVs. */
   int64_t filter_sweeps;
   int64_t filter_degree;
   int64_t block_size;

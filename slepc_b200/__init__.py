@@ -76,7 +76,12 @@ _SIGS = {
     "b200_mat_norm_inf": (ctypes.c_int, [_vp, _dp]),
     "b200_eps_set_type": (ctypes.c_int, [_vp, ctypes.c_int]),
     "b200_eps_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
-    "b200_eps_set_mixed_eta": (ctypes.c_int, [_vp, ctypes.c_double]),
+    "b200_bv_gram_schmidt": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _dp, _dp]),
+    "b200_bv_resize": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    "b200_bv_copy": (ctypes.c_int, [_vp, _vp]),
+    "b200_bv_normalize": (ctypes.c_int, [_vp, _dp]),
+    "b200_bv_mult_inplace_trans": (ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "b200_rowblock_gram": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp]),
     "b200_eps_set_mixed_options": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                   ctypes.c_int]),
     "b200_eps_lobpcg_set_block_size": (ctypes.c_int, [_vp, ctypes.c_int]),
@@ -482,6 +487,35 @@ class BV:
         _check(lib().b200_bv_orthogonalize_vec(self.handle, v_ptr, _d(H), ctypes.byref(nrm), ctypes.byref(lnd)))
         return H[:k], nrm.value, bool(lnd.value)
 
+    def gramSchmidt(self, j, v_ptr=None, h_ptr=None, c_ptr=None, norms=True):
+        """One classical Gram-Schmidt pass (the BV gramschmidt op, b200_bv_gram_schmidt): returns
+        (onorm, norm) when norms is set (a synchronisation), else None."""
+        if not norms:
+            _check(lib().b200_bv_gram_schmidt(self.handle, j, v_ptr, h_ptr, c_ptr, None, None))
+            return None
+        on, nr = ctypes.c_double(), ctypes.c_double()
+        _check(lib().b200_bv_gram_schmidt(self.handle, j, v_ptr, h_ptr, c_ptr, ctypes.byref(on), ctypes.byref(nr)))
+        return on.value, nr.value
+
+    def resize(self, m, copy=True):
+        _check(lib().b200_bv_resize(self.handle, m, 1 if copy else 0))
+
+    def copy(self, Y):
+        """BVCopy: the active columns of this BV into Y from Y's leading column l."""
+        _check(lib().b200_bv_copy(self.handle, Y.handle))
+
+    def normalize(self):
+        """BVNormalize (real): unit 2-norm active columns; returns their previous norms."""
+        l, k = self.getActiveColumns()
+        nrm = np.zeros(max(k - l, 1))
+        _check(lib().b200_bv_normalize(self.handle, _d(nrm)))
+        return nrm[: k - l]
+
+    def multInPlaceTranspose(self, Q, s, e):
+        """BVMultInPlaceHermitianTranspose (real): V(:,s:e) = V Q(s:e,:)^T."""
+        Q = np.asfortranarray(Q, dtype=np.float64)
+        _check(lib().b200_bv_mult_inplace_trans(self.handle, _d(Q), Q.shape[0], s, e))
+
     def orthogonalize(self, k):
         R = np.zeros((k, k), order="F")
         _check(lib().b200_bv_orthogonalize(self.handle, _d(R), k))
@@ -645,14 +679,10 @@ class EPS:
         Chebyshev-filtered Rayleigh-Ritz refinement of the block of leading Ritz vectors."""
         _check(lib().b200_eps_set_precision(self.handle, precision))
 
-    def setMixedEta(self, eta):
-        """DGKS threshold of the FP32-basis phase (0, the default: one pass per column; negative: 0.7071)."""
-        _check(lib().b200_eps_set_mixed_eta(self.handle, eta))
-
-    def setMixedOptions(self, tol_low=0.0, degree=0, guard=-1, max_sweeps=0, fp32_first_pass=False):
-        """Parameters of the mixed form; 0 (or -1 for guard) keeps the default."""
+    def setMixedOptions(self, tol_low=0.0, degree=0, guard=-1, max_sweeps=0, fp64_gram=False):
+        """Parameters of the mixed form (b200_eps_set_mixed_options); 0 (or -1 for guard) keeps the default."""
         _check(lib().b200_eps_set_mixed_options(self.handle, tol_low, degree, guard, max_sweeps,
-                                                int(bool(fp32_first_pass))))
+                                                int(bool(fp64_gram))))
 
     def setInitialSpaceDevice(self, v0_ptr):
         _check(lib().b200_eps_set_initial_space_device(self.handle, v0_ptr))
@@ -735,6 +765,12 @@ def orthogonalize_column_noalloc(n, ld, ncols, V_ptr, j, H_ptr, stream=None):
     _check(lib().b200_orthogonalize_column_noalloc(n, ld, ncols, V_ptr, j, H_ptr, ctypes.byref(nrm),
                                                    ctypes.byref(lnd), stream))
     return nrm.value, bool(lnd.value)
+
+
+def rowblock_gram(n, bp, X_ptr, Y_ptr=None, tensor_cores=True, G_ptr=None, stream=None):
+    """G = X^T Y (bp x bp, FP64, row-major) of row-major FP32 device blocks (b200_rowblock_gram):
+    on the tensor cores (TF32 inputs, FP32 accumulation) or in FP64 on the CUDA cores."""
+    _check(lib().b200_rowblock_gram(n, bp, X_ptr, Y_ptr, 1 if tensor_cores else 0, G_ptr, stream))
 
 
 def solve_csr_host(csr, v0, nev, ncv, tol=1e-8, which=LARGEST_MAGNITUDE, mpd=0, max_it=0, want_vectors=True,

@@ -12,10 +12,12 @@
  * B200 CSR SpMV on VECCUDA arrays (precedent: MatMult_Cyclic_CUDA in
  * src/svd/impls/cyclic/cycliccuda/cycliccuda.cu:16-48).
  *
- * The BV type keeps SLEPc's own Gram-Schmidt driver (bvorthog.c), which calls
- * this type's dotvec / multvec / scale / norm ops.  The EPS type hands a whole
- * Hermitian solve to b200_eps_solve, which fuses the DGKS passes and keeps a
- * Lanczos run on the device with one host synchronisation.
+ * The BV type keeps SLEPc's own DGKS driver (BVOrthogonalizeGS, bvorthog.c:145-217)
+ * and fills its gramschmidt op (bvimpl.h:53) with b200_bv_gram_schmidt, so a
+ * stock EPSSolve with -bv_type b200 alone runs every Gram-Schmidt pass on the
+ * device pass kernel.  The optional EPS type hands a whole Hermitian solve to
+ * b200_eps_solve, which also fuses the DGKS passes and keeps a Lanczos run on
+ * the device with one host synchronisation.
  */
 #include <slepc/private/bvimpl.h>
 #include <slepc/private/epsimpl.h>
@@ -122,8 +124,10 @@ static PetscErrorCode MatB200Get(Mat S, b200_mat *A)
 /* ------------------------------------------------------------------- BV --- */
 
 typedef struct {
-  b200_bv bv; /* device storage: ld x (m+1) doubles */
-  Vec     v;  /* VECSEQCUDA over the storage (for getarray / getmat paths) */
+  b200_bv bv;    /* device storage: ld x (m+1) doubles */
+  Vec     v;     /* VECSEQCUDA over the storage (for getarray / getmat paths) */
+  double *stage; /* device staging of the host h / c arrays of BVOrthogonalizeVec (2 (m+1) doubles) */
+  Mat     Aget;  /* dense CUDA matrix over the active columns (getmat / restoremat) */
 } BV_B200;
 
 /* the ABI keeps its own active columns; mirror SLEPc's before every op */
@@ -329,12 +333,151 @@ static PetscErrorCode BVMatMult_B200(BV V, Mat A, BV W)
   PetscFunctionReturn(PETSC_SUCCESS);
 }
 
+/* The gramschmidt op (bvimpl.h:53): one CGS pass through b200_bv_gram_schmidt, called 1-3 times
+   by BVOrthogonalizeGS's DGKS loop (bvorthog.c:174-203) in place of BVOrthogonalizeCGS1.  Column
+   variant (v NULL): SLEPc passes h = c = NULL and the coefficients live in the VECCUDA bv->buffer
+   (column j accumulates, column 0 is the scratch c, BV_AddCoefficients_Default, bvimpl.h:306-320).
+   Vector variant: h and c are BVOrthogonalizeVec's host arrays, staged through device memory. */
+static PetscErrorCode BVGramSchmidt_B200(BV bv, PetscInt j, Vec v, PetscBool *which, PetscScalar *h, PetscScalar *c,
+                                         PetscReal *onrm, PetscReal *nrm)
+{
+  BV_B200     *ctx = (BV_B200 *)bv->data;
+  PetscScalar *buf, *pv;
+  double       on = 0.0, nr = 0.0;
+  PetscInt     jb = v ? bv->k : j;
+
+  PetscFunctionBegin;
+  PetscCheck(!bv->matrix && !bv->indef, PetscObjectComm((PetscObject)bv), PETSC_ERR_SUP,
+             "BV b200: standard inner product only");
+  PetscCall(BVB200Sync(bv));
+  if (!v) {
+    PetscCall(VecCUDAGetArray(bv->buffer, &buf));
+    B200Call(b200_bv_gram_schmidt(ctx->bv, (int)j, NULL, buf + j * (bv->nc + bv->m), buf, onrm ? &on : NULL,
+                                  nrm ? &nr : NULL));
+    PetscCall(VecCUDARestoreArray(bv->buffer, &buf));
+  } else {
+    PetscCallCUDA(cudaMemcpy(ctx->stage, h, sizeof(double) * jb, cudaMemcpyHostToDevice));
+    PetscCall(VecCUDAGetArray(v, &pv));
+    B200Call(b200_bv_gram_schmidt(ctx->bv, 0, pv, ctx->stage, ctx->stage + bv->m + 1, onrm ? &on : NULL,
+                                  nrm ? &nr : NULL));
+    PetscCall(VecCUDARestoreArray(v, &pv));
+    PetscCallCUDA(cudaMemcpy(h, ctx->stage, sizeof(double) * jb, cudaMemcpyDeviceToHost));
+    PetscCallCUDA(cudaMemcpy(c, ctx->stage + bv->m + 1, sizeof(double) * (jb + 1), cudaMemcpyDeviceToHost));
+  }
+  if (onrm) *onrm = on;
+  if (nrm) *nrm = nr;
+  PetscFunctionReturn(PETSC_SUCCESS);
+}
+
+/* BVResize (bvbasic.c:338): new storage through the ABI, the Vec over it rebuilt. */
+static PetscErrorCode BVResize_B200(BV bv, PetscInt m, PetscBool copy)
+{
+  BV_B200 *ctx = (BV_B200 *)bv->data;
+  double  *V;
+
+  PetscFunctionBegin;
+  B200Call(b200_bv_resize(ctx->bv, (int)m, copy ? 1 : 0));
+  PetscCall(VecDestroy(&ctx->v));
+  B200Call(b200_bv_get_array(ctx->bv, &V));
+  PetscCall(VecCreateSeqCUDAWithArray(PetscObjectComm((PetscObject)bv), 1, m * bv->ld, V, &ctx->v));
+  PetscCallCUDA(cudaFree(ctx->stage));
+  PetscCallCUDA(cudaMalloc((void **)&ctx->stage, sizeof(double) * 2 * (m + 1)));
+  PetscFunctionReturn(PETSC_SUCCESS);
+}
+
+/* BVCopy (bvbasic.c:1779): active columns of V into W from W's leading column. */
+static PetscErrorCode BVCopy_B200(BV V, BV W)
+{
+  BV_B200 *v = (BV_B200 *)V->data, *w = (BV_B200 *)W->data;
+
+  PetscFunctionBegin;
+  PetscCall(BVB200Sync(V));
+  PetscCall(BVB200Sync(W));
+  B200Call(b200_bv_copy(v->bv, w->bv));
+  PetscFunctionReturn(PETSC_SUCCESS);
+}
+
+/* duplicate op (BVDuplicate_Private, bvbasic.c:1619-1632, has already set W's type and sizes):
+   carry the orthogonalisation settings into W's device object. */
+static PetscErrorCode BVDuplicate_B200(BV V, BV W)
+{
+  BV_B200 *w = (BV_B200 *)W->data;
+
+  PetscFunctionBegin;
+  B200Call(b200_bv_set_orthog_eta(w->bv, V->orthog_eta));
+  if (V->orthog_block == BV_ORTHOG_BLOCK_CHOL) B200Call(b200_bv_set_orthog_block(w->bv, B200_ORTHOG_BLOCK_CHOL));
+  else if (V->orthog_block == BV_ORTHOG_BLOCK_SVQB) B200Call(b200_bv_set_orthog_block(w->bv, B200_ORTHOG_BLOCK_SVQB));
+  PetscFunctionReturn(PETSC_SUCCESS);
+}
+
+/* getmat / restoremat (bvbasic.c:1556, BVRestoreMat_Default :1590): a dense CUDA matrix placed over
+   the active columns of the device storage; nothing is copied either way. */
+static PetscErrorCode BVGetMat_B200(BV bv, Mat *A)
+{
+  BV_B200 *ctx = (BV_B200 *)bv->data;
+  double  *V;
+  PetscInt m = bv->k - bv->l;
+
+  PetscFunctionBegin;
+  B200Call(b200_bv_get_array(ctx->bv, &V));
+  if (!ctx->Aget) {
+    PetscCall(MatCreateDenseCUDA(PetscObjectComm((PetscObject)bv), bv->n, PETSC_DECIDE, bv->N, m, NULL, &ctx->Aget));
+    PetscCall(MatDenseSetLDA(ctx->Aget, bv->ld));
+  }
+  PetscCall(MatDenseCUDAPlaceArray(ctx->Aget, V + (bv->nc + bv->l) * bv->ld));
+  *A = ctx->Aget;
+  PetscFunctionReturn(PETSC_SUCCESS);
+}
+
+static PetscErrorCode BVRestoreMat_B200(BV bv, Mat *A)
+{
+  BV_B200 *ctx = (BV_B200 *)bv->data;
+
+  PetscFunctionBegin;
+  PetscCall(MatDenseCUDAResetArray(ctx->Aget));
+  PetscCall(MatDestroy(&ctx->Aget)); /* the active columns may differ at the next getmat */
+  *A = NULL;
+  PetscFunctionReturn(PETSC_SUCCESS);
+}
+
+/* multinplacetrans (BVMultInPlaceHermitianTranspose, bvops.c:268), real scalars. */
+static PetscErrorCode BVMultInPlaceTrans_B200(BV V, Mat Q, PetscInt s, PetscInt e)
+{
+  BV_B200           *ctx = (BV_B200 *)V->data;
+  const PetscScalar *q;
+  PetscInt           ldq;
+
+  PetscFunctionBegin;
+  PetscCall(BVB200Sync(V));
+  PetscCall(MatDenseGetLDA(Q, &ldq));
+  PetscCall(MatDenseGetArrayRead(Q, &q));
+  B200Call(b200_bv_mult_inplace_trans(ctx->bv, q, (int)ldq, (int)s, (int)e));
+  PetscCall(MatDenseRestoreArrayRead(Q, &q));
+  PetscFunctionReturn(PETSC_SUCCESS);
+}
+
+/* normalize (BVNormalize, bvglobal.c:829) for real eigenvectors (eigi null or zero on [l,k)). */
+static PetscErrorCode BVNormalize_B200(BV bv, PetscScalar *eigi)
+{
+  BV_B200 *ctx = (BV_B200 *)bv->data;
+  PetscInt i;
+
+  PetscFunctionBegin;
+  for (i = bv->l; eigi && i < bv->k; i++)
+    PetscCheck(eigi[i] == 0.0, PetscObjectComm((PetscObject)bv), PETSC_ERR_SUP, "BV b200: complex pairs not supported");
+  PetscCall(BVB200Sync(bv));
+  B200Call(b200_bv_normalize(ctx->bv, NULL));
+  PetscFunctionReturn(PETSC_SUCCESS);
+}
+
 static PetscErrorCode BVDestroy_B200(BV bv)
 {
   BV_B200 *ctx = (BV_B200 *)bv->data;
 
   PetscFunctionBegin;
   PetscCall(VecDestroy(&ctx->v));
+  PetscCall(MatDestroy(&ctx->Aget));
+  PetscCallCUDA(cudaFree(ctx->stage));
   PetscCall(VecDestroy(&bv->cv[0]));
   PetscCall(VecDestroy(&bv->cv[1]));
   B200Call(b200_bv_destroy(ctx->bv));
@@ -363,6 +506,7 @@ PetscErrorCode BVCreate_B200(BV bv)
   PetscCall(VecCreateSeqCUDAWithArray(PetscObjectComm((PetscObject)bv), 1, bv->m * bv->ld, V, &ctx->v));
   PetscCall(BVCreateVecEmpty(bv, &bv->cv[0]));
   PetscCall(BVCreateVecEmpty(bv, &bv->cv[1]));
+  PetscCallCUDA(cudaMalloc((void **)&ctx->stage, sizeof(double) * 2 * (bv->m + 1)));
 
   bv->ops->mult             = BVMult_B200;
   bv->ops->multvec          = BVMultVec_B200;
@@ -379,6 +523,14 @@ PetscErrorCode BVCreate_B200(BV bv)
   bv->ops->restorearray     = BVRestoreArray_B200;
   bv->ops->getarrayread     = BVGetArrayRead_B200;
   bv->ops->restorearrayread = BVRestoreArrayRead_B200;
+  bv->ops->gramschmidt      = BVGramSchmidt_B200;
+  bv->ops->resize           = BVResize_B200;
+  bv->ops->copy             = BVCopy_B200;
+  bv->ops->duplicate        = BVDuplicate_B200;
+  bv->ops->getmat           = BVGetMat_B200;
+  bv->ops->restoremat       = BVRestoreMat_B200;
+  bv->ops->multinplacetrans = BVMultInPlaceTrans_B200;
+  bv->ops->normalize        = BVNormalize_B200;
   bv->ops->destroy          = BVDestroy_B200;
   PetscFunctionReturn(PETSC_SUCCESS);
 }
@@ -389,6 +541,7 @@ typedef struct {
   b200_eps E;
   b200_mat A;   /* borrowed from a b200csr shell, or owned when built from AIJ */
   Mat      own; /* shell created here from an AIJ operator */
+  PetscBool mixed; /* -eps_b200_precision mixed: b200_eps_set_precision(B200_PRECISION_MIXED) */
 } EPS_B200KS;
 
 static int WhichToB200(EPSWhich w)
@@ -435,6 +588,24 @@ static PetscErrorCode EPSSetUp_B200KS(EPS eps)
   B200Call(b200_eps_set_dimensions(ctx->E, (int)eps->nev, (int)eps->ncv, (int)eps->mpd));
   B200Call(b200_eps_set_tolerances(ctx->E, eps->tol == (PetscReal)PETSC_DETERMINE ? 0.0 : eps->tol, (int)eps->max_it));
   B200Call(b200_eps_set_which_eigenpairs(ctx->E, WhichToB200(eps->which)));
+  B200Call(b200_eps_set_precision(ctx->E, ctx->mixed ? B200_PRECISION_MIXED : B200_PRECISION_FP64));
+  PetscFunctionReturn(PETSC_SUCCESS);
+}
+
+/* -eps_b200_precision fp64|mixed (EPSSetFromOptions calls this, epsopts.c) */
+static PetscErrorCode EPSSetFromOptions_B200KS(EPS eps, PetscOptionItems *PetscOptionsObject)
+{
+  EPS_B200KS *ctx = (EPS_B200KS *)eps->data;
+  const char *list[] = {"fp64", "mixed"};
+  PetscInt    idx = ctx->mixed ? 1 : 0;
+  PetscBool   flg;
+
+  PetscFunctionBegin;
+  PetscOptionsHeadBegin(PetscOptionsObject, "EPS b200ks options");
+  PetscCall(PetscOptionsEList("-eps_b200_precision", "Arithmetic of the B200 solve", "b200_eps_set_precision", list, 2,
+                              list[idx], &idx, &flg));
+  if (flg) ctx->mixed = idx == 1 ? PETSC_TRUE : PETSC_FALSE;
+  PetscOptionsHeadEnd();
   PetscFunctionReturn(PETSC_SUCCESS);
 }
 
@@ -500,6 +671,7 @@ PetscErrorCode EPSCreate_B200KS(EPS eps)
   eps->useds               = PETSC_FALSE;
   eps->categ               = EPS_CATEGORY_KRYLOV;
   eps->ops->setup          = EPSSetUp_B200KS;
+  eps->ops->setfromoptions = EPSSetFromOptions_B200KS;
   eps->ops->setupsort      = EPSSetUpSort_Default;
   eps->ops->solve          = EPSSolve_B200KS;
   eps->ops->destroy        = EPSDestroy_B200KS;

@@ -84,6 +84,7 @@ struct SpmvSell {
   int *rest_rows = nullptr;  // rows left out of the slices (block SpMV: one warp per row)
   int nrest = 0;
   float *vals32 = nullptr;   // FP32 copy of vals for the mixed-precision solver (FP64 matrices only)
+  int max_width = 0;         // widest slice (host copy; sizes the row-block SpMM's staging)
 };
 cudaError_t spmv_sell_launch(const SpmvSell &S, int n, const SpmvTiles &rest, const int *rowptr, const int *colind,
                              const double *vals, const double *x, double *y, cudaStream_t stream,

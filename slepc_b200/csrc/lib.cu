@@ -178,6 +178,8 @@ static b200_status part_build_sell(CsrPart &P, const int *rowptr_host, cudaStrea
     B200_CUDA_CHECK(sell_gather(P.rows, S, P.rowptr, P.colind, P.vals, P.f32, s));
   }
   S.entries = sp.entries;
+  S.max_width = 0;
+  for (int w : sp.width) S.max_width = w > S.max_width ? w : S.max_width;
   S.nrest = (int)sp.rest_rows.size();
   if (S.nrest) {
     B200_CUDA_CHECK(cudaMalloc(&S.rest_rows, sizeof(int) * sp.rest_rows.size()));
@@ -799,6 +801,127 @@ extern "C" b200_status b200_bv_orthogonalize_vec(b200_bv bv, double *v, double *
   return B200_OK;
 }
 
+// One classical Gram-Schmidt pass with the contract of the BV gramschmidt op
+// (include/slepc/private/bvimpl.h:53, used in place of BVOrthogonalizeCGS1, bvorthog.c:91-132):
+// c = V^T w with c[jb] = w^T w (BVDotColumnInc / BVDotVec), w -= V c (BVMultColumn / BVMultVec),
+// h += c (BV_AddCoefficients), onorm = sqrt(w^T w) before the pass (BV_SquareRoot / BVNormVec),
+// norm = sqrt(onorm^2 - c^T c), or the explicit norm of the updated vector when that estimate is
+// not positive.  The DOT is the fused pass kernel's plain-dot mode; the update is BVMultVec's kernel.
+extern "C" b200_status b200_bv_gram_schmidt(b200_bv bv, int j, double *v, double *h, double *c, double *onorm,
+                                            double *norm) {
+  B200_ARG_CHECK(bv, "null argument");
+  const bool column = v == nullptr;
+  const int jb = column ? j : bv->k;
+  B200_ARG_CHECK(jb >= 0 && jb < bv->m + (column ? 0 : 1) && (!column || j < bv->m), "column index out of range");
+  cudaStream_t s = bv->stream;
+  const int wcol = column ? j : bv->m;
+  if (!column) B200_CUDA_CHECK(copy_launch(col(bv, bv->m), v, bv->n, s));  // staged in the work column
+  double *w = col(bv, wcol);
+  GsPassArgs a{};
+  a.V = bv->V;
+  a.ld = bv->ld;
+  a.total_cols = bv->m + 1;
+  a.n = bv->n;
+  a.jb = jb;
+  a.wcol = wcol;
+  a.step = -1;
+  B200_CUDA_CHECK(gs_dot_launch(a, bv->gs, s));  // cnew[0..jb-1] = V^T w, cnew[jb] = w^T w
+  const double *cnew = bv->gs.cnew;
+  if (jb > 0) B200_CUDA_CHECK(multvec_launch(bv->V, bv->ld, bv->n, jb, cnew, -1.0, 1.0, w, s));
+  if (c) B200_CUDA_CHECK(cudaMemcpyAsync(c, cnew, sizeof(double) * (jb + 1), cudaMemcpyDeviceToDevice, s));
+  double *hh = h ? h : bv->coefbuf + (size_t)j * bv->ldc;
+  if (jb > 0 && (h || column)) B200_CUDA_CHECK(axmy_launch(hh, cnew, -1.0, jb, s));  // h += c
+  if (!column) B200_CUDA_CHECK(copy_launch(v, w, bv->n, s));
+  if (!onorm && !norm) return B200_OK;
+  B200_CHECK(bv_reserve(bv, 0, 0));
+  B200_CUDA_CHECK(cudaMemcpyAsync(bv->hpin + 64, cnew, sizeof(double) * (jb + 1), cudaMemcpyDeviceToHost, s));
+  B200_CUDA_CHECK(cudaStreamSynchronize(s));
+  const double *hc = bv->hpin + 64;
+  const double self = hc[jb];
+  if (column && !(self > -10.0 * 2.220446049250313e-16)) {  // BV_SafeSqrt
+    b200_set_last_error(__FILE__, __LINE__, "invalid inner product (negative self dot product)");
+    return B200_ERR_INNER;
+  }
+  const double beta = self < 0.0 ? 0.0 : std::sqrt(self);
+  if (onorm) *onorm = beta;
+  if (norm) {
+    double sum = 0.0;
+    for (int i = 0; i < jb; ++i) sum += hc[i] * hc[i];  // BV_SquareSum
+    const double t = beta * beta - sum;
+    if (t > 0.0) {
+      *norm = std::sqrt(t);
+    } else {  // BV_NormVecOrColumn
+      double ss = 0.0;
+      B200_CUDA_CHECK(sumsq_launch(w, bv->n, bv->scal, bv->red, bv->red_len, s));
+      B200_CUDA_CHECK(cudaMemcpyAsync(&ss, bv->scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+      B200_CUDA_CHECK(cudaStreamSynchronize(s));
+      *norm = std::sqrt(ss);
+    }
+  }
+  return B200_OK;
+}
+
+// BVResize (bvbasic.c:338-388, BVResize_Svec svec.c:261-300): new storage of m columns, the first
+// min(m, old m) columns copied when copy is set; l and k are clipped to m.
+extern "C" b200_status b200_bv_resize(b200_bv bv, int m, int copy) {
+  B200_ARG_CHECK(bv && m > 0, "the number of columns must be positive");
+  if (m == bv->m) return B200_OK;
+  b200_bv nb = nullptr;
+  B200_CHECK(b200_bv_create(bv->n, m, bv->stream, &nb));
+  if (copy) {
+    const int keep = std::min(m, bv->m);
+    B200_CUDA_CHECK(cudaMemcpyAsync(nb->V, bv->V, sizeof(double) * (size_t)bv->ld * keep, cudaMemcpyDeviceToDevice,
+                                    bv->stream));
+  }
+  nb->eta = bv->eta;
+  nb->orthog_block = bv->orthog_block;
+  nb->seed = bv->seed;
+  nb->nrand = bv->nrand;
+  nb->l = std::min(bv->l, m);
+  nb->k = std::min(bv->k, m);
+  B200_CUDA_CHECK(cudaStreamSynchronize(bv->stream));
+  std::swap(*bv, *nb);  // the caller's handle keeps its identity and gets the new storage
+  return b200_bv_destroy(nb);
+}
+
+// BVCopy (bvbasic.c:1779-1808, BVCopy_Svec svec.c:233-247): Y(:, Y.l + j) = X(:, X.l + j) for the
+// k - l active columns of X; Y needs as many columns from its l.
+extern "C" b200_status b200_bv_copy(b200_bv X, b200_bv Y) {
+  B200_ARG_CHECK(X && Y && X->n == Y->n, "mismatching local dimension");
+  const int nc = X->k - X->l;
+  B200_ARG_CHECK(nc <= Y->m - Y->l, "Y has not enough non-leading columns");
+  if (X == Y || nc <= 0) return B200_OK;
+  B200_CUDA_CHECK(cudaMemcpy2DAsync(col(Y, Y->l), sizeof(double) * Y->ld, col(X, X->l), sizeof(double) * X->ld,
+                                    sizeof(double) * X->n, nc, cudaMemcpyDeviceToDevice, X->stream));
+  if (Y->stream != X->stream) B200_CUDA_CHECK(cudaStreamSynchronize(X->stream));
+  return B200_OK;
+}
+
+// BVNormalize (bvglobal.c:829-866) for real scalars (eigi NULL): every active column scaled to unit
+// 2-norm (a zero column is left as it is); norms_host (nullable, k - l values) receives the norms.
+extern "C" b200_status b200_bv_normalize(b200_bv bv, double *norms_host) {
+  B200_ARG_CHECK(bv, "null argument");
+  const int nc = bv->k - bv->l;
+  if (nc <= 0) return B200_OK;
+  std::vector<double> nrm((size_t)nc);
+  B200_CHECK(bv_column_norms(bv, nrm.data()));
+  for (int i = 0; i < nc; ++i)
+    if (nrm[i] != 0.0 && nrm[i] != 1.0) B200_CUDA_CHECK(scale_launch(col(bv, bv->l + i), bv->n, 1.0 / nrm[i], bv->stream));
+  if (norms_host) memcpy(norms_host, nrm.data(), sizeof(double) * nc);
+  return B200_OK;
+}
+
+// BVMultInPlaceHermitianTranspose (bvops.c:268-296) for real scalars: V(:,s:e) = V(:,l:k) Q(s:e,l:k)^T,
+// i.e. the in-place product with the transpose of the host matrix Q (leading dimension ldq >= e).
+extern "C" b200_status b200_bv_mult_inplace_trans(b200_bv bv, const double *Q, int ldq, int s, int e) {
+  B200_ARG_CHECK(bv && Q && 0 <= s && s <= e && e <= bv->m && ldq >= e, "invalid arguments");
+  const int k = bv->k;
+  std::vector<double> Qt((size_t)k * std::max(e, 1));  // Qt(i, c) = Q(c, i): leading dimension k
+  for (int c = s; c < e; ++c)
+    for (int i = 0; i < k; ++i) Qt[(size_t)c * k + i] = Q[(size_t)i * ldq + c];
+  return b200_bv_mult_inplace(bv, Qt.data(), k, s, e);
+}
+
 extern "C" b200_status b200_bv_scale_column(b200_bv bv, int j, double alpha) {
   B200_ARG_CHECK(bv && j < bv->m, "column index out of range");
   if (j < 0) {
@@ -1278,9 +1401,8 @@ extern "C" b200_status b200_eps_destroy(b200_eps eps) {
   cudaFree(eps->resid_buf);
   cudaFree(eps->op_buf);
   cudaFree(eps->dinv);
-  cudaFree(eps->V32);
-  cudaFree(eps->wv);
-  cudaFree(eps->blk);
+  cudaFree(eps->rb32);
+  cudaFree(eps->rb64);
   cudaFree(eps->mred);
   delete eps;
   return B200_OK;
@@ -1367,21 +1489,16 @@ extern "C" b200_status b200_eps_set_precision(b200_eps eps, int precision) {
   return B200_OK;
 }
 
-extern "C" b200_status b200_eps_set_mixed_eta(b200_eps eps, double eta) {
-  B200_ARG_CHECK(eps && eta <= 1.0, "eta must be at most 1");
-  eps->mixed_eta1 = eta;
-  return B200_OK;
-}
-
 extern "C" b200_status b200_eps_set_mixed_options(b200_eps eps, double tol_low, int degree, int guard,
-                                                  int max_sweeps, int fp32_first_pass) {
+                                                  int max_sweeps, int fp64_gram) {
   B200_ARG_CHECK(eps, "null argument");
   B200_ARG_CHECK(degree <= 4096 && max_sweeps <= 100000, "degree or max_sweeps too large");
+  B200_ARG_CHECK(guard <= 127, "guard too large: the block holds at most 128 vectors");
   eps->mixed_tol_low = tol_low > 0.0 ? tol_low : 0.0;
   eps->mixed_degree = degree > 0 ? degree : 0;
   eps->mixed_guard = guard >= 0 ? guard : -1;
   eps->mixed_max_sweeps = max_sweeps > 0 ? max_sweeps : 0;
-  eps->mixed_fp32_pass = fp32_first_pass ? 1 : 0;
+  eps->mixed_fp64_gram = fp64_gram ? 1 : 0;
   return B200_OK;
 }
 

@@ -109,22 +109,18 @@ struct b200_eps_s {
   int nini_eff = 0;  // initial vectors kept by BVInsertVecs in the last setup
   double *dinv = nullptr;  // device inverse diagonal for the Jacobi preconditioner
   const void *dinv_of = nullptr;
-  // mixed-precision Krylov-Schur (b200_eps_set_precision): parameters and device buffers
+  // mixed-precision form (b200_eps_set_precision): parameters and device buffers
   int precision = B200_PRECISION_FP64;
-  double mixed_tol_low = 0.0;  // phase-1 tolerance (0: default)
-  int mixed_degree = 0;        // Chebyshev degree (0: default)
-  int mixed_guard = -1;        // guard columns of the refinement block (-1: default)
-  int mixed_max_sweeps = 0;    // refinement sweeps (0: default)
-  int mixed_fp32_pass = 0;     // first Gram-Schmidt pass in FP32 arithmetic
-  double mixed_eta1 = 0.0;     // DGKS threshold of the FP32-basis phase (0: one pass; < 0: the BV's 0.7071)
-  float *V32 = nullptr;        // FP32 basis, ld32 x (ncv + 1)
-  size_t V32_cap = 0;
-  int ld32 = 0;
-  double *wv = nullptr;        // FP64 vector being orthogonalised (n + 2)
-  size_t wv_cap = 0;
-  double *blk = nullptr;       // 5 FP64 blocks of ldb x kb for the refinement phase
-  size_t blk_cap = 0;
-  double *mred = nullptr;      // reductions and small device matrices of the refinement phase
+  double mixed_tol_low = 0.0;  // tolerance of the FP32 phase (0: default)
+  int mixed_degree = 0;        // largest Chebyshev degree of one sweep (0: default)
+  int mixed_guard = -1;        // block columns beyond nev (-1: default)
+  int mixed_max_sweeps = 0;    // sweeps per phase (0: default)
+  int mixed_fp64_gram = 0;     // 1: FP64 Gram for the FP32 phase's orthonormalisation (0: tensor cores)
+  float *rb32 = nullptr;       // FP32 row-major blocks (4 x n x block width)
+  size_t rb32_cap = 0;
+  double *rb64 = nullptr;      // FP64 row-major blocks (4 x n x block width)
+  size_t rb64_cap = 0;
+  double *mred = nullptr;      // small device matrices and reduction work of the mixed form
   size_t mred_cap = 0;
 };
 

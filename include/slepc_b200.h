@@ -308,6 +308,13 @@ b200_status b200_eps_set_tolerances(b200_eps eps, double tol, int max_it);
 b200_status b200_eps_set_which_eigenpairs(b200_eps eps, int which);
 /* EPSKrylovSchurSetRestart (krylovschur.c:351-361), keep in [0.1,0.9]. */
 b200_status b200_eps_krylovschur_set_restart(b200_eps eps, double keep);
+/* EPSKrylovSchurSetLocking / GetLocking (krylovschur.c:427-500): lock = 1
+ * (default) locks converged pairs at each restart; 0 selects the non-locking
+ * variant (krylovschur.c:295: the kept vectors include the converged ones,
+ * which stay in the active subspace), which needs mpd = ncv (krylovschur.c:116,
+ * B200_ERR_SUP otherwise).  The mixed-precision form, a block method, ignores it. */
+b200_status b200_eps_krylovschur_set_locking(b200_eps eps, int lock);
+b200_status b200_eps_krylovschur_get_locking(b200_eps eps, int *lock);
 /* EPSSetInitialSpace with one vector (epssetup.c:613, inserted at setup by BVInsertVecs). */
 b200_status b200_eps_set_initial_space(b200_eps eps, const double *v0_host);
 b200_status b200_eps_set_initial_space_device(b200_eps eps, const double *v0_dev);

@@ -75,6 +75,11 @@ def set_threads(n):
     lib().oracle_set_threads(int(n))
 
 
+def set_locking(lock):
+    """EPSKrylovSchurSetLocking for the oracle's Krylov-Schur (process-wide; True by default)."""
+    lib().oracle_set_locking(1 if lock else 0)
+
+
 def spmv(A, x):
     rowptr, colind, vals = _csr(A)
     x = np.ascontiguousarray(x, dtype=np.float64)

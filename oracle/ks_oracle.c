@@ -473,6 +473,11 @@ static int get_start_vector(obv *bv, int i, int nini, int *breakdown)
  * X (n x nconv, ld = n) the converged Ritz vectors sorted by SlepcSortEigenvalues,
  * evals (nconv) sorted values; info.
  */
+/* EPSKrylovSchurSetLocking (krylovschur.c:427-434): 1 (default) locks converged pairs at a restart;
+   0 selects the non-locking variant (krylovschur.c:295), which keeps them in the active subspace. */
+static int g_ks_lock = 1;
+void oracle_set_locking(int lock) { g_ks_lock = lock ? 1 : 0; }
+
 static int eps_solve_op(const orc_op *op, const double *v0, int nev, int ncv, int mpd, double tol, int max_it,
                         int which, int max_restarts, double *evals, double *X, double *errest_out, int *info_out)
 {
@@ -576,6 +581,10 @@ static int eps_solve_op(const orc_op *op, const double *v0, int nev, int ncv, in
     else {
       l = (int)((nv - k) * keep);
       if (l < 1) l = 1;
+    }
+    if (!g_ks_lock && l > 0) { /* non-locking variant: reset the number of converged pairs */
+      l += k;
+      k = 0;
     }
 
     if (info.reason == ORC_ITERATING) {

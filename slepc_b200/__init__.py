@@ -76,6 +76,8 @@ _SIGS = {
     "b200_mat_norm_inf": (ctypes.c_int, [_vp, _dp]),
     "b200_eps_set_type": (ctypes.c_int, [_vp, ctypes.c_int]),
     "b200_eps_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_eps_krylovschur_set_locking": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_eps_krylovschur_get_locking": (ctypes.c_int, [_vp, _ip]),
     "b200_bv_gram_schmidt": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _dp, _dp]),
     "b200_bv_resize": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
     "b200_bv_copy": (ctypes.c_int, [_vp, _vp]),
@@ -678,6 +680,15 @@ class EPS:
         on an FP32 basis with FP32 matrix values to a loose tolerance, then FP64
         Chebyshev-filtered Rayleigh-Ritz refinement of the block of leading Ritz vectors."""
         _check(lib().b200_eps_set_precision(self.handle, precision))
+
+    def setKrylovSchurLocking(self, lock):
+        """EPSKrylovSchurSetLocking (the non-locking variant needs mpd = ncv)."""
+        _check(lib().b200_eps_krylovschur_set_locking(self.handle, 1 if lock else 0))
+
+    def getKrylovSchurLocking(self):
+        v = ctypes.c_int()
+        _check(lib().b200_eps_krylovschur_get_locking(self.handle, ctypes.byref(v)))
+        return bool(v.value)
 
     def setMixedOptions(self, tol_low=0.0, degree=0, guard=-1, max_sweeps=0, fp64_gram=False):
         """Parameters of the mixed form (b200_eps_set_mixed_options); 0 (or -1 for guard) keeps the default."""

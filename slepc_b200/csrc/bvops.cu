@@ -16,6 +16,11 @@
 //   residual     EPSComputeResidualNorm_Private (src/eps/interface/epssolve.c:666-722):
 //                SpMV fused with r = Ax - lambda x and its sum of squares
 //   random       stand-in for BVSetRandomColumn (bvops.c:360-379)
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <atomic>
+
 #include "common.h"
 #include "kernels.h"
 
@@ -169,6 +174,134 @@ __global__ void __launch_bounds__(kGemmThreads) panel_dmma_kernel(const TI *X, i
       }
     }
   }
+}
+
+// The same FP64 tensor-core product with the panel loads taken off the critical path: a producer warp
+// streams each 64-row panel of X into a ring of shared-memory stages with one 2-D TMA load of 72 rows x
+// kp columns (the box's 8 extra rows -- the next panel's first rows, or the zero fill past n -- give the
+// 72-double column stride that keeps the fragment loads at two wavefronts; their values are never
+// used), so the DMMA k-loop of one panel overlaps the loads of the next ones.  The eight consumer warps
+// compute rows 8w..8w+7 against every 8-column tile of Q (kept in shared memory) and write their
+// 8 x 2 results per tile straight from registers.  In place is safe: a panel has landed in shared
+// memory (its full barrier) before any of its rows is written, prefetches read other panels, and the
+// only rows two CTAs touch at once are the discarded extra rows.  Waits are bounded; a timeout sets
+// g_panel_err and the CTA stops (panel_gemm_error reads it).
+constexpr int kTmaRows = kRB + 8;          // rows of a panel's TMA box (the panel's column stride in shared memory)
+constexpr int kTmaThreads = kGemmThreads + 32;
+__device__ int g_panel_err;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ bool mbar_wait_parity(uint64_t *bar, uint32_t parity) {
+  for (long long it = 0; it < kSpinLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(kTmaThreads, 1) panel_dmma_tma_kernel(const __grid_constant__ CUtensorMap tx, double *Y,
+                                                                        int ldy, int n, int kq,
+                                                                        const double *__restrict__ Q, int ldq, int nc,
+                                                                        double alpha, double beta, int stages) {
+  extern __shared__ __align__(16) unsigned char tma_raw[];  // stages start 128-byte aligned (TMA destinations)
+  double *sm = reinterpret_cast<double *>(tma_raw + ((128u - (smem_addr(tma_raw) & 127u)) & 127u));
+  __shared__ __align__(8) uint64_t full[8], empty[8];
+  __shared__ int last_issue[8];
+  __shared__ volatile int stop;
+  const int kp = (kq + 3) & ~3;
+  constexpr int ncp = NT * 8;
+  const int SQ = dmma_q_stride(ncp);
+  const size_t stage_elems = (size_t)kp * kTmaRows;
+  double *Xst = sm;                               // stages x [kp][kTmaRows]
+  double *Qs = sm + (size_t)stages * stage_elems; // kp x SQ
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int npanels = (n + kRB - 1) / kRB;
+  const int mine = blockIdx.x < npanels ? (npanels - 1 - blockIdx.x) / gridDim.x + 1 : 0;  // panels of this CTA
+  if (tid == 0) {
+    for (int s = 0; s < stages; ++s) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&full[s])), "r"(1) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&empty[s])), "r"(kGemmThreads / 32)
+                   : "memory");
+      last_issue[s] = -1;
+    }
+    stop = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int idx = tid; idx < kp * ncp; idx += kTmaThreads) {
+    const int k = idx / ncp, j = idx - k * ncp;
+    Qs[k * SQ + j] = (k < kq && j < nc) ? Q[(size_t)k + (size_t)j * ldq] : 0.0;
+  }
+  __syncthreads();
+  const uint32_t stage_bytes = (uint32_t)(stage_elems * sizeof(double));
+  if (warp == kGemmThreads / 32) {
+    if (lane == 0) {
+      for (int i = 0; i < mine && !stop; ++i) {
+        const int s = i % stages;
+        if (i >= stages && !mbar_wait_parity(&empty[s], ((i / stages) - 1) & 1)) {
+          atomicOr(&g_panel_err, kDevErrTimeout);
+          stop = 1;
+          break;
+        }
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&full[s])),
+                     "r"(stage_bytes)
+                     : "memory");
+        const int r0 = (blockIdx.x + i * gridDim.x) * kRB;
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+            "[%4];" ::"r"(smem_addr(Xst + (size_t)s * stage_elems)),
+            "l"(reinterpret_cast<uint64_t>(&tx)), "r"(r0), "r"(0), "r"(smem_addr(&full[s]))
+            : "memory");
+        last_issue[s] = i;
+      }
+    }
+  } else {
+    const int g = lane >> 2, t = lane & 3;
+    for (int i = 0; i < mine && !stop; ++i) {
+      const int s = i % stages;
+      if (!mbar_wait_parity(&full[s], (i / stages) & 1)) {
+        atomicOr(&g_panel_err, kDevErrTimeout);
+        stop = 1;
+        break;
+      }
+      const double *xa = Xst + (size_t)s * stage_elems + t * kTmaRows + warp * 8 + g;
+      const double *qb = Qs + t * SQ + g;
+      double acc[NT][2];
+#pragma unroll
+      for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = 0.0;
+      for (int k0 = 0; k0 < kp; k0 += 4) {
+        const double a = xa[k0 * kTmaRows];
+#pragma unroll
+        for (int j = 0; j < NT; ++j) dmma_8x8x4(acc[j], a, qb[k0 * SQ + 8 * j]);
+      }
+      __syncwarp();
+      if (lane == 0)
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s])) : "memory");
+      const long long r = (long long)(blockIdx.x + i * gridDim.x) * kRB + warp * 8 + g;
+      if (r < n) {
+#pragma unroll
+        for (int j = 0; j < NT; ++j)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int c = 8 * j + 2 * t + h;
+            if (c < nc) {
+              double *y = Y + (size_t)c * ldy + r;
+              *y = beta == 0.0 ? alpha * acc[j][h] : alpha * acc[j][h] + beta * *y;
+            }
+          }
+      }
+    }
+  }
+  __syncthreads();
+  // loads issued but never consumed (only after a timeout) land before the CTA exits
+  if (tid == 0)
+    for (int s = 0; s < stages; ++s)
+      if (last_issue[s] >= 0) mbar_wait_parity(&full[s], (last_issue[s] / stages) & 1);
 }
 
 // Y(:,j) = alpha * X(:,0:nx) Q(0:nx,j) + beta * Y(:,j), one thread per row, Q column in registers-free loop.
@@ -568,11 +701,79 @@ unsigned grid_for(long long len, int threads) {
 
 }  // namespace
 
+std::atomic<bool> g_panel_launched{false};  // a pipelined product ran since the last error check
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void *ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      ptr = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+  }();
+  return fn;
+}
+
+// The pipelined FP64 product when X is FP64, 16-byte aligned with an even leading dimension, and two
+// or more stages fit in shared memory beside Q; cudaErrorNotSupported otherwise (the caller falls back).
+cudaError_t panel_dmma_tma_launch(const double *X, int ldx, double *Y, int ldy, int n, int kq, const double *Q, int ldq,
+                                  int nc, cudaStream_t stream, double alpha, double beta) {
+  const int kp = (kq + 3) & ~3, nt = (nc + 7) / 8, ncp = 8 * nt;
+  if (kp > 256 || ((uintptr_t)X & 15) || (ldx & 1) || nt < 1 || nt > 16) return cudaErrorNotSupported;
+  const size_t stage = sizeof(double) * (size_t)kp * kTmaRows;
+  const size_t qbytes = sizeof(double) * (size_t)kp * dmma_q_stride(ncp);
+  const size_t avail = max_dynamic_smem() - 1024 - 128;  // static barriers, alignment and slack
+  if (avail < qbytes + 2 * stage) return cudaErrorNotSupported;
+  int stages = (int)((avail - qbytes) / stage);
+  if (stages > 8) stages = 8;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return cudaErrorNotSupported;
+  CUtensorMap tm;
+  const cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)kq};
+  const cuuint64_t strides[1] = {(cuuint64_t)ldx * sizeof(double)};
+  const cuuint32_t box[2] = {(cuuint32_t)kTmaRows, (cuuint32_t)kp};
+  const cuuint32_t estr[2] = {1, 1};
+  if (enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(X), dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return cudaErrorNotSupported;
+  const size_t smem = qbytes + (size_t)stages * stage + 128;
+  const int npanels = (n + kRB - 1) / kRB;
+  int grid = num_sms();
+  if (grid > npanels) grid = npanels;
+  cudaError_t err = cudaSuccess;
+  switch (nt) {
+#define B200_TMA_CASE(NT)                                                                                       \
+  case NT:                                                                                                      \
+    err = cudaFuncSetAttribute(panel_dmma_tma_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+    if (err != cudaSuccess) return err;                                                                         \
+    panel_dmma_tma_kernel<NT><<<grid, kTmaThreads, smem, stream>>>(tm, Y, ldy, n, kq, Q, ldq, nc, alpha, beta,      \
+                                                                   stages);                                    \
+    break;
+    B200_TMA_CASE(1) B200_TMA_CASE(2) B200_TMA_CASE(3) B200_TMA_CASE(4) B200_TMA_CASE(5) B200_TMA_CASE(6)
+    B200_TMA_CASE(7) B200_TMA_CASE(8) B200_TMA_CASE(9) B200_TMA_CASE(10) B200_TMA_CASE(11) B200_TMA_CASE(12)
+    B200_TMA_CASE(13) B200_TMA_CASE(14) B200_TMA_CASE(15) B200_TMA_CASE(16)
+#undef B200_TMA_CASE
+    default:
+      return cudaErrorNotSupported;
+  }
+  count_launch();
+  g_panel_launched.store(true);
+  return cudaGetLastError();
+}
+
 template <typename TI, typename TO>
 cudaError_t panel_gemm_launch(const TI *X, int ldx, TO *Y, int ldy, int n, int kq, const double *Q, int ldq, int nc,
                               cudaStream_t stream, double alpha = 1.0, double beta = 0.0) {
   if (nc <= 0 || kq <= 0 || n <= 0) return cudaSuccess;
   if (nc > 16 * 8 || kq > kMaxCols) return cudaErrorInvalidValue;
+  if constexpr (sizeof(TI) == sizeof(double) && sizeof(TO) == sizeof(double)) {
+    const cudaError_t err = panel_dmma_tma_launch(reinterpret_cast<const double *>(X), ldx,
+                                                  reinterpret_cast<double *>(Y), ldy, n, kq, Q, ldq, nc, stream,
+                                                  alpha, beta);
+    if (err != cudaErrorNotSupported) return err;
+  }
   {
     // FP64 tensor cores when the padded panel and Q fit in shared memory
     const int kp = (kq + 3) & ~3, nt = (nc + 7) / 8, ncp = 8 * nt;
@@ -631,6 +832,20 @@ cudaError_t panel_gemm_launch(const TI *X, int ldx, TO *Y, int ldy, int n, int k
   }
   count_launch();
   return cudaGetLastError();
+}
+
+cudaError_t panel_gemm_error(int *err, cudaStream_t stream) {
+  int v = 0;
+  *err = 0;
+  if (!g_panel_launched.exchange(false)) return cudaSuccess;
+  cudaError_t e = cudaMemcpyFromSymbolAsync(&v, g_panel_err, sizeof(int), 0, cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e == cudaSuccess && v) {
+    const int zero = 0;
+    e = cudaMemcpyToSymbolAsync(g_panel_err, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, stream);
+  }
+  *err = v;
+  return e;
 }
 
 cudaError_t multinplace_launch(double *V, int ld, int n, int l, int k, const double *Q, int ldq, int s, int e,

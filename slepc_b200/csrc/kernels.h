@@ -174,6 +174,10 @@ cudaError_t csr_transpose_device(int rows, int cols, long long nnz, const int *r
                                  cudaStream_t s);
 
 // ---- Dense tall-skinny operations (bvops.cu)
+// Device error bits of the TMA-pipelined panel product since the last call (read, then cleared;
+// synchronises the stream when such a product ran since then): kDevErrTimeout when a bounded wait
+// gave up.
+cudaError_t panel_gemm_error(int *err, cudaStream_t stream);
 // V(:,s:e) = V(:,l:k) * Q(l:k,s:e), row-blocked, in place; Q points at element (l,s).
 cudaError_t multinplace_launch(double *V, int ld, int n, int l, int k, const double *Q, int ldq, int s, int e,
                                cudaStream_t stream);

@@ -729,6 +729,9 @@ static b200_status bv_read_state(b200_bv bv, GsState *out) {
     return B200_ERR_INNER;
   }
   if (out->err) B200_DEV_ERR("a Gram-Schmidt kernel reported a device-side error (bounded wait expired)");
+  int perr = 0;
+  B200_CUDA_CHECK(panel_gemm_error(&perr, bv->stream));
+  if (perr) B200_DEV_ERR("the panel product kernel reported a device-side error (bounded wait expired)");
   return B200_OK;
 }
 
@@ -1443,6 +1446,18 @@ extern "C" b200_status b200_eps_set_which_eigenpairs(b200_eps eps, int which) {
   return B200_OK;
 }
 
+extern "C" b200_status b200_eps_krylovschur_set_locking(b200_eps eps, int lock) {
+  B200_ARG_CHECK(eps, "null argument");
+  eps->lock = lock ? 1 : 0;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_krylovschur_get_locking(b200_eps eps, int *lock) {
+  B200_ARG_CHECK(eps && lock, "null argument");
+  *lock = eps->lock;
+  return B200_OK;
+}
+
 extern "C" b200_status b200_eps_krylovschur_set_restart(b200_eps eps, double keep) {
   B200_ARG_CHECK(eps && keep >= 0.1 && keep <= 0.9, "keep must be in [0.1,0.9]");
   eps->keep = keep;
@@ -1601,6 +1616,10 @@ static b200_status eps_setup(b200_eps eps) {
   }
   if (mpd <= 0) mpd = ncv;
   B200_ARG_CHECK(ncv <= nev + mpd, "the value of ncv must not be larger than nev+mpd");
+  if (!eps->lock && mpd < ncv) {  // krylovschur.c:116
+    b200_set_last_error(__FILE__, __LINE__, "should not use the mpd parameter in the non-locking variant");
+    return B200_ERR_SUP;
+  }
   B200_ARG_CHECK(ncv <= n, "ncv cannot exceed the problem size");
   B200_ARG_CHECK(ncv + 2 < kMaxCols, "ncv too large for this build (ncv <= 251)");
   eps->n_ = n;
@@ -1718,6 +1737,10 @@ extern "C" b200_status b200_eps_solve(b200_eps eps) {
 
     if (eps->reason != B200_CONVERGED_ITERATING || breakdown || k == nv) l = 0;
     else l = std::max(1, (int)((nv - k) * eps->keep));
+    if (!eps->lock && l > 0) {  // non-locking variant (krylovschur.c:295): reset the converged count
+      l += k;
+      k = 0;
+    }
 
     if (eps->reason == B200_CONVERGED_ITERATING) {
       if (breakdown || k == nv) {

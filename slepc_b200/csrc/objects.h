@@ -79,6 +79,7 @@ struct b200_eps_s {
   int max_it = 0;
   int which = B200_LARGEST_MAGNITUDE;
   double keep = 0.5;  // krylovschur.c:122
+  int lock = 1;       // EPSKrylovSchurSetLocking (krylovschur.c:427-434; locking by default)
   std::vector<double> v0;
   const double *v0_dev = nullptr;
   int nini = 0;

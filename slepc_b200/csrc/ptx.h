@@ -2,12 +2,14 @@
 // mbarriers, 2-D TMA tile loads, and the tcgen05 tensor-core instructions (TMEM allocation,
 // shared-memory operand descriptors, MMA issue, commit, TMEM loads).
 //
-// Operand layout used here: an MN-major operand in the canonical 128-byte-swizzled form that a
-// TMA tile load with CU_TENSOR_MAP_SWIZZLE_128B and a 128-byte inner box writes.  For 32-bit
-// elements an "MN block" is 32 elements (128 bytes) wide; a tile of R rows (the K dimension) of one
-// MN block is R x 128 bytes, row r at byte 128 r with its 16-byte chunks permuted by r mod 8.  One
-// MMA of kind::tf32 consumes K = 8 rows, i.e. one 1024-byte swizzle atom of every MN block; the MN
-// blocks of a wider operand sit LBO bytes apart.
+// Operand layout used here: an MN-major TF32 operand, for which the tensor cores accept one
+// shared-memory layout only, the 128-byte swizzle with 32-byte atomicity (descriptor layout type
+// SWIZZLE_128B_BASE32B); a TMA tile load with CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B and a 128-byte
+// inner box writes exactly that.  An "MN block" is 32 elements (128 bytes) wide; a tile of R rows
+// (the K dimension) of one MN block is R x 128 bytes, row r at byte 128 r with its four 32-byte
+// chunks permuted by r mod 4, so a swizzle atom is 4 rows (512 bytes, the SBO between K atoms).  One
+// MMA of kind::tf32 consumes K = 8 rows (two atoms, 1024 bytes); the MN blocks of a wider operand
+// sit LBO bytes apart.
 #pragma once
 
 #include <cuda.h>
@@ -73,15 +75,16 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// Shared-memory matrix descriptor: start address, leading and stride byte offsets, layout
-// 128-byte swizzle (type 2), descriptor version 1 (sm_100), base offset 0 (1024-byte aligned atoms).
-__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+// Shared-memory matrix descriptor: start address, leading and stride byte offsets, descriptor
+// version 1 (sm_100), base offset 0 (atoms aligned to their swizzle period), layout type 1 =
+// 128-byte swizzle with 32-byte atomicity (the layout of MN-major TF32 operands).
+__device__ __forceinline__ uint64_t smem_desc_sw128_32b(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
   d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
   d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
   d |= (uint64_t)1 << 46;  // version
-  d |= (uint64_t)2 << 61;  // SWIZZLE_128B
+  d |= (uint64_t)1 << 61;  // SWIZZLE_128B_BASE32B
   return d;
 }
 

@@ -184,7 +184,8 @@ __global__ void __launch_bounds__(kRbThreads) rb_spmm_rest_kernel(int nrest, int
 // ---------------------------------------------------------------- tensor-core Gram (TF32)
 //
 // G = X^T Y over row tiles of KT rows.  Warp 0 (one lane) streams each tile of X (and Y) into a
-// ring of shared-memory stages with 2-D TMA loads (128-byte swizzle, one box per 32-column strip);
+// ring of shared-memory stages with 2-D TMA loads (128-byte swizzle with 32-byte atoms, the only
+// layout the tensor cores take for MN-major TF32; one box per 32-column strip);
 // warp 1 (one lane) issues, for every 8 rows of the tile, one tcgen05.mma kind::tf32 of shape
 // BP x BP x 8 with both operands MN-major (the strips are the MN blocks, LBO apart), accumulating in
 // TMEM, and commits each stage back to the producer; at the end all four warps read the BP x BP FP32
@@ -269,8 +270,8 @@ __global__ void __launch_bounds__(128, 1) rb_gram_tf32_kernel(const __grid_const
       const uint32_t b0 = CROSS ? a0 + C::TILE : a0;
 #pragma unroll
       for (int k = 0; k < C::KT / 8; ++k)
-        ptx::mma_tf32(tmem, ptx::smem_desc_sw128(a0 + 1024u * k, C::STRIP, 1024),
-                      ptx::smem_desc_sw128(b0 + 1024u * k, C::STRIP, 1024), idesc, t > 0 || k > 0);
+        ptx::mma_tf32(tmem, ptx::smem_desc_sw128_32b(a0 + 1024u * k, C::STRIP, 512),
+                      ptx::smem_desc_sw128_32b(b0 + 1024u * k, C::STRIP, 512), idesc, t > 0 || k > 0);
       ptx::mma_commit(&empty[s]);  // the stage is free once these MMAs have read it
     }
     consumed = t;
@@ -693,8 +694,8 @@ cudaError_t rb_make_tmap_f32(CUtensorMap *tm, const float *X, int n, int bp) {
   const cuuint32_t box[2] = {32, (cuuint32_t)kt};
   const cuuint32_t estr[2] = {1, 1};
   CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(X), dims, strides, box, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 

@@ -9,6 +9,8 @@ time one kernel family in isolation with CUDA events:
   python slepc_b200/kernel_bench.py cross            # A x, A^T z, A^T A x of the 2M x 500k power-law matrix
   python slepc_b200/kernel_bench.py batched          # the batched Krylov-Schur launch on a small k-NN batch
   python slepc_b200/kernel_bench.py lobpcg --lgrid 512   # LOBPCG per block orthogonalization type
+  python slepc_b200/kernel_bench.py mixed            # the mixed-precision solve with per-filter timing
+  python slepc_b200/kernel_bench.py rbgram           # the tensor-core and FP64 block Gram products
 
 Prints one JSON line per kernel family: average ms per call and algorithmic GB/s.
 """
@@ -124,9 +126,9 @@ def spmm(args, torch):
 
 
 def mixed(args, torch):
-    """A mixed-precision solve of the 3-D Laplacian (nev 32, ncv 80) cut after --restarts restarts
-    of the FP32-basis phase and --sweeps refinement sweeps: a short, complete run of every kernel of
-    the mixed form (for profiling); prints the solver's counters."""
+    """The mixed-precision solve of the 3-D Laplacian (nev 32, ncv 80, tol 1e-8) with per-filter timing:
+    the solver's counters and the block SpMV's algorithmic GB/s (device-counted bytes over the CUDA-event
+    time of the filters)."""
     csr = P.laplacian_3d(args.grid)
     n = len(csr[0]) - 1
     A = S.Mat().createAIJ(csr)
@@ -137,13 +139,49 @@ def mixed(args, torch):
     E.setWhichEigenpairs(S.LARGEST_REAL)
     E.setInitialSpace(P.start_vector(n, 0))
     E.setPrecision(S.EPS.Precision.MIXED)
-    E.setMaxRestarts(args.restarts)
-    E.setMixedOptions(tol_low=1e-6, degree=32, max_sweeps=args.sweeps)
+    if args.fp64_gram:
+        E.setMixedOptions(fp64_gram=True)
+    E.solve()
+    E.setTiming(True)
     E.solve()
     st = E.getStats()
+    nconv = E.getConverged()
+    err = max(E.computeError(i) for i in range(min(nconv, 32))) if nconv else None
     E.destroy()
     A.destroy()
-    return {"kernel": "mixed solve (FP32-basis phase + refinement)", "n": n, **st}
+    gbs = st["gs_bytes"] / (st["ms_spmv"] * 1e-3) / 1e9 if st["ms_spmv"] > 0 else None
+    return {"kernel": "mixed solve (Chebyshev-filtered block, FP32 then FP64)", "n": n, "nconv": nconv,
+            "max_rel_residual": err, "filter_GBps": gbs, **st}
+
+
+def rbgram(args, torch):
+    """G = X^T X and X^T Y of n x 64 row-major FP32 blocks through b200_rowblock_gram (tensor cores and
+    FP64), each call timed with CUDA events (the call also allocates and frees its work arrays)."""
+    n, bp = args.n, 64
+    X = torch.randn((n, bp), dtype=torch.float32, device="cuda")
+    Y = torch.randn((n, bp), dtype=torch.float32, device="cuda")
+    G = torch.empty((bp, bp), dtype=torch.float64, device="cuda")
+    out = []
+    for tc in (True, False):
+        for cross in (False, True):
+            yp = Y.data_ptr() if cross else None
+            for _ in range(args.warmup):
+                S.rowblock_gram(n, bp, X.data_ptr(), yp, tc, G.data_ptr())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ms = 0.0
+            for _ in range(args.reps):
+                torch.cuda.synchronize()
+                e0.record()
+                S.rowblock_gram(n, bp, X.data_ptr(), yp, tc, G.data_ptr())
+                e1.record()
+                torch.cuda.synchronize()
+                ms += e0.elapsed_time(e1)
+            ms /= args.reps
+            algo = n * bp * 4 * (2 if cross else 1)
+            out.append({"kernel": ("rb_gram_tf32_kernel (tcgen05)" if tc else "rb_gram2_kernel (FP64)") +
+                        (" X^T Y" if cross else " X^T X"), "n": n, "bp": bp, "ms_per_call": ms,
+                        "algorithmic_bytes": algo, "GBps_call": algo / (ms * 1e-3) / 1e9})
+    return out
 
 
 def lobpcg(args, torch):
@@ -320,13 +358,12 @@ def multinplace(args, torch):
 
 def main():
     p = argparse.ArgumentParser()
-    p.add_argument("kernel", choices=["gs", "spmv", "spmm", "mixed", "multinplace", "cross", "batched", "lobpcg",
+    p.add_argument("kernel", choices=["gs", "spmv", "spmm", "mixed", "rbgram", "multinplace", "cross", "batched", "lobpcg",
                                       "lobpcg_ops", "all"])
     p.add_argument("--lgrid", type=int, default=512, help="lobpcg: side of the 2-D diffusion grid")
     p.add_argument("--block", nargs="+", default=["gs", "chol", "svqb"], help="lobpcg: block orthogonalizations")
     p.add_argument("--phases", action="store_true", help="lobpcg: also a run with per-phase times")
-    p.add_argument("--restarts", type=int, default=3, help="mixed: restarts of the FP32-basis phase")
-    p.add_argument("--sweeps", type=int, default=1, help="mixed: refinement sweeps")
+    p.add_argument("--fp64-gram", action="store_true", help="mixed: FP64 orthonormalisation Gram (no tensor cores)")
     p.add_argument("--nb", type=int, default=48, help="columns of the BVMatMult block")
     p.add_argument("--nprob", type=int, default=64)
     p.add_argument("--threads", type=int, default=512)
@@ -354,8 +391,8 @@ def main():
         elif k in ("lobpcg", "lobpcg_ops"):
             for line in (lobpcg if k == "lobpcg" else lobpcg_ops)(args, torch):
                 print(json.dumps(line), flush=True)
-        elif k == "cross":
-            for line in cross(args, torch):
+        elif k in ("cross", "rbgram"):
+            for line in (cross if k == "cross" else rbgram)(args, torch):
                 print(json.dumps(line), flush=True)
         else:
             print(json.dumps({"spmv": spmv, "spmm": spmm, "mixed": mixed, "multinplace": multinplace}[k](args, torch)),

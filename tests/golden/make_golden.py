@@ -10,6 +10,7 @@ The JSON files are committed; the tests never read the SLEPc tree.
 
 Sources:
   src/eps/tutorials/output/ex2_1.out, ex2_1_alt.out   (ex2.c -n 72 -eps_nev 4 -eps_ncv 20)
+  src/eps/tests/output/test2_1.out                     (test2.c, 1-D Laplacian n=30, locking 0 and 1)
   src/sys/classes/bv/tests/output/test2_1.out         (test2.c, n=20 k=8, CGS)
   src/sys/classes/ds/tests/output/test2_1.out         (test2.c, DSHEP n=12, ld=n+2)
   src/sys/classes/bv/tests/output/test1_1_bv_type-svec.out (test1.c, n=10 k=5 l=3, -verbose)
@@ -39,6 +40,21 @@ def ex2(root):
                      "values": [float(v) for v in vals_line.replace(",", " ").split()]}
     return {"source": "src/eps/tutorials/output/ex2_1.out (+ _alt)", "args": {"n": 72, "nev": 4, "ncv": 20,
             "which": "largest_magnitude"}, "digits": 5, "outputs": out}
+
+
+def eps_test2(root):
+    """EPS test2: 1-D Laplacian n=30, nev=4, tol=max(1000 eps, 1e-9) = 1e-9, largest and smallest real;
+    the same expected output for -eps_type krylovschur -eps_krylovschur_locking {0 1} (test2.c:109-112)."""
+    txt = read(root, "src/eps/tests/output/test2_1.out")
+
+    def values(section):
+        block = txt.split(section)[1].split("\n", 1)[1].split("- - -")[0]
+        line = [ln for ln in block.strip().splitlines() if "," in ln][0]
+        return [float(v) for v in line.replace(",", " ").split()]
+
+    return {"source": "src/eps/tests/output/test2_1.out", "args": {"n": 30, "nev": 4, "tol": 1e-9,
+            "locking": [0, 1]}, "digits": 5,
+            "largest_real": values("Largest eigenvalues"), "smallest_real": values("Smallest eigenvalues")}
 
 
 def bv_test2(root):
@@ -146,7 +162,7 @@ def petsc_binary(root):
 
 
 def main(root):
-    fixtures = {"ex2_1.json": ex2(root), "bv_test2.json": bv_test2(root), "ds_test2.json": ds_test2(root),
+    fixtures = {"ex2_1.json": ex2(root), "eps_test2.json": eps_test2(root), "bv_test2.json": bv_test2(root), "ds_test2.json": ds_test2(root),
                 "bv_test1.json": bv_test1(root), "petsc_binary.json": petsc_binary(root),
                 "bv_test11.json": bv_test11(root)}
     for name, obj in fixtures.items():

@@ -29,12 +29,13 @@ from tests import helpers as H
 pytestmark = pytest.mark.gpu
 
 
-def gpu_solve(csr, v0, nev, ncv, which, tol=1e-8, max_restarts=0):
+def gpu_solve(csr, v0, nev, ncv, which, tol=1e-8, max_restarts=0, lock=True):
     A = S.Mat().createAIJ(csr)
     E = S.EPS().create()
     E.setOperators(A)
     E.setProblemType(S.EPS.ProblemType.HEP)
     E.setDimensions(nev, ncv)
+    E.setKrylovSchurLocking(lock)
     E.setTolerances(tol)
     E.setWhichEigenpairs(which)
     E.setInitialSpace(v0)
@@ -332,3 +333,64 @@ def test_config2_full_size_vs_oracle():
     _report("config2_128_vs_oracle", gpu_its=g["its"], oracle_its=fx["its"], oracle_wall_s=fx["wall_s"],
             oracle_threads=fx["threads"], distinct_window=len(gd), clusters=clusters,
             max_eig_rel_diff=float(np.max(np.abs(gd - od) / od)))
+
+
+@pytest.mark.parametrize("lock", [True, False])
+def test_eps_test2_golden_both_locking_variants(oracle_mod, lock):
+    """src/eps/tests/test2.c -eps_type krylovschur -eps_krylovschur_locking {0 1} (output/test2_1.out):
+    1-D Laplacian n=30, nev=4, tol=1e-9, largest and smallest real -- the reference's digits in both
+    variants, and the oracle's eigenvalues (1e-10) and iteration count (+-2) with the same variant."""
+    from tests.test_oracle_golden import laplacian_1d
+
+    g = H.golden("eps_test2.json")
+    csr = laplacian_1d(g["args"]["n"])
+    A = P.to_scipy(csr)
+    v0 = P.start_vector(A.shape[0], 5)
+    oracle_mod.set_locking(lock)
+    try:
+        for which, owhich, key in ((S.LARGEST_REAL, oracle_mod.LARGEST_REAL, "largest_real"),
+                                   (S.SMALLEST_REAL, oracle_mod.SMALLEST_REAL, "smallest_real")):
+            gg = gpu_solve(csr, v0, 4, 19, which, tol=g["args"]["tol"], lock=lock)
+            o = oracle_mod.eps_solve(A, v0, nev=4, ncv=19, tol=g["args"]["tol"], which=owhich)
+            assert gg["reason"] == S.CONVERGED_TOL and gg["nconv"] >= 4
+            assert [float("%.5f" % v) for v in gg["evals"][:4]] == g[key]
+            np.testing.assert_allclose(gg["evals"][:4], o.evals[:4], rtol=1e-10)
+            assert abs(gg["its"] - o.its) <= 2
+            assert gg["err"][:4].max() <= 1e-9
+    finally:
+        oracle_mod.set_locking(True)
+
+
+def test_nonlocking_2d_laplacian_vs_oracle(oracle_mod):
+    """The non-locking variant on the 2-D Laplacian 60x60 (nev 8, ncv 20, several restarts) against the
+    oracle's non-locking run on the same start vector."""
+    csr = P.laplacian_2d(60)
+    A = P.to_scipy(csr)
+    v0 = P.start_vector(A.shape[0], 1)
+    g = gpu_solve(csr, v0, 8, 20, S.LARGEST_REAL, tol=1e-9, lock=False)
+    oracle_mod.set_locking(False)
+    try:
+        o = oracle_mod.eps_solve(A, v0, nev=8, ncv=20, tol=1e-9, which=oracle_mod.LARGEST_REAL)
+    finally:
+        oracle_mod.set_locking(True)
+    assert g["reason"] == S.CONVERGED_TOL and o.its > 3
+    assert abs(g["its"] - o.its) <= 2
+    np.testing.assert_allclose(g["evals"][:8], o.evals[:8], rtol=1e-10)
+    assert H.eig_set_match(g["evals"], P.laplacian_2d_eigs(60), 0) < 1e-10
+    assert g["err"][:8].max() <= 1e-9
+
+
+def test_nonlocking_rejects_restricted_mpd():
+    """krylovschur.c:116: the non-locking variant does not take an mpd below ncv."""
+    csr = P.laplacian_2d(30)
+    A = S.Mat().createAIJ(csr)
+    E = S.EPS().create()
+    E.setOperators(A)
+    E.setDimensions(6, 30, 12)
+    E.setKrylovSchurLocking(False)
+    assert not E.getKrylovSchurLocking()
+    with pytest.raises(S.B200Error) as ei:
+        E.solve()
+    assert ei.value.status == 11
+    E.destroy()
+    A.destroy()

@@ -25,6 +25,39 @@ def test_ex2_golden_digits(oracle_mod):
             assert oracle_mod.residual(A, r.X[:, i], r.evals[i]) <= 1e-8
 
 
+def laplacian_1d(n):
+    """The 1-D Laplacian of src/eps/tests/test2.c (2 on the diagonal, -1 beside it)."""
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        for j, v in ((i - 1, -1.0), (i, 2.0), (i + 1, -1.0)):
+            if 0 <= j < n:
+                rows.append(i)
+                cols.append(j)
+                vals.append(v)
+    rowptr = np.searchsorted(rows, np.arange(n + 1)).astype(np.int32)
+    return rowptr, np.array(cols, dtype=np.int32), np.array(vals)
+
+
+@pytest.mark.parametrize("lock", [True, False])
+def test_eps_test2_golden_both_locking_variants(oracle_mod, lock):
+    """src/eps/tests/test2.c -eps_type krylovschur -eps_krylovschur_locking {0 1} -> output/test2_1.out:
+    the largest and smallest four eigenvalues of the 1-D Laplacian n=30 at tol 1e-9, in both variants
+    (the non-locking one keeps converged pairs in the active subspace, krylovschur.c:295)."""
+    g = H.golden("eps_test2.json")
+    A = P.to_scipy(laplacian_1d(g["args"]["n"]))
+    oracle_mod.set_locking(lock)
+    try:
+        for which, key in ((oracle_mod.LARGEST_REAL, "largest_real"), (oracle_mod.SMALLEST_REAL, "smallest_real")):
+            r = oracle_mod.eps_solve(A, P.start_vector(A.shape[0], 5), nev=4, ncv=19, tol=g["args"]["tol"],
+                                     which=which)
+            assert r.reason == oracle_mod.CONVERGED_TOL and r.nconv >= 4
+            assert [float("%.5f" % v) for v in r.evals[:4]] == g[key]
+            for i in range(4):
+                assert oracle_mod.residual(A, r.X[:, i], r.evals[i]) <= 1e-9
+    finally:
+        oracle_mod.set_locking(True)
+
+
 def test_bv_test2_golden(oracle_mod):
     """src/sys/classes/bv/tests/test2.c: CGS orthogonality and the ones-vector norm 2.50931."""
     g = H.golden("bv_test2.json")

@@ -352,7 +352,8 @@ b200_status b200_rowblock_gram(int n, int bp, const float *X_dev, const float *Y
 /* Mixed-form parameters (0 or a negative value keeps the default): tol_low,
  * the tolerance of the FP32 phase (default 5e-7, never below tol; the phase
  * also ends when a sweep no longer halves the largest wanted residual);
- * degree, the largest Chebyshev degree of one sweep (default 160); guard,
+ * degree, the largest Chebyshev degree of one sweep (default 400; a sweep
+ * runs in segments, each followed by an orthonormalisation); guard,
  * block columns beyond nev (default max(8, nev/2); the block is 64 columns
  * when nev + guard <= 64, else 128, at most 128); max_sweeps, per phase
  * (default 60); fp64_gram: 1 forms the FP32 phase's orthonormalisation Gram

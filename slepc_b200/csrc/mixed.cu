@@ -13,7 +13,8 @@
 //  weakest Ritz value of the block) and amplifies the wanted end, then re-orthonormalises the block
 //  and performs a Rayleigh-Ritz step.  The degree of each sweep is chosen from the current
 //  residuals and Ritz values (the Chebyshev growth at the Ritz value that is furthest from its
-//  target), capped so that the block's condition number stays bounded.
+//  target); the sweep runs in segments, each re-orthonormalised, so that the block's condition
+//  number stays bounded (by 20 in FP32, where the orthonormalisation Gram matrix is TF32).
 //
 //  Phase 1 (FP32): the block and the matrix values are FP32; the filter's block SpMV accumulates
 //  in FP32 (rowblock.cu rb_spmm_kernel).  The orthonormalisation projection X^T X runs on the
@@ -23,9 +24,13 @@
 //  the residual norms are FP64 sums.  The phase stops at tol_low (default 5e-7) or when a sweep no
 //  longer halves the largest wanted residual (the FP32 rounding floor).
 //
-//  Phase 2 (FP64): the block is widened to FP64 and the same sweeps run in FP64 (FP64 block SpMV
-//  with the FP64 matrix, FP64 Gram products, SVQB, Rayleigh-Ritz) until every wanted residual is
-//  below tol.  A block method also finds every copy of a repeated eigenvalue in the block's reach,
+//  One more FP32 sweep follows, sized by the Chebyshev growth for the final tolerance (progress
+//  below the FP32 floor cannot be measured in FP32, only predicted).
+//
+//  Phase 2 (FP64): the block is widened to FP64; a short polish filter over a wide interval removes
+//  the FP32 rounding noise spread over the unwanted spectrum, and further FP64 sweeps (FP64 block
+//  SpMV with the FP64 matrix, FP64 Gram products, SVQB, Rayleigh-Ritz) run until every wanted
+//  residual is below tol.  A block method also finds every copy of a repeated eigenvalue in the block's reach,
 //  which a single-vector Krylov run finds only through rounding.
 #include <algorithm>
 #include <cmath>
@@ -51,11 +56,13 @@ using namespace b200;
 namespace {
 
 constexpr double kDefaultTolLow = 5e-7;
-constexpr int kDefaultDegreeCap = 160;   // largest degree of one sweep
+constexpr int kDefaultDegreeCap = 400;   // largest degree of one sweep
 constexpr int kMinDegree = 6;
 constexpr int kDefaultMaxSweeps = 60;    // per phase
-constexpr double kAmpCap32 = 300.0;     // growth of the best Ritz value per FP32 sweep (block condition)
-constexpr double kAmpCap64 = 1e4;       // the same in FP64
+constexpr double kSegCap32 = 20.0;      // growth of the best Ritz value per filter segment, FP32 (block condition)
+constexpr double kSegCap64 = 1e4;       // the same in FP64
+constexpr double kWide = 0.1;           // polish interval: pulled back by this fraction
+constexpr double kPolishGrowth = 300.0; // damping of the FP32 rounding noise by the polish filter
 constexpr int kBufs = 4;                // row-major blocks per precision
 
 template <typename T>
@@ -99,7 +106,8 @@ struct Block {
   int x = 0;  // index of the current block among the buffers of the phase
   bool x32 = true;
   int64_t spmm_cols = 0;
-  int max_degree = 0;
+  int max_degree = 0;  // largest degree of one sweep
+  int segments = 0;
   // timing mode: device time and algorithmic bytes of the filters' block SpMVs
   cudaEvent_t f0 = nullptr, f1 = nullptr;
   double filter_ms = 0.0, filter_bytes = 0.0;
@@ -225,23 +233,37 @@ struct Block {
   }
 
   // Interval [a, b] the filter damps, from the Ritz values (wanted end first) and the Gershgorin bounds.
-  void interval(double *a, double *b) const {
+  // wide > 0 pulls the edge next to the wanted end back by that fraction of the interval: the polish
+  // filter damps everything up to there much faster at the price of leaving the band next to the
+  // block's weakest Ritz value undamped.
+  void interval(double *a, double *b, double wide = 0.0) const {
     const double worst = theta[bp - 1];
     if (which == B200_LARGEST_REAL) {
       *a = bounds[0];
-      *b = worst;
+      *b = worst - wide * (worst - bounds[0]);
     } else if (which == B200_SMALLEST_REAL) {
-      *a = worst;
+      *a = worst + wide * (bounds[1] - worst);
       *b = bounds[1];
     } else {
-      *a = -std::fabs(worst);
-      *b = std::fabs(worst);
+      *a = -std::fabs(worst) * (1.0 - wide);
+      *b = std::fabs(worst) * (1.0 - wide);
     }
   }
 
+  // Degree of the polish filter: growth `growth` at the weakest wanted Ritz value over the wide interval.
+  int polish_degree(double wide, double growth, int cap) const {
+    double a, b;
+    interval(&a, &b, wide);
+    const double e = 0.5 * (b - a), c = 0.5 * (b + a);
+    const double t = std::fabs((theta[nev - 1] - c) / e);
+    if (!(e > 0.0) || !(t > 1.0) || !std::isfinite(t)) return kMinDegree;
+    const int d = (int)std::ceil(std::acosh(growth) / std::acosh(t));
+    return std::max(4, std::min(d, cap));
+  }
+
   // Degree of the next sweep: enough Chebyshev growth at the slowest unconverged wanted Ritz value
-  // to bring its residual to target, capped so the best Ritz value grows by at most amp_cap.
-  int choose_degree(double target, double amp_cap, int cap) const {
+  // to bring its residual to target (the sweep runs in segments, filter_segments), at most cap.
+  int choose_degree(double target, int cap) const {
     double a, b;
     interval(&a, &b);
     const double e = 0.5 * (b - a), c = 0.5 * (b + a);
@@ -252,19 +274,16 @@ struct Block {
       const double t = std::fabs((theta[i] - c) / e);
       if (!(t > 1.0)) continue;
       const double d = std::acosh(std::max(rel[i] / target, 1.0)) / std::acosh(t);
-      need = std::max(need, 1.15 * d + 2.0);
+      need = std::max(need, 1.1 * d + 2.0);
     }
-    const double tb = std::fabs((theta[0] - c) / e);
-    double lim = cap;
-    if (tb > 1.0 && std::isfinite(tb)) lim = std::min(lim, std::acosh(amp_cap) / std::acosh(tb));
-    int d = (int)std::ceil(std::min(need, lim));
-    return std::max(kMinDegree, std::min(d, cap));
+    const int d = (int)std::ceil(std::min(need, (double)cap));
+    return std::max(kMinDegree, d);
   }
 
   // One filter application of degree d to the current block (the scaled three-term recurrence).
-  b200_status filter(int d) {
+  b200_status filter(int d, double wide = 0.0) {
     double a, b;
-    interval(&a, &b);
+    interval(&a, &b, wide);
     const double e = 0.5 * (b - a), c = 0.5 * (b + a);
     const double best = theta[0];
     if (!(e > 0.0) || best == c || !std::isfinite(e) || d < 1) return B200_OK;
@@ -285,7 +304,6 @@ struct Block {
       sigma = sn;
     }
     x = cur;
-    max_degree = std::max(max_degree, d);
     if (timed) {
       float ms = 0.f;
       cudaEventRecord(f1, s);
@@ -293,6 +311,27 @@ struct Block {
         filter_ms += ms;
     } else {
       filter_bytes = bytes0;  // bytes are reported only with their time
+    }
+    return B200_OK;
+  }
+
+  // A sweep of total degree D in segments whose growth of the best Ritz value stays below seg_cap,
+  // each segment but the last followed by SVQB: the block's condition number stays near seg_cap, which
+  // the tensor-core (TF32) Gram matrix of the FP32 phase resolves, and the FP64 Rayleigh-Ritz step
+  // runs once per sweep.
+  b200_status filter_segments(int D, double seg_cap, double wide = 0.0) {
+    double a, b;
+    interval(&a, &b, wide);
+    const double e = 0.5 * (b - a), c = 0.5 * (b + a);
+    const double tb = std::fabs((theta[0] - c) / e);
+    int seg = D;
+    if (e > 0.0 && tb > 1.0 && std::isfinite(tb)) seg = std::max(4, (int)std::floor(std::acosh(seg_cap) / std::acosh(tb)));
+    for (int done = 0; done < D;) {
+      const int d = std::min(seg, D - done);
+      B200_CHECK(filter(d, wide));
+      done += d;
+      ++segments;
+      if (done < D) B200_CHECK(svqb());
     }
     return B200_OK;
   }
@@ -399,8 +438,9 @@ b200_status b200::mixed_solve(b200_eps eps) {
   B200_CHECK(B.rayleigh_ritz());
   double last = B.max_wanted();
   while (sweeps1 < max_sweeps && B.max_wanted() > tol_low) {
-    const int d = B.choose_degree(tol_low, kAmpCap32, deg_cap);
-    B200_CHECK(B.filter(d));
+    const int d = B.choose_degree(tol_low, deg_cap);
+    B.max_degree = std::max(B.max_degree, d);
+    B200_CHECK(B.filter_segments(d, kSegCap32));
     B200_CHECK(B.svqb());
     B200_CHECK(B.rayleigh_ritz());
     ++sweeps1;
@@ -408,17 +448,37 @@ b200_status b200::mixed_solve(b200_eps eps) {
     if (now > 0.5 * last) break;  // no longer halving: the FP32 rounding floor
     last = now;
   }
+  // The FP32 residual floor (about 1e-7: the block and A X are rounded to FP32) hides further
+  // progress on the wanted pairs.  One more FP32 sweep, its degree taken from the Chebyshev growth
+  // that brings the measured residuals to the FP64 target, converges the error components next to
+  // the wanted end at half the bytes of an FP64 sweep; FP64 then only has to remove the broadband
+  // rounding noise.
+  if (tol < tol_low && sweeps1 < max_sweeps) {
+    const int d = B.choose_degree(0.5 * tol, deg_cap);
+    B.max_degree = std::max(B.max_degree, d);
+    B200_CHECK(B.filter_segments(d, kSegCap32));
+    B200_CHECK(B.svqb());
+    B200_CHECK(B.rayleigh_ritz());
+    ++sweeps1;
+  }
   cudaEventRecord(t1, s);
 
   // ---------------------------------------------------------------- phase 2 (FP64 block)
+  // The FP32 rounding noise of the block lies in every direction, so a short polish filter over a wide
+  // interval (the unwanted spectrum up to kWide of the way from the block's weakest Ritz value) damps
+  // it by kPolishGrowth in a few FP64 degrees; SVQB and the FP64 Rayleigh-Ritz step follow.
   B.x32 = false;
   B200_CUDA_CHECK(rb_widen_launch(B.b32[B.x], B.b64[0], (long long)blk, s));
   B.x = 0;
-  B200_CHECK(B.rayleigh_ritz());
   int sweeps2 = 0;
+  B200_CHECK(B.filter(B.polish_degree(kWide, kPolishGrowth, deg_cap), kWide));
+  B200_CHECK(B.svqb());
+  B200_CHECK(B.rayleigh_ritz());
+  ++sweeps2;
   while (B.leading_converged(tol) < nev && sweeps2 < max_sweeps) {
-    const int d = B.choose_degree(0.25 * tol, kAmpCap64, deg_cap);
-    B200_CHECK(B.filter(d));
+    const int d = B.choose_degree(0.25 * tol, deg_cap);
+    B.max_degree = std::max(B.max_degree, d);
+    B200_CHECK(B.filter_segments(d, kSegCap64));
     B200_CHECK(B.svqb());
     B200_CHECK(B.rayleigh_ritz());
     ++sweeps2;

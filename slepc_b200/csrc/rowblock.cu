@@ -19,6 +19,7 @@ namespace b200 {
 namespace {
 
 constexpr int kRbThreads = 256;
+constexpr int kChunk = 8;  // nonzeros of a row whose gathers are issued together
 
 // Lane mapping of a block row: 16-byte vector accesses (4 floats or 2 doubles), LPR lanes per row,
 // CPL vectors per lane, RPI rows per warp iteration.
@@ -83,35 +84,49 @@ __global__ void __launch_bounds__(kRbThreads) rb_spmm_kernel(int nslices, int n,
       const int i = it + sub;
       const int r = 32 * sl + i;
       if (r < n && ((m >> i) & 1u)) {
-        TX acc[M::CPL][M::VEC];
+        // the row's own X and Z first, then every gather of a chunk of kChunk nonzeros before any
+        // product: kChunk independent 16-byte loads per lane in flight (padding entries read the row
+        // itself, already cached, with a zero coefficient)
+        TX xr[M::CPL][M::VEC], z[M::CPL][M::VEC], acc[M::CPL][M::VEC];
 #pragma unroll
-        for (int cv = 0; cv < M::CPL; ++cv)
+        for (int cv = 0; cv < M::CPL; ++cv) {
+          const size_t o = (size_t)r * BP + (size_t)(li + cv * M::LPR) * M::VEC;
+          vld(X + o, xr[cv]);
+          if (Z) vld(Z + o, z[cv]);
 #pragma unroll
           for (int e = 0; e < M::VEC; ++e) acc[cv][e] = TX(0);
-#pragma unroll 4
-        for (int k = 0; k < w; ++k) {
-          const int c = wc[k * 32 + i];
-          if (c >= 0) {
-            const TX a = (TX)wv[k * 32 + i];
+        }
+        for (int k0 = 0; k0 < w; k0 += kChunk) {
+          int cc[kChunk];
+          TX aa[kChunk];
 #pragma unroll
-            for (int cv = 0; cv < M::CPL; ++cv) {
-              TX x[M::VEC];
-              vld(X + (size_t)c * BP + (size_t)(li + cv * M::LPR) * M::VEC, x);
-#pragma unroll
-              for (int e = 0; e < M::VEC; ++e) acc[cv][e] = fma(a, x[e], acc[cv][e]);
-            }
+          for (int u = 0; u < kChunk; ++u) {
+            const int k = k0 + u;
+            const int c = k < w ? wc[k * 32 + i] : -1;
+            cc[u] = c >= 0 ? c : r;
+            aa[u] = c >= 0 ? (TX)wv[k * 32 + i] : TX(0);
           }
+          TX xv[kChunk][M::CPL][M::VEC];
+#pragma unroll
+          for (int u = 0; u < kChunk; ++u)
+#pragma unroll
+            for (int cv = 0; cv < M::CPL; ++cv)
+              vld(X + (size_t)cc[u] * BP + (size_t)(li + cv * M::LPR) * M::VEC, xv[u][cv]);
+#pragma unroll
+          for (int u = 0; u < kChunk; ++u)
+#pragma unroll
+            for (int cv = 0; cv < M::CPL; ++cv)
+#pragma unroll
+              for (int e = 0; e < M::VEC; ++e) acc[cv][e] = fma(aa[u], xv[u][cv][e], acc[cv][e]);
         }
 #pragma unroll
         for (int cv = 0; cv < M::CPL; ++cv) {
           const size_t o = (size_t)r * BP + (size_t)(li + cv * M::LPR) * M::VEC;
-          TX xr[M::VEC], z[M::VEC], out[M::VEC];
-          vld(X + o, xr);
-          if (Z) vld(Z + o, z);
+          TX out[M::VEC];
 #pragma unroll
           for (int e = 0; e < M::VEC; ++e) {
-            double v = alpha * ((double)acc[cv][e] - shift * (double)xr[e]);
-            if (Z) v -= beta * (double)z[e];
+            double v = alpha * ((double)acc[cv][e] - shift * (double)xr[cv][e]);
+            if (Z) v -= beta * (double)z[cv][e];
             out[e] = (TX)v;
           }
           vst(Y + o, out);
@@ -324,7 +339,8 @@ __global__ void rb_reduce_kernel(const TP *__restrict__ partials, int nparts, in
 //
 // G = X^T X and H = X^T W, every product and sum in FP64 (FP32 inputs are exact in FP64).  Grid
 // (row ranges) x (64 x 64 quadrants of the bp x bp result); 256 threads, a 4 x 4 register tile of
-// G and of H per thread; 16-row slabs of the three column strips staged in shared memory.
+// G and of H per thread; 16-row slabs of the three column strips staged in shared memory, the next
+// slab fetched into registers while the current one is consumed.
 constexpr int kSlab = 16;
 constexpr int kQ = 64;
 template <typename TX, int BP>
@@ -340,15 +356,30 @@ __global__ void __launch_bounds__(256) rb_gram2_kernel(const TX *__restrict__ X,
 #pragma unroll
     for (int b = 0; b < 4; ++b) g[a][b] = h[a][b] = 0.0;
   const int r0 = blockIdx.x * rows_per_cta, r1 = min(n, r0 + rows_per_cta);
-  for (int slab = r0; slab < r1; slab += kSlab) {
-    for (int e = threadIdx.x; e < kSlab * kQ; e += 256) {
-      const int rr = e / kQ, c = e % kQ, r = slab + rr;
+  // the next slab is fetched into registers while the current one is consumed from shared memory
+  constexpr int kPer = kSlab * kQ / 256;
+  double pa[kPer], pb[kPer], pw[kPer];
+  auto fetch = [&](int slab) {
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int e = threadIdx.x + 256 * u, rr = e / kQ, c = e % kQ, r = slab + rr;
       const bool in = r < r1;
-      xa[rr][c] = in ? (double)X[(size_t)r * BP + qi * kQ + c] : 0.0;
-      xb[rr][c] = in ? (double)X[(size_t)r * BP + qj * kQ + c] : 0.0;
-      wb[rr][c] = in ? (double)W[(size_t)r * BP + qj * kQ + c] : 0.0;
+      pa[u] = in ? (double)X[(size_t)r * BP + qi * kQ + c] : 0.0;
+      pb[u] = in ? (double)X[(size_t)r * BP + qj * kQ + c] : 0.0;
+      pw[u] = in ? (double)W[(size_t)r * BP + qj * kQ + c] : 0.0;
+    }
+  };
+  if (r0 < r1) fetch(r0);
+  for (int slab = r0; slab < r1; slab += kSlab) {
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int e = threadIdx.x + 256 * u, rr = e / kQ, c = e % kQ;
+      xa[rr][c] = pa[u];
+      xb[rr][c] = pb[u];
+      wb[rr][c] = pw[u];
     }
     __syncthreads();
+    if (slab + kSlab < r1) fetch(slab + kSlab);
 #pragma unroll 4
     for (int rr = 0; rr < kSlab; ++rr) {
       double a[4], b[4], w[4];

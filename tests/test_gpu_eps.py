@@ -386,7 +386,7 @@ def test_nonlocking_rejects_restricted_mpd():
     A = S.Mat().createAIJ(csr)
     E = S.EPS().create()
     E.setOperators(A)
-    E.setDimensions(6, 30, 12)
+    E.setDimensions(20, 30, 12)
     E.setKrylovSchurLocking(False)
     assert not E.getKrylovSchurLocking()
     with pytest.raises(S.B200Error) as ei:

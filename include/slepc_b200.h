@@ -349,6 +349,18 @@ b200_status b200_eps_set_precision(b200_eps eps, int precision);
  * cores.  Allocates its work arrays; synchronises the stream. */
 b200_status b200_rowblock_gram(int n, int bp, const float *X_dev, const float *Y_dev, int tensor_cores,
                                double *G_dev, void *stream);
+/* The neural operator's contraction kernel, exposed for tests and benchmarks:
+ * C[z] = alpha A[z] B[z] + beta C[z] for z < batch on device FP32 views
+ * (A m x k, B k x n, C m x n; element (i, j) of matrix z of a view at
+ * p + z*bs + i*rs + j*cs, any strides).  tcgen05 kind::tf32 MMAs, three per
+ * step (high and low TF32 parts), FP32 accumulation in TMEM: FP32-level
+ * accuracy.  split = 1 lets long depths split across CTAs (partial tiles
+ * summed in a fixed order); sum_batch = 1 writes the single sum over z into
+ * C (bsc ignored).  Allocates its work arrays; synchronises the stream. */
+b200_status b200_tc_sgemm(int batch, int m, int n, int k, float alpha, const float *A_dev, long long ars,
+                          long long acs, long long abs_, const float *B_dev, long long brs, long long bcs,
+                          long long bbs, float beta, float *C_dev, long long rsc, long long csc, long long bsc,
+                          int split, int sum_batch, void *stream);
 /* Mixed-form parameters (0 or a negative value keeps the default): tol_low,
  * the tolerance of the FP32 phase (default 5e-7, never below tol; the phase
  * also ends when a sweep no longer halves the largest wanted residual);
@@ -423,6 +435,21 @@ typedef struct {
 b200_status b200_eps_get_stats(b200_eps eps, b200_eps_stats *stats);
 /* Enable per-phase CUDA-event timing (adds events around each phase). */
 b200_status b200_eps_set_timing(b200_eps eps, int on);
+
+/* EPSMonitorSet (src/eps/interface/epsmon.c:96) / EPSMonitorCancel: a monitor
+ * is called on the host once per outer iteration, where EPSSolve_KrylovSchur
+ * calls EPSMonitor (krylovschur.c:339; for the mixed form, once per sweep),
+ * with the iteration number, the number of converged pairs, the current Ritz
+ * values and error estimates and their count (real scalars: no eigi).  Up to
+ * 8 monitors; a nonzero return aborts the solve with B200_ERR_STATE.
+ * b200_eps_monitor_jsonl adds a built-in monitor writing one JSON line per
+ * iteration to path: its, nconv, nest, eigr, errest, the host milliseconds
+ * since the solve started and the Gram-Schmidt algorithmic bytes so far. */
+typedef int (*b200_eps_monitor_fn)(b200_eps eps, int its, int nconv, const double *eigr, const double *errest,
+                                   int nest, void *ctx);
+b200_status b200_eps_monitor_set(b200_eps eps, b200_eps_monitor_fn fn, void *ctx);
+b200_status b200_eps_monitor_cancel(b200_eps eps);
+b200_status b200_eps_monitor_jsonl(b200_eps eps, const char *path);
 
 /* One call from host buffers to host results: create the matrix, solve,
  * copy eigenvalues (nconv), eigenvectors (n x nconv column-major, nullable)

@@ -38,6 +38,7 @@ MAT_OPERATOR = -1
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
 _vp = ctypes.c_void_p
+_ll = ctypes.c_longlong
 _lib = None
 
 
@@ -76,6 +77,9 @@ _SIGS = {
     "b200_mat_norm_inf": (ctypes.c_int, [_vp, _dp]),
     "b200_eps_set_type": (ctypes.c_int, [_vp, ctypes.c_int]),
     "b200_eps_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200_eps_monitor_set": (ctypes.c_int, [_vp, _vp, _vp]),
+    "b200_eps_monitor_cancel": (ctypes.c_int, [_vp]),
+    "b200_eps_monitor_jsonl": (ctypes.c_int, [_vp, ctypes.c_char_p]),
     "b200_eps_krylovschur_set_locking": (ctypes.c_int, [_vp, ctypes.c_int]),
     "b200_eps_krylovschur_get_locking": (ctypes.c_int, [_vp, _ip]),
     "b200_bv_gram_schmidt": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _dp, _dp]),
@@ -84,6 +88,9 @@ _SIGS = {
     "b200_bv_normalize": (ctypes.c_int, [_vp, _dp]),
     "b200_bv_mult_inplace_trans": (ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "b200_rowblock_gram": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp]),
+    "b200_tc_sgemm": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, _vp,
+                                     _ll, _ll, _ll, _vp, _ll, _ll, _ll, ctypes.c_float, _vp, _ll, _ll, _ll,
+                                     ctypes.c_int, ctypes.c_int, _vp]),
     "b200_eps_set_mixed_options": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                   ctypes.c_int]),
     "b200_eps_lobpcg_set_block_size": (ctypes.c_int, [_vp, ctypes.c_int]),
@@ -681,6 +688,31 @@ class EPS:
         Chebyshev-filtered Rayleigh-Ritz refinement of the block of leading Ritz vectors."""
         _check(lib().b200_eps_set_precision(self.handle, precision))
 
+    _MonitorFn = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int,
+                                  ctypes.c_void_p)
+
+    def setMonitor(self, fn):
+        """EPSMonitorSet: fn(its, nconv, eigr, errest) is called once per outer iteration with numpy
+        copies of the nest current values and estimates; a true return value aborts the solve."""
+        def tramp(_eps, its, nconv, eigr, errest, nest, _ctx):
+            try:
+                r = fn(its, nconv, np.ctypeslib.as_array(eigr, (nest,)).copy(),
+                       np.ctypeslib.as_array(errest, (nest,)).copy())
+                return 1 if r else 0
+            except Exception:
+                return 1
+        cb = self._MonitorFn(tramp)
+        self._monitors = getattr(self, "_monitors", []) + [cb]  # keep the callbacks alive
+        _check(lib().b200_eps_monitor_set(self.handle, ctypes.cast(cb, ctypes.c_void_p), None))
+
+    def setMonitorJSONL(self, path):
+        """The built-in monitor: one JSON line per outer iteration written to path."""
+        _check(lib().b200_eps_monitor_jsonl(self.handle, os.fsencode(path)))
+
+    def cancelMonitor(self):
+        _check(lib().b200_eps_monitor_cancel(self.handle))
+        self._monitors = []
+
     def setKrylovSchurLocking(self, lock):
         """EPSKrylovSchurSetLocking (the non-locking variant needs mpd = ncv)."""
         _check(lib().b200_eps_krylovschur_set_locking(self.handle, 1 if lock else 0))
@@ -782,6 +814,14 @@ def rowblock_gram(n, bp, X_ptr, Y_ptr=None, tensor_cores=True, G_ptr=None, strea
     """G = X^T Y (bp x bp, FP64, row-major) of row-major FP32 device blocks (b200_rowblock_gram):
     on the tensor cores (TF32 inputs, FP32 accumulation) or in FP64 on the CUDA cores."""
     _check(lib().b200_rowblock_gram(n, bp, X_ptr, Y_ptr, 1 if tensor_cores else 0, G_ptr, stream))
+
+
+def tc_sgemm(batch, m, n, k, alpha, A, B, beta, C, split=False, sum_batch=False, stream=None):
+    """C[z] = alpha A[z] B[z] + beta C[z] on the tensor cores (b200_tc_sgemm).  A, B and C are
+    (ptr, rs, cs, bs) device views of FP32 matrices: element (i, j) of matrix z at
+    ptr + z*bs + i*rs + j*cs (elements)."""
+    _check(lib().b200_tc_sgemm(batch, m, n, k, alpha, *A, *B, beta, *C, 1 if split else 0, 1 if sum_batch else 0,
+                               stream))
 
 
 def solve_csr_host(csr, v0, nev, ncv, tol=1e-8, which=LARGEST_MAGNITUDE, mpd=0, max_it=0, want_vectors=True,

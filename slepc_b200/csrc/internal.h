@@ -27,6 +27,10 @@ int num_sms_host();
 b200_status lobpcg_solve(b200_eps eps);
 // BVMatMult: Y(:, Y.l+j) = A V(:, V.l+j) over the active columns (block SpMV for square CSR).
 b200_status bv_mat_mult(b200_bv V, b200_mat A, b200_bv Y);
+// EPSMonitor (epsmon.c:39): run the monitors of eps; B200_ERR_STATE when one returns nonzero.
+b200_status eps_monitor(b200_eps eps, int its, int nconv, const double *eigr, const double *errest, int nest);
+// Start the monitor clock of a solve.
+void eps_monitor_start(b200_eps eps);
 // Krylov-Schur with b200_eps_set_precision(MIXED) after the setup (mixed.cu).
 b200_status mixed_solve(b200_eps eps);
 // Read the Gram-Schmidt control block after a stream synchronisation (maps device errors).

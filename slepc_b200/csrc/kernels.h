@@ -234,4 +234,14 @@ cudaError_t inverse_diagonal_launch(int n, const int *rowptr, const int *colind,
 // Counter-based uniform [0,1) column (stands in for PETSc's VecSetRandom).
 cudaError_t random_launch(double *x, int n, uint64_t seed, uint64_t stream_id, cudaStream_t stream);
 
+// ---- Strided batched FP32 GEMM on the tensor cores (tcgemm.cu)
+// C[z] = alpha A[z] B[z] + beta C[z] for z < batch (A m x k, B k x n; element (i, j) of a view at
+// p + z * bs + i * rs + j * cs), three-product TF32 (FP32-level accuracy).  With a workspace of
+// ws_floats floats the depth may be split across CTAs and summed in a fixed order; sum_batch (needs
+// ws) writes the single sum over z into C.  err collects kDevErrTimeout from bounded waits.
+cudaError_t tc_sgemm(cudaStream_t s, int batch, int m, int n, int k, float alpha, const float *A, long long ars,
+                     long long acs, long long abs_, const float *B, long long brs, long long bcs, long long bbs,
+                     float beta, float *C, long long rsc, long long csc, long long bsc, int *err, float *ws,
+                     size_t ws_floats, bool sum_batch);
+
 }  // namespace b200

@@ -19,9 +19,12 @@
 // u_k (unit norm): 1 - (y_k . u_k)^2 / (y_k . y_k), averaged over b and k
 // (invariant to the sign and scale of y_k).  Adam updates the parameters.
 //
-// Every contraction is one call of a strided, batched FP32 GEMM (64 x 64
-// tiles, FP32 accumulation); elementwise kernels add biases and apply gelu and
+// Every contraction is one call of the strided, batched tensor-core GEMM of
+// tcgemm.cu (tcgen05 TF32 MMAs, three products per step for FP32-level
+// accuracy, FP32 accumulation in TMEM; long reductions split across CTAs and
+// summed in a fixed order); elementwise kernels add biases and apply gelu and
 // its derivative; reductions (bias gradients, the loss) use fixed orders.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -46,6 +49,9 @@ struct b200_neural_op_s {
   size_t act_len = 0;
   float *loss_bk = nullptr;  // B x K per-output losses
   std::vector<float> hloss;
+  float *ws = nullptr;       // split-depth partial products of the GEMMs
+  size_t ws_len = 0;
+  int *dev_err = nullptr;    // device error bits of the GEMMs (bounded waits)
 };
 
 namespace b200 {
@@ -55,58 +61,6 @@ struct MView {
   const float *p;
   long long rs, cs, bs;  // element (i, j) of matrix z at p + z*bs + i*rs + j*cs
 };
-
-constexpr int kTM = 64, kTN = 64, kTK = 16;
-
-// C[z] = alpha * A[z] B[z] + beta * C[z]   (A: m x k, B: k x n, C: m x n)
-__global__ void __launch_bounds__(256) sgemm_kernel(int m, int n, int k, float alpha, MView A, MView B, float beta,
-                                                    float *C, long long rsc, long long csc, long long bsc) {
-  __shared__ float As[kTK][kTM + 1], Bs[kTK][kTN + 1];
-  const long long z = blockIdx.z;
-  const float *Ab = A.p + z * A.bs, *Bb = B.p + z * B.bs;
-  float *Cb = C + z * bsc;
-  const int i0 = blockIdx.y * kTM, j0 = blockIdx.x * kTN;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  float acc[4][4];
-#pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) acc[r][c] = 0.f;
-  for (int k0 = 0; k0 < k; k0 += kTK) {
-    for (int t = threadIdx.x; t < kTK * kTM; t += 256) {
-      const int kk = t / kTM, ii = t % kTM, gi = i0 + ii, gk = k0 + kk;
-      As[kk][ii] = (gi < m && gk < k) ? Ab[gi * A.rs + gk * A.cs] : 0.f;
-    }
-    for (int t = threadIdx.x; t < kTK * kTN; t += 256) {
-      const int kk = t / kTN, jj = t % kTN, gj = j0 + jj, gk = k0 + kk;
-      Bs[kk][jj] = (gj < n && gk < k) ? Bb[gk * B.rs + gj * B.cs] : 0.f;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < kTK; ++kk) {
-      float a[4], b[4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) a[r] = As[kk][ty + 16 * r];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) b[c] = Bs[kk][tx + 16 * c];
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) acc[r][c] = fmaf(a[r], b[c], acc[r][c]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const int i = i0 + ty + 16 * r, j = j0 + tx + 16 * c;
-      if (i < m && j < n) {
-        float *cp = Cb + i * rsc + j * csc;
-        *cp = beta != 0.f ? alpha * acc[r][c] + beta * *cp : alpha * acc[r][c];
-      }
-    }
-}
 
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
 __device__ __forceinline__ float gelu_grad(float x) {
@@ -194,13 +148,12 @@ unsigned grid_len(long long len) {
   return (unsigned)(g < 148 * 16 ? (g > 0 ? g : 1) : 148 * 16);
 }
 
-cudaError_t gemm(cudaStream_t s, int batch, int m, int n, int k, float alpha, MView A, MView B, float beta, float *C,
-                 long long rsc, long long csc, long long bsc) {
-  if (m <= 0 || n <= 0 || batch <= 0) return cudaSuccess;
-  const dim3 grid((n + kTN - 1) / kTN, (m + kTM - 1) / kTM, batch);
-  sgemm_kernel<<<grid, 256, 0, s>>>(m, n, k, alpha, A, B, beta, C, rsc, csc, bsc);
-  count_launch();
-  return cudaGetLastError();
+// Every contraction of the network: the tensor-core GEMM of tcgemm.cu with the operator's split-depth
+// workspace and device error word.
+cudaError_t gemm(b200_neural_op op, int batch, int m, int n, int k, float alpha, MView A, MView B, float beta,
+                 float *C, long long rsc, long long csc, long long bsc, bool sum_batch = false) {
+  return tc_sgemm(op->stream, batch, m, n, k, alpha, A.p, A.rs, A.cs, A.bs, B.p, B.rs, B.cs, B.bs, beta, C, rsc, csc,
+                  bsc, op->dev_err, op->ws, op->ws_len, sum_batch);
 }
 
 }  // namespace
@@ -264,6 +217,32 @@ b200_status reserve(b200_neural_op op, int B) {
     return B200_ERR_NOMEM;
   }
   op->act_len = len;
+  // split-depth workspace: the widest summed weight gradient over the batch, four depth splits
+  const size_t W = op->W, mn = std::max({W * 3, W * W, (size_t)op->H * W, (size_t)op->K * op->H});
+  const size_t ws_len = std::max<size_t>(mn * (size_t)B * 4, (size_t)1 << 22);
+  if (ws_len > op->ws_len) {
+    cudaFree(op->ws);
+    op->ws = nullptr;
+    op->ws_len = 0;
+    if (cudaMalloc(&op->ws, sizeof(float) * ws_len) != cudaSuccess) {
+      b200_set_last_error(__FILE__, __LINE__, "cudaMalloc failed for the neural-operator GEMM workspace");
+      return B200_ERR_NOMEM;
+    }
+    op->ws_len = ws_len;
+  }
+  return B200_OK;
+}
+
+// Reads and clears the GEMMs' device error bits (the stream is synchronised by the caller); bits
+// that a training step's backward pass sets are reported by the next call that reads them.
+b200_status gemm_status(b200_neural_op op) {
+  int e = 0;
+  B200_CUDA_CHECK(cudaMemcpy(&e, op->dev_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    B200_CUDA_CHECK(cudaMemset(op->dev_err, 0, sizeof(int)));
+    b200_set_last_error(__FILE__, __LINE__, "a tensor-core GEMM gave up a bounded wait");
+    return B200_ERR_CUDA;
+  }
   return B200_OK;
 }
 
@@ -273,24 +252,20 @@ float *grd(b200_neural_op op, size_t off) { return op->grads + off; }
 // Channel mix Out[b] (Co x P) = Wt (Co x Ci) In[b] (Ci x P) (+ beta Out)
 cudaError_t mix(b200_neural_op op, int B, int Co, int Ci, const float *Wt, const float *In, float *Out, float beta) {
   const long long P = op->P;
-  return gemm(op->stream, B, Co, (int)P, Ci, 1.f, MView{Wt, Ci, 1, 0}, MView{In, P, 1, (long long)Ci * P}, beta, Out,
+  return gemm(op, B, Co, (int)P, Ci, 1.f, MView{Wt, Ci, 1, 0}, MView{In, P, 1, (long long)Ci * P}, beta, Out,
               P, 1, (long long)Co * P);
 }
 // Transposed mix Out[b] (Ci x P) = Wt^T (Ci x Co) In[b] (Co x P)
 cudaError_t mix_t(b200_neural_op op, int B, int Co, int Ci, const float *Wt, const float *In, float *Out, float beta) {
   const long long P = op->P;
-  return gemm(op->stream, B, Ci, (int)P, Co, 1.f, MView{Wt, 1, Ci, 0}, MView{In, P, 1, (long long)Co * P}, beta, Out,
+  return gemm(op, B, Ci, (int)P, Co, 1.f, MView{Wt, 1, Ci, 0}, MView{In, P, 1, (long long)Co * P}, beta, Out,
               P, 1, (long long)Ci * P);
 }
-// Weight gradient dWt (Co x Ci) = sum_b D[b] (Co x P) X[b]^T (P x Ci), accumulated over b in order
+// Weight gradient dWt (Co x Ci) = sum_b D[b] (Co x P) X[b]^T (P x Ci): one product summed over b
 cudaError_t mix_grad(b200_neural_op op, int B, int Co, int Ci, const float *D, const float *X, float *dWt) {
   const long long P = op->P;
-  for (int b = 0; b < B; ++b) {
-    cudaError_t e = gemm(op->stream, 1, Co, Ci, (int)P, 1.f, MView{D + (long long)b * Co * P, P, 1, 0},
-                         MView{X + (long long)b * Ci * P, 1, P, 0}, b ? 1.f : 0.f, dWt, Ci, 1, 0);
-    if (e != cudaSuccess) return e;
-  }
-  return cudaSuccess;
+  return gemm(op, B, Co, Ci, (int)P, 1.f, MView{D, P, 1, (long long)Co * P}, MView{X, 1, P, (long long)Ci * P}, 0.f,
+              dWt, Ci, 1, 0, true);
 }
 cudaError_t bias_act(b200_neural_op op, int B, int C, float *U, const float *bias, float *V, int act) {
   const long long total = (long long)B * C * op->P;
@@ -312,17 +287,17 @@ cudaError_t gelu_bwd(b200_neural_op op, long long total, const float *dV, const 
 cudaError_t to_modes(b200_neural_op op, int nz, const float *X, float *T1, float *C) {
   const int N = op->N, M = op->M;
   const long long P = op->P, NM = (long long)N * M, M2 = (long long)M * M;
-  cudaError_t e = gemm(op->stream, nz, M, N, N, 1.f, MView{op->S, 1, M, 0}, MView{X, N, 1, P}, 0.f, T1, N, 1, NM);
+  cudaError_t e = gemm(op, nz, M, N, N, 1.f, MView{op->S, 1, M, 0}, MView{X, N, 1, P}, 0.f, T1, N, 1, NM);
   if (e != cudaSuccess) return e;
-  return gemm(op->stream, nz, M, M, N, 1.f, MView{T1, N, 1, NM}, MView{op->S, M, 1, 0}, 0.f, C, M, 1, M2);
+  return gemm(op, nz, M, M, N, 1.f, MView{T1, N, 1, NM}, MView{op->S, M, 1, 0}, 0.f, C, M, 1, M2);
 }
 // Fields X[z] (N x N) = S C[z] S^T (+ beta X)
 cudaError_t from_modes(b200_neural_op op, int nz, const float *C, float *T2, float *X, float beta) {
   const int N = op->N, M = op->M;
   const long long P = op->P, NM = (long long)N * M, M2 = (long long)M * M;
-  cudaError_t e = gemm(op->stream, nz, N, M, M, 1.f, MView{op->S, M, 1, 0}, MView{C, M, 1, M2}, 0.f, T2, M, 1, NM);
+  cudaError_t e = gemm(op, nz, N, M, M, 1.f, MView{op->S, M, 1, 0}, MView{C, M, 1, M2}, 0.f, T2, M, 1, NM);
   if (e != cudaSuccess) return e;
-  return gemm(op->stream, nz, N, N, M, 1.f, MView{T2, M, 1, NM}, MView{op->S, 1, M, 0}, beta, X, N, 1, P);
+  return gemm(op, nz, N, N, M, 1.f, MView{T2, M, 1, NM}, MView{op->S, 1, M, 0}, beta, X, N, 1, P);
 }
 
 b200_status forward(b200_neural_op op, int B, const float *feat, Acts &a) {
@@ -337,7 +312,7 @@ b200_status forward(b200_neural_op op, int B, const float *feat, Acts &a) {
     B200_CUDA_CHECK(to_modes(op, B * W, Vl, a.T1, Cl));
     // per mode q: Dh_q (B x W_o) = C_q (B x W_c) R_q^T (W_c x W_o)
     const float *R = prm(op, op->oR[l]);
-    B200_CUDA_CHECK(gemm(op->stream, (int)M2, B, W, W, 1.f, MView{Cl, W * M2, M2, 1}, MView{R, M2, W * M2, 1}, 0.f,
+    B200_CUDA_CHECK(gemm(op, (int)M2, B, W, W, 1.f, MView{Cl, W * M2, M2, 1}, MView{R, M2, W * M2, 1}, 0.f,
                          a.Dh, W * M2, M2, 1));
     B200_CUDA_CHECK(from_modes(op, B * W, a.Dh, a.T2, Ul, 0.f));
     B200_CUDA_CHECK(mix(op, B, W, W, prm(op, op->oW[l]), Vl, Ul, 1.f));
@@ -377,9 +352,9 @@ b200_status backward(b200_neural_op op, int B, Acts &a) {
     // spectral path: dDh = S^T dU S; dR_q = dDh_q^T C_q; dC_q = dDh_q R_q; dV += S dC S^T
     B200_CUDA_CHECK(to_modes(op, B * W, dU, a.T1, a.dDh));
     const float *R = prm(op, op->oR[l]);
-    B200_CUDA_CHECK(gemm(op->stream, (int)M2, W, W, B, 1.f, MView{a.dDh, M2, W * M2, 1}, MView{Cl, W * M2, M2, 1}, 0.f,
+    B200_CUDA_CHECK(gemm(op, (int)M2, W, W, B, 1.f, MView{a.dDh, M2, W * M2, 1}, MView{Cl, W * M2, M2, 1}, 0.f,
                          grd(op, op->oR[l]), W * M2, M2, 1));
-    B200_CUDA_CHECK(gemm(op->stream, (int)M2, B, W, W, 1.f, MView{a.dDh, W * M2, M2, 1}, MView{R, W * M2, M2, 1}, 0.f,
+    B200_CUDA_CHECK(gemm(op, (int)M2, B, W, W, 1.f, MView{a.dDh, W * M2, M2, 1}, MView{R, W * M2, M2, 1}, 0.f,
                          a.dCh, W * M2, M2, 1));
     B200_CUDA_CHECK(from_modes(op, B * W, a.dCh, a.T2, dVn, 1.f));
     float *t = dV;
@@ -402,6 +377,7 @@ b200_status loss(b200_neural_op op, int B, const float *targets, Acts &a, bool w
   B200_CUDA_CHECK(cudaMemcpyAsync(op->hloss.data(), op->loss_bk, sizeof(float) * op->hloss.size(),
                                   cudaMemcpyDeviceToHost, op->stream));
   B200_CUDA_CHECK(cudaStreamSynchronize(op->stream));
+  B200_CHECK(gemm_status(op));
   double s = 0.0;
   for (float v : op->hloss) s += v;
   if (loss_out) *loss_out = (float)(s / (double)op->hloss.size());
@@ -449,7 +425,8 @@ extern "C" b200_status b200_neural_op_create(int N, int width, int modes, int la
             cudaMalloc(&op->grads, sizeof(float) * off) == cudaSuccess &&
             cudaMalloc(&op->adam_m, sizeof(float) * off) == cudaSuccess &&
             cudaMalloc(&op->adam_v, sizeof(float) * off) == cudaSuccess &&
-            cudaMalloc(&op->S, sizeof(float) * (size_t)N * modes) == cudaSuccess;
+            cudaMalloc(&op->S, sizeof(float) * (size_t)N * modes) == cudaSuccess &&
+            cudaMalloc(&op->dev_err, sizeof(int)) == cudaSuccess;
   if (ok) {
     std::vector<float> S((size_t)N * modes);
     const double c = std::sqrt(2.0 / (N + 1));
@@ -459,6 +436,7 @@ extern "C" b200_status b200_neural_op_create(int N, int width, int modes, int la
          cudaMemsetAsync(op->params, 0, sizeof(float) * off, op->stream) == cudaSuccess &&
          cudaMemsetAsync(op->adam_m, 0, sizeof(float) * off, op->stream) == cudaSuccess &&
          cudaMemsetAsync(op->adam_v, 0, sizeof(float) * off, op->stream) == cudaSuccess &&
+         cudaMemsetAsync(op->dev_err, 0, sizeof(int), op->stream) == cudaSuccess &&
          cudaStreamSynchronize(op->stream) == cudaSuccess;
   }
   if (!ok) {
@@ -479,6 +457,8 @@ extern "C" b200_status b200_neural_op_destroy(b200_neural_op op) {
   cudaFree(op->S);
   cudaFree(op->act);
   cudaFree(op->loss_bk);
+  cudaFree(op->ws);
+  cudaFree(op->dev_err);
   delete op;
   return B200_OK;
 }
@@ -515,7 +495,7 @@ extern "C" b200_status b200_neural_op_forward(b200_neural_op op, int batch, cons
   B200_CUDA_CHECK(cudaMemcpyAsync(out_dev, a.Y, sizeof(float) * (size_t)batch * op->K * op->P,
                                   cudaMemcpyDeviceToDevice, op->stream));
   B200_CUDA_CHECK(cudaStreamSynchronize(op->stream));
-  return B200_OK;
+  return gemm_status(op);
 }
 
 extern "C" b200_status b200_neural_op_loss_grad(b200_neural_op op, int batch, const float *features_dev,
@@ -530,8 +510,9 @@ extern "C" b200_status b200_neural_op_loss_grad(b200_neural_op op, int batch, co
   if (grads_host) {
     B200_CUDA_CHECK(
         cudaMemcpyAsync(grads_host, op->grads, sizeof(float) * op->nparams, cudaMemcpyDeviceToHost, op->stream));
+    B200_CUDA_CHECK(cudaStreamSynchronize(op->stream));
+    return gemm_status(op);
   }
-  B200_CUDA_CHECK(cudaStreamSynchronize(op->stream));
   return B200_OK;
 }
 

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -1407,6 +1408,7 @@ extern "C" b200_status b200_eps_destroy(b200_eps eps) {
   cudaFree(eps->rb32);
   cudaFree(eps->rb64);
   cudaFree(eps->mred);
+  if (eps->monitor_jsonl) fclose(eps->monitor_jsonl);
   delete eps;
   return B200_OK;
 }
@@ -1592,6 +1594,60 @@ extern "C" b200_status b200_eps_set_max_restarts(b200_eps eps, int max_restarts)
   return B200_OK;
 }
 
+// ---- EPSMonitor (src/eps/interface/epsmon.c:39-60, 96-130)
+static double host_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+void b200::eps_monitor_start(b200_eps eps) { eps->monitor_t0 = host_ms(); }
+
+b200_status b200::eps_monitor(b200_eps eps, int its, int nconv, const double *eigr, const double *errest, int nest) {
+  for (auto &m : eps->monitors)
+    if (m.first(eps, its, nconv, eigr, errest, nest, m.second) != 0) {
+      b200_set_last_error(__FILE__, __LINE__, "a monitor returned an error");
+      return B200_ERR_STATE;
+    }
+  if (eps->monitor_jsonl) {
+    FILE *f = eps->monitor_jsonl;
+    fprintf(f, "{\"its\": %d, \"nconv\": %d, \"nest\": %d, \"ms\": %.3f, \"gs_bytes\": %lld, \"eigr\": [", its, nconv,
+            nest, host_ms() - eps->monitor_t0, (long long)eps->stats.gs_bytes);
+    for (int i = 0; i < nest; ++i) fprintf(f, "%s%.17g", i ? ", " : "", eigr[i]);
+    fprintf(f, "], \"errest\": [");
+    for (int i = 0; i < nest; ++i) fprintf(f, "%s%.6e", i ? ", " : "", errest[i]);
+    fprintf(f, "]}\n");
+    fflush(f);
+  }
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_monitor_set(b200_eps eps, b200_eps_monitor_fn fn, void *ctx) {
+  B200_ARG_CHECK(eps, "null argument");
+  if (!fn) return b200_eps_monitor_cancel(eps);
+  B200_ARG_CHECK(eps->monitors.size() < 8, "too many monitors (at most 8)");
+  eps->monitors.emplace_back(fn, ctx);
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_monitor_cancel(b200_eps eps) {
+  B200_ARG_CHECK(eps, "null argument");
+  eps->monitors.clear();
+  if (eps->monitor_jsonl) fclose(eps->monitor_jsonl);
+  eps->monitor_jsonl = nullptr;
+  return B200_OK;
+}
+
+extern "C" b200_status b200_eps_monitor_jsonl(b200_eps eps, const char *path) {
+  B200_ARG_CHECK(eps && path, "null argument");
+  FILE *f = fopen(path, "w");
+  if (!f) {
+    b200_set_last_error(__FILE__, __LINE__, "cannot open the monitor file");
+    return B200_ERR_IO;
+  }
+  if (eps->monitor_jsonl) fclose(eps->monitor_jsonl);
+  eps->monitor_jsonl = f;
+  return B200_OK;
+}
+
 extern "C" b200_status b200_eps_set_timing(b200_eps eps, int on) {
   B200_ARG_CHECK(eps, "null argument");
   eps->timing = on;
@@ -1678,6 +1734,7 @@ extern "C" b200_status b200_eps_solve(b200_eps eps) {
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
   cudaEventRecord(t0, eps->stream);
+  eps_monitor_start(eps);
   RunTimer timer;
   timer.on = eps->timing != 0;
   double ms_restart = 0.0;
@@ -1737,6 +1794,7 @@ extern "C" b200_status b200_eps_solve(b200_eps eps) {
 
     if (eps->reason != B200_CONVERGED_ITERATING || breakdown || k == nv) l = 0;
     else l = std::max(1, (int)((nv - k) * eps->keep));
+    const int nconv_mon = k;   // what EPSMonitor reports (before the non-locking reset)
     if (!eps->lock && l > 0) {  // non-locking variant (krylovschur.c:295): reset the converged count
       l += k;
       k = 0;
@@ -1765,6 +1823,8 @@ extern "C" b200_status b200_eps_solve(b200_eps eps) {
     }
     eps->nconv = k;
     eps->stats.restarts++;
+    if (!eps->monitors.empty() || eps->monitor_jsonl)  // krylovschur.c:339
+      B200_CHECK(eps_monitor(eps, eps->its, nconv_mon, eps->eigr.data(), eps->errest.data(), nv));
     if (eps->max_restarts > 0 && eps->stats.restarts >= eps->max_restarts &&
         eps->reason == B200_CONVERGED_ITERATING)
       break;

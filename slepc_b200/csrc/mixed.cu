@@ -187,6 +187,13 @@ struct Block {
 
   // Rayleigh-Ritz on the current block: W = A X, the pencil (X^T A X, X^T X) in FP64, its
   // eigenvectors Q (wanted end first), X <- X Q, W <- W Q, residual norms ||W_c - theta_c X_c||.
+  int its = 0;  // sweeps so far (the monitor's iteration number)
+  b200_status monitor() {
+    ++its;
+    if (eps->monitors.empty() && !eps->monitor_jsonl) return B200_OK;
+    return eps_monitor(eps, its, leading_converged(eps->tol_), theta.data(), rel.data(), bp);
+  }
+
   b200_status rayleigh_ritz() {
     const int wb = free_buf({x});
     B200_CUDA_CHECK(spmm(buf(x), nullptr, buf(wb), 1.0, 0.0, 0.0));
@@ -406,6 +413,7 @@ b200_status b200::mixed_solve(b200_eps eps) {
   B.rel.assign(bp, 1.0);
 
   memset(&eps->stats, 0, sizeof(eps->stats));
+  eps_monitor_start(eps);
   if (eps->timing) {
     cudaEventCreate(&B.f0);
     cudaEventCreate(&B.f1);
@@ -443,6 +451,7 @@ b200_status b200::mixed_solve(b200_eps eps) {
     B200_CHECK(B.filter_segments(d, kSegCap32));
     B200_CHECK(B.svqb());
     B200_CHECK(B.rayleigh_ritz());
+    B200_CHECK(B.monitor());
     ++sweeps1;
     const double now = B.max_wanted();
     if (now > 0.5 * last) break;  // no longer halving: the FP32 rounding floor
@@ -459,6 +468,7 @@ b200_status b200::mixed_solve(b200_eps eps) {
     B200_CHECK(B.filter_segments(d, kSegCap32));
     B200_CHECK(B.svqb());
     B200_CHECK(B.rayleigh_ritz());
+    B200_CHECK(B.monitor());
     ++sweeps1;
   }
   cudaEventRecord(t1, s);
@@ -474,6 +484,7 @@ b200_status b200::mixed_solve(b200_eps eps) {
   B200_CHECK(B.filter(B.polish_degree(kWide, kPolishGrowth, deg_cap), kWide));
   B200_CHECK(B.svqb());
   B200_CHECK(B.rayleigh_ritz());
+  B200_CHECK(B.monitor());
   ++sweeps2;
   while (B.leading_converged(tol) < nev && sweeps2 < max_sweeps) {
     const int d = B.choose_degree(0.25 * tol, deg_cap);
@@ -481,6 +492,7 @@ b200_status b200::mixed_solve(b200_eps eps) {
     B200_CHECK(B.filter_segments(d, kSegCap64));
     B200_CHECK(B.svqb());
     B200_CHECK(B.rayleigh_ritz());
+    B200_CHECK(B.monitor());
     ++sweeps2;
   }
   const int lead = B.leading_converged(tol);

@@ -4,6 +4,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstdio>
+#include <utility>
 #include <vector>
 
 #include "common.h"
@@ -110,6 +112,10 @@ struct b200_eps_s {
   int nini_eff = 0;  // initial vectors kept by BVInsertVecs in the last setup
   double *dinv = nullptr;  // device inverse diagonal for the Jacobi preconditioner
   const void *dinv_of = nullptr;
+  // EPSMonitorSet: host callbacks per outer iteration; the built-in JSON-lines monitor
+  std::vector<std::pair<b200_eps_monitor_fn, void *>> monitors;
+  FILE *monitor_jsonl = nullptr;
+  double monitor_t0 = 0.0;  // host time (ms) at the start of the solve
   // mixed-precision form (b200_eps_set_precision): parameters and device buffers
   int precision = B200_PRECISION_FP64;
   double mixed_tol_low = 0.0;  // tolerance of the FP32 phase (0: default)

@@ -581,8 +581,11 @@ cudaError_t spmm_t(const SpmvSell &S, int n, const int *rowptr, const int *colin
   cudaError_t e = ensure_smem(rb_spmm_kernel<TV, TX, BP>, smem);
   if (e != cudaSuccess) return e;
   if (S.nslices > 0) {
-    int per_sm = (int)((200 * 1024) / (smem > 0 ? smem : 1));
-    per_sm = per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
+    // one resident wave: the grid-stride loop then spreads the slices evenly over the CTAs
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rb_spmm_kernel<TV, TX, BP>, kRbThreads, smem);
+    if (e != cudaSuccess) return e;
+    per_sm = per_sm < 1 ? 1 : per_sm;
     long long g = (S.nslices + (kRbThreads / 32) - 1) / (kRbThreads / 32);
     const long long cap = (long long)num_sms_host() * per_sm;
     if (g > cap) g = cap;

@@ -394,3 +394,50 @@ def test_nonlocking_rejects_restricted_mpd():
     assert ei.value.status == 11
     E.destroy()
     A.destroy()
+
+
+def test_monitor_once_per_restart(tmp_path):
+    """EPSMonitorSet: the callback runs once per outer iteration with the iteration number, the
+    converged count (nondecreasing with locking) and the current estimates; the JSON-lines monitor
+    writes the same iterations; a monitor that returns true aborts the solve."""
+    import json as _json
+
+    csr = P.laplacian_2d(60)
+    n = len(csr[0]) - 1
+    A = S.Mat().createAIJ(csr)
+    E = S.EPS().create()
+    E.setOperators(A)
+    E.setDimensions(8, 20)
+    E.setTolerances(1e-9)
+    E.setWhichEigenpairs(S.LARGEST_REAL)
+    E.setInitialSpace(P.start_vector(n, 1))
+    seen = []
+    E.setMonitor(lambda its, nconv, eigr, errest: seen.append((its, nconv, eigr[nconv:nconv + 1].copy(), len(errest))))
+    path = tmp_path / "monitor.jsonl"
+    E.setMonitorJSONL(str(path))
+    E.solve()
+    its = E.getIterationNumber()
+    assert [s[0] for s in seen] == list(range(1, its + 1))
+    assert all(a[1] <= b[1] for a, b in zip(seen, seen[1:]))
+    assert seen[-1][1] == E.getConverged()
+    lines = [_json.loads(x) for x in path.read_text().splitlines()]
+    assert [d["its"] for d in lines] == list(range(1, its + 1))
+    assert lines[-1]["nconv"] == E.getConverged() and len(lines[-1]["errest"]) == lines[-1]["nest"]
+    assert all(a["ms"] <= b["ms"] and a["gs_bytes"] <= b["gs_bytes"] for a, b in zip(lines, lines[1:]))
+    # a monitor asking to stop
+    E.cancelMonitor()
+    E.setMonitor(lambda its, nconv, eigr, errest: its >= 2)
+    with pytest.raises(S.B200Error) as ei:
+        E.solve()
+    assert ei.value.status == 7
+    E.cancelMonitor()
+    # the mixed form reports once per sweep
+    seen.clear()
+    E.setMonitor(lambda its, nconv, eigr, errest: seen.append((its, nconv)))
+    E.setPrecision(S.EPS.Precision.MIXED)
+    E.solve()
+    st = E.getStats()
+    assert [s[0] for s in seen] == list(range(1, st["phase1_restarts"] + st["filter_sweeps"] + 1))
+    assert seen[-1][1] >= 8
+    E.destroy()
+    A.destroy()

@@ -67,6 +67,12 @@ def parse():
     p.add_argument("--train-fields", type=int, default=256, help="learned workload: training fields")
     p.add_argument("--eval-fields", type=int, default=16, help="learned workload: held-out fields per step")
     p.add_argument("--epochs", type=int, default=120, help="learned workload: training epochs")
+    p.add_argument("--learn-orthog", choices=["gs", "chol"], default="chol",
+                   help="learned workload: block orthogonalization of the LOBPCG solves (BVOrthogBlockType)")
+    p.add_argument("--learn-modes", type=int, default=12, help="learned workload: sine modes per direction")
+    p.add_argument("--cpu-max-it", type=int, default=0,
+                   help="learned workload: iterations of the oracle's CPU sample (0: a complete solve); the "
+                        "per-iteration time is scaled by the GPU solve's iterations from the random block")
     p.add_argument("--workload", choices=["laplacian3d", "cross", "batched", "learned"], default="laplacian3d",
                    help="laplacian3d: the EPS headline case; cross: largest singular triplets of the "
                         "2,000,000 x 500,000 power-law matrix through A^T A; batched: 4096 k-NN graph "
@@ -823,13 +829,19 @@ EVAL_SEED0 = 100000
 
 
 def learned_config(args, extra=None):
-    d = {"workload": (f"{args.learn_nev} smallest eigenpairs of -div(kappa grad u) on a {args.learn_grid}^2 grid "
-                      "(5-point FV, kappa = exp(GRF), variance 1, correlation length U[0.05, 0.2]) by LOBPCG (Jacobi, "
-                      f"block {args.learn_nev}, tol 1e-8) on {args.eval_fields} held-out fields, started from the "
-                      "neural operator's block; the network (width 32, 12 x 12 modes, 4 layers) trained on the "
-                      f"plain solver's eigenvectors of {args.train_fields} fields, {args.epochs} epochs"),
+    reduced = ""
+    if args.learn_grid == 512 and (args.train_fields < 2000 or args.eval_fields < 200):
+        reduced = (f"the 512^2 / 2000 training / 200 held-out configuration reduced to {args.train_fields} training "
+                   f"and {args.eval_fields} held-out fields: ")
+    orth = {"gs": "Gram-Schmidt", "chol": "Cholesky"}[args.learn_orthog]
+    d = {"workload": (reduced + f"{args.learn_nev} smallest eigenpairs of -div(kappa grad u) on a {args.learn_grid}^2 "
+                      "grid (5-point FV, kappa = exp(GRF), variance 1, correlation length U[0.05, 0.2]) by LOBPCG "
+                      f"(Jacobi, block {args.learn_nev}, {orth} block orthogonalization, tol 1e-8) on "
+                      f"{args.eval_fields} held-out fields, started from the neural operator's block; the network "
+                      f"(width 32, {args.learn_modes} x {args.learn_modes} modes, 4 layers, tensor-core GEMMs) trained "
+                      f"on the plain solver's eigenvectors of {args.train_fields} fields, {args.epochs} epochs"),
          "grid": args.learn_grid, "nev": args.learn_nev, "train_fields": args.train_fields,
-         "eval_fields": args.eval_fields, "epochs": args.epochs, "tol": 1e-8,
+         "eval_fields": args.eval_fields, "epochs": args.epochs, "tol": 1e-8, "orthog_block": args.learn_orthog,
          "l2": "fields of %d x %d cells; every solve is a separate operator" % (args.learn_grid, args.learn_grid),
          "parallelism": "single GPU"}
     if extra:
@@ -850,9 +862,10 @@ def run_b200_learned(args):
     ranks = Ranks("nccl", timeout_s=3600)  # replicas: each rank trains and evaluates its own copy
     N, nev = args.learn_grid, args.learn_nev
     t0 = time.perf_counter()
-    F, T, its_train = LN.dataset(S, N, range(args.train_fields), nev)
+    ob = S.BV.OrthogBlockType.CHOL if args.learn_orthog == "chol" else None
+    F, T, its_train = LN.dataset(S, N, range(args.train_fields), nev, orthog_block=ob)
     t_data = time.perf_counter() - t0
-    dims = (N, 32, 12, 4, 64, nev)
+    dims = (N, 32, args.learn_modes, 4, 64, nev)
     op = S.NeuralOperator().create(*dims)
     op.setParams(LN.init_params(*dims, seed=0))
     Fd, Td = torch.from_numpy(F).cuda(), torch.from_numpy(T).cuda()
@@ -871,7 +884,7 @@ def run_b200_learned(args):
         out = []
         for i, (csr, _, _) in enumerate(probs):
             X0 = blocks[i].T.astype(np.float64) if learned else None
-            out.append(LN.solve_lowest(S, csr, nev, X0=X0))
+            out.append(LN.solve_lowest(S, csr, nev, X0=X0, orthog_block=ob))
         return out
 
     for _ in range(args.warmup):
@@ -905,7 +918,7 @@ def run_b200_learned(args):
         hf = torch.from_numpy(np.stack([LN.features(k) for _, k, _ in probs])).pin_memory()
         blocks = LN.predict(op, hf.cuda(non_blocking=True))
         for i, (csr, _, _) in enumerate(probs):
-            LN.solve_lowest(S, csr, nev, X0=blocks[i].T.astype(np.float64))
+            LN.solve_lowest(S, csr, nev, X0=blocks[i].T.astype(np.float64), orthog_block=ob)
     e2e_s = ranks.max((time.perf_counter() - t0) / args.steps)
     captured = [LN.captured(r["X"], b.T.astype(np.float64)) for r, b in zip(res_r, LN.predict(op, feats))]
     its_l = [r["its"] for r in res_l]
@@ -918,11 +931,19 @@ def run_b200_learned(args):
         threads = os.cpu_count() or 1
         oracle.set_threads(threads)
         csr0 = probs[0][0]
+        oob = oracle.ORTHOG_BLOCK_CHOL if args.learn_orthog == "chol" else oracle.ORTHOG_BLOCK_GS
         t0 = time.perf_counter()
-        r = oracle.lobpcg(P.to_scipy(csr0), nev, tol=1e-8, max_it=100000)
+        r = oracle.lobpcg(P.to_scipy(csr0), nev, tol=1e-8, max_it=args.cpu_max_it or 100000, orthog_block=oob)
         tc = time.perf_counter() - t0
-        cpu = {"value": tc, "unit": "s per field", "cores": threads, "kind": "port",
-               "sample": f"oracle LOBPCG from the random block on held-out field {seeds[0]} ({r.its} iterations)"}
+        if args.cpu_max_it:
+            its_gpu = res_r[0]["its"]
+            cpu = {"value": tc / max(r.its, 1) * its_gpu, "unit": "s per field", "cores": threads, "kind": "port",
+                   "sample": f"oracle LOBPCG from the random block on held-out field {seeds[0]}: {r.its} iterations "
+                             f"in {tc:.1f} s, scaled to the {its_gpu} iterations of the GPU solve from the random "
+                             "block"}
+        else:
+            cpu = {"value": tc, "unit": "s per field", "cores": threads, "kind": "port",
+                   "sample": f"oracle LOBPCG from the random block on held-out field {seeds[0]} ({r.its} iterations)"}
     if rank == 0:
         n = args.eval_fields
         line = {"metric": "time_to_all_residuals_le_1e-8_per_field", "value": ms_step / 1e3 / n, "unit": "s",

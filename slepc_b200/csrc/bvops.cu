@@ -176,17 +176,13 @@ __global__ void __launch_bounds__(kGemmThreads) panel_dmma_kernel(const TI *X, i
   }
 }
 
-// The same FP64 tensor-core product with the panel loads taken off the critical path: a producer warp
-// streams each 64-row panel of X into a ring of shared-memory stages with one 2-D TMA load of 72 rows x
-// kp columns (the box's 8 extra rows -- the next panel's first rows, or the zero fill past n -- give the
-// 72-double column stride that keeps the fragment loads at two wavefronts; their values are never
-// used), so the DMMA k-loop of one panel overlaps the loads of the next ones.  The eight consumer warps
-// compute rows 8w..8w+7 against every 8-column tile of Q (kept in shared memory) and write their
-// 8 x 2 results per tile straight from registers.  In place is safe: a panel has landed in shared
-// memory (its full barrier) before any of its rows is written, prefetches read other panels, and the
-// only rows two CTAs touch at once are the discarded extra rows.  Waits are bounded; a timeout sets
-// g_panel_err and the CTA stops (panel_gemm_error reads it).
-constexpr int kTmaRows = kRB + 8;          // rows of a panel's TMA box (the panel's column stride in shared memory)
+// The FP64 tensor-core product with the panel loads taken off the critical path (restart and BVMult):
+// a producer warp streams each 64-row panel of X into a ring of shared-memory stages with one 2-D TMA
+// load per panel, so the MMA k-loop of one panel overlaps the loads of the next ones.  In place is
+// safe: a panel has landed in shared memory (its full barrier) before any of its rows is written,
+// prefetches read other panels, and the only rows two CTAs touch at once are a box's extra rows past
+// its panel, whose values are never used.  Waits are bounded; a timeout sets g_panel_err and the CTA
+// stops (panel_gemm_error reads it).
 constexpr int kTmaThreads = kGemmThreads + 32;
 __device__ int g_panel_err;
 
@@ -204,25 +200,54 @@ __device__ __forceinline__ bool mbar_wait_parity(uint64_t *bar, uint32_t parity)
   return false;
 }
 
-template <int NT>
-__global__ void __launch_bounds__(kTmaThreads, 1) panel_dmma_tma_kernel(const __grid_constant__ CUtensorMap tx, double *Y,
-                                                                        int ldy, int n, int kq,
-                                                                        const double *__restrict__ Q, int ldq, int nc,
-                                                                        double alpha, double beta, int stages) {
-  extern __shared__ __align__(16) unsigned char tma_raw[];  // stages start 128-byte aligned (TMA destinations)
+// The MMAs are the larger FP64 shapes (mma.sync.m16n8k16 .f64; m16n8k8 with KM = 8): 9% faster than
+// m8n8k4 on the 128^3 restart (fewer fragment loads per flop; the shapes share one peak) with the
+// same result bits.  TMA box of 68 rows: a column stride of 4 mod 16 doubles keeps every fragment
+// load of a half warp on distinct banks.  Eight consumer warps as four 16-row strips times two
+// halves of the 8-column tiles of Q.  Per KM-deep step a warp loads its A fragment once (KM/2
+// doubles a lane) and reuses it across its tiles; Q's stride is also 4 mod 16.  Fragments
+// (g = lane / 4, t = lane % 4): A element i at row g + 8 (i % 2), depth t + 4 (i / 2); B element i
+// at depth t + 4 i, column g; D element i at row g + 8 (i / 2), column 2 t + i % 2.
+constexpr int kM16Box = kRB + 4;  // rows of a panel's TMA box (column stride in shared memory)
+__host__ __device__ inline int dmma16_q_stride(int ncp) { return ncp + ((4 - ncp % 16) + 16) % 16; }
+
+template <int KM>
+__device__ __forceinline__ void dmma_16x8(double (&d)[4], const double (&a)[KM / 2], const double (&b)[KM / 4]) {
+  if constexpr (KM == 8) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+  } else {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+        "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+          "d"(b[1]), "d"(b[2]), "d"(b[3]));
+  }
+}
+
+template <int NT, int KM>
+__global__ void __launch_bounds__(kTmaThreads, 1) panel_dmma16_kernel(const __grid_constant__ CUtensorMap tx, double *Y,
+                                                                      int ldy, int n, int kq,
+                                                                      const double *__restrict__ Q, int ldq, int nc,
+                                                                      double alpha, double beta, int stages) {
+  extern __shared__ __align__(16) unsigned char tma_raw[];
   double *sm = reinterpret_cast<double *>(tma_raw + ((128u - (smem_addr(tma_raw) & 127u)) & 127u));
   __shared__ __align__(8) uint64_t full[8], empty[8];
   __shared__ int last_issue[8];
   __shared__ volatile int stop;
-  const int kp = (kq + 3) & ~3;
+  constexpr int NTW = (NT + 1) / 2;  // 8-column tiles per consumer warp
   constexpr int ncp = NT * 8;
-  const int SQ = dmma_q_stride(ncp);
-  const size_t stage_elems = (size_t)kp * kTmaRows;
-  double *Xst = sm;                               // stages x [kp][kTmaRows]
-  double *Qs = sm + (size_t)stages * stage_elems; // kp x SQ
+  const int kp = (kq + KM - 1) / KM * KM;
+  const int SQ = dmma16_q_stride(ncp);
+  const size_t stage_elems = (size_t)kp * kM16Box;
+  double *Xst = sm;
+  double *Qs = sm + (size_t)stages * stage_elems;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int npanels = (n + kRB - 1) / kRB;
-  const int mine = blockIdx.x < npanels ? (npanels - 1 - blockIdx.x) / gridDim.x + 1 : 0;  // panels of this CTA
+  const int mine = blockIdx.x < npanels ? (npanels - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   if (tid == 0) {
     for (int s = 0; s < stages; ++s) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&full[s])), "r"(1) : "memory");
@@ -233,9 +258,9 @@ __global__ void __launch_bounds__(kTmaThreads, 1) panel_dmma_tma_kernel(const __
     stop = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (int idx = tid; idx < kp * ncp; idx += kTmaThreads) {
-    const int k = idx / ncp, j = idx - k * ncp;
-    Qs[k * SQ + j] = (k < kq && j < nc) ? Q[(size_t)k + (size_t)j * ldq] : 0.0;
+  for (int idx = tid; idx < kp * SQ; idx += kTmaThreads) {
+    const int k = idx / SQ, j = idx - k * SQ;
+    Qs[idx] = (k < kq && j < nc) ? Q[(size_t)k + (size_t)j * ldq] : 0.0;
   }
   __syncthreads();
   const uint32_t stage_bytes = (uint32_t)(stage_elems * sizeof(double));
@@ -262,6 +287,8 @@ __global__ void __launch_bounds__(kTmaThreads, 1) panel_dmma_tma_kernel(const __
     }
   } else {
     const int g = lane >> 2, t = lane & 3;
+    const int strip = warp & 3, half = warp >> 2;
+    const int j0 = half * NTW, j1 = (half + 1) * NTW < NT ? (half + 1) * NTW : NT;
     for (int i = 0; i < mine && !stop; ++i) {
       const int s = i % stages;
       if (!mbar_wait_parity(&full[s], (i / stages) & 1)) {
@@ -269,36 +296,47 @@ __global__ void __launch_bounds__(kTmaThreads, 1) panel_dmma_tma_kernel(const __
         stop = 1;
         break;
       }
-      const double *xa = Xst + (size_t)s * stage_elems + t * kTmaRows + warp * 8 + g;
-      const double *qb = Qs + t * SQ + g;
-      double acc[NT][2];
+      const double *xa = Xst + (size_t)s * stage_elems + (size_t)t * kM16Box + strip * 16 + g;
+      double acc[NTW][4];
 #pragma unroll
-      for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = 0.0;
-      for (int k0 = 0; k0 < kp; k0 += 4) {
-        const double a = xa[k0 * kTmaRows];
+      for (int j = 0; j < NTW; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
+      for (int k0 = 0; k0 < kp; k0 += KM) {
+        double a[KM / 2];
 #pragma unroll
-        for (int j = 0; j < NT; ++j) dmma_8x8x4(acc[j], a, qb[k0 * SQ + 8 * j]);
+        for (int e = 0; e < KM / 2; ++e) a[e] = xa[(size_t)(k0 + 4 * (e / 2)) * kM16Box + 8 * (e % 2)];
+#pragma unroll
+        for (int jj = 0; jj < NTW; ++jj) {
+          const int j = j0 + jj;
+          if (j < j1) {
+            double b[KM / 4];
+#pragma unroll
+            for (int e = 0; e < KM / 4; ++e) b[e] = Qs[(size_t)(k0 + t + 4 * e) * SQ + 8 * j + g];
+            dmma_16x8<KM>(acc[jj], a, b);
+          }
+        }
       }
       __syncwarp();
       if (lane == 0)
         asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s])) : "memory");
-      const long long r = (long long)(blockIdx.x + i * gridDim.x) * kRB + warp * 8 + g;
-      if (r < n) {
+      const long long rb = (long long)(blockIdx.x + i * gridDim.x) * kRB + strip * 16 + g;
 #pragma unroll
-        for (int j = 0; j < NT; ++j)
+      for (int jj = 0; jj < NTW; ++jj) {
+        const int j = j0 + jj;
+        if (j < j1) {
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int c = 8 * j + 2 * t + h;
-            if (c < nc) {
+          for (int e = 0; e < 4; ++e) {
+            const long long r = rb + 8 * (e / 2);
+            const int c = 8 * j + 2 * t + (e % 2);
+            if (r < n && c < nc) {
               double *y = Y + (size_t)c * ldy + r;
-              *y = beta == 0.0 ? alpha * acc[j][h] : alpha * acc[j][h] + beta * *y;
+              *y = beta == 0.0 ? alpha * acc[jj][e] : alpha * acc[jj][e] + beta * *y;
             }
           }
+        }
       }
     }
   }
   __syncthreads();
-  // loads issued but never consumed (only after a timeout) land before the CTA exits
   if (tid == 0)
     for (int s = 0; s < stages; ++s)
       if (last_issue[s] >= 0) mbar_wait_parity(&full[s], (last_issue[s] / stages) & 1);
@@ -416,6 +454,86 @@ __global__ void __launch_bounds__(256) gram_partial_kernel(const double *__restr
     for (int b = 0; b < TM; ++b) {
       const int i = TM * ty + a, j = TM * tx + b;
       if (i < cy && j < cx) partial[(size_t)blockIdx.x * npairs + (y0 + i) + (size_t)(x0 + j) * ny] = acc[a][b];
+    }
+}
+
+// Both Gram blocks of a Rayleigh-Ritz step from one pass over two T-column blocks (T = 16 TM, one
+// tile): M1 = Y^T X and M2 = Y^T Y, staged and summed exactly as gram_partial_kernel does each of
+// them (same panels, same row order per pair), so each has the bits of its own gram_partial_kernel
+// call.  partial[blk * 2 (nx ny) + ...] holds M1 in pair columns 0..nx-1 and M2 in nx..2nx-1.
+template <int TM>
+__global__ void __launch_bounds__(256) gram_dual_kernel(const double *__restrict__ X, int ldx,
+                                                        const double *__restrict__ Y, int ldy, int nc, int n,
+                                                        double *partial) {
+  constexpr int T = 16 * TM;
+  constexpr int kLoads = kGramRows * T / 256;
+  __shared__ double Xs[kGramRows][T + 1], Ys[kGramRows][T + 1];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const long long rows_per = (n + gridDim.x - 1) / gridDim.x;
+  const long long r0 = (long long)blockIdx.x * rows_per;
+  const long long r1 = min((long long)n, r0 + rows_per);
+  double a1[TM][TM], a2[TM][TM];
+#pragma unroll
+  for (int a = 0; a < TM; ++a)
+#pragma unroll
+    for (int b = 0; b < TM; ++b) a1[a][b] = a2[a][b] = 0.0;
+  double xr[kLoads], yr[kLoads];
+  auto load = [&](long long p0, int pr) {
+#pragma unroll
+    for (int u = 0; u < kLoads; ++u) {
+      const int e = threadIdx.x + 256 * u;
+      const int r = e % kGramRows, c = e / kGramRows;
+      xr[u] = (r < pr && c < nc) ? X[(size_t)c * ldx + p0 + r] : 0.0;
+      yr[u] = (r < pr && c < nc) ? Y[(size_t)c * ldy + p0 + r] : 0.0;
+    }
+  };
+  long long p0 = r0;
+  int pr = p0 < r1 ? (int)min((long long)kGramRows, r1 - p0) : 0;
+  if (pr > 0) load(p0, pr);
+  while (pr > 0) {
+#pragma unroll
+    for (int u = 0; u < kLoads; ++u) {
+      const int e = threadIdx.x + 256 * u;
+      const int r = e % kGramRows, c = e / kGramRows;
+      Xs[r][c] = xr[u];
+      Ys[r][c] = yr[u];
+    }
+    __syncthreads();
+    const long long pn = p0 + kGramRows;
+    const int prn = pn < r1 ? (int)min((long long)kGramRows, r1 - pn) : 0;
+    if (prn > 0) load(pn, prn);
+    for (int r = 0; r < pr; ++r) {
+      double yv[TM], xv[TM], zv[TM];
+#pragma unroll
+      for (int a = 0; a < TM; ++a) yv[a] = Ys[r][TM * ty + a];
+#pragma unroll
+      for (int b = 0; b < TM; ++b) {
+        xv[b] = Xs[r][TM * tx + b];
+        zv[b] = Ys[r][TM * tx + b];
+      }
+#pragma unroll
+      for (int a = 0; a < TM; ++a)
+#pragma unroll
+        for (int b = 0; b < TM; ++b) {
+          a1[a][b] = fma(yv[a], xv[b], a1[a][b]);
+          a2[a][b] = fma(yv[a], zv[b], a2[a][b]);
+        }
+    }
+    __syncthreads();
+    p0 = pn;
+    pr = prn;
+  }
+  const size_t npairs = (size_t)nc * nc;
+#pragma unroll
+  for (int a = 0; a < TM; ++a)
+#pragma unroll
+    for (int b = 0; b < TM; ++b) {
+      const int i = TM * ty + a, j = TM * tx + b;
+      if (i < nc && j < nc) {
+        double *pb = partial + (size_t)blockIdx.x * 2 * npairs;
+        pb[i + (size_t)j * nc] = a1[a][b];
+        pb[npairs + i + (size_t)j * nc] = a2[a][b];
+      }
     }
 }
 
@@ -717,13 +835,14 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 // The pipelined FP64 product when X is FP64, 16-byte aligned with an even leading dimension, and two
 // or more stages fit in shared memory beside Q; cudaErrorNotSupported otherwise (the caller falls back).
-cudaError_t panel_dmma_tma_launch(const double *X, int ldx, double *Y, int ldy, int n, int kq, const double *Q, int ldq,
-                                  int nc, cudaStream_t stream, double alpha, double beta) {
-  const int kp = (kq + 3) & ~3, nt = (nc + 7) / 8, ncp = 8 * nt;
+template <int KM>
+cudaError_t panel_dmma16_launch(const double *X, int ldx, double *Y, int ldy, int n, int kq, const double *Q, int ldq,
+                                int nc, cudaStream_t stream, double alpha, double beta) {
+  const int kp = (kq + KM - 1) / KM * KM, nt = (nc + 7) / 8, ncp = 8 * nt;
   if (kp > 256 || ((uintptr_t)X & 15) || (ldx & 1) || nt < 1 || nt > 16) return cudaErrorNotSupported;
-  const size_t stage = sizeof(double) * (size_t)kp * kTmaRows;
-  const size_t qbytes = sizeof(double) * (size_t)kp * dmma_q_stride(ncp);
-  const size_t avail = max_dynamic_smem() - 1024 - 128;  // static barriers, alignment and slack
+  const size_t stage = sizeof(double) * (size_t)kp * kM16Box;
+  const size_t qbytes = sizeof(double) * (size_t)kp * dmma16_q_stride(ncp);
+  const size_t avail = max_dynamic_smem() - 1024 - 128;
   if (avail < qbytes + 2 * stage) return cudaErrorNotSupported;
   int stages = (int)((avail - qbytes) / stage);
   if (stages > 8) stages = 8;
@@ -732,7 +851,7 @@ cudaError_t panel_dmma_tma_launch(const double *X, int ldx, double *Y, int ldy, 
   CUtensorMap tm;
   const cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)kq};
   const cuuint64_t strides[1] = {(cuuint64_t)ldx * sizeof(double)};
-  const cuuint32_t box[2] = {(cuuint32_t)kTmaRows, (cuuint32_t)kp};
+  const cuuint32_t box[2] = {(cuuint32_t)kM16Box, (cuuint32_t)kp};
   const cuuint32_t estr[2] = {1, 1};
   if (enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(X), dims, strides, box, estr,
           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -744,17 +863,17 @@ cudaError_t panel_dmma_tma_launch(const double *X, int ldx, double *Y, int ldy, 
   if (grid > npanels) grid = npanels;
   cudaError_t err = cudaSuccess;
   switch (nt) {
-#define B200_TMA_CASE(NT)                                                                                       \
-  case NT:                                                                                                      \
-    err = cudaFuncSetAttribute(panel_dmma_tma_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-    if (err != cudaSuccess) return err;                                                                         \
-    panel_dmma_tma_kernel<NT><<<grid, kTmaThreads, smem, stream>>>(tm, Y, ldy, n, kq, Q, ldq, nc, alpha, beta,      \
-                                                                   stages);                                    \
+#define B200_M16_CASE(NT)                                                                                          \
+  case NT:                                                                                                         \
+    err = cudaFuncSetAttribute(panel_dmma16_kernel<NT, KM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+    if (err != cudaSuccess) return err;                                                                            \
+    panel_dmma16_kernel<NT, KM><<<grid, kTmaThreads, smem, stream>>>(tm, Y, ldy, n, kq, Q, ldq, nc, alpha, beta,      \
+                                                                     stages);                                      \
     break;
-    B200_TMA_CASE(1) B200_TMA_CASE(2) B200_TMA_CASE(3) B200_TMA_CASE(4) B200_TMA_CASE(5) B200_TMA_CASE(6)
-    B200_TMA_CASE(7) B200_TMA_CASE(8) B200_TMA_CASE(9) B200_TMA_CASE(10) B200_TMA_CASE(11) B200_TMA_CASE(12)
-    B200_TMA_CASE(13) B200_TMA_CASE(14) B200_TMA_CASE(15) B200_TMA_CASE(16)
-#undef B200_TMA_CASE
+    B200_M16_CASE(1) B200_M16_CASE(2) B200_M16_CASE(3) B200_M16_CASE(4) B200_M16_CASE(5) B200_M16_CASE(6)
+    B200_M16_CASE(7) B200_M16_CASE(8) B200_M16_CASE(9) B200_M16_CASE(10) B200_M16_CASE(11) B200_M16_CASE(12)
+    B200_M16_CASE(13) B200_M16_CASE(14) B200_M16_CASE(15) B200_M16_CASE(16)
+#undef B200_M16_CASE
     default:
       return cudaErrorNotSupported;
   }
@@ -763,13 +882,14 @@ cudaError_t panel_dmma_tma_launch(const double *X, int ldx, double *Y, int ldy, 
   return cudaGetLastError();
 }
 
+
 template <typename TI, typename TO>
 cudaError_t panel_gemm_launch(const TI *X, int ldx, TO *Y, int ldy, int n, int kq, const double *Q, int ldq, int nc,
                               cudaStream_t stream, double alpha = 1.0, double beta = 0.0) {
   if (nc <= 0 || kq <= 0 || n <= 0) return cudaSuccess;
   if (nc > 16 * 8 || kq > kMaxCols) return cudaErrorInvalidValue;
   if constexpr (sizeof(TI) == sizeof(double) && sizeof(TO) == sizeof(double)) {
-    const cudaError_t err = panel_dmma_tma_launch(reinterpret_cast<const double *>(X), ldx,
+    const cudaError_t err = panel_dmma16_launch<16>(reinterpret_cast<const double *>(X), ldx,
                                                   reinterpret_cast<double *>(Y), ldy, n, kq, Q, ldq, nc, stream,
                                                   alpha, beta);
     if (err != cudaErrorNotSupported) return err;
@@ -954,6 +1074,49 @@ cudaError_t dot_launch(const double *X, int ldx, int nx, const double *Y, int ld
   }
   count_launch();
   dot_final_kernel<<<(npairs + 31) / 32, 256, 0, stream>>>(work, blocks, nx, ny, M, ldm);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t dot_dual_launch(const double *X, int ldx, const double *Y, int ldy, int nc, int n, double *M, double *work,
+                            int work_len, cudaStream_t stream, int ctas_per_sm) {
+  if (nc <= 0) return cudaSuccess;
+  if (nc > 64 || nc * nc < 64) return cudaErrorNotSupported;
+  const int npairs2 = 2 * nc * nc;
+  int blocks = num_sms() * (ctas_per_sm > 0 ? ctas_per_sm : 1);
+  if (blocks * npairs2 > work_len) blocks = work_len / npairs2;
+  if (blocks < 1) return cudaErrorInvalidValue;
+  const int tm = nc > 48 ? 4 : (nc + 15) / 16;
+  switch (tm) {
+    case 1: gram_dual_kernel<1><<<blocks, 256, 0, stream>>>(X, ldx, Y, ldy, nc, n, work); break;
+    case 2: gram_dual_kernel<2><<<blocks, 256, 0, stream>>>(X, ldx, Y, ldy, nc, n, work); break;
+    case 3: gram_dual_kernel<3><<<blocks, 256, 0, stream>>>(X, ldx, Y, ldy, nc, n, work); break;
+    default: gram_dual_kernel<4><<<blocks, 256, 0, stream>>>(X, ldx, Y, ldy, nc, n, work); break;
+  }
+  count_launch();
+  dot_final_kernel<<<(npairs2 + 31) / 32, 256, 0, stream>>>(work, blocks, 2 * nc, nc, M, nc);
+  count_launch();
+  return cudaGetLastError();
+}
+
+// R(:, j) = AX(:, j) - theta[j] X(:, j), j < ncols (each element rounded as BVCopy + VecAXPY give it)
+__global__ void resid_block_kernel(double *R, int ldr, const double *__restrict__ AX, int ldax,
+                                   const double *__restrict__ X, int ldx, int n, int ncols, ThetaArg th) {
+  const long long total = (long long)n * ncols;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(t / n);
+    const long long i = t - (long long)j * n;
+    R[i + (size_t)j * ldr] = __dsub_rn(AX[i + (size_t)j * ldax], __dmul_rn(th.v[j], X[i + (size_t)j * ldx]));
+  }
+}
+
+cudaError_t resid_block_launch(double *R, int ldr, const double *AX, int ldax, const double *X, int ldx, int n,
+                               int ncols, const double *theta, cudaStream_t stream) {
+  if (ncols <= 0 || n <= 0) return cudaSuccess;
+  if (ncols > kThetaMax) return cudaErrorInvalidValue;
+  ThetaArg th{};
+  for (int j = 0; j < ncols; ++j) th.v[j] = theta[j];
+  resid_block_kernel<<<grid_for((long long)n * ncols, 256), 256, 0, stream>>>(R, ldr, AX, ldax, X, ldx, n, ncols, th);
   count_launch();
   return cudaGetLastError();
 }

@@ -19,6 +19,9 @@ b200_status eps_insert_initial_space(b200_eps eps, b200_bv V, int max_cols);
 b200_status bv_orthogonalize_block(b200_bv bv);
 // BVOrthogonalizeVec + scale by 1/norm for several device vectors, one synchronisation.
 b200_status bv_orthonormalize_vecs(b200_bv bv, double *const *vecs, int count, int *breakdown);
+// BVDot(W, Z, MA) and BVDot(Z, Z, MB) over the same active column count, one pass over both blocks
+// and one synchronisation (the Gram pair of a Rayleigh-Ritz step; each as b200_bv_dot computes it).
+b200_status bv_dot_pair(b200_bv W, b200_bv Z, double *MA, double *MB, int ldm);
 // Column norms of the active columns, one synchronisation.
 b200_status bv_column_norms(b200_bv bv, double *nrm);
 // Streaming multiprocessors of the current device.

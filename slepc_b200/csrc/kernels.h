@@ -211,6 +211,17 @@ inline int dot_ctas_per_sm(int nx, int ny) { return (long long)nx * ny <= 64 * 6
 // ctas_per_sm (row blocks per SM of the partial sums).
 cudaError_t dot_launch(const double *X, int ldx, int nx, const double *Y, int ldy, int ny, int n, double *M, int ldm,
                        double *work, int work_len, cudaStream_t stream, int ctas_per_sm = 1);
+// M (nc x 2nc, ld nc) = [Y^T X | Y^T Y] from one pass over X and Y (nc <= 64 columns each; each
+// half has the bits of its own dot_launch); cudaErrorNotSupported outside that range.
+cudaError_t dot_dual_launch(const double *X, int ldx, const double *Y, int ldy, int nc, int n, double *M, double *work,
+                            int work_len, cudaStream_t stream, int ctas_per_sm);
+// R(:, j) = AX(:, j) - theta[j] X(:, j) for j < ncols <= kThetaMax (theta on the host).
+constexpr int kThetaMax = 128;
+struct ThetaArg {
+  double v[kThetaMax];
+};
+cudaError_t resid_block_launch(double *R, int ldr, const double *AX, int ldax, const double *X, int ldx, int n,
+                               int ncols, const double *theta, cudaStream_t stream);
 cudaError_t scale_launch(double *x, long long len, double alpha, cudaStream_t stream);
 cudaError_t copy_launch(double *dst, const double *src, long long len, cudaStream_t stream);
 // out[c] = ||X(:,c)||_2 for c < k (device), deterministic (fixed row split, fixed order).

@@ -84,20 +84,33 @@ __global__ void gelu_bwd_kernel(const float *__restrict__ dV, const float *__res
     dU[t] = dV[t] * gelu_grad(U[t]);
 }
 
-// db[c] = sum over b and p of D[b][c][p]: one block per channel, fixed order
-__global__ void bias_grad_kernel(const float *__restrict__ D, int B, int C, int P, float *db) {
+// db[c] = sum over b and p of D[b][c][p] in two fixed-order stages: block (c, s) sums its slice
+// s of the B * P entries of channel c into part[c * S + s]; bias_final_kernel adds the S slices.
+constexpr int kBiasSlices = 64;
+__global__ void bias_grad_kernel(const float *__restrict__ D, int B, int C, int P, float *part) {
   __shared__ float red[256];
-  const int c = blockIdx.x;
+  const int c = blockIdx.x, sl = blockIdx.y;
+  const long long total = (long long)B * P, per = (total + kBiasSlices - 1) / kBiasSlices;
+  const long long e0 = sl * per, e1 = min(total, e0 + per);
   float s = 0.f;
-  for (int b = 0; b < B; ++b)
-    for (int p = threadIdx.x; p < P; p += blockDim.x) s += D[((long long)b * C + c) * P + p];
+  for (long long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    const long long b = e / P, p = e - b * P;
+    s += D[(b * C + c) * P + p];
+  }
   red[threadIdx.x] = s;
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {
     if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) db[c] = red[0];
+  if (threadIdx.x == 0) part[(size_t)c * kBiasSlices + sl] = red[0];
+}
+__global__ void bias_final_kernel(const float *__restrict__ part, int C, float *db) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  float s = 0.f;
+  for (int q = 0; q < kBiasSlices; ++q) s += part[(size_t)c * kBiasSlices + q];
+  db[c] = s;
 }
 
 // Per (k, b): l = 1 - (y.u)^2/(y.y) and dY = (-2 (y.u)/(y.y) u + 2 (y.u)^2/(y.y)^2 y) * scale
@@ -274,7 +287,10 @@ cudaError_t bias_act(b200_neural_op op, int B, int C, float *U, const float *bia
   return cudaGetLastError();
 }
 cudaError_t bias_grad(b200_neural_op op, int B, int C, const float *D, float *db) {
-  bias_grad_kernel<<<C, 256, 0, op->stream>>>(D, B, C, op->P, db);
+  // the slices go to the GEMM workspace (free between GEMMs on the same stream)
+  bias_grad_kernel<<<dim3(C, kBiasSlices), 256, 0, op->stream>>>(D, B, C, op->P, op->ws);
+  count_launch();
+  bias_final_kernel<<<(C + 127) / 128, 128, 0, op->stream>>>(op->ws, C, db);
   count_launch();
   return cudaGetLastError();
 }

@@ -1216,6 +1216,36 @@ extern "C" b200_status b200_bv_dot(b200_bv X, b200_bv Y, double *M, int ldm) {
   return B200_OK;
 }
 
+namespace b200 {
+b200_status bv_dot_pair(b200_bv W, b200_bv Z, double *MA, double *MB, int ldm) {
+  B200_ARG_CHECK(W && Z && MA && MB && W->n == Z->n, "invalid BVDot pair arguments");
+  const int nc = Z->k - Z->l;
+  B200_ARG_CHECK(W->k - W->l == nc && ldm >= Z->k && ldm >= W->k, "BVDot pair: column ranges differ");
+  if (nc <= 0) return B200_OK;
+  const size_t sq = (size_t)nc * nc;
+  const int cps = dot_ctas_per_sm(nc, nc);
+  B200_CHECK(bv_reserve(Z, 2 * sq, 2 * sq * num_sms_host() * cps));
+  cudaError_t e = dot_dual_launch(col(W, W->l), W->ld, col(Z, Z->l), Z->ld, nc, Z->n, Z->qbuf, Z->red, Z->red_len,
+                                  Z->stream, cps);
+  if (e == cudaErrorNotSupported) {  // more than 64 columns: the two products one after the other
+    e = dot_launch(col(W, W->l), W->ld, nc, col(Z, Z->l), Z->ld, nc, Z->n, Z->qbuf, nc, Z->red, Z->red_len, Z->stream,
+                   cps);
+    if (e == cudaSuccess)
+      e = dot_launch(col(Z, Z->l), Z->ld, nc, col(Z, Z->l), Z->ld, nc, Z->n, Z->qbuf + sq, nc, Z->red, Z->red_len,
+                     Z->stream, cps);
+  }
+  B200_CUDA_CHECK(e);
+  B200_CUDA_CHECK(cudaMemcpyAsync(Z->hpin, Z->qbuf, sizeof(double) * 2 * sq, cudaMemcpyDeviceToHost, Z->stream));
+  B200_CUDA_CHECK(cudaStreamSynchronize(Z->stream));
+  for (int j = 0; j < nc; ++j)
+    for (int i = 0; i < nc; ++i) {
+      MA[(size_t)(Z->l + i) + (size_t)(W->l + j) * ldm] = Z->hpin[i + (size_t)j * nc];
+      MB[(size_t)(Z->l + i) + (size_t)(Z->l + j) * ldm] = Z->hpin[sq + i + (size_t)j * nc];
+    }
+  return B200_OK;
+}
+}  // namespace b200
+
 extern "C" b200_status b200_bv_dot_vec(b200_bv X, const double *y, double *q) {
   B200_ARG_CHECK(X && y && q, "null argument");
   const int k = X->k - X->l;

@@ -255,8 +255,13 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
     }
     // 7. residuals R = AX - X diag(eigr)
     int ini = lock ? nconv : 0;
-    B200_CUDA_CHECK(bv_copy(AX, R));
-    for (int j = ini; j < bs; ++j) B200_CUDA_CHECK(axmy_launch(col(R, j), col(X, j), eigr[locked + j], n, R->stream));
+    if (AX->l == ini && AX->k == bs && R->l == ini && R->k == bs) {  // BVCopy + VecAXPY per column, one launch
+      B200_CUDA_CHECK(resid_block_launch(col(R, ini), R->ld, col(AX, ini), AX->ld, col(X, ini), X->ld, n, bs - ini,
+                                         eigr.data() + locked + ini, R->stream));
+    } else {
+      B200_CUDA_CHECK(bv_copy(AX, R));
+      for (int j = ini; j < bs; ++j) B200_CUDA_CHECK(axmy_launch(col(R, j), col(X, j), eigr[locked + j], n, R->stream));
+    }
     // 8. residual norms and the active set
     int k = ini;
     bool countc = true;
@@ -368,11 +373,11 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
     eps->stats.lanczos_steps += nv;
     t0 = phase_begin();
     std::fill(MA.begin(), MA.end(), 0.0);
-    B200_CHECK(b200_bv_dot(W, Z, MA.data(), mpd));
+    std::fill(MB.begin(), MB.end(), 0.0);
+    // BVMatProject's M = Z^T W and BVDot's Z^T Z, one pass over both blocks
+    B200_CHECK(bv_dot_pair(W, Z, MA.data(), MB.data(), mpd));
     if (flip)
       for (double &v : MA) v = -v;
-    std::fill(MB.begin(), MB.end(), 0.0);
-    B200_CHECK(b200_bv_dot(Z, Z, MB.data(), mpd));  // BVMatProject_Dot
     // 24. the projected pencil
     B200_CHECK(ds_ghep(nv, mpd, MA, MB, wr, Q));
     for (int j = 0; j < nv; ++j)

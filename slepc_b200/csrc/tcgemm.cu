@@ -63,47 +63,70 @@ __device__ __forceinline__ float tf32_hi(float x) {
   return __uint_as_float(r);
 }
 
-// Stages rows r0..r0+R-1 (of `rows`) and depths k0..kend-1 of the operand element (r, kk) at
-// p[r * rs + kk * ks] into the hi / lo tiles, zero outside.  The loop runs along whichever of
-// r and kk has unit stride, so the global reads coalesce for row- and column-major views.
+// A thread's share of one operand chunk (R rows x kTcK depths) in registers: element u of the thread
+// is e = threadIdx.x + kTcThreads u of the tile, walked along whichever of r and kk has unit stride
+// so that the global reads coalesce for row- and column-major views.
 template <int R>
-__device__ __forceinline__ void stage_tile(const float *p, long long rs, long long ks, int r0, int rows, int k0,
-                                           int kend, unsigned char *hi, unsigned char *lo) {
-  const bool r_fast = rs == 1 && ks != 1;
-  for (int e = threadIdx.x; e < R * kTcK; e += kTcThreads) {
-    const int r = r_fast ? e % R : e / kTcK, kk = r_fast ? e / R : e % kTcK;
-    const int gr = r0 + r, gk = k0 + kk;
-    const float x = (gr < rows && gk < kend) ? __ldg(p + gr * rs + gk * ks) : 0.f;
-    const float h = tf32_hi(x);
-    const uint32_t o = core_off(r, kk);
-    *reinterpret_cast<float *>(hi + o) = h;
-    *reinterpret_cast<float *>(lo + o) = x - h;
+struct Chunk {
+  static constexpr int kPer = R * kTcK / kTcThreads;
+  float v[kPer];
+  __device__ __forceinline__ static void coords(bool r_fast, int u, int &r, int &kk) {
+    const int e = threadIdx.x + kTcThreads * u;
+    r = r_fast ? e % R : e / kTcK;
+    kk = r_fast ? e / R : e % kTcK;
   }
-}
+  // global -> registers (zero outside rows x [k0, kend)); element (r, kk) at p[r * rs + kk * ks]
+  __device__ __forceinline__ void load(const float *p, long long rs, long long ks, int r0, int rows, int k0,
+                                       int kend) {
+    const bool r_fast = rs == 1 && ks != 1;
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      int r, kk;
+      coords(r_fast, u, r, kk);
+      const int gr = r0 + r, gk = k0 + kk;
+      v[u] = (gr < rows && gk < kend) ? __ldg(p + gr * rs + gk * ks) : 0.f;
+    }
+  }
+  // registers -> the hi / lo tiles (TF32 high part and FP32 remainder)
+  __device__ __forceinline__ void store(long long rs, long long ks, unsigned char *hi, unsigned char *lo) const {
+    const bool r_fast = rs == 1 && ks != 1;
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      int r, kk;
+      coords(r_fast, u, r, kk);
+      const float h = tf32_hi(v[u]);
+      const uint32_t o = core_off(r, kk);
+      *reinterpret_cast<float *>(hi + o) = h;
+      *reinterpret_cast<float *>(lo + o) = v[u] - h;
+    }
+  }
+};
 
-
-// One 128 x NT tile of the product for blockIdx.z = z * ksplit + part: depths [part * kper, +kper) of
-// matrix z, written to C + blockIdx.z * bsc (ksplit = 1: the plain batched product).
-template <int NT>
+// One TM x NT tile of the product for blockIdx.z = z * ksplit + part: depths [part * kper, +kper) of
+// matrix z, written to C + blockIdx.z * bsc (ksplit = 1: the plain batched product).  Two shared
+// stages: while the MMAs of chunk c read one stage, the threads load chunk c + 1 into registers and
+// then (once the MMAs of chunk c - 1 have released it) split it into the other stage.  TM = 128: row
+// i of the tile in TMEM lane i; TM = 64: rows 16w..16w+15 in lanes 32w..32w+15.
+template <int TM, int NT>
 __global__ void __launch_bounds__(kTcThreads) tc_sgemm_kernel(int m, int n, int k, int ksplit, int kper, float alpha,
                                                               View A, View B, float beta, float *C, long long rsc,
                                                               long long csc, long long bsc, int *err) {
-  constexpr int kABytes = kTcM * kTcK * 4, kBBytes = NT * kTcK * 4;
+  constexpr int kABytes = TM * kTcK * 4, kBBytes = NT * kTcK * 4, kStage = 2 * (kABytes + kBBytes);
   constexpr uint32_t kCols = NT < 32 ? 32 : NT;  // TMEM columns (a power of two >= 32)
   extern __shared__ unsigned char raw[];
-  __shared__ __align__(8) uint64_t done;
+  __shared__ __align__(8) uint64_t done[2];
   __shared__ uint32_t tmem_base;
   __shared__ volatile int abort_flag;
   const uint32_t s0 = ptx::smem_u32(raw);
   unsigned char *sm = raw + ((128u - (s0 & 127u)) & 127u);
-  unsigned char *Ahi = sm, *Alo = sm + kABytes, *Bhi = sm + 2 * kABytes, *Blo = sm + 2 * kABytes + kBBytes;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long zz = blockIdx.z, z = zz / ksplit;
   const int kbeg = (int)(zz % ksplit) * kper, kend = min(k, kbeg + kper);
-  const int i0 = blockIdx.x * kTcM, j0 = blockIdx.y * NT;  // row tiles on x: up to 2^31 - 1
+  const int i0 = blockIdx.x * TM, j0 = blockIdx.y * NT;  // row tiles on x: up to 2^31 - 1
   const float *Ab = A.p + z * A.bs, *Bb = B.p + z * B.bs;
   if (threadIdx.x == 0) {
-    ptx::mbar_init(&done, 1);
+    ptx::mbar_init(&done[0], 1);
+    ptx::mbar_init(&done[1], 1);
     abort_flag = 0;
     ptx::fence_mbar_init();
   }
@@ -115,11 +138,22 @@ __global__ void __launch_bounds__(kTcThreads) tc_sgemm_kernel(int m, int n, int 
   __syncthreads();
   ptx::tc_fence_after();
   const uint32_t tmem = tmem_base;
-  constexpr uint32_t idesc = idesc_tf32_k(kTcM, NT);
-  int ch = 0;
-  for (int k0 = kbeg; k0 < kend; k0 += kTcK, ++ch) {
-    stage_tile<kTcM>(Ab, A.rs, A.cs, i0, m, k0, kend, Ahi, Alo);
-    stage_tile<NT>(Bb, B.cs, B.rs, j0, n, k0, kend, Bhi, Blo);
+  constexpr uint32_t idesc = idesc_tf32_k(TM, NT);
+  const int nch = kend > kbeg ? (kend - kbeg + kTcK - 1) / kTcK : 0;
+  Chunk<TM> ra;
+  Chunk<NT> rb;
+  if (nch > 0) {
+    ra.load(Ab, A.rs, A.cs, i0, m, kbeg, kend);
+    rb.load(Bb, B.cs, B.rs, j0, n, kbeg, kend);
+  }
+  for (int ch = 0; ch < nch; ++ch) {
+    const int st = ch & 1;
+    unsigned char *Ahi = sm + st * kStage, *Alo = Ahi + kABytes, *Bhi = Alo + kABytes, *Blo = Bhi + kBBytes;
+    if (ch >= 2 && !ptx::mbar_wait(&done[st], ((ch - 2) >> 1) & 1)) abort_flag = 1;  // chunk ch-2 released it
+    __syncthreads();
+    if (abort_flag) break;
+    ra.store(A.rs, A.cs, Ahi, Alo);
+    rb.store(B.cs, B.rs, Bhi, Blo);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic-proxy stores -> MMA reads
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -132,28 +166,34 @@ __global__ void __launch_bounds__(kTcThreads) tc_sgemm_kernel(int m, int n, int 
         ptx::mma_tf32(tmem, desc_kmajor(ah + ko), desc_kmajor(bl + ko), idesc, true);
         ptx::mma_tf32(tmem, desc_kmajor(al + ko), desc_kmajor(bh + ko), idesc, true);
       }
-      ptx::mma_commit(&done);
+      ptx::mma_commit(&done[st]);
     }
-    if (!ptx::mbar_wait(&done, ch & 1)) abort_flag = 1;  // the MMAs have read the tiles
-    __syncthreads();
-    if (abort_flag) break;
+    if (ch + 1 < nch) {  // the next chunk's global loads overlap this chunk's MMAs
+      const int k1 = kbeg + (ch + 1) * kTcK;
+      ra.load(Ab, A.rs, A.cs, i0, m, k1, kend);
+      rb.load(Bb, B.cs, B.rs, j0, n, k1, kend);
+    }
   }
+  // the last commit arrives after every earlier MMA of this thread has completed
+  if (!abort_flag && nch > 0 && !ptx::mbar_wait(&done[(nch - 1) & 1], ((nch - 1) >> 1) & 1)) abort_flag = 1;
+  __syncthreads();
   ptx::tc_fence_after();
-  const int row = i0 + warp * 32 + lane;
+  const bool live = TM == 128 || lane < 16;
+  const int row = i0 + (TM == 128 ? warp * 32 + lane : warp * 16 + (lane & 15));
   const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
   float *Cr = C + zz * bsc + (long long)row * rsc;
   if (!abort_flag) {
 #pragma unroll
     for (int c0 = 0; c0 < NT; c0 += 8) {
       float v[8];
-      if (ch > 0) {
+      if (nch > 0) {
         ptx::tmem_ld8(tl + (uint32_t)c0, v);
         ptx::tmem_wait_ld();
       } else {
 #pragma unroll
         for (int u = 0; u < 8; ++u) v[u] = 0.f;  // an empty depth range: the product is zero
       }
-      if (row < m) {
+      if (live && row < m) {
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
           const int j = j0 + c0 + u;
@@ -185,24 +225,33 @@ __global__ void tc_reduce_kernel(const float *__restrict__ W, int m, int n, int 
   }
 }
 
-template <int NT>
+template <int TM, int NT>
 cudaError_t launch_nt(cudaStream_t s, int zcount, int m, int n, int k, int ksplit, int kper, float alpha, View A,
                       View B, float beta, float *C, long long rsc, long long csc, long long bsc, int *err) {
-  const size_t smem = (size_t)(2 * kTcM * kTcK * 4 + 2 * NT * kTcK * 4) + 128;
-  cudaError_t e = cudaFuncSetAttribute(tc_sgemm_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const size_t smem = (size_t)2 * 2 * (TM * kTcK * 4 + NT * kTcK * 4) + 128;
+  cudaError_t e = cudaFuncSetAttribute(tc_sgemm_kernel<TM, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   if ((n + NT - 1) / NT > 65535) return cudaErrorInvalidValue;
-  const dim3 grid((m + kTcM - 1) / kTcM, (n + NT - 1) / NT, zcount);
-  tc_sgemm_kernel<NT><<<grid, kTcThreads, smem, s>>>(m, n, k, ksplit, kper, alpha, A, B, beta, C, rsc, csc, bsc, err);
+  const dim3 grid((m + TM - 1) / TM, (n + NT - 1) / NT, zcount);
+  tc_sgemm_kernel<TM, NT><<<grid, kTcThreads, smem, s>>>(m, n, k, ksplit, kper, alpha, A, B, beta, C, rsc, csc, bsc,
+                                                         err);
   count_launch();
   return cudaGetLastError();
 }
 
+template <int TM>
+cudaError_t launch_tm(cudaStream_t s, int zcount, int m, int n, int k, int ksplit, int kper, float alpha, View A,
+                      View B, float beta, float *C, long long rsc, long long csc, long long bsc, int *err) {
+  if (n <= 16) return launch_nt<TM, 16>(s, zcount, m, n, k, ksplit, kper, alpha, A, B, beta, C, rsc, csc, bsc, err);
+  if (n <= 32) return launch_nt<TM, 32>(s, zcount, m, n, k, ksplit, kper, alpha, A, B, beta, C, rsc, csc, bsc, err);
+  return launch_nt<TM, 64>(s, zcount, m, n, k, ksplit, kper, alpha, A, B, beta, C, rsc, csc, bsc, err);
+}
+
+// 64-row tiles when the output has at most 64 rows (no MMA rows and staging spent on padding)
 cudaError_t launch_any(cudaStream_t s, int zcount, int m, int n, int k, int ksplit, int kper, float alpha, View A,
                        View B, float beta, float *C, long long rsc, long long csc, long long bsc, int *err) {
-  if (n <= 16) return launch_nt<16>(s, zcount, m, n, k, ksplit, kper, alpha, A, B, beta, C, rsc, csc, bsc, err);
-  if (n <= 32) return launch_nt<32>(s, zcount, m, n, k, ksplit, kper, alpha, A, B, beta, C, rsc, csc, bsc, err);
-  return launch_nt<64>(s, zcount, m, n, k, ksplit, kper, alpha, A, B, beta, C, rsc, csc, bsc, err);
+  if (m <= 64) return launch_tm<64>(s, zcount, m, n, k, ksplit, kper, alpha, A, B, beta, C, rsc, csc, bsc, err);
+  return launch_tm<128>(s, zcount, m, n, k, ksplit, kper, alpha, A, B, beta, C, rsc, csc, bsc, err);
 }
 
 }  // namespace
@@ -221,14 +270,14 @@ cudaError_t tc_sgemm(cudaStream_t s, int batch, int m, int n, int k, float alpha
     Bv = View{Av.p, Av.cs, Av.rs, Av.bs};
     Av = t;
   }
-  const int NT = n <= 16 ? 16 : n <= 32 ? 32 : 64;
-  const long long tiles = (long long)((m + kTcM - 1) / kTcM) * ((n + NT - 1) / NT) * batch;
+  const int NT = n <= 16 ? 16 : n <= 32 ? 32 : 64, TM = m <= 64 ? 64 : kTcM;
+  const long long tiles = (long long)((m + TM - 1) / TM) * ((n + NT - 1) / NT) * batch;
   const long long mn = (long long)m * n;
-  // Split the depth when the tiles leave SMs idle and the depth is long: about two CTAs per SM,
-  // at least 128 deep per split, within the workspace.
+  // Split the depth when the tiles leave SMs idle and the depth is long: about four CTAs per SM,
+  // at least 256 deep per split, within the workspace.
   int ksplit = 1;
-  if (ws && k >= 256 && tiles < 2 * 148) {
-    ksplit = (int)std::min<long long>((2 * 148 + tiles - 1) / tiles, k / 128);
+  if (ws && k >= 512 && tiles < 4 * 148) {
+    ksplit = (int)std::min<long long>((4 * 148 + tiles - 1) / tiles, k / 256);
     ksplit = (int)std::min<long long>(ksplit, (long long)(ws_floats / (mn * batch)));
     if (ksplit < 1) ksplit = 1;
   }

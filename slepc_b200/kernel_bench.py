@@ -356,10 +356,40 @@ def multinplace(args, torch):
             "GBps": algo / (ms * 1e-3) / 1e9, "TFLOPs": flops / (ms * 1e-3) / 1e12}
 
 
+def neural(args, torch):
+    """One Adam training step of the neural operator (width 32, 12 x 12 modes, 4 layers, hidden 64,
+    16 outputs) on a batch of --nb synthetic fields of --lgrid^2 cells: device time per step and its
+    launches (the contractions are tensor-core GEMMs)."""
+    N, B = args.lgrid, args.nb
+    dims = (N, 32, 12, 4, 64, 16)
+    op = S.NeuralOperator().create(*dims)
+    from slepc_b200 import learned as LN
+
+    op.setParams(LN.init_params(*dims, seed=0))
+    g = torch.Generator(device="cuda").manual_seed(0)
+    F = torch.randn((B, 3, N * N), generator=g, device="cuda", dtype=torch.float32)
+    T = torch.randn((B, 16, N * N), generator=g, device="cuda", dtype=torch.float32)
+    for _ in range(args.warmup):
+        op.trainStep(F, T, 1e-4)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = S.kernel_launch_count()
+    e0.record()
+    for _ in range(args.reps):
+        op.trainStep(F, T, 1e-4)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.reps
+    launches = (S.kernel_launch_count() - l0) / args.reps
+    op.destroy()
+    return {"kernel": "neural-operator training step (forward, loss, backward, Adam)", "grid": N, "batch": B,
+            "ms": ms, "launches_per_step": launches, "ms_per_field": ms / B}
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("kernel", choices=["gs", "spmv", "spmm", "mixed", "rbgram", "multinplace", "cross", "batched", "lobpcg",
-                                      "lobpcg_ops", "all"])
+                                      "lobpcg_ops", "neural", "all"])
     p.add_argument("--lgrid", type=int, default=512, help="lobpcg: side of the 2-D diffusion grid")
     p.add_argument("--block", nargs="+", default=["gs", "chol", "svqb"], help="lobpcg: block orthogonalizations")
     p.add_argument("--phases", action="store_true", help="lobpcg: also a run with per-phase times")
@@ -395,7 +425,8 @@ def main():
             for line in (cross if k == "cross" else rbgram)(args, torch):
                 print(json.dumps(line), flush=True)
         else:
-            print(json.dumps({"spmv": spmv, "spmm": spmm, "mixed": mixed, "multinplace": multinplace}[k](args, torch)),
+            print(json.dumps({"spmv": spmv, "spmm": spmm, "mixed": mixed, "multinplace": multinplace,
+                              "neural": neural}[k](args, torch)),
                   flush=True)
 
 

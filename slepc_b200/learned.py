@@ -76,12 +76,13 @@ def solve_lowest(S, csr, nev=16, tol=1e-8, X0=None, max_it=100000, orthog_block=
     return out
 
 
-def dataset(S, N, seeds, nev=16):
-    """Features (len(seeds), 3, N*N) and targets (len(seeds), nev, N*N), float32, from plain solves."""
+def dataset(S, N, seeds, nev=16, orthog_block=None):
+    """Features (len(seeds), 3, N*N) and targets (len(seeds), nev, N*N), float32, from plain solves
+    (orthog_block: the BVOrthogBlockType of the solver's blocks, Gram-Schmidt when None)."""
     F, T, its = [], [], []
     for sd in seeds:
         csr, kappa, _ = P.diffusion_problem(N, int(sd))
-        r = solve_lowest(S, csr, nev)
+        r = solve_lowest(S, csr, nev, orthog_block=orthog_block)
         if r["nconv"] < nev:
             raise RuntimeError(f"plain solve of field {sd} converged {r['nconv']} < {nev} pairs")
         X = r["X"] / np.linalg.norm(r["X"], axis=0)

@@ -361,6 +361,14 @@ b200_status b200_tc_sgemm(int batch, int m, int n, int k, float alpha, const flo
                           long long acs, long long abs_, const float *B_dev, long long brs, long long bcs,
                           long long bbs, float beta, float *C_dev, long long rsc, long long csc, long long bsc,
                           int split, int sum_batch, void *stream);
+/* The same product queued on the stream without allocation or synchronisation: the caller passes
+ * the split-depth workspace (ws_floats floats, null for none: no depth split, and sum_batch then
+ * not allowed) and a device int that collects the error bits of bounded waits (read it after a
+ * synchronisation; nonzero means the product is invalid). */
+b200_status b200_tc_sgemm_async(int batch, int m, int n, int k, float alpha, const float *A_dev, long long ars,
+                                long long acs, long long abs_, const float *B_dev, long long brs, long long bcs,
+                                long long bbs, float beta, float *C_dev, long long rsc, long long csc, long long bsc,
+                                int sum_batch, float *ws_dev, size_t ws_floats, int *err_dev, void *stream);
 /* Mixed-form parameters (0 or a negative value keeps the default): tol_low,
  * the tolerance of the FP32 phase (default 5e-7, never below tol; the phase
  * also ends when a sweep no longer halves the largest wanted residual);
@@ -460,6 +468,13 @@ b200_status b200_eps_solve_csr_host(int n, int64_t nnz, const int *rowptr_host, 
                                     const double *vals_host, const double *v0_host, int nev, int ncv, int mpd,
                                     double tol, int max_it, int which, double *evals_host, double *X_host,
                                     double *errest_host, int *info_host, void *stream);
+/* The same with the arithmetic form chosen (B200_PRECISION_FP64 or
+ * B200_PRECISION_MIXED, b200_eps_set_precision); X_host then needs room for
+ * nconv vectors, at most max(ncv, 128). */
+b200_status b200_eps_solve_csr_host_ex(int n, int64_t nnz, const int *rowptr_host, const int *colind_host,
+                                       const double *vals_host, const double *v0_host, int nev, int ncv, int mpd,
+                                       double tol, int max_it, int which, int precision, double *evals_host,
+                                       double *X_host, double *errest_host, int *info_host, void *stream);
 
 /* ----------------------------------------------------- PETSc binary I/O --- */
 

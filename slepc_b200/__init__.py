@@ -88,6 +88,12 @@ _SIGS = {
     "b200_bv_normalize": (ctypes.c_int, [_vp, _dp]),
     "b200_bv_mult_inplace_trans": (ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "b200_rowblock_gram": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp]),
+    "b200_eps_solve_csr_host_ex": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, _ip, _ip, _dp, _dp, ctypes.c_int,
+                                                  ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                                  ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _ip, _vp]),
+    "b200_tc_sgemm_async": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                           _vp, _ll, _ll, _ll, _vp, _ll, _ll, _ll, ctypes.c_float, _vp, _ll, _ll, _ll,
+                                           ctypes.c_int, _vp, ctypes.c_size_t, _vp, _vp]),
     "b200_tc_sgemm": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, _vp,
                                      _ll, _ll, _ll, _vp, _ll, _ll, _ll, ctypes.c_float, _vp, _ll, _ll, _ll,
                                      ctypes.c_int, ctypes.c_int, _vp]),
@@ -824,28 +830,38 @@ def tc_sgemm(batch, m, n, k, alpha, A, B, beta, C, split=False, sum_batch=False,
                                stream))
 
 
+def tc_sgemm_async(batch, m, n, k, alpha, A, B, beta, C, ws=None, ws_floats=0, err=None, sum_batch=False,
+                   stream=None):
+    """b200_tc_sgemm_async: the same product queued without allocation or synchronisation; ws (device
+    pointer, ws_floats floats) the split-depth workspace, err a device int for the error bits."""
+    _check(lib().b200_tc_sgemm_async(batch, m, n, k, alpha, *A, *B, beta, *C, 1 if sum_batch else 0, ws, ws_floats,
+                                     err, stream))
+
+
 def solve_csr_host(csr, v0, nev, ncv, tol=1e-8, which=LARGEST_MAGNITUDE, mpd=0, max_it=0, want_vectors=True,
-                   stream=None, out=None):
-    """One call from host CSR arrays to host eigenpairs (b200_eps_solve_csr_host).  out: an optional
-    C-contiguous float64 array of shape (ncv + 1, n) that receives the eigenvectors (row i = vector i),
-    for callers that keep a reused (for instance page-locked) output buffer."""
+                   stream=None, out=None, precision=0):
+    """One call from host CSR arrays to host eigenpairs (b200_eps_solve_csr_host_ex).  out: an optional
+    C-contiguous float64 array of shape (ncv + 1, n), (max(ncv + 1, 128), n) for the mixed form, that
+    receives the eigenvectors (row i = vector i), for callers that keep a reused (for instance
+    page-locked) output buffer.  precision: EPS.Precision.FP64 (0) or MIXED (1)."""
     rowptr, colind, vals = (np.ascontiguousarray(csr[0], dtype=np.int32), np.ascontiguousarray(csr[1], dtype=np.int32),
                             np.ascontiguousarray(csr[2], dtype=np.float64))
     n = len(rowptr) - 1
     v0 = np.ascontiguousarray(v0, dtype=np.float64)
-    evals = np.zeros(ncv + 1)
-    errest = np.zeros(ncv + 1)
+    rows = ncv + 1 if not precision else max(ncv + 1, 128)  # the mixed form returns up to its block size
+    evals = np.zeros(rows)
+    errest = np.zeros(rows)
     # np.empty: only the rows the library writes (nconv of them) are ever touched
     if want_vectors and out is not None:
-        if out.shape != (ncv + 1, n) or out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]:
-            raise B200Error(1, "out must be a C-contiguous float64 array of shape (ncv + 1, n)")
+        if out.shape != (rows, n) or out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]:
+            raise B200Error(1, f"out must be a C-contiguous float64 array of shape ({rows}, n)")
         X = out
     else:
-        X = np.empty((ncv + 1, n)) if want_vectors else None
+        X = np.empty((rows, n)) if want_vectors else None
     info = np.zeros(8, dtype=np.int32)
-    _check(lib().b200_eps_solve_csr_host(n, int(rowptr[-1]), _i(rowptr), _i(colind), _d(vals), _d(v0), nev, ncv, mpd,
-                                         tol, max_it, which, _d(evals), _d(X) if want_vectors else None, _d(errest),
-                                         _i(info), stream))
+    _check(lib().b200_eps_solve_csr_host_ex(n, int(rowptr[-1]), _i(rowptr), _i(colind), _d(vals), _d(v0), nev, ncv,
+                                            mpd, tol, max_it, which, int(precision), _d(evals),
+                                            _d(X) if want_vectors else None, _d(errest), _i(info), stream))
     nconv = int(info[0])
     return {"evals": evals[:nconv].copy(), "X": X[:nconv].T if want_vectors else None,
             "errest": errest[:nconv].copy(), "nconv": nconv, "its": int(info[1]), "reason": int(info[2]),

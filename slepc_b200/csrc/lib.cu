@@ -1982,11 +1982,20 @@ extern "C" b200_status b200_eps_solve_csr_host(int n, int64_t nnz, const int *ro
                                                const double *vals, const double *v0, int nev, int ncv, int mpd,
                                                double tol, int max_it, int which, double *evals, double *X,
                                                double *errest, int *info, void *stream) {
+  return b200_eps_solve_csr_host_ex(n, nnz, rowptr, colind, vals, v0, nev, ncv, mpd, tol, max_it, which,
+                                    B200_PRECISION_FP64, evals, X, errest, info, stream);
+}
+
+extern "C" b200_status b200_eps_solve_csr_host_ex(int n, int64_t nnz, const int *rowptr, const int *colind,
+                                                  const double *vals, const double *v0, int nev, int ncv, int mpd,
+                                                  double tol, int max_it, int which, int precision, double *evals,
+                                                  double *X, double *errest, int *info, void *stream) {
   b200_mat A = nullptr;
   b200_eps E = nullptr;
   B200_CHECK(b200_mat_create_csr(n, nnz, rowptr, colind, vals, stream, &A));
   b200_status s = b200_eps_create(stream, &E);
   if (s == B200_OK) s = b200_eps_set_operators(E, A);
+  if (s == B200_OK && precision != B200_PRECISION_FP64) s = b200_eps_set_precision(E, precision);
   if (s == B200_OK) s = b200_eps_set_dimensions(E, nev, ncv, mpd);
   if (s == B200_OK) s = b200_eps_set_tolerances(E, tol, max_it);
   if (s == B200_OK) s = b200_eps_set_which_eigenpairs(E, which);

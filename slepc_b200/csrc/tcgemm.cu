@@ -39,11 +39,6 @@ struct View {
   long long rs, cs, bs;
 };
 
-// Byte offset of element (row, kk) of a K-major, non-swizzled tile (K chunk of kTcK).
-__device__ __forceinline__ uint32_t core_off(int row, int kk) {
-  return (uint32_t)(((row >> 3) * (kTcK / 4) + (kk >> 2)) * kCoreBytes + (row & 7) * 16 + (kk & 3) * 4);
-}
-
 __device__ __forceinline__ uint64_t desc_kmajor(uint32_t saddr) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
@@ -63,39 +58,41 @@ __device__ __forceinline__ float tf32_hi(float x) {
   return __uint_as_float(r);
 }
 
-// A thread's share of one operand chunk (R rows x kTcK depths) in registers: element u of the thread
-// is e = threadIdx.x + kTcThreads u of the tile, walked along whichever of r and kk has unit stride
-// so that the global reads coalesce for row- and column-major views.
+// A thread's share of one operand chunk (R rows x kTcK depths) in registers.  The tile holds
+// (R / 8) x (kTcK / 4) core matrices of 8 rows x 4 depths (128 contiguous bytes each); warp w takes
+// core matrices q = 4 u + w, so each warp-wide store fills one whole core matrix (conflict-free),
+// and lane l holds its element (rl, kl) -- rl = l % 8, kl = l / 8 when the rows have unit stride in
+// global memory (8 consecutive rows = one 32-byte sector per depth), rl = l / 4, kl = l % 4 when the
+// depths do (16 contiguous bytes per row).
 template <int R>
 struct Chunk {
-  static constexpr int kPer = R * kTcK / kTcThreads;
+  static constexpr int kKG = kTcK / 4;           // core matrices along the depth
+  static constexpr int kPer = (R / 8) * kKG / 4;  // core matrices per warp
   float v[kPer];
-  __device__ __forceinline__ static void coords(bool r_fast, int u, int &r, int &kk) {
-    const int e = threadIdx.x + kTcThreads * u;
-    r = r_fast ? e % R : e / kTcK;
-    kk = r_fast ? e / R : e % kTcK;
-  }
   // global -> registers (zero outside rows x [k0, kend)); element (r, kk) at p[r * rs + kk * ks]
   __device__ __forceinline__ void load(const float *p, long long rs, long long ks, int r0, int rows, int k0,
                                        int kend) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const bool r_fast = rs == 1 && ks != 1;
+    const int rl = r_fast ? (lane & 7) : (lane >> 2), kl = r_fast ? (lane >> 3) : (lane & 3);
 #pragma unroll
     for (int u = 0; u < kPer; ++u) {
-      int r, kk;
-      coords(r_fast, u, r, kk);
-      const int gr = r0 + r, gk = k0 + kk;
+      const int q = 4 * u + warp;
+      const int gr = r0 + (q / kKG) * 8 + rl, gk = k0 + (q % kKG) * 4 + kl;
       v[u] = (gr < rows && gk < kend) ? __ldg(p + gr * rs + gk * ks) : 0.f;
     }
   }
-  // registers -> the hi / lo tiles (TF32 high part and FP32 remainder)
+  // registers -> the hi / lo tiles (TF32 high part and FP32 remainder); byte offset of element
+  // (rl, kl) of core matrix q: q * 128 + rl * 16 + kl * 4
   __device__ __forceinline__ void store(long long rs, long long ks, unsigned char *hi, unsigned char *lo) const {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const bool r_fast = rs == 1 && ks != 1;
+    const int rl = r_fast ? (lane & 7) : (lane >> 2), kl = r_fast ? (lane >> 3) : (lane & 3);
+    const uint32_t o0 = (uint32_t)(rl * 16 + kl * 4);
 #pragma unroll
     for (int u = 0; u < kPer; ++u) {
-      int r, kk;
-      coords(r_fast, u, r, kk);
+      const uint32_t o = (uint32_t)(4 * u + warp) * kCoreBytes + o0;
       const float h = tf32_hi(v[u]);
-      const uint32_t o = core_off(r, kk);
       *reinterpret_cast<float *>(hi + o) = h;
       *reinterpret_cast<float *>(lo + o) = v[u] - h;
     }
@@ -228,7 +225,8 @@ __global__ void tc_reduce_kernel(const float *__restrict__ W, int m, int n, int 
 template <int TM, int NT>
 cudaError_t launch_nt(cudaStream_t s, int zcount, int m, int n, int k, int ksplit, int kper, float alpha, View A,
                       View B, float beta, float *C, long long rsc, long long csc, long long bsc, int *err) {
-  const size_t smem = (size_t)2 * 2 * (TM * kTcK * 4 + NT * kTcK * 4) + 128;
+  const int stages = kper <= kTcK ? 1 : 2;  // one chunk per CTA: the second stage would sit idle
+  const size_t smem = (size_t)stages * 2 * (TM * kTcK * 4 + NT * kTcK * 4) + 128;
   cudaError_t e = cudaFuncSetAttribute(tc_sgemm_kernel<TM, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   if ((n + NT - 1) / NT > 65535) return cudaErrorInvalidValue;
@@ -300,6 +298,18 @@ cudaError_t tc_sgemm(cudaStream_t s, int batch, int m, int n, int k, float alpha
 }  // namespace b200
 
 using namespace b200;
+
+extern "C" b200_status b200_tc_sgemm_async(int batch, int m, int n, int k, float alpha, const float *A, long long ars,
+                                           long long acs, long long abs_, const float *B, long long brs, long long bcs,
+                                           long long bbs, float beta, float *C, long long rsc, long long csc,
+                                           long long bsc, int sum_batch, float *ws, size_t ws_floats, int *err,
+                                           void *stream) {
+  B200_ARG_CHECK(batch > 0 && m > 0 && n > 0 && k >= 0 && A && B && C && err, "invalid GEMM arguments");
+  B200_ARG_CHECK(batch <= 65535 && (!sum_batch || ws), "batch above 65535, or sum_batch without a workspace");
+  B200_CUDA_CHECK(tc_sgemm((cudaStream_t)stream, batch, m, n, k, alpha, A, ars, acs, abs_, B, brs, bcs, bbs, beta, C,
+                           rsc, csc, bsc, err, ws, ws_floats, sum_batch != 0));
+  return B200_OK;
+}
 
 extern "C" b200_status b200_tc_sgemm(int batch, int m, int n, int k, float alpha, const float *A, long long ars,
                                      long long acs, long long abs_, const float *B, long long brs, long long bcs,

@@ -352,7 +352,7 @@ def multinplace(args, torch):
     ms /= args.reps
     algo = 8 * n * (k + e) + 8 * k * e
     flops = 2.0 * n * k * e
-    return {"kernel": "BVMultInPlace (panel_dmma_kernel)", "n": n, "k": k, "e-s": e, "ms": ms, "algorithmic_bytes": algo,
+    return {"kernel": "BVMultInPlace (panel_dmma16_kernel, mma.sync m16n8k16 f64)", "n": n, "k": k, "e-s": e, "ms": ms, "algorithmic_bytes": algo,
             "GBps": algo / (ms * 1e-3) / 1e9, "TFLOPs": flops / (ms * 1e-3) / 1e12}
 
 
@@ -386,10 +386,60 @@ def neural(args, torch):
             "ms": ms, "launches_per_step": launches, "ms_per_field": ms / B}
 
 
+def tcgemm(args, torch):
+    """The neural operator's two heaviest GEMM shapes on a --lgrid^2 grid, batch --nb, width 32, on
+    the tensor cores (b200_tc_sgemm_async, CUDA events on the launching stream, L2 flushed between
+    calls): the channel mix Out[b] = W In[b]
+    (32 x 32 times 32 x P per sample) and the weight gradient dW = sum_b D[b] X[b]^T (32 x 32 from
+    two 32 x P blocks per sample); algorithmic bytes = every operand read once and C written once."""
+    P_, B, W = args.lgrid ** 2, args.nb, 32
+    g = torch.Generator(device="cuda").manual_seed(0)
+    In = torch.randn((B, W, P_), generator=g, device="cuda")
+    D = torch.randn((B, W, P_), generator=g, device="cuda")
+    Wt = torch.randn((W, W), generator=g, device="cuda")
+    Out = torch.empty((B, W, P_), device="cuda")
+    dW = torch.empty((W, W), device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        ms = 0.0
+        for _ in range(args.reps):
+            flush.fill_(1.0)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        return ms / args.reps
+
+    ws = torch.empty(1 << 22, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    mix = lambda: S.tc_sgemm_async(B, W, P_, W, 1.0, (Wt.data_ptr(), W, 1, 0), (In.data_ptr(), P_, 1, W * P_), 0.0,
+                                   (Out.data_ptr(), P_, 1, W * P_), ws.data_ptr(), ws.numel(), err.data_ptr(),
+                                   stream=stream)
+    wgrad = lambda: S.tc_sgemm_async(B, W, W, P_, 1.0, (D.data_ptr(), P_, 1, W * P_), (In.data_ptr(), 1, P_, W * P_),
+                                     0.0, (dW.data_ptr(), W, 1, 0), ws.data_ptr(), ws.numel(), err.data_ptr(),
+                                     sum_batch=True, stream=stream)
+    out = []
+    for name, fn, algo in [("mix Out[b] = W In[b]", mix, 4 * (2 * B * W * P_ + W * W)),
+                           ("weight gradient sum_b D[b] X[b]^T", wgrad, 4 * (2 * B * W * P_ + W * W))]:
+        ms = timed(fn)
+        out.append({"kernel": f"tc_sgemm_kernel: {name}", "grid": args.lgrid, "batch": B, "ms": ms,
+                    "algorithmic_bytes": algo, "GBps": algo / (ms * 1e-3) / 1e9})
+    torch.cuda.synchronize()
+    if int(err.item()) != 0:
+        raise RuntimeError(f"tensor-core GEMM error bits {int(err.item())}")
+    return out
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("kernel", choices=["gs", "spmv", "spmm", "mixed", "rbgram", "multinplace", "cross", "batched", "lobpcg",
-                                      "lobpcg_ops", "neural", "all"])
+                                      "lobpcg_ops", "neural", "tcgemm", "all"])
     p.add_argument("--lgrid", type=int, default=512, help="lobpcg: side of the 2-D diffusion grid")
     p.add_argument("--block", nargs="+", default=["gs", "chol", "svqb"], help="lobpcg: block orthogonalizations")
     p.add_argument("--phases", action="store_true", help="lobpcg: also a run with per-phase times")
@@ -421,8 +471,8 @@ def main():
         elif k in ("lobpcg", "lobpcg_ops"):
             for line in (lobpcg if k == "lobpcg" else lobpcg_ops)(args, torch):
                 print(json.dumps(line), flush=True)
-        elif k in ("cross", "rbgram"):
-            for line in (cross if k == "cross" else rbgram)(args, torch):
+        elif k in ("cross", "rbgram", "tcgemm"):
+            for line in {"cross": cross, "rbgram": rbgram, "tcgemm": tcgemm}[k](args, torch):
                 print(json.dumps(line), flush=True)
         else:
             print(json.dumps({"spmv": spmv, "spmm": spmm, "mixed": mixed, "multinplace": multinplace,

@@ -121,3 +121,24 @@ def test_deterministic():
     runs = [_run(A, B, np.zeros((m, n), np.float32), 1.0, 0.0, (k, 1, 0), (n, 1, 0), (n, 1, 0), 1, m, n, k,
                  split=True) for _ in range(2)]
     np.testing.assert_array_equal(runs[0], runs[1])
+
+
+def test_async_entry_matches_synchronous_one():
+    # b200_tc_sgemm_async with a caller workspace and error word gives the synchronous entry's bits
+    import torch
+
+    rng = np.random.default_rng(21)
+    batch, Co, Ci, P = 3, 32, 16, 30000
+    D = rng.standard_normal((batch, Co, P)).astype(np.float32)
+    X = rng.standard_normal((batch, Ci, P)).astype(np.float32)
+    ref = _run(D, X, np.zeros((Co, Ci), np.float32), 1.0, 0.0, (P, 1, Co * P), (1, P, Ci * P), (Ci, 1, 0),
+               batch, Co, Ci, P, split=True, sum_batch=True)
+    Dd, Xd = _dev(D), _dev(X)
+    C = torch.zeros((Co, Ci), dtype=torch.float32, device="cuda")
+    ws = torch.empty(Co * Ci * batch * 64, dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    S.tc_sgemm_async(batch, Co, Ci, P, 1.0, (Dd.data_ptr(), P, 1, Co * P), (Xd.data_ptr(), 1, P, Ci * P), 0.0,
+                     (C.data_ptr(), Ci, 1, 0), ws.data_ptr(), ws.numel(), err.data_ptr(), sum_batch=True)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    np.testing.assert_array_equal(C.cpu().numpy(), ref)

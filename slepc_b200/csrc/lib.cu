@@ -1039,7 +1039,8 @@ b200_status b200::bv_column_norms(b200_bv bv, double *nrm) {
 // non-positive eigenvalue of the SVQB Gram matrix (a numerically rank-deficient block, for which
 // the reference would divide by zero or take the square root of a negative number) is reported as
 // a breakdown.
-static b200_status bv_orthogonalize_gram(b200_bv bv, double *R, int ldr) {
+// The device half: C, V2 -= V1 C and G queued on the stream with their read-back into bv->hpin.
+static b200_status bv_gram_enqueue(b200_bv bv) {
   const int l = bv->l, k = bv->k, nc = k - l, n = bv->n, ld = bv->ld;
   if (nc <= 0) return B200_OK;
   const size_t nC = (size_t)l * nc, nG = (size_t)nc * nc;
@@ -1054,7 +1055,16 @@ static b200_status bv_orthogonalize_gram(b200_bv bv, double *R, int ldr) {
   B200_CUDA_CHECK(
       dot_launch(col(bv, l), ld, nc, col(bv, l), ld, nc, n, Gdev, nc, bv->red, bv->red_len, s, cps_g));
   B200_CUDA_CHECK(cudaMemcpyAsync(bv->hpin, bv->qbuf, sizeof(double) * (nC + nG), cudaMemcpyDeviceToHost, s));
-  B200_CUDA_CHECK(cudaStreamSynchronize(s));
+  return B200_OK;
+}
+
+// The host half, after a synchronisation of the stream: factor G, then queue V2 := V2 S.
+static b200_status bv_gram_finish(b200_bv bv, double *R, int ldr) {
+  const int l = bv->l, k = bv->k, nc = k - l, n = bv->n, ld = bv->ld;
+  if (nc <= 0) return B200_OK;
+  const size_t nC = (size_t)l * nc, nG = (size_t)nc * nc;
+  cudaStream_t s = bv->stream;
+  double *Gdev = bv->qbuf + nC;
   std::vector<double> C(bv->hpin, bv->hpin + nC), G(bv->hpin + nC, bv->hpin + nC + nG), Rf(nG, 0.0), S(nG, 0.0);
   int info = 0;
   if (bv->orthog_block == B200_ORTHOG_BLOCK_CHOL) {
@@ -1120,6 +1130,28 @@ static b200_status bv_orthogonalize_gram(b200_bv bv, double *R, int ldr) {
   }
   return B200_OK;
 }
+
+static b200_status bv_orthogonalize_gram(b200_bv bv, double *R, int ldr) {
+  B200_CHECK(bv_gram_enqueue(bv));
+  B200_CUDA_CHECK(cudaStreamSynchronize(bv->stream));
+  return bv_gram_finish(bv, R, ldr);
+}
+
+namespace b200 {
+b200_status bv_orthogonalize_pair(b200_bv a, b200_bv b) {
+  B200_ARG_CHECK(a && b && a != b, "invalid BVOrthogonalize pair");
+  const bool gram = a->orthog_block != B200_ORTHOG_BLOCK_GS && b->orthog_block != B200_ORTHOG_BLOCK_GS;
+  if (!gram || a->stream != b->stream) {
+    B200_CHECK(b200_bv_orthogonalize(a, nullptr, 0));
+    return b200_bv_orthogonalize(b, nullptr, 0);
+  }
+  B200_CHECK(bv_gram_enqueue(a));
+  B200_CHECK(bv_gram_enqueue(b));
+  B200_CUDA_CHECK(cudaStreamSynchronize(a->stream));
+  B200_CHECK(bv_gram_finish(a, nullptr, 0));
+  return bv_gram_finish(b, nullptr, 0);
+}
+}  // namespace b200
 
 extern "C" b200_status b200_bv_orthogonalize(b200_bv bv, double *R, int ldr) {
   B200_ARG_CHECK(bv && (!R || ldr >= bv->k), "R leading dimension too small");

@@ -351,8 +351,11 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
       }
     }
     // 11. orthonormalise the preconditioned residuals; 13-16 the conjugate directions
-    B200_CHECK(b200_bv_orthogonalize(R, nullptr, 0));
-    if (its > 1) B200_CHECK(b200_bv_orthogonalize(P, nullptr, 0));
+    if (its > 1) {
+      B200_CHECK(bv_orthogonalize_pair(R, P));  // independent blocks: one host round trip for both
+    } else {
+      B200_CHECK(b200_bv_orthogonalize(R, nullptr, 0));
+    }
     phase_end(t0, eps->stats.ms_orth);
     // 17-23. Z = [X R P] and the Gram matrices Z^T A Z, Z^T Z
     active(Z, 0, bs);

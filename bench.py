@@ -65,11 +65,14 @@ def parse():
     p.add_argument("--learn-grid", type=int, default=64, help="learned workload: N of the N x N diffusion grid")
     p.add_argument("--learn-nev", type=int, default=16, help="learned workload: eigenpairs (LOBPCG block)")
     p.add_argument("--train-fields", type=int, default=256, help="learned workload: training fields")
-    p.add_argument("--eval-fields", type=int, default=16, help="learned workload: held-out fields per step")
+    p.add_argument("--eval-fields", type=int, default=16,
+                   help="learned workload: held-out fields per step (every step, warm-up included, its own)")
     p.add_argument("--epochs", type=int, default=120, help="learned workload: training epochs")
     p.add_argument("--learn-orthog", choices=["gs", "chol"], default="chol",
                    help="learned workload: block orthogonalization of the LOBPCG solves (BVOrthogBlockType)")
     p.add_argument("--learn-modes", type=int, default=12, help="learned workload: sine modes per direction")
+    p.add_argument("--e2e-steps", type=int, default=0,
+                   help="learned workload: timed steps repeated end to end (0: all of them)")
     p.add_argument("--cpu-max-it", type=int, default=0,
                    help="learned workload: iterations of the oracle's CPU sample (0: a complete solve); the "
                         "per-iteration time is scaled by the GPU solve's iterations from the random block")
@@ -808,19 +811,23 @@ EVAL_SEED0 = 100000
 
 
 def learned_config(args, extra=None):
+    held = args.eval_fields * args.steps
     reduced = ""
-    if args.learn_grid == 512 and (args.train_fields < 2000 or args.eval_fields < 200):
+    if args.learn_grid == 512 and (args.train_fields < 2000 or held < 200):
         reduced = (f"the 512^2 / 2000 training / 200 held-out configuration reduced to {args.train_fields} training "
-                   f"and {args.eval_fields} held-out fields: ")
+                   f"and {held} held-out fields: ")
     orth = {"gs": "Gram-Schmidt", "chol": "Cholesky"}[args.learn_orthog]
     d = {"workload": (reduced + f"{args.learn_nev} smallest eigenpairs of -div(kappa grad u) on a {args.learn_grid}^2 "
                       "grid (5-point FV, kappa = exp(GRF), variance 1, correlation length U[0.05, 0.2]) by LOBPCG "
-                      f"(Jacobi, block {args.learn_nev}, {orth} block orthogonalization, tol 1e-8) on "
-                      f"{args.eval_fields} held-out fields, started from the neural operator's block; the network "
+                      f"(Jacobi, block {args.learn_nev}, {orth} block orthogonalization, tol 1e-8) on {held} held-out "
+                      f"fields ({args.eval_fields} per step; {args.warmup * args.eval_fields} more in the warm-up steps), "
+                      "started from the "
+                      "neural operator's block; the network "
                       f"(width 32, {args.learn_modes} x {args.learn_modes} modes, 4 layers, tensor-core GEMMs) trained "
                       f"on the plain solver's eigenvectors of {args.train_fields} fields, {args.epochs} epochs"),
          "grid": args.learn_grid, "nev": args.learn_nev, "train_fields": args.train_fields,
-         "eval_fields": args.eval_fields, "epochs": args.epochs, "tol": 1e-8, "orthog_block": args.learn_orthog,
+         "eval_fields": held, "eval_fields_per_step": args.eval_fields, "epochs": args.epochs, "tol": 1e-8,
+         "orthog_block": args.learn_orthog,
          "l2": "fields of %d x %d cells; every solve is a separate operator" % (args.learn_grid, args.learn_grid),
          "parallelism": "single GPU"}
     if extra:
@@ -852,22 +859,33 @@ def run_b200_learned(args):
     hist = LN.train(op, Fd, Td, epochs=args.epochs, batch=8, lr=2e-3, lr_final=2e-4)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
-    # held-out fields: each rank evaluates its own (weak scaling)
-    seeds = list(range(EVAL_SEED0 + rank * args.eval_fields, EVAL_SEED0 + (rank + 1) * args.eval_fields))
-    probs = [P.diffusion_problem(N, sd) for sd in seeds]
-    feats = torch.from_numpy(np.stack([LN.features(k) for _, k, _ in probs])).cuda()
-    launches0 = None
+    # held-out fields: every step (warm-up and timed) solves its own eval_fields fields, and each rank
+    # its own range of seeds (weak scaling)
+    E = args.eval_fields
+    span = (args.warmup + args.steps) * E
+    base = EVAL_SEED0 + rank * span
 
-    def step(learned):
-        blocks = LN.predict(op, feats) if learned else None
+    def fields(step_index):
+        seeds_i = list(range(base + step_index * E, base + (step_index + 1) * E))
+        probs_i = [P.diffusion_problem(N, sd) for sd in seeds_i]
+        feats_i = torch.from_numpy(np.stack([LN.features(k) for _, k, _ in probs_i])).cuda()
+        return seeds_i, probs_i, feats_i
+
+    warm = [fields(i) for i in range(args.warmup)]
+    timed = [fields(args.warmup + i) for i in range(args.steps)]
+    seeds = [sd for sd_i, _, _ in timed for sd in sd_i]
+
+    def step(batch, learned):
+        _, probs_i, feats_i = batch
+        blocks = LN.predict(op, feats_i) if learned else None
         out = []
-        for i, (csr, _, _) in enumerate(probs):
+        for i, (csr, _, _) in enumerate(probs_i):
             X0 = blocks[i].T.astype(np.float64) if learned else None
             out.append(LN.solve_lowest(S, csr, nev, X0=X0, orthog_block=ob))
         return out
 
-    for _ in range(args.warmup):
-        step(True)
+    for bt in warm:
+        step(bt, True)
     torch.cuda.synchronize()
     ranks.barrier()
     torch.cuda.synchronize()
@@ -876,8 +894,9 @@ def run_b200_learned(args):
     launches0 = S.kernel_launch_count()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
-    for _ in range(args.steps):
-        res_l = step(True)
+    res_l = []
+    for bt in timed:
+        res_l += step(bt, True)
     ev1.record()
     torch.cuda.synchronize()
     ranks.barrier()
@@ -885,24 +904,31 @@ def run_b200_learned(args):
     clk = clocks.stop()
     launches = S.kernel_launch_count() - launches0
     ms_step = ranks.max(ev0.elapsed_time(ev1) / args.steps)
+    # the same timed fields from the seeded random block (the fallback)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    res_r = step(False)
+    res_r = []
+    for bt in timed:
+        res_r += step(bt, False)
     e1.record()
     torch.cuda.synchronize()
-    ms_random = ranks.max(e0.elapsed_time(e1))
-    # end to end: host fields in, host eigenpairs out (features up, network, block down, solve, pairs down)
+    ms_random = ranks.max(e0.elapsed_time(e1) / args.steps)
+    # end to end on the first e2e_steps timed steps: host fields in, host eigenpairs out (features up,
+    # network, block down, solve, pairs down)
+    ne2e = max(1, min(args.e2e_steps or args.steps, args.steps))
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        hf = torch.from_numpy(np.stack([LN.features(k) for _, k, _ in probs])).pin_memory()
+    for _, probs_i, _ in timed[:ne2e]:
+        hf = torch.from_numpy(np.stack([LN.features(k) for _, k, _ in probs_i])).pin_memory()
         blocks = LN.predict(op, hf.cuda(non_blocking=True))
-        for i, (csr, _, _) in enumerate(probs):
+        for i, (csr, _, _) in enumerate(probs_i):
             LN.solve_lowest(S, csr, nev, X0=blocks[i].T.astype(np.float64), orthog_block=ob)
-    e2e_s = ranks.max((time.perf_counter() - t0) / args.steps)
-    captured = [LN.captured(r["X"], b.T.astype(np.float64)) for r, b in zip(res_r, LN.predict(op, feats))]
+    e2e_s = ranks.max((time.perf_counter() - t0) / ne2e)
+    preds = np.concatenate([LN.predict(op, f) for _, _, f in timed])
+    captured = [LN.captured(r["X"], b.T.astype(np.float64)) for r, b in zip(res_r, preds)]
     its_l = [r["its"] for r in res_l]
     its_r = [r["its"] for r in res_r]
     ok = all(r["nconv"] >= nev and r["max_error"] <= 1e-8 for r in res_l + res_r)
+    probs = timed[0][1]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle
@@ -924,7 +950,8 @@ def run_b200_learned(args):
             cpu = {"value": tc, "unit": "s per field", "cores": threads, "kind": "port",
                    "sample": f"oracle LOBPCG from the random block on held-out field {seeds[0]} ({r.its} iterations)"}
     if rank == 0:
-        n = args.eval_fields
+        n = E
+        wins = int(sum(1 for a_, b_ in zip(its_l, its_r) if a_ < b_))
         line = {"metric": "time_to_all_residuals_le_1e-8_per_field", "value": ms_step / 1e3 / n, "unit": "s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
                 "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64 solve, f32 network",
@@ -936,11 +963,13 @@ def run_b200_learned(args):
                                       "mean_iterations_learned": float(np.mean(its_l)),
                                       "mean_iterations_random": float(np.mean(its_r)),
                                       "iterations_learned": its_l, "iterations_random": its_r,
+                                      "fields_with_fewer_iterations": wins, "fields": len(its_l),
+                                      "held_out_seeds": seeds,
                                       "mean_captured_subspace": float(np.mean(captured)),
                                       "all_pairs_converged_to_1e-8": ok},
                 "roofline": None,
                 "e2e": {"value": e2e_s / n, "unit": "s", "h2d_bytes_per_step": int(n * 3 * N * N * 4),
-                        "d2h_bytes_per_step": int(n * nev * N * N * 12)},
+                        "d2h_bytes_per_step": int(n * nev * N * N * 12), "steps": ne2e},
                 "gpu_launches": int(launches), "clocks": clk, "cpu_baseline": cpu}
         print(json.dumps(line))
     op.destroy()

@@ -964,6 +964,12 @@ def run_b200_learned(args):
                                       "mean_iterations_random": float(np.mean(its_r)),
                                       "iterations_learned": its_l, "iterations_random": its_r,
                                       "fields_with_fewer_iterations": wins, "fields": len(its_l),
+                                      "max_error_learned": [r["max_error"] for r in res_l],
+                                      "max_error_random": [r["max_error"] for r in res_r],
+                                      "nconv_learned": [r["nconv"] for r in res_l],
+                                      "nconv_random": [r["nconv"] for r in res_r],
+                                      "reason_learned": [r["reason"] for r in res_l],
+                                      "reason_random": [r["reason"] for r in res_r],
                                       "held_out_seeds": seeds,
                                       "mean_captured_subspace": float(np.mean(captured)),
                                       "all_pairs_converged_to_1e-8": ok},

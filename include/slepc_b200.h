@@ -431,8 +431,10 @@ typedef struct {
   int64_t column_visits;  /* sum over Lanczos steps j of (j+2): basis columns one CGS pass reads */
   /* mixed precision (zero otherwise): sweeps of the FP64 phase, the largest Chebyshev degree of a
    * sweep, block columns, sweeps of the FP32 phase, device time of the two phases, and block-SpMV
-   * columns (block width x block SpMVs).  In the mixed form with timing on, ms_spmv and gs_bytes
-   * hold the device time and the algorithmic bytes of the Chebyshev filters' block SpMVs. */
+   * columns (block width x block SpMVs).  In the mixed form gs_passes counts the block
+   * orthonormalisations (SVQB) and restarts the Rayleigh-Ritz steps; with timing on, ms_spmv and
+   * gs_bytes hold the device time and the algorithmic bytes of the Chebyshev filters' block SpMVs,
+   * ms_orth and ms_restart the wall time of the orthonormalisations and Rayleigh-Ritz steps. */
   int64_t filter_sweeps;
   int64_t filter_degree;
   int64_t block_size;

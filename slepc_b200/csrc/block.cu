@@ -24,7 +24,7 @@ namespace {
 constexpr int kBlockThreads = 256;
 constexpr int kGroup = 8;  // columns of the block per pass over a long row
 constexpr int kChunk = 8;  // nonzeros of a slice row held in registers
-constexpr int kCols = 4;   // block columns whose gathers are issued together
+constexpr int kCols = 2;   // block columns whose gathers are issued together (80 registers, 3 CTAs per SM)
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -39,7 +39,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 // throughout).  Each row's products are rounded and summed in index order, as the single-vector
 // sliced-ELL SpMV does, so a column of the result has the same bits as that SpMV.
 template <typename VT, int CB>
-__global__ void __launch_bounds__(kBlockThreads) spmm_sell_kernel(int nslices, int n, const long long *__restrict__ off,
+__global__ void __launch_bounds__(kBlockThreads, 3) spmm_sell_kernel(int nslices, int n, const long long *__restrict__ off,
                                                                   const int *__restrict__ width,
                                                                   const unsigned *__restrict__ mask,
                                                                   const VT *__restrict__ sval,

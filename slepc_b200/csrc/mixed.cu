@@ -33,6 +33,7 @@
 //  residual is below tol.  A block method also finds every copy of a repeated eigenvalue in the block's reach,
 //  which a single-vector Krylov run finds only through rounding.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <initializer_list>
@@ -111,6 +112,13 @@ struct Block {
   // timing mode: device time and algorithmic bytes of the filters' block SpMVs
   cudaEvent_t f0 = nullptr, f1 = nullptr;
   double filter_ms = 0.0, filter_bytes = 0.0;
+  // orthonormalisations and Rayleigh-Ritz steps: counts, and in timing mode their host wall time
+  // (the stream is idle when they start: a timed filter ends with a synchronisation)
+  int64_t svqb_count = 0, rr_count = 0;
+  double svqb_ms = 0.0, rr_ms = 0.0;
+  double wall_ms(std::chrono::steady_clock::time_point t0) const {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
 
   void *buf(int i) const { return x32 ? (void *)b32[i] : (void *)b64[i]; }
   int free_buf(std::initializer_list<int> used) const {
@@ -134,6 +142,17 @@ struct Block {
   // SVQB of the current block: G = X^T X (tensor cores in FP32, FP64 otherwise), G = V D V^T,
   // X <- X V D^{-1/2} (directions below 1e-12 of the largest are floored, not dropped).
   b200_status svqb() {
+    const auto t0 = std::chrono::steady_clock::now();
+    ++svqb_count;
+    b200_status st = svqb_inner();
+    if (eps->timing && st == B200_OK) {
+      if (cudaStreamSynchronize(s) != cudaSuccess) return B200_ERR_CUDA;
+      svqb_ms += wall_ms(t0);
+    }
+    return st;
+  }
+
+  b200_status svqb_inner() {
     if (x32 && !eps->mixed_fp64_gram) {
       CUtensorMap tm;
       B200_CUDA_CHECK(rb_make_tmap_f32(&tm, b32[x], n, bp));
@@ -195,6 +214,14 @@ struct Block {
   }
 
   b200_status rayleigh_ritz() {
+    const auto t0 = std::chrono::steady_clock::now();
+    ++rr_count;
+    b200_status st = rayleigh_ritz_inner();
+    if (eps->timing && st == B200_OK) rr_ms += wall_ms(t0);  // ends with a synchronisation
+    return st;
+  }
+
+  b200_status rayleigh_ritz_inner() {
     const int wb = free_buf({x});
     B200_CUDA_CHECK(spmm(buf(x), nullptr, buf(wb), 1.0, 0.0, 0.0));
     B200_CUDA_CHECK(rb_gram2_f64_launch(buf(x), buf(wb), x32, n, bp, GH, work, s));
@@ -527,6 +554,10 @@ b200_status b200::mixed_solve(b200_eps eps) {
   eps->stats.kernel_launches = (int64_t)(launch_count() - launches0);
   eps->stats.ms_spmv = B.filter_ms;                // timing mode: the filters' block SpMVs
   eps->stats.gs_bytes = (int64_t)B.filter_bytes;   // and their algorithmic bytes
+  eps->stats.gs_passes = B.svqb_count;             // block orthonormalisations (SVQB)
+  eps->stats.ms_orth = B.svqb_ms;                  // timing mode: their wall time
+  eps->stats.restarts = B.rr_count;                // Rayleigh-Ritz steps
+  eps->stats.ms_restart = B.rr_ms;                 // timing mode: their wall time
   if (B.f0) cudaEventDestroy(B.f0);
   if (B.f1) cudaEventDestroy(B.f1);
   eps->solved = true;

@@ -927,7 +927,8 @@ def run_b200_learned(args):
     captured = [LN.captured(r["X"], b.T.astype(np.float64)) for r, b in zip(res_r, preds)]
     its_l = [r["its"] for r in res_l]
     its_r = [r["its"] for r in res_r]
-    ok = all(r["nconv"] >= nev and r["max_error"] <= 1e-8 for r in res_l + res_r)
+    good = lambda rs: all(r["nconv"] >= nev and r["max_error"] <= 1e-8 for r in rs)
+    ok = good(res_l + res_r)
     probs = timed[0][1]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -972,7 +973,9 @@ def run_b200_learned(args):
                                       "reason_random": [r["reason"] for r in res_r],
                                       "held_out_seeds": seeds,
                                       "mean_captured_subspace": float(np.mean(captured)),
-                                      "all_pairs_converged_to_1e-8": ok},
+                                      "all_pairs_converged_to_1e-8": ok,
+                                      "learned_all_pairs_le_1e-8": good(res_l),
+                                      "random_all_pairs_le_1e-8": good(res_r)},
                 "roofline": None,
                 "e2e": {"value": e2e_s / n, "unit": "s", "h2d_bytes_per_step": int(n * 3 * N * N * 4),
                         "d2h_bytes_per_step": int(n * nev * N * N * 12), "steps": ne2e},

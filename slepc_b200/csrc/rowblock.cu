@@ -411,6 +411,88 @@ __global__ void __launch_bounds__(256) rb_gram2_kernel(const TX *__restrict__ X,
     }
 }
 
+// ---------------------------------------------------------------- FP64 Gram pair on the FP64 MMA path
+//
+// The same G = X^T X and H = X^T W (64-column row-major blocks, products and sums in FP64) with
+// mma.sync.m16n8k16 f64: per 32-row chunk the CTA converts X and W to FP64 in shared memory (row
+// stride 68 doubles, 4 mod 16: every fragment load of a half warp hits distinct banks); warp w
+// accumulates the 16 x 64 strip 16 (w % 4).. of G (w < 4) or of H (w >= 4) over its CTA's rows,
+// the next chunk fetched into registers while the current one is consumed.  Fragments (g = lane / 4,
+// t = lane % 4): A = X^T, element e at row g + 8 (e % 2), depth t + 4 (e / 2); B element e at depth
+// t + 4 e, column g; D element e at row g + 8 (e / 2), column 2 t + e % 2.  The CTA's partial sums
+// go to partials[cta][G then H] as rb_gram2_kernel writes them.
+constexpr int kMmaRows = 32;   // rows per shared chunk (two 16-deep MMA steps)
+constexpr int kMmaLd = 68;     // doubles per chunk row in shared memory
+__device__ __forceinline__ void dmma16816(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+        "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
+template <typename TX>
+__global__ void __launch_bounds__(256) rb_gram2_mma_kernel(const TX *__restrict__ X, const TX *__restrict__ W, int n,
+                                                           int rows_per_cta, double *__restrict__ partials) {
+  constexpr int BP = 64;
+  __shared__ double xs[kMmaRows * kMmaLd], ws[kMmaRows * kMmaLd];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int mb = warp & 3;          // 16-row strip of the output
+  const bool hw = warp >= 4;        // H = X^T W (else G = X^T X)
+  const double *bsrc = hw ? ws : xs;
+  double acc[8][4];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
+  const int r0 = blockIdx.x * rows_per_cta, r1 = min(n, r0 + rows_per_cta);
+  // a chunk: kMmaRows x 64 values of X and of W, 8 of each per thread (two 16-byte vectors of FP32,
+  // or four of FP64)
+  constexpr int kPer = kMmaRows * BP / 256;
+  TX px[kPer], pw[kPer];
+  auto fetch = [&](int c0) {
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int e = threadIdx.x * kPer + u, rr = e / BP, c = e % BP, r = c0 + rr;
+      const bool in = r < r1;
+      px[u] = in ? X[(size_t)r * BP + c] : TX(0);
+      pw[u] = in ? W[(size_t)r * BP + c] : TX(0);
+    }
+  };
+  if (r0 < r1) fetch(r0);
+  for (int c0 = r0; c0 < r1; c0 += kMmaRows) {
+    __syncthreads();  // the previous chunk is consumed
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int e = threadIdx.x * kPer + u, rr = e / BP, c = e % BP;
+      xs[rr * kMmaLd + c] = (double)px[u];
+      ws[rr * kMmaLd + c] = (double)pw[u];
+    }
+    __syncthreads();
+    if (c0 + kMmaRows < r1) fetch(c0 + kMmaRows);
+#pragma unroll
+    for (int k0 = 0; k0 < kMmaRows; k0 += 16) {
+      double a[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) a[e] = xs[(k0 + t + 4 * (e >> 1)) * kMmaLd + 16 * mb + g + 8 * (e & 1)];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        double b[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) b[e] = bsrc[(k0 + t + 4 * e) * kMmaLd + 8 * j + g];
+        dmma16816(acc[j], a, b);
+      }
+    }
+  }
+  double *out = partials + (size_t)blockIdx.x * 2 * BP * BP + (hw ? (size_t)BP * BP : 0);
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int row = 16 * mb + g + 8 * (e >> 1), col = 8 * j + 2 * t + (e & 1);
+      out[(size_t)row * BP + col] = acc[j][e];
+    }
+}
+
 // ---------------------------------------------------------------- rotation Y = X M
 //
 // 256 threads; a tile of RT = 16 TR rows of X in shared memory (row stride BP + 1), M (converted to
@@ -637,6 +719,18 @@ cudaError_t gram_tc_t(const CUtensorMap &tx, const CUtensorMap &ty, int n, doubl
 template <typename TX, int BP>
 cudaError_t gram2_t(const TX *X, const TX *W, int n, double *GH, double *work, cudaStream_t s) {
   const int ctas = rb_gram_ctas(n, BP);
+  if constexpr (BP == 64) {  // the FP64 MMA path
+    int rows = (n + ctas - 1) / ctas;
+    rows = (rows + kMmaRows - 1) / kMmaRows * kMmaRows;
+    const int gx = (n + rows - 1) / rows;
+    rb_gram2_mma_kernel<TX><<<gx > 0 ? gx : 1, 256, 0, s>>>(X, W, n, rows, work);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    rb_reduce_kernel<double><<<(2 * BP * BP + 255) / 256, 256, 0, s>>>(work, gx > 0 ? gx : 1, 2 * BP * BP, GH);
+    count_launch();
+    return cudaGetLastError();
+  }
   int rows = (n + ctas - 1) / ctas;
   rows = (rows + kSlab - 1) / kSlab * kSlab;
   const int gx = (n + rows - 1) / rows;

@@ -3,7 +3,7 @@
 The tensor-core Gram product (tcgen05 kind::tf32) reads its FP32 inputs with 10
 mantissa bits, so it is checked elementwise against the FP64 product within a
 TF32 bound, 1.25 * 2^-9 * (|X|^T |Y|) (each input rounded by less than 2^-10
-relative, plus FP32 accumulation); the FP64 Gram is checked to 1e-12.  Sizes
+relative, plus FP32 accumulation); the FP64 Gram (FP64 MMAs for 64 columns) is checked to 1e-12.  Sizes
 include a partial last tile (n not a multiple of the tile height), a block
 narrower than one tile, both block widths (64, 128), X^T X and X^T Y.
 """
@@ -54,7 +54,7 @@ def test_tensor_core_gram_within_tf32_bound(n, bp, cross):
         assert np.abs(G / s - ref).max() <= 1e-4 * np.abs(ref).max()
 
 
-@pytest.mark.parametrize("n,bp", [(10007, 64), (5003, 128)])
+@pytest.mark.parametrize("n,bp", [(10007, 64), (5003, 128), (262147, 64), (31, 64)])
 def test_fp64_gram_exact_products(n, bp):
     X, Y = _blocks(n, bp, 7)
     ref = X.astype(np.float64).T @ Y.astype(np.float64)
@@ -63,8 +63,9 @@ def test_fp64_gram_exact_products(n, bp):
 
 
 def test_gram_deterministic():
-    X, _ = _blocks(77777, 64, 3)
+    X, Y = _blocks(77777, 64, 3)
     assert np.array_equal(_gram(X, None, True), _gram(X, None, True))
+    assert np.array_equal(_gram(X, Y, False), _gram(X, Y, False))
 
 
 def test_gram_rejects_bad_width():

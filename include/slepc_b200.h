@@ -377,8 +377,8 @@ b200_status b200_tc_sgemm_async(int batch, int m, int n, int k, float alpha, con
  * block columns beyond nev (default max(8, nev/2); the block is 64 columns
  * when nev + guard <= 64, else 128, at most 128); max_sweeps, per phase
  * (default 60); fp64_gram: 1 forms the FP32 phase's orthonormalisation Gram
- * matrix in FP64 on the CUDA cores instead of on the tensor cores (0,
- * default). */
+ * matrix in FP64 (FP64 MMAs) instead of in TF32 on the tcgen05 tensor cores
+ * (0, default). */
 b200_status b200_eps_set_mixed_options(b200_eps eps, double tol_low, int degree, int guard, int max_sweeps,
                                        int fp64_gram);
 

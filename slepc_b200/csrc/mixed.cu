@@ -48,6 +48,9 @@
 extern "C" void scipy_dsyevd_(const char *jobz, const char *uplo, const int *n, double *a, const int *lda, double *w,
                               double *work, const int *lwork, int *iwork, const int *liwork, int *info, size_t,
                               size_t);
+extern "C" void scipy_dpotrf_(const char *uplo, const int *n, double *a, const int *lda, int *info, size_t);
+extern "C" void scipy_dtrtri_(const char *uplo, const char *diag, const int *n, double *a, const int *lda, int *info,
+                              size_t, size_t);
 extern "C" void scipy_dsygvd_(const int *, const char *, const char *, const int *, double *, const int *, double *,
                               const int *, double *, double *, const int *, int *, const int *, int *, size_t,
                               size_t);
@@ -114,7 +117,7 @@ struct Block {
   double filter_ms = 0.0, filter_bytes = 0.0;
   // orthonormalisations and Rayleigh-Ritz steps: counts, and in timing mode their host wall time
   // (the stream is idle when they start: a timed filter ends with a synchronisation)
-  int64_t svqb_count = 0, rr_count = 0;
+  int64_t svqb_count = 0, rr_count = 0, cholqr_count = 0;
   double svqb_ms = 0.0, rr_ms = 0.0;
   double wall_ms(std::chrono::steady_clock::time_point t0) const {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -139,7 +142,8 @@ struct Block {
     return rb_spmm_launch(P->sell, n, P->rowptr, P->colind, cv, sv, vf32, x32, bp, Xin, Zin, Y, alpha, shift, beta, s);
   }
 
-  // SVQB of the current block: G = X^T X (tensor cores in FP32, FP64 otherwise), G = V D V^T,
+  // Orthonormalisation of the current block: G = X^T X (tensor cores in FP32, FP64 otherwise),
+  // scaled to unit diagonal; Cholesky QR when G factors with margin, else SVQB: G = V D V^T,
   // X <- X V D^{-1/2} (directions below 1e-12 of the largest are floored, not dropped).
   b200_status svqb() {
     const auto t0 = std::chrono::steady_clock::now();
@@ -178,6 +182,32 @@ struct Block {
     }
     for (int i = 0; i < bp; ++i)
       for (int j = 0; j < bp; ++j) G[(size_t)i * bp + j] *= dsc[i] * dsc[j];
+    // Cholesky QR when the scaled Gram matrix factors with margin (every pivot above 1e-4, i.e. a
+    // condition number below about 1e4, which the filter segments keep): X <- X D R^{-1} with
+    // D R^{-1} upper triangular -- a different orthonormal basis of the same span as SVQB's, for a
+    // 64 x 64 Cholesky and triangular inverse on the host instead of an eigendecomposition.
+    {
+      std::vector<double> R(G);
+      int info = 0;
+      scipy_dpotrf_("U", &bp, R.data(), &bp, &info, 1);
+      bool ok = info == 0;
+      for (int j = 0; ok && j < bp; ++j) ok = R[(size_t)j * bp + j] * R[(size_t)j * bp + j] > 1e-4;
+      if (ok) {
+        scipy_dtrtri_("U", "N", &bp, R.data(), &bp, &info, 1, 1);
+        ok = info == 0;
+      }
+      if (ok) {
+        ++cholqr_count;
+        // M[k][c] = dsc[k] Rinv(k, c); Rinv column-major and upper triangular
+        for (int k = 0; k < bp; ++k)
+          for (int c = 0; c < bp; ++c) Q[(size_t)k * bp + c] = k <= c ? dsc[k] * R[(size_t)c * bp + k] : 0.0;
+        B200_CUDA_CHECK(cudaMemcpyAsync(M, Q.data(), sizeof(double) * bp * bp, cudaMemcpyHostToDevice, s));
+        const int y = free_buf({x});
+        B200_CUDA_CHECK(rb_rotate_launch(buf(x), buf(y), x32, n, bp, M, s));
+        x = y;
+        return B200_OK;
+      }
+    }
     std::vector<double> w(bp);
     B200_CHECK(syevd(G.data(), w.data()));
     const double wmax = w[bp - 1] > 0.0 ? w[bp - 1] : 1.0;

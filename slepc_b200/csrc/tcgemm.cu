@@ -3,16 +3,19 @@
 //   C[z] = alpha * A[z] B[z] + beta * C[z],  A: m x k, B: k x n, C: m x n, element (i, j) of matrix z of
 //   a view at p + z * bs + i * rs + j * cs (any strides: the transposed views of the backward pass too).
 //
-// The larger output dimension goes on the 128-row MMA side (C or C^T is computed).  A CTA of 128
-// threads owns a 128 x NT output tile (NT = 16..64).  For each 32-deep K chunk the threads stage the
-// A and B tiles into shared memory in the K-major, non-swizzled core-matrix layout (8 rows x 16 bytes
-// per core matrix; LBO = 128 bytes between core matrices along K, SBO = 1024 bytes between 8-row
-// groups), each value split into a TF32 high part (round to nearest) and the FP32 remainder; one
-// thread issues, per 8-deep K step, three tcgen05.mma kind::tf32 products hi*hi + hi*lo + lo*hi into
-// the FP32 accumulator in TMEM (the split keeps about 21 bits of every product: FP32-level results
-// from TF32 tensor cores, the three-product TF32 emulation of FP32 GEMM); the MMAs' commit releases
-// the shared memory for the next chunk.  The four warps then read the accumulator (warp w owns TMEM
-// lanes 32w..32w+31 = rows) and apply alpha and beta.  Every wait is bounded.
+// The larger output dimension goes on the MMA's row side (C or C^T is computed).  A CTA of 128
+// threads owns a TM x NT output tile (TM = 128, or 64 when the output has at most 64 rows; NT = 16,
+// 32 or 64).  For each 32-deep K chunk the threads stage the A and B tiles into shared memory in the
+// K-major, non-swizzled core-matrix layout (8 rows x 16 bytes per core matrix; LBO = 128 bytes
+// between core matrices along K, SBO = 1024 bytes between 8-row groups; each warp store fills one
+// whole core matrix, so the stores are free of bank conflicts), each value split into a TF32 high
+// part (round to nearest) and the FP32 remainder; one thread issues, per 8-deep K step, three
+// tcgen05.mma kind::tf32 products hi*hi + hi*lo + lo*hi into the FP32 accumulator in TMEM (the split
+// keeps about 21 bits of every product: FP32-level results from TF32 tensor cores, the
+// three-product TF32 emulation of FP32 GEMM).  Two shared stages: the next chunk is loaded into
+// registers while the MMAs of the current one run, and split into the other stage once the MMAs
+// two chunks back have committed.  The four warps then read the accumulator (tcgen05.ld) and apply
+// alpha and beta.  Every wait is bounded.
 //
 // When the tiles leave SMs idle and the depth is long (the weight gradients: 32 x 32 outputs over
 // 262,144 grid points), the depth is split across CTAs into a workspace of partial tiles, and a

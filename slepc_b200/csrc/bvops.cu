@@ -457,83 +457,92 @@ __global__ void __launch_bounds__(256) gram_partial_kernel(const double *__restr
     }
 }
 
-// Both Gram blocks of a Rayleigh-Ritz step from one pass over two T-column blocks (T = 16 TM, one
-// tile): M1 = Y^T X and M2 = Y^T Y, staged and summed exactly as gram_partial_kernel does each of
-// them (same panels, same row order per pair), so each has the bits of its own gram_partial_kernel
-// call.  partial[blk * 2 (nx ny) + ...] holds M1 in pair columns 0..nx-1 and M2 in nx..2nx-1.
-template <int TM>
-__global__ void __launch_bounds__(256) gram_dual_kernel(const double *__restrict__ X, int ldx,
-                                                        const double *__restrict__ Y, int ldy, int nc, int n,
-                                                        double *partial) {
-  constexpr int T = 16 * TM;
-  constexpr int kLoads = kGramRows * T / 256;
-  __shared__ double Xs[kGramRows][T + 1], Ys[kGramRows][T + 1];
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const long long rows_per = (n + gridDim.x - 1) / gridDim.x;
+// The Gram pair on the FP64 MMA path (mma.sync.m16n8k16.f64), nc <= 64 columns: per 32-row chunk
+// the CTA stages the columns of X and Y in shared memory (column stride 36 doubles, 4 mod 16: the
+// fragment loads of a half warp hit distinct banks), the next chunk fetched into registers while the
+// current one is consumed; warp w < 2 NMB accumulates the 16-row strip w % NMB of M1 = Y^T X
+// (w < NMB) or of M2 = Y^T Y over its CTA's rows.  Fragments (g = lane / 4, t = lane % 4): A = Y^T,
+// element e at row g + 8 (e % 2), depth t + 4 (e / 2); B element e at depth t + 4 e, column g; D
+// element e at row g + 8 (e / 2), column 2 t + e % 2.  Partial sums partial[cta][M1 then M2], each (i + j nc).
+constexpr int kDualRows = 32;  // rows per staged chunk
+constexpr int kDualLd = 36;    // doubles per staged column
+__device__ __forceinline__ void dmma_m16n8k16(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+        "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
+template <int NMB>
+__global__ void __launch_bounds__(256) gram_dual_mma_kernel(const double *__restrict__ X, int ldx,
+                                                            const double *__restrict__ Y, int ldy, int nc, int n,
+                                                            double *partial) {
+  constexpr int NC = 16 * NMB;  // staged columns (zero past nc)
+  __shared__ double xs[NC * kDualLd], ys[NC * kDualLd];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const bool active = warp < 2 * NMB;
+  const int mb = warp % NMB;
+  const bool self = warp >= NMB;  // M2 = Y^T Y
+  const double *bs = self ? ys : xs;
+  const int nnb = (nc + 7) / 8;
+  const long long rows_per = ((long long)(n + gridDim.x - 1) / gridDim.x + kDualRows - 1) / kDualRows * kDualRows;
   const long long r0 = (long long)blockIdx.x * rows_per;
   const long long r1 = min((long long)n, r0 + rows_per);
-  double a1[TM][TM], a2[TM][TM];
+  double acc[2 * NMB][4];
 #pragma unroll
-  for (int a = 0; a < TM; ++a)
+  for (int j = 0; j < 2 * NMB; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
+  constexpr int kPer = kDualRows * NC / 256;
+  double px[kPer], py[kPer];
+  auto fetch = [&](long long p0) {
 #pragma unroll
-    for (int b = 0; b < TM; ++b) a1[a][b] = a2[a][b] = 0.0;
-  double xr[kLoads], yr[kLoads];
-  auto load = [&](long long p0, int pr) {
-#pragma unroll
-    for (int u = 0; u < kLoads; ++u) {
-      const int e = threadIdx.x + 256 * u;
-      const int r = e % kGramRows, c = e / kGramRows;
-      xr[u] = (r < pr && c < nc) ? X[(size_t)c * ldx + p0 + r] : 0.0;
-      yr[u] = (r < pr && c < nc) ? Y[(size_t)c * ldy + p0 + r] : 0.0;
+    for (int u = 0; u < kPer; ++u) {
+      const int e = threadIdx.x + 256 * u, c = e / kDualRows, r = e % kDualRows;
+      const long long row = p0 + r;
+      const bool in = row < r1 && c < nc;
+      px[u] = in ? X[(size_t)c * ldx + row] : 0.0;
+      py[u] = in ? Y[(size_t)c * ldy + row] : 0.0;
     }
   };
-  long long p0 = r0;
-  int pr = p0 < r1 ? (int)min((long long)kGramRows, r1 - p0) : 0;
-  if (pr > 0) load(p0, pr);
-  while (pr > 0) {
+  if (r0 < r1) fetch(r0);
+  for (long long p0 = r0; p0 < r1; p0 += kDualRows) {
+    __syncthreads();  // the previous chunk is consumed
 #pragma unroll
-    for (int u = 0; u < kLoads; ++u) {
-      const int e = threadIdx.x + 256 * u;
-      const int r = e % kGramRows, c = e / kGramRows;
-      Xs[r][c] = xr[u];
-      Ys[r][c] = yr[u];
+    for (int u = 0; u < kPer; ++u) {
+      const int e = threadIdx.x + 256 * u, c = e / kDualRows, r = e % kDualRows;
+      xs[c * kDualLd + r] = px[u];
+      ys[c * kDualLd + r] = py[u];
     }
     __syncthreads();
-    const long long pn = p0 + kGramRows;
-    const int prn = pn < r1 ? (int)min((long long)kGramRows, r1 - pn) : 0;
-    if (prn > 0) load(pn, prn);
-    for (int r = 0; r < pr; ++r) {
-      double yv[TM], xv[TM], zv[TM];
+    if (p0 + kDualRows < r1) fetch(p0 + kDualRows);
+    if (active) {
 #pragma unroll
-      for (int a = 0; a < TM; ++a) yv[a] = Ys[r][TM * ty + a];
+      for (int k0 = 0; k0 < kDualRows; k0 += 16) {
+        double a[8];
 #pragma unroll
-      for (int b = 0; b < TM; ++b) {
-        xv[b] = Xs[r][TM * tx + b];
-        zv[b] = Ys[r][TM * tx + b];
-      }
+        for (int e = 0; e < 8; ++e) a[e] = ys[(16 * mb + g + 8 * (e & 1)) * kDualLd + k0 + t + 4 * (e >> 1)];
 #pragma unroll
-      for (int a = 0; a < TM; ++a)
+        for (int j = 0; j < 2 * NMB; ++j) {
+          if (j < nnb) {
+            double b[4];
 #pragma unroll
-        for (int b = 0; b < TM; ++b) {
-          a1[a][b] = fma(yv[a], xv[b], a1[a][b]);
-          a2[a][b] = fma(yv[a], zv[b], a2[a][b]);
+            for (int e = 0; e < 4; ++e) b[e] = bs[(8 * j + g) * kDualLd + k0 + t + 4 * e];
+            dmma_m16n8k16(acc[j], a, b);
+          }
         }
-    }
-    __syncthreads();
-    p0 = pn;
-    pr = prn;
-  }
-  const size_t npairs = (size_t)nc * nc;
-#pragma unroll
-  for (int a = 0; a < TM; ++a)
-#pragma unroll
-    for (int b = 0; b < TM; ++b) {
-      const int i = TM * ty + a, j = TM * tx + b;
-      if (i < nc && j < nc) {
-        double *pb = partial + (size_t)blockIdx.x * 2 * npairs;
-        pb[i + (size_t)j * nc] = a1[a][b];
-        pb[npairs + i + (size_t)j * nc] = a2[a][b];
       }
+    }
+  }
+  if (!active) return;
+  const size_t npairs = (size_t)nc * nc;
+  double *pb = partial + (size_t)blockIdx.x * 2 * npairs + (self ? npairs : 0);
+#pragma unroll
+  for (int j = 0; j < 2 * NMB; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int i = 16 * mb + g + 8 * (e >> 1), col = 8 * j + 2 * t + (e & 1);
+      if (i < nc && col < nc) pb[i + (size_t)col * nc] = acc[j][e];
     }
 }
 
@@ -1086,12 +1095,12 @@ cudaError_t dot_dual_launch(const double *X, int ldx, const double *Y, int ldy, 
   int blocks = num_sms() * (ctas_per_sm > 0 ? ctas_per_sm : 1);
   if (blocks * npairs2 > work_len) blocks = work_len / npairs2;
   if (blocks < 1) return cudaErrorInvalidValue;
-  const int tm = nc > 48 ? 4 : (nc + 15) / 16;
-  switch (tm) {
-    case 1: gram_dual_kernel<1><<<blocks, 256, 0, stream>>>(X, ldx, Y, ldy, nc, n, work); break;
-    case 2: gram_dual_kernel<2><<<blocks, 256, 0, stream>>>(X, ldx, Y, ldy, nc, n, work); break;
-    case 3: gram_dual_kernel<3><<<blocks, 256, 0, stream>>>(X, ldx, Y, ldy, nc, n, work); break;
-    default: gram_dual_kernel<4><<<blocks, 256, 0, stream>>>(X, ldx, Y, ldy, nc, n, work); break;
+  const int nmb = (nc + 15) / 16;  // the FP64 MMA form (16-row strips of both Gram blocks)
+  switch (nmb) {
+    case 1: gram_dual_mma_kernel<1><<<blocks, 256, 0, stream>>>(X, ldx, Y, ldy, nc, n, work); break;
+    case 2: gram_dual_mma_kernel<2><<<blocks, 256, 0, stream>>>(X, ldx, Y, ldy, nc, n, work); break;
+    case 3: gram_dual_mma_kernel<3><<<blocks, 256, 0, stream>>>(X, ldx, Y, ldy, nc, n, work); break;
+    default: gram_dual_mma_kernel<4><<<blocks, 256, 0, stream>>>(X, ldx, Y, ldy, nc, n, work); break;
   }
   count_launch();
   dot_final_kernel<<<(npairs2 + 31) / 32, 256, 0, stream>>>(work, blocks, 2 * nc, nc, M, nc);

@@ -20,13 +20,17 @@ b200_status bv_orthogonalize_block(b200_bv bv);
 // BVOrthogonalizeVec + scale by 1/norm for several device vectors, one synchronisation.
 b200_status bv_orthonormalize_vecs(b200_bv bv, double *const *vecs, int count, int *breakdown);
 // BVDot(W, Z, MA) and BVDot(Z, Z, MB) over the same active column count, one pass over both blocks
-// and one synchronisation (the Gram pair of a Rayleigh-Ritz step; each as b200_bv_dot computes it).
+// (FP64 MMAs) and one synchronisation: the Gram pair of a Rayleigh-Ritz step.
 b200_status bv_dot_pair(b200_bv W, b200_bv Z, double *MA, double *MB, int ldm);
 // BVOrthogonalize of two independent blocks (no R) with the Cholesky or SVQB block types: both
 // Gram products read back in one synchronisation (otherwise one block after the other).
 b200_status bv_orthogonalize_pair(b200_bv a, b200_bv b);
 // Column norms of the active columns, one synchronisation.
 b200_status bv_column_norms(b200_bv bv, double *nrm);
+// Stream-ordered device allocation from the library's per-device pool (freed memory is kept for
+// reuse by the process) and its release on the same stream.
+cudaError_t pool_alloc(void **p, size_t bytes, cudaStream_t s);
+cudaError_t pool_free(void *p, cudaStream_t s);
 // Streaming multiprocessors of the current device.
 int num_sms_host();
 // EPSSolve with EPSLOBPCG (lobpcg.cu).

@@ -211,8 +211,8 @@ inline int dot_ctas_per_sm(int nx, int ny) { return (long long)nx * ny <= 64 * 6
 // ctas_per_sm (row blocks per SM of the partial sums).
 cudaError_t dot_launch(const double *X, int ldx, int nx, const double *Y, int ldy, int ny, int n, double *M, int ldm,
                        double *work, int work_len, cudaStream_t stream, int ctas_per_sm = 1);
-// M (nc x 2nc, ld nc) = [Y^T X | Y^T Y] from one pass over X and Y (nc <= 64 columns each; each
-// half has the bits of its own dot_launch); cudaErrorNotSupported outside that range.
+// M (nc x 2nc, ld nc) = [Y^T X | Y^T Y] from one pass over X and Y on the FP64 MMA path (8 <= nc <= 64
+// columns each; FP64 products and sums, in the MMA's order); cudaErrorNotSupported outside that range.
 cudaError_t dot_dual_launch(const double *X, int ldx, const double *Y, int ldy, int nc, int n, double *M, double *work,
                             int work_len, cudaStream_t stream, int ctas_per_sm);
 // R(:, j) = AX(:, j) - theta[j] X(:, j) for j < ncols <= kThetaMax (theta on the host).

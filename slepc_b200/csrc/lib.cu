@@ -50,6 +50,36 @@ extern "C" uint64_t b200_kernel_launch_count(void) { return g_launches.load(); }
 namespace b200 {
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 uint64_t launch_count() { return g_launches.load(); }
+// Stream-ordered allocations from one pool per device that keeps what is freed (release threshold
+// at the maximum) for the next allocation of the process: the mixed form's gigabyte blocks.
+static cudaMemPool_t device_pool(int dev) {
+  static cudaMemPool_t pools[64] = {};
+  if (dev < 0 || dev >= 64) return nullptr;
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = p;
+  }
+  return pools[dev];
+}
+
+cudaError_t pool_alloc(void **p, size_t bytes, cudaStream_t s) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  cudaMemPool_t pool = device_pool(dev);
+  if (!pool) return cudaErrorMemoryAllocation;
+  return cudaMallocFromPoolAsync(p, bytes, pool, s);
+}
+
+cudaError_t pool_free(void *p, cudaStream_t s) { return p ? cudaFreeAsync(p, s) : cudaSuccess; }
+
 int num_sms_host() {
   int dev = 0, v = 0;
   cudaGetDevice(&dev);
@@ -1467,9 +1497,10 @@ extern "C" b200_status b200_eps_destroy(b200_eps eps) {
   cudaFree(eps->resid_buf);
   cudaFree(eps->op_buf);
   cudaFree(eps->dinv);
-  cudaFree(eps->rb32);
-  cudaFree(eps->rb64);
-  cudaFree(eps->mred);
+  if (eps->rb32 || eps->rb64 || eps->mred) cudaStreamSynchronize(eps->stream);  // no kernel still reads them
+  if (eps->rb32) pool_free(eps->rb32, eps->stream);
+  if (eps->rb64) pool_free(eps->rb64, eps->stream);
+  if (eps->mred) pool_free(eps->mred, eps->stream);
   if (eps->monitor_jsonl) fclose(eps->monitor_jsonl);
   delete eps;
   return B200_OK;

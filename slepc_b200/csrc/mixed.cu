@@ -69,17 +69,21 @@ constexpr double kWide = 0.1;           // polish interval: pulled back by this 
 constexpr double kPolishGrowth = 300.0; // damping of the FP32 rounding noise by the polish filter
 constexpr int kBufs = 4;                // row-major blocks per precision
 
+// The blocks come from the library's stream-ordered pool (pool_alloc): a solve that follows another
+// EPS's destruction -- the one-call host API creates one per call -- reuses the same gigabytes
+// instead of mapping them again.
 template <typename T>
-b200_status ensure(T **p, size_t *cap, size_t count) {
+b200_status ensure(T **p, size_t *cap, size_t count, cudaStream_t s) {
   if (*cap >= count && *p) return B200_OK;
-  cudaFree(*p);
+  if (*p) pool_free(*p, s);
   *p = nullptr;
   *cap = 0;
-  if (cudaMalloc(p, sizeof(T) * (count ? count : 1)) != cudaSuccess) {
-    *p = nullptr;
-    b200_set_last_error(__FILE__, __LINE__, "cudaMalloc failed for the mixed-precision buffers");
+  void *q = nullptr;
+  if (pool_alloc(&q, sizeof(T) * (count ? count : 1), s) != cudaSuccess) {
+    b200_set_last_error(__FILE__, __LINE__, "device allocation failed for the mixed-precision buffers");
     return B200_ERR_NOMEM;
   }
+  *p = static_cast<T *>(q);
   *cap = count;
   return B200_OK;
 }
@@ -443,8 +447,8 @@ b200_status b200::mixed_solve(b200_eps eps) {
   B.which = which;
   B.P = &eps->A->a;
   const size_t blk = (size_t)n * bp;
-  B200_CHECK(ensure(&eps->rb32, &eps->rb32_cap, kBufs * blk));
-  B200_CHECK(ensure(&eps->rb64, &eps->rb64_cap, kBufs * blk));
+  B200_CHECK(ensure(&eps->rb32, &eps->rb32_cap, kBufs * blk, eps->stream));
+  B200_CHECK(ensure(&eps->rb64, &eps->rb64_cap, kBufs * blk, eps->stream));
   for (int i = 0; i < kBufs; ++i) {
     B.b32[i] = eps->rb32 + (size_t)i * blk;
     B.b64[i] = eps->rb64 + (size_t)i * blk;
@@ -454,7 +458,8 @@ b200_status b200::mixed_solve(b200_eps eps) {
   const size_t work_len = std::max((size_t)ctas * 2 * sq, (size_t)bp * 1024);
   // mred: G|H (2 bp^2), M (bp^2), theta, res, Gershgorin work and bounds, then the reduction work
   const int gw = 1 << 16;
-  B200_CHECK(ensure(&eps->mred, &eps->mred_cap, 3 * sq + 2 * (size_t)bp + 8 + gw + work_len + (size_t)ctas * sq / 2 + 8));
+  B200_CHECK(ensure(&eps->mred, &eps->mred_cap, 3 * sq + 2 * (size_t)bp + 8 + gw + work_len + (size_t)ctas * sq / 2 + 8,
+                    eps->stream));
   B.GH = eps->mred;
   B.M = B.GH + 2 * sq;
   B.theta_d = B.M + sq;

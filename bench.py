@@ -317,12 +317,16 @@ def run_b200(args):
     # the caller's page-locked output block, allocated once and reused by every call
     h_out = torch.empty((args.ncv + 1 if not mixed else max(args.ncv + 1, 128), n),
                         dtype=torch.float64).pin_memory().numpy()
+    form = S.EPS.Precision.MIXED if mixed else S.EPS.Precision.FP64
+    # one untimed call first, as a service would have made: the library's device pool then holds the
+    # mixed form's blocks for the timed calls (the FP64 form allocates per call either way)
+    S.solve_csr_host(h_csr, h_v0, args.nev, args.ncv, tol=1e-8, which=S.LARGEST_REAL, out=h_out, precision=form)
     barrier()
     t0 = time.perf_counter()
     e2e_last = None
     for _ in range(args.steps):
         e2e_last = S.solve_csr_host(h_csr, h_v0, args.nev, args.ncv, tol=1e-8, which=S.LARGEST_REAL, out=h_out,
-                                    precision=S.EPS.Precision.MIXED if mixed else S.EPS.Precision.FP64)
+                                    precision=form)
     e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
     h2d = csr[0].nbytes + csr[1].nbytes + csr[2].nbytes + v0.nbytes
     d2h = e2e_last["nconv"] * (n * 8 + 16)

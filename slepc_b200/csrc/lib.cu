@@ -567,6 +567,17 @@ extern "C" b200_status b200_csr_spmv(int n, const int *rowptr, const int *colind
 }
 
 // ------------------------------------------------------------------- BV ---
+// hpin is written by the host only after the host-to-device copies out of it have run: those
+// copies record hpin_ev, and a writer waits for that event instead of draining the stream.
+static cudaError_t hpin_acquire(b200_bv bv) { return bv->hpin_ev ? cudaEventSynchronize(bv->hpin_ev) : cudaSuccess; }
+static cudaError_t hpin_release(b200_bv bv) {
+  if (!bv->hpin_ev) {
+    cudaError_t e = cudaEventCreateWithFlags(&bv->hpin_ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaEventRecord(bv->hpin_ev, bv->stream);
+}
+
 static void bv_free(b200_bv bv) {
   if (!bv) return;
   cudaFree(bv->V);
@@ -580,6 +591,10 @@ static void bv_free(b200_bv bv) {
   cudaFree(bv->red);
   cudaFree(bv->scal);
   cudaFree(bv->qbuf);
+  if (bv->hpin_ev) {
+    cudaEventSynchronize(bv->hpin_ev);
+    cudaEventDestroy(bv->hpin_ev);
+  }
   cudaFreeHost(bv->hpin);
   delete bv;
 }
@@ -597,6 +612,7 @@ static b200_status bv_reserve(b200_bv bv, size_t q, size_t red) {
       b200_set_last_error(__FILE__, __LINE__, "pinned host allocation failed");
       return B200_ERR_NOMEM;
     }
+    hpin_acquire(bv);
     cudaFree(bv->qbuf);
     cudaFreeHost(bv->hpin);
     bv->qbuf = nq;
@@ -1149,8 +1165,10 @@ static b200_status bv_gram_finish(b200_bv bv, double *R, int ldr) {
     for (int j = 0; j < nc; ++j)
       for (int i = 0; i < nc; ++i) S[(size_t)j * nc + i] *= D[i] / std::sqrt(eig[j]);
   }
+  B200_CUDA_CHECK(hpin_acquire(bv));
   memcpy(bv->hpin, S.data(), sizeof(double) * nG);
   B200_CUDA_CHECK(cudaMemcpyAsync(Gdev, bv->hpin, sizeof(double) * nG, cudaMemcpyHostToDevice, s));
+  B200_CUDA_CHECK(hpin_release(bv));
   B200_CUDA_CHECK(multinplace_launch(bv->V, ld, n, l, k, Gdev, nc, l, k, s));
   if (R) {
     for (int j = 0; j < nc; ++j) {
@@ -1217,11 +1235,12 @@ extern "C" b200_status b200_bv_mult_inplace(b200_bv bv, const double *Q, int ldq
   const int kq = bv->k - bv->l, nc = e - s;
   B200_CHECK(bv_reserve(bv, (size_t)kq * nc, 0));
   // pack Q(l:k, s:e) into pinned memory, then one host-to-device copy
-  B200_CUDA_CHECK(cudaStreamSynchronize(bv->stream));
+  B200_CUDA_CHECK(hpin_acquire(bv));
   for (int j = 0; j < nc; ++j)
     memcpy(bv->hpin + (size_t)j * kq, Q + (size_t)bv->l + (size_t)(s + j) * ldq, sizeof(double) * kq);
   B200_CUDA_CHECK(
       cudaMemcpyAsync(bv->qbuf, bv->hpin, sizeof(double) * (size_t)kq * nc, cudaMemcpyHostToDevice, bv->stream));
+  B200_CUDA_CHECK(hpin_release(bv));
   return bv_multinplace_dev(bv, bv->qbuf, kq, s, e);
 }
 
@@ -1237,11 +1256,12 @@ extern "C" b200_status b200_bv_mult(b200_bv Y, double alpha, double beta, b200_b
   B200_ARG_CHECK(ldq >= X->k, "Q leading dimension too small");
   if (ny <= 0) return B200_OK;
   B200_CHECK(bv_reserve(Y, (size_t)nx * ny, 0));
-  B200_CUDA_CHECK(cudaStreamSynchronize(Y->stream));
+  B200_CUDA_CHECK(hpin_acquire(Y));
   for (int j = 0; j < ny; ++j)
     for (int i = 0; i < nx; ++i) Y->hpin[i + (size_t)j * nx] = Q[(size_t)(X->l + i) + (size_t)(Y->l + j) * ldq];
   B200_CUDA_CHECK(
       cudaMemcpyAsync(Y->qbuf, Y->hpin, sizeof(double) * (size_t)nx * ny, cudaMemcpyHostToDevice, Y->stream));
+  B200_CUDA_CHECK(hpin_release(Y));
   B200_CUDA_CHECK(mult_launch(col(Y, Y->l), Y->ld, col(X, X->l), X->ld, X->n, nx, ny, Y->qbuf, nx, alpha, beta, Y->stream));
   return B200_OK;
 }

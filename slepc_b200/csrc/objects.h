@@ -67,6 +67,7 @@ struct b200_bv_s {
   double *qbuf = nullptr;     // device staging of coefficient matrices
   size_t qbuf_len = 0;
   double *hpin = nullptr;     // pinned host staging
+  cudaEvent_t hpin_ev = nullptr;  // recorded after each host-to-device copy out of hpin
   size_t hpin_len = 0;
   uint64_t seed = 0x5eedULL, nrand = 0;
 };

@@ -445,14 +445,14 @@ __global__ void __launch_bounds__(256) rb_gram2_mma_kernel(const TX *__restrict_
 #pragma unroll
   for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
   const int r0 = blockIdx.x * rows_per_cta, r1 = min(n, r0 + rows_per_cta);
-  // a chunk: kMmaRows x 64 values of X and of W, 8 of each per thread (two 16-byte vectors of FP32,
-  // or four of FP64)
+  // a chunk: kMmaRows x 64 values of X and of W, 8 of each per thread; element e = tid + 256 u, so a
+  // warp reads 32 consecutive values of a row and writes 32 consecutive doubles (no bank conflicts)
   constexpr int kPer = kMmaRows * BP / 256;
   TX px[kPer], pw[kPer];
   auto fetch = [&](int c0) {
 #pragma unroll
     for (int u = 0; u < kPer; ++u) {
-      const int e = threadIdx.x * kPer + u, rr = e / BP, c = e % BP, r = c0 + rr;
+      const int e = threadIdx.x + 256 * u, rr = e / BP, c = e % BP, r = c0 + rr;
       const bool in = r < r1;
       px[u] = in ? X[(size_t)r * BP + c] : TX(0);
       pw[u] = in ? W[(size_t)r * BP + c] : TX(0);
@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(256) rb_gram2_mma_kernel(const TX *__restrict_
     __syncthreads();  // the previous chunk is consumed
 #pragma unroll
     for (int u = 0; u < kPer; ++u) {
-      const int e = threadIdx.x * kPer + u, rr = e / BP, c = e % BP;
+      const int e = threadIdx.x + 256 * u, rr = e / BP, c = e % BP;
       xs[rr * kMmaLd + c] = (double)px[u];
       ws[rr * kMmaLd + c] = (double)pw[u];
     }

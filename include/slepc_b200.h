@@ -349,6 +349,14 @@ b200_status b200_eps_set_precision(b200_eps eps, int precision);
  * cores.  Allocates its work arrays; synchronises the stream. */
 b200_status b200_rowblock_gram(int n, int bp, const float *X_dev, const float *Y_dev, int tensor_cores,
                                double *G_dev, void *stream);
+/* The mixed form's filter step, exposed for tests and benchmarks: on row-major
+ * device blocks of n rows and bp = 64 or 128 columns (FP32 when x32 = 1, with
+ * the operator's values in FP32; FP64 otherwise), Y = alpha (A X - shift X)
+ * - beta Z (Z nullable: no beta term) with the sliced-ELL block SpMV (products
+ * accumulated in the block's precision, the affine update in FP64).  Builds
+ * the operator's sliced-ELL and FP32 copies on first use; synchronises. */
+b200_status b200_rowblock_spmm(b200_mat A, int bp, int x32, const void *X_dev, const void *Z_dev, void *Y_dev,
+                               double alpha, double shift, double beta, void *stream);
 /* The neural operator's contraction kernel, exposed for tests and benchmarks:
  * C[z] = alpha A[z] B[z] + beta C[z] for z < batch on device FP32 views
  * (A m x k, B k x n, C m x n; element (i, j) of matrix z of a view at

@@ -91,6 +91,8 @@ _SIGS = {
     "b200_eps_solve_csr_host_ex": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, _ip, _ip, _dp, _dp, ctypes.c_int,
                                                   ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                                   ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _ip, _vp]),
+    "b200_rowblock_spmm": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_double, _vp]),
     "b200_tc_sgemm_async": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                            _vp, _ll, _ll, _ll, _vp, _ll, _ll, _ll, ctypes.c_float, _vp, _ll, _ll, _ll,
                                            ctypes.c_int, _vp, ctypes.c_size_t, _vp, _vp]),
@@ -820,6 +822,12 @@ def rowblock_gram(n, bp, X_ptr, Y_ptr=None, tensor_cores=True, G_ptr=None, strea
     """G = X^T Y (bp x bp, FP64, row-major) of row-major FP32 device blocks (b200_rowblock_gram):
     on the tensor cores (TF32 inputs, FP32 accumulation) or in FP64 on the CUDA cores."""
     _check(lib().b200_rowblock_gram(n, bp, X_ptr, Y_ptr, 1 if tensor_cores else 0, G_ptr, stream))
+
+
+def rowblock_spmm(A, bp, X_ptr, Y_ptr, Z_ptr=None, alpha=1.0, shift=0.0, beta=0.0, x32=True, stream=None):
+    """Y = alpha (A X - shift X) - beta Z on row-major device blocks (b200_rowblock_spmm); A a Mat
+    created from a square CSR."""
+    _check(lib().b200_rowblock_spmm(A.handle, bp, 1 if x32 else 0, X_ptr, Z_ptr, Y_ptr, alpha, shift, beta, stream))
 
 
 def tc_sgemm(batch, m, n, k, alpha, A, B, beta, C, split=False, sum_batch=False, stream=None):

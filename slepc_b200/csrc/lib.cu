@@ -24,6 +24,7 @@
 #include "ds_hep.h"
 #include "internal.h"
 #include "kernels.h"
+#include "rowblock.h"
 #include "objects.h"
 
 using namespace b200;
@@ -421,6 +422,23 @@ b200_status b200::mat_mixed_prepare(b200_mat A, cudaStream_t s) {
     B200_CUDA_CHECK(to_f32_launch(P.vals32, static_cast<const double *>(P.vals), P.nnz, s));
     B200_CUDA_CHECK(to_f32_launch(P.sell.vals32, static_cast<const double *>(P.sell.vals), P.sell.entries, s));
   }
+  return B200_OK;
+}
+
+extern "C" b200_status b200_rowblock_spmm(b200_mat A, int bp, int x32, const void *X, const void *Z, void *Y,
+                                          double alpha, double shift, double beta, void *stream) {
+  B200_ARG_CHECK(A && X && Y && (bp == 64 || bp == 128), "A, X, Y required; bp = 64 or 128");
+  B200_ARG_CHECK(A->kind == kMatCsr && A->m == A->n, "the block SpMV needs a square CSR operator");
+  B200_ARG_CHECK((((uintptr_t)X | (uintptr_t)Y | (uintptr_t)(Z ? Z : X)) & 15) == 0, "blocks must be 16-byte aligned");
+  cudaStream_t s = (cudaStream_t)stream;
+  B200_CHECK(mat_mixed_prepare(A, s));
+  const CsrPart &P = A->a;
+  const bool vf32 = x32 ? true : P.f32;
+  const void *sv = x32 ? (P.f32 ? P.sell.vals : (const void *)P.sell.vals32) : P.sell.vals;
+  const void *cv = x32 ? (P.f32 ? P.vals : (const void *)P.vals32) : P.vals;
+  B200_CUDA_CHECK(rb_spmm_launch(P.sell, P.rows, P.rowptr, P.colind, cv, sv, vf32, x32 != 0, bp, X, Z, Y, alpha, shift,
+                                 beta, s));
+  B200_CUDA_CHECK(cudaStreamSynchronize(s));
   return B200_OK;
 }
 

@@ -76,3 +76,46 @@ def test_gram_rejects_bad_width():
     Gd = torch.zeros((96, 96), dtype=torch.float64, device="cuda")
     with pytest.raises(S.B200Error):
         S.rowblock_gram(100, 96, Xd.data_ptr(), None, True, Gd.data_ptr())
+
+
+def _irregular_csr(n, seed):
+    # rows of 0..9 nonzeros plus a few rows longer than a 32-row slice admits (the rest path)
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(0, 10, n)
+    lens[rng.choice(n, 7, replace=False)] = rng.integers(40, 90, 7)
+    rowptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    colind = np.concatenate([np.sort(rng.choice(n, k, replace=False)) for k in lens]).astype(np.int32)
+    vals = rng.standard_normal(int(rowptr[-1]))
+    return rowptr, colind, vals
+
+
+@pytest.mark.parametrize("bp", [64, 128])
+@pytest.mark.parametrize("x32", [True, False])
+def test_block_spmv_filter_step_against_numpy(bp, x32):
+    # Y = alpha (A X - shift X) - beta Z, the Chebyshev filter step, against an FP64 reference on the
+    # same (FP32-rounded when x32) values: FP32 products within 2^-20 of |A||X|, FP64 within 1e-13
+    import scipy.sparse as sp
+    import torch
+
+    n = 5003
+    rowptr, colind, vals = _irregular_csr(n, bp + int(x32))
+    A = S.Mat().createAIJ((rowptr, colind, vals))
+    dt = np.float32 if x32 else np.float64
+    rng = np.random.default_rng(5)
+    X = rng.standard_normal((n, bp)).astype(dt)
+    Z = rng.standard_normal((n, bp)).astype(dt)
+    Xd, Zd = torch.from_numpy(X).cuda(), torch.from_numpy(Z).cuda()
+    Yd = torch.full((n, bp), np.nan, dtype=Xd.dtype, device="cuda")
+    alpha, shift, beta = 0.7, 0.3, 0.2
+    S.rowblock_spmm(A, bp, Xd.data_ptr(), Yd.data_ptr(), Zd.data_ptr(), alpha, shift, beta, x32=x32)
+    torch.cuda.synchronize()
+    Y = Yd.cpu().numpy().astype(np.float64)
+    v = vals.astype(np.float32).astype(np.float64) if x32 else vals
+    M = sp.csr_matrix((v, colind, rowptr), shape=(n, n))
+    X64, Z64 = X.astype(np.float64), Z.astype(np.float64)
+    ref = alpha * (M @ X64 - shift * X64) - beta * Z64
+    bound = alpha * (abs(M) @ np.abs(X64) + shift * np.abs(X64)) + beta * np.abs(Z64)
+    tol = 2.0 ** -20 if x32 else 1e-13
+    assert np.isfinite(Y).all()
+    assert (np.abs(Y - ref) <= tol * bound + 1e-300).all(), (np.abs(Y - ref) / np.maximum(bound, 1e-300)).max()
+    A.destroy()

@@ -31,6 +31,17 @@ b200_status bv_column_norms(b200_bv bv, double *nrm);
 // reuse by the process) and its release on the same stream.
 cudaError_t pool_alloc(void **p, size_t bytes, cudaStream_t s);
 cudaError_t pool_free(void *p, cudaStream_t s);
+// Buffers of the Mat, BV and EPS objects, from the same pool through a library stream: the
+// allocation has completed when dev_malloc returns and dev_free first waits for the device, so
+// both keep cudaMalloc/cudaFree's synchronous meaning for buffers used on any stream, while a
+// create/destroy per call (the one-call host solve) reuses memory instead of mapping and unmapping
+// it each time.
+cudaError_t dev_malloc(void **p, size_t bytes);
+void dev_free(void *p);
+template <typename T>
+inline cudaError_t dev_malloc(T **p, size_t bytes) {
+  return dev_malloc(reinterpret_cast<void **>(p), bytes);
+}
 // Streaming multiprocessors of the current device.
 int num_sms_host();
 // EPSSolve with EPSLOBPCG (lobpcg.cu).

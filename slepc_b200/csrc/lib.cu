@@ -17,6 +17,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -51,11 +52,19 @@ extern "C" uint64_t b200_kernel_launch_count(void) { return g_launches.load(); }
 namespace b200 {
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 uint64_t launch_count() { return g_launches.load(); }
-// Stream-ordered allocations from one pool per device that keeps what is freed (release threshold
-// at the maximum) for the next allocation of the process: the mixed form's gigabyte blocks.
+// Stream-ordered allocations from one pool per device that keeps up to kPoolKeep bytes of what is
+// freed for the next allocation of the process (the mixed form's gigabyte blocks, the basis and
+// matrix arrays of a repeated solve); beyond that the driver returns memory at the next
+// synchronisation.
+static constexpr uint64_t kPoolKeep = 16ull << 30;
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pools[64] = {};
+static cudaStream_t g_alloc_streams[64] = {};
+
 static cudaMemPool_t device_pool(int dev) {
-  static cudaMemPool_t pools[64] = {};
   if (dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  cudaMemPool_t *pools = g_pools;
   if (!pools[dev]) {
     cudaMemPoolProps props{};
     props.allocType = cudaMemAllocationTypePinned;
@@ -63,11 +72,24 @@ static cudaMemPool_t device_pool(int dev) {
     props.location.id = dev;
     cudaMemPool_t p = nullptr;
     if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
-    uint64_t keep = UINT64_MAX;
+    uint64_t keep = kPoolKeep;
     cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
     pools[dev] = p;
   }
   return pools[dev];
+}
+
+// The library's own non-blocking stream on device dev, on which object buffers are allocated and
+// freed (so that every reuse of a freed block by a later object is ordered on one stream).
+static cudaStream_t alloc_stream(int dev) {
+  if (dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (!g_alloc_streams[dev]) {
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+    g_alloc_streams[dev] = st;
+  }
+  return g_alloc_streams[dev];
 }
 
 cudaError_t pool_alloc(void **p, size_t bytes, cudaStream_t s) {
@@ -80,6 +102,40 @@ cudaError_t pool_alloc(void **p, size_t bytes, cudaStream_t s) {
 }
 
 cudaError_t pool_free(void *p, cudaStream_t s) { return p ? cudaFreeAsync(p, s) : cudaSuccess; }
+
+cudaError_t dev_malloc(void **p, size_t bytes) {
+  *p = nullptr;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  cudaMemPool_t pool = device_pool(dev);
+  cudaStream_t s = alloc_stream(dev);
+  if (!pool || !s) return cudaErrorMemoryAllocation;
+  e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    if (*p) cudaFreeAsync(*p, s);
+    *p = nullptr;
+    // an allocation that the kept memory blocks: hand the pool's unused memory back and retry once
+    if (e == cudaErrorMemoryAllocation) {
+      cudaGetLastError();
+      cudaStreamSynchronize(s);
+      cudaMemPoolTrimTo(pool, 0);
+      e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) *p = nullptr;
+    }
+  }
+  return e;
+}
+
+void dev_free(void *p) {
+  if (!p) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceSynchronize();
+  cudaFreeAsync(p, alloc_stream(dev));
+}
 
 int num_sms_host() {
   int dev = 0, v = 0;
@@ -97,26 +153,26 @@ int num_sms_host() {
 
 // ------------------------------------------------------------------ Mat ---
 static void part_free(CsrPart &P) {
-  cudaFree(P.rowptr);
-  cudaFree(P.colind);
-  cudaFree(P.vals);
-  cudaFree(P.blocks);
-  cudaFree(P.wt.tiles);
-  cudaFree(P.wt.segs);
-  cudaFree(P.wt.longrows);
-  cudaFree(P.wt.partials);
-  cudaFree(P.sell.off);
-  cudaFree(P.sell.width);
-  cudaFree(P.sell.mask);
-  cudaFree(P.sell.vals);
-  cudaFree(P.sell.cols);
-  cudaFree(P.sell.rest.tiles);
-  cudaFree(P.sell.rest.segs);
-  cudaFree(P.sell.rest.longrows);
-  cudaFree(P.sell.rest.partials);
-  cudaFree(P.sell.rest_rows);
-  cudaFree(P.sell.vals32);
-  cudaFree(P.vals32);
+  dev_free(P.rowptr);
+  dev_free(P.colind);
+  dev_free(P.vals);
+  dev_free(P.blocks);
+  dev_free(P.wt.tiles);
+  dev_free(P.wt.segs);
+  dev_free(P.wt.longrows);
+  dev_free(P.wt.partials);
+  dev_free(P.sell.off);
+  dev_free(P.sell.width);
+  dev_free(P.sell.mask);
+  dev_free(P.sell.vals);
+  dev_free(P.sell.cols);
+  dev_free(P.sell.rest.tiles);
+  dev_free(P.sell.rest.segs);
+  dev_free(P.sell.rest.longrows);
+  dev_free(P.sell.rest.partials);
+  dev_free(P.sell.rest_rows);
+  dev_free(P.sell.vals32);
+  dev_free(P.vals32);
   P = CsrPart{};
 }
 
@@ -127,11 +183,11 @@ static b200_status part_alloc(CsrPart &P, int rows, int cols, int64_t nnz, bool 
   P.f32 = f32;
   P.lanes = spmv_choose_lanes(rows, nnz);
   const size_t vsz = f32 ? sizeof(float) : sizeof(double);
-  if (cudaMalloc(&P.rowptr, sizeof(int) * ((size_t)rows + 1)) != cudaSuccess ||
-      cudaMalloc(&P.colind, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)) != cudaSuccess ||
-      cudaMalloc(&P.vals, vsz * (size_t)(nnz > 0 ? nnz : 1)) != cudaSuccess) {
+  if (dev_malloc(&P.rowptr, sizeof(int) * ((size_t)rows + 1)) != cudaSuccess ||
+      dev_malloc(&P.colind, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)) != cudaSuccess ||
+      dev_malloc(&P.vals, vsz * (size_t)(nnz > 0 ? nnz : 1)) != cudaSuccess) {
     part_free(P);
-    b200_set_last_error(__FILE__, __LINE__, "cudaMalloc failed for the CSR arrays");
+    b200_set_last_error(__FILE__, __LINE__, "device allocation failed for the CSR arrays");
     return B200_ERR_NOMEM;
   }
   return B200_OK;
@@ -159,7 +215,7 @@ static b200_status part_set_schedules(CsrPart &P, const int *rowptr_host, cudaSt
   if (!P.f32) {
     std::vector<int> b = spmv_row_blocks(P.rows, rowptr_host);
     P.nblocks = (int)b.size() - 1;
-    B200_CUDA_CHECK(cudaMalloc(&P.blocks, sizeof(int) * b.size()));
+    B200_CUDA_CHECK(dev_malloc(&P.blocks, sizeof(int) * b.size()));
     B200_CUDA_CHECK(cudaMemcpyAsync(P.blocks, b.data(), sizeof(int) * b.size(), cudaMemcpyHostToDevice, s));
   }
   WarpTiles wt = spmv_warp_tiles(P.rows, rowptr_host);
@@ -167,14 +223,14 @@ static b200_status part_set_schedules(CsrPart &P, const int *rowptr_host, cudaSt
   P.wt.nsegs = (int)wt.segs.size();
   P.wt.nlong = (int)wt.longrows.size();
   if (P.wt.ntiles) {
-    B200_CUDA_CHECK(cudaMalloc(&P.wt.tiles, sizeof(int4) * wt.tiles.size()));
+    B200_CUDA_CHECK(dev_malloc(&P.wt.tiles, sizeof(int4) * wt.tiles.size()));
     B200_CUDA_CHECK(
         cudaMemcpyAsync(P.wt.tiles, wt.tiles.data(), sizeof(int4) * wt.tiles.size(), cudaMemcpyHostToDevice, s));
   }
   if (P.wt.nsegs) {
-    B200_CUDA_CHECK(cudaMalloc(&P.wt.segs, sizeof(int2) * wt.segs.size()));
-    B200_CUDA_CHECK(cudaMalloc(&P.wt.partials, sizeof(double) * wt.segs.size()));
-    B200_CUDA_CHECK(cudaMalloc(&P.wt.longrows, sizeof(int3) * wt.longrows.size()));
+    B200_CUDA_CHECK(dev_malloc(&P.wt.segs, sizeof(int2) * wt.segs.size()));
+    B200_CUDA_CHECK(dev_malloc(&P.wt.partials, sizeof(double) * wt.segs.size()));
+    B200_CUDA_CHECK(dev_malloc(&P.wt.longrows, sizeof(int3) * wt.longrows.size()));
     B200_CUDA_CHECK(
         cudaMemcpyAsync(P.wt.segs, wt.segs.data(), sizeof(int2) * wt.segs.size(), cudaMemcpyHostToDevice, s));
     B200_CUDA_CHECK(cudaMemcpyAsync(P.wt.longrows, wt.longrows.data(), sizeof(int3) * wt.longrows.size(),
@@ -198,11 +254,11 @@ static b200_status part_build_sell(CsrPart &P, const int *rowptr_host, cudaStrea
   SpmvSell &S = P.sell;
   S.nslices = (int)sp.off.size();
   const size_t vsz = P.f32 ? sizeof(float) : sizeof(double);
-  B200_CUDA_CHECK(cudaMalloc(&S.off, sizeof(long long) * (S.nslices ? S.nslices : 1)));
-  B200_CUDA_CHECK(cudaMalloc(&S.width, sizeof(int) * (S.nslices ? S.nslices : 1)));
-  B200_CUDA_CHECK(cudaMalloc(&S.mask, sizeof(unsigned) * (S.nslices ? S.nslices : 1)));
-  B200_CUDA_CHECK(cudaMalloc(&S.vals, vsz * (size_t)(sp.entries ? sp.entries : 1)));
-  B200_CUDA_CHECK(cudaMalloc(&S.cols, sizeof(int) * (size_t)(sp.entries ? sp.entries : 1)));
+  B200_CUDA_CHECK(dev_malloc(&S.off, sizeof(long long) * (S.nslices ? S.nslices : 1)));
+  B200_CUDA_CHECK(dev_malloc(&S.width, sizeof(int) * (S.nslices ? S.nslices : 1)));
+  B200_CUDA_CHECK(dev_malloc(&S.mask, sizeof(unsigned) * (S.nslices ? S.nslices : 1)));
+  B200_CUDA_CHECK(dev_malloc(&S.vals, vsz * (size_t)(sp.entries ? sp.entries : 1)));
+  B200_CUDA_CHECK(dev_malloc(&S.cols, sizeof(int) * (size_t)(sp.entries ? sp.entries : 1)));
   if (S.nslices) {
     B200_CUDA_CHECK(cudaMemcpyAsync(S.off, sp.off.data(), sizeof(long long) * S.nslices, cudaMemcpyHostToDevice, s));
     B200_CUDA_CHECK(cudaMemcpyAsync(S.width, sp.width.data(), sizeof(int) * S.nslices, cudaMemcpyHostToDevice, s));
@@ -214,7 +270,7 @@ static b200_status part_build_sell(CsrPart &P, const int *rowptr_host, cudaStrea
   for (int w : sp.width) S.max_width = w > S.max_width ? w : S.max_width;
   S.nrest = (int)sp.rest_rows.size();
   if (S.nrest) {
-    B200_CUDA_CHECK(cudaMalloc(&S.rest_rows, sizeof(int) * sp.rest_rows.size()));
+    B200_CUDA_CHECK(dev_malloc(&S.rest_rows, sizeof(int) * sp.rest_rows.size()));
     B200_CUDA_CHECK(cudaMemcpyAsync(S.rest_rows, sp.rest_rows.data(), sizeof(int) * sp.rest_rows.size(),
                                     cudaMemcpyHostToDevice, s));
   }
@@ -223,14 +279,14 @@ static b200_status part_build_sell(CsrPart &P, const int *rowptr_host, cudaStrea
   S.rest.nsegs = (int)wt.segs.size();
   S.rest.nlong = (int)wt.longrows.size();
   if (S.rest.ntiles) {
-    B200_CUDA_CHECK(cudaMalloc(&S.rest.tiles, sizeof(int4) * wt.tiles.size()));
+    B200_CUDA_CHECK(dev_malloc(&S.rest.tiles, sizeof(int4) * wt.tiles.size()));
     B200_CUDA_CHECK(
         cudaMemcpyAsync(S.rest.tiles, wt.tiles.data(), sizeof(int4) * wt.tiles.size(), cudaMemcpyHostToDevice, s));
   }
   if (S.rest.nsegs) {
-    B200_CUDA_CHECK(cudaMalloc(&S.rest.segs, sizeof(int2) * wt.segs.size()));
-    B200_CUDA_CHECK(cudaMalloc(&S.rest.partials, sizeof(double) * wt.segs.size()));
-    B200_CUDA_CHECK(cudaMalloc(&S.rest.longrows, sizeof(int3) * wt.longrows.size()));
+    B200_CUDA_CHECK(dev_malloc(&S.rest.segs, sizeof(int2) * wt.segs.size()));
+    B200_CUDA_CHECK(dev_malloc(&S.rest.partials, sizeof(double) * wt.segs.size()));
+    B200_CUDA_CHECK(dev_malloc(&S.rest.longrows, sizeof(int3) * wt.longrows.size()));
     B200_CUDA_CHECK(
         cudaMemcpyAsync(S.rest.segs, wt.segs.data(), sizeof(int2) * wt.segs.size(), cudaMemcpyHostToDevice, s));
     B200_CUDA_CHECK(cudaMemcpyAsync(S.rest.longrows, wt.longrows.data(), sizeof(int3) * wt.longrows.size(),
@@ -393,9 +449,9 @@ b200_status mat_create_cross_ex(b200_mat A, bool swapped, b200_mat *C) {
   M->base = A;
   M->stream = A->stream;
   const int wlen = swapped ? A->n : A->m;
-  if (cudaMalloc(&M->work, sizeof(double) * (size_t)wlen) != cudaSuccess) {
+  if (dev_malloc(&M->work, sizeof(double) * (size_t)wlen) != cudaSuccess) {
     delete M;
-    b200_set_last_error(__FILE__, __LINE__, "cudaMalloc failed for the cross-product work vector");
+    b200_set_last_error(__FILE__, __LINE__, "device allocation failed for the cross-product work vector");
     return B200_ERR_NOMEM;
   }
   *C = M;
@@ -417,8 +473,8 @@ b200_status b200::mat_mixed_prepare(b200_mat A, cudaStream_t s) {
   CsrPart &P = A->a;
   B200_CHECK(part_build_sell(P, nullptr, s));
   if (!P.f32 && !P.vals32) {
-    B200_CUDA_CHECK(cudaMalloc(&P.vals32, sizeof(float) * (size_t)(P.nnz > 0 ? P.nnz : 1)));
-    B200_CUDA_CHECK(cudaMalloc(&P.sell.vals32, sizeof(float) * (size_t)(P.sell.entries > 0 ? P.sell.entries : 1)));
+    B200_CUDA_CHECK(dev_malloc(&P.vals32, sizeof(float) * (size_t)(P.nnz > 0 ? P.nnz : 1)));
+    B200_CUDA_CHECK(dev_malloc(&P.sell.vals32, sizeof(float) * (size_t)(P.sell.entries > 0 ? P.sell.entries : 1)));
     B200_CUDA_CHECK(to_f32_launch(P.vals32, static_cast<const double *>(P.vals), P.nnz, s));
     B200_CUDA_CHECK(to_f32_launch(P.sell.vals32, static_cast<const double *>(P.sell.vals), P.sell.entries, s));
   }
@@ -570,7 +626,7 @@ extern "C" b200_status b200_mat_destroy(b200_mat A) {
   if (!A) return B200_OK;
   part_free(A->a);
   part_free(A->at);
-  cudaFree(A->work);
+  dev_free(A->work);
   delete A;
   return B200_OK;
 }
@@ -598,17 +654,17 @@ static cudaError_t hpin_release(b200_bv bv) {
 
 static void bv_free(b200_bv bv) {
   if (!bv) return;
-  cudaFree(bv->V);
-  cudaFree(bv->gs.st);
-  cudaFree(bv->gs.coef);
-  cudaFree(bv->gs.cnew);
-  cudaFree(bv->gs.partials);
-  cudaFree(bv->coefbuf);
-  cudaFree(bv->hvec);
-  cudaFree(bv->T);
-  cudaFree(bv->red);
-  cudaFree(bv->scal);
-  cudaFree(bv->qbuf);
+  dev_free(bv->V);
+  dev_free(bv->gs.st);
+  dev_free(bv->gs.coef);
+  dev_free(bv->gs.cnew);
+  dev_free(bv->gs.partials);
+  dev_free(bv->coefbuf);
+  dev_free(bv->hvec);
+  dev_free(bv->T);
+  dev_free(bv->red);
+  dev_free(bv->scal);
+  dev_free(bv->qbuf);
   if (bv->hpin_ev) {
     cudaEventSynchronize(bv->hpin_ev);
     cudaEventDestroy(bv->hpin_ev);
@@ -624,14 +680,14 @@ static b200_status bv_reserve(b200_bv bv, size_t q, size_t red) {
   if (q > bv->qbuf_len || q + 64 > bv->hpin_len) {
     B200_CUDA_CHECK(cudaStreamSynchronize(bv->stream));
     double *nq = nullptr, *nh = nullptr;
-    B200_CUDA_CHECK(cudaMalloc(&nq, sizeof(double) * q));
+    B200_CUDA_CHECK(dev_malloc(&nq, sizeof(double) * q));
     if (cudaMallocHost(&nh, sizeof(double) * (q + 64)) != cudaSuccess) {
-      cudaFree(nq);
+      dev_free(nq);
       b200_set_last_error(__FILE__, __LINE__, "pinned host allocation failed");
       return B200_ERR_NOMEM;
     }
     hpin_acquire(bv);
-    cudaFree(bv->qbuf);
+    dev_free(bv->qbuf);
     cudaFreeHost(bv->hpin);
     bv->qbuf = nq;
     bv->hpin = nh;
@@ -641,8 +697,8 @@ static b200_status bv_reserve(b200_bv bv, size_t q, size_t red) {
   if (red > (size_t)bv->red_len) {
     B200_CUDA_CHECK(cudaStreamSynchronize(bv->stream));
     double *nr = nullptr;
-    B200_CUDA_CHECK(cudaMalloc(&nr, sizeof(double) * red));
-    cudaFree(bv->red);
+    B200_CUDA_CHECK(dev_malloc(&nr, sizeof(double) * red));
+    dev_free(bv->red);
     bv->red = nr;
     bv->red_len = (int)red;
   }
@@ -669,17 +725,17 @@ extern "C" b200_status b200_bv_create(int n, int m, void *stream, b200_bv *out) 
   bool ok = true;
   // one spare chunk of rows past the last column: the bulk copies of a ragged
   // final chunk round up to 16 bytes
-  ok = ok && cudaMalloc(&bv->V, sizeof(double) * ((size_t)bv->ld * (m + 1) + 32)) == cudaSuccess;
-  ok = ok && cudaMalloc(&bv->gs.st, sizeof(GsState)) == cudaSuccess;
-  ok = ok && cudaMalloc(&bv->gs.coef, sizeof(double) * kMaxCols) == cudaSuccess;
-  ok = ok && cudaMalloc(&bv->gs.cnew, sizeof(double) * (kMaxCols + 1)) == cudaSuccess;
-  ok = ok && cudaMalloc(&bv->gs.partials, sizeof(double) * (size_t)(kMaxCols + 1) * 2 * sms) == cudaSuccess;
-  ok = ok && cudaMalloc(&bv->coefbuf, sizeof(double) * (size_t)bv->ldc * (m + 1)) == cudaSuccess;
-  ok = ok && cudaMalloc(&bv->hvec, sizeof(double) * (kMaxCols + 1)) == cudaSuccess;
-  ok = ok && cudaMalloc(&bv->T, sizeof(double) * 2 * (size_t)bv->ldt) == cudaSuccess;
-  ok = ok && cudaMalloc(&bv->red, sizeof(double) * (size_t)bv->red_len) == cudaSuccess;
-  ok = ok && cudaMalloc(&bv->scal, sizeof(double) * 16) == cudaSuccess;
-  ok = ok && cudaMalloc(&bv->qbuf, sizeof(double) * bv->qbuf_len) == cudaSuccess;
+  ok = ok && dev_malloc(&bv->V, sizeof(double) * ((size_t)bv->ld * (m + 1) + 32)) == cudaSuccess;
+  ok = ok && dev_malloc(&bv->gs.st, sizeof(GsState)) == cudaSuccess;
+  ok = ok && dev_malloc(&bv->gs.coef, sizeof(double) * kMaxCols) == cudaSuccess;
+  ok = ok && dev_malloc(&bv->gs.cnew, sizeof(double) * (kMaxCols + 1)) == cudaSuccess;
+  ok = ok && dev_malloc(&bv->gs.partials, sizeof(double) * (size_t)(kMaxCols + 1) * 2 * sms) == cudaSuccess;
+  ok = ok && dev_malloc(&bv->coefbuf, sizeof(double) * (size_t)bv->ldc * (m + 1)) == cudaSuccess;
+  ok = ok && dev_malloc(&bv->hvec, sizeof(double) * (kMaxCols + 1)) == cudaSuccess;
+  ok = ok && dev_malloc(&bv->T, sizeof(double) * 2 * (size_t)bv->ldt) == cudaSuccess;
+  ok = ok && dev_malloc(&bv->red, sizeof(double) * (size_t)bv->red_len) == cudaSuccess;
+  ok = ok && dev_malloc(&bv->scal, sizeof(double) * 16) == cudaSuccess;
+  ok = ok && dev_malloc(&bv->qbuf, sizeof(double) * bv->qbuf_len) == cudaSuccess;
   ok = ok && cudaMallocHost(&bv->hpin, sizeof(double) * bv->hpin_len) == cudaSuccess;
   if (!ok) {
     bv_free(bv);
@@ -1532,9 +1588,9 @@ extern "C" b200_status b200_eps_create(void *stream, b200_eps *eps) {
 extern "C" b200_status b200_eps_destroy(b200_eps eps) {
   if (!eps) return B200_OK;
   b200_bv_destroy(eps->V);
-  cudaFree(eps->resid_buf);
-  cudaFree(eps->op_buf);
-  cudaFree(eps->dinv);
+  dev_free(eps->resid_buf);
+  dev_free(eps->op_buf);
+  dev_free(eps->dinv);
   if (eps->rb32 || eps->rb64 || eps->mred) cudaStreamSynchronize(eps->stream);  // no kernel still reads them
   if (eps->rb32) pool_free(eps->rb32, eps->stream);
   if (eps->rb64) pool_free(eps->rb64, eps->stream);
@@ -1547,7 +1603,7 @@ extern "C" b200_status b200_eps_destroy(b200_eps eps) {
 extern "C" b200_status b200_eps_set_operators(b200_eps eps, b200_mat A) {
   B200_ARG_CHECK(eps && A, "null argument");
   B200_ARG_CHECK(A->m == A->n, "the operator of an eigenproblem must be square");
-  cudaFree(eps->op_buf);
+  dev_free(eps->op_buf);
   eps->op_buf = nullptr;
   eps->A = A;
   eps->solved = false;
@@ -1829,7 +1885,7 @@ static b200_status eps_setup(b200_eps eps) {
   eps->errest.assign(ncv + 1, 0.0);
   eps->perm.assign(ncv + 1, 0);
   for (int i = 0; i <= ncv; ++i) eps->perm[i] = i;
-  if (!eps->resid_buf) B200_CUDA_CHECK(cudaMalloc(&eps->resid_buf, sizeof(double) * 8));
+  if (!eps->resid_buf) B200_CUDA_CHECK(dev_malloc(&eps->resid_buf, sizeof(double) * 8));
   return B200_OK;
 }
 
@@ -2060,7 +2116,7 @@ extern "C" b200_status b200_eps_compute_error(b200_eps eps, int i, int type, dou
     B200_CUDA_CHECK(residual_launch(A->n, A->a.rowptr, A->a.colind, static_cast<const double *>(A->a.vals), col(V, p),
                                     shift, eps->resid_buf, V->red, V->red_len, A->a.lanes, V->stream));
   } else {
-    if (!eps->op_buf) B200_CUDA_CHECK(cudaMalloc(&eps->op_buf, sizeof(double) * (size_t)A->n));
+    if (!eps->op_buf) B200_CUDA_CHECK(dev_malloc(&eps->op_buf, sizeof(double) * (size_t)A->n));
     B200_CUDA_CHECK(mat_spmv(A, col(V, p), eps->op_buf, V->stream));
     B200_CUDA_CHECK(diff_sumsq_launch(eps->op_buf, col(V, p), shift, A->n, eps->resid_buf, V->red, V->red_len,
                                       V->stream));

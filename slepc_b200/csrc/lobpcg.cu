@@ -169,7 +169,7 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
   }
   if (!eps->V) B200_CHECK(b200_bv_create(n, ncv, eps->stream, &eps->V));
   b200_bv V = eps->V;
-  if (!eps->resid_buf) B200_CUDA_CHECK(cudaMalloc(&eps->resid_buf, sizeof(double) * 8));
+  if (!eps->resid_buf) B200_CUDA_CHECK(dev_malloc(&eps->resid_buf, sizeof(double) * 8));
   B200_CUDA_CHECK(cudaMemsetAsync(V->V, 0, sizeof(double) * V->ld * (size_t)(V->m + 1), V->stream));
   V->nrand = 0;
   Blocks B;
@@ -191,9 +191,9 @@ b200_status b200::lobpcg_solve(b200_eps eps) {
   if (eps->pc == B200_PC_JACOBI) {
     B200_ARG_CHECK(A->kind == kMatCsr && !A->a.f32, "the Jacobi preconditioner needs an FP64 CSR operator");
     if (eps->dinv_of != (const void *)A) {
-      cudaFree(eps->dinv);
+      dev_free(eps->dinv);
       eps->dinv = nullptr;
-      B200_CUDA_CHECK(cudaMalloc(&eps->dinv, sizeof(double) * (size_t)n));
+      B200_CUDA_CHECK(dev_malloc(&eps->dinv, sizeof(double) * (size_t)n));
       B200_CUDA_CHECK(inverse_diagonal_launch(n, A->a.rowptr, A->a.colind, static_cast<const double *>(A->a.vals),
                                               eps->dinv, eps->stream));
       eps->dinv_of = A;

@@ -110,6 +110,10 @@ __device__ __forceinline__ bool consumer_sync_or(bool v) {
       : "memory");
   return out != 0;
 }
+// Barrier 1 over the consumer warps only, without a vote.
+__device__ __forceinline__ void consumer_sync() {
+  asm volatile("bar.sync 1, %0;" ::"n"(kConsumers) : "memory");
+}
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -300,6 +304,7 @@ __global__ void __launch_bounds__(kThreads, ctas_per_sm<TS>()) gs_pass_kernel(Pa
   DecideShared *dsh = reinterpret_cast<DecideShared *>(cacc + kMaxCols + 1);
   __shared__ int is_last, timed_out, n_issued;
   __shared__ double upd[2 * kConsumers];      // partial update sums (TPR*CH = kConsumers per chunk), by chunk parity
+  __shared__ double wps[kMaxChunk];           // w' of the current chunk (updated and scaled), read by the dot
   __shared__ float coef32_s[sizeof(TS) == sizeof(float) ? kMaxCols : 1];  // FP32 coefficients (fast update)
   const size_t head = 128 + sizeof(double) * (2 * kMaxCols + 1) + ((sizeof(DecideShared) + 127) / 128) * 128;
   unsigned char *stage_base = smem_raw + ((head + 127) / 128) * 128;
@@ -361,8 +366,9 @@ __global__ void __launch_bounds__(kThreads, ctas_per_sm<TS>()) gs_pass_kernel(Pa
     // Update mapping: the chunk's rows form CH/32 groups of 32; the 8 consumer warps split into
     // TPR = 8/(CH/32) parts, warp w taking row group w % (CH/32) and columns part, part+TPR, ...
     // (one column, 32 consecutive rows per instruction: no bank conflicts).  Partial sums meet
-    // in upd[part][row] behind the chunk's barrier; each warp then folds them into w' while it
-    // runs the dot, and warp g writes row group g of w' back to global memory.
+    // in upd[part][row] behind the chunk's barrier; consumer thread r then folds them into row r
+    // of w' (fixed order), keeps it in wps for the dot and writes it back to global memory, and
+    // a second barrier hands wps to the dot.
     const int groups = CH / 32;  // 1..8
     const int TPR = kConsumerWarps / groups;
     const int part = warp / groups;
@@ -417,28 +423,29 @@ __global__ void __launch_bounds__(kThreads, ctas_per_sm<TS>()) gs_pass_kernel(Pa
       } else if (!ok) {
         break;
       }
-      // w' = w - sum of the parts (fixed order), scaled; used by the dot, written by one warp
-      auto wprime = [&](int r) -> double {
-        double wv = wsrc[r];
-        if (do_update) {
-          double tot = 0.0;
-          for (int q = 0; q < TPR; ++q) tot += up[q * CH + r];
-          wv -= tot;
+      // w' = w - sum of the parts (fixed order), scaled: once per row, for the dot and global memory
+      if (rewrite) {
+        for (int r = tid; r < rows; r += kConsumers) {
+          double wv = wsrc[r];
+          if (do_update) {
+            double tot = 0.0;
+            for (int q = 0; q < TPR; ++q) tot += up[q * CH + r];
+            wv -= tot;
+          }
+          if (do_scale) wv *= scale;
+          wps[r] = wv;
+          Vw[r0 + r] = wv;
         }
-        if (do_scale) wv *= scale;
-        return wv;
-      };
-      if (rewrite && warp < groups) {
-        const int r = warp * 32 + lane;
-        if (r < rows) Vw[r0 + r] = wprime(r);
+        if (do_dot) consumer_sync();
       }
+      const double *wd = rewrite ? wps : wsrc;  // the vector the dot multiplies
       if (do_dot && fast_dot) {
         // FP32 products summed in FP32 over the chunk's rows of this lane, then added in FP64
         float facc[MAXCPW];
 #pragma unroll
         for (int t = 0; t < MAXCPW; ++t) facc[t] = 0.f;
         for (int r = lane; r < rows; r += 32) {
-          const float wr = __double2float_rn(rewrite ? wprime(r) : wsrc[r]);
+          const float wr = __double2float_rn(wd[r]);
 #pragma unroll
           for (int t = 0; t < MAXCPW; ++t) {
             const int c = warp + kConsumerWarps * t;
@@ -450,7 +457,7 @@ __global__ void __launch_bounds__(kThreads, ctas_per_sm<TS>()) gs_pass_kernel(Pa
         for (int t = 0; t < MAXCPW; ++t) acc[t] += (double)facc[t];
       } else if (do_dot) {
         for (int r = lane; r < rows; r += 32) {
-          const double wr = rewrite ? wprime(r) : wsrc[r];
+          const double wr = wd[r];
 #pragma unroll
           for (int t = 0; t < MAXCPW; ++t) {
             const int c = warp + kConsumerWarps * t;

@@ -274,6 +274,11 @@ template <int MAXCPW, typename TS>
 __global__ void __launch_bounds__(kThreads, ctas_per_sm<TS>()) gs_pass_kernel(PassParams p,
                                                                              const __grid_constant__ CUtensorMap tmap) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  // Launched as a programmatic dependent of the previous kernel in the stream: wait until that
+  // grid has finished and its writes (the control block, coefficients, w) are visible, then let
+  // the next pass be launched at once (its CTAs take each SM as this grid's CTA leaves it).
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" :::);
   GsState *st = p.st;
   const GsPassArgs &a = p.a;
   if (a.step >= 0 && st->halt && st->halt_step < a.step) return;
@@ -598,8 +603,17 @@ cudaError_t launch_pass_t(const PassParams &p, const CUtensorMap &tm, size_t sme
     if (e != cudaSuccess) return e;
     attr_set[dev] = true;
   }
-  gs_pass_kernel<M, TS><<<p.G, kThreads, smem, stream>>>(p, tm);
-  return cudaGetLastError();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)p.G);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, gs_pass_kernel<M, TS>, p, tm);
 }
 
 cudaError_t launch_pass(const GsPassArgs &a, const GsWork &w, int first, int plain_dot, cudaStream_t stream) {

@@ -601,8 +601,7 @@ def run_b200_cross(args):
                              "bound": "hbm", "achieved": spmv_gbs, "peak": peak, "unit": "GB/s",
                              "frac": (spmv_gbs / peak) if spmv_gbs else None, "peak_kind": peak_kind,
                              "traffic": None, "gs_achieved": gs_gbs,
-                             "share_orth": (tstats["ms_orth"] / tstats["ms_total"] if tstats["ms_total"] and not mixed
-                                            else None),
+                             "share_orth": tstats["ms_orth"] / tstats["ms_total"] if tstats["ms_total"] else None,
                              "share_spmv": tstats["ms_spmv"] / tstats["ms_total"] if tstats["ms_total"] else None,
                              "share_restart": tstats["ms_restart"] / tstats["ms_total"] if tstats["ms_total"] else None},
                 "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},

@@ -27,9 +27,10 @@ template <typename TX, int BP>
 struct Map {
   static constexpr int VEC = 16 / (int)sizeof(TX);
   static constexpr int NVEC = BP / VEC;
-  // FP32 64-column blocks: 8 lanes per row with two vectors each (4 rows per warp iteration: twice
-  // the gathers in flight per warp, 7% faster than 16 lanes x one vector on the 128^3 Laplacian)
-  static constexpr int LPR = (sizeof(TX) == 4 && BP == 64) ? 8 : (NVEC < 32 ? NVEC : 32);
+  // 64-column blocks: FP32 with 8 lanes per row and two vectors each (4 rows per warp iteration:
+  // twice the gathers in flight per warp, 7% faster than 16 lanes x one vector on the 128^3
+  // Laplacian), FP64 with 16 lanes per row and two vectors each (2 rows per warp iteration)
+  static constexpr int LPR = (BP == 64) ? (sizeof(TX) == 4 ? 8 : 16) : (NVEC < 32 ? NVEC : 32);
   static constexpr int CPL = NVEC / LPR;
   static constexpr int RPI = 32 / LPR;
 };

@@ -218,6 +218,10 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_sell_kernel(int nslices, in
                                                                  const int *__restrict__ scol,
                                                                  const XT *__restrict__ x, double *__restrict__ y,
                                                                  const GsState *__restrict__ st, int step) {
+  // Launched as a programmatic dependent of the previous kernel (the Gram-Schmidt pass that wrote
+  // x): wait for that grid and its writes, then let the next kernel be launched.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" :::);
   if (st && st->halt && st->halt_step < step) return;
   const int lane = threadIdx.x & 31;
   const int nwarps = gridDim.x * (kSpmvThreads / 32);
@@ -544,8 +548,19 @@ cudaError_t spmv_sell_launch_t(const SpmvSell &S, const VT *svals, int n, const 
   if (S.nslices > 0) {
     int grid = (S.nslices + kSpmvThreads / 32 - 1) / (kSpmvThreads / 32);
     if (grid > sms * per_sm) grid = sms * per_sm;
-    spmv_sell_kernel<VT, XT><<<grid, kSpmvThreads, 0, stream>>>(S.nslices, n, S.off, S.width, S.mask, svals, S.cols, x,
-                                                                y, st, step);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kSpmvThreads);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, spmv_sell_kernel<VT, XT>, S.nslices, n, (const long long *)S.off,
+                                       (const int *)S.width, (const unsigned *)S.mask, svals, (const int *)S.cols, x,
+                                       y, st, step);
+    if (e != cudaSuccess) return e;
     count_launch();
   }
   if (rest.ntiles > 0 || rest.nsegs > 0) {

@@ -131,10 +131,17 @@ cudaError_t dev_malloc(void **p, size_t bytes) {
 
 void dev_free(void *p) {
   if (!p) return;
-  int dev = 0;
-  cudaGetDevice(&dev);
+  // the buffer's own device (an object may be destroyed while another device is current)
+  int cur = 0, dev = 0;
+  cudaGetDevice(&cur);
+  dev = cur;
+  cudaPointerAttributes pa;
+  if (cudaPointerGetAttributes(&pa, p) == cudaSuccess && pa.type == cudaMemoryTypeDevice) dev = pa.device;
+  else cudaGetLastError();
+  if (dev != cur) cudaSetDevice(dev);
   cudaDeviceSynchronize();
   cudaFreeAsync(p, alloc_stream(dev));
+  if (dev != cur) cudaSetDevice(cur);
 }
 
 int num_sms_host() {

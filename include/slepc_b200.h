@@ -167,7 +167,10 @@ b200_status b200_bv_get_active_columns(b200_bv bv, int *l, int *k);
 b200_status b200_bv_set_orthog_eta(b200_bv bv, double eta);
 /* BVSetOrthogonalization / BVGetOrthogonalization block type (BVOrthogBlockType,
  * include/slepcbv.h:84-88; bvbasic.c:975-987; default GS, bvfunc.c:179): the
- * method of b200_bv_orthogonalize.  TSQR and TSQRCHOL return B200_ERR_SUP. */
+ * method of b200_bv_orthogonalize.  TSQR and TSQRCHOL (bvorthog.c:615-660) run
+ * the Householder QR of the active columns on the device with one process's
+ * semantics of bvlapack.c:347-560 (geqrf + orgqr; R with LAPACK's signs);
+ * TSQRCHOL factors a copy and applies R^{-1}.  Both need n >= k - l. */
 #define B200_ORTHOG_BLOCK_GS 0
 #define B200_ORTHOG_BLOCK_CHOL 1
 #define B200_ORTHOG_BLOCK_TSQR 2

@@ -427,7 +427,8 @@ class BV:
     """Column-major basis of vectors resident in HBM (the new BV type)."""
 
     class OrthogBlockType:
-        """BVOrthogBlockType (include/slepcbv.h:84-88); TSQR and TSQRCHOL are not provided."""
+        """BVOrthogBlockType (include/slepcbv.h:84-88); TSQR and TSQRCHOL are the Householder QR of
+        the active columns on the device (one process's geqrf + orgqr, R with LAPACK's signs)."""
         GS, CHOL, TSQR, TSQRCHOL, SVQB = 0, 1, 2, 3, 4
 
     def __init__(self):

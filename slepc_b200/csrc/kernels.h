@@ -179,6 +179,14 @@ cudaError_t csr_transpose_device(int rows, int cols, long long nnz, const int *r
 // gave up.
 cudaError_t panel_gemm_error(int *err, cudaStream_t stream);
 // V(:,s:e) = V(:,l:k) * Q(l:k,s:e), row-blocked, in place; Q points at element (l,s).
+// Householder QR of an n x nc column-major block (tsqr.cu): geqr2 in place (R above the diagonal,
+// reflectors below, tau), and org2r (the block overwritten with Q).  work: householder_qr_parts(n)
+// * (nc + 1) + nc doubles; scale: nc doubles.
+int householder_qr_parts(int n);
+cudaError_t householder_qr_launch(double *X, long long ld, int n, int nc, double *tau, double *scale, double *work,
+                                  cudaStream_t s);
+cudaError_t householder_q_launch(double *X, long long ld, int n, int nc, const double *tau, double *work,
+                                 cudaStream_t s);
 cudaError_t multinplace_launch(double *V, int ld, int n, int l, int k, const double *Q, int ldq, int s, int e,
                                cudaStream_t stream);
 // The same on an FP32 basis (products and sums FP64, results rounded to FP32).

@@ -803,12 +803,7 @@ extern "C" b200_status b200_bv_set_orthog_eta(b200_bv bv, double eta) {
 
 extern "C" b200_status b200_bv_set_orthog_block(b200_bv bv, int type) {
   B200_ARG_CHECK(bv, "null BV");
-  if (type == B200_ORTHOG_BLOCK_TSQR || type == B200_ORTHOG_BLOCK_TSQRCHOL) {
-    b200_set_last_error(__FILE__, __LINE__, "the TSQR block orthogonalizations are not supported");
-    return B200_ERR_SUP;
-  }
-  B200_ARG_CHECK(type == B200_ORTHOG_BLOCK_GS || type == B200_ORTHOG_BLOCK_CHOL || type == B200_ORTHOG_BLOCK_SVQB,
-                 "unknown block orthogonalization type");
+  B200_ARG_CHECK(type >= B200_ORTHOG_BLOCK_GS && type <= B200_ORTHOG_BLOCK_SVQB, "unknown block orthogonalization type");
   bv->orthog_block = type;
   return B200_OK;
 }
@@ -1266,10 +1261,86 @@ static b200_status bv_orthogonalize_gram(b200_bv bv, double *R, int ldr) {
   return bv_gram_finish(bv, R, ldr);
 }
 
+// BVOrthogonalize_TSQR / _TSQRCHOL (bvorthog.c:615-660) on one process: block Gram-Schmidt
+// against the leading l columns (BVOrthogonalize_BlockGS, bvorthog.c:492-502), then the
+// Householder QR of V(:, l:k) on the device (bvlapack.c:347-440 with one rank: geqrf + orgqr; for
+// TSQRCHOL only R, from a copy, then V(:, l:k) := V(:, l:k) R^{-1} as BVMatTriInv_LAPACK_Private
+// and BVMultInPlace do).  R(0:l, l:k) holds the Gram-Schmidt coefficients, R(l:k, l:k) the
+// triangular factor with LAPACK's signs.
+static b200_status bv_orthogonalize_tsqr(b200_bv bv, double *R, int ldr) {
+  const int l = bv->l, k = bv->k, nc = k - l, n = bv->n, ld = bv->ld;
+  if (nc <= 0) return B200_OK;
+  if (n < nc) {
+    b200_set_last_error(__FILE__, __LINE__, "TSQR needs at least as many rows as active columns");
+    return B200_ERR_SUP;
+  }
+  const bool chol = bv->orthog_block == B200_ORTHOG_BLOCK_TSQRCHOL;
+  cudaStream_t s = bv->stream;
+  std::vector<double> C((size_t)l * nc);
+  if (l > 0) {
+    const size_t nC = (size_t)l * nc;
+    const int cps_c = dot_ctas_per_sm(nc, l);
+    B200_CHECK(bv_reserve(bv, nC, nC * cps_c * num_sms_host()));
+    B200_CUDA_CHECK(dot_launch(col(bv, l), ld, nc, bv->V, ld, l, n, bv->qbuf, l, bv->red, bv->red_len, s, cps_c));
+    B200_CUDA_CHECK(mult_launch(col(bv, l), ld, bv->V, ld, n, l, nc, bv->qbuf, l, -1.0, 1.0, s));
+    B200_CUDA_CHECK(cudaMemcpyAsync(C.data(), bv->qbuf, sizeof(double) * nC, cudaMemcpyDeviceToHost, s));
+  }
+  const size_t wlen = (size_t)householder_qr_parts(n) * (nc + 1) + 3 * (size_t)nc;
+  double *work = nullptr, *copy = nullptr;
+  B200_CUDA_CHECK(dev_malloc(&work, sizeof(double) * wlen));
+  double *tau = work + (wlen - 2 * (size_t)nc), *scale = work + (wlen - (size_t)nc);
+  if (chol && dev_malloc(&copy, sizeof(double) * (size_t)ld * nc) != cudaSuccess) {
+    dev_free(work);
+    b200_set_last_error(__FILE__, __LINE__, "device allocation failed for the TSQRCHOL copy");
+    return B200_ERR_NOMEM;
+  }
+  double *X = chol ? copy : col(bv, l);
+  cudaError_t e = cudaSuccess;
+  if (chol) e = cudaMemcpyAsync(copy, col(bv, l), sizeof(double) * (size_t)ld * nc, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess) e = householder_qr_launch(X, ld, n, nc, tau, scale, work, s);
+  std::vector<double> Rf((size_t)nc * nc, 0.0);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(Rf.data(), sizeof(double) * nc, X, sizeof(double) * ld, sizeof(double) * nc, nc,
+                          cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && !chol) e = householder_q_launch(X, ld, n, nc, tau, work, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  dev_free(copy);
+  dev_free(work);
+  if (e != cudaSuccess) {
+    b200_set_last_error(__FILE__, __LINE__, cudaGetErrorString(e));
+    return B200_ERR_CUDA;
+  }
+  for (int j = 0; j < nc; ++j)
+    for (int i = j + 1; i < nc; ++i) Rf[(size_t)j * nc + i] = 0.0;
+  if (chol) {
+    std::vector<double> S = Rf;
+    int info = 0;
+    scipy_dtrtri_("U", "N", &nc, S.data(), &nc, &info, 1, 1);
+    if (info) {
+      b200_set_last_error(__FILE__, __LINE__, "LAPACK dtrtri failed in BVOrthogonalize (TSQRCHOL)");
+      return B200_ERR_LAPACK;
+    }
+    B200_CHECK(bv_reserve(bv, (size_t)nc * nc, 0));
+    B200_CUDA_CHECK(hpin_acquire(bv));
+    memcpy(bv->hpin, S.data(), sizeof(double) * (size_t)nc * nc);
+    B200_CUDA_CHECK(cudaMemcpyAsync(bv->qbuf, bv->hpin, sizeof(double) * (size_t)nc * nc, cudaMemcpyHostToDevice, s));
+    B200_CUDA_CHECK(hpin_release(bv));
+    B200_CUDA_CHECK(multinplace_launch(bv->V, ld, n, l, k, bv->qbuf, nc, l, k, s));
+  }
+  if (R) {
+    for (int j = 0; j < nc; ++j) {
+      for (int i = 0; i < l; ++i) R[i + (size_t)(l + j) * ldr] = C[i + (size_t)j * l];
+      for (int i = 0; i < nc; ++i) R[l + i + (size_t)(l + j) * ldr] = Rf[i + (size_t)j * nc];
+    }
+  }
+  return B200_OK;
+}
+
 namespace b200 {
 b200_status bv_orthogonalize_pair(b200_bv a, b200_bv b) {
   B200_ARG_CHECK(a && b && a != b, "invalid BVOrthogonalize pair");
-  const bool gram = a->orthog_block != B200_ORTHOG_BLOCK_GS && b->orthog_block != B200_ORTHOG_BLOCK_GS;
+  auto is_gram = [](int t) { return t == B200_ORTHOG_BLOCK_CHOL || t == B200_ORTHOG_BLOCK_SVQB; };
+  const bool gram = is_gram(a->orthog_block) && is_gram(b->orthog_block);
   if (!gram || a->stream != b->stream) {
     B200_CHECK(b200_bv_orthogonalize(a, nullptr, 0));
     return b200_bv_orthogonalize(b, nullptr, 0);
@@ -1284,6 +1355,8 @@ b200_status bv_orthogonalize_pair(b200_bv a, b200_bv b) {
 
 extern "C" b200_status b200_bv_orthogonalize(b200_bv bv, double *R, int ldr) {
   B200_ARG_CHECK(bv && (!R || ldr >= bv->k), "R leading dimension too small");
+  if (bv->orthog_block == B200_ORTHOG_BLOCK_TSQR || bv->orthog_block == B200_ORTHOG_BLOCK_TSQRCHOL)
+    return bv_orthogonalize_tsqr(bv, R, ldr);
   if (bv->orthog_block != B200_ORTHOG_BLOCK_GS) return bv_orthogonalize_gram(bv, R, ldr);
   if (!R) return bv_orthogonalize_block(bv);
   for (int j = bv->l; j < bv->k; ++j) {
@@ -1746,12 +1819,7 @@ extern "C" b200_status b200_eps_set_preconditioner(b200_eps eps, int pc) {
 
 extern "C" b200_status b200_eps_set_bv_orthog_block(b200_eps eps, int type) {
   B200_ARG_CHECK(eps, "null EPS");
-  if (type == B200_ORTHOG_BLOCK_TSQR || type == B200_ORTHOG_BLOCK_TSQRCHOL) {
-    b200_set_last_error(__FILE__, __LINE__, "the TSQR block orthogonalizations are not supported");
-    return B200_ERR_SUP;
-  }
-  B200_ARG_CHECK(type == B200_ORTHOG_BLOCK_GS || type == B200_ORTHOG_BLOCK_CHOL || type == B200_ORTHOG_BLOCK_SVQB,
-                 "unknown block orthogonalization type");
+  B200_ARG_CHECK(type >= B200_ORTHOG_BLOCK_GS && type <= B200_ORTHOG_BLOCK_SVQB, "unknown block orthogonalization type");
   eps->orthog_block = type;
   if (eps->V) eps->V->orthog_block = type;
   return B200_OK;

@@ -141,12 +141,12 @@ def test_bv_orthogonalize_block_types_vs_oracle(oracle_mod, block, l):
     assert np.abs(V @ R[:, l:] - V0[:, l:]).max() < 1e-11
 
 
-def test_bv_orthog_block_unsupported_and_breakdown():
+def test_bv_orthog_block_unknown_type_and_breakdown():
     bv = S.BV().create(100, 4)
     with pytest.raises(S.B200Error):
-        bv.setOrthogonalizationBlock(S.BV.OrthogBlockType.TSQR)
-    with pytest.raises(S.B200Error):
         bv.setOrthogonalizationBlock(7)
+    with pytest.raises(S.B200Error):
+        bv.setOrthogonalizationBlock(-1)
     # a zero column: SVQB reports a breakdown instead of dividing by zero
     x = np.random.default_rng(0).standard_normal(100)
     bv.setColumns(np.stack([x, np.zeros(100), x + 1, np.ones(100)], axis=1))

@@ -127,7 +127,7 @@ def test_oracle_sample_mode_stops(oracle_mod):
 def test_bv_test11_block_orthogonalization_golden(oracle_mod, block):
     """src/sys/classes/bv/tests/test11.c with -bv_orthog_block chol / svqb (-resid for test11_6):
     columns [0,l) and then [l,k) orthogonalized, every check the expected output lists below
-    100 eps.  (Gram-Schmidt is pinned by test2; the TSQR types are not provided.)"""
+    100 eps.  (Gram-Schmidt is pinned by test2; the TSQR types by tests/test_gpu_tsqr.py.)"""
     g = H.golden("bv_test11.json")
     eps = np.finfo(float).eps
     t = {"chol": oracle_mod.ORTHOG_BLOCK_CHOL, "svqb": oracle_mod.ORTHOG_BLOCK_SVQB}[block]

@@ -1,4 +1,4 @@
-"""Static check of bench.py: every name a function reads is bound somewhere.
+"""Static check of bench.py and kernel_bench.py: every name a function reads is bound.
 
 The workload paths of bench.py (cross, batched, learned) run only on a GPU, so a
 name left over from another workload's code would first fail there, after the
@@ -10,6 +10,8 @@ builtins.
 import ast
 import builtins
 import os
+
+import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -33,8 +35,9 @@ def _bound_in(node):
     return names
 
 
-def test_bench_functions_read_only_bound_names():
-    with open(os.path.join(ROOT, "bench.py")) as f:
+@pytest.mark.parametrize("path", ["bench.py", os.path.join("slepc_b200", "kernel_bench.py")])
+def test_bench_functions_read_only_bound_names(path):
+    with open(os.path.join(ROOT, path)) as f:
         tree = ast.parse(f.read())
     module = set(dir(builtins))
     for node in tree.body:

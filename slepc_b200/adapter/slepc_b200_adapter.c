@@ -405,8 +405,8 @@ static PetscErrorCode BVDuplicate_B200(BV V, BV W)
 
   PetscFunctionBegin;
   B200Call(b200_bv_set_orthog_eta(w->bv, V->orthog_eta));
-  if (V->orthog_block == BV_ORTHOG_BLOCK_CHOL) B200Call(b200_bv_set_orthog_block(w->bv, B200_ORTHOG_BLOCK_CHOL));
-  else if (V->orthog_block == BV_ORTHOG_BLOCK_SVQB) B200Call(b200_bv_set_orthog_block(w->bv, B200_ORTHOG_BLOCK_SVQB));
+  /* B200_ORTHOG_BLOCK_* number the five BVOrthogBlockType values in the same order */
+  B200Call(b200_bv_set_orthog_block(w->bv, (int)V->orthog_block));
   PetscFunctionReturn(PETSC_SUCCESS);
 }
 
